@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the single-phase RK3 step: cell-RK3-steps/s, FP32-mixed vs plain FP64.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl dfdm|reference] [--config chan550]
+
+Workload (default): the Re_tau = 550 constant-flux channel DNS on 256 x 192 x 256 cells (tanh-stretched y,
+periodic x/z), seeded Poiseuille + 10 % uniform-noise initial condition.  One step = one full
+compute_time_step_RK3 (three stages: RHS + RK update, projection, constant-flux shift).  The state is resident
+in HBM; the per-step working set (~0.6 GB FP32) exceeds the 126 MB L2, so no flush is needed between steps.
+
+With N > 1 (torchrun) every rank advances its own independent replica of the case (the requests of the serving
+loop shard this way; there is no data-path collective): value = N * cells * K / max-over-ranks(time).
+
+`--impl reference` times the reference's algorithm on the host cores instead: the reference's Fortran/MPI build
+cannot be built here, so this is the repository's FP64 C++ restatement (the oracle), OpenMP over all host cores,
+on a bounded sample of the same workload (whole RK3 steps of the same grid, as many as fit in ~90 s).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "dopamine-fdm_b200"))
+
+import numpy as np  # noqa: E402
+
+from dfdm import cases  # noqa: E402
+
+METRIC = "cell-RK3-steps/s"
+UNIT = "cell-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="dfdm", choices=["dfdm", "reference"])
+    ap.add_argument("--config", default="chan550")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def workload_name(c):
+    Nx, Ny, Nz = c.cells
+    return f"{c.name}: {Nx}x{Ny}x{Nz} cells"
+
+
+def config_dict(c, extra=None):
+    d = {"workload": workload_name(c), "grid_faces": [c.nx, c.ny, c.nz], "cells": c.n_cells,
+         "y": "walls, tanh alpha=%g" % c.alpha_grid if c.y_bc_type == 1 else "periodic",
+         "nu": c.nu, "dt": c.dt, "sgs_model": c.sgs_model, "flow_forcing_mode": c.flow_forcing_mode,
+         "ic": c.ic, "seed": c.seed, "l2": "per-step working set larger than the 126 MB L2 (no flush)"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+# ---------------------------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.strip().split(",") for r in self.f.read().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------------------------
+def run_reference(args, c):
+    """Reference arm: the FP64 C++ restatement of the reference (oracle), OpenMP on all host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.build()
+    ncores = os.cpu_count() or 1
+    oracle.set_threads(ncores)
+    o = oracle.Oracle(c)
+    U, V, W, P = cases.initial_condition(c)
+    o.set_state(U, V, W, P)
+    budget = 90.0
+    t0 = time.perf_counter()
+    o.step(1)   # warm-up: first touch of every array
+    t_first = time.perf_counter() - t0
+    n = 0
+    t0 = time.perf_counter()
+    while n < max(1, args.steps):
+        o.step(1)
+        n += 1
+        if time.perf_counter() - t0 + t_first > budget:
+            break
+    el = time.perf_counter() - t0
+    value = c.n_cells * n / el
+    sample = f"{n} full RK3 steps of the {workload_name(c)} case after 1 warm-up step"
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": n, "warmup": 1,
+            "ms_per_step": 1e3 * el / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded Poiseuille + 10% uniform noise)",
+            "config": config_dict(c), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": "port", "sample": sample,
+                             "note": "reference Fortran/MPI build unavailable on this box; FP64 C++ restatement"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def cpu_baseline(c, seconds):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.build()
+    ncores = os.cpu_count() or 1
+    oracle.set_threads(ncores)
+    o = oracle.Oracle(c)
+    U, V, W, P = cases.initial_condition(c)
+    o.set_state(U, V, W, P)
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        o.step(1)
+        n += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    el = time.perf_counter() - t0
+    o.close()
+    return {"value": c.n_cells * n / el, "unit": UNIT, "cores": ncores, "kind": "port",
+            "sample": f"{n} full RK3 step(s) of the {workload_name(c)} case from the initial condition "
+                      f"(FP64 C++ restatement, OpenMP on {ncores} threads)"}
+
+
+# ---------------------------------------------------------------------------------------------------------------
+def main():
+    args = parse()
+    ws, rank, local = dist_env()
+    c = cases.get(args.config)
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args, c)), flush=True)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from dfdm.native import KERNELS, Solver
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sh = stream.cuda_stream
+
+    def barrier_sync():
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    U, V, W, P = cases.initial_condition(c)
+
+    def timed_run(prec, sample_clocks=False):
+        s = Solver(c, prec, graphs=True)
+        s.set_stream(sh)
+        s.set_state(U, V, W, P)
+        s.compute_time_step_RK3(args.warmup)
+        barrier_sync()
+        l0 = s.launch_count()
+        clk = ClockSampler(local) if sample_clocks else None
+        if clk:
+            clk.start()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.compute_time_step_RK3_async(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+        clocks = clk.stop() if clk else None
+        ms = e0.elapsed_time(e1)
+        barrier_sync()
+        launches = s.launch_count() - l0
+        return s, max_over_ranks(ms), clocks, launches
+
+    s32, ms32, clocks, launches = timed_run("fp32", sample_clocks=True)
+    value = ws * c.n_cells * args.steps / (ms32 / 1e3)
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "fp32-mixed (FP32 fields/stencils/FFTs, FP64 y-solves and reductions)",
+           "data": "synthetic: seeded laminar Poiseuille + 10% uniform noise, no dataset",
+           "config": config_dict(c, {"parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"}),
+           "clocks": clocks, "gpu_launches": launches}
+
+    # ---- plain FP64 form and the FP32-vs-FP64 error after warmup + K steps from the same state ----
+    if not args.no_fp64:
+        s64, ms64, _, _ = timed_run("fp64")
+        v64 = ws * c.n_cells * args.steps / (ms64 / 1e3)
+        a = s32.get_state()
+        b = s64.get_state()
+        rel = {k: float(np.linalg.norm((x - y).ravel()) / max(np.linalg.norm(y.ravel()), 1e-300))
+               for k, x, y in zip("UVWP", a, b)}
+        out["fp64"] = {"value": v64, "ms_per_step": ms64 / args.steps,
+                       "fp32_speedup": value / v64,
+                       "rel_l2_fp32_vs_fp64": rel, "steps_compared": args.warmup + args.steps}
+        s64.close()
+
+    # ---- roofline: per-kernel-family device time of one stage, dominant family against HBM peak ----
+    peak, peak_kind = measured_peaks()
+    fams = ["stage", "fwd_x", "fwd_z", "y_solve", "inv_z", "inv_x", "correct"]
+    iters = 20
+    kt = {}
+    for fam in fams:
+        for _ in range(3):
+            s32.launch_kernel_async(fam, 2)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(iters):
+            s32.launch_kernel_async(fam, 2)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / iters
+        b = s32.kernel_bytes(fam)
+        kt[fam] = {"ms": ms, "alg_bytes": b, "GBps": b / (ms * 1e-3) / 1e9, "frac": b / (ms * 1e-3) / 1e9 / peak}
+    dom = max(kt, key=lambda k: kt[k]["ms"])
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        try:
+            traffic = json.load(open(tfile)).get(c.name, {}).get(dom)
+        except Exception:
+            traffic = None
+    out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": kt[dom]["GBps"], "peak": peak, "unit": "GB/s",
+                       "frac": kt[dom]["GBps"] / peak, "traffic": traffic, "peak_kind": peak_kind,
+                       "alg_bytes_per_launch": kt[dom]["alg_bytes"], "avg_launch_ms": kt[dom]["ms"]}
+    # whole-step roofline of the M1 model: 88 words per cell-step + 2 for the constant-flux shift
+    words = 88 + (2 if c.flow_forcing_mode == 1 else 0)
+    step_bytes = words * 4 * c.n_cells
+    out["step_roofline"] = {"model": f"M1 {words} words/cell-step", "bytes_per_step": step_bytes,
+                            "achieved_GBps": step_bytes / (ms32 / args.steps * 1e-3) / 1e9,
+                            "frac_of_peak": step_bytes / (ms32 / args.steps * 1e-3) / 1e9 / peak}
+    out["kernels"] = kt
+
+    # ---- end to end through the C ABI with host buffers (the reference's FP64 ghosted arrays, pinned) ----
+    if not args.no_e2e:
+        shp = c.shapes()
+
+        def pinned(key):
+            n1, n2, n3 = shp[key]
+            t = torch.empty((n3, n2, n1), dtype=torch.float64, pin_memory=True)
+            return t.numpy().T   # Fortran-ordered view of pinned memory
+
+        hU, hV, hW, hP = pinned("U"), pinned("V"), pinned("W"), pinned("P")
+        hU[...] = U; hV[...] = V; hW[...] = W; hP[...] = P
+        oU, oV, oW, oP = pinned("U"), pinned("V"), pinned("W"), pinned("P")
+        ne = max(1, min(args.steps, 10))
+        s32.set_state(hU, hV, hW, hP)
+        s32.compute_time_step_RK3(1)
+        barrier_sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(ne):
+            s32.set_state(hU, hV, hW)                 # H2D of the step's input state
+            s32.compute_time_step_RK3(1)
+            s32.get_state((oU, oV, oW, oP))           # D2H of the step's result
+        e1.record(stream)
+        e1.synchronize()
+        ms_e = max_over_ranks(e0.elapsed_time(e1))
+        bi = 8 * (hU.size + hV.size + hW.size)
+        bo = 8 * (oU.size + oV.size + oW.size + oP.size)
+        out["e2e"] = {"value": ws * c.n_cells * ne / (ms_e / 1e3), "unit": UNIT, "h2d_bytes_per_step": bi,
+                      "d2h_bytes_per_step": bo, "steps": ne,
+                      "path": "dfdm_set_state(U,V,W) + dfdm_compute_time_step_rk3(1) + dfdm_get_state(U,V,W,P) "
+                              "per step, FP64 ghosted host arrays in pinned memory"}
+
+    # ---- CPU baseline: the FP64 restatement on the host cores (rank 0 at N = 1 only) ----
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(c, args.cpu_seconds)
+
+    s32.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1074 @@
+// dfdm_api.cu -- the C ABI (include/dfdm.h): context set-up, the RK3 step driver, state transfer and the unit
+// entry points that mirror the reference's Fortran subroutines.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "dfdm.h"
+#include "dfdm_common.cuh"
+#include "fft_smem.cuh"
+#include "kernels_diag.cuh"
+#include "kernels_poisson.cuh"
+#include "kernels_step.cuh"
+
+using namespace dfdm;
+
+namespace {
+
+thread_local std::string g_err;
+thread_local long long g_launches = 0;   // kernels enqueued by this thread (read back into the context)
+
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                       \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) {                                                                       \
+            return fail(e_ == cudaErrorMemoryAllocation ? DFDM_ERR_NOMEM : DFDM_ERR_CUDA,              \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+        }                                                                                              \
+    } while (0)
+
+#define CKL()                                                                                          \
+    do {                                                                                               \
+        cudaError_t e_ = cudaGetLastError();                                                           \
+        if (e_ != cudaSuccess) return fail(DFDM_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+        ++g_launches;                                                                                  \
+    } while (0)
+
+const double PI = 4.0 * std::atan(1.0);   // pi = 4d0*datan(1d0)
+const int MAX_NY = 1024;                  // y solve keeps Ny pivots per column in shared memory (8 KB per row of 32)
+
+}  // namespace
+
+// ----------------------------------------------------------------------------------------------------------------
+struct dfdm_ctx {
+    dfdm_params prm;
+    int prec = DFDM_FP64;
+    size_t ts = 8;                 // sizeof storage type
+    int nx = 0, ny = 0, nz = 0, nxg = 0, nyg = 0, nzg = 0;
+    int yper = 0;
+    Dims d{};
+    // host metrics (1-based, as the reference's arrays)
+    std::vector<double> x, y, z, xg, yg, zg;
+    double dx = 0, dz = 0, Ly = 0;
+    int nwl = 0, wm_filter_mode = 0, wm = 0, les = 0;
+    double dPdx = 0, dPdz = 0;
+    // device memory
+    std::vector<void *> allocs;
+    void *u = nullptr, *v = nullptr, *w = nullptr, *uo = nullptr, *vo = nullptr, *wo = nullptr;
+    void *f1u = nullptr, *f1v = nullptr, *f1w = nullptr, *us = nullptr, *vs = nullptr, *wsf = nullptr;
+    void *nut = nullptr, *p = nullptr, *phi = nullptr, *spec = nullptr, *rhs3 = nullptr;
+    void *my_t = nullptr, *mz_t = nullptr;      // 6 metric arrays each, storage type
+    double *my_d = nullptr, *mz_d = nullptr;    // same in double
+    void *tw_x = nullptr, *twr_x = nullptr, *tw_z = nullptr, *tw_y = nullptr;
+    FFTPlan plan_x{}, plan_z{}, plan_y{};
+    double *d_kxx = nullptr, *d_kzz = nullptr, *d_kyy = nullptr, *d_lo = nullptr, *d_di = nullptr, *d_up = nullptr;
+    double *d_dxc = nullptr, *d_dyc = nullptr, *d_dzc = nullptr;
+    WallState wsd{};
+    double *red_part = nullptr, *red_out = nullptr;
+    int red_blocks = 0;
+    unsigned long long *d_maxdiv = nullptr;
+    int *d_flag = nullptr;
+    double *staging = nullptr;
+    size_t staging_n = 0;
+    // launch geometry
+    int lx = 8, tzx = 8;
+    size_t smem_x = 0, smem_z = 0, smem_y = 0, smem_ys = 0;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    double t = 0.0;
+    bool wmf_seeded = false;
+    // graphs
+    bool graphs = false;
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+    long long launches = 0;          // kernels enqueued (host-side count)
+    long long graph_launches = 0;    // kernels in the captured step graph
+};
+
+namespace {
+
+template <typename T> struct Impl;
+
+int dalloc(dfdm_ctx *c, void **p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(DFDM_ERR_NOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+    }
+    c->allocs.push_back(*p);
+    CK(cudaMemsetAsync(*p, 0, bytes, c->stream));
+    return DFDM_OK;
+}
+
+void centres_of(const std::vector<double> &f, int n, std::vector<double> &c) {
+    // src/initialization.f90:250-270 (f and c 1-based)
+    int nm = n - 1;
+    std::vector<double> m(nm + 1);
+    for (int i = 1; i <= nm; ++i) m[i] = 0.5 * (f[i] + f[i + 1]);
+    c.assign(nm + 3, 0.0);
+    for (int i = 1; i <= nm; ++i) c[i + 1] = m[i];
+    c[1] = m[1] - 2.0 * (m[1] - f[1]);
+    c[nm + 2] = m[nm] + 2.0 * (f[n] - m[nm]);
+}
+
+// Metric arrays of one direction, offset by one (index -1 valid), 6 arrays of length N+3 each:
+//   [0] dc, [1] df, [2] w0, [3] w1, [4] 1/dc, [5] 1/df  -- see Metric1D
+void build_metric(const std::vector<double> &f, const std::vector<double> &g, int nf, int N, std::vector<double> &out) {
+    const int L = N + 3;
+    out.assign(6 * (size_t)L, 0.0);
+    int ng = nf + 1;
+    for (int jp = -1; jp <= N + 1; ++jp) {
+        int j = jp + 2;   // reference index
+        size_t o = (size_t)(jp + 1);
+        if (j - 1 >= 1 && j <= nf) out[0 * L + o] = f[j] - f[j - 1];
+        if (j + 1 <= ng && j >= 1) out[1 * L + o] = g[j + 1] - g[j];
+        if (j >= 1 && j <= nf && j + 1 <= ng) {
+            double w0 = (g[j + 1] - f[j]) / (g[j + 1] - g[j]);
+            out[2 * L + o] = w0;
+            out[3 * L + o] = 1.0 - w0;
+        }
+        if (out[0 * L + o] != 0.0) out[4 * L + o] = 1.0 / out[0 * L + o];
+        if (out[1 * L + o] != 0.0) out[5 * L + o] = 1.0 / out[1 * L + o];
+    }
+}
+
+template <typename T> Metric1D<T> metric_view(void *base, int N) {
+    const int L = N + 3;
+    T *b = (T *)base;
+    Metric1D<T> m;
+    m.dc = b + 0 * L + 1; m.df = b + 1 * L + 1; m.w0 = b + 2 * L + 1; m.w1 = b + 3 * L + 1;
+    m.idc = b + 4 * L + 1; m.idf = b + 5 * L + 1;
+    return m;
+}
+
+template <typename T> int upload_as(dfdm_ctx *c, void **dst, const std::vector<double> &h) {
+    std::vector<T> tmp(h.size());
+    for (size_t i = 0; i < h.size(); ++i) tmp[i] = (T)h[i];
+    int rc = dalloc(c, dst, tmp.size() * sizeof(T));
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(*dst, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DFDM_OK;
+}
+
+template <typename T> int upload_twiddles(dfdm_ctx *c, void **dst, int n, int count) {
+    std::vector<double> h(2 * (size_t)count);
+    for (int k = 0; k < count; ++k) {
+        double a = -2.0 * PI * (double)k / (double)n;
+        h[2 * k] = std::cos(a);
+        h[2 * k + 1] = std::sin(a);
+    }
+    return upload_as<T>(c, dst, h);
+}
+
+template <typename T> StepArgs<T> step_args(dfdm_ctx *c) {
+    StepArgs<T> a;
+    a.d = c->d;
+    a.my = metric_view<T>(c->my_t, c->d.Ny);
+    a.mz = metric_view<T>(c->mz_t, c->d.Nz);
+    a.myd = metric_view<double>(c->my_d, c->d.Ny);
+    a.mzd = metric_view<double>(c->mz_d, c->d.Nz);
+    double inv_dx = 1.0 / c->dx;
+    a.nu = (T)c->prm.nu;
+    a.inv_dx = (T)inv_dx;
+    a.inv_dx2 = (T)(inv_dx * inv_dx);
+    a.dx2 = (T)(c->dx * c->dx);
+    a.dPdx = (T)c->dPdx;
+    a.dPdz = (T)c->dPdz;
+    a.w_adv = (T)((c->prm.advection_scheme == 1) ? 0.0 : 0.5);
+    a.nwl = c->nwl;
+    a.wm = c->wm;
+    a.sgs_model = c->prm.sgs_model;
+    a.C_amd = (T)c->prm.C_amd;
+    a.c_V = (T)(2.5 * c->prm.Cs_vreman * c->prm.Cs_vreman);
+    a.nu_d = c->prm.nu;
+    a.Ly = c->Ly;
+    a.yg2 = c->yg[2];
+    a.ygtop = c->Ly - c->yg[c->nyg - 1];
+    return a;
+}
+
+template <typename T> PoissonArgs<T> poisson_args(dfdm_ctx *c) {
+    PoissonArgs<T> a;
+    a.d = c->d;
+    a.my = metric_view<T>(c->my_t, c->d.Ny);
+    a.mz = metric_view<T>(c->mz_t, c->d.Nz);
+    a.inv_dx = (T)(1.0 / c->dx);
+    a.norm = (double)((long long)c->d.Nx * (long long)c->d.Nz);
+    a.pdiv = c->prm.dt * (3.0 / 4.0);
+    return a;
+}
+
+dim3 cell_grid(const Dims &d) { return dim3((d.Nx + 31) / 32, (d.Ny + 7) / 8, d.Nz); }
+const dim3 CELL_BLOCK(32, 8, 1);
+
+template <typename T> struct Impl {
+    typedef typename cplx_t<T>::type C;
+    static T *f(void *p) { return (T *)p; }
+
+    static int setup_kernels(dfdm_ctx *c) {
+        const Dims &d = c->d;
+        const int M = d.Nx / 2;
+        c->lx = std::max(1, std::min(64, 1024 / std::max(1, M)));
+        c->smem_x = 2 * (size_t)c->lx * M * sizeof(C);
+        c->tzx = (sizeof(T) == 8) ? 8 : 16;
+        c->smem_z = 2 * (size_t)d.Nz * c->tzx * sizeof(C);
+        c->smem_y = 2 * (size_t)d.Ny * c->tzx * sizeof(C);
+        c->smem_ys = (size_t)d.Ny * 32 * sizeof(double);
+        size_t maxs = std::max(std::max(c->smem_x, c->smem_z), std::max(c->smem_y, c->smem_ys));
+        if (maxs > 227 * 1024) return fail(DFDM_ERR_UNSUPPORTED, "grid too large for the shared-memory transforms");
+        CK(cudaFuncSetAttribute(k_fwd_x<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_x));
+        CK(cudaFuncSetAttribute(k_fwd_x<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_x));
+        CK(cudaFuncSetAttribute(k_inv_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_x));
+        CK(cudaFuncSetAttribute(k_col_fft<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(c->smem_z, c->smem_y)));
+        CK(cudaFuncSetAttribute(k_col_fft<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(c->smem_z, c->smem_y)));
+        CK(cudaFuncSetAttribute(k_col_fft<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(c->smem_z, c->smem_y)));
+        CK(cudaFuncSetAttribute(k_ysolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ys));
+        return DFDM_OK;
+    }
+
+    // ---- one kernel family of one stage ----
+    static int launch(dfdm_ctx *c, int which, int s) {
+        const Dims &d = c->d;
+        cudaStream_t st = c->stream;
+        switch (which) {
+        case 0: {   // SGS
+            if (!c->les) return DFDM_OK;
+            k_sgs<T><<<cell_grid(d), CELL_BLOCK, 0, st>>>(step_args<T>(c), f(c->u), f(c->v), f(c->w), f(c->nut));
+            CKL();
+            return DFDM_OK;
+        }
+        case 8: {   // wall model (filter update at stage 1)
+            if (!c->wm) return DFDM_OK;
+            dim3 g((d.Nx + 127) / 128, d.Nz);
+            int filt = c->wm_filter_mode == 1;
+            if (s == 1 && filt) {
+                k_wm_filter<T><<<g, 128, 0, st>>>(step_args<T>(c), c->wsd, f(c->u), f(c->w), c->wmf_seeded ? 0 : 1,
+                                                 c->prm.dt, c->prm.wm_filter_Tf_fac);
+                CKL();
+                c->wmf_seeded = true;
+            }
+            if (s == 1 || !filt) {   // with the filter the stress only changes with the filter (once per step)
+                k_wall_model<T><<<g, 128, 0, st>>>(step_args<T>(c), c->wsd, f(c->u), f(c->w), filt);
+                CKL();
+            }
+            return DFDM_OK;
+        }
+        case 1: {   // fused RHS + RK update
+            StageCoef sc;
+            sc.stage = s;
+            sc.dt_a11 = c->prm.dt * (8.0 / 15.0);
+            sc.dt = c->prm.dt;
+            sc.c1 = (s == 2) ? 1.0 / 4.0 : 1.0 / 4.0;
+            sc.c2 = (s == 2) ? 5.0 / 12.0 : 3.0 / 4.0;
+            Fields<T> fl{f(c->u), f(c->v), f(c->w), f(c->nut)};
+            if (c->les)
+                k_stage<T, true><<<cell_grid(d), CELL_BLOCK, 0, st>>>(step_args<T>(c), fl, c->wsd.tau_x, c->wsd.tau_z, sc,
+                    f(c->uo), f(c->vo), f(c->wo), f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf), nullptr);
+            else
+                k_stage<T, false><<<cell_grid(d), CELL_BLOCK, 0, st>>>(step_args<T>(c), fl, c->wsd.tau_x, c->wsd.tau_z, sc,
+                    f(c->uo), f(c->vo), f(c->wo), f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf), nullptr);
+            CKL();
+            return DFDM_OK;
+        }
+        case 2: {   // div + forward x
+            long long lines = (long long)d.Ny * d.Nz;
+            int nb = (int)((lines + c->lx - 1) / c->lx);
+            k_fwd_x<T, true><<<nb, 256, c->smem_x, st>>>(poisson_args<T>(c), c->lx, f(c->us), f(c->vs), f(c->wsf), nullptr,
+                                                         (C *)c->spec, c->plan_x, (const C *)c->tw_x, (const C *)c->twr_x);
+            CKL();
+            return DFDM_OK;
+        }
+        case 3: case 5: {   // z transforms
+            dim3 g((d.Nxc + c->tzx - 1) / c->tzx, d.Ny);
+            if (which == 3)
+                k_col_fft<T, 0><<<g, 256, c->smem_z, st>>>(d, c->tzx, (C *)c->spec, c->plan_z, (const C *)c->tw_z, c->d_kxx, c->d_kyy, c->d_kzz);
+            else
+                k_col_fft<T, 1><<<g, 256, c->smem_z, st>>>(d, c->tzx, (C *)c->spec, c->plan_z, (const C *)c->tw_z, c->d_kxx, c->d_kyy, c->d_kzz);
+            CKL();
+            return DFDM_OK;
+        }
+        case 4: {   // y solve
+            if (d.yper) {
+                dim3 g((d.Nxc + c->tzx - 1) / c->tzx, d.Nz);
+                k_col_fft<T, 2><<<g, 256, c->smem_y, st>>>(d, c->tzx, (C *)c->spec, c->plan_y, (const C *)c->tw_y, c->d_kxx, c->d_kyy, c->d_kzz);
+            } else {
+                dim3 g((d.Nxc + 31) / 32, d.Nz);
+                k_ysolve<T><<<g, 32, c->smem_ys, st>>>(d, (C *)c->spec, c->d_kxx, c->d_kzz, c->d_lo, c->d_di, c->d_up);
+            }
+            CKL();
+            return DFDM_OK;
+        }
+        case 6: {   // inverse x
+            long long lines = (long long)d.Ny * d.Nz;
+            int nb = (int)((lines + c->lx - 1) / c->lx);
+            k_inv_x<T><<<nb, 256, c->smem_x, st>>>(poisson_args<T>(c), c->lx, (const C *)c->spec, f(c->phi), c->plan_x,
+                                                   (const C *)c->tw_x, (const C *)c->twr_x);
+            CKL();
+            return DFDM_OK;
+        }
+        case 7: {   // correction (+ P at stage 3)
+            k_correct<T><<<cell_grid(d), CELL_BLOCK, 0, st>>>(poisson_args<T>(c), f(c->phi), f(c->us), f(c->vs), f(c->wsf),
+                                                              f(c->u), f(c->v), f(c->w), s == 3 ? f(c->p) : nullptr);
+            CKL();
+            return DFDM_OK;
+        }
+        case 9: {   // constant-flux shift
+            if (c->prm.flow_forcing_mode != 1) return DFDM_OK;
+            k_bulk_partial<T><<<c->red_blocks, 256, 0, st>>>(d, f(c->u), c->d_dyc, c->d_dzc, c->red_part);
+            CKL();
+            k_bulk_final<<<1, 32, 0, st>>>(c->red_blocks, c->red_part, c->prm.Ub_target, c->red_out);
+            CKL();
+            k_shift<T><<<c->red_blocks, 256, 0, st>>>(d, f(c->u), c->red_out);
+            CKL();
+            return DFDM_OK;
+        }
+        }
+        return fail(DFDM_ERR_INVALID, "unknown kernel family");
+    }
+
+    static int poisson_chain(dfdm_ctx *c, int s) {
+        int rc;
+        for (int k = 2; k <= 7; ++k)
+            if ((rc = launch(c, k, s))) return rc;
+        return DFDM_OK;
+    }
+
+    // compute_time_step_RK3, single-phase flag set (src/time_integration.f90:120-713)
+    static int step_enqueue(dfdm_ctx *c) {
+        int rc;
+        for (int s = 1; s <= 3; ++s) {
+            if ((rc = launch(c, 0, s))) return rc;   // SGS (step start, then stages 2 and 3)
+            if ((rc = launch(c, 8, s))) return rc;   // wall model
+            if ((rc = launch(c, 1, s))) return rc;   // RHS + RK update
+            if ((rc = poisson_chain(c, s))) return rc;
+        }
+        return launch(c, 9, 3);
+    }
+};
+
+template <typename F> int dispatch(dfdm_ctx *c, F fn) {
+    if (c->prec == DFDM_FP64) return fn(Impl<double>());
+    return fn(Impl<float>());
+}
+
+int check_ctx(dfdm_ctx *c) {
+    if (!c) return fail(DFDM_ERR_INVALID, "null context");
+    return DFDM_OK;
+}
+
+int ensure_staging(dfdm_ctx *c, size_t n) {
+    if (c->staging_n >= n) return DFDM_OK;
+    if (c->staging) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(c->staging);
+        c->allocs.erase(std::remove(c->allocs.begin(), c->allocs.end(), (void *)c->staging), c->allocs.end());
+        c->staging = nullptr;
+        c->staging_n = 0;
+    }
+    void *p = nullptr;
+    int rc = dalloc(c, &p, n * sizeof(double));
+    if (rc) return rc;
+    c->staging = (double *)p;
+    c->staging_n = n;
+    return DFDM_OK;
+}
+
+int reduce_grid(const Dims &d) {
+    long long b = (d.cells + 255) / 256;
+    return (int)std::max(1LL, std::min(b, 148LL * 8));
+}
+
+void destroy_graph(dfdm_ctx *c) {
+    if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
+    if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
+}
+
+int validate(const dfdm_grid *g, const dfdm_params *p) {
+    if (!g || !p) return fail(DFDM_ERR_INVALID, "null grid or params");
+    if (!g->x || !g->y || !g->z) return fail(DFDM_ERR_INVALID, "grid face arrays must not be NULL");
+    if (g->nx % 2 || g->nz % 2) return fail(DFDM_ERR_INVALID, "Error: nx and nz must be even");
+    if (g->nx < 6 || g->nz < 6 || g->ny < 4) return fail(DFDM_ERR_INVALID, "grid too small (nx, nz >= 6, ny >= 4)");
+    if (g->x_bc_type != 0 || g->z_bc_type != 0)
+        return fail(DFDM_ERR_UNSUPPORTED, "only periodic x and z are on the single-phase path (x_bc_type = z_bc_type = 0)");
+    if (g->y_bc_type != 0 && g->y_bc_type != 1) return fail(DFDM_ERR_INVALID, "y_bc_type must be 0 or 1");
+    if (g->y_bc_type == 1 && (g->bc_face_ylo != 1 || g->bc_face_yhi != 1))
+        return fail(DFDM_ERR_UNSUPPORTED, "only no-slip y walls (bc_face_ylo = bc_face_yhi = 1) are supported");
+    if (p->sgs_model < 0 || p->sgs_model > 2) return fail(DFDM_ERR_INVALID, "ERROR: sgs_model must be 0 (DNS), 1 (Vreman) or 2 (AMD)");
+    if (p->flat_wall_model_flag < 0 || p->flat_wall_model_flag > 1)
+        return fail(DFDM_ERR_UNSUPPORTED, "flat_wall_model_flag must be 0 or 1 (the rough-wall law is off the path)");
+    if (p->flat_wall_model_flag == 1 && g->y_bc_type != 1) return fail(DFDM_ERR_INVALID, "the flat-wall model needs y walls");
+    if (p->advection_scheme != 0 && p->advection_scheme != 1)
+        return fail(DFDM_ERR_UNSUPPORTED, "advection_scheme must be 0 or 1 (the hybrid upwind scheme is off the path)");
+    if (!(p->dt > 0.0)) return fail(DFDM_ERR_INVALID, "ERROR: &NUMERICS dt must be > 0");
+    if (!(p->nu >= 0.0)) return fail(DFDM_ERR_INVALID, "ERROR: &PHYSICS nu must be set");
+    if (p->precision != DFDM_FP64 && p->precision != DFDM_FP32_MIXED) return fail(DFDM_ERR_INVALID, "unknown precision");
+    if (p->wm_filter_mode == 1 && (p->flat_wall_model_flag == 0 || !(p->wm_filter_Tf_fac > 0.0)))
+        return fail(DFDM_ERR_INVALID, "ERROR: wm_filter_mode=1 needs flat_wall_model_flag>0 and wm_filter_Tf_fac>0");
+    FFTPlan tmp;
+    int Nx = g->nx - 2, Nz = g->nz - 2;
+    int Ny = g->y_bc_type == 0 ? g->ny - 2 : g->ny - 1;
+    if (!make_fft_plan(Nx / 2, tmp) || !make_fft_plan(Nz, tmp) || (g->y_bc_type == 0 && !make_fft_plan(Ny, tmp)))
+        return fail(DFDM_ERR_UNSUPPORTED, "transform lengths must factor into 2, 3 and 5");
+    if (Ny > MAX_NY) return fail(DFDM_ERR_UNSUPPORTED, "ny too large for the y solve");
+    for (int i = 1; i < g->nx; ++i) if (!(g->x[i] > g->x[i - 1])) return fail(DFDM_ERR_INVALID, "x faces must increase");
+    for (int i = 1; i < g->ny; ++i) if (!(g->y[i] > g->y[i - 1])) return fail(DFDM_ERR_INVALID, "y faces must increase");
+    for (int i = 1; i < g->nz; ++i) if (!(g->z[i] > g->z[i - 1])) return fail(DFDM_ERR_INVALID, "z faces must increase");
+    return DFDM_OK;
+}
+
+size_t footprint(const dfdm_grid *g, const dfdm_params *p) {
+    size_t ts = p->precision == DFDM_FP64 ? 8 : 4;
+    size_t Nx = g->nx - 2, Nz = g->nz - 2, Ny = g->y_bc_type == 0 ? g->ny - 2 : g->ny - 1;
+    size_t cells = Nx * Ny * Nz, spec = (Nx / 2 + 1) * Ny * Nz;
+    size_t n = cells * ts * (3 /*u*/ + 3 /*uo*/ + 3 /*F1*/ + 3 /*u**/ + 1 /*P*/ + 1 /*phi*/ + (p->sgs_model ? 1 : 0));
+    n += spec * 2 * ts;
+    n += 6 * Nx * Nz * 2 * 8;   // wall planes
+    n += 1 << 20;               // metrics, twiddles, reductions
+    return n;
+}
+
+}  // namespace
+
+// ================================================================================================================
+extern "C" {
+
+const char *dfdm_last_error(void) { return g_err.c_str(); }
+const char *dfdm_version(void) { return "dfdm-b200 0.1 (sm_100a)"; }
+
+void dfdm_default_params(dfdm_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->nu = -1.0;
+    p->dt = 0.0;
+    p->sgs_model = 2;            // src/global.f90:305
+    p->Cs_vreman = 0.17;         // :306
+    p->C_amd = 1.0 / 3.0;        // :307
+    p->flat_wall_model_flag = 0; // :312
+    p->advection_scheme = 0;
+    p->adv_wall_layers = -1;
+    p->wm_filter_mode = -1;
+    p->wm_filter_Tf_fac = 1.0;
+    p->flow_forcing_mode = 0;
+    p->precision = DFDM_FP64;
+}
+
+int dfdm_footprint_bytes(const dfdm_grid *grid, const dfdm_params *params, size_t *bytes) {
+    g_err.clear();
+    int rc = validate(grid, params);
+    if (rc) return rc;
+    if (!bytes) return fail(DFDM_ERR_INVALID, "null output");
+    *bytes = footprint(grid, params);
+    return DFDM_OK;
+}
+
+int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
+    g_err.clear();
+    if (!out) return fail(DFDM_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    int rc = validate(g, prm);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(DFDM_ERR_CUDA, "no CUDA device: the dfdm library has no CPU fallback");
+    }
+    dfdm_ctx *c = new dfdm_ctx();
+    c->prm = *prm;
+    c->prec = prm->precision;
+    c->ts = c->prec == DFDM_FP64 ? 8 : 4;
+    c->nx = g->nx; c->ny = g->ny; c->nz = g->nz;
+    c->nxg = g->nx + 1; c->nyg = g->ny + 1; c->nzg = g->nz + 1;
+    c->yper = g->y_bc_type == 0;
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return fail(DFDM_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    c->stream = c->own_stream;
+    auto bail = [&](int code) { dfdm_destroy(c); return code; };
+
+    // ---- grid (src/initialization.f90:243-345) ----
+    c->x.assign(c->nx + 1, 0.0); c->y.assign(c->ny + 1, 0.0); c->z.assign(c->nz + 1, 0.0);
+    for (int i = 1; i <= c->nx; ++i) c->x[i] = g->x[i - 1];
+    for (int j = 1; j <= c->ny; ++j) c->y[j] = g->y[j - 1];
+    for (int k = 1; k <= c->nz; ++k) c->z[k] = g->z[k - 1];
+    centres_of(c->x, c->nx, c->xg); centres_of(c->y, c->ny, c->yg); centres_of(c->z, c->nz, c->zg);
+    double dxmin = 1e300, dzmin = 1e300;
+    for (int i = 1; i <= c->nxg - 1; ++i) dxmin = std::min(dxmin, c->xg[i + 1] - c->xg[i]);
+    for (int k = 1; k <= c->nzg - 1; ++k) dzmin = std::min(dzmin, c->zg[k + 1] - c->zg[k]);
+    c->dx = dxmin; c->dz = dzmin;
+    c->Ly = c->y[c->ny] - c->y[1];
+    Dims &d = c->d;
+    d.Nx = c->nx - 2; d.Nz = c->nz - 2;
+    d.Ny = c->yper ? c->ny - 2 : c->ny - 1;
+    d.NyV = c->yper ? d.Ny : d.Ny - 1;
+    d.Nxc = d.Nx / 2 + 1;
+    d.yper = c->yper;
+    d.plane = (long long)d.Nx * d.Ny;
+    d.cells = d.plane * d.Nz;
+    // automatic defaults (src/input_output.f90:938-940, :967-970)
+    c->nwl = prm->adv_wall_layers;
+    if (c->nwl < 0) { c->nwl = 0; if (prm->flat_wall_model_flag > 0 && prm->advection_scheme != 1) c->nwl = 8; }
+    c->wm_filter_mode = prm->wm_filter_mode;
+    if (c->wm_filter_mode < 0) { c->wm_filter_mode = 0; if (prm->flat_wall_model_flag > 0) c->wm_filter_mode = 1; }
+    c->wm = (!c->yper && prm->flat_wall_model_flag > 0) ? 1 : 0;
+    c->les = prm->sgs_model != 0;
+    // dPdx = 0 under constant flux (src/time_integration.f90:212-216); steady forcing otherwise
+    c->dPdx = prm->flow_forcing_mode == 1 ? 0.0 : prm->dPdx;
+    c->dPdz = prm->dPdz;
+
+    // ---- fields ----
+    const size_t F = (size_t)d.cells * c->ts;
+    void **fields[] = {&c->u, &c->v, &c->w, &c->uo, &c->vo, &c->wo, &c->f1u, &c->f1v, &c->f1w,
+                       &c->us, &c->vs, &c->wsf, &c->p, &c->phi};
+    for (void **fp : fields)
+        if ((rc = dalloc(c, fp, F))) return bail(rc);
+    if ((rc = dalloc(c, &c->nut, c->les ? F : c->ts))) return bail(rc);
+    if ((rc = dalloc(c, &c->spec, (size_t)d.Nxc * d.Ny * d.Nz * 2 * c->ts))) return bail(rc);
+
+    // ---- metrics ----
+    std::vector<double> my, mz;
+    build_metric(c->y, c->yg, c->ny, d.Ny, my);
+    build_metric(c->z, c->zg, c->nz, d.Nz, mz);
+    void *tmp = nullptr;
+    if ((rc = upload_as<double>(c, &tmp, my))) return bail(rc);
+    c->my_d = (double *)tmp;
+    if ((rc = upload_as<double>(c, &tmp, mz))) return bail(rc);
+    c->mz_d = (double *)tmp;
+    if (c->prec == DFDM_FP64) { c->my_t = c->my_d; c->mz_t = c->mz_d; }
+    else {
+        if ((rc = upload_as<float>(c, &c->my_t, my))) return bail(rc);
+        if ((rc = upload_as<float>(c, &c->mz_t, mz))) return bail(rc);
+    }
+    std::vector<double> dxc(d.Nx), dyc(d.Ny), dzc(d.Nz);
+    for (int i = 0; i < d.Nx; ++i) dxc[i] = c->x[i + 2] - c->x[i + 1];
+    for (int j = 0; j < d.Ny; ++j) dyc[j] = c->y[j + 2] - c->y[j + 1];
+    for (int k = 0; k < d.Nz; ++k) dzc[k] = c->z[k + 2] - c->z[k + 1];
+    if ((rc = upload_as<double>(c, &tmp, dxc))) return bail(rc);
+    c->d_dxc = (double *)tmp;
+    if ((rc = upload_as<double>(c, &tmp, dyc))) return bail(rc);
+    c->d_dyc = (double *)tmp;
+    if ((rc = upload_as<double>(c, &tmp, dzc))) return bail(rc);
+    c->d_dzc = (double *)tmp;
+
+    // ---- modified wavenumbers (src/initialization.f90:417-434, :480-489) and Dyy (:507-535) ----
+    int nxp = d.Nx, nzp = d.Nz;
+    std::vector<double> kxx(d.Nxc), kzz(d.Nz), kyy(std::max(1, d.Ny));
+    int cx = (int)std::ceil((double)nxp / 2.0), cz = (int)std::ceil((double)nzp / 2.0);
+    for (int i = 0; i < d.Nxc; ++i) {
+        double ii = (i <= cx) ? (double)i : (double)(-nxp + i);
+        kxx[i] = 2.0 * (std::cos(2.0 * PI * ii / (double)nxp) - 1.0) / std::pow(c->dx, 2.0);
+    }
+    for (int k = 0; k < nzp; ++k) {
+        double kk = (k <= cz) ? (double)k : (double)(-nzp + k);
+        kzz[k] = 2.0 * (std::cos(2.0 * PI * kk / (double)nzp) - 1.0) / std::pow(c->dz, 2.0);
+    }
+    if (c->yper) {
+        int nyp = d.Ny;
+        double dy = c->y[2] - c->y[1];
+        int cy = (int)std::ceil((double)nyp / 2.0);
+        for (int j = 0; j < nyp; ++j) {
+            double jj = (j <= cy) ? (double)j : (double)(-nyp + j);
+            kyy[j] = 2.0 * (std::cos(2.0 * PI * jj / (double)nyp) - 1.0) / std::pow(dy, 2.0);
+        }
+    }
+    std::vector<double> lo(d.Ny, 0.0), di(d.Ny, 0.0), up(d.Ny, 0.0);
+    if (!c->yper) {
+        const std::vector<double> &y = c->y, &yg = c->yg;
+        int nyg = c->nyg;
+        auto abc = [&](int j, double &a, double &b, double &cc) {
+            a = 1.0 / (y[j] - y[j - 1]) / (yg[j + 1] - yg[j]);
+            b = 1.0 / (y[j] - y[j - 1]) * (-1.0 / (yg[j + 1] - yg[j]) - 1.0 / (yg[j] - yg[j - 1]));
+            cc = 1.0 / (y[j] - y[j - 1]) / (yg[j] - yg[j - 1]);
+        };
+        for (int j = 3; j <= nyg - 2; ++j) {
+            double a, b, cc; abc(j, a, b, cc);
+            up[j - 2] = a; lo[j - 2] = cc; di[j - 2] = b;
+        }
+        double a, b, cc;
+        abc(2, a, b, cc); di[0] = b + cc; up[0] = a;
+        abc(nyg - 1, a, b, cc); di[nyg - 3] = a + b; lo[nyg - 3] = cc;
+    }
+    if ((rc = upload_as<double>(c, &tmp, kxx))) return bail(rc);
+    c->d_kxx = (double *)tmp;
+    if ((rc = upload_as<double>(c, &tmp, kzz))) return bail(rc);
+    c->d_kzz = (double *)tmp;
+    if ((rc = upload_as<double>(c, &tmp, kyy))) return bail(rc);
+    c->d_kyy = (double *)tmp;
+    if ((rc = upload_as<double>(c, &tmp, lo))) return bail(rc);
+    c->d_lo = (double *)tmp;
+    if ((rc = upload_as<double>(c, &tmp, di))) return bail(rc);
+    c->d_di = (double *)tmp;
+    if ((rc = upload_as<double>(c, &tmp, up))) return bail(rc);
+    c->d_up = (double *)tmp;
+
+    // ---- FFT plans and twiddles ----
+    make_fft_plan(d.Nx / 2, c->plan_x);
+    make_fft_plan(d.Nz, c->plan_z);
+    if (c->yper) make_fft_plan(d.Ny, c->plan_y);
+    auto tws = [&](void **dst, int n, int count) {
+        return c->prec == DFDM_FP64 ? upload_twiddles<double>(c, dst, n, count) : upload_twiddles<float>(c, dst, n, count);
+    };
+    if ((rc = tws(&c->tw_x, d.Nx / 2, d.Nx / 2))) return bail(rc);
+    if ((rc = tws(&c->twr_x, d.Nx, d.Nx / 2 + 1))) return bail(rc);
+    if ((rc = tws(&c->tw_z, d.Nz, d.Nz))) return bail(rc);
+    if ((rc = tws(&c->tw_y, c->yper ? d.Ny : 1, c->yper ? d.Ny : 1))) return bail(rc);
+
+    // ---- wall model planes ----
+    size_t wp = (size_t)2 * d.Nz * d.Nx * sizeof(double);
+    double **wsp[] = {&c->wsd.tau_x, &c->wsd.tau_z, &c->wsd.ux, &c->wsd.wx, &c->wsd.tx, &c->wsd.uz, &c->wsd.wz, &c->wsd.tz};
+    for (double **pp : wsp)
+        if ((rc = dalloc(c, (void **)pp, wp))) return bail(rc);
+
+    // ---- reductions ----
+    c->red_blocks = reduce_grid(d);
+    if ((rc = dalloc(c, &tmp, (size_t)2 * c->red_blocks * sizeof(double)))) return bail(rc);
+    c->red_part = (double *)tmp;
+    if ((rc = dalloc(c, &tmp, 4 * sizeof(double)))) return bail(rc);
+    c->red_out = (double *)tmp;
+    if ((rc = dalloc(c, &tmp, sizeof(unsigned long long)))) return bail(rc);
+    c->d_maxdiv = (unsigned long long *)tmp;
+    if ((rc = dalloc(c, &tmp, sizeof(int)))) return bail(rc);
+    c->d_flag = (int *)tmp;
+
+    rc = dispatch(c, [&](auto impl) { return decltype(impl)::setup_kernels(c); });
+    if (rc) return bail(rc);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(DFDM_ERR_CUDA, "set-up synchronisation failed"));
+    *out = c;
+    return DFDM_OK;
+}
+
+int dfdm_destroy(dfdm_ctx *c) {
+    if (!c) return DFDM_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    destroy_graph(c);
+    for (void *p : c->allocs) cudaFree(p);
+    c->allocs.clear();
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return DFDM_OK;
+}
+
+int dfdm_set_stream(dfdm_ctx *c, void *s) {
+    if (int rc = check_ctx(c)) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    c->stream = s ? (cudaStream_t)s : c->own_stream;
+    destroy_graph(c);
+    return DFDM_OK;
+}
+
+int dfdm_synchronize(dfdm_ctx *c) {
+    if (int rc = check_ctx(c)) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return DFDM_OK;
+}
+
+// ---- state transfer ----
+static int put_field(dfdm_ctx *c, int kind, void *dst, const double *src, int n1, int n2, int n3) {
+    size_t n = (size_t)n1 * n2 * n3;
+    int rc = ensure_staging(c, n);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(c->staging, src, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    int gb = reduce_grid(c->d);
+    if (c->prec == DFDM_FP64) k_unpack<double><<<gb, 256, 0, c->stream>>>(c->d, kind, n1, n2, c->staging, (double *)dst);
+    else k_unpack<float><<<gb, 256, 0, c->stream>>>(c->d, kind, n1, n2, c->staging, (float *)dst);
+    CKL();
+    return DFDM_OK;
+}
+
+static int get_field(dfdm_ctx *c, int kind, const void *srcf, double *dst, int n1, int n2, int n3) {
+    size_t n = (size_t)n1 * n2 * n3;
+    int rc = ensure_staging(c, n);
+    if (rc) return rc;
+    int gb = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
+    if (c->prec == DFDM_FP64) k_pack<double><<<gb, 256, 0, c->stream>>>(c->d, kind, n1, n2, n3, (const double *)srcf, c->staging);
+    else k_pack<float><<<gb, 256, 0, c->stream>>>(c->d, kind, n1, n2, n3, (const float *)srcf, c->staging);
+    CKL();
+    CK(cudaMemcpyAsync(dst, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return DFDM_OK;
+}
+
+int dfdm_set_state(dfdm_ctx *c, const double *U, const double *V, const double *W, const double *P) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (!U || !V || !W) return fail(DFDM_ERR_INVALID, "U, V and W must not be NULL");
+    int rc;
+    if ((rc = put_field(c, FK_U, c->u, U, c->nx, c->nyg, c->nzg))) return rc;
+    if ((rc = put_field(c, FK_V, c->v, V, c->nxg, c->ny, c->nzg))) return rc;
+    if ((rc = put_field(c, FK_W, c->w, W, c->nxg, c->nyg, c->nz))) return rc;
+    if (P && (rc = put_field(c, FK_P, c->p, P, c->nxg, c->nyg, c->nzg))) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return DFDM_OK;
+}
+
+int dfdm_get_state(dfdm_ctx *c, double *U, double *V, double *W, double *P) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    int rc;
+    if (U) { if ((rc = get_field(c, FK_U, c->u, U, c->nx, c->nyg, c->nzg))) return rc; CK(cudaStreamSynchronize(c->stream)); }
+    if (V) { if ((rc = get_field(c, FK_V, c->v, V, c->nxg, c->ny, c->nzg))) return rc; CK(cudaStreamSynchronize(c->stream)); }
+    if (W) { if ((rc = get_field(c, FK_W, c->w, W, c->nxg, c->nyg, c->nz))) return rc; CK(cudaStreamSynchronize(c->stream)); }
+    if (P) { if ((rc = get_field(c, FK_P, c->p, P, c->nxg, c->nyg, c->nzg))) return rc; CK(cudaStreamSynchronize(c->stream)); }
+    return DFDM_OK;
+}
+
+int dfdm_get_nu_t(dfdm_ctx *c, double *nu_t) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (!nu_t) return fail(DFDM_ERR_INVALID, "null output");
+    if (!c->les) { std::memset(nu_t, 0, sizeof(double) * (size_t)c->nxg * c->nyg * c->nzg); return DFDM_OK; }
+    int rc = get_field(c, FK_NUT, c->nut, nu_t, c->nxg, c->nyg, c->nzg);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return DFDM_OK;
+}
+
+int dfdm_set_nu_t(dfdm_ctx *c, const double *nu_t) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (!c->les) return fail(DFDM_ERR_INVALID, "nu_t is only stored for LES (sgs_model > 0)");
+    int rc = put_field(c, FK_NUT, c->nut, nu_t, c->nxg, c->nyg, c->nzg);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return DFDM_OK;
+}
+
+int dfdm_set_time(dfdm_ctx *c, double t) {
+    if (int rc = check_ctx(c)) return rc;
+    c->t = t;
+    return DFDM_OK;
+}
+
+int dfdm_get_time(dfdm_ctx *c, double *t) {
+    if (int rc = check_ctx(c)) return rc;
+    if (t) *t = c->t;
+    return DFDM_OK;
+}
+
+// ---- the step ----
+static int step_n(dfdm_ctx *c, int nsteps) {
+    for (int n = 0; n < nsteps; ++n) {
+        double to = c->t;
+        bool can_graph = c->graphs && (c->wm_filter_mode != 1 || !c->wm || c->wmf_seeded);
+        if (can_graph) {
+            if (!c->gexec) {
+                CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+                long long before = g_launches;
+                int rc = dispatch(c, [&](auto impl) { return decltype(impl)::step_enqueue(c); });
+                c->graph_launches = g_launches - before;
+                g_launches = before;
+                cudaGraph_t g = nullptr;
+                cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+                if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+                if (e != cudaSuccess) return fail(DFDM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+                c->graph = g;
+                CK(cudaGraphInstantiate(&c->gexec, c->graph, 0));
+            }
+            CK(cudaGraphLaunch(c->gexec, c->stream));
+            c->launches += c->graph_launches;
+        } else {
+            long long before = g_launches;
+            int rc = dispatch(c, [&](auto impl) { return decltype(impl)::step_enqueue(c); });
+            c->launches += g_launches - before;
+            if (rc) return rc;
+        }
+        c->t = to + 1.0 * c->prm.dt;   // t = to + rk_t(3)*dt
+    }
+    return DFDM_OK;
+}
+
+int dfdm_compute_time_step_rk3_async(dfdm_ctx *c, int nsteps) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (nsteps < 0) return fail(DFDM_ERR_INVALID, "nsteps must be >= 0");
+    return step_n(c, nsteps);
+}
+
+int dfdm_compute_time_step_rk3(dfdm_ctx *c, int nsteps, double *t) {
+    int rc = dfdm_compute_time_step_rk3_async(c, nsteps);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    if (t) *t = c->t;
+    return DFDM_OK;
+}
+
+int dfdm_enable_graphs(dfdm_ctx *c, int enable) {
+    if (int rc = check_ctx(c)) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    c->graphs = enable != 0;
+    if (!c->graphs) destroy_graph(c);
+    return DFDM_OK;
+}
+
+// ---- unit entry points ----
+int dfdm_compute_sgs_model(dfdm_ctx *c) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    int rc = dispatch(c, [&](auto impl) { return decltype(impl)::launch(c, 0, 1); });
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return DFDM_OK;
+}
+
+int dfdm_compute_wall_model(dfdm_ctx *c, int update_filter, double *tau_x, double *tau_z) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (c->wm) {
+        int rc = dispatch(c, [&](auto impl) { return decltype(impl)::launch(c, 8, update_filter ? 1 : 2); });
+        if (rc) return rc;
+    }
+    const Dims &d = c->d;
+    size_t nx_n = (size_t)c->nx * 2 * c->nzg, nz_n = (size_t)c->nxg * 2 * c->nz;
+    int rc = ensure_staging(c, std::max(nx_n, nz_n));
+    if (rc) return rc;
+    if (tau_x) {
+        k_pack_tau<<<64, 256, 0, c->stream>>>(d, 0, c->nx, c->nzg, c->wsd.tau_x, c->staging);
+        CKL();
+        CK(cudaMemcpyAsync(tau_x, c->staging, nx_n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    if (tau_z) {
+        k_pack_tau<<<64, 256, 0, c->stream>>>(d, 1, c->nxg, c->nz, c->wsd.tau_z, c->staging);
+        CKL();
+        CK(cudaMemcpyAsync(tau_z, c->staging, nz_n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return DFDM_OK;
+}
+
+int dfdm_compute_rhs(dfdm_ctx *c, double *rhs_u, double *rhs_v, double *rhs_w) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    const Dims &d = c->d;
+    if (!c->rhs3) {
+        int rc = dalloc(c, &c->rhs3, (size_t)3 * d.cells * c->ts);
+        if (rc) return rc;
+    }
+    int rc = dispatch(c, [&](auto impl) {
+        typedef decltype(impl) I;
+        typedef typename std::remove_pointer<decltype(I::f(nullptr))>::type T;
+        StageCoef sc{1, 0.0, 0.0, 0.0, 0.0};
+        Fields<T> fl{I::f(c->u), I::f(c->v), I::f(c->w), I::f(c->nut)};
+        if (c->les)
+            k_stage<T, true><<<cell_grid(d), CELL_BLOCK, 0, c->stream>>>(step_args<T>(c), fl, c->wsd.tau_x, c->wsd.tau_z, sc,
+                nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, I::f(c->rhs3));
+        else
+            k_stage<T, false><<<cell_grid(d), CELL_BLOCK, 0, c->stream>>>(step_args<T>(c), fl, c->wsd.tau_x, c->wsd.tau_z, sc,
+                nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, I::f(c->rhs3));
+        CKL();
+        return DFDM_OK;
+    });
+    if (rc) return rc;
+    struct { double *dst; int n1, n2, n3; } outs[3] = {
+        {rhs_u, c->nx - 2, c->nyg - 2, c->nzg - 2},
+        {rhs_v, c->nxg - 2, c->ny - 2, c->nzg - 2},
+        {rhs_w, c->nxg - 2, c->nyg - 2, c->nz - 2}};
+    for (int q = 0; q < 3; ++q) {
+        if (!outs[q].dst) continue;
+        size_t n = (size_t)outs[q].n1 * outs[q].n2 * outs[q].n3;
+        if ((rc = ensure_staging(c, n))) return rc;
+        int gb = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
+        if (c->prec == DFDM_FP64)
+            k_pack_interior<double><<<gb, 256, 0, c->stream>>>(d, outs[q].n1, outs[q].n2, outs[q].n3, (const double *)c->rhs3 + q * d.cells, c->staging);
+        else
+            k_pack_interior<float><<<gb, 256, 0, c->stream>>>(d, outs[q].n1, outs[q].n2, outs[q].n3, (const float *)c->rhs3 + q * d.cells, c->staging);
+        CKL();
+        CK(cudaMemcpyAsync(outs[q].dst, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return DFDM_OK;
+}
+
+int dfdm_apply_boundary_conditions(dfdm_ctx *c, int after_projection) {
+    (void)after_projection;
+    return check_ctx(c);
+}
+
+int dfdm_compute_projection_step(dfdm_ctx *c, int save_p) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    size_t F = (size_t)c->d.cells * c->ts;
+    CK(cudaMemcpyAsync(c->us, c->u, F, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->vs, c->v, F, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->wsf, c->w, F, cudaMemcpyDeviceToDevice, c->stream));
+    int rc = dispatch(c, [&](auto impl) { return decltype(impl)::poisson_chain(c, save_p ? 3 : 1); });
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return DFDM_OK;
+}
+
+int dfdm_solve_poisson(dfdm_ctx *c, const double *rhs_in, double *phi_out) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (!rhs_in || !phi_out) return fail(DFDM_ERR_INVALID, "null array");
+    const Dims &d = c->d;
+    int n1 = c->nxg - 1, n2 = c->nyg - 2, n3 = c->nzg - 1;
+    size_t n = (size_t)n1 * n2 * n3;
+    int rc = ensure_staging(c, n);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(c->staging, rhs_in, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    rc = dispatch(c, [&](auto impl) {
+        typedef decltype(impl) I;
+        typedef typename std::remove_pointer<decltype(I::f(nullptr))>::type T;
+        typedef typename cplx_t<T>::type C;
+        int gb = reduce_grid(d);
+        k_unpack_rhs_p<T><<<gb, 256, 0, c->stream>>>(d, n1, n2, c->staging, I::f(c->phi));
+        CKL();
+        long long lines = (long long)d.Ny * d.Nz;
+        int nb = (int)((lines + c->lx - 1) / c->lx);
+        k_fwd_x<T, false><<<nb, 256, c->smem_x, c->stream>>>(poisson_args<T>(c), c->lx, nullptr, nullptr, nullptr, I::f(c->phi),
+                                                             (C *)c->spec, c->plan_x, (const C *)c->tw_x, (const C *)c->twr_x);
+        CKL();
+        int r2;
+        if ((r2 = I::launch(c, 3, 1))) return r2;
+        if ((r2 = I::launch(c, 4, 1))) return r2;
+        if ((r2 = I::launch(c, 5, 1))) return r2;
+        if ((r2 = I::launch(c, 6, 1))) return r2;
+        int gb2 = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
+        k_pack_rhs_p<T><<<gb2, 256, 0, c->stream>>>(d, n1, n2, n3, I::f(c->phi), c->staging);
+        CKL();
+        return DFDM_OK;
+    });
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(phi_out, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DFDM_OK;
+}
+
+int dfdm_compute_bulk_velocity(dfdm_ctx *c, double *Ub) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (!Ub) return fail(DFDM_ERR_INVALID, "null output");
+    int rc = dispatch(c, [&](auto impl) {
+        typedef decltype(impl) I;
+        typedef typename std::remove_pointer<decltype(I::f(nullptr))>::type T;
+        k_bulk_partial<T><<<c->red_blocks, 256, 0, c->stream>>>(c->d, I::f(c->u), c->d_dyc, c->d_dzc, c->red_part);
+        CKL();
+        k_bulk_final<<<1, 32, 0, c->stream>>>(c->red_blocks, c->red_part, 0.0, c->red_out);
+        CKL();
+        return DFDM_OK;
+    });
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(Ub, c->red_out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DFDM_OK;
+}
+
+int dfdm_check_divergence(dfdm_ctx *c, double *max_div) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (!max_div) return fail(DFDM_ERR_INVALID, "null output");
+    CK(cudaMemsetAsync(c->d_maxdiv, 0, sizeof(unsigned long long), c->stream));
+    int rc = dispatch(c, [&](auto impl) {
+        typedef decltype(impl) I;
+        typedef typename std::remove_pointer<decltype(I::f(nullptr))>::type T;
+        k_maxdiv<T><<<c->red_blocks, 256, 0, c->stream>>>(c->d, I::f(c->u), I::f(c->v), I::f(c->w), c->d_dxc, c->d_dyc,
+                                                          c->d_dzc, c->d_maxdiv);
+        CKL();
+        return DFDM_OK;
+    });
+    if (rc) return rc;
+    unsigned long long bits = 0;
+    CK(cudaMemcpyAsync(&bits, c->d_maxdiv, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::memcpy(max_div, &bits, sizeof(double));
+    return DFDM_OK;
+}
+
+int dfdm_kinetic_energy(dfdm_ctx *c, double *ke) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (!ke) return fail(DFDM_ERR_INVALID, "null output");
+    int rc = dispatch(c, [&](auto impl) {
+        typedef decltype(impl) I;
+        typedef typename std::remove_pointer<decltype(I::f(nullptr))>::type T;
+        k_ke_partial<T><<<c->red_blocks, 256, 0, c->stream>>>(c->d, I::f(c->u), I::f(c->v), I::f(c->w), c->dx, c->d_dyc,
+                                                              c->d_dzc, c->red_part);
+        CKL();
+        k_ratio_final<<<1, 32, 0, c->stream>>>(c->red_blocks, c->red_part, c->red_out + 2);
+        CKL();
+        return DFDM_OK;
+    });
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(ke, c->red_out + 2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DFDM_OK;
+}
+
+int dfdm_check_finite(dfdm_ctx *c) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    CK(cudaMemsetAsync(c->d_flag, 0, sizeof(int), c->stream));
+    int rc = dispatch(c, [&](auto impl) {
+        typedef decltype(impl) I;
+        typedef typename std::remove_pointer<decltype(I::f(nullptr))>::type T;
+        k_finite<T><<<c->red_blocks, 256, 0, c->stream>>>(c->d.cells, I::f(c->u), I::f(c->v), I::f(c->w), c->d_flag);
+        CKL();
+        return DFDM_OK;
+    });
+    if (rc) return rc;
+    int flag = 0;
+    CK(cudaMemcpyAsync(&flag, c->d_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (flag) return fail(DFDM_ERR_NOT_FINITE, "NaN, Inf or |U| > 1e8 in the velocity field");
+    return DFDM_OK;
+}
+
+int dfdm_pad_field(dfdm_ctx *c, int field, int extra_planes, double *out) {
+    (void)field; (void)extra_planes; (void)out;
+    if (int rc = check_ctx(c)) return rc;
+    return fail(DFDM_ERR_UNSUPPORTED,
+                "pad_field_dev serves the hybrid advection scheme, the immersed boundary and the particles; "
+                "none of them is on the single-phase path");
+}
+
+int dfdm_launch_kernel_async(dfdm_ctx *c, int which, int rk_stage) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (which < 0 || which > 9 || rk_stage < 1 || rk_stage > 3) return fail(DFDM_ERR_INVALID, "bad kernel id or stage");
+    long long before = g_launches;
+    int rc = dispatch(c, [&](auto impl) { return decltype(impl)::launch(c, which, rk_stage); });
+    c->launches += g_launches - before;
+    return rc;
+}
+
+int dfdm_launch_count(dfdm_ctx *c, long long *count) {
+    if (int rc = check_ctx(c)) return rc;
+    if (!count) return fail(DFDM_ERR_INVALID, "null output");
+    *count = c->launches;
+    return DFDM_OK;
+}
+
+int dfdm_kernel_bytes(dfdm_ctx *c, int which, double *bytes) {
+    if (int rc = check_ctx(c)) return rc;
+    if (!bytes) return fail(DFDM_ERR_INVALID, "null output");
+    const Dims &d = c->d;
+    double cell = (double)d.cells * (double)c->ts;
+    double spec = (double)d.Nxc * d.Ny * d.Nz * 2.0 * (double)c->ts;
+    double b = 0.0;
+    switch (which) {
+    case 0: b = c->les ? 4.0 * cell : 0.0; break;                 // read U,V,W; write nu_t
+    case 1: b = 12.0 * cell + (c->les ? cell : 0.0); break;       // stage 1: 3 in, 9 out; stages 2/3: 9 in, 3 out
+    case 2: b = 3.0 * cell + spec; break;                         // read u*, write spectrum
+    case 3: case 4: case 5: b = 2.0 * spec; break;                // read + write spectrum
+    case 6: b = spec + cell; break;                               // read spectrum, write phi
+    case 7: b = 7.0 * cell; break;                                // read phi, u*; write u (+P at stage 3)
+    default: return fail(DFDM_ERR_INVALID, "bad kernel id");
+    }
+    *bytes = b;
+    return DFDM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,262 @@
+// kernels_diag.cuh -- reductions (FP64 compensated sums), the constant-flux shift and the ghosted state transfers.
+#pragma once
+
+#include "dfdm_common.cuh"
+
+namespace dfdm {
+
+// Kahan-compensated accumulator in double.
+struct Kahan {
+    double s, c;
+    __device__ __forceinline__ void init() { s = 0.0; c = 0.0; }
+    __device__ __forceinline__ void add(double x) {
+        double y = x - c;
+        double t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+};
+
+// Block reduction of two compensated sums; thread 0 writes the block's pair to out[2*blockIdx].
+__device__ __forceinline__ void block_sum2(double a, double b, double *out) {
+    __shared__ double sa[32], sb[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { sa[wid] = a; sb[wid] = b; }
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        a = lane < nw ? sa[lane] : 0.0;
+        b = lane < nw ? sb[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+        }
+        if (lane == 0) { out[2 * blockIdx.x] = a; out[2 * blockIdx.x + 1] = b; }
+    }
+}
+
+// compute_bulk_velocity (src/monitor.f90:463-523): sum of 0.5 (U_i + U_{i-1}) dy_j dz_k over the independent
+// cells and of the weights dy_j dz_k, one partial pair per block (deterministic, no atomics).
+template <typename T>
+__global__ void __launch_bounds__(256) k_bulk_partial(Dims d, const T *__restrict__ U, const double *__restrict__ dyc,
+                                                      const double *__restrict__ dzc, double *__restrict__ part) {
+    Kahan s, w; s.init(); w.init();
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(p % d.Nx);
+        long long q = p / d.Nx;
+        int j = (int)(q % d.Ny), k = (int)(q / d.Ny);
+        double a = dyc[j] * dzc[k];
+        double u0 = (double)U[p], um = (double)U[idx3(d, wrap(i - 1, d.Nx), j, k)];
+        s.add(0.5 * (u0 + um) * a);
+        w.add(a);
+    }
+    block_sum2(s.s, w.s, part);
+}
+
+// Final pass over the block partials in a fixed order; writes Ub and the shift Ub_target - Ub.
+__global__ void k_bulk_final(int nparts, const double *__restrict__ part, double Ub_target, double *__restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    Kahan s, w; s.init(); w.init();
+    for (int b = 0; b < nparts; ++b) { s.add(part[2 * b]); w.add(part[2 * b + 1]); }
+    double Ub = s.s / fmax(w.s, 1e-14);
+    out[0] = Ub;
+    out[1] = Ub_target - Ub;
+}
+
+// U += (Ub_target - Ub) on every independent U face (src/time_integration.f90:581-583).
+template <typename T>
+__global__ void __launch_bounds__(256) k_shift(Dims d, T *__restrict__ U, const double *__restrict__ dU) {
+    T s = (T)dU[1];
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x)
+        U[p] = U[p] + s;
+}
+
+// check_divergence (src/projection.f90:607-639): max |div u| over the independent centres, in double.
+// The maximum of non-negative doubles is taken with an integer atomicMax on their bit patterns (exact).
+template <typename T>
+__global__ void __launch_bounds__(256) k_maxdiv(Dims d, const T *__restrict__ U, const T *__restrict__ V,
+                                                const T *__restrict__ W, const double *__restrict__ dxc,
+                                                const double *__restrict__ dyc, const double *__restrict__ dzc,
+                                                unsigned long long *__restrict__ out) {
+    double m = 0.0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(p % d.Nx);
+        long long q = p / d.Nx;
+        int j = (int)(q % d.Ny), k = (int)(q / d.Ny);
+        double du = (double)U[p] - (double)U[idx3(d, wrap(i - 1, d.Nx), j, k)];
+        double dv = (double)ld_yf(V, d, i, j, k) - (double)ld_yf(V, d, i, j - 1, k);
+        double dw = (double)W[p] - (double)W[idx3(d, i, j, wrap(k - 1, d.Nz))];
+        double dv_ = fabs(du / dxc[i] + dv / dyc[j] + dw / dzc[k]);
+        m = fmax(m, dv_);
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// Volume-weighted kinetic energy 0.5 <u.u> with face velocities averaged to the centres (compensated sums).
+template <typename T>
+__global__ void __launch_bounds__(256) k_ke_partial(Dims d, const T *__restrict__ U, const T *__restrict__ V,
+                                                    const T *__restrict__ W, double dx, const double *__restrict__ dyc,
+                                                    const double *__restrict__ dzc, double *__restrict__ part) {
+    Kahan s, w; s.init(); w.init();
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(p % d.Nx);
+        long long q = p / d.Nx;
+        int j = (int)(q % d.Ny), k = (int)(q / d.Ny);
+        double vol = dyc[j] * dzc[k] * dx;
+        double uc = 0.5 * ((double)U[p] + (double)U[idx3(d, wrap(i - 1, d.Nx), j, k)]);
+        double vc = 0.5 * ((double)ld_yf(V, d, i, j, k) + (double)ld_yf(V, d, i, j - 1, k));
+        double wc = 0.5 * ((double)W[p] + (double)W[idx3(d, i, j, wrap(k - 1, d.Nz))]);
+        s.add(0.5 * (uc * uc + vc * vc + wc * wc) * vol);
+        w.add(vol);
+    }
+    block_sum2(s.s, w.s, part);
+}
+
+__global__ void k_ratio_final(int nparts, const double *__restrict__ part, double *__restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    Kahan s, w; s.init(); w.init();
+    for (int b = 0; b < nparts; ++b) { s.add(part[2 * b]); w.add(part[2 * b + 1]); }
+    out[0] = s.s / w.s;
+}
+
+// NaN / Inf / |U| > 1e8 guard of output_monitor (src/monitor.f90:32-52).
+template <typename T>
+__global__ void __launch_bounds__(256) k_finite(long long n, const T *__restrict__ a, const T *__restrict__ b,
+                                                const T *__restrict__ c, int *__restrict__ flag) {
+    int bad = 0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        double x = (double)a[p], y = (double)b[p], z = (double)c[p];
+        if (!(fabs(x) <= 1e8) || !(fabs(y) <= 1e8) || !(fabs(z) <= 1e8)) bad = 1;
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
+// ---- state transfer ---------------------------------------------------------------------------------------------
+// Field kinds of the ghosted reference arrays.
+enum FieldKind { FK_U = 0, FK_V = 1, FK_W = 2, FK_P = 3, FK_NUT = 4 };
+
+// Device index and sign of one ghosted reference element (Fortran 1-based (I,J,K)).  Mirrors the ghost rules of
+// apply_boundary_conditions (velocities), finish_pressure_ghosts (P) and sgs_fill_ghosts (nu_t); sign 0 means the
+// element is zero.
+__device__ __forceinline__ long long map_ghost(const Dims &d, int kind, int I, int J, int K, int &sign) {
+    sign = 1;
+    int i = I - 2, j = J - 2, k = K - 2;
+    i = ((i % d.Nx) + d.Nx) % d.Nx;   // x periodic for every field (faces and centres alike)
+    k = ((k % d.Nz) + d.Nz) % d.Nz;   // z periodic
+    if (d.yper) {
+        if (kind == FK_P) {
+            if (j < 0 || j >= d.Ny) j = 0;          // P(1) = P(2), P(nyg-1) = P(2), P(nyg) = P(nyg-1)
+        } else {
+            j = ((j % d.Ny) + d.Ny) % d.Ny;
+        }
+    } else if (kind == FK_V) {
+        if (j < 0 || j >= d.Ny - 1) sign = 0;       // wall faces
+    } else if (kind == FK_P) {
+        if (j < 0) j = 0;
+        if (j >= d.Ny) j = d.Ny - 1;
+    } else if (kind == FK_NUT) {
+        if (j < 0 || j >= d.Ny) sign = 0;
+    } else {   // U, W: no-slip mirror
+        if (j < 0) { j = 0; sign = -1; }
+        if (j >= d.Ny) { j = d.Ny - 1; sign = -1; }
+    }
+    return idx3(d, i, j, k);
+}
+
+// Expand a device field into its ghosted FP64 reference array (n1 x n2 x n3, Fortran order).
+template <typename T>
+__global__ void __launch_bounds__(256) k_pack(Dims d, int kind, int n1, int n2, int n3, const T *__restrict__ f,
+                                              double *__restrict__ out) {
+    long long n = (long long)n1 * n2 * n3;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        int I = (int)(p % n1) + 1;
+        long long q = p / n1;
+        int J = (int)(q % n2) + 1, K = (int)(q / n2) + 1;
+        int sg;
+        long long s = map_ghost(d, kind, I, J, K, sg);
+        out[p] = sg == 0 ? 0.0 : (sg > 0 ? (double)f[s] : -(double)f[s]);
+    }
+}
+
+// Extract the independent cells of a ghosted FP64 reference array (n1 x n2 x n3) into a device field.
+template <typename T>
+__global__ void __launch_bounds__(256) k_unpack(Dims d, int kind, int n1, int n2, const double *__restrict__ in,
+                                                T *__restrict__ f) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(p % d.Nx);
+        long long q = p / d.Nx;
+        int j = (int)(q % d.Ny), k = (int)(q / d.Ny);
+        T v;
+        if (kind == FK_V && !d.yper && j == d.Ny - 1) v = T(0);   // top wall face
+        else v = (T)in[((long long)(k + 1) * n2 + (j + 1)) * n1 + (i + 1)];
+        f[p] = v;
+    }
+}
+
+// rhs arrays in the reference's interior shapes (2:n1+1, 2:n2+1, 2:n3+1): device element (i,j,k) -> (i,j,k)
+// for i < Nx etc.; the duplicated last periodic cell repeats index 0.
+template <typename T>
+__global__ void __launch_bounds__(256) k_pack_interior(Dims d, int n1, int n2, int n3, const T *__restrict__ f,
+                                                       double *__restrict__ out) {
+    long long n = (long long)n1 * n2 * n3;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(p % n1);
+        long long q = p / n1;
+        int j = (int)(q % n2), k = (int)(q / n2);
+        i = i % d.Nx; k = k % d.Nz; if (d.yper) j = j % d.Ny;
+        out[p] = (double)f[idx3(d, i, j, k)];
+    }
+}
+
+// Wall-stress planes to the reference's tau_x (nx,2,nzg) [is_z = 0] or tau_z (nxg,2,nz) [is_z = 1] shapes.
+// Interior rows map to the device planes; the duplicated periodic row repeats row 0 and the ghost rows copy the
+// nearest computed row, as compute_flat_wall_eqwm does (src/wallmodel.f90:515-522, :571-578).
+__global__ void k_pack_tau(Dims d, int is_z, int n1, int n3, const double *__restrict__ t, double *__restrict__ out) {
+    long long n = (long long)n1 * 2 * n3;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(p % n1) - 1;
+        long long q = p / n1;
+        int iw = (int)(q % 2), k = (int)(q / 2) - 1;
+        if (!is_z) {   // U faces in x (clamp), centres in z (wrap the duplicate and the ghosts to row 0)
+            i = min(max(i, 0), d.Nx - 1);
+            if (k < 0 || k >= d.Nz) k = 0;
+        } else {       // centres in x (wrap), faces in z (clamp)
+            if (i < 0 || i >= d.Nx) i = 0;
+            k = min(max(k, 0), d.Nz - 1);
+        }
+        out[p] = t[((long long)iw * d.Nz + k) * d.Nx + i];
+    }
+}
+
+// Real field in the rhs_p shape (2:nxg, 2:nyg-1, 2:nzg) -> independent centres.
+template <typename T>
+__global__ void __launch_bounds__(256) k_unpack_rhs_p(Dims d, int n1, int n2, const double *__restrict__ in, T *__restrict__ f) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(p % d.Nx);
+        long long q = p / d.Nx;
+        int j = (int)(q % d.Ny), k = (int)(q / d.Ny);
+        f[p] = (T)in[((long long)k * n2 + j) * n1 + i];
+    }
+}
+
+// Independent centres -> rhs_p shape with apply_periodic_xz_pressure's copies (rhs_p(nxg-1) = rhs_p(2),
+// rhs_p(:,:,nzg-1) = rhs_p(:,:,2), periodic y: rhs_p(:,nyg-1,:) = rhs_p(:,2,:)); the outermost planes (nxg, nzg)
+// that the reference leaves unset at one rank are written as copies of the next wrap.
+template <typename T>
+__global__ void __launch_bounds__(256) k_pack_rhs_p(Dims d, int n1, int n2, int n3, const T *__restrict__ f, double *__restrict__ out) {
+    long long n = (long long)n1 * n2 * n3;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(p % n1);
+        long long q = p / n1;
+        int j = (int)(q % n2), k = (int)(q / n2);
+        i = i % d.Nx; k = k % d.Nz; if (d.yper) j = j % d.Ny;
+        out[p] = (double)f[idx3(d, i, j, k)];
+    }
+}
+
+}  // namespace dfdm

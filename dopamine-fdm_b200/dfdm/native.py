@@ -1,0 +1,266 @@
+"""Python host binding of libdfdm.so: one class whose methods carry the names of the reference's subroutines.
+
+Every method calls the C ABI declared in include/dfdm.h.  There is no CPU fallback: if the library is missing
+or no GPU is present the calls raise DfdmError.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_double, c_int, c_size_t, c_void_p
+from typing import Optional
+
+import numpy as np
+
+from . import build as _build
+from .abi import (DFDM_FP32_MIXED, DFDM_FP64, PRECISIONS, DfdmGrid, DfdmParams, GridHolder, dptr,
+                  make_params)
+from .cases import Case
+
+_lib = None
+
+KERNELS = {"sgs": 0, "stage": 1, "fwd_x": 2, "fwd_z": 3, "y_solve": 4, "inv_z": 5, "inv_x": 6, "correct": 7,
+           "wall_model": 8, "flux_shift": 9}
+
+# Every exported symbol of include/dfdm.h (checked by the CPU test suite).
+EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_create", "dfdm_destroy",
+           "dfdm_footprint_bytes", "dfdm_set_stream", "dfdm_synchronize", "dfdm_set_state", "dfdm_get_state",
+           "dfdm_get_nu_t", "dfdm_set_nu_t", "dfdm_set_time", "dfdm_get_time", "dfdm_compute_time_step_rk3",
+           "dfdm_compute_time_step_rk3_async", "dfdm_enable_graphs", "dfdm_compute_sgs_model", "dfdm_compute_rhs",
+           "dfdm_compute_wall_model", "dfdm_apply_boundary_conditions", "dfdm_compute_projection_step",
+           "dfdm_solve_poisson", "dfdm_compute_bulk_velocity", "dfdm_check_divergence", "dfdm_kinetic_energy",
+           "dfdm_check_finite", "dfdm_pad_field", "dfdm_launch_kernel_async", "dfdm_kernel_bytes",
+           "dfdm_launch_count"]
+
+
+class DfdmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"dfdm error {code}: {msg}")
+        self.code = code
+
+
+def lib_path() -> str:
+    return _build.LIB_PATH
+
+
+def load(build_if_missing: bool = True):
+    """Load libdfdm.so (building it with nvcc first when it is absent and nvcc exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIB_PATH
+    if not os.path.exists(path):
+        if not build_if_missing:
+            raise DfdmError(2, f"{path} is missing; build it with dfdm.build.build()")
+        _build.build()
+    L = ctypes.CDLL(path)
+    P = POINTER(c_double)
+    sig = {
+        "dfdm_default_params": (None, [POINTER(DfdmParams)]),
+        "dfdm_last_error": (c_char_p, []),
+        "dfdm_version": (c_char_p, []),
+        "dfdm_create": (c_int, [POINTER(DfdmGrid), POINTER(DfdmParams), POINTER(c_void_p)]),
+        "dfdm_destroy": (c_int, [c_void_p]),
+        "dfdm_footprint_bytes": (c_int, [POINTER(DfdmGrid), POINTER(DfdmParams), POINTER(c_size_t)]),
+        "dfdm_set_stream": (c_int, [c_void_p, c_void_p]),
+        "dfdm_synchronize": (c_int, [c_void_p]),
+        "dfdm_set_state": (c_int, [c_void_p, P, P, P, P]),
+        "dfdm_get_state": (c_int, [c_void_p, P, P, P, P]),
+        "dfdm_get_nu_t": (c_int, [c_void_p, P]),
+        "dfdm_set_nu_t": (c_int, [c_void_p, P]),
+        "dfdm_set_time": (c_int, [c_void_p, c_double]),
+        "dfdm_get_time": (c_int, [c_void_p, P]),
+        "dfdm_compute_time_step_rk3": (c_int, [c_void_p, c_int, P]),
+        "dfdm_compute_time_step_rk3_async": (c_int, [c_void_p, c_int]),
+        "dfdm_enable_graphs": (c_int, [c_void_p, c_int]),
+        "dfdm_compute_sgs_model": (c_int, [c_void_p]),
+        "dfdm_compute_rhs": (c_int, [c_void_p, P, P, P]),
+        "dfdm_compute_wall_model": (c_int, [c_void_p, c_int, P, P]),
+        "dfdm_apply_boundary_conditions": (c_int, [c_void_p, c_int]),
+        "dfdm_compute_projection_step": (c_int, [c_void_p, c_int]),
+        "dfdm_solve_poisson": (c_int, [c_void_p, P, P]),
+        "dfdm_compute_bulk_velocity": (c_int, [c_void_p, P]),
+        "dfdm_check_divergence": (c_int, [c_void_p, P]),
+        "dfdm_kinetic_energy": (c_int, [c_void_p, P]),
+        "dfdm_check_finite": (c_int, [c_void_p]),
+        "dfdm_pad_field": (c_int, [c_void_p, c_int, c_int, P]),
+        "dfdm_launch_kernel_async": (c_int, [c_void_p, c_int, c_int]),
+        "dfdm_kernel_bytes": (c_int, [c_void_p, c_int, P]),
+        "dfdm_launch_count": (c_int, [c_void_p, POINTER(ctypes.c_longlong)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return load().dfdm_last_error().decode()
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise DfdmError(rc, last_error())
+
+
+def footprint_bytes(case: Case, precision="fp32") -> int:
+    g = GridHolder(case)
+    p = make_params(case, PRECISIONS.get(precision, precision))
+    out = c_size_t(0)
+    _check(load().dfdm_footprint_bytes(ctypes.byref(g.grid), ctypes.byref(p), ctypes.byref(out)))
+    return int(out.value)
+
+
+class Solver:
+    """One case resident on the GPU, driven through the C ABI.
+
+    Method names follow the reference's subroutines: compute_time_step_RK3 (src/time_integration.f90:120),
+    compute_sgs_model (src/sgs_model.f90:27), compute_rhs_u/v/w (src/equations.f90), compute_wall_model
+    (src/wallmodel.f90:197), apply_boundary_conditions (src/boundary_conditions.f90:186),
+    compute_projection_step (src/projection.f90:21), solve_poisson_equation (src/projection.f90:100),
+    compute_bulk_velocity (src/monitor.f90:463) and check_divergence (src/projection.f90:607).
+    """
+
+    def __init__(self, case: Case, precision="fp64", graphs: bool = False, stream: Optional[int] = None):
+        self.case = case
+        self.precision = PRECISIONS.get(precision, precision)
+        self._g = GridHolder(case)
+        self._p = make_params(case, self.precision)
+        self.shapes = case.shapes()
+        h = c_void_p()
+        _check(load().dfdm_create(ctypes.byref(self._g.grid), ctypes.byref(self._p), ctypes.byref(h)))
+        self.h = h
+        if stream is not None:
+            self.set_stream(stream)
+        if graphs:
+            _check(load().dfdm_enable_graphs(self.h, 1))
+
+    # ---- lifetime ----
+    def close(self):
+        if getattr(self, "h", None):
+            load().dfdm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream: Optional[int]):
+        _check(load().dfdm_set_stream(self.h, c_void_p(stream) if stream else None))
+
+    def synchronize(self):
+        _check(load().dfdm_synchronize(self.h))
+
+    def enable_graphs(self, on: bool = True):
+        _check(load().dfdm_enable_graphs(self.h, int(on)))
+
+    # ---- state ----
+    def _arr(self, key):
+        return np.zeros(self.shapes[key], order="F")
+
+    def set_state(self, U, V, W, P=None):
+        f = lambda a: None if a is None else np.asfortranarray(a, dtype=np.float64)
+        U, V, W, P = f(U), f(V), f(W), f(P)
+        _check(load().dfdm_set_state(self.h, dptr(U), dptr(V), dptr(W), dptr(P)))
+
+    def get_state(self, out=None):
+        U, V, W, P = out if out is not None else (self._arr("U"), self._arr("V"), self._arr("W"), self._arr("P"))
+        _check(load().dfdm_get_state(self.h, dptr(U), dptr(V), dptr(W), dptr(P)))
+        return U, V, W, P
+
+    def get_nu_t(self):
+        a = self._arr("P")
+        _check(load().dfdm_get_nu_t(self.h, dptr(a)))
+        return a
+
+    def set_nu_t(self, a):
+        a = np.asfortranarray(a, dtype=np.float64)
+        _check(load().dfdm_set_nu_t(self.h, dptr(a)))
+
+    @property
+    def t(self) -> float:
+        v = c_double(0.0)
+        _check(load().dfdm_get_time(self.h, ctypes.byref(v)))
+        return v.value
+
+    # ---- the step ----
+    def compute_time_step_RK3(self, nsteps: int = 1) -> float:
+        t = c_double(0.0)
+        _check(load().dfdm_compute_time_step_rk3(self.h, int(nsteps), ctypes.byref(t)))
+        return t.value
+
+    def compute_time_step_RK3_async(self, nsteps: int = 1) -> None:
+        _check(load().dfdm_compute_time_step_rk3_async(self.h, int(nsteps)))
+
+    # ---- unit entry points ----
+    def compute_sgs_model(self):
+        _check(load().dfdm_compute_sgs_model(self.h))
+
+    def compute_rhs(self):
+        fu, fv, fw = self._arr("rhs_u"), self._arr("rhs_v"), self._arr("rhs_w")
+        _check(load().dfdm_compute_rhs(self.h, dptr(fu), dptr(fv), dptr(fw)))
+        return fu, fv, fw
+
+    def compute_wall_model(self, update_filter: bool = True):
+        tx, tz = self._arr("tau_x"), self._arr("tau_z")
+        _check(load().dfdm_compute_wall_model(self.h, int(update_filter), dptr(tx), dptr(tz)))
+        return tx, tz
+
+    def apply_boundary_conditions(self, after_projection: bool = False):
+        _check(load().dfdm_apply_boundary_conditions(self.h, int(after_projection)))
+
+    def compute_projection_step(self, save_p: bool = False):
+        _check(load().dfdm_compute_projection_step(self.h, int(save_p)))
+
+    def solve_poisson_equation(self, rhs_p):
+        a = np.asfortranarray(rhs_p, dtype=np.float64)
+        out = np.zeros_like(a, order="F")
+        _check(load().dfdm_solve_poisson(self.h, dptr(a), dptr(out)))
+        return out
+
+    def compute_bulk_velocity(self) -> float:
+        v = c_double(0.0)
+        _check(load().dfdm_compute_bulk_velocity(self.h, ctypes.byref(v)))
+        return v.value
+
+    def check_divergence(self) -> float:
+        v = c_double(0.0)
+        _check(load().dfdm_check_divergence(self.h, ctypes.byref(v)))
+        return v.value
+
+    def kinetic_energy(self) -> float:
+        v = c_double(0.0)
+        _check(load().dfdm_kinetic_energy(self.h, ctypes.byref(v)))
+        return v.value
+
+    def check_finite(self) -> None:
+        _check(load().dfdm_check_finite(self.h))
+
+    def pad_field(self, field: int = 1, extra_planes: int = 1):
+        _check(load().dfdm_pad_field(self.h, int(field), int(extra_planes), None))
+
+    # ---- profiling hooks ----
+    def launch_kernel_async(self, which, rk_stage: int = 2):
+        which = KERNELS.get(which, which)
+        _check(load().dfdm_launch_kernel_async(self.h, int(which), int(rk_stage)))
+
+    def launch_count(self) -> int:
+        v = ctypes.c_longlong(0)
+        _check(load().dfdm_launch_count(self.h, ctypes.byref(v)))
+        return int(v.value)
+
+    def kernel_bytes(self, which) -> float:
+        which = KERNELS.get(which, which)
+        v = c_double(0.0)
+        _check(load().dfdm_kernel_bytes(self.h, int(which), ctypes.byref(v)))
+        return v.value

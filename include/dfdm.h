@@ -1,0 +1,163 @@
+/*
+ * dfdm.h -- C ABI of the B200 library for dopamine-fdm's single-phase fractional-step RK3 time step.
+ *
+ * The library replaces, on one GPU, the Fortran subroutines that make up one time step of the reference
+ * solver (the RK3 driver, the momentum right-hand side, the AMD/Vreman eddy viscosity, the flat-wall
+ * equilibrium wall model, the FFT x tridiagonal pressure Poisson solve with the velocity correction, and the
+ * ghost fills). Every entry point is a plain C function with plain pointers and sizes, so a Fortran host can
+ * bind it through ISO_C_BINDING (Bind(C, name="dfdm_...")).
+ *
+ * Array conventions (all host arrays): IEEE double, Fortran column-major order, in the reference's ghosted
+ * one-rank shapes with nxg = nx+1, nyg = ny+1, nzg = nz+1 (nx, ny, nz = namelist face counts):
+ *   U (nx ,nyg,nzg)   V (nxg,ny ,nzg)   W (nxg,nyg,nz )   P, nu_t (nxg,nyg,nzg)
+ *   rhs_u (2:nx-1,2:nyg-1,2:nzg-1)  rhs_v (2:nxg-1,2:ny-1,2:nzg-1)  rhs_w (2:nxg-1,2:nyg-1,2:nz-1)
+ *   rhs_p (2:nxg,2:nyg-1,2:nzg)
+ * On the device the library keeps only the independent cells (periodic duplicates and ghosts are implied by
+ * the boundary rules), in FP64 or in FP32 storage (DFDM_FP32_MIXED). Ghosts are regenerated on every copy
+ * back to the host, exactly as apply_boundary_conditions / finish_pressure_ghosts would leave them.
+ *
+ * Every function returns a status code (DFDM_OK = 0); dfdm_last_error() gives the message of the last
+ * failure on the calling thread. A context owns one CUDA stream and all of its device memory; contexts are not
+ * thread-safe. Calls are synchronous unless their name ends in _async.
+ */
+#ifndef DFDM_H
+#define DFDM_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define DFDM_OK               0
+#define DFDM_ERR_INVALID      1   /* invalid argument or grid */
+#define DFDM_ERR_CUDA         2   /* CUDA runtime error (message in dfdm_last_error) */
+#define DFDM_ERR_NOMEM        3   /* device allocation failed */
+#define DFDM_ERR_UNSUPPORTED  4   /* configuration outside the single-phase path */
+#define DFDM_ERR_NOT_FINITE   5   /* NaN/Inf or |U| > 1e8 found by the monitor guard */
+#define DFDM_ERR_TIMEOUT      6   /* a bounded device wait gave up */
+
+/* ---- storage precision ---- */
+#define DFDM_FP64        0   /* plain FP64: every field and every kernel in double */
+#define DFDM_FP32_MIXED  1   /* FP32 fields, stencils and FFTs; FP64 tridiagonal solves and reductions */
+
+/* Grid of one case (one rank of the reference: x_global = x etc.).
+ * Mirrors the &DOMAIN / &BOUNDARY_CONDITIONS namelists (src/input_output.f90:29-107) and the face arrays built
+ * by generateGrid (src/genGridandIC.f90:14-265). Centres, ghost centres, dx/dz, weights, modified wavenumbers
+ * and the Dyy operator are derived inside the library exactly as src/initialization.f90:243-644 does. */
+typedef struct dfdm_grid {
+    int nx, ny, nz;            /* face counts (namelist nx, ny, nz); nx and nz even */
+    const double *x;           /* x(1:nx) face coordinates, uniform */
+    const double *y;           /* y(1:ny) face coordinates, may be stretched */
+    const double *z;           /* z(1:nz) face coordinates, uniform */
+    int x_bc_type;             /* 0 periodic (the only value on this path) */
+    int y_bc_type;             /* 0 periodic, 1 walls */
+    int z_bc_type;             /* 0 periodic (the only value on this path) */
+    int bc_face_ylo, bc_face_yhi; /* 1 no-slip (the only value on this path) */
+} dfdm_grid;
+
+/* Physics and numerics of one case (&PHYSICS / &NUMERICS subset the step reads; defaults in
+ * src/global.f90:305-312 and src/input_output.f90:109-127). Automatic values (-1) are resolved as
+ * src/input_output.f90:938-940 (adv_wall_layers) and :967-970 (wm_filter_mode) do. */
+typedef struct dfdm_params {
+    double nu;                 /* kinematic viscosity */
+    double dt;                 /* fixed time step (cfl_adaptive = 0) */
+    double dPdx, dPdz;         /* imposed mean pressure gradients (flow_forcing_mode = 0) */
+    int    sgs_model;          /* 0 DNS, 1 Vreman, 2 AMD */
+    double Cs_vreman;          /* Vreman constant (0.17) */
+    double C_amd;              /* AMD constant (1/3) */
+    int    flat_wall_model_flag; /* 0 no-slip walls, 1 smooth Reichardt EQWM */
+    int    advection_scheme;   /* 0 skew-symmetric blend, 1 divergence form */
+    int    adv_wall_layers;    /* -1 automatic */
+    int    wm_filter_mode;     /* -1 automatic, 0 raw, 1 temporal filter */
+    double wm_filter_Tf_fac;   /* filter time-scale factor (1.0) */
+    int    flow_forcing_mode;  /* 0 prescribed dPdx, 1 constant flux */
+    double Ub_target;          /* bulk velocity target of the constant-flux forcing */
+    int    precision;          /* DFDM_FP64 or DFDM_FP32_MIXED */
+} dfdm_params;
+
+typedef struct dfdm_ctx dfdm_ctx;
+
+/* Fill *p with the reference defaults (src/global.f90:305-312, src/input_output.f90:109-127). */
+void dfdm_default_params(dfdm_params *p);
+
+/* Text of the last failure on this thread ("" after success). */
+const char *dfdm_last_error(void);
+
+/* Library version string. */
+const char *dfdm_version(void);
+
+/* ---- lifetime: replaces initialize's device part (src/initialization.f90:37-862) ---- */
+int dfdm_create(const dfdm_grid *grid, const dfdm_params *params, dfdm_ctx **out);
+int dfdm_destroy(dfdm_ctx *ctx);
+/* Bytes of device memory a context of this grid and precision would hold (serving admission). */
+int dfdm_footprint_bytes(const dfdm_grid *grid, const dfdm_params *params, size_t *bytes);
+
+/* Run the context's work on an externally owned CUDA stream (cudaStream_t passed as void*); NULL restores the
+ * context's own stream. */
+int dfdm_set_stream(dfdm_ctx *ctx, void *cuda_stream);
+int dfdm_synchronize(dfdm_ctx *ctx);
+
+/* ---- state transfer: the reference's U, V, W, P, nu_t module arrays (src/global.f90:139,300) ----
+ * set_state reads the interior (independent) cells; ghosts are implied. P may be NULL. */
+int dfdm_set_state(dfdm_ctx *ctx, const double *U, const double *V, const double *W, const double *P);
+int dfdm_get_state(dfdm_ctx *ctx, double *U, double *V, double *W, double *P);
+int dfdm_get_nu_t(dfdm_ctx *ctx, double *nu_t);
+int dfdm_set_nu_t(dfdm_ctx *ctx, const double *nu_t);
+int dfdm_set_time(dfdm_ctx *ctx, double t);
+int dfdm_get_time(dfdm_ctx *ctx, double *t);
+
+/* ---- the step: compute_time_step_RK3 (src/time_integration.f90:120-713) ----
+ * Advances nsteps full RK3 steps on the resident state and returns the new time in *t (may be NULL). */
+int dfdm_compute_time_step_rk3(dfdm_ctx *ctx, int nsteps, double *t);
+/* Same, enqueued on the context's stream without a host synchronisation. */
+int dfdm_compute_time_step_rk3_async(dfdm_ctx *ctx, int nsteps);
+/* Capture one full step in a CUDA graph on first use and replay it (same numerics as the plain call). */
+int dfdm_enable_graphs(dfdm_ctx *ctx, int enable);
+
+/* ---- unit entry points, one per reference subroutine, on the resident state ---- */
+/* compute_sgs_model(U,V,W,nu_t) (src/sgs_model.f90:27-45, ghosts :538-609) */
+int dfdm_compute_sgs_model(dfdm_ctx *ctx);
+/* compute_rhs_u / _v / _w (src/equations.f90:25-257, :261-485, :489-721) on the resident U,V,W,nu_t and wall
+ * stresses; results in the reference's rhs shapes. Any output pointer may be NULL. */
+int dfdm_compute_rhs(dfdm_ctx *ctx, double *rhs_u, double *rhs_v, double *rhs_w);
+/* update_wm_filter + compute_wall_model (src/wallmodel.f90:397-439, :197-233, :442-583); tau_x (nx,2,nzg) and
+ * tau_z (nxg,2,nz) may be NULL. update_filter = 1 advances the temporal filter first (stage 1 of a step). */
+int dfdm_compute_wall_model(dfdm_ctx *ctx, int update_filter, double *tau_x, double *tau_z);
+/* apply_boundary_conditions (src/boundary_conditions.f90:186-260). On the device the ghost cells are implied by
+ * the index rules, so this validates the context and returns; kept for drop-in completeness. */
+int dfdm_apply_boundary_conditions(dfdm_ctx *ctx, int after_projection);
+/* compute_projection_step (src/projection.f90:21-34): div, Poisson solve and velocity correction of the
+ * resident velocity. save_p = 1 also stores P = phi/(dt*3/4) as the third RK stage does. */
+int dfdm_compute_projection_step(dfdm_ctx *ctx, int save_p);
+/* solve_poisson_equation's solve alone (src/projection.f90:100-382): rhs_p in, pseudo-pressure out, both in
+ * the reference shape (2:nxg,2:nyg-1,2:nzg); the output ghost planes follow apply_periodic_xz_pressure. */
+int dfdm_solve_poisson(dfdm_ctx *ctx, const double *rhs_p_in, double *phi_out);
+/* compute_bulk_velocity (src/monitor.f90:463-523), FP64 compensated sum. */
+int dfdm_compute_bulk_velocity(dfdm_ctx *ctx, double *Ub);
+/* check_divergence (src/projection.f90:607-639): max |div u| over the interior. */
+int dfdm_check_divergence(dfdm_ctx *ctx, double *max_div);
+/* Kinetic energy 0.5*<u.u> (volume-weighted, compensated sum) -- diagnostic with no reference counterpart. */
+int dfdm_kinetic_energy(dfdm_ctx *ctx, double *ke);
+/* Monitor guard of output_monitor (src/monitor.f90:32-52): DFDM_ERR_NOT_FINITE if any velocity is NaN/Inf or
+ * |U| > 1e8. */
+int dfdm_check_finite(dfdm_ctx *ctx);
+/* pad_field_dev (src/halo_pad.f90:185-194) is called only by the hybrid advection scheme, the immersed
+ * boundary and the particles, none of which is on the single-phase path: returns DFDM_ERR_UNSUPPORTED. */
+int dfdm_pad_field(dfdm_ctx *ctx, int field, int extra_planes, double *out);
+
+/* ---- profiling hooks: launch one kernel family of one RK stage on the context's stream, no sync ----
+ * which: 0 SGS, 1 stage (RHS + RK update), 2 div + forward x-FFT, 3 forward z-FFT, 4 y solve,
+ *        5 inverse z-FFT, 6 inverse x-FFT, 7 velocity correction */
+int dfdm_launch_kernel_async(dfdm_ctx *ctx, int which, int rk_stage);
+/* Algorithmic HBM bytes one launch of that kernel family moves (the roofline numerator). */
+int dfdm_kernel_bytes(dfdm_ctx *ctx, int which, double *bytes);
+/* Number of the library's own kernels enqueued by this context so far (graph replays included). */
+int dfdm_launch_count(dfdm_ctx *ctx, long long *count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DFDM_H */

@@ -1,0 +1,78 @@
+"""CPU tests of the drop-in boundary: the C-ABI library loads, exports every symbol include/dfdm.h declares,
+validates its inputs like the reference's input checks, and refuses to run without a GPU (no CPU fallback)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, has_gpu
+from dfdm import abi, cases, native
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "dfdm.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:int|void|const char \*)\s*(dfdm_\w+)\s*\(", text, re.M)))
+
+
+def test_library_builds_and_exports_every_header_symbol():
+    L = native.load()
+    declared = header_symbols()
+    assert declared, "no declarations parsed from include/dfdm.h"
+    assert sorted(native.EXPORTS) == declared
+    for name in declared:
+        assert hasattr(L, name), name
+    assert b"sm_100a" in L.dfdm_version()
+
+
+def test_default_params_match_reference_defaults():
+    L = native.load()
+    p = abi.DfdmParams()
+    L.dfdm_default_params(ctypes.byref(p))
+    assert p.sgs_model == 2 and abs(p.Cs_vreman - 0.17) < 1e-15 and abs(p.C_amd - 1.0 / 3.0) < 1e-15
+    assert p.adv_wall_layers == -1 and p.wm_filter_mode == -1 and p.flat_wall_model_flag == 0
+
+
+@pytest.mark.parametrize("mutate,code,msg", [
+    (dict(nx=17), 1, "even"),
+    (dict(sgs_model=3), 1, "sgs_model"),
+    (dict(advection_scheme=2), 4, "hybrid"),
+    (dict(flat_wall_model_flag=2), 4, "rough"),
+    (dict(dt=0.0), 1, "dt"),
+])
+def test_invalid_inputs_are_rejected_with_the_reference_message(mutate, code, msg):
+    c = cases.chan_small().with_(**mutate)
+    with pytest.raises(native.DfdmError) as e:
+        native.footprint_bytes(c)
+    assert e.value.code == code and msg in str(e.value)
+
+
+def test_footprint_scales_with_precision():
+    c = cases.chan550()
+    b64 = native.footprint_bytes(c, "fp64")
+    b32 = native.footprint_bytes(c, "fp32")
+    assert 1.9 < b64 / b32 < 2.05
+    assert b32 < 2e9   # the 13M-cell throughput case fits easily in 180 GB
+
+
+def test_every_config_has_supported_transform_lengths():
+    for name in ("tgv64", "chan180", "les395", "chan550", "tgv_small", "chan_small", "chan_les_amd_small"):
+        c = cases.get(name)
+        assert native.footprint_bytes(c, "fp64") > 0
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-GPU behaviour")
+def test_no_cpu_fallback_without_gpu():
+    with pytest.raises(native.DfdmError) as e:
+        native.Solver(cases.chan_small())
+    assert e.value.code == 2 and "no CPU fallback" in str(e.value)
+
+
+def test_case_shapes_follow_the_reference_allocation():
+    c = cases.chan550()
+    s = c.shapes()
+    assert s["U"] == (258, 194, 259) and s["V"] == (259, 193, 259) and s["W"] == (259, 194, 258)
+    assert c.cells == (256, 192, 256) and c.n_cells == 12582912
+    t = cases.tgv()
+    assert t.cells == (64, 64, 64)
