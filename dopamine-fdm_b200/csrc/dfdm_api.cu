@@ -73,6 +73,7 @@ struct dfdm_ctx {
     void *tw_x = nullptr, *twr_x = nullptr, *tw_z = nullptr, *tw_y = nullptr;
     FFTPlan plan_x{}, plan_z{}, plan_y{};
     double *d_kxx = nullptr, *d_kzz = nullptr, *d_kyy = nullptr, *d_lo = nullptr, *d_di = nullptr, *d_up = nullptr;
+    double *d_rpiv = nullptr;                   // 1/D(r) of every (kx,kz) tridiagonal system, layout (kz, r, kx)
     double *d_dxc = nullptr, *d_dyc = nullptr, *d_dzc = nullptr;
     WallState wsd{};
     double *red_part = nullptr, *red_out = nullptr;
@@ -83,6 +84,7 @@ struct dfdm_ctx {
     size_t staging_n = 0;
     // launch geometry
     int lx = 8, tzx = 8;
+    int kc_stage = 8, kc_sgs = 8;               // z-planes per block of the tiled kernels
     size_t smem_x = 0, smem_z = 0, smem_y = 0, smem_ys = 0;
     cudaStream_t own_stream = nullptr, stream = nullptr;
     double t = 0.0;
@@ -91,6 +93,7 @@ struct dfdm_ctx {
     bool graphs = false;
     cudaGraphExec_t gexec = nullptr;
     cudaGraph_t graph = nullptr;
+    bool unit_projection = false;    // dfdm_compute_projection_step: u* is the resident state, not an increment
     long long launches = 0;          // kernels enqueued (host-side count)
     long long graph_launches = 0;    // kernels in the captured step graph
 };
@@ -208,14 +211,29 @@ template <typename T> PoissonArgs<T> poisson_args(dfdm_ctx *c) {
     a.inv_dx = (T)(1.0 / c->dx);
     a.norm = (double)((long long)c->d.Nx * (long long)c->d.Nz);
     a.pdiv = c->prm.dt * (3.0 / 4.0);
+    a.fNx = make_fastdiv((unsigned)c->d.Nx);
+    a.fNy = make_fastdiv((unsigned)c->d.Ny);
+    a.fM = make_fastdiv((unsigned)(c->d.Nx / 2));
+    a.fM1 = make_fastdiv((unsigned)(c->d.Nx / 2 + 1));
     return a;
 }
 
 dim3 cell_grid(const Dims &d) { return dim3((d.Nx + 31) / 32, (d.Ny + 7) / 8, d.Nz); }
 const dim3 CELL_BLOCK(32, 8, 1);
+constexpr int TILE_X = 32, TILE_Y = 8;   // (i,j) tile of the 2.5-D blocked kernels
+dim3 tile_grid(const Dims &d, int kc) { return dim3((d.Nx + TILE_X - 1) / TILE_X, (d.Ny + TILE_Y - 1) / TILE_Y, (d.Nz + kc - 1) / kc); }
+// z-planes per block: enough blocks for about four waves at the measured occupancy, at most 32 planes
+int choose_kc(const Dims &d, int blocks_per_sm, int nsm) {
+    long long cols = (long long)((d.Nx + TILE_X - 1) / TILE_X) * ((d.Ny + TILE_Y - 1) / TILE_Y);
+    long long want = 4LL * nsm * std::max(1, blocks_per_sm);
+    long long chunks = std::max(1LL, (want + cols - 1) / cols);
+    int kc = (int)((d.Nz + chunks - 1) / chunks);
+    return std::max(2, std::min(32, kc));
+}
 
 template <typename T> struct Impl {
     typedef typename cplx_t<T>::type C;
+    static constexpr int CT = (sizeof(T) == 8) ? 8 : 16;   // kx columns per block of the column transforms
     static T *f(void *p) { return (T *)p; }
 
     static int setup_kernels(dfdm_ctx *c) {
@@ -223,19 +241,49 @@ template <typename T> struct Impl {
         const int M = d.Nx / 2;
         c->lx = std::max(1, std::min(64, 1024 / std::max(1, M)));
         c->smem_x = 2 * (size_t)c->lx * M * sizeof(C);
-        c->tzx = (sizeof(T) == 8) ? 8 : 16;
+        c->tzx = CT;
         c->smem_z = 2 * (size_t)d.Nz * c->tzx * sizeof(C);
         c->smem_y = 2 * (size_t)d.Ny * c->tzx * sizeof(C);
-        c->smem_ys = (size_t)d.Ny * 32 * sizeof(double);
+        c->smem_ys = (size_t)d.Ny * 32 * sizeof(C);
         size_t maxs = std::max(std::max(c->smem_x, c->smem_z), std::max(c->smem_y, c->smem_ys));
         if (maxs > 227 * 1024) return fail(DFDM_ERR_UNSUPPORTED, "grid too large for the shared-memory transforms");
         CK(cudaFuncSetAttribute(k_fwd_x<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_x));
         CK(cudaFuncSetAttribute(k_fwd_x<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_x));
         CK(cudaFuncSetAttribute(k_inv_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_x));
-        CK(cudaFuncSetAttribute(k_col_fft<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(c->smem_z, c->smem_y)));
-        CK(cudaFuncSetAttribute(k_col_fft<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(c->smem_z, c->smem_y)));
-        CK(cudaFuncSetAttribute(k_col_fft<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(c->smem_z, c->smem_y)));
+        int cs = (int)std::max(c->smem_z, c->smem_y);
+        CK(cudaFuncSetAttribute(k_col_fft<T, 0, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs));
+        CK(cudaFuncSetAttribute(k_col_fft<T, 1, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs));
+        CK(cudaFuncSetAttribute(k_col_fft<T, 2, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs));
         CK(cudaFuncSetAttribute(k_ysolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ys));
+        int dev = 0, nsm = 148, occ = 1;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        if (c->les) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tiled<T, true, TILE_X, TILE_Y, 0>, TILE_X * TILE_Y, 0));
+        else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tiled<T, false, TILE_X, TILE_Y, 0>, TILE_X * TILE_Y, 0));
+        c->kc_stage = choose_kc(d, occ, nsm);
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tiled<T, false, TILE_X, TILE_Y, 1>, TILE_X * TILE_Y, 0));
+        c->kc_sgs = choose_kc(d, occ, nsm);
+        return DFDM_OK;
+    }
+
+    // FP32-mixed stage 3 carries the increment du = u* - uo through the projection: div(du) has no FP32
+    // cancellation, so the saved pressure P = phi/(dt*3/4) does not inherit the O(eps |u| dx / dt) noise that the
+    // rounding of the stored velocity would otherwise put into phi.  Stages 1-2 and the FP64 form keep the
+    // reference's u* = uo + du exactly.
+    static bool incr_form(const dfdm_ctx *c, int s) { return c->prec == DFDM_FP32_MIXED && s == 3 && !c->unit_projection; }
+
+    static int stage_kernel(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
+        const Dims &d = c->d;
+        dim3 g = tile_grid(d, c->kc_stage);
+        if (c->les)
+            k_tiled<T, true, TILE_X, TILE_Y, 0><<<g, TILE_X * TILE_Y, 0, c->stream>>>(step_args<T>(c), f(c->u), f(c->v),
+                f(c->w), f(c->nut), c->wsd.tau_x, c->wsd.tau_z, sc, c->kc_stage, f(c->uo), f(c->vo), f(c->wo), f(c->f1u),
+                f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf), rhs_only, nullptr);
+        else
+            k_tiled<T, false, TILE_X, TILE_Y, 0><<<g, TILE_X * TILE_Y, 0, c->stream>>>(step_args<T>(c), f(c->u), f(c->v),
+                f(c->w), nullptr, c->wsd.tau_x, c->wsd.tau_z, sc, c->kc_stage, f(c->uo), f(c->vo), f(c->wo), f(c->f1u),
+                f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf), rhs_only, nullptr);
+        CKL();
         return DFDM_OK;
     }
 
@@ -246,7 +294,10 @@ template <typename T> struct Impl {
         switch (which) {
         case 0: {   // SGS
             if (!c->les) return DFDM_OK;
-            k_sgs<T><<<cell_grid(d), CELL_BLOCK, 0, st>>>(step_args<T>(c), f(c->u), f(c->v), f(c->w), f(c->nut));
+            StageCoef sc{1, 0.0, 0.0, 0.0, 0.0, 0};
+            k_tiled<T, false, TILE_X, TILE_Y, 1><<<tile_grid(d, c->kc_sgs), TILE_X * TILE_Y, 0, st>>>(
+                step_args<T>(c), f(c->u), f(c->v), f(c->w), nullptr, nullptr, nullptr, sc, c->kc_sgs, nullptr, nullptr,
+                nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, f(c->nut));
             CKL();
             return DFDM_OK;
         }
@@ -271,17 +322,10 @@ template <typename T> struct Impl {
             sc.stage = s;
             sc.dt_a11 = c->prm.dt * (8.0 / 15.0);
             sc.dt = c->prm.dt;
-            sc.c1 = (s == 2) ? 1.0 / 4.0 : 1.0 / 4.0;
+            sc.c1 = 1.0 / 4.0;
             sc.c2 = (s == 2) ? 5.0 / 12.0 : 3.0 / 4.0;
-            Fields<T> fl{f(c->u), f(c->v), f(c->w), f(c->nut)};
-            if (c->les)
-                k_stage<T, true><<<cell_grid(d), CELL_BLOCK, 0, st>>>(step_args<T>(c), fl, c->wsd.tau_x, c->wsd.tau_z, sc,
-                    f(c->uo), f(c->vo), f(c->wo), f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf), nullptr);
-            else
-                k_stage<T, false><<<cell_grid(d), CELL_BLOCK, 0, st>>>(step_args<T>(c), fl, c->wsd.tau_x, c->wsd.tau_z, sc,
-                    f(c->uo), f(c->vo), f(c->wo), f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf), nullptr);
-            CKL();
-            return DFDM_OK;
+            sc.incr = incr_form(c, s);
+            return stage_kernel(c, sc, nullptr);
         }
         case 2: {   // div + forward x
             long long lines = (long long)d.Ny * d.Nz;
@@ -294,19 +338,19 @@ template <typename T> struct Impl {
         case 3: case 5: {   // z transforms
             dim3 g((d.Nxc + c->tzx - 1) / c->tzx, d.Ny);
             if (which == 3)
-                k_col_fft<T, 0><<<g, 256, c->smem_z, st>>>(d, c->tzx, (C *)c->spec, c->plan_z, (const C *)c->tw_z, c->d_kxx, c->d_kyy, c->d_kzz);
+                k_col_fft<T, 0, CT><<<g, 256, c->smem_z, st>>>(d, (C *)c->spec, c->plan_z, (const C *)c->tw_z, c->d_kxx, c->d_kyy, c->d_kzz);
             else
-                k_col_fft<T, 1><<<g, 256, c->smem_z, st>>>(d, c->tzx, (C *)c->spec, c->plan_z, (const C *)c->tw_z, c->d_kxx, c->d_kyy, c->d_kzz);
+                k_col_fft<T, 1, CT><<<g, 256, c->smem_z, st>>>(d, (C *)c->spec, c->plan_z, (const C *)c->tw_z, c->d_kxx, c->d_kyy, c->d_kzz);
             CKL();
             return DFDM_OK;
         }
         case 4: {   // y solve
             if (d.yper) {
                 dim3 g((d.Nxc + c->tzx - 1) / c->tzx, d.Nz);
-                k_col_fft<T, 2><<<g, 256, c->smem_y, st>>>(d, c->tzx, (C *)c->spec, c->plan_y, (const C *)c->tw_y, c->d_kxx, c->d_kyy, c->d_kzz);
+                k_col_fft<T, 2, CT><<<g, 256, c->smem_y, st>>>(d, (C *)c->spec, c->plan_y, (const C *)c->tw_y, c->d_kxx, c->d_kyy, c->d_kzz);
             } else {
                 dim3 g((d.Nxc + 31) / 32, d.Nz);
-                k_ysolve<T><<<g, 32, c->smem_ys, st>>>(d, (C *)c->spec, c->d_kxx, c->d_kzz, c->d_lo, c->d_di, c->d_up);
+                k_ysolve<T><<<g, 32, c->smem_ys, st>>>(d, (C *)c->spec, c->d_rpiv, c->d_lo, c->d_up);
             }
             CKL();
             return DFDM_OK;
@@ -320,8 +364,11 @@ template <typename T> struct Impl {
             return DFDM_OK;
         }
         case 7: {   // correction (+ P at stage 3)
+            bool inc = incr_form(c, s);
             k_correct<T><<<cell_grid(d), CELL_BLOCK, 0, st>>>(poisson_args<T>(c), f(c->phi), f(c->us), f(c->vs), f(c->wsf),
-                                                              f(c->u), f(c->v), f(c->w), s == 3 ? f(c->p) : nullptr);
+                                                              f(c->u), f(c->v), f(c->w), s == 3 ? f(c->p) : nullptr,
+                                                              inc ? f(c->uo) : nullptr, inc ? f(c->vo) : nullptr,
+                                                              inc ? f(c->wo) : nullptr);
             CKL();
             return DFDM_OK;
         }
@@ -423,6 +470,8 @@ int validate(const dfdm_grid *g, const dfdm_params *p) {
     if (!make_fft_plan(Nx / 2, tmp) || !make_fft_plan(Nz, tmp) || (g->y_bc_type == 0 && !make_fft_plan(Ny, tmp)))
         return fail(DFDM_ERR_UNSUPPORTED, "transform lengths must factor into 2, 3 and 5");
     if (Ny > MAX_NY) return fail(DFDM_ERR_UNSUPPORTED, "ny too large for the y solve");
+    if ((double)Nx * Ny * Nz * 3.0 >= 2147483647.0)
+        return fail(DFDM_ERR_UNSUPPORTED, "grid too large for one context (32-bit cell indexing)");
     for (int i = 1; i < g->nx; ++i) if (!(g->x[i] > g->x[i - 1])) return fail(DFDM_ERR_INVALID, "x faces must increase");
     for (int i = 1; i < g->ny; ++i) if (!(g->y[i] > g->y[i - 1])) return fail(DFDM_ERR_INVALID, "y faces must increase");
     for (int i = 1; i < g->nz; ++i) if (!(g->z[i] > g->z[i - 1])) return fail(DFDM_ERR_INVALID, "z faces must increase");
@@ -613,6 +662,26 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
     c->d_di = (double *)tmp;
     if ((rc = upload_as<double>(c, &tmp, up))) return bail(rc);
     c->d_up = (double *)tmp;
+    if (!c->yper) {
+        // pivots of the no-interchange zgtsv elimination of every (kx,kz) system (src/projection.f90:284-295)
+        std::vector<double> rpiv((size_t)d.Nxc * d.Ny * d.Nz);
+        for (int kz = 0; kz < d.Nz; ++kz)
+            for (int kx = 0; kx < d.Nxc; ++kx) {
+                double lam = kxx[kx] + kzz[kz];
+                double D = di[0] + lam;
+                if (kx == 0 && kz == 0) D = 3.0 / 2.0 * D;
+                size_t b = (size_t)kz * d.Ny * d.Nxc + kx;
+                rpiv[b] = 1.0 / D;
+                for (int r = 1; r < d.Ny; ++r) {
+                    double m = lo[r] / D;
+                    D = (di[r] + lam) - m * up[r - 1];
+                    if (D == 0.0) return bail(fail(DFDM_ERR_INVALID, "singular pressure operator"));
+                    rpiv[b + (size_t)r * d.Nxc] = 1.0 / D;
+                }
+            }
+        if ((rc = upload_as<double>(c, &tmp, rpiv))) return bail(rc);
+        c->d_rpiv = (double *)tmp;
+    }
 
     // ---- FFT plans and twiddles ----
     make_fft_plan(d.Nx / 2, c->plan_x);
@@ -858,17 +927,8 @@ int dfdm_compute_rhs(dfdm_ctx *c, double *rhs_u, double *rhs_v, double *rhs_w) {
     }
     int rc = dispatch(c, [&](auto impl) {
         typedef decltype(impl) I;
-        typedef typename std::remove_pointer<decltype(I::f(nullptr))>::type T;
-        StageCoef sc{1, 0.0, 0.0, 0.0, 0.0};
-        Fields<T> fl{I::f(c->u), I::f(c->v), I::f(c->w), I::f(c->nut)};
-        if (c->les)
-            k_stage<T, true><<<cell_grid(d), CELL_BLOCK, 0, c->stream>>>(step_args<T>(c), fl, c->wsd.tau_x, c->wsd.tau_z, sc,
-                nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, I::f(c->rhs3));
-        else
-            k_stage<T, false><<<cell_grid(d), CELL_BLOCK, 0, c->stream>>>(step_args<T>(c), fl, c->wsd.tau_x, c->wsd.tau_z, sc,
-                nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, I::f(c->rhs3));
-        CKL();
-        return DFDM_OK;
+        StageCoef sc{1, 0.0, 0.0, 0.0, 0.0, 0};
+        return I::stage_kernel(c, sc, I::f(c->rhs3));
     });
     if (rc) return rc;
     struct { double *dst; int n1, n2, n3; } outs[3] = {
@@ -903,7 +963,9 @@ int dfdm_compute_projection_step(dfdm_ctx *c, int save_p) {
     CK(cudaMemcpyAsync(c->us, c->u, F, cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaMemcpyAsync(c->vs, c->v, F, cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaMemcpyAsync(c->wsf, c->w, F, cudaMemcpyDeviceToDevice, c->stream));
+    c->unit_projection = true;
     int rc = dispatch(c, [&](auto impl) { return decltype(impl)::poisson_chain(c, save_p ? 3 : 1); });
+    c->unit_projection = false;
     if (rc) return rc;
     CK(cudaStreamSynchronize(c->stream));
     return DFDM_OK;

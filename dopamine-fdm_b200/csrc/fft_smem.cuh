@@ -14,10 +14,31 @@
 
 namespace dfdm {
 
+// Division by a runtime constant with a multiply-high (Granlund & Montgomery, "Division by invariant integers
+// using multiplication", 1994): for d >= 2, l = ceil(log2 d), m = ceil(2^(31+l)/d) < 2^32 and
+// n / d = umulhi(n, m) >> (l-1) for every n < 2^22 (checked exhaustively for d <= 4096 when the plan is built).
+struct FastDiv {
+    unsigned d, m;
+    int s;
+};
+inline FastDiv make_fastdiv(unsigned d) {
+    FastDiv f;
+    f.d = d; f.m = 0; f.s = 0;
+    if (d <= 1) return f;
+    int l = 0;
+    while ((1u << l) < d) ++l;
+    f.m = (unsigned)((((unsigned long long)1 << (31 + l)) + d - 1) / d);
+    f.s = l - 1;
+    return f;
+}
+__device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv &f) { return f.d <= 1 ? n : (__umulhi(n, f.m) >> f.s); }
+
 struct FFTPlan {
-    int n;          // transform length
-    int nrad;       // number of passes
-    int rad[16];    // radix of each pass
+    int n;           // transform length
+    int nrad;        // number of passes
+    int rad[16];     // radix of each pass
+    FastDiv ns[16];  // division by Ns (product of the radices of the earlier passes)
+    FastDiv nb[16];  // division by n / rad (butterflies per line)
 };
 
 template <typename C> __device__ __forceinline__ C cadd(C a, C b) { C r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
@@ -69,10 +90,11 @@ __device__ __forceinline__ void dft_small(C *v, int R) {
 }
 
 // Transforms `nlines` lines held in shared memory.  Element e of line l lives at buf[l*ldl + e*lde].
-// LINES_FAST selects the thread mapping: consecutive threads take consecutive lines (column tiles, lde > 1)
-// or consecutive butterflies of one line (row tiles, lde == 1), which keeps shared-memory accesses unit-stride.
+// LINES_FAST selects the thread mapping: consecutive threads take consecutive lines (column tiles, lde > 1, the
+// line count NL is then a compile-time constant) or consecutive butterflies of one line (row tiles, lde == 1),
+// which keeps shared-memory accesses unit-stride.  No integer division is executed per butterfly.
 // tw: global table W_n^k, k = 0..n-1 (storage precision).  Returns the buffer that holds the result.
-template <typename T, bool INV, bool LINES_FAST>
+template <typename T, bool INV, bool LINES_FAST, int NL = 1>
 __device__ typename cplx_t<T>::type *fft_lines(typename cplx_t<T>::type *buf0, typename cplx_t<T>::type *buf1,
                                                int nlines, int ldl, int lde, const FFTPlan &p,
                                                const typename cplx_t<T>::type *__restrict__ tw) {
@@ -83,13 +105,15 @@ __device__ typename cplx_t<T>::type *fft_lines(typename cplx_t<T>::type *buf0, t
     for (int ps = 0; ps < p.nrad; ++ps) {
         const int R = p.rad[ps];
         const int nb = n / R;
-        const int total = nb * nlines;
+        const int total = nb * (LINES_FAST ? NL : nlines);
         const int twstep = n / (Ns * R);
+        const FastDiv fns = p.ns[ps], fnb = p.nb[ps];
         for (int b = threadIdx.x; b < total; b += blockDim.x) {
             int line, j;
-            if (LINES_FAST) { line = b % nlines; j = b / nlines; }
-            else { j = b % nb; line = b / nb; }
-            const int k = j % Ns;
+            if (LINES_FAST) { line = b % NL; j = b / NL; }
+            else { line = (int)fdiv((unsigned)b, fnb); j = b - line * nb; }
+            const int q = (int)fdiv((unsigned)j, fns);
+            const int k = j - q * Ns;
             C v[5];
             const C *s = src + line * ldl;
 #pragma unroll 5
@@ -105,7 +129,7 @@ __device__ typename cplx_t<T>::type *fft_lines(typename cplx_t<T>::type *buf0, t
             }
             dft_small<T, INV>(v, R);
             C *d = dst + line * ldl;
-            const int base = (j / Ns) * Ns * R + k;
+            const int base = q * Ns * R + k;
 #pragma unroll 5
             for (int r = 0; r < 5; ++r)
                 if (r < R) d[(base + r * Ns) * lde] = v[r];
@@ -126,6 +150,12 @@ inline bool make_fft_plan(int n, FFTPlan &p) {
     while (m % 2 == 0 && p.nrad < 16) { p.rad[p.nrad++] = 2; m /= 2; }
     while (m % 3 == 0 && p.nrad < 16) { p.rad[p.nrad++] = 3; m /= 3; }
     while (m % 5 == 0 && p.nrad < 16) { p.rad[p.nrad++] = 5; m /= 5; }
+    int Ns = 1;
+    for (int ps = 0; ps < p.nrad; ++ps) {
+        p.ns[ps] = make_fastdiv((unsigned)Ns);
+        p.nb[ps] = make_fastdiv((unsigned)(n / p.rad[ps]));
+        Ns *= p.rad[ps];
+    }
     return m == 1;
 }
 

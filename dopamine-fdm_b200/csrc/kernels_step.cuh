@@ -47,39 +47,35 @@ __device__ __forceinline__ double solve_u_tau(double u_ref, double y_ref, double
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// Eddy viscosity at the cell centres: compute_vreman pass 1 (src/sgs_model.f90:118-223) with the AMD
+// Eddy viscosity at one cell centre: compute_vreman pass 1 (src/sgs_model.f90:118-223) with the AMD
 // (Rozema et al. 2015) or Vreman (2004) closure and the wall-modelled first-cell gradient override (:158-172).
-// Ghost values are implied by the read rules (sgs_fill_ghosts, :458-531).
-template <typename T>
-__global__ void __launch_bounds__(256) k_sgs(StepArgs<T> a, const T *__restrict__ U, const T *__restrict__ V,
-                                             const T *__restrict__ W, T *__restrict__ nut) {
+// Ghost values come from the neighbourhood accessor (sgs_fill_ghosts' rules, :458-531).
+template <typename T, typename Q>
+__device__ __forceinline__ T nut_at(const StepArgs<T> &a, const Q &q, int j, int k) {
     const Dims &d = a.d;
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
-    if (i >= d.Nx || j >= d.Ny) return;
     typedef Arith<T> A;
     const Metric1D<T> &my = a.my, &mz = a.mz;
-    int im = wrap(i - 1, d.Nx), ip = wrap(i + 1, d.Nx), km = wrap(k - 1, d.Nz), kp = wrap(k + 1, d.Nz);
     T dz_c = mz.dc[k], dz2 = dz_c * dz_c;
     T inv_dz_k = A::inv(mz.dc, mz.idc, k), inv_zg_km = A::inv(mz.df, mz.idf, k - 1), inv_zg_kp = A::inv(mz.df, mz.idf, k);
     T dy_c = my.dc[j], dy2_c = dy_c * dy_c;
     T inv_yg_jm = A::inv(my.df, my.idf, j - 1), inv_yg_jp = A::inv(my.df, my.idf, j), inv_dy_j = A::inv(my.dc, my.idc, j);
     T inv_dx = a.inv_dx, dx2 = a.dx2;
-    T Uc = __ldg(U + idx3(d, i, j, k));
-    T a11 = (Uc - __ldg(U + idx3(d, im, j, k))) * inv_dx;
-    T a21 = T(0.5) * ((Uc - ld_yc(U, d, i, j - 1, k)) * inv_yg_jm + (ld_yc(U, d, i, j + 1, k) - Uc) * inv_yg_jp);
-    T a31 = T(0.5) * ((Uc - __ldg(U + idx3(d, i, j, km))) * inv_zg_km + (__ldg(U + idx3(d, i, j, kp)) - Uc) * inv_zg_kp);
-    T Vc = ld_yf(V, d, i, j, k);
-    T a12 = T(0.5) * ((Vc - ld_yf(V, d, im, j, k)) + (ld_yf(V, d, ip, j, k) - Vc)) * inv_dx;
-    T a22 = (Vc - ld_yf(V, d, i, j - 1, k)) * inv_dy_j;
-    T a32 = T(0.5) * ((Vc - ld_yf(V, d, i, j, km)) * inv_zg_km + (ld_yf(V, d, i, j, kp) - Vc) * inv_zg_kp);
-    T Wc = __ldg(W + idx3(d, i, j, k));
-    T a13 = T(0.5) * ((Wc - __ldg(W + idx3(d, im, j, k))) + (__ldg(W + idx3(d, ip, j, k)) - Wc)) * inv_dx;
-    T a23 = T(0.5) * ((Wc - ld_yc(W, d, i, j - 1, k)) * inv_yg_jm + (ld_yc(W, d, i, j + 1, k) - Wc) * inv_yg_jp);
-    T a33 = (Wc - __ldg(W + idx3(d, i, j, km))) * inv_dz_k;
+    T Uc = q.U(0, 0, 0), Um = q.U(-1, 0, 0);
+    T a11 = (Uc - Um) * inv_dx;
+    T a21 = T(0.5) * ((Uc - q.U(0, -1, 0)) * inv_yg_jm + (q.U(0, 1, 0) - Uc) * inv_yg_jp);
+    T a31 = T(0.5) * ((Uc - q.U(0, 0, -1)) * inv_zg_km + (q.U(0, 0, 1) - Uc) * inv_zg_kp);
+    T Vc = q.V(0, 0, 0);
+    T a12 = T(0.5) * ((Vc - q.V(-1, 0, 0)) + (q.V(1, 0, 0) - Vc)) * inv_dx;
+    T a22 = (Vc - q.V(0, -1, 0)) * inv_dy_j;
+    T a32 = T(0.5) * ((Vc - q.V(0, 0, -1)) * inv_zg_km + (q.V(0, 0, 1) - Vc) * inv_zg_kp);
+    T Wc = q.W(0, 0, 0), Wkm = q.W(0, 0, -1);
+    T a13 = T(0.5) * ((Wc - q.W(-1, 0, 0)) + (q.W(1, 0, 0) - Wc)) * inv_dx;
+    T a23 = T(0.5) * ((Wc - q.W(0, -1, 0)) * inv_yg_jm + (q.W(0, 1, 0) - Wc) * inv_yg_jp);
+    T a33 = (Wc - Wkm) * inv_dz_k;
     if (a.wm && (j == 0 || j == d.Ny - 1)) {
         double y_w = (j == 0) ? a.yg2 : a.ygtop;
-        double u_c = 0.5 * ((double)__ldg(U + idx3(d, im, j, k)) + (double)Uc);
-        double w_c = 0.5 * ((double)__ldg(W + idx3(d, i, j, km)) + (double)Wc);
+        double u_c = 0.5 * ((double)Um + (double)Uc);
+        double w_c = 0.5 * ((double)Wkm + (double)Wc);
         double u_mag = sqrt(u_c * u_c + w_c * w_c);
         if (u_mag > 1e-14) {
             double u_tau = solve_u_tau(u_mag, y_w, a.nu_d);
@@ -104,7 +100,7 @@ __global__ void __launch_bounds__(256) k_sgs(StepArgs<T> a, const T *__restrict_
         T B_beta = b11 * b22 - b12 * b12 + b11 * b33 - b13 * b13 + b22 * b33 - b23 * b23;
         if (alpha_sq > T(1e-20) && B_beta > T(0)) nu_t = a.c_V * sqrt(B_beta / alpha_sq);
     }
-    nut[idx3(d, i, j, k)] = nu_t;
+    return nu_t;
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -172,38 +168,33 @@ __global__ void k_wall_model(StepArgs<T> a, WallState ws, const T *__restrict__ 
 
 // ---------------------------------------------------------------------------------------------------------------
 // Right-hand sides (src/equations.f90), evaluated in the reference's expression order at one index (i,j,k).
-template <typename T> struct Fields {
-    const T *__restrict__ U; const T *__restrict__ V; const T *__restrict__ W; const T *__restrict__ nut;
-};
-
-template <typename T, bool LES>
-__device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Fields<T> &f, const double *__restrict__ tau_x,
-                                      int i, int j, int k) {
+// `q` is a neighbourhood accessor: q.U(di,dj,dk) is U at (i+di, j+dj, k+dk) with every boundary rule already
+// applied (periodic wraps, no-slip mirror, zero wall faces, zero nu_t ghosts), so the formulas below see the
+// same values the reference reads from its ghosted arrays.
+template <typename T, bool LES, typename Q>
+__device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Q &q, const double *__restrict__ tau_x, int i, int j, int k) {
     const Dims &d = a.d;
     typedef Arith<T> A;
     const Metric1D<T> &my = a.my, &mz = a.mz;
-    int im = wrap(i - 1, d.Nx), ip = wrap(i + 1, d.Nx), km = wrap(k - 1, d.Nz), kp = wrap(k + 1, d.Nz);
-    const T *U = f.U, *V = f.V, *W = f.W;
-    T Uc = __ldg(U + idx3(d, i, j, k)), Uim = __ldg(U + idx3(d, im, j, k)), Uip = __ldg(U + idx3(d, ip, j, k));
-    T Ujm = ld_yc(U, d, i, j - 1, k), Ujp = ld_yc(U, d, i, j + 1, k);
-    T Ukm = __ldg(U + idx3(d, i, j, km)), Ukp = __ldg(U + idx3(d, i, j, kp));
+    T Uc = q.U(0, 0, 0), Uim = q.U(-1, 0, 0), Uip = q.U(1, 0, 0);
+    T Ujm = q.U(0, -1, 0), Ujp = q.U(0, 1, 0), Ukm = q.U(0, 0, -1), Ukp = q.U(0, 0, 1);
     bool wm_band = a.wm && (j + 2 <= 1 + a.nwl || j + 2 >= d.Ny + 2 - a.nwl);
     T wa = wm_band ? T(0) : a.w_adv, wd = T(1) - wa;
     // -d(uu)/dx
     T t1 = T(0.5) * (Uc + Uip), t0 = T(0.5) * (Uim + Uc);
     T r = -(wd * (t1 * t1 - t0 * t0) + wa * Uc * (t1 - t0)) * a.inv_dx;
     // -d(uv)/dy: u at y faces j-1, j (weighted), v at x faces (plain average)
+    T V00 = q.V(0, 0, 0), V10 = q.V(1, 0, 0), V0m = q.V(0, -1, 0), V1m = q.V(1, -1, 0);
     {
         T u1 = my.w0[j] * Uc + my.w1[j] * Ujp, u0 = my.w0[j - 1] * Ujm + my.w1[j - 1] * Uc;
-        T v1 = T(0.5) * (ld_yf(V, d, i, j, k) + ld_yf(V, d, ip, j, k));
-        T v0 = T(0.5) * (ld_yf(V, d, i, j - 1, k) + ld_yf(V, d, ip, j - 1, k));
+        T v1 = T(0.5) * (V00 + V10), v0 = T(0.5) * (V0m + V1m);
         r = r - A::div(wd * (u1 * v1 - u0 * v0) + wa * T(0.5) * (v0 + v1) * (u1 - u0), my.dc, my.idc, j);
     }
     // -d(uw)/dz
+    T W00 = q.W(0, 0, 0), W10 = q.W(1, 0, 0), W0m = q.W(0, 0, -1), W1m = q.W(1, 0, -1);
     {
         T u1 = mz.w0[k] * Uc + mz.w1[k] * Ukp, u0 = mz.w0[k - 1] * Ukm + mz.w1[k - 1] * Uc;
-        T w1 = T(0.5) * (__ldg(W + idx3(d, i, j, k)) + __ldg(W + idx3(d, ip, j, k)));
-        T w0 = T(0.5) * (__ldg(W + idx3(d, i, j, km)) + __ldg(W + idx3(d, ip, j, km)));
+        T w1 = T(0.5) * (W00 + W10), w0 = T(0.5) * (W0m + W1m);
         r = r - A::div(wd * (u1 * w1 - u0 * w0) + wa * T(0.5) * (w0 + w1) * (u1 - u0), mz.dc, mz.idc, k);
     }
     // viscous: d(2 nu_x du/dx)/dx + d(nu_y (du/dy + dv/dx))/dy + d(nu_z (du/dz + dw/dx))/dz + dPdx
@@ -211,57 +202,50 @@ __device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Fields<T> &f, 
     T nu = a.nu;
     T nu_x1 = nu, nu_x2 = nu, nu_y1 = nu, nu_y2 = nu, nu_z1 = nu, nu_z2 = nu;
     if (LES) {
-        const T *N = f.nut;
-        T n_c = ld_nu(N, d, i, j, k), n_p = ld_nu(N, d, ip, j, k);
+        T n_c = q.N(0, 0, 0), n_p = q.N(1, 0, 0);
         nu_x1 = nu + n_c; nu_x2 = nu + n_p;
         if (!(d.yper == 0 && j == 0))
-            nu_y1 = nu + T(0.5) * (my.w0[j - 1] * ld_nu(N, d, i, j - 1, k) + my.w1[j - 1] * n_c +
-                                   my.w0[j - 1] * ld_nu(N, d, ip, j - 1, k) + my.w1[j - 1] * n_p);
+            nu_y1 = nu + T(0.5) * (my.w0[j - 1] * q.N(0, -1, 0) + my.w1[j - 1] * n_c + my.w0[j - 1] * q.N(1, -1, 0) + my.w1[j - 1] * n_p);
         if (!(d.yper == 0 && j == d.Ny - 1))
-            nu_y2 = nu + T(0.5) * (my.w0[j] * n_c + my.w1[j] * ld_nu(N, d, i, j + 1, k) +
-                                   my.w0[j] * n_p + my.w1[j] * ld_nu(N, d, ip, j + 1, k));
-        nu_z1 = nu + T(0.5) * (mz.w0[k - 1] * (ld_nu(N, d, i, j, km) + ld_nu(N, d, ip, j, km)) + mz.w1[k - 1] * (n_c + n_p));
-        nu_z2 = nu + T(0.5) * (mz.w0[k] * (n_c + n_p) + mz.w1[k] * (ld_nu(N, d, i, j, kp) + ld_nu(N, d, ip, j, kp)));
+            nu_y2 = nu + T(0.5) * (my.w0[j] * n_c + my.w1[j] * q.N(0, 1, 0) + my.w0[j] * n_p + my.w1[j] * q.N(1, 1, 0));
+        nu_z1 = nu + T(0.5) * (mz.w0[k - 1] * (q.N(0, 0, -1) + q.N(1, 0, -1)) + mz.w1[k - 1] * (n_c + n_p));
+        nu_z2 = nu + T(0.5) * (mz.w0[k] * (n_c + n_p) + mz.w1[k] * (q.N(0, 0, 1) + q.N(1, 0, 1)));
     }
     T tj = A::div(Ujp - Uc, my.df, my.idf, j), tjm = A::div(Uc - Ujm, my.df, my.idf, j - 1);
-    T fy2 = nu_y2 * (tj + (ld_yf(V, d, ip, j, k) - ld_yf(V, d, i, j, k)) * a.inv_dx);
-    T fy1 = nu_y1 * (tjm + (ld_yf(V, d, ip, j - 1, k) - ld_yf(V, d, i, j - 1, k)) * a.inv_dx);
+    T fy2 = nu_y2 * (tj + (V10 - V00) * a.inv_dx);
+    T fy1 = nu_y1 * (tjm + (V1m - V0m) * a.inv_dx);
     if (a.wm) {
-        if (j == 0) fy1 = (T)tau_x[(long long)k * d.Nx + i];
-        if (j == d.Ny - 1) fy2 = (T)tau_x[((long long)d.Nz + k) * d.Nx + i];
+        if (j == 0) fy1 = (T)tau_x[k * d.Nx + i];
+        if (j == d.Ny - 1) fy2 = (T)tau_x[(d.Nz + k) * d.Nx + i];
     }
     T tk = A::div(Ukp - Uc, mz.df, mz.idf, k), tkm = A::div(Uc - Ukm, mz.df, mz.idf, k - 1);
-    T fz2 = nu_z2 * (tk + (__ldg(W + idx3(d, ip, j, k)) - __ldg(W + idx3(d, i, j, k))) * a.inv_dx);
-    T fz1 = nu_z1 * (tkm + (__ldg(W + idx3(d, ip, j, km)) - __ldg(W + idx3(d, i, j, km))) * a.inv_dx);
+    T fz2 = nu_z2 * (tk + (W10 - W00) * a.inv_dx);
+    T fz1 = nu_z1 * (tkm + (W1m - W0m) * a.inv_dx);
     r = r + T(2) * a.inv_dx2 * (nu_x2 * (Uip - Uc) - nu_x1 * (Uc - Uim)) + inv_dy3 * (fy2 - fy1) + inv_dz3 * (fz2 - fz1) + a.dPdx;
     return r;
 }
 
-template <typename T, bool LES>
-__device__ __forceinline__ T rhs_v_at(const StepArgs<T> &a, const Fields<T> &f, int i, int j, int k) {
+template <typename T, bool LES, typename Q>
+__device__ __forceinline__ T rhs_v_at(const StepArgs<T> &a, const Q &q, int i, int j, int k) {
     const Dims &d = a.d;
     typedef Arith<T> A;
     const Metric1D<T> &my = a.my, &mz = a.mz;
-    int im = wrap(i - 1, d.Nx), ip = wrap(i + 1, d.Nx), km = wrap(k - 1, d.Nz), kp = wrap(k + 1, d.Nz);
-    const T *U = f.U, *V = f.V, *W = f.W;
+    (void)i; (void)d;
     T wa = a.w_adv, wd = T(1) - wa;
-    T Vc = ld_yf(V, d, i, j, k), Vjm = ld_yf(V, d, i, j - 1, k), Vjp = ld_yf(V, d, i, j + 1, k);
-    T Vim = ld_yf(V, d, im, j, k), Vip = ld_yf(V, d, ip, j, k);
-    T Vkm = ld_yf(V, d, i, j, km), Vkp = ld_yf(V, d, i, j, kp);
+    T Vc = q.V(0, 0, 0), Vjm = q.V(0, -1, 0), Vjp = q.V(0, 1, 0);
+    T Vim = q.V(-1, 0, 0), Vip = q.V(1, 0, 0), Vkm = q.V(0, 0, -1), Vkp = q.V(0, 0, 1);
     // -d(vv)/dy
     T t1 = T(0.5) * (Vc + Vjp), t0 = T(0.5) * (Vjm + Vc);
     T r = -A::div(wd * (t1 * t1 - t0 * t0) + wa * Vc * (t1 - t0), my.df, my.idf, j);
     // -d(uv)/dx: u at y face j (weighted), v at x faces
-    T Uc = __ldg(U + idx3(d, i, j, k)), Um = __ldg(U + idx3(d, im, j, k));
-    T Ucp = ld_yc(U, d, i, j + 1, k), Ump = ld_yc(U, d, im, j + 1, k);
+    T Uc = q.U(0, 0, 0), Um = q.U(-1, 0, 0), Ucp = q.U(0, 1, 0), Ump = q.U(-1, 1, 0);
     {
         T u1 = my.w0[j] * Uc + my.w1[j] * Ucp, u0 = my.w0[j] * Um + my.w1[j] * Ump;
         T v1 = T(0.5) * (Vc + Vip), v0 = T(0.5) * (Vim + Vc);
         r = r - (wd * (u1 * v1 - u0 * v0) + wa * T(0.5) * (u0 + u1) * (v1 - v0)) * a.inv_dx;
     }
     // -d(vw)/dz: v at z faces (weighted), w at y face j (weighted)
-    T Wc = __ldg(W + idx3(d, i, j, k)), Wjp = ld_yc(W, d, i, j + 1, k);
-    T Wkm = __ldg(W + idx3(d, i, j, km)), Wkmjp = ld_yc(W, d, i, j + 1, km);
+    T Wc = q.W(0, 0, 0), Wjp = q.W(0, 1, 0), Wkm = q.W(0, 0, -1), Wkmjp = q.W(0, 1, -1);
     {
         T v1 = mz.w0[k] * Vc + mz.w1[k] * Vkp, v0 = mz.w0[k - 1] * Vkm + mz.w1[k - 1] * Vc;
         T w1 = my.w0[j] * Wc + my.w1[j] * Wjp, w0 = my.w0[j] * Wkm + my.w1[j] * Wkmjp;
@@ -275,15 +259,14 @@ __device__ __forceinline__ T rhs_v_at(const StepArgs<T> &a, const Fields<T> &f, 
     T nu = a.nu;
     T nu_x1 = nu, nu_x2 = nu, nu_y1 = nu, nu_y2 = nu, nu_z1 = nu, nu_z2 = nu;
     if (LES) {
-        const T *N = f.nut;
-        T n_c = ld_nu(N, d, i, j, k), n_jp = ld_nu(N, d, i, j + 1, k);
+        T n_c = q.N(0, 0, 0), n_jp = q.N(0, 1, 0);
         T w0 = my.w0[j], w1 = my.w1[j];
-        nu_x1 = nu + T(0.5) * (w0 * ld_nu(N, d, im, j, k) + w1 * ld_nu(N, d, im, j + 1, k) + w0 * n_c + w1 * n_jp);
-        nu_x2 = nu + T(0.5) * (w0 * n_c + w1 * n_jp + w0 * ld_nu(N, d, ip, j, k) + w1 * ld_nu(N, d, ip, j + 1, k));
+        nu_x1 = nu + T(0.5) * (w0 * q.N(-1, 0, 0) + w1 * q.N(-1, 1, 0) + w0 * n_c + w1 * n_jp);
+        nu_x2 = nu + T(0.5) * (w0 * n_c + w1 * n_jp + w0 * q.N(1, 0, 0) + w1 * q.N(1, 1, 0));
         nu_y1 = nu + n_c;
         nu_y2 = nu + n_jp;
-        nu_z1 = nu + mz.w0[k - 1] * (w0 * ld_nu(N, d, i, j, km) + w1 * ld_nu(N, d, i, j + 1, km)) + mz.w1[k - 1] * (w0 * n_c + w1 * n_jp);
-        nu_z2 = nu + mz.w0[k] * (w0 * n_c + w1 * n_jp) + mz.w1[k] * (w0 * ld_nu(N, d, i, j, kp) + w1 * ld_nu(N, d, i, j + 1, kp));
+        nu_z1 = nu + mz.w0[k - 1] * (w0 * q.N(0, 0, -1) + w1 * q.N(0, 1, -1)) + mz.w1[k - 1] * (w0 * n_c + w1 * n_jp);
+        nu_z2 = nu + mz.w0[k] * (w0 * n_c + w1 * n_jp) + mz.w1[k] * (w0 * q.N(0, 0, 1) + w1 * q.N(0, 1, 1));
     }
     T fx2 = nu_x2 * ((Vip - Vc) * a.inv_dx + (Ucp - Uc) * inv_dy3);
     T fx1 = nu_x1 * ((Vc - Vim) * a.inv_dx + (Ump - Um) * inv_dy3);
@@ -293,32 +276,27 @@ __device__ __forceinline__ T rhs_v_at(const StepArgs<T> &a, const Fields<T> &f, 
     return r;
 }
 
-template <typename T, bool LES>
-__device__ __forceinline__ T rhs_w_at(const StepArgs<T> &a, const Fields<T> &f, const double *__restrict__ tau_z,
-                                      int i, int j, int k) {
+template <typename T, bool LES, typename Q>
+__device__ __forceinline__ T rhs_w_at(const StepArgs<T> &a, const Q &q, const double *__restrict__ tau_z, int i, int j, int k) {
     const Dims &d = a.d;
     typedef Arith<T> A;
     const Metric1D<T> &my = a.my, &mz = a.mz;
-    int im = wrap(i - 1, d.Nx), ip = wrap(i + 1, d.Nx), km = wrap(k - 1, d.Nz), kp = wrap(k + 1, d.Nz);
-    const T *U = f.U, *V = f.V, *W = f.W;
     bool wm_band = a.wm && (j + 2 <= 1 + a.nwl || j + 2 >= d.Ny + 2 - a.nwl);
     T wa = wm_band ? T(0) : a.w_adv, wd = T(1) - wa;
-    T Wc = __ldg(W + idx3(d, i, j, k)), Wkm = __ldg(W + idx3(d, i, j, km)), Wkp = __ldg(W + idx3(d, i, j, kp));
-    T Wim = __ldg(W + idx3(d, im, j, k)), Wip = __ldg(W + idx3(d, ip, j, k));
-    T Wjm = ld_yc(W, d, i, j - 1, k), Wjp = ld_yc(W, d, i, j + 1, k);
+    T Wc = q.W(0, 0, 0), Wkm = q.W(0, 0, -1), Wkp = q.W(0, 0, 1);
+    T Wim = q.W(-1, 0, 0), Wip = q.W(1, 0, 0), Wjm = q.W(0, -1, 0), Wjp = q.W(0, 1, 0);
     // -d(ww)/dz
     T t1 = T(0.5) * (Wc + Wkp), t0 = T(0.5) * (Wkm + Wc);
     T r = -A::div(wd * (t1 * t1 - t0 * t0) + wa * Wc * (t1 - t0), mz.df, mz.idf, k);
     // -d(uw)/dx: u at z face k (weighted), w at x faces
-    T Uc = __ldg(U + idx3(d, i, j, k)), Um = __ldg(U + idx3(d, im, j, k));
-    T Ukp = __ldg(U + idx3(d, i, j, kp)), Umkp = __ldg(U + idx3(d, im, j, kp));
+    T Uc = q.U(0, 0, 0), Um = q.U(-1, 0, 0), Ukp = q.U(0, 0, 1), Umkp = q.U(-1, 0, 1);
     {
         T u1 = mz.w0[k] * Uc + mz.w1[k] * Ukp, u0 = mz.w0[k] * Um + mz.w1[k] * Umkp;
         T w1 = T(0.5) * (Wc + Wip), w0 = T(0.5) * (Wim + Wc);
         r = r - (wd * (u1 * w1 - u0 * w0) + wa * T(0.5) * (u0 + u1) * (w1 - w0)) * a.inv_dx;
     }
     // -d(vw)/dy: v at z face k (weighted), w at y faces (weighted)
-    T Vc = ld_yf(V, d, i, j, k), Vkp = ld_yf(V, d, i, j, kp), Vjm = ld_yf(V, d, i, j - 1, k), Vjmkp = ld_yf(V, d, i, j - 1, kp);
+    T Vc = q.V(0, 0, 0), Vkp = q.V(0, 0, 1), Vjm = q.V(0, -1, 0), Vjmkp = q.V(0, -1, 1);
     {
         T v1 = mz.w0[k] * Vc + mz.w1[k] * Vkp, v0 = mz.w0[k] * Vjm + mz.w1[k] * Vjmkp;
         T w1 = my.w0[j] * Wc + my.w1[j] * Wjp, w0 = my.w0[j - 1] * Wjm + my.w1[j - 1] * Wc;
@@ -331,17 +309,14 @@ __device__ __forceinline__ T rhs_w_at(const StepArgs<T> &a, const Fields<T> &f, 
     T nu = a.nu;
     T nu_x1 = nu, nu_x2 = nu, nu_y1 = nu, nu_y2 = nu, nu_z1 = nu, nu_z2 = nu;
     if (LES) {
-        const T *N = f.nut;
-        T n_c = ld_nu(N, d, i, j, k), n_kp = ld_nu(N, d, i, j, kp);
+        T n_c = q.N(0, 0, 0), n_kp = q.N(0, 0, 1);
         T z0 = mz.w0[k], z1 = mz.w1[k];
-        nu_x1 = nu + T(0.5) * (z0 * (n_c + ld_nu(N, d, im, j, k)) + z1 * (n_kp + ld_nu(N, d, im, j, kp)));
-        nu_x2 = nu + T(0.5) * (z0 * (n_c + ld_nu(N, d, ip, j, k)) + z1 * (n_kp + ld_nu(N, d, ip, j, kp)));
+        nu_x1 = nu + T(0.5) * (z0 * (n_c + q.N(-1, 0, 0)) + z1 * (n_kp + q.N(-1, 0, 1)));
+        nu_x2 = nu + T(0.5) * (z0 * (n_c + q.N(1, 0, 0)) + z1 * (n_kp + q.N(1, 0, 1)));
         if (!(d.yper == 0 && j == 0))
-            nu_y1 = nu + z0 * (my.w0[j - 1] * ld_nu(N, d, i, j - 1, k) + my.w1[j - 1] * n_c) +
-                    z1 * (my.w0[j - 1] * ld_nu(N, d, i, j - 1, kp) + my.w1[j - 1] * n_kp);
+            nu_y1 = nu + z0 * (my.w0[j - 1] * q.N(0, -1, 0) + my.w1[j - 1] * n_c) + z1 * (my.w0[j - 1] * q.N(0, -1, 1) + my.w1[j - 1] * n_kp);
         if (!(d.yper == 0 && j == d.Ny - 1))
-            nu_y2 = nu + z0 * (my.w0[j] * n_c + my.w1[j] * ld_nu(N, d, i, j + 1, k)) +
-                    z1 * (my.w0[j] * n_kp + my.w1[j] * ld_nu(N, d, i, j + 1, kp));
+            nu_y2 = nu + z0 * (my.w0[j] * n_c + my.w1[j] * q.N(0, 1, 0)) + z1 * (my.w0[j] * n_kp + my.w1[j] * q.N(0, 1, 1));
         nu_z1 = nu + n_c;
         nu_z2 = nu + n_kp;
     }
@@ -349,8 +324,8 @@ __device__ __forceinline__ T rhs_w_at(const StepArgs<T> &a, const Fields<T> &f, 
     T fy2 = nu_y2 * (tj + (Vkp - Vc) * inv_dz3);
     T fy1 = nu_y1 * (tjm + (Vjmkp - Vjm) * inv_dz3);
     if (a.wm) {
-        if (j == 0) fy1 = (T)tau_z[(long long)k * d.Nx + i];
-        if (j == d.Ny - 1) fy2 = (T)tau_z[((long long)d.Nz + k) * d.Nx + i];
+        if (j == 0) fy1 = (T)tau_z[k * d.Nx + i];
+        if (j == d.Ny - 1) fy2 = (T)tau_z[(d.Nz + k) * d.Nx + i];
     }
     T fx2 = nu_x2 * ((Wip - Wc) * a.inv_dx + (Ukp - Uc) * inv_dz3);
     T fx1 = nu_x1 * ((Wc - Wim) * a.inv_dx + (Umkp - Um) * inv_dz3);
@@ -359,8 +334,7 @@ __device__ __forceinline__ T rhs_w_at(const StepArgs<T> &a, const Fields<T> &f, 
     return r;
 }
 
-// Fused stage kernel: the three right-hand sides at (i,j,k) and the Butcher-form RK3 update
-// (src/time_integration.f90:255-259, :393-397, :525-532).  Stage 1 also writes the base state uo and F1.
+// Stage coefficients of the Butcher-form RK3 update (src/time_integration.f90:255-259, :393-397, :525-532):
 //   s = 1: u* = uo + (dt a11) F1                 (F1 = rhs, uo = u)
 //   s = 2: u* = uo + dt (a21 F1 + a22 rhs)
 //   s = 3: u* = uo + dt (a31 F1 + a33 rhs)        (a32 = 0, so F2 is never needed)
@@ -369,38 +343,118 @@ struct StageCoef {
     double dt_a11;   // dt*rk_coef(1,1), stage 1
     double dt;       // dt, stages 2 and 3
     double c1, c2;   // rk_coef(s,1) and rk_coef(s,s), stages 2 and 3
+    int incr;        // store the increment du = dt (c1 F1 + c2 rhs) instead of u* = uo + du (FP32-mixed stage 3)
 };
 
-template <typename T, bool LES>
-__global__ void __launch_bounds__(256) k_stage(StepArgs<T> a, Fields<T> f, const double *__restrict__ tau_x,
-                                               const double *__restrict__ tau_z, StageCoef sc,
-                                               T *__restrict__ uo, T *__restrict__ vo, T *__restrict__ wo,
-                                               T *__restrict__ f1u, T *__restrict__ f1v, T *__restrict__ f1w,
-                                               T *__restrict__ us, T *__restrict__ vs, T *__restrict__ wsf,
-                                               T *__restrict__ rhs_only) {
+// Shared-memory neighbourhood of one thread: three z-planes (k-1, k, k+1) of each field, each plane a
+// (TX+2) x (TY+2) tile with a one-cell halo in x and y.
+template <typename T, int PX> struct TileQ {
+    const T *u[3], *v[3], *w[3], *n[3];
+    int c;   // local index of the centre cell
+    __device__ __forceinline__ T U(int di, int dj, int dk) const { return u[dk + 1][c + dj * PX + di]; }
+    __device__ __forceinline__ T V(int di, int dj, int dk) const { return v[dk + 1][c + dj * PX + di]; }
+    __device__ __forceinline__ T W(int di, int dj, int dk) const { return w[dk + 1][c + dj * PX + di]; }
+    __device__ __forceinline__ T N(int di, int dj, int dk) const { return n[dk + 1][c + dj * PX + di]; }
+};
+
+// Tiled kernels (KIND 0: fused stage, KIND 1: eddy viscosity), 2.5-D blocked: a block owns a TX x TY column of (i,j) cells and marches through a chunk of
+// kc z-planes.  Each z-plane of U, V, W (and nu_t) is loaded from HBM once per block, with its halo, into a
+// rotating set of three shared planes; the boundary rules are applied while loading.  Every thread then evaluates
+// the three right-hand sides of its cell from shared memory and writes the RK3 update (or, with rhs_only, the
+// right-hand sides themselves for the unit entry point).
+template <typename T, bool LES, int TX, int TY, int KIND>
+__global__ void __launch_bounds__(TX *TY) k_tiled(StepArgs<T> a, const T *__restrict__ U, const T *__restrict__ V,
+                                                  const T *__restrict__ W, const T *__restrict__ NU,
+                                                  const double *__restrict__ tau_x, const double *__restrict__ tau_z,
+                                                  StageCoef sc, int kc, T *__restrict__ uo, T *__restrict__ vo,
+                                                  T *__restrict__ wo, T *__restrict__ f1u, T *__restrict__ f1v,
+                                                  T *__restrict__ f1w, T *__restrict__ us, T *__restrict__ vs,
+                                                  T *__restrict__ wsf, T *__restrict__ rhs_only, T *__restrict__ nut_out) {
+    constexpr int PX = TX + 2, PY = TY + 2, PS = PX * PY, NT = TX * TY;
+    constexpr int NF = LES ? 4 : 3;
+    __shared__ T sm[NF][3][PS];
     const Dims &d = a.d;
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
-    if (i >= d.Nx || j >= d.Ny) return;
-    long long p = idx3(d, i, j, k);
-    T ru = rhs_u_at<T, LES>(a, f, tau_x, i, j, k);
-    T rw = rhs_w_at<T, LES>(a, f, tau_z, i, j, k);
-    bool vrow = j < d.NyV;
-    T rv = vrow ? rhs_v_at<T, LES>(a, f, i, j, k) : T(0);
-    if (rhs_only) {   // unit entry point: F = rhs, no update
-        rhs_only[p] = ru; rhs_only[d.cells + p] = rv; rhs_only[2 * d.cells + p] = rw;
-        return;
-    }
-    if (sc.stage == 1) {
-        T u0 = f.U[p], w0 = f.W[p];
-        T c = (T)sc.dt_a11;
-        uo[p] = u0; f1u[p] = ru; us[p] = u0 + c * ru;
-        wo[p] = w0; f1w[p] = rw; wsf[p] = w0 + c * rw;
-        if (vrow) { T v0 = f.V[p]; vo[p] = v0; f1v[p] = rv; vs[p] = v0 + c * rv; }
-    } else {
-        T c1 = (T)sc.c1, c2 = (T)sc.c2, dtt = (T)sc.dt;
-        us[p] = uo[p] + dtt * (c1 * f1u[p] + c2 * ru);
-        wsf[p] = wo[p] + dtt * (c1 * f1w[p] + c2 * rw);
-        if (vrow) vs[p] = vo[p] + dtt * (c1 * f1v[p] + c2 * rv);
+    const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
+    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+    const int k0 = blockIdx.z * kc, kend = min(k0 + kc, Nz);
+    const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool active = i < Nx && j < Ny;
+    const int plane = Nx * Ny;
+
+    auto load_plane = [&](int slot, int k) {
+        int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k);
+        const int kb = kw * plane;
+        for (int e = threadIdx.x; e < PS; e += NT) {
+            int jj = e / PX, ii = e - jj * PX;
+            int gi = i0 - 1 + ii;
+            gi = gi < 0 ? gi + Nx : gi;
+            while (gi >= Nx) gi -= Nx;
+            int gj = j0 - 1 + jj;
+            T u, v, w, nu = T(0);
+            if (d.yper) {
+                int g = gj < 0 ? gj + Ny : gj;
+                while (g >= Ny) g -= Ny;
+                int o = kb + g * Nx + gi;
+                u = __ldg(U + o); v = __ldg(V + o); w = __ldg(W + o);
+                if (LES) nu = __ldg(NU + o);
+            } else {
+                int g = gj < 0 ? 0 : (gj >= Ny ? Ny - 1 : gj);
+                int o = kb + g * Nx + gi;
+                u = __ldg(U + o); w = __ldg(W + o);
+                if (gj < 0 || gj >= Ny) { u = -u; w = -w; v = T(0); }   // no-slip mirror, zero wall faces
+                else { v = __ldg(V + o); if (LES) nu = __ldg(NU + o); }
+            }
+            sm[0][slot][e] = u; sm[1][slot][e] = v; sm[2][slot][e] = w;
+            if (LES) sm[NF - 1][slot][e] = nu;
+        }
+    };
+
+    int s_m = 0, s_0 = 1, s_p = 2;
+    load_plane(s_m, k0 - 1);
+    load_plane(s_0, k0);
+    const int cloc = (ty + 1) * PX + tx + 1;
+    for (int k = k0; k < kend; ++k) {
+        load_plane(s_p, k + 1);
+        __syncthreads();
+        if (active) {
+            TileQ<T, PX> q;
+            q.c = cloc;
+            q.u[0] = sm[0][s_m]; q.u[1] = sm[0][s_0]; q.u[2] = sm[0][s_p];
+            q.v[0] = sm[1][s_m]; q.v[1] = sm[1][s_0]; q.v[2] = sm[1][s_p];
+            q.w[0] = sm[2][s_m]; q.w[1] = sm[2][s_0]; q.w[2] = sm[2][s_p];
+            q.n[0] = sm[NF - 1][s_m]; q.n[1] = sm[NF - 1][s_0]; q.n[2] = sm[NF - 1][s_p];
+            const int p = k * plane + j * Nx + i;
+            if (KIND == 1) {
+                nut_out[p] = nut_at<T>(a, q, j, k);
+            } else {
+            T ru = rhs_u_at<T, LES>(a, q, tau_x, i, j, k);
+            T rw = rhs_w_at<T, LES>(a, q, tau_z, i, j, k);
+            const bool vrow = j < d.NyV;
+            T rv = vrow ? rhs_v_at<T, LES>(a, q, i, j, k) : T(0);
+            if (rhs_only) {
+                rhs_only[p] = ru; rhs_only[d.cells + p] = rv; rhs_only[2 * d.cells + p] = rw;
+            } else if (sc.stage == 1) {
+                T c = (T)sc.dt_a11;
+                T u0 = q.U(0, 0, 0), w0 = q.W(0, 0, 0);
+                uo[p] = u0; f1u[p] = ru; us[p] = u0 + c * ru;
+                wo[p] = w0; f1w[p] = rw; wsf[p] = w0 + c * rw;
+                if (vrow) { T v0 = q.V(0, 0, 0); vo[p] = v0; f1v[p] = rv; vs[p] = v0 + c * rv; }
+            } else if (sc.incr) {
+                T c1 = (T)sc.c1, c2 = (T)sc.c2, dtt = (T)sc.dt;
+                us[p] = dtt * (c1 * f1u[p] + c2 * ru);
+                wsf[p] = dtt * (c1 * f1w[p] + c2 * rw);
+                if (vrow) vs[p] = dtt * (c1 * f1v[p] + c2 * rv);
+            } else {
+                T c1 = (T)sc.c1, c2 = (T)sc.c2, dtt = (T)sc.dt;
+                us[p] = uo[p] + dtt * (c1 * f1u[p] + c2 * ru);
+                wsf[p] = wo[p] + dtt * (c1 * f1w[p] + c2 * rw);
+                if (vrow) vs[p] = vo[p] + dtt * (c1 * f1v[p] + c2 * rv);
+            }
+            }
+        }
+        __syncthreads();
+        int t = s_m; s_m = s_0; s_0 = s_p; s_p = t;
     }
 }
 

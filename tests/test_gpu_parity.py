@@ -112,7 +112,7 @@ def test_full_step_parity_fp32_mixed(oracle_mod, name):
     s.compute_time_step_RK3(n)
     Uo, Vo, Wo, Po = o.get_state()
     Ug, Vg, Wg, Pg = s.get_state()
-    for key, a, b in (("U", Ug, Uo), ("V", Vg, Vo), ("W", Wg, Wo)):
+    for key, a, b in (("U", Ug, Uo), ("V", Vg, Vo), ("W", Wg, Wo), ("P", Pg, Po)):
         assert rel_l2(a, b) <= TOL32, (key, rel_l2(a, b))
 
 
