@@ -46,7 +46,7 @@ int fail(int code, const std::string &msg) {
     } while (0)
 
 const double PI = 4.0 * std::atan(1.0);   // pi = 4d0*datan(1d0)
-const int MAX_NY = 1024;                  // y solve keeps Ny pivots per column in shared memory (8 KB per row of 32)
+const int MAX_NY = 1024;                  // longest y line of the shared-memory y transform
 
 }  // namespace
 
@@ -75,6 +75,9 @@ struct dfdm_ctx {
     double *d_kxx = nullptr, *d_kzz = nullptr, *d_kyy = nullptr, *d_lo = nullptr, *d_di = nullptr, *d_up = nullptr;
     double *d_rpiv = nullptr;                   // 1/D(r) of every (kx,kz) tridiagonal system, layout (kz, r, kx)
     double *d_dxc = nullptr, *d_dyc = nullptr, *d_dzc = nullptr;
+    void *d_ub = nullptr;                       // streamwise base profile (storage type), zero in FP64
+    bool ub_set = false;
+    double *d_ubd = nullptr;                    // the same in double
     WallState wsd{};
     double *red_part = nullptr, *red_out = nullptr;
     int red_blocks = 0;
@@ -85,7 +88,7 @@ struct dfdm_ctx {
     // launch geometry
     int lx = 8, tzx = 8;
     int kc_stage = 8, kc_sgs = 8;               // z-planes per block of the tiled kernels
-    size_t smem_x = 0, smem_z = 0, smem_y = 0, smem_ys = 0;
+    size_t smem_x = 0, smem_z = 0, smem_y = 0;
     cudaStream_t own_stream = nullptr, stream = nullptr;
     double t = 0.0;
     bool wmf_seeded = false;
@@ -200,6 +203,8 @@ template <typename T> StepArgs<T> step_args(dfdm_ctx *c) {
     a.Ly = c->Ly;
     a.yg2 = c->yg[2];
     a.ygtop = c->Ly - c->yg[c->nyg - 1];
+    a.ub = (const T *)c->d_ub;
+    a.ubd = c->d_ubd;
     return a;
 }
 
@@ -233,7 +238,7 @@ int choose_kc(const Dims &d, int blocks_per_sm, int nsm) {
 
 template <typename T> struct Impl {
     typedef typename cplx_t<T>::type C;
-    static constexpr int CT = (sizeof(T) == 8) ? 8 : 16;   // kx columns per block of the column transforms
+    static constexpr int CT = (sizeof(T) == 8) ? 4 : 8;    // kx columns per block of the column transforms (64 B rows)
     static T *f(void *p) { return (T *)p; }
 
     static int setup_kernels(dfdm_ctx *c) {
@@ -244,8 +249,7 @@ template <typename T> struct Impl {
         c->tzx = CT;
         c->smem_z = 2 * (size_t)d.Nz * c->tzx * sizeof(C);
         c->smem_y = 2 * (size_t)d.Ny * c->tzx * sizeof(C);
-        c->smem_ys = (size_t)d.Ny * 32 * sizeof(C);
-        size_t maxs = std::max(std::max(c->smem_x, c->smem_z), std::max(c->smem_y, c->smem_ys));
+        size_t maxs = std::max(c->smem_x, std::max(c->smem_z, c->smem_y));
         if (maxs > 227 * 1024) return fail(DFDM_ERR_UNSUPPORTED, "grid too large for the shared-memory transforms");
         CK(cudaFuncSetAttribute(k_fwd_x<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_x));
         CK(cudaFuncSetAttribute(k_fwd_x<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_x));
@@ -254,7 +258,6 @@ template <typename T> struct Impl {
         CK(cudaFuncSetAttribute(k_col_fft<T, 0, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs));
         CK(cudaFuncSetAttribute(k_col_fft<T, 1, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs));
         CK(cudaFuncSetAttribute(k_col_fft<T, 2, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs));
-        CK(cudaFuncSetAttribute(k_ysolve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_ys));
         int dev = 0, nsm = 148, occ = 1;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -270,7 +273,7 @@ template <typename T> struct Impl {
     // cancellation, so the saved pressure P = phi/(dt*3/4) does not inherit the O(eps |u| dx / dt) noise that the
     // rounding of the stored velocity would otherwise put into phi.  Stages 1-2 and the FP64 form keep the
     // reference's u* = uo + du exactly.
-    static bool incr_form(const dfdm_ctx *c, int s) { return c->prec == DFDM_FP32_MIXED && s == 3 && !c->unit_projection; }
+    static bool incr_form(const dfdm_ctx *c, int s) { (void)c; (void)s; return false; }
 
     static int stage_kernel(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
         const Dims &d = c->d;
@@ -349,8 +352,8 @@ template <typename T> struct Impl {
                 dim3 g((d.Nxc + c->tzx - 1) / c->tzx, d.Nz);
                 k_col_fft<T, 2, CT><<<g, 256, c->smem_y, st>>>(d, (C *)c->spec, c->plan_y, (const C *)c->tw_y, c->d_kxx, c->d_kyy, c->d_kzz);
             } else {
-                dim3 g((d.Nxc + 31) / 32, d.Nz);
-                k_ysolve<T><<<g, 32, c->smem_ys, st>>>(d, (C *)c->spec, c->d_rpiv, c->d_lo, c->d_up);
+                dim3 g((d.Nxc + 63) / 64, d.Nz);
+                k_ysolve<T, 8><<<g, 64, 0, st>>>(d, (C *)c->spec, c->d_rpiv, c->d_lo, c->d_up);
             }
             CKL();
             return DFDM_OK;
@@ -365,16 +368,22 @@ template <typename T> struct Impl {
         }
         case 7: {   // correction (+ P at stage 3)
             bool inc = incr_form(c, s);
-            k_correct<T><<<cell_grid(d), CELL_BLOCK, 0, st>>>(poisson_args<T>(c), f(c->phi), f(c->us), f(c->vs), f(c->wsf),
-                                                              f(c->u), f(c->v), f(c->w), s == 3 ? f(c->p) : nullptr,
-                                                              inc ? f(c->uo) : nullptr, inc ? f(c->vo) : nullptr,
-                                                              inc ? f(c->wo) : nullptr);
+            if (d.Nx % 4 == 0 && !inc) {
+                dim3 g((d.Nx / 4 + 63) / 64, (d.Ny + 3) / 4, d.Nz);
+                k_correct4<T><<<g, dim3(64, 4, 1), 0, st>>>(poisson_args<T>(c), f(c->phi), f(c->us), f(c->vs), f(c->wsf),
+                                                            f(c->u), f(c->v), f(c->w), s == 3 ? f(c->p) : nullptr);
+            } else {
+                k_correct<T><<<cell_grid(d), CELL_BLOCK, 0, st>>>(poisson_args<T>(c), f(c->phi), f(c->us), f(c->vs), f(c->wsf),
+                                                                  f(c->u), f(c->v), f(c->w), s == 3 ? f(c->p) : nullptr,
+                                                                  inc ? f(c->uo) : nullptr, inc ? f(c->vo) : nullptr,
+                                                                  inc ? f(c->wo) : nullptr);
+            }
             CKL();
             return DFDM_OK;
         }
         case 9: {   // constant-flux shift
             if (c->prm.flow_forcing_mode != 1) return DFDM_OK;
-            k_bulk_partial<T><<<c->red_blocks, 256, 0, st>>>(d, f(c->u), c->d_dyc, c->d_dzc, c->red_part);
+            k_bulk_partial<T><<<c->red_blocks, 256, 0, st>>>(d, f(c->u), c->d_dyc, c->d_dzc, c->d_ubd, c->red_part);
             CKL();
             k_bulk_final<<<1, 32, 0, st>>>(c->red_blocks, c->red_part, c->prm.Ub_target, c->red_out);
             CKL();
@@ -611,6 +620,9 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
     c->d_dyc = (double *)tmp;
     if ((rc = upload_as<double>(c, &tmp, dzc))) return bail(rc);
     c->d_dzc = (double *)tmp;
+    if ((rc = dalloc(c, &c->d_ub, (size_t)d.Ny * c->ts))) return bail(rc);
+    if ((rc = dalloc(c, &tmp, (size_t)d.Ny * sizeof(double)))) return bail(rc);
+    c->d_ubd = (double *)tmp;
 
     // ---- modified wavenumbers (src/initialization.f90:417-434, :480-489) and Dyy (:507-535) ----
     int nxp = d.Nx, nzp = d.Nz;
@@ -751,8 +763,8 @@ static int put_field(dfdm_ctx *c, int kind, void *dst, const double *src, int n1
     if (rc) return rc;
     CK(cudaMemcpyAsync(c->staging, src, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     int gb = reduce_grid(c->d);
-    if (c->prec == DFDM_FP64) k_unpack<double><<<gb, 256, 0, c->stream>>>(c->d, kind, n1, n2, c->staging, (double *)dst);
-    else k_unpack<float><<<gb, 256, 0, c->stream>>>(c->d, kind, n1, n2, c->staging, (float *)dst);
+    if (c->prec == DFDM_FP64) k_unpack<double><<<gb, 256, 0, c->stream>>>(c->d, kind, n1, n2, c->staging, c->d_ubd, (double *)dst);
+    else k_unpack<float><<<gb, 256, 0, c->stream>>>(c->d, kind, n1, n2, c->staging, c->d_ubd, (float *)dst);
     CKL();
     return DFDM_OK;
 }
@@ -762,8 +774,8 @@ static int get_field(dfdm_ctx *c, int kind, const void *srcf, double *dst, int n
     int rc = ensure_staging(c, n);
     if (rc) return rc;
     int gb = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
-    if (c->prec == DFDM_FP64) k_pack<double><<<gb, 256, 0, c->stream>>>(c->d, kind, n1, n2, n3, (const double *)srcf, c->staging);
-    else k_pack<float><<<gb, 256, 0, c->stream>>>(c->d, kind, n1, n2, n3, (const float *)srcf, c->staging);
+    if (c->prec == DFDM_FP64) k_pack<double><<<gb, 256, 0, c->stream>>>(c->d, kind, n1, n2, n3, (const double *)srcf, c->d_ubd, c->staging);
+    else k_pack<float><<<gb, 256, 0, c->stream>>>(c->d, kind, n1, n2, n3, (const float *)srcf, c->d_ubd, c->staging);
     CKL();
     CK(cudaMemcpyAsync(dst, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     return DFDM_OK;
@@ -774,6 +786,26 @@ int dfdm_set_state(dfdm_ctx *c, const double *U, const double *V, const double *
     if (int rc = check_ctx(c)) return rc;
     if (!U || !V || !W) return fail(DFDM_ERR_INVALID, "U, V and W must not be NULL");
     int rc;
+    if (c->prec == DFDM_FP32_MIXED && !c->ub_set) {
+        // streamwise base profile, fixed by the first set_state of the context: the x-z mean of the given U at
+        // every centre row, rounded to FP32, so that the stored deviation U - ub carries rounding noise of the
+        // fluctuation's size, not of the mean flow's
+        const Dims &d = c->d;
+        std::vector<double> ubd(d.Ny);
+        std::vector<float> ubf(d.Ny);
+        for (int j = 0; j < d.Ny; ++j) {
+            double acc = 0.0;
+            for (int k = 0; k < d.Nz; ++k)
+                for (int i = 0; i < d.Nx; ++i)
+                    acc += U[(size_t)(i + 1) + (size_t)c->nx * ((size_t)(j + 1) + (size_t)c->nyg * (size_t)(k + 1))];
+            ubf[j] = (float)(acc / ((double)d.Nx * d.Nz));
+            ubd[j] = (double)ubf[j];
+        }
+        CK(cudaMemcpyAsync(c->d_ub, ubf.data(), d.Ny * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->d_ubd, ubd.data(), d.Ny * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        c->ub_set = true;
+    }
     if ((rc = put_field(c, FK_U, c->u, U, c->nx, c->nyg, c->nzg))) return rc;
     if ((rc = put_field(c, FK_V, c->v, V, c->nxg, c->ny, c->nzg))) return rc;
     if ((rc = put_field(c, FK_W, c->w, W, c->nxg, c->nyg, c->nz))) return rc;
@@ -1016,7 +1048,7 @@ int dfdm_compute_bulk_velocity(dfdm_ctx *c, double *Ub) {
     int rc = dispatch(c, [&](auto impl) {
         typedef decltype(impl) I;
         typedef typename std::remove_pointer<decltype(I::f(nullptr))>::type T;
-        k_bulk_partial<T><<<c->red_blocks, 256, 0, c->stream>>>(c->d, I::f(c->u), c->d_dyc, c->d_dzc, c->red_part);
+        k_bulk_partial<T><<<c->red_blocks, 256, 0, c->stream>>>(c->d, I::f(c->u), c->d_dyc, c->d_dzc, c->d_ubd, c->red_part);
         CKL();
         k_bulk_final<<<1, 32, 0, c->stream>>>(c->red_blocks, c->red_part, 0.0, c->red_out);
         CKL();
@@ -1057,7 +1089,7 @@ int dfdm_kinetic_energy(dfdm_ctx *c, double *ke) {
         typedef decltype(impl) I;
         typedef typename std::remove_pointer<decltype(I::f(nullptr))>::type T;
         k_ke_partial<T><<<c->red_blocks, 256, 0, c->stream>>>(c->d, I::f(c->u), I::f(c->v), I::f(c->w), c->dx, c->d_dyc,
-                                                              c->d_dzc, c->red_part);
+                                                              c->d_dzc, c->d_ubd, c->red_part);
         CKL();
         k_ratio_final<<<1, 32, 0, c->stream>>>(c->red_blocks, c->red_part, c->red_out + 2);
         CKL();

@@ -43,14 +43,15 @@ __device__ __forceinline__ void block_sum2(double a, double b, double *out) {
 // cells and of the weights dy_j dz_k, one partial pair per block (deterministic, no atomics).
 template <typename T>
 __global__ void __launch_bounds__(256) k_bulk_partial(Dims d, const T *__restrict__ U, const double *__restrict__ dyc,
-                                                      const double *__restrict__ dzc, double *__restrict__ part) {
+                                                      const double *__restrict__ dzc, const double *__restrict__ ubd,
+                                                      double *__restrict__ part) {
     Kahan s, w; s.init(); w.init();
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x) {
         int i = (int)(p % d.Nx);
         long long q = p / d.Nx;
         int j = (int)(q % d.Ny), k = (int)(q / d.Ny);
         double a = dyc[j] * dzc[k];
-        double u0 = (double)U[p], um = (double)U[idx3(d, wrap(i - 1, d.Nx), j, k)];
+        double u0 = (double)U[p] + ubd[j], um = (double)U[idx3(d, wrap(i - 1, d.Nx), j, k)] + ubd[j];
         s.add(0.5 * (u0 + um) * a);
         w.add(a);
     }
@@ -101,14 +102,15 @@ __global__ void __launch_bounds__(256) k_maxdiv(Dims d, const T *__restrict__ U,
 template <typename T>
 __global__ void __launch_bounds__(256) k_ke_partial(Dims d, const T *__restrict__ U, const T *__restrict__ V,
                                                     const T *__restrict__ W, double dx, const double *__restrict__ dyc,
-                                                    const double *__restrict__ dzc, double *__restrict__ part) {
+                                                    const double *__restrict__ dzc, const double *__restrict__ ubd,
+                                                    double *__restrict__ part) {
     Kahan s, w; s.init(); w.init();
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x) {
         int i = (int)(p % d.Nx);
         long long q = p / d.Nx;
         int j = (int)(q % d.Ny), k = (int)(q / d.Ny);
         double vol = dyc[j] * dzc[k] * dx;
-        double uc = 0.5 * ((double)U[p] + (double)U[idx3(d, wrap(i - 1, d.Nx), j, k)]);
+        double uc = 0.5 * (((double)U[p] + ubd[j]) + ((double)U[idx3(d, wrap(i - 1, d.Nx), j, k)] + ubd[j]));
         double vc = 0.5 * ((double)ld_yf(V, d, i, j, k) + (double)ld_yf(V, d, i, j - 1, k));
         double wc = 0.5 * ((double)W[p] + (double)W[idx3(d, i, j, wrap(k - 1, d.Nz))]);
         s.add(0.5 * (uc * uc + vc * vc + wc * wc) * vol);
@@ -143,7 +145,7 @@ enum FieldKind { FK_U = 0, FK_V = 1, FK_W = 2, FK_P = 3, FK_NUT = 4 };
 // Device index and sign of one ghosted reference element (Fortran 1-based (I,J,K)).  Mirrors the ghost rules of
 // apply_boundary_conditions (velocities), finish_pressure_ghosts (P) and sgs_fill_ghosts (nu_t); sign 0 means the
 // element is zero.
-__device__ __forceinline__ long long map_ghost(const Dims &d, int kind, int I, int J, int K, int &sign) {
+__device__ __forceinline__ long long map_ghost(const Dims &d, int kind, int I, int J, int K, int &sign, int &jdev) {
     sign = 1;
     int i = I - 2, j = J - 2, k = K - 2;
     i = ((i % d.Nx) + d.Nx) % d.Nx;   // x periodic for every field (faces and centres alike)
@@ -165,35 +167,42 @@ __device__ __forceinline__ long long map_ghost(const Dims &d, int kind, int I, i
         if (j < 0) { j = 0; sign = -1; }
         if (j >= d.Ny) { j = d.Ny - 1; sign = -1; }
     }
+    jdev = j;
     return idx3(d, i, j, k);
 }
 
 // Expand a device field into its ghosted FP64 reference array (n1 x n2 x n3, Fortran order).
 template <typename T>
 __global__ void __launch_bounds__(256) k_pack(Dims d, int kind, int n1, int n2, int n3, const T *__restrict__ f,
-                                              double *__restrict__ out) {
+                                              const double *__restrict__ ubd, double *__restrict__ out) {
     long long n = (long long)n1 * n2 * n3;
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
         int I = (int)(p % n1) + 1;
         long long q = p / n1;
         int J = (int)(q % n2) + 1, K = (int)(q / n2) + 1;
-        int sg;
-        long long s = map_ghost(d, kind, I, J, K, sg);
-        out[p] = sg == 0 ? 0.0 : (sg > 0 ? (double)f[s] : -(double)f[s]);
+        int sg, jd;
+        long long s = map_ghost(d, kind, I, J, K, sg, jd);
+        double v = (double)f[s];
+        if (kind == FK_U) v += ubd[jd];
+        out[p] = sg == 0 ? 0.0 : (sg > 0 ? v : -v);
     }
 }
 
 // Extract the independent cells of a ghosted FP64 reference array (n1 x n2 x n3) into a device field.
 template <typename T>
 __global__ void __launch_bounds__(256) k_unpack(Dims d, int kind, int n1, int n2, const double *__restrict__ in,
-                                                T *__restrict__ f) {
+                                                const double *__restrict__ ubd, T *__restrict__ f) {
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x) {
         int i = (int)(p % d.Nx);
         long long q = p / d.Nx;
         int j = (int)(q % d.Ny), k = (int)(q / d.Ny);
         T v;
         if (kind == FK_V && !d.yper && j == d.Ny - 1) v = T(0);   // top wall face
-        else v = (T)in[((long long)(k + 1) * n2 + (j + 1)) * n1 + (i + 1)];
+        else {
+            double x = in[((long long)(k + 1) * n2 + (j + 1)) * n1 + (i + 1)];
+            if (kind == FK_U) x -= ubd[j];
+            v = (T)x;
+        }
         f[p] = v;
     }
 }

@@ -145,51 +145,76 @@ __global__ void __launch_bounds__(256) k_col_fft(Dims d, typename cplx_t<T>::typ
 // src/poisson_gpu.f90:445-489), solved by the no-interchange branch of LAPACK zgtsv in double.  The
 // elimination pivots D(r) depend only on the mode, so 1/D(r) is tabulated once at set-up (table layout
 // (kz, r, kx), double); each solve is then a pair of division-free recurrences
-//   b'(r) = b(r) - m(r) b'(r-1),  m(r) = DL(r-1)/D(r-1)          (forward, b' kept in shared memory)
+//   b'(r) = b(r) - m(r) b'(r-1),  m(r) = DL(r-1)/D(r-1)          (forward, b' written back in place)
 //   x(n-1) = b'(n-1)/D(n-1),  x(r) = (b'(r) - DU(r) x(r+1))/D(r)  (backward)
 // The pressure operator is similar to a symmetric negative-definite matrix once the null mode is pinned, so
 // elimination without interchanges is stable.  One thread owns one (kx,kz) column and a warp covers 32
-// consecutive kx, so every row access is coalesced; loads do not alias the shared-memory stores, so the
-// compiler pipelines them across rows.
-template <typename T>
-__global__ void __launch_bounds__(32) k_ysolve(Dims d, typename cplx_t<T>::type *__restrict__ spec,
+// consecutive kx, so every row access is coalesced.  The recurrences are latency chains, so each sweep keeps a
+// ring of PF rows in flight: the loads for row r+PF are issued before row r is stored.
+template <typename T, int PF>
+__global__ void __launch_bounds__(64) k_ysolve(Dims d, typename cplx_t<T>::type *__restrict__ spec,
                                                const double *__restrict__ rpiv, const double *__restrict__ lo,
                                                const double *__restrict__ up) {
     typedef typename cplx_t<T>::type C;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *sb = (C *)smem_raw;   // [Ny][32]
-    const int c = threadIdx.x;
     const int Nxc = d.Nxc;
-    const int kx = blockIdx.x * 32 + c, kz = blockIdx.y;
+    const int kx = blockIdx.x * blockDim.x + threadIdx.x, kz = blockIdx.y;
     if (kx >= Nxc) return;
     const int n = d.Ny;
     C *col = spec + kz * n * Nxc + kx;
     const double *rp = rpiv + kz * n * Nxc + kx;
-    C v = col[0];
-    sb[c] = v;
-    double br = (double)v.x, bi = (double)v.y;
-    double rprev = __ldg(rp);
-#pragma unroll 4
-    for (int r = 1; r < n; ++r) {
-        double m = __ldg(lo + r) * rprev;
-        v = col[r * Nxc];
-        rprev = __ldg(rp + r * Nxc);
-        br = (double)v.x - m * br;
-        bi = (double)v.y - m * bi;
-        C o; o.x = (T)br; o.y = (T)bi;
-        sb[r * 32 + c] = o;
+    C bq[PF];
+    double rq[PF];
+    // forward elimination, rows 0..n-1
+#pragma unroll
+    for (int q = 0; q < PF; ++q) {
+        if (q < n) { bq[q] = col[q * Nxc]; rq[q] = __ldg(rp + q * Nxc); }
     }
+    double br = (double)bq[0].x, bi = (double)bq[0].y, rprev = rq[0];
+    for (int r0 = 0; r0 < n; r0 += PF) {
+#pragma unroll
+        for (int q = 0; q < PF; ++q) {
+            const int r = r0 + q;
+            if (r >= n) break;
+            C v = bq[q];
+            double rcur = rq[q];
+            const int rn = r + PF;
+            if (rn < n) { bq[q] = col[rn * Nxc]; rq[q] = __ldg(rp + rn * Nxc); }
+            if (r > 0) {
+                double m = __ldg(lo + r) * rprev;
+                br = (double)v.x - m * br;
+                bi = (double)v.y - m * bi;
+                C o; o.x = (T)br; o.y = (T)bi;
+                if (r < n - 1) col[r * Nxc] = o;
+            }
+            rprev = rcur;
+        }
+    }
+    // back substitution, rows n-1..0
     double xr = br * rprev, xi = bi * rprev;
-    v.x = (T)xr; v.y = (T)xi;
-    col[(n - 1) * Nxc] = v;
-#pragma unroll 4
-    for (int r = n - 2; r >= 0; --r) {
-        double u = __ldg(up + r), rv = __ldg(rp + r * Nxc);
-        C b = sb[r * 32 + c];
-        xr = ((double)b.x - u * xr) * rv;
-        xi = ((double)b.y - u * xi) * rv;
-        v.x = (T)xr; v.y = (T)xi;
-        col[r * Nxc] = v;
+    {
+        C o; o.x = (T)xr; o.y = (T)xi;
+        col[(n - 1) * Nxc] = o;
+    }
+#pragma unroll
+    for (int q = 0; q < PF; ++q) {
+        const int r = n - 2 - q;
+        if (r >= 0) { bq[q] = col[r * Nxc]; rq[q] = __ldg(rp + r * Nxc); }
+    }
+    for (int r0 = n - 2; r0 >= 0; r0 -= PF) {
+#pragma unroll
+        for (int q = 0; q < PF; ++q) {
+            const int r = r0 - q;
+            if (r < 0) break;
+            C b = bq[q];
+            double rv = rq[q];
+            const int rn = r - PF;
+            if (rn >= 0) { bq[q] = col[rn * Nxc]; rq[q] = __ldg(rp + rn * Nxc); }
+            double u = __ldg(up + r);
+            xr = ((double)b.x - u * xr) * rv;
+            xi = ((double)b.y - u * xi) * rv;
+            C o; o.x = (T)xr; o.y = (T)xi;
+            col[r * Nxc] = o;
+        }
     }
 }
 
@@ -265,6 +290,57 @@ __global__ void __launch_bounds__(256) k_correct(PoissonArgs<T> a, const T *__re
     if (P) {
         if (sizeof(T) == 8) P[p] = (T)((double)pc / a.pdiv);
         else P[p] = pc * (T)(1.0 / a.pdiv);
+    }
+}
+
+// Same correction, four consecutive x cells per thread with 16-byte (FP32) / 2x16-byte (FP64) accesses; needs
+// Nx % 4 == 0.  One block row covers 64 x 4 cells of one (j,k) line pair.
+template <typename T> struct Vec4;
+template <> struct Vec4<float> { typedef float4 type; };
+template <> struct Vec4<double> { typedef double4 type; };
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_correct4(PoissonArgs<T> a, const T *__restrict__ phi, const T *__restrict__ us,
+                                                  const T *__restrict__ vs, const T *__restrict__ ws, T *__restrict__ U,
+                                                  T *__restrict__ V, T *__restrict__ W, T *__restrict__ P) {
+    typedef typename Vec4<T>::type V4;
+    typedef Arith<T> A;
+    const Dims &d = a.d;
+    const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz, plane = Nx * Ny, nq = Nx >> 2;
+    const int iq = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (iq >= nq || j >= Ny) return;
+    const int i = iq << 2;
+    const int p = k * plane + j * Nx + i;
+    const V4 pc = *reinterpret_cast<const V4 *>(phi + p);
+    const T pnext = __ldg(phi + (i + 4 == Nx ? p + 4 - Nx : p + 4));
+    const V4 pz = *reinterpret_cast<const V4 *>(phi + (k == Nz - 1 ? p - (Nz - 1) * plane : p + plane));
+    const T idx = a.inv_dx, idz = A::inv(a.mz.df, a.mz.idf, k);
+    V4 u = *reinterpret_cast<const V4 *>(us + p), w = *reinterpret_cast<const V4 *>(ws + p);
+    u.x = u.x - (pc.y - pc.x) * idx; u.y = u.y - (pc.z - pc.y) * idx;
+    u.z = u.z - (pc.w - pc.z) * idx; u.w = u.w - (pnext - pc.w) * idx;
+    w.x = w.x - (pz.x - pc.x) * idz; w.y = w.y - (pz.y - pc.y) * idz;
+    w.z = w.z - (pz.z - pc.z) * idz; w.w = w.w - (pz.w - pc.w) * idz;
+    *reinterpret_cast<V4 *>(U + p) = u;
+    *reinterpret_cast<V4 *>(W + p) = w;
+    if (j < d.NyV) {
+        const V4 py = *reinterpret_cast<const V4 *>(phi + (j == Ny - 1 ? p - (Ny - 1) * Nx : p + Nx));
+        const T idy = A::inv(a.my.df, a.my.idf, j);
+        V4 v = *reinterpret_cast<const V4 *>(vs + p);
+        v.x = v.x - (py.x - pc.x) * idy; v.y = v.y - (py.y - pc.y) * idy;
+        v.z = v.z - (py.z - pc.z) * idy; v.w = v.w - (py.w - pc.w) * idy;
+        *reinterpret_cast<V4 *>(V + p) = v;
+    }
+    if (P) {
+        V4 o;
+        if (sizeof(T) == 8) {
+            o.x = (T)((double)pc.x / a.pdiv); o.y = (T)((double)pc.y / a.pdiv);
+            o.z = (T)((double)pc.z / a.pdiv); o.w = (T)((double)pc.w / a.pdiv);
+        } else {
+            const T r = (T)(1.0 / a.pdiv);
+            o.x = pc.x * r; o.y = pc.y * r; o.z = pc.z * r; o.w = pc.w * r;
+        }
+        *reinterpret_cast<V4 *>(P + p) = o;
     }
 }
 

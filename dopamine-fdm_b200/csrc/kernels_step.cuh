@@ -18,6 +18,10 @@ template <typename T> struct StepArgs {
     int sgs_model;               // 1 Vreman, 2 AMD
     T C_amd, c_V;
     double nu_d, Ly, yg2, ygtop; // wall distances of the first centres: yg(2), Ly - yg(nyg-1)
+    // Streamwise base profile: U is stored as U - ub(j) (FP32-mixed; all zeros in FP64).  ub is exactly
+    // representable in the storage type; ubd is the same profile in double.
+    const T *ub;
+    const double *ubd;
 };
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -125,11 +129,12 @@ __global__ void k_wm_filter(StepArgs<T> a, WallState ws, const T *__restrict__ U
         long long p = ((long long)iw * d.Nz + k) * d.Nx + i;
         double eps = 1.0;
         if (!seed && ws.tx[p] > 0.0) eps = fmin(1.0, dt * kap * ws.tx[p] / (Tf_fac * ym));
-        ws.ux[p] = (1.0 - eps) * ws.ux[p] + eps * (double)U[idx3(d, i, jm, k)];
+        const double ubm = a.ubd[jm];
+        ws.ux[p] = (1.0 - eps) * ws.ux[p] + eps * ((double)U[idx3(d, i, jm, k)] + ubm);
         ws.wx[p] = (1.0 - eps) * ws.wx[p] + eps * 0.5 * ((double)W[idx3(d, i, jm, km)] + (double)W[idx3(d, i, jm, k)]);
         eps = 1.0;
         if (!seed && ws.tz[p] > 0.0) eps = fmin(1.0, dt * kap * ws.tz[p] / (Tf_fac * ym));
-        ws.uz[p] = (1.0 - eps) * ws.uz[p] + eps * 0.5 * ((double)U[idx3(d, im, jm, k)] + (double)U[idx3(d, i, jm, k)]);
+        ws.uz[p] = (1.0 - eps) * ws.uz[p] + eps * 0.5 * (((double)U[idx3(d, im, jm, k)] + ubm) + ((double)U[idx3(d, i, jm, k)] + ubm));
         ws.wz[p] = (1.0 - eps) * ws.wz[p] + eps * (double)W[idx3(d, i, jm, k)];
     }
 }
@@ -146,7 +151,8 @@ __global__ void k_wall_model(StepArgs<T> a, WallState ws, const T *__restrict__ 
         double y_match = fmax((iw == 0) ? a.yg2 : a.ygtop, 1e-14);
         long long p = ((long long)iw * d.Nz + k) * d.Nx + i;
         // U faces
-        double Uw = (double)U[idx3(d, i, jw, k)];
+        const double ubw = a.ubd[jw];
+        double Uw = (double)U[idx3(d, i, jw, k)] + ubw;
         double W_at = 0.5 * ((double)W[idx3(d, i, jw, km)] + (double)W[idx3(d, i, jw, k)]);
         double u_ref = sqrt(Uw * Uw + W_at * W_at), u_match = u_ref, num = Uw;
         if (filter) { u_match = sqrt(ws.ux[p] * ws.ux[p] + ws.wx[p] * ws.wx[p]); num = ws.ux[p]; u_ref = u_match; }
@@ -155,7 +161,7 @@ __global__ void k_wall_model(StepArgs<T> a, WallState ws, const T *__restrict__ 
         double tv = u_tau * u_tau * num / fmax(u_ref, 1e-30);
         ws.tau_x[p] = (iw == 0) ? tv : -tv;
         // W faces
-        double uc = 0.5 * ((double)U[idx3(d, im, jw, k)] + Uw);
+        double uc = 0.5 * (((double)U[idx3(d, im, jw, k)] + ubw) + Uw);
         double Ww = (double)W[idx3(d, i, jw, k)];
         u_ref = sqrt(uc * uc + Ww * Ww); u_match = u_ref; num = Ww;
         if (filter) { u_match = sqrt(ws.uz[p] * ws.uz[p] + ws.wz[p] * ws.wz[p]); num = ws.wz[p]; u_ref = u_match; }
@@ -357,11 +363,13 @@ template <typename T, int PX> struct TileQ {
     __device__ __forceinline__ T N(int di, int dj, int dk) const { return n[dk + 1][c + dj * PX + di]; }
 };
 
-// Tiled kernels (KIND 0: fused stage, KIND 1: eddy viscosity), 2.5-D blocked: a block owns a TX x TY column of (i,j) cells and marches through a chunk of
-// kc z-planes.  Each z-plane of U, V, W (and nu_t) is loaded from HBM once per block, with its halo, into a
-// rotating set of three shared planes; the boundary rules are applied while loading.  Every thread then evaluates
-// the three right-hand sides of its cell from shared memory and writes the RK3 update (or, with rhs_only, the
-// right-hand sides themselves for the unit entry point).
+// Tiled kernels (KIND 0: fused stage, KIND 1: eddy viscosity), 2.5-D blocked: a block owns a TX x TY column of
+// (i,j) cells and marches through a chunk of kc z-planes.  Each z-plane of U, V, W (and nu_t) is read from HBM once
+// per block, with its one-cell halo, into one of four rotating shared planes; the boundary rules are applied while
+// loading.  The loads of plane k+2 are issued into registers before the cells of plane k are evaluated, so their
+// latency hides behind the arithmetic, and one barrier per plane suffices.  Every thread evaluates the three
+// right-hand sides of its cell from shared memory and writes the RK3 update (or, with rhs_only, the right-hand
+// sides themselves for the unit entry point; with KIND 1, nu_t).
 template <typename T, bool LES, int TX, int TY, int KIND>
 __global__ void __launch_bounds__(TX *TY) k_tiled(StepArgs<T> a, const T *__restrict__ U, const T *__restrict__ V,
                                                   const T *__restrict__ W, const T *__restrict__ NU,
@@ -372,7 +380,8 @@ __global__ void __launch_bounds__(TX *TY) k_tiled(StepArgs<T> a, const T *__rest
                                                   T *__restrict__ wsf, T *__restrict__ rhs_only, T *__restrict__ nut_out) {
     constexpr int PX = TX + 2, PY = TY + 2, PS = PX * PY, NT = TX * TY;
     constexpr int NF = LES ? 4 : 3;
-    __shared__ T sm[NF][3][PS];
+    constexpr int PER = (PS + NT - 1) / NT;   // plane elements per thread
+    __shared__ T sm[NF][4][PS];
     const Dims &d = a.d;
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
     const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
@@ -382,79 +391,104 @@ __global__ void __launch_bounds__(TX *TY) k_tiled(StepArgs<T> a, const T *__rest
     const bool active = i < Nx && j < Ny;
     const int plane = Nx * Ny;
 
-    auto load_plane = [&](int slot, int k) {
-        int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k);
-        const int kb = kw * plane;
-        for (int e = threadIdx.x; e < PS; e += NT) {
+    // This thread's share of a plane: offsets within the plane (or -1) and the boundary rule of each element.
+    int off[PER];
+    signed char rule[PER];   // 0 interior, 1 wall ghost row (mirror U/W, zero V/nu_t)
+    T ubq[PER];              // streamwise base profile of the element's row
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        int e = threadIdx.x + q * NT;
+        off[q] = -1; rule[q] = 0; ubq[q] = T(0);
+        if (e < PS) {
             int jj = e / PX, ii = e - jj * PX;
             int gi = i0 - 1 + ii;
             gi = gi < 0 ? gi + Nx : gi;
             while (gi >= Nx) gi -= Nx;
-            int gj = j0 - 1 + jj;
-            T u, v, w, nu = T(0);
+            int gj = j0 - 1 + jj, g;
             if (d.yper) {
-                int g = gj < 0 ? gj + Ny : gj;
+                g = gj < 0 ? gj + Ny : gj;
                 while (g >= Ny) g -= Ny;
-                int o = kb + g * Nx + gi;
-                u = __ldg(U + o); v = __ldg(V + o); w = __ldg(W + o);
-                if (LES) nu = __ldg(NU + o);
             } else {
-                int g = gj < 0 ? 0 : (gj >= Ny ? Ny - 1 : gj);
-                int o = kb + g * Nx + gi;
-                u = __ldg(U + o); w = __ldg(W + o);
-                if (gj < 0 || gj >= Ny) { u = -u; w = -w; v = T(0); }   // no-slip mirror, zero wall faces
-                else { v = __ldg(V + o); if (LES) nu = __ldg(NU + o); }
+                g = gj < 0 ? 0 : (gj >= Ny ? Ny - 1 : gj);
+                rule[q] = (gj < 0 || gj >= Ny) ? 1 : 0;
             }
-            sm[0][slot][e] = u; sm[1][slot][e] = v; sm[2][slot][e] = w;
-            if (LES) sm[NF - 1][slot][e] = nu;
+            off[q] = g * Nx + gi;
+            ubq[q] = __ldg(a.ub + g);
+        }
+    }
+    T ru_[PER], rv_[PER], rw_[PER], rn_[PER];
+    auto fetch = [&](int k) {
+        int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k);
+        const int kb = kw * plane;
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            if (off[q] < 0) continue;
+            int o = kb + off[q];
+            ru_[q] = __ldg(U + o) + ubq[q]; rw_[q] = __ldg(W + o);
+            if (rule[q]) { ru_[q] = -ru_[q]; rw_[q] = -rw_[q]; rv_[q] = T(0); rn_[q] = T(0); }   // no-slip mirror
+            else { rv_[q] = __ldg(V + o); rn_[q] = LES ? __ldg(NU + o) : T(0); }
+        }
+    };
+    auto commit = [&](int slot) {
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            if (off[q] < 0) continue;
+            int e = threadIdx.x + q * NT;
+            sm[0][slot][e] = ru_[q]; sm[1][slot][e] = rv_[q]; sm[2][slot][e] = rw_[q];
+            if (LES) sm[NF - 1][slot][e] = rn_[q];
         }
     };
 
-    int s_m = 0, s_0 = 1, s_p = 2;
-    load_plane(s_m, k0 - 1);
-    load_plane(s_0, k0);
+    // planes k0-1, k0, k0+1 into slots 0, 1, 2; plane k lives in slot (k - k0 + 1) & 3
+    fetch(k0 - 1); commit(0);
+    fetch(k0); commit(1);
+    fetch(k0 + 1); commit(2);
+    __syncthreads();
     const int cloc = (ty + 1) * PX + tx + 1;
     for (int k = k0; k < kend; ++k) {
-        load_plane(s_p, k + 1);
-        __syncthreads();
+        const bool more = k + 2 <= kend;
+        if (more) fetch(k + 2);
+        const int sm_ = (k - k0) & 3, s0 = (k - k0 + 1) & 3, sp = (k - k0 + 2) & 3;
         if (active) {
+            const int p = k * plane + j * Nx + i;
             TileQ<T, PX> q;
             q.c = cloc;
-            q.u[0] = sm[0][s_m]; q.u[1] = sm[0][s_0]; q.u[2] = sm[0][s_p];
-            q.v[0] = sm[1][s_m]; q.v[1] = sm[1][s_0]; q.v[2] = sm[1][s_p];
-            q.w[0] = sm[2][s_m]; q.w[1] = sm[2][s_0]; q.w[2] = sm[2][s_p];
-            q.n[0] = sm[NF - 1][s_m]; q.n[1] = sm[NF - 1][s_0]; q.n[2] = sm[NF - 1][s_p];
-            const int p = k * plane + j * Nx + i;
+            q.u[0] = sm[0][sm_]; q.u[1] = sm[0][s0]; q.u[2] = sm[0][sp];
+            q.v[0] = sm[1][sm_]; q.v[1] = sm[1][s0]; q.v[2] = sm[1][sp];
+            q.w[0] = sm[2][sm_]; q.w[1] = sm[2][s0]; q.w[2] = sm[2][sp];
+            q.n[0] = sm[NF - 1][sm_]; q.n[1] = sm[NF - 1][s0]; q.n[2] = sm[NF - 1][sp];
             if (KIND == 1) {
                 nut_out[p] = nut_at<T>(a, q, j, k);
             } else {
-            T ru = rhs_u_at<T, LES>(a, q, tau_x, i, j, k);
-            T rw = rhs_w_at<T, LES>(a, q, tau_z, i, j, k);
-            const bool vrow = j < d.NyV;
-            T rv = vrow ? rhs_v_at<T, LES>(a, q, i, j, k) : T(0);
-            if (rhs_only) {
-                rhs_only[p] = ru; rhs_only[d.cells + p] = rv; rhs_only[2 * d.cells + p] = rw;
-            } else if (sc.stage == 1) {
-                T c = (T)sc.dt_a11;
-                T u0 = q.U(0, 0, 0), w0 = q.W(0, 0, 0);
-                uo[p] = u0; f1u[p] = ru; us[p] = u0 + c * ru;
-                wo[p] = w0; f1w[p] = rw; wsf[p] = w0 + c * rw;
-                if (vrow) { T v0 = q.V(0, 0, 0); vo[p] = v0; f1v[p] = rv; vs[p] = v0 + c * rv; }
-            } else if (sc.incr) {
-                T c1 = (T)sc.c1, c2 = (T)sc.c2, dtt = (T)sc.dt;
-                us[p] = dtt * (c1 * f1u[p] + c2 * ru);
-                wsf[p] = dtt * (c1 * f1w[p] + c2 * rw);
-                if (vrow) vs[p] = dtt * (c1 * f1v[p] + c2 * rv);
-            } else {
-                T c1 = (T)sc.c1, c2 = (T)sc.c2, dtt = (T)sc.dt;
-                us[p] = uo[p] + dtt * (c1 * f1u[p] + c2 * ru);
-                wsf[p] = wo[p] + dtt * (c1 * f1w[p] + c2 * rw);
-                if (vrow) vs[p] = vo[p] + dtt * (c1 * f1v[p] + c2 * rv);
-            }
+                const bool vrow = j < d.NyV;
+                const bool upd = !rhs_only && sc.stage != 1;
+                T ou = T(0), ov = T(0), ow = T(0), fu = T(0), fv = T(0), fw = T(0);
+                if (upd) {   // issue the base-state and F1 loads before the arithmetic
+                    ou = uo[p]; ow = wo[p]; fu = f1u[p]; fw = f1w[p];
+                    if (vrow) { ov = vo[p]; fv = f1v[p]; }
+                }
+                T ru = rhs_u_at<T, LES>(a, q, tau_x, i, j, k);
+                T rw = rhs_w_at<T, LES>(a, q, tau_z, i, j, k);
+                T rv = vrow ? rhs_v_at<T, LES>(a, q, i, j, k) : T(0);
+                if (rhs_only) {
+                    rhs_only[p] = ru; rhs_only[d.cells + p] = rv; rhs_only[2 * d.cells + p] = rw;
+                } else if (sc.stage == 1) {
+                    T c = (T)sc.dt_a11;
+                    T u0 = __ldg(U + p), w0 = q.W(0, 0, 0);   // U as stored (deviation from the base profile)
+                    uo[p] = u0; f1u[p] = ru; us[p] = u0 + c * ru;
+                    wo[p] = w0; f1w[p] = rw; wsf[p] = w0 + c * rw;
+                    if (vrow) { T v0 = q.V(0, 0, 0); vo[p] = v0; f1v[p] = rv; vs[p] = v0 + c * rv; }
+                } else {
+                    T c1 = (T)sc.c1, c2 = (T)sc.c2, dtt = (T)sc.dt;
+                    if (sc.incr) { ou = T(0); ow = T(0); ov = T(0); }
+                    us[p] = ou + dtt * (c1 * fu + c2 * ru);
+                    wsf[p] = ow + dtt * (c1 * fw + c2 * rw);
+                    if (vrow) vs[p] = ov + dtt * (c1 * fv + c2 * rv);
+                }
             }
         }
+        if (more) commit((k - k0 + 3) & 3);
         __syncthreads();
-        int t = s_m; s_m = s_0; s_0 = s_p; s_p = t;
     }
 }
 

@@ -116,6 +116,16 @@ def test_full_step_parity_fp32_mixed(oracle_mod, name):
         assert rel_l2(a, b) <= TOL32, (key, rel_l2(a, b))
 
 
+@pytest.mark.parametrize("name", ["chan_small", "tgv_small"])
+def test_fp32_mixed_100_steps_within_1e5(oracle_mod, name):
+    """The FP32-mixed target: <= 1e-5 relative L2 of u, v, w and p against the FP64 oracle after 100 steps."""
+    c, o, s = _pair(oracle_mod, name, "fp32")
+    o.step(100)
+    s.compute_time_step_RK3(100)
+    for key, a, b in zip("UVWP", s.get_state(), o.get_state()):
+        assert rel_l2(a, b) <= TOL32, (key, rel_l2(a, b))
+
+
 def test_graphs_match_plain_launches(oracle_mod):
     c = cases.chan_les_amd_small()
     U, V, W, P = cases.initial_condition(c)
