@@ -89,10 +89,47 @@ __device__ __forceinline__ void dft_small(C *v, int R) {
     }
 }
 
+// One Stockham pass of compile-time radix R over `nlines` lines (see the header comment for the index map).
+template <typename T, bool INV, bool LINES_FAST, int NL, int R>
+__device__ __forceinline__ void fft_pass(const typename cplx_t<T>::type *__restrict__ src,
+                                         typename cplx_t<T>::type *__restrict__ dst, int nlines, int ldl, int lde,
+                                         int n, int Ns, const FastDiv &fns, const FastDiv &fnb,
+                                         const typename cplx_t<T>::type *__restrict__ tw) {
+    typedef typename cplx_t<T>::type C;
+    const int nb = n / R;
+    const int total = nb * (LINES_FAST ? NL : nlines);
+    const int twstep = n / (Ns * R);
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+        int line, j;
+        if (LINES_FAST) { line = b % NL; j = b / NL; }
+        else { line = (int)fdiv((unsigned)b, fnb); j = b - line * nb; }
+        const int q = (int)fdiv((unsigned)j, fns);
+        const int k = j - q * Ns;
+        C v[R];
+        const C *s = src + line * ldl;
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = s[(j + r * nb) * lde];
+        if (k != 0) {
+            const int tk = k * twstep;
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                C w = __ldg(tw + r * tk);
+                v[r] = INV ? cmulc(v[r], w) : cmul(v[r], w);
+            }
+        }
+        dft_small<T, INV>(v, R);
+        C *d = dst + line * ldl;
+        const int base = q * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) d[(base + r * Ns) * lde] = v[r];
+    }
+}
+
 // Transforms `nlines` lines held in shared memory.  Element e of line l lives at buf[l*ldl + e*lde].
 // LINES_FAST selects the thread mapping: consecutive threads take consecutive lines (column tiles, lde > 1, the
 // line count NL is then a compile-time constant) or consecutive butterflies of one line (row tiles, lde == 1),
-// which keeps shared-memory accesses unit-stride.  No integer division is executed per butterfly.
+// which keeps shared-memory accesses unit-stride.  The radix of every pass is dispatched once per pass to a
+// compile-time kernel body; no integer division is executed per butterfly.
 // tw: global table W_n^k, k = 0..n-1 (storage precision).  Returns the buffer that holds the result.
 template <typename T, bool INV, bool LINES_FAST, int NL = 1>
 __device__ typename cplx_t<T>::type *fft_lines(typename cplx_t<T>::type *buf0, typename cplx_t<T>::type *buf1,
@@ -104,35 +141,11 @@ __device__ typename cplx_t<T>::type *fft_lines(typename cplx_t<T>::type *buf0, t
     int Ns = 1;
     for (int ps = 0; ps < p.nrad; ++ps) {
         const int R = p.rad[ps];
-        const int nb = n / R;
-        const int total = nb * (LINES_FAST ? NL : nlines);
-        const int twstep = n / (Ns * R);
-        const FastDiv fns = p.ns[ps], fnb = p.nb[ps];
-        for (int b = threadIdx.x; b < total; b += blockDim.x) {
-            int line, j;
-            if (LINES_FAST) { line = b % NL; j = b / NL; }
-            else { line = (int)fdiv((unsigned)b, fnb); j = b - line * nb; }
-            const int q = (int)fdiv((unsigned)j, fns);
-            const int k = j - q * Ns;
-            C v[5];
-            const C *s = src + line * ldl;
-#pragma unroll 5
-            for (int r = 0; r < 5; ++r)
-                if (r < R) v[r] = s[(j + r * nb) * lde];
-            if (k != 0) {
-#pragma unroll 4
-                for (int r = 1; r < 5; ++r)
-                    if (r < R) {
-                        C w = __ldg(tw + r * k * twstep);
-                        v[r] = INV ? cmulc(v[r], w) : cmul(v[r], w);
-                    }
-            }
-            dft_small<T, INV>(v, R);
-            C *d = dst + line * ldl;
-            const int base = q * Ns * R + k;
-#pragma unroll 5
-            for (int r = 0; r < 5; ++r)
-                if (r < R) d[(base + r * Ns) * lde] = v[r];
+        switch (R) {
+        case 4: fft_pass<T, INV, LINES_FAST, NL, 4>(src, dst, nlines, ldl, lde, n, Ns, p.ns[ps], p.nb[ps], tw); break;
+        case 2: fft_pass<T, INV, LINES_FAST, NL, 2>(src, dst, nlines, ldl, lde, n, Ns, p.ns[ps], p.nb[ps], tw); break;
+        case 3: fft_pass<T, INV, LINES_FAST, NL, 3>(src, dst, nlines, ldl, lde, n, Ns, p.ns[ps], p.nb[ps], tw); break;
+        default: fft_pass<T, INV, LINES_FAST, NL, 5>(src, dst, nlines, ldl, lde, n, Ns, p.ns[ps], p.nb[ps], tw); break;
         }
         __syncthreads();
         C *t = src; src = dst; dst = t;

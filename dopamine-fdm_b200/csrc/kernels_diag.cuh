@@ -157,12 +157,12 @@ __device__ __forceinline__ long long map_ghost(const Dims &d, int kind, int I, i
             j = ((j % d.Ny) + d.Ny) % d.Ny;
         }
     } else if (kind == FK_V) {
-        if (j < 0 || j >= d.Ny - 1) sign = 0;       // wall faces
+        if (j < 0 || j >= d.Ny - 1) { sign = 0; j = 0; }   // wall faces (index kept valid, never read)
     } else if (kind == FK_P) {
         if (j < 0) j = 0;
         if (j >= d.Ny) j = d.Ny - 1;
     } else if (kind == FK_NUT) {
-        if (j < 0 || j >= d.Ny) sign = 0;
+        if (j < 0 || j >= d.Ny) { sign = 0; j = 0; }
     } else {   // U, W: no-slip mirror
         if (j < 0) { j = 0; sign = -1; }
         if (j >= d.Ny) { j = d.Ny - 1; sign = -1; }
@@ -182,9 +182,13 @@ __global__ void __launch_bounds__(256) k_pack(Dims d, int kind, int n1, int n2, 
         int J = (int)(q % n2) + 1, K = (int)(q / n2) + 1;
         int sg, jd;
         long long s = map_ghost(d, kind, I, J, K, sg, jd);
-        double v = (double)f[s];
-        if (kind == FK_U) v += ubd[jd];
-        out[p] = sg == 0 ? 0.0 : (sg > 0 ? v : -v);
+        double v = 0.0;
+        if (sg != 0) {
+            v = (double)f[s];
+            if (kind == FK_U) v += ubd[jd];
+            if (sg < 0) v = -v;
+        }
+        out[p] = v;
     }
 }
 

@@ -149,9 +149,9 @@ __global__ void __launch_bounds__(256) k_col_fft(Dims d, typename cplx_t<T>::typ
 //   x(n-1) = b'(n-1)/D(n-1),  x(r) = (b'(r) - DU(r) x(r+1))/D(r)  (backward)
 // The pressure operator is similar to a symmetric negative-definite matrix once the null mode is pinned, so
 // elimination without interchanges is stable.  One thread owns one (kx,kz) column and a warp covers 32
-// consecutive kx, so every row access is coalesced.  The recurrences are latency chains, so each sweep keeps a
-// ring of PF rows in flight: the loads for row r+PF are issued before row r is stored.
-template <typename T, int PF>
+// consecutive kx, so every row access is coalesced.  Each sweep works in chunks of CH rows: the chunk's loads
+// are all issued before its recurrence runs, so one memory latency is paid per CH rows.
+template <typename T, int CH>
 __global__ void __launch_bounds__(64) k_ysolve(Dims d, typename cplx_t<T>::type *__restrict__ spec,
                                                const double *__restrict__ rpiv, const double *__restrict__ lo,
                                                const double *__restrict__ up) {
@@ -162,58 +162,50 @@ __global__ void __launch_bounds__(64) k_ysolve(Dims d, typename cplx_t<T>::type 
     const int n = d.Ny;
     C *col = spec + kz * n * Nxc + kx;
     const double *rp = rpiv + kz * n * Nxc + kx;
-    C bq[PF];
-    double rq[PF];
-    // forward elimination, rows 0..n-1
+    C v0 = col[0];
+    double br = (double)v0.x, bi = (double)v0.y, rprev = __ldg(rp);
+    for (int r0 = 1; r0 < n; r0 += CH) {
+        C v[CH];
+        double rv[CH], lv[CH];
 #pragma unroll
-    for (int q = 0; q < PF; ++q) {
-        if (q < n) { bq[q] = col[q * Nxc]; rq[q] = __ldg(rp + q * Nxc); }
-    }
-    double br = (double)bq[0].x, bi = (double)bq[0].y, rprev = rq[0];
-    for (int r0 = 0; r0 < n; r0 += PF) {
-#pragma unroll
-        for (int q = 0; q < PF; ++q) {
+        for (int q = 0; q < CH; ++q) {
             const int r = r0 + q;
-            if (r >= n) break;
-            C v = bq[q];
-            double rcur = rq[q];
-            const int rn = r + PF;
-            if (rn < n) { bq[q] = col[rn * Nxc]; rq[q] = __ldg(rp + rn * Nxc); }
-            if (r > 0) {
-                double m = __ldg(lo + r) * rprev;
-                br = (double)v.x - m * br;
-                bi = (double)v.y - m * bi;
-                C o; o.x = (T)br; o.y = (T)bi;
-                if (r < n - 1) col[r * Nxc] = o;
+            if (r < n) { v[q] = col[r * Nxc]; rv[q] = __ldg(rp + r * Nxc); lv[q] = __ldg(lo + r); }
+        }
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            const int r = r0 + q;
+            if (r < n) {
+                const double m = lv[q] * rprev;
+                br = (double)v[q].x - m * br;
+                bi = (double)v[q].y - m * bi;
+                if (r < n - 1) { C o; o.x = (T)br; o.y = (T)bi; col[r * Nxc] = o; }
+                rprev = rv[q];
             }
-            rprev = rcur;
         }
     }
-    // back substitution, rows n-1..0
     double xr = br * rprev, xi = bi * rprev;
     {
         C o; o.x = (T)xr; o.y = (T)xi;
         col[(n - 1) * Nxc] = o;
     }
+    for (int r0 = n - 2; r0 >= 0; r0 -= CH) {
+        C v[CH];
+        double rv[CH], uv[CH];
 #pragma unroll
-    for (int q = 0; q < PF; ++q) {
-        const int r = n - 2 - q;
-        if (r >= 0) { bq[q] = col[r * Nxc]; rq[q] = __ldg(rp + r * Nxc); }
-    }
-    for (int r0 = n - 2; r0 >= 0; r0 -= PF) {
-#pragma unroll
-        for (int q = 0; q < PF; ++q) {
+        for (int q = 0; q < CH; ++q) {
             const int r = r0 - q;
-            if (r < 0) break;
-            C b = bq[q];
-            double rv = rq[q];
-            const int rn = r - PF;
-            if (rn >= 0) { bq[q] = col[rn * Nxc]; rq[q] = __ldg(rp + rn * Nxc); }
-            double u = __ldg(up + r);
-            xr = ((double)b.x - u * xr) * rv;
-            xi = ((double)b.y - u * xi) * rv;
-            C o; o.x = (T)xr; o.y = (T)xi;
-            col[r * Nxc] = o;
+            if (r >= 0) { v[q] = col[r * Nxc]; rv[q] = __ldg(rp + r * Nxc); uv[q] = __ldg(up + r); }
+        }
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            const int r = r0 - q;
+            if (r >= 0) {
+                xr = ((double)v[q].x - uv[q] * xr) * rv[q];
+                xi = ((double)v[q].y - uv[q] * xi) * rv[q];
+                C o; o.x = (T)xr; o.y = (T)xi;
+                col[r * Nxc] = o;
+            }
         }
     }
 }

@@ -363,15 +363,24 @@ template <typename T, int PX> struct TileQ {
     __device__ __forceinline__ T N(int di, int dj, int dk) const { return n[dk + 1][c + dj * PX + di]; }
 };
 
+// Asynchronous global -> shared copies (cp.async, 4 or 8 bytes per element).
+template <int B> __device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(B));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
 // Tiled kernels (KIND 0: fused stage, KIND 1: eddy viscosity), 2.5-D blocked: a block owns a TX x TY column of
-// (i,j) cells and marches through a chunk of kc z-planes.  Each z-plane of U, V, W (and nu_t) is read from HBM once
-// per block, with its one-cell halo, into one of four rotating shared planes; the boundary rules are applied while
-// loading.  The loads of plane k+2 are issued into registers before the cells of plane k are evaluated, so their
-// latency hides behind the arithmetic, and one barrier per plane suffices.  Every thread evaluates the three
+// (i,j) cells and marches through a chunk of kc z-planes.  Each z-plane of U, V, W (and nu_t) is copied from HBM
+// once per block, with its one-cell halo, into one of four rotating shared planes by cp.async: the copies of
+// plane k+2 are in flight while the cells of plane k are evaluated, and one barrier per plane suffices.  After
+// its copies land, each thread adds the streamwise base profile to the U elements it copied and applies the wall
+// rules (no-slip mirror of U and W, zero V and nu_t on the ghost rows).  Every thread then evaluates the three
 // right-hand sides of its cell from shared memory and writes the RK3 update (or, with rhs_only, the right-hand
 // sides themselves for the unit entry point; with KIND 1, nu_t).
 template <typename T, bool LES, int TX, int TY, int KIND>
-__global__ void __launch_bounds__(TX *TY) k_tiled(StepArgs<T> a, const T *__restrict__ U, const T *__restrict__ V,
+__global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 4 : 2) k_tiled(StepArgs<T> a, const T *__restrict__ U, const T *__restrict__ V,
                                                   const T *__restrict__ W, const T *__restrict__ NU,
                                                   const double *__restrict__ tau_x, const double *__restrict__ tau_z,
                                                   StageCoef sc, int kc, T *__restrict__ uo, T *__restrict__ vo,
@@ -381,7 +390,7 @@ __global__ void __launch_bounds__(TX *TY) k_tiled(StepArgs<T> a, const T *__rest
     constexpr int PX = TX + 2, PY = TY + 2, PS = PX * PY, NT = TX * TY;
     constexpr int NF = LES ? 4 : 3;
     constexpr int PER = (PS + NT - 1) / NT;   // plane elements per thread
-    __shared__ T sm[NF][4][PS];
+    __shared__ __align__(16) T sm[NF][4][PS];
     const Dims &d = a.d;
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
     const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
@@ -391,14 +400,14 @@ __global__ void __launch_bounds__(TX *TY) k_tiled(StepArgs<T> a, const T *__rest
     const bool active = i < Nx && j < Ny;
     const int plane = Nx * Ny;
 
-    // This thread's share of a plane: offsets within the plane (or -1) and the boundary rule of each element.
+    // This thread's share of a plane: offsets within the plane (or -1), the wall rule and the base profile.
     int off[PER];
-    signed char rule[PER];   // 0 interior, 1 wall ghost row (mirror U/W, zero V/nu_t)
-    T ubq[PER];              // streamwise base profile of the element's row
+    bool ghost[PER];   // wall ghost row: mirror U/W, zero V/nu_t
+    T ubq[PER];
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
         int e = threadIdx.x + q * NT;
-        off[q] = -1; rule[q] = 0; ubq[q] = T(0);
+        off[q] = -1; ghost[q] = false; ubq[q] = T(0);
         if (e < PS) {
             int jj = e / PX, ii = e - jj * PX;
             int gi = i0 - 1 + ii;
@@ -410,44 +419,55 @@ __global__ void __launch_bounds__(TX *TY) k_tiled(StepArgs<T> a, const T *__rest
                 while (g >= Ny) g -= Ny;
             } else {
                 g = gj < 0 ? 0 : (gj >= Ny ? Ny - 1 : gj);
-                rule[q] = (gj < 0 || gj >= Ny) ? 1 : 0;
+                ghost[q] = (gj < 0 || gj >= Ny);
             }
             off[q] = g * Nx + gi;
             ubq[q] = __ldg(a.ub + g);
         }
     }
-    T ru_[PER], rv_[PER], rw_[PER], rn_[PER];
-    auto fetch = [&](int k) {
+    auto issue = [&](int slot, int k) {
         int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k);
         const int kb = kw * plane;
 #pragma unroll
         for (int q = 0; q < PER; ++q) {
             if (off[q] < 0) continue;
-            int o = kb + off[q];
-            ru_[q] = __ldg(U + o) + ubq[q]; rw_[q] = __ldg(W + o);
-            if (rule[q]) { ru_[q] = -ru_[q]; rw_[q] = -rw_[q]; rv_[q] = T(0); rn_[q] = T(0); }   // no-slip mirror
-            else { rv_[q] = __ldg(V + o); rn_[q] = LES ? __ldg(NU + o) : T(0); }
+            const int o = kb + off[q], e = threadIdx.x + q * NT;
+            cp_async<sizeof(T)>(&sm[0][slot][e], U + o);
+            cp_async<sizeof(T)>(&sm[2][slot][e], W + o);
+            if (!ghost[q]) {
+                cp_async<sizeof(T)>(&sm[1][slot][e], V + o);
+                if (LES) cp_async<sizeof(T)>(&sm[NF - 1][slot][e], NU + o);
+            }
         }
     };
-    auto commit = [&](int slot) {
+    auto fix = [&](int slot) {   // after this thread's copies have landed
 #pragma unroll
         for (int q = 0; q < PER; ++q) {
             if (off[q] < 0) continue;
-            int e = threadIdx.x + q * NT;
-            sm[0][slot][e] = ru_[q]; sm[1][slot][e] = rv_[q]; sm[2][slot][e] = rw_[q];
-            if (LES) sm[NF - 1][slot][e] = rn_[q];
+            const int e = threadIdx.x + q * NT;
+            T u = sm[0][slot][e] + ubq[q];
+            if (ghost[q]) {
+                u = -u;
+                sm[2][slot][e] = -sm[2][slot][e];
+                sm[1][slot][e] = T(0);
+                if (LES) sm[NF - 1][slot][e] = T(0);
+            }
+            sm[0][slot][e] = u;
         }
     };
 
     // planes k0-1, k0, k0+1 into slots 0, 1, 2; plane k lives in slot (k - k0 + 1) & 3
-    fetch(k0 - 1); commit(0);
-    fetch(k0); commit(1);
-    fetch(k0 + 1); commit(2);
+    issue(0, k0 - 1); issue(1, k0); issue(2, k0 + 1);
+    cp_async_commit();
+    cp_async_wait_all();
+    fix(0); fix(1); fix(2);
     __syncthreads();
     const int cloc = (ty + 1) * PX + tx + 1;
     for (int k = k0; k < kend; ++k) {
         const bool more = k + 2 <= kend;
-        if (more) fetch(k + 2);
+        const int snext = (k - k0 + 3) & 3;
+        if (more) issue(snext, k + 2);
+        cp_async_commit();
         const int sm_ = (k - k0) & 3, s0 = (k - k0 + 1) & 3, sp = (k - k0 + 2) & 3;
         if (active) {
             const int p = k * plane + j * Nx + i;
@@ -487,7 +507,8 @@ __global__ void __launch_bounds__(TX *TY) k_tiled(StepArgs<T> a, const T *__rest
                 }
             }
         }
-        if (more) commit((k - k0 + 3) & 3);
+        cp_async_wait_all();
+        if (more) fix(snext);
         __syncthreads();
     }
 }
