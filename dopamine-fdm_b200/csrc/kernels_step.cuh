@@ -187,8 +187,16 @@ __device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Q &q, const do
     bool wm_band = a.wm && (j + 2 <= 1 + a.nwl || j + 2 >= d.Ny + 2 - a.nwl);
     T wa = wm_band ? T(0) : a.w_adv, wd = T(1) - wa;
     // -d(uu)/dx
-    T t1 = T(0.5) * (Uc + Uip), t0 = T(0.5) * (Uim + Uc);
-    T r = -(wd * (t1 * t1 - t0 * t0) + wa * Uc * (t1 - t0)) * a.inv_dx;
+    T r;
+    if constexpr (sizeof(T) == 4) {
+        // FP32: t1^2 - t0^2 = (t1 - t0)(t1 + t0) with t1 - t0 from the stored deviations (no cancellation)
+        T dlt = T(0.5) * (q.Ud(1, 0, 0) - q.Ud(-1, 0, 0));
+        T sum = T(0.5) * (Uip + Uim) + Uc;
+        r = -dlt * (wd * sum + wa * Uc) * a.inv_dx;
+    } else {
+        T t1 = T(0.5) * (Uc + Uip), t0 = T(0.5) * (Uim + Uc);
+        r = -(wd * (t1 * t1 - t0 * t0) + wa * Uc * (t1 - t0)) * a.inv_dx;
+    }
     // -d(uv)/dy: u at y faces j-1, j (weighted), v at x faces (plain average)
     T V00 = q.V(0, 0, 0), V10 = q.V(1, 0, 0), V0m = q.V(0, -1, 0), V1m = q.V(1, -1, 0);
     {
@@ -201,7 +209,14 @@ __device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Q &q, const do
     {
         T u1 = mz.w0[k] * Uc + mz.w1[k] * Ukp, u0 = mz.w0[k - 1] * Ukm + mz.w1[k - 1] * Uc;
         T w1 = T(0.5) * (W00 + W10), w0 = T(0.5) * (W0m + W1m);
-        r = r - A::div(wd * (u1 * w1 - u0 * w0) + wa * T(0.5) * (w0 + w1) * (u1 - u0), mz.dc, mz.idc, k);
+        if constexpr (sizeof(T) == 4) {
+            // u1 w1 - u0 w0 = u1 (w1 - w0) + w0 (u1 - u0); u1 - u0 from deviations (same row: the profile cancels)
+            T Udc = q.Ud(0, 0, 0);
+            T du = (mz.w0[k] * Udc + mz.w1[k] * q.Ud(0, 0, 1)) - (mz.w0[k - 1] * q.Ud(0, 0, -1) + mz.w1[k - 1] * Udc);
+            r = r - A::div(wd * (u1 * (w1 - w0) + w0 * du) + wa * T(0.5) * (w0 + w1) * du, mz.dc, mz.idc, k);
+        } else {
+            r = r - A::div(wd * (u1 * w1 - u0 * w0) + wa * T(0.5) * (w0 + w1) * (u1 - u0), mz.dc, mz.idc, k);
+        }
     }
     // viscous: d(2 nu_x du/dx)/dx + d(nu_y (du/dy + dv/dx))/dy + d(nu_z (du/dz + dw/dx))/dz + dPdx
     T inv_dz3 = A::inv(mz.dc, mz.idc, k), inv_dy3 = A::inv(my.dc, my.idc, j);
@@ -224,10 +239,16 @@ __device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Q &q, const do
         if (j == 0) fy1 = (T)tau_x[k * d.Nx + i];
         if (j == d.Ny - 1) fy2 = (T)tau_x[(d.Nz + k) * d.Nx + i];
     }
-    T tk = A::div(Ukp - Uc, mz.df, mz.idf, k), tkm = A::div(Uc - Ukm, mz.df, mz.idf, k - 1);
+    T dUkp = Ukp - Uc, dUkm = Uc - Ukm, dUip = Uip - Uc, dUim = Uc - Uim;
+    if constexpr (sizeof(T) == 4) {   // x and z differences of U from the deviations
+        T Udc = q.Ud(0, 0, 0);
+        dUkp = q.Ud(0, 0, 1) - Udc; dUkm = Udc - q.Ud(0, 0, -1);
+        dUip = q.Ud(1, 0, 0) - Udc; dUim = Udc - q.Ud(-1, 0, 0);
+    }
+    T tk = A::div(dUkp, mz.df, mz.idf, k), tkm = A::div(dUkm, mz.df, mz.idf, k - 1);
     T fz2 = nu_z2 * (tk + (W10 - W00) * a.inv_dx);
     T fz1 = nu_z1 * (tkm + (W1m - W0m) * a.inv_dx);
-    r = r + T(2) * a.inv_dx2 * (nu_x2 * (Uip - Uc) - nu_x1 * (Uc - Uim)) + inv_dy3 * (fy2 - fy1) + inv_dz3 * (fz2 - fz1) + a.dPdx;
+    r = r + T(2) * a.inv_dx2 * (nu_x2 * dUip - nu_x1 * dUim) + inv_dy3 * (fy2 - fy1) + inv_dz3 * (fz2 - fz1) + a.dPdx;
     return r;
 }
 
@@ -248,7 +269,12 @@ __device__ __forceinline__ T rhs_v_at(const StepArgs<T> &a, const Q &q, int i, i
     {
         T u1 = my.w0[j] * Uc + my.w1[j] * Ucp, u0 = my.w0[j] * Um + my.w1[j] * Ump;
         T v1 = T(0.5) * (Vc + Vip), v0 = T(0.5) * (Vim + Vc);
-        r = r - (wd * (u1 * v1 - u0 * v0) + wa * T(0.5) * (u0 + u1) * (v1 - v0)) * a.inv_dx;
+        if constexpr (sizeof(T) == 4) {   // u1 v1 - u0 v0 = u1 (v1 - v0) + v0 (u1 - u0), u1 - u0 from deviations
+            T du = my.w0[j] * (q.Ud(0, 0, 0) - q.Ud(-1, 0, 0)) + my.w1[j] * (q.Ud(0, 1, 0) - q.Ud(-1, 1, 0));
+            r = r - (wd * (u1 * (v1 - v0) + v0 * du) + wa * T(0.5) * (u0 + u1) * (v1 - v0)) * a.inv_dx;
+        } else {
+            r = r - (wd * (u1 * v1 - u0 * v0) + wa * T(0.5) * (u0 + u1) * (v1 - v0)) * a.inv_dx;
+        }
     }
     // -d(vw)/dz: v at z faces (weighted), w at y face j (weighted)
     T Wc = q.W(0, 0, 0), Wjp = q.W(0, 1, 0), Wkm = q.W(0, 0, -1), Wkmjp = q.W(0, 1, -1);
@@ -299,7 +325,12 @@ __device__ __forceinline__ T rhs_w_at(const StepArgs<T> &a, const Q &q, const do
     {
         T u1 = mz.w0[k] * Uc + mz.w1[k] * Ukp, u0 = mz.w0[k] * Um + mz.w1[k] * Umkp;
         T w1 = T(0.5) * (Wc + Wip), w0 = T(0.5) * (Wim + Wc);
-        r = r - (wd * (u1 * w1 - u0 * w0) + wa * T(0.5) * (u0 + u1) * (w1 - w0)) * a.inv_dx;
+        if constexpr (sizeof(T) == 4) {   // u1 w1 - u0 w0 = u1 (w1 - w0) + w0 (u1 - u0), u1 - u0 from deviations
+            T du = mz.w0[k] * (q.Ud(0, 0, 0) - q.Ud(-1, 0, 0)) + mz.w1[k] * (q.Ud(0, 0, 1) - q.Ud(-1, 0, 1));
+            r = r - (wd * (u1 * (w1 - w0) + w0 * du) + wa * T(0.5) * (u0 + u1) * (w1 - w0)) * a.inv_dx;
+        } else {
+            r = r - (wd * (u1 * w1 - u0 * w0) + wa * T(0.5) * (u0 + u1) * (w1 - w0)) * a.inv_dx;
+        }
     }
     // -d(vw)/dy: v at z face k (weighted), w at y faces (weighted)
     T Vc = q.V(0, 0, 0), Vkp = q.V(0, 0, 1), Vjm = q.V(0, -1, 0), Vjmkp = q.V(0, -1, 1);
@@ -356,8 +387,11 @@ struct StageCoef {
 // (TX+2) x (TY+2) tile with a one-cell halo in x and y.
 template <typename T, int PX> struct TileQ {
     const T *u[3], *v[3], *w[3], *n[3];
-    int c;   // local index of the centre cell
-    __device__ __forceinline__ T U(int di, int dj, int dk) const { return u[dk + 1][c + dj * PX + di]; }
+    int c;       // local index of the centre cell
+    T ub[3];     // streamwise base profile of rows j-1, j, j+1 (mirrored on wall ghost rows)
+    // U (total) and Ud (stored deviation from the base profile; equal to U in FP64, where the profile is zero)
+    __device__ __forceinline__ T U(int di, int dj, int dk) const { return u[dk + 1][c + dj * PX + di] + ub[dj + 1]; }
+    __device__ __forceinline__ T Ud(int di, int dj, int dk) const { return u[dk + 1][c + dj * PX + di]; }
     __device__ __forceinline__ T V(int di, int dj, int dk) const { return v[dk + 1][c + dj * PX + di]; }
     __device__ __forceinline__ T W(int di, int dj, int dk) const { return w[dk + 1][c + dj * PX + di]; }
     __device__ __forceinline__ T N(int di, int dj, int dk) const { return n[dk + 1][c + dj * PX + di]; }
@@ -380,7 +414,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // right-hand sides of its cell from shared memory and writes the RK3 update (or, with rhs_only, the right-hand
 // sides themselves for the unit entry point; with KIND 1, nu_t).
 template <typename T, bool LES, int TX, int TY, int KIND>
-__global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 4 : 2) k_tiled(StepArgs<T> a, const T *__restrict__ U, const T *__restrict__ V,
+__global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepArgs<T> a, const T *__restrict__ U, const T *__restrict__ V,
                                                   const T *__restrict__ W, const T *__restrict__ NU,
                                                   const double *__restrict__ tau_x, const double *__restrict__ tau_z,
                                                   StageCoef sc, int kc, T *__restrict__ uo, T *__restrict__ vo,
@@ -403,11 +437,10 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 4 : 2) k_tiled(StepAr
     // This thread's share of a plane: offsets within the plane (or -1), the wall rule and the base profile.
     int off[PER];
     bool ghost[PER];   // wall ghost row: mirror U/W, zero V/nu_t
-    T ubq[PER];
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
         int e = threadIdx.x + q * NT;
-        off[q] = -1; ghost[q] = false; ubq[q] = T(0);
+        off[q] = -1; ghost[q] = false;
         if (e < PS) {
             int jj = e / PX, ii = e - jj * PX;
             int gi = i0 - 1 + ii;
@@ -422,7 +455,6 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 4 : 2) k_tiled(StepAr
                 ghost[q] = (gj < 0 || gj >= Ny);
             }
             off[q] = g * Nx + gi;
-            ubq[q] = __ldg(a.ub + g);
         }
     }
     auto issue = [&](int slot, int k) {
@@ -440,21 +472,27 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 4 : 2) k_tiled(StepAr
             }
         }
     };
-    auto fix = [&](int slot) {   // after this thread's copies have landed
+    auto fix = [&](int slot) {   // after this thread's copies have landed: wall ghost rows
 #pragma unroll
         for (int q = 0; q < PER; ++q) {
-            if (off[q] < 0) continue;
+            if (off[q] < 0 || !ghost[q]) continue;
             const int e = threadIdx.x + q * NT;
-            T u = sm[0][slot][e] + ubq[q];
-            if (ghost[q]) {
-                u = -u;
-                sm[2][slot][e] = -sm[2][slot][e];
-                sm[1][slot][e] = T(0);
-                if (LES) sm[NF - 1][slot][e] = T(0);
-            }
-            sm[0][slot][e] = u;
+            sm[0][slot][e] = -sm[0][slot][e];   // deviation mirrored; the row profile is mirrored in TileQ::ub
+            sm[2][slot][e] = -sm[2][slot][e];
+            sm[1][slot][e] = T(0);
+            if (LES) sm[NF - 1][slot][e] = T(0);
         }
     };
+    // base profile of the thread's rows j-1, j, j+1 (a wall ghost row carries minus its mirror row's profile)
+    T ubr[3];
+#pragma unroll
+    for (int dj = -1; dj <= 1; ++dj) {
+        int gj = min(j, Ny - 1) + dj;
+        T sgn = T(1);
+        if (d.yper) { gj = gj < 0 ? gj + Ny : (gj >= Ny ? gj - Ny : gj); }
+        else if (gj < 0 || gj >= Ny) { gj = gj < 0 ? 0 : Ny - 1; sgn = T(-1); }
+        ubr[dj + 1] = sgn * __ldg(a.ub + gj);
+    }
 
     // planes k0-1, k0, k0+1 into slots 0, 1, 2; plane k lives in slot (k - k0 + 1) & 3
     issue(0, k0 - 1); issue(1, k0); issue(2, k0 + 1);
@@ -473,6 +511,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 4 : 2) k_tiled(StepAr
             const int p = k * plane + j * Nx + i;
             TileQ<T, PX> q;
             q.c = cloc;
+            q.ub[0] = ubr[0]; q.ub[1] = ubr[1]; q.ub[2] = ubr[2];
             q.u[0] = sm[0][sm_]; q.u[1] = sm[0][s0]; q.u[2] = sm[0][sp];
             q.v[0] = sm[1][sm_]; q.v[1] = sm[1][s0]; q.v[2] = sm[1][sp];
             q.w[0] = sm[2][sm_]; q.w[1] = sm[2][s0]; q.w[2] = sm[2][sp];
@@ -494,7 +533,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 4 : 2) k_tiled(StepAr
                     rhs_only[p] = ru; rhs_only[d.cells + p] = rv; rhs_only[2 * d.cells + p] = rw;
                 } else if (sc.stage == 1) {
                     T c = (T)sc.dt_a11;
-                    T u0 = __ldg(U + p), w0 = q.W(0, 0, 0);   // U as stored (deviation from the base profile)
+                    T u0 = q.Ud(0, 0, 0), w0 = q.W(0, 0, 0);   // U as stored (deviation from the base profile)
                     uo[p] = u0; f1u[p] = ru; us[p] = u0 + c * ru;
                     wo[p] = w0; f1w[p] = rw; wsf[p] = w0 + c * rw;
                     if (vrow) { T v0 = q.V(0, 0, 0); vo[p] = v0; f1v[p] = rv; vs[p] = v0 + c * rv; }
