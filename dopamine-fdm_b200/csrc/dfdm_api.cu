@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -1037,6 +1038,84 @@ int dfdm_solve_poisson(dfdm_ctx *c, const double *rhs_in, double *phi_out) {
     });
     if (rc) return rc;
     CK(cudaMemcpyAsync(phi_out, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DFDM_OK;
+}
+
+}  // extern "C"
+
+// Staging array of dfdm_solve_poisson_noalloc. It is reserved once per device when the module is loaded there, so
+// the entry point itself never allocates; every call on a device shares it.
+static __device__ __align__(256) double g_noalloc_scratch[DFDM_NOALLOC_MAX_POINTS];
+
+namespace {
+const int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+// Address of the staging array on the current device, looked up on the first call for that device.
+int noalloc_scratch(double **out) {
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(DFDM_ERR_UNSUPPORTED, "device ordinal beyond 63");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            return fail(DFDM_ERR_CUDA, std::string("cudaGetSymbolAddress of the staging array: ") + cudaGetErrorString(e));
+        }
+        g_noalloc_ptr[dev] = (double *)p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return DFDM_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int dfdm_solve_poisson_noalloc(dfdm_ctx *c, const double *rhs_in, double *phi_out) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (!rhs_in || !phi_out) return fail(DFDM_ERR_INVALID, "null array");
+    const Dims &d = c->d;
+    int n1 = c->nxg - 1, n2 = c->nyg - 2, n3 = c->nzg - 1;
+    size_t n = (size_t)n1 * n2 * n3;
+    if (n > (size_t)DFDM_NOALLOC_MAX_POINTS)
+        return fail(DFDM_ERR_INVALID, "rhs_p has " + std::to_string(n) + " points; dfdm_solve_poisson_noalloc takes at most " +
+                                          std::to_string(DFDM_NOALLOC_MAX_POINTS) + " (use dfdm_solve_poisson)");
+    double *scratch = nullptr;
+    if (int rc = noalloc_scratch(&scratch)) return rc;
+    // The host copy fills scratch[0, n) before the unpack kernel reads it, and the pack kernel rewrites
+    // scratch[0, n) before the copy back: nothing has to start at zero.
+    CK(cudaMemcpyAsync(scratch, rhs_in, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    long long before = g_launches;
+    int rc = dispatch(c, [&](auto impl) {
+        typedef decltype(impl) I;
+        typedef typename std::remove_pointer<decltype(I::f(nullptr))>::type T;
+        typedef typename cplx_t<T>::type C;
+        int gb = reduce_grid(d);
+        k_unpack_rhs_p<T><<<gb, 256, 0, c->stream>>>(d, n1, n2, scratch, I::f(c->phi));
+        CKL();
+        long long lines = (long long)d.Ny * d.Nz;
+        int nb = (int)((lines + c->lx - 1) / c->lx);
+        k_fwd_x<T, false><<<nb, 256, c->smem_x, c->stream>>>(poisson_args<T>(c), c->lx, nullptr, nullptr, nullptr, I::f(c->phi),
+                                                             (C *)c->spec, c->plan_x, (const C *)c->tw_x, (const C *)c->twr_x);
+        CKL();
+        int r2;
+        if ((r2 = I::launch(c, 3, 1))) return r2;
+        if ((r2 = I::launch(c, 4, 1))) return r2;
+        if ((r2 = I::launch(c, 5, 1))) return r2;
+        if ((r2 = I::launch(c, 6, 1))) return r2;
+        int gb2 = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
+        k_pack_rhs_p<T><<<gb2, 256, 0, c->stream>>>(d, n1, n2, n3, I::f(c->phi), scratch);
+        CKL();
+        return DFDM_OK;
+    });
+    c->launches += g_launches - before;
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(phi_out, scratch, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return DFDM_OK;
 }

@@ -30,7 +30,7 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_compute_wall_model", "dfdm_apply_boundary_conditions", "dfdm_compute_projection_step",
            "dfdm_solve_poisson", "dfdm_compute_bulk_velocity", "dfdm_check_divergence", "dfdm_kinetic_energy",
            "dfdm_check_finite", "dfdm_pad_field", "dfdm_launch_kernel_async", "dfdm_kernel_bytes",
-           "dfdm_launch_count"]
+           "dfdm_launch_count", "dfdm_solve_poisson_noalloc"]
 
 
 class DfdmError(RuntimeError):
@@ -226,6 +226,13 @@ class Solver:
         a = np.asfortranarray(rhs_p, dtype=np.float64)
         out = np.zeros_like(a, order="F")
         _check(load().dfdm_solve_poisson(self.h, dptr(a), dptr(out)))
+        return out
+
+    def solve_poisson_noalloc(self, rhs_p):
+        """dfdm_solve_poisson through the library's fixed staging array: no device allocation in the call."""
+        a = np.asfortranarray(rhs_p, dtype=np.float64)
+        out = np.zeros_like(a, order="F")
+        _check(load().dfdm_solve_poisson_noalloc(self.h, dptr(a), dptr(out)))
         return out
 
     def compute_bulk_velocity(self) -> float:

@@ -134,6 +134,21 @@ int dfdm_compute_projection_step(dfdm_ctx *ctx, int save_p);
 /* solve_poisson_equation's solve alone (src/projection.f90:100-382): rhs_p in, pseudo-pressure out, both in
  * the reference shape (2:nxg,2:nyg-1,2:nzg); the output ghost planes follow apply_periodic_xz_pressure. */
 int dfdm_solve_poisson(dfdm_ctx *ctx, const double *rhs_p_in, double *phi_out);
+/* No counterpart in the reference: dfdm_solve_poisson with no device allocation in the call.
+ * dfdm_solve_poisson grows a per-context staging buffer with cudaMalloc on first use (and frees and regrows it,
+ * which waits for the whole device, when a larger copy comes along). Hosts that pack many contexts onto one GPU
+ * up to its memory limit, or that run other contexts' steps on concurrent streams, cannot take that: the
+ * cudaMalloc may fail on a full device and the cudaFree stalls every stream. This variant stages rhs_p and phi
+ * through one file-scope device array of DFDM_NOALLOC_MAX_POINTS doubles (16 MiB, reserved when the library is
+ * loaded on a device) and otherwise runs the same kernels on the context's own buffers.
+ *  - Sizes: (nxg-1)*(nyg-2)*(nzg-1) must not exceed DFDM_NOALLOC_MAX_POINTS, else DFDM_ERR_INVALID.
+ *  - The first call on a device looks the array's address up on the current device; make that first call
+ *    before any stream capture begins. The context's device must be current, as for every entry point.
+ *  - Every call, from any context, shares the one array and leaves its contents behind; each call writes the
+ *    part it reads before reading it. Calls whose GPU work overlaps (different streams, or different host
+ *    threads) race on the array: serialise them. */
+#define DFDM_NOALLOC_MAX_POINTS 2097152
+int dfdm_solve_poisson_noalloc(dfdm_ctx *ctx, const double *rhs_p_in, double *phi_out);
 /* compute_bulk_velocity (src/monitor.f90:463-523), FP64 compensated sum. */
 int dfdm_compute_bulk_velocity(dfdm_ctx *ctx, double *Ub);
 /* check_divergence (src/projection.f90:607-639): max |div u| over the interior. */
