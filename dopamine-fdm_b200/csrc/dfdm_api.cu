@@ -15,6 +15,7 @@
 #include "dfdm_common.cuh"
 #include "fft_smem.cuh"
 #include "kernels_diag.cuh"
+#include "kernels_fft2l.cuh"
 #include "kernels_poisson.cuh"
 #include "kernels_step.cuh"
 
@@ -90,6 +91,10 @@ struct dfdm_ctx {
     int lx = 8, tzx = 8;
     int kc_stage = 8, kc_sgs = 8;               // z-planes per block of the tiled kernels
     size_t smem_x = 0, smem_z = 0, smem_y = 0;
+    // two-level register transforms (fft_reg.cuh) where the length has a split; Stockham otherwise
+    bool x2 = false, z2 = false, y2 = false;
+    int lx2 = 1, thr_z2 = 256, thr_y2 = 256;
+    size_t smem_x2 = 0, smem_xi2 = 0, smem_z2 = 0, smem_y2 = 0;
     cudaStream_t own_stream = nullptr, stream = nullptr;
     double t = 0.0;
     bool wmf_seeded = false;
@@ -98,6 +103,7 @@ struct dfdm_ctx {
     cudaGraphExec_t gexec = nullptr;
     cudaGraph_t graph = nullptr;
     bool unit_projection = false;    // dfdm_compute_projection_step: u* is the resident state, not an increment
+    bool projected = false;          // the resident velocity is a full step's output (no set_state since)
     long long launches = 0;          // kernels enqueued (host-side count)
     long long graph_launches = 0;    // kernels in the captured step graph
 };
@@ -240,7 +246,73 @@ int choose_kc(const Dims &d, int blocks_per_sm, int nsm) {
 template <typename T> struct Impl {
     typedef typename cplx_t<T>::type C;
     static constexpr int CT = (sizeof(T) == 8) ? 4 : 8;    // kx columns per block of the column transforms (64 B rows)
+    static constexpr int NL = (sizeof(T) == 8) ? 8 : 16;   // kx columns per block of the two-level column transforms
     static T *f(void *p) { return (T *)p; }
+    // threads of a two-level column block: one work item per thread in the longer step
+    static int col_threads(int n1, int n2) { return std::min(256, ((NL * std::max(n1, n2) + 31) / 32) * 32); }
+
+    static int setup_fft2l(dfdm_ctx *c) {
+        const Dims &d = c->d;
+        int rc = DFDM_OK;
+        auto setattr = [&](const void *fn, size_t bytes) {
+            if (rc) return;
+            cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+            if (e != cudaSuccess) rc = fail(DFDM_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+        };
+        c->x2 = with_fft2l(d.Nx / 2, [&](auto n) {
+            constexpr int N = decltype(n)::value;
+            const size_t perline = (size_t)(RowLayout<N>::LDA + RowLayout<N>::LDT) * sizeof(C);
+            c->lx2 = (int)std::max<size_t>(1, std::min<size_t>(64, 73728 / perline));   // <= 72 KB: 3 blocks per SM
+            c->smem_x2 = (size_t)c->lx2 * perline;
+            c->smem_xi2 = (size_t)c->lx2 * RowLayout<N>::LDT * sizeof(C);
+            setattr((const void *)k_fwd_x2<T, true, N>, c->smem_x2);
+            setattr((const void *)k_fwd_x2<T, false, N>, c->smem_x2);
+            setattr((const void *)k_inv_x2<T, N>, c->smem_xi2);
+        });
+        c->z2 = with_fft2l(d.Nz, [&](auto n) {
+            constexpr int N = decltype(n)::value;
+            c->smem_z2 = (size_t)N * NL * sizeof(C);
+            c->thr_z2 = col_threads(Split<N>::N1, Split<N>::N2);
+            setattr((const void *)k_col2<T, 0, NL, N>, c->smem_z2);
+            setattr((const void *)k_col2<T, 1, NL, N>, c->smem_z2);
+        });
+        c->y2 = d.yper && with_fft2l(d.Ny, [&](auto n) {
+            constexpr int N = decltype(n)::value;
+            c->smem_y2 = (size_t)2 * N * NL * sizeof(C);
+            c->thr_y2 = col_threads(Split<N>::N1, Split<N>::N2);
+            setattr((const void *)k_col2<T, 2, NL, N>, c->smem_y2);
+        });
+        return rc;
+    }
+
+    // div u* (from_div) or the real field src, and the forward real-to-complex x transform into the spectrum
+    static int fwd_x(dfdm_ctx *c, bool from_div, const T *src) {
+        const Dims &d = c->d;
+        cudaStream_t st = c->stream;
+        const long long lines = (long long)d.Ny * d.Nz;
+        if (c->x2) {
+            const int nb = (int)((lines + c->lx2 - 1) / c->lx2);
+            with_fft2l(d.Nx / 2, [&](auto n) {
+                constexpr int N = decltype(n)::value;
+                if (from_div)
+                    k_fwd_x2<T, true, N><<<nb, 256, c->smem_x2, st>>>(poisson_args<T>(c), c->lx2, f(c->us), f(c->vs), f(c->wsf),
+                                                                       nullptr, (C *)c->spec, (const C *)c->tw_x, (const C *)c->twr_x);
+                else
+                    k_fwd_x2<T, false, N><<<nb, 256, c->smem_x2, st>>>(poisson_args<T>(c), c->lx2, nullptr, nullptr, nullptr,
+                                                                        src, (C *)c->spec, (const C *)c->tw_x, (const C *)c->twr_x);
+            });
+        } else {
+            const int nb = (int)((lines + c->lx - 1) / c->lx);
+            if (from_div)
+                k_fwd_x<T, true><<<nb, 256, c->smem_x, st>>>(poisson_args<T>(c), c->lx, f(c->us), f(c->vs), f(c->wsf), nullptr,
+                                                             (C *)c->spec, c->plan_x, (const C *)c->tw_x, (const C *)c->twr_x);
+            else
+                k_fwd_x<T, false><<<nb, 256, c->smem_x, st>>>(poisson_args<T>(c), c->lx, nullptr, nullptr, nullptr, src,
+                                                              (C *)c->spec, c->plan_x, (const C *)c->tw_x, (const C *)c->twr_x);
+        }
+        CKL();
+        return DFDM_OK;
+    }
 
     static int setup_kernels(dfdm_ctx *c) {
         const Dims &d = c->d;
@@ -267,14 +339,17 @@ template <typename T> struct Impl {
         c->kc_stage = choose_kc(d, occ, nsm);
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tiled<T, false, TILE_X, TILE_Y, 1>, TILE_X * TILE_Y, 0));
         c->kc_sgs = choose_kc(d, occ, nsm);
-        return DFDM_OK;
+        return setup_fft2l(c);
     }
 
-    // FP32-mixed stage 3 carries the increment du = u* - uo through the projection: div(du) has no FP32
-    // cancellation, so the saved pressure P = phi/(dt*3/4) does not inherit the O(eps |u| dx / dt) noise that the
-    // rounding of the stored velocity would otherwise put into phi.  Stages 1-2 and the FP64 form keep the
-    // reference's u* = uo + du exactly.
-    static bool incr_form(const dfdm_ctx *c, int s) { (void)c; (void)s; return false; }
+    // FP32-mixed stage 3 carries the increment du = u* - uo through the Poisson solve once the resident velocity
+    // is the output of a full step (so div uo vanishes up to the rounding of its storage).  Solving for div(du)
+    // alone keeps that rounding noise, amplified by dx/dt, out of the saved pressure P = phi/(dt*3/4); the
+    // correction forms u = uo + du - grad(phi).  Right after set_state (a field that need not be solenoidal), in
+    // the unit entry points and in the FP64 form, u* = uo + du is projected as the reference does.
+    static bool incr_form(const dfdm_ctx *c, int s) {
+        return sizeof(T) == 4 && s == 3 && c->projected && !c->unit_projection;
+    }
 
     static int stage_kernel(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
         const Dims &d = c->d;
@@ -331,25 +406,39 @@ template <typename T> struct Impl {
             sc.incr = incr_form(c, s);
             return stage_kernel(c, sc, nullptr);
         }
-        case 2: {   // div + forward x
-            long long lines = (long long)d.Ny * d.Nz;
-            int nb = (int)((lines + c->lx - 1) / c->lx);
-            k_fwd_x<T, true><<<nb, 256, c->smem_x, st>>>(poisson_args<T>(c), c->lx, f(c->us), f(c->vs), f(c->wsf), nullptr,
-                                                         (C *)c->spec, c->plan_x, (const C *)c->tw_x, (const C *)c->twr_x);
-            CKL();
-            return DFDM_OK;
-        }
+        case 2:   // div + forward x
+            return fwd_x(c, true, nullptr);
         case 3: case 5: {   // z transforms
-            dim3 g((d.Nxc + c->tzx - 1) / c->tzx, d.Ny);
-            if (which == 3)
-                k_col_fft<T, 0, CT><<<g, 256, c->smem_z, st>>>(d, (C *)c->spec, c->plan_z, (const C *)c->tw_z, c->d_kxx, c->d_kyy, c->d_kzz);
-            else
-                k_col_fft<T, 1, CT><<<g, 256, c->smem_z, st>>>(d, (C *)c->spec, c->plan_z, (const C *)c->tw_z, c->d_kxx, c->d_kyy, c->d_kzz);
+            if (c->z2) {
+                dim3 g((d.Nxc + NL - 1) / NL, d.Ny);
+                with_fft2l(d.Nz, [&](auto n) {
+                    constexpr int N = decltype(n)::value;
+                    if (which == 3)
+                        k_col2<T, 0, NL, N><<<g, c->thr_z2, c->smem_z2, st>>>(d, (C *)c->spec, (const C *)c->tw_z, c->d_kxx,
+                                                                              c->d_kyy, c->d_kzz);
+                    else
+                        k_col2<T, 1, NL, N><<<g, c->thr_z2, c->smem_z2, st>>>(d, (C *)c->spec, (const C *)c->tw_z, c->d_kxx,
+                                                                              c->d_kyy, c->d_kzz);
+                });
+            } else {
+                dim3 g((d.Nxc + c->tzx - 1) / c->tzx, d.Ny);
+                if (which == 3)
+                    k_col_fft<T, 0, CT><<<g, 256, c->smem_z, st>>>(d, (C *)c->spec, c->plan_z, (const C *)c->tw_z, c->d_kxx, c->d_kyy, c->d_kzz);
+                else
+                    k_col_fft<T, 1, CT><<<g, 256, c->smem_z, st>>>(d, (C *)c->spec, c->plan_z, (const C *)c->tw_z, c->d_kxx, c->d_kyy, c->d_kzz);
+            }
             CKL();
             return DFDM_OK;
         }
         case 4: {   // y solve
-            if (d.yper) {
+            if (d.yper && c->y2) {
+                dim3 g((d.Nxc + NL - 1) / NL, d.Nz);
+                with_fft2l(d.Ny, [&](auto n) {
+                    constexpr int N = decltype(n)::value;
+                    k_col2<T, 2, NL, N><<<g, c->thr_y2, c->smem_y2, st>>>(d, (C *)c->spec, (const C *)c->tw_y, c->d_kxx,
+                                                                          c->d_kyy, c->d_kzz);
+                });
+            } else if (d.yper) {
                 dim3 g((d.Nxc + c->tzx - 1) / c->tzx, d.Nz);
                 k_col_fft<T, 2, CT><<<g, 256, c->smem_y, st>>>(d, (C *)c->spec, c->plan_y, (const C *)c->tw_y, c->d_kxx, c->d_kyy, c->d_kzz);
             } else {
@@ -361,18 +450,29 @@ template <typename T> struct Impl {
         }
         case 6: {   // inverse x
             long long lines = (long long)d.Ny * d.Nz;
-            int nb = (int)((lines + c->lx - 1) / c->lx);
-            k_inv_x<T><<<nb, 256, c->smem_x, st>>>(poisson_args<T>(c), c->lx, (const C *)c->spec, f(c->phi), c->plan_x,
-                                                   (const C *)c->tw_x, (const C *)c->twr_x);
+            if (c->x2) {
+                int nb = (int)((lines + c->lx2 - 1) / c->lx2);
+                with_fft2l(d.Nx / 2, [&](auto n) {
+                    constexpr int N = decltype(n)::value;
+                    k_inv_x2<T, N><<<nb, 256, c->smem_xi2, st>>>(poisson_args<T>(c), c->lx2, (const C *)c->spec, f(c->phi),
+                                                                  (const C *)c->tw_x, (const C *)c->twr_x);
+                });
+            } else {
+                int nb = (int)((lines + c->lx - 1) / c->lx);
+                k_inv_x<T><<<nb, 256, c->smem_x, st>>>(poisson_args<T>(c), c->lx, (const C *)c->spec, f(c->phi), c->plan_x,
+                                                       (const C *)c->tw_x, (const C *)c->twr_x);
+            }
             CKL();
             return DFDM_OK;
         }
         case 7: {   // correction (+ P at stage 3)
             bool inc = incr_form(c, s);
-            if (d.Nx % 4 == 0 && !inc) {
+            if (d.Nx % 4 == 0) {
                 dim3 g((d.Nx / 4 + 63) / 64, (d.Ny + 3) / 4, d.Nz);
                 k_correct4<T><<<g, dim3(64, 4, 1), 0, st>>>(poisson_args<T>(c), f(c->phi), f(c->us), f(c->vs), f(c->wsf),
-                                                            f(c->u), f(c->v), f(c->w), s == 3 ? f(c->p) : nullptr);
+                                                            f(c->u), f(c->v), f(c->w), s == 3 ? f(c->p) : nullptr,
+                                                            inc ? f(c->uo) : nullptr, inc ? f(c->vo) : nullptr,
+                                                            inc ? f(c->wo) : nullptr);
             } else {
                 k_correct<T><<<cell_grid(d), CELL_BLOCK, 0, st>>>(poisson_args<T>(c), f(c->phi), f(c->us), f(c->vs), f(c->wsf),
                                                                   f(c->u), f(c->v), f(c->w), s == 3 ? f(c->p) : nullptr,
@@ -811,6 +911,7 @@ int dfdm_set_state(dfdm_ctx *c, const double *U, const double *V, const double *
     if ((rc = put_field(c, FK_V, c->v, V, c->nxg, c->ny, c->nzg))) return rc;
     if ((rc = put_field(c, FK_W, c->w, W, c->nxg, c->nyg, c->nz))) return rc;
     if (P && (rc = put_field(c, FK_P, c->p, P, c->nxg, c->nyg, c->nzg))) return rc;
+    c->projected = false;
     CK(cudaStreamSynchronize(c->stream));
     return DFDM_OK;
 }
@@ -863,7 +964,8 @@ int dfdm_get_time(dfdm_ctx *c, double *t) {
 static int step_n(dfdm_ctx *c, int nsteps) {
     for (int n = 0; n < nsteps; ++n) {
         double to = c->t;
-        bool can_graph = c->graphs && (c->wm_filter_mode != 1 || !c->wm || c->wmf_seeded);
+        // the captured step is the steady one: filter seeded and (FP32-mixed) increment form at stage 3
+        bool can_graph = c->graphs && c->projected && (c->wm_filter_mode != 1 || !c->wm || c->wmf_seeded);
         if (can_graph) {
             if (!c->gexec) {
                 CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -887,6 +989,7 @@ static int step_n(dfdm_ctx *c, int nsteps) {
             if (rc) return rc;
         }
         c->t = to + 1.0 * c->prm.dt;   // t = to + rk_t(3)*dt
+        c->projected = true;
     }
     return DFDM_OK;
 }
@@ -1021,12 +1124,8 @@ int dfdm_solve_poisson(dfdm_ctx *c, const double *rhs_in, double *phi_out) {
         int gb = reduce_grid(d);
         k_unpack_rhs_p<T><<<gb, 256, 0, c->stream>>>(d, n1, n2, c->staging, I::f(c->phi));
         CKL();
-        long long lines = (long long)d.Ny * d.Nz;
-        int nb = (int)((lines + c->lx - 1) / c->lx);
-        k_fwd_x<T, false><<<nb, 256, c->smem_x, c->stream>>>(poisson_args<T>(c), c->lx, nullptr, nullptr, nullptr, I::f(c->phi),
-                                                             (C *)c->spec, c->plan_x, (const C *)c->tw_x, (const C *)c->twr_x);
-        CKL();
         int r2;
+        if ((r2 = I::fwd_x(c, false, I::f(c->phi)))) return r2;
         if ((r2 = I::launch(c, 3, 1))) return r2;
         if ((r2 = I::launch(c, 4, 1))) return r2;
         if ((r2 = I::launch(c, 5, 1))) return r2;
@@ -1098,12 +1197,8 @@ int dfdm_solve_poisson_noalloc(dfdm_ctx *c, const double *rhs_in, double *phi_ou
         int gb = reduce_grid(d);
         k_unpack_rhs_p<T><<<gb, 256, 0, c->stream>>>(d, n1, n2, scratch, I::f(c->phi));
         CKL();
-        long long lines = (long long)d.Ny * d.Nz;
-        int nb = (int)((lines + c->lx - 1) / c->lx);
-        k_fwd_x<T, false><<<nb, 256, c->smem_x, c->stream>>>(poisson_args<T>(c), c->lx, nullptr, nullptr, nullptr, I::f(c->phi),
-                                                             (C *)c->spec, c->plan_x, (const C *)c->tw_x, (const C *)c->twr_x);
-        CKL();
         int r2;
+        if ((r2 = I::fwd_x(c, false, I::f(c->phi)))) return r2;
         if ((r2 = I::launch(c, 3, 1))) return r2;
         if ((r2 = I::launch(c, 4, 1))) return r2;
         if ((r2 = I::launch(c, 5, 1))) return r2;

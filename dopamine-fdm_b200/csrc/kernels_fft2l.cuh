@@ -1,0 +1,244 @@
+// kernels_fft2l.cuh -- the Poisson transforms for lengths with a two-level split (fft_reg.cuh).
+//
+// Same operations, inputs, outputs and rounding points as the Stockham kernels of kernels_poisson.cuh
+// (k_fwd_x, k_col_fft, k_inv_x): only the transform itself is organised differently.  Step 1 of every transform
+// reads its operands straight from global memory (and, in the x kernels, forms them there: the divergence of u*
+// or the packed half-length spectrum), step 2 of the z transforms and of the inverse x transform writes straight
+// to global memory, so a line crosses shared memory once (twice for the forward x transform, whose real-to-
+// complex unpacking pairs elements k and M-k).
+#pragma once
+
+#include "fft_reg.cuh"
+#include "kernels_poisson.cuh"
+
+namespace dfdm {
+
+// ---- div u* (or a real field) + forward real-to-complex x transform, line length Nx = 2M ----------------------
+template <typename T, bool FROM_DIV, int M>
+__global__ void __launch_bounds__(256) k_fwd_x2(PoissonArgs<T> a, int lx, const T *__restrict__ U, const T *__restrict__ V,
+                                                const T *__restrict__ W, const T *__restrict__ src,
+                                                typename cplx_t<T>::type *__restrict__ spec,
+                                                const typename cplx_t<T>::type *__restrict__ tw,
+                                                const typename cplx_t<T>::type *__restrict__ twr) {
+    typedef typename cplx_t<T>::type C;
+    typedef Arith<T> A;
+    constexpr int N1 = Split<M>::N1, N2 = Split<M>::N2, Nx = 2 * M;
+    constexpr int LDA = RowLayout<M>::LDA, LDT = RowLayout<M>::LDT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *bt = (C *)smem_raw, *ba = bt + lx * LDT;
+    const Dims &d = a.d;
+    const int Ny = d.Ny, Nz = d.Nz, plane = Nx * Ny;
+    const int line0 = blockIdx.x * lx;
+    const int nl = min(lx, Ny * Nz - line0);
+    for (int b = threadIdx.x; b < nl * N2; b += blockDim.x) {
+        const int ll = b / N2, n2 = b - ll * N2;
+        const int line = line0 + ll;
+        C v[N1];
+        if (FROM_DIV) {
+            const int k = (int)fdiv((unsigned)line, a.fNy), j = line - k * Ny;
+            const int ob = k * plane + j * Nx;
+            const int dkm = (k == 0) ? (Nz - 1) * plane : -plane;
+            const int djm = (j > 0) ? -Nx : (Ny - 1) * Nx;
+            const bool vzero = (j == 0) && !d.yper;
+            const T inv_dyj = A::inv(a.my.dc, a.my.idc, j), inv_dzk = A::inv(a.mz.dc, a.mz.idc, k);
+#pragma unroll
+            for (int n1 = 0; n1 < N1; ++n1) {
+                const int i = 2 * (n1 * N2 + n2);
+                const int o = ob + i;
+                const T um = __ldg(U + (i == 0 ? ob + Nx - 1 : o - 1)), u0 = __ldg(U + o), u1 = __ldg(U + o + 1);
+                const T v0 = __ldg(V + o), v1 = __ldg(V + o + 1);
+                const T vm0 = vzero ? T(0) : __ldg(V + o + djm), vm1 = vzero ? T(0) : __ldg(V + o + 1 + djm);
+                const T w0 = __ldg(W + o), w1 = __ldg(W + o + 1), wm0 = __ldg(W + o + dkm), wm1 = __ldg(W + o + 1 + dkm);
+                v[n1].x = (u0 - um) * a.inv_dx + (v0 - vm0) * inv_dyj + (w0 - wm0) * inv_dzk;
+                v[n1].y = (u1 - u0) * a.inv_dx + (v1 - vm1) * inv_dyj + (w1 - wm1) * inv_dzk;
+            }
+        } else {
+            const T *s = src + (size_t)line * Nx;
+#pragma unroll
+            for (int n1 = 0; n1 < N1; ++n1) {
+                const int i = 2 * (n1 * N2 + n2);
+                v[n1].x = s[i];
+                v[n1].y = s[i + 1];
+            }
+        }
+        row_step1<T, false, M>(v, bt + ll * LDT, n2, tw);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < nl * N1; b += blockDim.x) {
+        const int ll = b / N1, k1 = b - ll * N1;
+        C v[N2];
+        const C *tl = bt + ll * LDT + k1 * (N2 + 1);
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) v[n2] = tl[n2];
+        Codelet<T, false, N2>::run(v);
+        C *al = ba + ll * LDA;
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) al[k1 + N1 * k2] = v[k2];
+    }
+    __syncthreads();
+    const int Nxc = d.Nxc;
+    for (int e = threadIdx.x; e < nl * (M + 1); e += blockDim.x) {
+        const int ll = e / (M + 1), kx = e - ll * (M + 1);
+        const C *res = ba + ll * LDA;
+        C Zk = res[kx == M ? 0 : kx];
+        C Zm = res[kx == 0 ? 0 : M - kx];
+        T Er = T(0.5) * (Zk.x + Zm.x), Ei = T(0.5) * (Zk.y - Zm.y);
+        T Dr = T(0.5) * (Zk.x - Zm.x), Di = T(0.5) * (Zk.y + Zm.y);
+        T Or = Di, Oi = -Dr;
+        C w = __ldg(twr + kx);
+        C X;
+        X.x = Er + (w.x * Or - w.y * Oi);
+        X.y = Ei + (w.x * Oi + w.y * Or);
+        spec[(size_t)(line0 + ll) * Nxc + kx] = X;
+    }
+}
+
+// ---- inverse complex-to-real x transform, writes phi = x / (nxp*nzp) -----------------------------------------
+template <typename T> struct Vec2;
+template <> struct Vec2<float> { typedef float2 type; };
+template <> struct Vec2<double> { typedef double2 type; };
+
+template <typename T, int M>
+__global__ void __launch_bounds__(256) k_inv_x2(PoissonArgs<T> a, int lx, const typename cplx_t<T>::type *__restrict__ spec,
+                                                T *__restrict__ phi, const typename cplx_t<T>::type *__restrict__ tw,
+                                                const typename cplx_t<T>::type *__restrict__ twr) {
+    typedef typename cplx_t<T>::type C;
+    typedef typename Vec2<T>::type T2;
+    constexpr int N1 = Split<M>::N1, N2 = Split<M>::N2, Nx = 2 * M;
+    constexpr int LDT = RowLayout<M>::LDT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *bt = (C *)smem_raw;
+    const Dims &d = a.d;
+    const int Nxc = d.Nxc;
+    const int line0 = blockIdx.x * lx;
+    const int nl = min(lx, d.Ny * d.Nz - line0);
+    for (int b = threadIdx.x; b < nl * N2; b += blockDim.x) {
+        const int ll = b / N2, n2 = b - ll * N2;
+        const C *row = spec + (size_t)(line0 + ll) * Nxc;
+        C v[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) {
+            const int kx = n1 * N2 + n2;
+            C X = row[kx], Xm = row[M - kx];
+            if (kx == 0) { X.y = T(0); Xm.y = T(0); }
+            T E2r = X.x + Xm.x, E2i = X.y - Xm.y;
+            T D2r = X.x - Xm.x, D2i = X.y + Xm.y;
+            C w = __ldg(twr + kx);
+            T O2r = D2r * w.x + D2i * w.y, O2i = D2i * w.x - D2r * w.y;
+            v[n1].x = E2r - O2i;
+            v[n1].y = E2i + O2r;
+        }
+        row_step1<T, true, M>(v, bt + ll * LDT, n2, tw);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < nl * N1; b += blockDim.x) {
+        const int ll = b / N1, k1 = b - ll * N1;
+        C v[N2];
+        const C *tl = bt + ll * LDT + k1 * (N2 + 1);
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) v[n2] = tl[n2];
+        Codelet<T, true, N2>::run(v);
+        T2 *out = reinterpret_cast<T2 *>(phi + (size_t)(line0 + ll) * Nx);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+            T2 o;
+            if (sizeof(T) == 8) { o.x = (T)((double)v[k2].x / a.norm); o.y = (T)((double)v[k2].y / a.norm); }
+            else { o.x = v[k2].x * (T)(1.0 / a.norm); o.y = v[k2].y * (T)(1.0 / a.norm); }
+            out[k1 + N1 * k2] = o;
+        }
+    }
+}
+
+// ---- z transforms (MODE 0 forward, 1 inverse) and the periodic-y solve (MODE 2) on tiles of NL kx columns ----
+// MODE 2: forward FFT along y, division by kxx+kyy+kzz with the (0,0,0) mode set to zero, inverse FFT, division
+// by nyp (src/projection.f90:246-273).
+template <typename T, int MODE, int NL, int L>
+__global__ void __launch_bounds__(256) k_col2(Dims d, typename cplx_t<T>::type *__restrict__ spec,
+                                              const typename cplx_t<T>::type *__restrict__ tw,
+                                              const double *__restrict__ kxx, const double *__restrict__ kyy,
+                                              const double *__restrict__ kzz) {
+    typedef typename cplx_t<T>::type C;
+    constexpr int N1 = Split<L>::N1, N2 = Split<L>::N2;
+    constexpr bool INV1 = (MODE == 1);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *t = (C *)smem_raw;          // step-1 outputs, [e*NL + c]
+    C *nat = t + L * NL;           // MODE 2: natural-order spectrum between the two transforms
+    const int kx0 = blockIdx.x * NL;
+    const int other = blockIdx.y;
+    const int Nxc = d.Nxc;
+    size_t base;
+    int rowstride;
+    if (MODE == 2) { base = (size_t)other * d.Ny * Nxc; rowstride = Nxc; }
+    else { base = (size_t)other * Nxc; rowstride = d.Ny * Nxc; }
+    C *colbase = spec + base + kx0;
+    for (int b = threadIdx.x; b < NL * N2; b += blockDim.x) {
+        const int c = b % NL, n2 = b / NL;
+        const bool ok = kx0 + c < Nxc;
+        C v[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) v[n1] = ok ? colbase[(size_t)(n1 * N2 + n2) * rowstride + c] : mkc<T>(T(0), T(0));
+        col_step1<T, INV1, L, NL>(v, t, c, n2, tw);
+    }
+    __syncthreads();
+    if (MODE != 2) {
+        for (int b = threadIdx.x; b < NL * N1; b += blockDim.x) {
+            const int c = b % NL, k1 = b / NL;
+            C v[N2];
+#pragma unroll
+            for (int n2 = 0; n2 < N2; ++n2) v[n2] = t[(k1 * N2 + n2) * NL + c];
+            Codelet<T, INV1, N2>::run(v);
+            if (kx0 + c < Nxc) {
+#pragma unroll
+                for (int k2 = 0; k2 < N2; ++k2) colbase[(size_t)(k1 + N1 * k2) * rowstride + c] = v[k2];
+            }
+        }
+        return;
+    }
+    // MODE 2: finish the forward transform, divide, write natural order
+    const int kz = other;
+    for (int b = threadIdx.x; b < NL * N1; b += blockDim.x) {
+        const int c = b % NL, k1 = b / NL, kx = kx0 + c;
+        C v[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) v[n2] = t[(k1 * N2 + n2) * NL + c];
+        Codelet<T, false, N2>::run(v);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+            const int j = k1 + N1 * k2;
+            C x = v[k2];
+            if (kx < Nxc) {
+                double wavenum_sum = kxx[kx] + kyy[j] + kzz[kz];
+                if (kx == 0 && j == 0 && kz == 0) { x.x = T(0); x.y = T(0); }
+                else { x.x = (T)((double)x.x / wavenum_sum); x.y = (T)((double)x.y / wavenum_sum); }
+            }
+            nat[j * NL + c] = x;
+        }
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < NL * N2; b += blockDim.x) {
+        const int c = b % NL, n2 = b / NL;
+        C v[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) v[n1] = nat[(n1 * N2 + n2) * NL + c];
+        col_step1<T, true, L, NL>(v, t, c, n2, tw);
+    }
+    __syncthreads();
+    const double nyp = (double)L;
+    for (int b = threadIdx.x; b < NL * N1; b += blockDim.x) {
+        const int c = b % NL, k1 = b / NL;
+        C v[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) v[n2] = t[(k1 * N2 + n2) * NL + c];
+        Codelet<T, true, N2>::run(v);
+        if (kx0 + c < Nxc) {
+#pragma unroll
+            for (int k2 = 0; k2 < N2; ++k2) {
+                C x = v[k2];
+                x.x = (T)((double)x.x / nyp); x.y = (T)((double)x.y / nyp);
+                colbase[(size_t)(k1 + N1 * k2) * rowstride + c] = x;
+            }
+        }
+    }
+}
+
+}  // namespace dfdm

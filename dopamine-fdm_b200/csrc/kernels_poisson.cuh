@@ -294,7 +294,8 @@ template <> struct Vec4<double> { typedef double4 type; };
 template <typename T>
 __global__ void __launch_bounds__(256) k_correct4(PoissonArgs<T> a, const T *__restrict__ phi, const T *__restrict__ us,
                                                   const T *__restrict__ vs, const T *__restrict__ ws, T *__restrict__ U,
-                                                  T *__restrict__ V, T *__restrict__ W, T *__restrict__ P) {
+                                                  T *__restrict__ V, T *__restrict__ W, T *__restrict__ P,
+                                                  const T *__restrict__ uo, const T *__restrict__ vo, const T *__restrict__ wo) {
     typedef typename Vec4<T>::type V4;
     typedef Arith<T> A;
     const Dims &d = a.d;
@@ -309,6 +310,11 @@ __global__ void __launch_bounds__(256) k_correct4(PoissonArgs<T> a, const T *__r
     const V4 pz = *reinterpret_cast<const V4 *>(phi + (k == Nz - 1 ? p - (Nz - 1) * plane : p + plane));
     const T idx = a.inv_dx, idz = A::inv(a.mz.df, a.mz.idf, k);
     V4 u = *reinterpret_cast<const V4 *>(us + p), w = *reinterpret_cast<const V4 *>(ws + p);
+    if (uo) {   // increment form: u* = uo + du, rounded as the stage kernel rounds it
+        const V4 bu = *reinterpret_cast<const V4 *>(uo + p), bw = *reinterpret_cast<const V4 *>(wo + p);
+        u.x = bu.x + u.x; u.y = bu.y + u.y; u.z = bu.z + u.z; u.w = bu.w + u.w;
+        w.x = bw.x + w.x; w.y = bw.y + w.y; w.z = bw.z + w.z; w.w = bw.w + w.w;
+    }
     u.x = u.x - (pc.y - pc.x) * idx; u.y = u.y - (pc.z - pc.y) * idx;
     u.z = u.z - (pc.w - pc.z) * idx; u.w = u.w - (pnext - pc.w) * idx;
     w.x = w.x - (pz.x - pc.x) * idz; w.y = w.y - (pz.y - pc.y) * idz;
@@ -319,6 +325,10 @@ __global__ void __launch_bounds__(256) k_correct4(PoissonArgs<T> a, const T *__r
         const V4 py = *reinterpret_cast<const V4 *>(phi + (j == Ny - 1 ? p - (Ny - 1) * Nx : p + Nx));
         const T idy = A::inv(a.my.df, a.my.idf, j);
         V4 v = *reinterpret_cast<const V4 *>(vs + p);
+        if (vo) {
+            const V4 bv = *reinterpret_cast<const V4 *>(vo + p);
+            v.x = bv.x + v.x; v.y = bv.y + v.y; v.z = bv.z + v.z; v.w = bv.w + v.w;
+        }
         v.x = v.x - (py.x - pc.x) * idy; v.y = v.y - (py.y - pc.y) * idy;
         v.z = v.z - (py.z - pc.z) * idy; v.w = v.w - (py.w - pc.w) * idy;
         *reinterpret_cast<V4 *>(V + p) = v;

@@ -380,7 +380,7 @@ struct StageCoef {
     double dt_a11;   // dt*rk_coef(1,1), stage 1
     double dt;       // dt, stages 2 and 3
     double c1, c2;   // rk_coef(s,1) and rk_coef(s,s), stages 2 and 3
-    int incr;        // store the increment du = dt (c1 F1 + c2 rhs) instead of u* = uo + du (FP32-mixed stage 3)
+    int incr;        // store the increment du = dt (c1 F1 + c2 rhs) instead of u* = uo + du; uo is not read
 };
 
 // Shared-memory neighbourhood of one thread: three z-planes (k-1, k, k+1) of each field, each plane a
@@ -523,8 +523,9 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
                 const bool upd = !rhs_only && sc.stage != 1;
                 T ou = T(0), ov = T(0), ow = T(0), fu = T(0), fv = T(0), fw = T(0);
                 if (upd) {   // issue the base-state and F1 loads before the arithmetic
-                    ou = uo[p]; ow = wo[p]; fu = f1u[p]; fw = f1w[p];
-                    if (vrow) { ov = vo[p]; fv = f1v[p]; }
+                    if (!sc.incr) { ou = uo[p]; ow = wo[p]; if (vrow) ov = vo[p]; }
+                    fu = f1u[p]; fw = f1w[p];
+                    if (vrow) fv = f1v[p];
                 }
                 T ru = rhs_u_at<T, LES>(a, q, tau_x, i, j, k);
                 T rw = rhs_w_at<T, LES>(a, q, tau_z, i, j, k);
@@ -538,8 +539,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
                     wo[p] = w0; f1w[p] = rw; wsf[p] = w0 + c * rw;
                     if (vrow) { T v0 = q.V(0, 0, 0); vo[p] = v0; f1v[p] = rv; vs[p] = v0 + c * rv; }
                 } else {
-                    T c1 = (T)sc.c1, c2 = (T)sc.c2, dtt = (T)sc.dt;
-                    if (sc.incr) { ou = T(0); ow = T(0); ov = T(0); }
+                    T c1 = (T)sc.c1, c2 = (T)sc.c2, dtt = (T)sc.dt;   // with sc.incr the base stays zero: du
                     us[p] = ou + dtt * (c1 * fu + c2 * ru);
                     wsf[p] = ow + dtt * (c1 * fw + c2 * rw);
                     if (vrow) vs[p] = ov + dtt * (c1 * fv + c2 * rv);
