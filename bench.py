@@ -49,6 +49,11 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-kernels", action="store_true", help="skip the per-kernel roofline timings")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream measurement")
+    ap.add_argument("--serve-requests", type=int, default=256)
+    ap.add_argument("--serve-rate", type=float, default=4.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--serve-saturated", type=int, default=48,
+                    help="requests of the saturated comparison (all arriving at once vs run alone back to back)")
     return ap.parse_args()
 
 
@@ -191,6 +196,46 @@ def cpu_baseline(c, seconds):
 
 
 # ---------------------------------------------------------------------------------------------------------------
+def serve_bench(args, local, rank, ws, gather):
+    """The serving stream (256 requests, Poisson arrivals at 4/s, FP32-mixed, 150 GB admission budget): p50/p99
+    latency from arrival to the result on the host, and the loop's throughput when saturated against the same
+    requests run alone back to back.  With N ranks each serves requests rank::N of the stream."""
+    from dfdm import serve
+    budget = 150e9
+    ex = serve.GpuExecutor(device=local)
+    serve.Scheduler(ex, budget).run(serve.make_stream(2, 100.0, seed=99, grids=(32,), steps=(10, 10)))   # warm-up
+    reqs = serve.make_stream(args.serve_requests, args.serve_rate, seed=5)[rank::ws]
+    sch = serve.Scheduler(ex, budget)
+    t0 = ex.now()
+    res = sch.run(reqs)
+    wall = ex.now() - t0
+    sub = [serve.Request(r.rid, r.case, r.nsteps, 0.0, r.precision) for r in reqs[:args.serve_saturated]]
+    iso = serve.run_isolated(ex, sub)
+    iso_wall = iso[-1].finished if iso else float("nan")
+    t0 = ex.now()
+    sat = serve.Scheduler(ex, budget).run(sub)
+    sat_wall = ex.now() - t0
+    work_sub = float(sum(r.work for r in sub))
+    parts = gather({"lat": [r.latency for r in res], "work": float(sum(r.work for r in reqs)), "wall": wall,
+                    "iso": work_sub / iso_wall, "sat": work_sub / sat_wall,
+                    "finite": all(r.summary.get("finite", 0.0) == 1.0 for r in res),
+                    "peak_active": sch.peak_active, "peak_bytes": sch.peak_bytes})
+    lat = [x for p in parts for x in p["lat"]]
+    iso_thr = sum(p["iso"] for p in parts)
+    sat_thr = sum(p["sat"] for p in parts)
+    return {"requests": len(lat), "arrival_rate_per_s": args.serve_rate, "p50_latency_s": serve.percentile(lat, 50),
+            "p99_latency_s": serve.percentile(lat, 99), "max_latency_s": max(lat) if lat else None,
+            "stream_wall_s": max(p["wall"] for p in parts),
+            "stream_throughput_cell_steps_per_s": sum(p["work"] for p in parts) / max(p["wall"] for p in parts),
+            "saturated_requests": min(args.serve_saturated, len(reqs)) * len(parts),
+            "saturated_throughput_cell_steps_per_s": sat_thr, "isolated_throughput_cell_steps_per_s": iso_thr,
+            "saturated_over_isolated": sat_thr / iso_thr, "all_finite": all(p["finite"] for p in parts),
+            "peak_active": max(p["peak_active"] for p in parts),
+            "peak_admitted_bytes": max(p["peak_bytes"] for p in parts), "admission_budget_bytes": budget,
+            "precision": "fp32-mixed", "stream": "seed 5: 50% Taylor-Green (Re log-uniform 400-3200), 50% "
+            "Re_tau=180 channel domain; N^3 cells, N in {32,48,64,96,128}; 200-2000 steps"}
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
@@ -345,6 +390,16 @@ def main():
                       "d2h_bytes_per_step": bo, "steps": ne,
                       "path": "dfdm_set_state(U,V,W) + dfdm_compute_time_step_rk3(1) + dfdm_get_state(U,V,W,P) "
                               "per step, FP64 ghosted host arrays in pinned memory"}
+
+    # ---- serving stream ----
+    if not args.no_serve:
+        def gather(obj):
+            if ws == 1:
+                return [obj]
+            parts = [None] * ws
+            dist.all_gather_object(parts, obj)
+            return parts
+        out["serve"] = serve_bench(args, local, rank, ws, gather)
 
     # ---- CPU baseline: the FP64 restatement on the host cores (rank 0 at N = 1 only) ----
     if rank == 0 and ws == 1 and not args.no_cpu:

@@ -1,0 +1,305 @@
+"""Request loop for independent simulations on one GPU (continuous batching of whole cases).
+
+A request is one case (grid, Reynolds number, initial-condition seed) and a step count.  Requests arrive over
+time.  They are admitted in arrival order as soon as their device footprint (dfdm_footprint_bytes) fits in the
+admission budget, and each admitted case stays resident in its own context on its own CUDA stream.  The loop
+advances every active case by chunks of whole steps (one CUDA-graph replay per step).  Chunks of different cases
+are enqueued on different streams, so their kernels overlap on the device.  A case that finishes returns its final
+state to the host and gives its memory back to the budget, and the next waiting request takes its place.
+
+The scheduling logic (Scheduler) is independent of the device: Scheduler.run drives an executor object, which the
+GPU path implements with dfdm contexts (GpuExecutor) and the CPU tests implement with a simulated clock.
+
+The synthetic request stream (make_stream) draws, from one seed, Poisson arrivals at a given rate.  Per request it
+draws a case type (Taylor-Green or Re_tau = 180 channel, 50/50), a cubic grid N^3 with N in {32, 48, 64, 96, 128}
+(channel: 4pi x 2 x 4pi/3, tanh 2.0), Re log-uniform in [400, 3200] for Taylor-Green, an initial-condition seed and
+a step count uniform in [200, 2000].
+"""
+from __future__ import annotations
+
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from . import cases
+from .cases import Case
+
+GRIDS = (32, 48, 64, 96, 128)
+
+
+@dataclass
+class Request:
+    rid: int
+    case: Case
+    nsteps: int
+    arrival: float          # seconds after the stream starts
+    precision: str = "fp32"
+
+    @property
+    def cells(self) -> int:
+        return self.case.n_cells
+
+    @property
+    def work(self) -> int:  # cell-steps
+        return self.cells * self.nsteps
+
+
+@dataclass
+class Result:
+    rid: int
+    arrival: float
+    admitted: float
+    finished: float
+    nsteps: int
+    cells: int
+    state: Optional[tuple] = None
+    summary: Dict[str, float] = field(default_factory=dict)
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def serve_case(kind: str, N: int, Re: float, seed: int) -> Case:
+    """One request's case: Taylor-Green in [0, 2pi]^3 or the Re_tau = 180 channel domain, on N^3 cells."""
+    if kind == "tgv":
+        c = cases.tgv(N=N, Re=Re, dt=1e-3, name=f"tgv{N}_Re{Re:.0f}")
+        c.seed = seed
+        return c
+    c = cases.channel(N, N, N, 4.0 * math.pi, 4.0 * math.pi / 3.0, 2.0, 180.0, 15.6, 1e-3, seed, 0, f"chan{N}")
+    return c
+
+
+def make_stream(n: int = 256, rate: float = 4.0, seed: int = 5, grids=GRIDS, steps=(200, 2000),
+                precision: str = "fp32") -> List[Request]:
+    """The synthetic request stream: Poisson arrivals at `rate` per second, all draws from PCG64(seed)."""
+    g = np.random.Generator(np.random.PCG64(seed))
+    t = 0.0
+    out = []
+    for rid in range(n):
+        t += g.exponential(1.0 / rate)
+        kind = "tgv" if g.random() < 0.5 else "chan"
+        N = int(grids[g.integers(0, len(grids))])
+        Re = float(math.exp(g.uniform(math.log(400.0), math.log(3200.0))))
+        ic_seed = int(g.integers(0, 2**31 - 1))
+        nsteps = int(g.integers(steps[0], steps[1] + 1))
+        out.append(Request(rid, serve_case(kind, N, Re, ic_seed), nsteps, t, precision))
+    return out
+
+
+def percentile(xs: List[float], q: float) -> float:
+    """Nearest-rank percentile (q in [0, 100])."""
+    if not xs:
+        return float("nan")
+    s = sorted(xs)
+    k = max(0, min(len(s) - 1, int(math.ceil(q / 100.0 * len(s))) - 1))
+    return s[k]
+
+
+class Scheduler:
+    """FIFO admission by device footprint, round-robin chunked stepping of the admitted cases.
+
+    executor protocol:
+      footprint(req) -> bytes            prepare(req)        (called at arrival; may start work in the background)
+      start(req) -> handle               can_enqueue(handle) -> bool  (False while the case is still being set up)
+      enqueue(handle, nsteps)            ready(handle) -> bool
+      finish(handle, req, keep_state) -> (state, summary)
+      reclaim() -> None                  (release the memory of finished cases; may wait for the device)
+      now() -> seconds                   idle(seconds or None)        (wait for device progress or an arrival)
+      defers_free: bool                  (finished cases hold their memory until reclaim())
+    """
+
+    def __init__(self, executor, budget_bytes: float, chunk_cell_steps: float = 2.5e7, max_active: int = 64,
+                 keep_state: bool = False):
+        self.ex = executor
+        self.budget = float(budget_bytes)
+        self.chunk_cell_steps = float(chunk_cell_steps)
+        self.max_active = int(max_active)
+        self.keep_state = keep_state
+        self.peak_bytes = 0.0
+        self.peak_active = 0
+        self.reclaims = 0
+
+    def chunk(self, req: Request, done: int) -> int:
+        k = int(max(1, round(self.chunk_cell_steps / max(1, req.cells))))
+        return min(k, req.nsteps - done)
+
+    def run(self, requests: List[Request], t0: Optional[float] = None) -> List[Result]:
+        ex = self.ex
+        defers = getattr(ex, "defers_free", False)
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        waiting: deque = deque()
+        active: List[dict] = []
+        results: List[Result] = []
+        used = 0.0       # footprint of admitted, unfinished cases
+        held = 0.0       # footprint of finished cases whose memory is not released yet
+        start = ex.now() if t0 is None else t0
+        while pending or waiting or active:
+            now = ex.now() - start
+            while pending and pending[0].arrival <= now:
+                r = pending.popleft()
+                fp = ex.footprint(r)
+                if fp > self.budget:
+                    raise ValueError(f"request {r.rid} needs {fp} bytes, more than the whole budget")
+                ex.prepare(r)
+                waiting.append((r, fp))
+            # admission: arrival order, head of line waits until its footprint fits
+            while waiting and len(active) < self.max_active:
+                r, fp = waiting[0]
+                if used + held + fp > self.budget and held > 0:
+                    ex.reclaim()
+                    held = 0.0
+                    self.reclaims += 1
+                if used + held + fp > self.budget:
+                    break
+                waiting.popleft()
+                used += fp
+                h = ex.start(r)
+                active.append({"req": r, "h": h, "fp": fp, "done": 0, "inflight": 0, "admitted": ex.now() - start})
+            self.peak_bytes = max(self.peak_bytes, used + held)
+            self.peak_active = max(self.peak_active, len(active))
+            progressed = False
+            for a in list(active):
+                r = a["req"]
+                if a["inflight"] and not ex.ready(a["h"]):
+                    continue
+                if not a["inflight"] and not ex.can_enqueue(a["h"]):
+                    continue
+                a["done"] += a["inflight"]
+                a["inflight"] = 0
+                if a["done"] >= r.nsteps:
+                    state, summary = ex.finish(a["h"], r, self.keep_state)
+                    results.append(Result(r.rid, r.arrival, a["admitted"], ex.now() - start, r.nsteps, r.cells,
+                                          state, summary))
+                    used -= a["fp"]
+                    if defers:
+                        held += a["fp"]
+                    active.remove(a)
+                    progressed = True
+                    continue
+                k = self.chunk(r, a["done"])
+                ex.enqueue(a["h"], k)
+                a["inflight"] = k
+                progressed = True
+            if not progressed:
+                nxt = pending[0].arrival - (ex.now() - start) if pending else None
+                ex.idle(nxt)
+        ex.reclaim()
+        return sorted(results, key=lambda x: x.rid)
+
+
+def summarize(results: List[Result], wall: float) -> Dict[str, float]:
+    lat = [r.latency for r in results]
+    work = sum(r.cells * r.nsteps for r in results)
+    return {"requests": len(results), "p50_latency_s": percentile(lat, 50), "p99_latency_s": percentile(lat, 99),
+            "mean_latency_s": float(np.mean(lat)) if lat else float("nan"), "cell_steps": float(work),
+            "wall_s": wall, "throughput_cell_steps_per_s": work / wall if wall > 0 else float("nan")}
+
+
+class GpuExecutor:
+    """Executor on one GPU: one dfdm context (CUDA-graph steps) and one CUDA stream per admitted request.
+
+    The host-side initial condition of a request is built on worker threads from the moment it arrives (no device
+    memory is touched before admission); at admission another worker creates the context and uploads the state, so
+    the loop keeps feeding the device meanwhile.  Finished contexts are kept until reclaim(): releasing device
+    memory waits for the whole device, which would stall every other case.
+    """
+
+    defers_free = True
+
+    def __init__(self, device: int = 0, graphs: bool = True, workers: int = 4):
+        import torch
+        from concurrent.futures import ThreadPoolExecutor
+        from .native import Solver, footprint_bytes
+        self.torch = torch
+        self.Solver = Solver
+        self._footprint = footprint_bytes
+        self.device = device
+        self.graphs = graphs
+        self.ic_pool = ThreadPoolExecutor(max_workers=workers)
+        self.setup_pool = ThreadPoolExecutor(max_workers=workers)
+        self.ics: Dict[int, object] = {}
+        self.finished: List = []
+        self.streams: List = []     # CUDA streams of released contexts, reused
+
+    def now(self) -> float:
+        return time.perf_counter()
+
+    def idle(self, until_next_arrival: Optional[float]) -> None:
+        time.sleep(min(2e-4, max(0.0, until_next_arrival)) if until_next_arrival is not None else 2e-4)
+
+    def footprint(self, req: Request) -> int:
+        return self._footprint(req.case, req.precision)
+
+    def prepare(self, req: Request) -> None:
+        self.ics[req.rid] = self.ic_pool.submit(cases.initial_condition, req.case)
+
+    def _setup(self, req: Request, ic, st):
+        self.torch.cuda.set_device(self.device)
+        s = self.Solver(req.case, req.precision, graphs=self.graphs, stream=st.cuda_stream)
+        s.set_state(*ic.result())
+        return s
+
+    def start(self, req: Request):
+        if req.rid not in self.ics:
+            self.prepare(req)
+        ic = self.ics.pop(req.rid)
+        st = self.streams.pop() if self.streams else self.torch.cuda.Stream(device=self.device)
+        return {"fut": self.setup_pool.submit(self._setup, req, ic, st), "s": None, "st": st,
+                "ev": self.torch.cuda.Event()}
+
+    def can_enqueue(self, h) -> bool:
+        if h["s"] is None:
+            if not h["fut"].done():
+                return False
+            h["s"] = h["fut"].result()
+        return True
+
+    def enqueue(self, h, nsteps: int) -> None:
+        h["s"].compute_time_step_RK3_async(nsteps)
+        h["ev"].record(h["st"])
+
+    def ready(self, h) -> bool:
+        return h["ev"].query()
+
+    def finish(self, h, req: Request, keep_state: bool):
+        s = h["s"]
+        summary = {"t": s.t, "kinetic_energy": s.kinetic_energy()}
+        try:
+            s.check_finite()
+            summary["finite"] = 1.0
+        except Exception:
+            summary["finite"] = 0.0
+        state = s.get_state() if keep_state else None
+        self.finished.append((s, h["st"]))
+        return state, summary
+
+    def reclaim(self) -> None:
+        for s, st in self.finished:
+            s.close()
+            self.streams.append(st)
+        self.finished = []
+
+
+def run_isolated(executor, requests: List[Request], keep_state: bool = False) -> List[Result]:
+    """Every request alone, back to back (the isolated-run reference for the loop's throughput): set-up, steps,
+    result, in turn."""
+    out = []
+    t0 = executor.now()
+    for r in requests:
+        a = executor.now() - t0
+        executor.prepare(r)
+        h = executor.start(r)
+        while not executor.can_enqueue(h):
+            executor.idle(None)
+        executor.enqueue(h, r.nsteps)
+        while not executor.ready(h):
+            executor.idle(None)
+        state, summary = executor.finish(h, r, keep_state)
+        out.append(Result(r.rid, a, a, executor.now() - t0, r.nsteps, r.cells, state, summary))
+    executor.reclaim()
+    return out
