@@ -201,39 +201,15 @@ def serve_bench(args, local, rank, ws, gather):
     latency from arrival to the result on the host, and the loop's throughput when saturated against the same
     requests run alone back to back.  With N ranks each serves requests rank::N of the stream."""
     from dfdm import serve
-    budget = 150e9
     ex = serve.GpuExecutor(device=local)
-    serve.Scheduler(ex, budget).run(serve.make_stream(2, 100.0, seed=99, grids=(32,), steps=(10, 10)))   # warm-up
-    reqs = serve.make_stream(args.serve_requests, args.serve_rate, seed=5)[rank::ws]
-    sch = serve.Scheduler(ex, budget)
-    t0 = ex.now()
-    res = sch.run(reqs)
-    wall = ex.now() - t0
-    sub = [serve.Request(r.rid, r.case, r.nsteps, 0.0, r.precision) for r in reqs[:args.serve_saturated]]
-    iso = serve.run_isolated(ex, sub)
-    iso_wall = iso[-1].finished if iso else float("nan")
-    t0 = ex.now()
-    sat = serve.Scheduler(ex, budget).run(sub)
-    sat_wall = ex.now() - t0
-    work_sub = float(sum(r.work for r in sub))
-    parts = gather({"lat": [r.latency for r in res], "work": float(sum(r.work for r in reqs)), "wall": wall,
-                    "iso": work_sub / iso_wall, "sat": work_sub / sat_wall,
-                    "finite": all(r.summary.get("finite", 0.0) == 1.0 for r in res),
-                    "peak_active": sch.peak_active, "peak_bytes": sch.peak_bytes})
-    lat = [x for p in parts for x in p["lat"]]
-    iso_thr = sum(p["iso"] for p in parts)
-    sat_thr = sum(p["sat"] for p in parts)
-    return {"requests": len(lat), "arrival_rate_per_s": args.serve_rate, "p50_latency_s": serve.percentile(lat, 50),
-            "p99_latency_s": serve.percentile(lat, 99), "max_latency_s": max(lat) if lat else None,
-            "stream_wall_s": max(p["wall"] for p in parts),
-            "stream_throughput_cell_steps_per_s": sum(p["work"] for p in parts) / max(p["wall"] for p in parts),
-            "saturated_requests": min(args.serve_saturated, len(reqs)) * len(parts),
-            "saturated_throughput_cell_steps_per_s": sat_thr, "isolated_throughput_cell_steps_per_s": iso_thr,
-            "saturated_over_isolated": sat_thr / iso_thr, "all_finite": all(p["finite"] for p in parts),
-            "peak_active": max(p["peak_active"] for p in parts),
-            "peak_admitted_bytes": max(p["peak_bytes"] for p in parts), "admission_budget_bytes": budget,
-            "precision": "fp32-mixed", "stream": "seed 5: 50% Taylor-Green (Re log-uniform 400-3200), 50% "
-            "Re_tau=180 channel domain; N^3 cells, N in {32,48,64,96,128}; 200-2000 steps"}
+    serve.Scheduler(ex, 150e9).run(serve.make_stream(2, 100.0, seed=99, grids=(32,), steps=(10, 10)))   # warm-up
+    reqs = serve.make_stream(args.serve_requests, args.serve_rate, seed=5)
+    out = serve.measure_stream(ex, reqs, rank, ws, gather, 150e9, args.serve_saturated)
+    out.pop("rids")
+    out.update({"arrival_rate_per_s": args.serve_rate, "precision": "fp32-mixed",
+                "stream": "seed 5: 50% Taylor-Green (Re log-uniform 400-3200), 50% Re_tau=180 channel domain; "
+                          "N^3 cells, N in {32,48,64,96,128}; 200-2000 steps"})
+    return out
 
 
 def main():

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -67,6 +68,9 @@ struct dfdm_ctx {
     double dPdx = 0, dPdz = 0;
     // device memory
     std::vector<void *> allocs;
+    char *arena = nullptr;            // one allocation holding every buffer that dfdm_create makes
+    size_t arena_size = 0, arena_off = 0;
+    bool in_create = false;
     void *u = nullptr, *v = nullptr, *w = nullptr, *uo = nullptr, *vo = nullptr, *wo = nullptr;
     void *f1u = nullptr, *f1v = nullptr, *f1w = nullptr, *us = nullptr, *vs = nullptr, *wsf = nullptr;
     void *nut = nullptr, *p = nullptr, *phi = nullptr, *spec = nullptr, *rhs3 = nullptr;
@@ -114,6 +118,18 @@ template <typename T> struct Impl;
 
 int dalloc(dfdm_ctx *c, void **p, size_t bytes) {
     if (bytes == 0) bytes = 16;
+    if (c->in_create) {   // carve from the context's arena (256-byte aligned)
+        const size_t need = (bytes + 255) & ~(size_t)255;
+        if (c->arena_off + need > c->arena_size) {
+            *p = nullptr;
+            return fail(DFDM_ERR_NOMEM, "context arena exhausted (" + std::to_string(c->arena_off + need) + " > " +
+                                            std::to_string(c->arena_size) + " bytes)");
+        }
+        *p = c->arena + c->arena_off;
+        c->arena_off += need;
+        CK(cudaMemsetAsync(*p, 0, bytes, c->stream));
+        return DFDM_OK;
+    }
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) {
         *p = nullptr;
@@ -588,16 +604,22 @@ int validate(const dfdm_grid *g, const dfdm_params *p) {
     return DFDM_OK;
 }
 
-size_t footprint(const dfdm_grid *g, const dfdm_params *p) {
+// Bytes of the buffers dfdm_create carves from the context's arena (every sub-allocation 256-byte aligned).
+size_t arena_bytes(const dfdm_grid *g, const dfdm_params *p) {
     size_t ts = p->precision == DFDM_FP64 ? 8 : 4;
     size_t Nx = g->nx - 2, Nz = g->nz - 2, Ny = g->y_bc_type == 0 ? g->ny - 2 : g->ny - 1;
     size_t cells = Nx * Ny * Nz, spec = (Nx / 2 + 1) * Ny * Nz;
     size_t n = cells * ts * (3 /*u*/ + 3 /*uo*/ + 3 /*F1*/ + 3 /*u**/ + 1 /*P*/ + 1 /*phi*/ + (p->sgs_model ? 1 : 0));
     n += spec * 2 * ts;
-    n += 6 * Nx * Nz * 2 * 8;   // wall planes
-    n += 1 << 20;               // metrics, twiddles, reductions
+    if (g->y_bc_type != 0) n += (Nx / 2 + 1) * Ny * Nz * 8;   // pivot table of the y solves
+    n += 8 * Nx * Nz * 2 * 8;   // wall planes
+    n += 1 << 20;               // metrics, twiddles, reductions, alignment
     return n;
 }
+// FP64 staging of the ghosted host arrays (set_state / get_state and the unit entry points), allocated on first use.
+size_t staging_bytes(const dfdm_grid *g) { return ((size_t)g->nx + 1) * ((size_t)g->ny + 1) * ((size_t)g->nz + 1) * 8; }
+
+size_t footprint(const dfdm_grid *g, const dfdm_params *p) { return arena_bytes(g, p) + staging_bytes(g); }
 
 }  // namespace
 
@@ -687,6 +709,20 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
     // dPdx = 0 under constant flux (src/time_integration.f90:212-216); steady forcing otherwise
     c->dPdx = prm->flow_forcing_mode == 1 ? 0.0 : prm->dPdx;
     c->dPdz = prm->dPdz;
+
+    // ---- one arena for every buffer made here ----
+    c->arena_size = arena_bytes(g, prm);
+    {
+        cudaError_t e = cudaMalloc((void **)&c->arena, c->arena_size);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            c->arena = nullptr;
+            return bail(fail(DFDM_ERR_NOMEM, "cudaMalloc of the " + std::to_string(c->arena_size) +
+                                                 "-byte context arena failed: " + cudaGetErrorString(e)));
+        }
+        c->allocs.push_back(c->arena);
+    }
+    c->in_create = true;
 
     // ---- fields ----
     const size_t F = (size_t)d.cells * c->ts;
@@ -824,6 +860,7 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
     c->d_maxdiv = (unsigned long long *)tmp;
     if ((rc = dalloc(c, &tmp, sizeof(int)))) return bail(rc);
     c->d_flag = (int *)tmp;
+    c->in_create = false;   // later buffers (host staging, the unit RHS output) are separate allocations
 
     rc = dispatch(c, [&](auto impl) { return decltype(impl)::setup_kernels(c); });
     if (rc) return bail(rc);
@@ -1212,6 +1249,179 @@ int dfdm_solve_poisson_noalloc(dfdm_ctx *c, const double *rhs_in, double *phi_ou
     if (rc) return rc;
     CK(cudaMemcpyAsync(phi_out, scratch, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return DFDM_OK;
+}
+
+}  // extern "C"
+
+namespace {
+// ---- the reference's restart format (one rank, little-endian stream) ----
+const int32_t SNAP_MAGIC = -4242;
+
+bool put_block(FILE *f, const double *a, int n1, int n2, int n3) {
+    const int32_t h[3] = {n1, n2, n3};
+    const size_t n = (size_t)n1 * n2 * n3;
+    return fwrite(h, sizeof(int32_t), 3, f) == 3 && fwrite(a, sizeof(double), n, f) == n;
+}
+int get_block(FILE *f, std::vector<double> &a, int n1, int n2, int n3, const char *what) {
+    int32_t h[3];
+    if (fread(h, sizeof(int32_t), 3, f) != 3) return fail(DFDM_ERR_INVALID, std::string("restart file ends before ") + what);
+    if (h[0] != n1 || h[1] != n2 || h[2] != n3)
+        return fail(DFDM_ERR_INVALID, std::string("restart file field block size mismatch for ") + what + ": found " +
+                                          std::to_string(h[0]) + " " + std::to_string(h[1]) + " " + std::to_string(h[2]) +
+                                          " expected " + std::to_string(n1) + " " + std::to_string(n2) + " " + std::to_string(n3));
+    a.resize((size_t)n1 * n2 * n3);
+    if (fread(a.data(), sizeof(double), a.size(), f) != a.size())
+        return fail(DFDM_ERR_INVALID, std::string("restart file ends inside the ") + what + " block");
+    return DFDM_OK;
+}
+// the six mesh arrays of the header: faces x, y, z (1-based host copies) and their centres
+std::vector<std::vector<double>> mesh_arrays(const dfdm_ctx *c) {
+    std::vector<std::vector<double>> m;
+    const std::vector<double> *f[3] = {&c->x, &c->y, &c->z};
+    const int n[3] = {c->nx, c->ny, c->nz};
+    for (int a = 0; a < 3; ++a) m.emplace_back(f[a]->begin() + 1, f[a]->begin() + 1 + n[a]);
+    for (int a = 0; a < 3; ++a) {
+        std::vector<double> xm(n[a] - 1);
+        for (int i = 0; i < n[a] - 1; ++i) xm[i] = 0.5 * ((*f[a])[i + 1] + (*f[a])[i + 2]);
+        m.push_back(xm);
+    }
+    return m;
+}
+// filter planes between the device layout (iw*Nz + k)*Nx + i and the reference shapes (nx,2,nzg) / (nxg,2,nz)
+// with the x/z ghost planes zero (write_distributed_field_block with interior_only)
+void wmf_to_ref(const dfdm_ctx *c, const std::vector<double> &dev, bool xface, std::vector<double> &ref) {
+    const Dims &d = c->d;
+    const int n1 = xface ? c->nx : c->nxg, n3 = xface ? c->nzg : c->nz;
+    ref.assign((size_t)n1 * 2 * n3, 0.0);
+    for (int k = 2; k <= n3 - 1; ++k)
+        for (int iw = 0; iw < 2; ++iw)
+            for (int i = 2; i <= n1 - 1; ++i) {
+                const int di = (i - 2) % d.Nx, dk = (k - 2) % d.Nz;
+                ref[(size_t)(i - 1) + (size_t)n1 * (iw + 2 * (size_t)(k - 1))] = dev[((size_t)iw * d.Nz + dk) * d.Nx + di];
+            }
+}
+void wmf_from_ref(const dfdm_ctx *c, const std::vector<double> &ref, bool xface, std::vector<double> &dev) {
+    const Dims &d = c->d;
+    const int n1 = xface ? c->nx : c->nxg;
+    dev.assign((size_t)2 * d.Nz * d.Nx, 0.0);
+    for (int iw = 0; iw < 2; ++iw)
+        for (int k = 0; k < d.Nz; ++k)
+            for (int i = 0; i < d.Nx; ++i)
+                dev[((size_t)iw * d.Nz + k) * d.Nx + i] = ref[(size_t)(i + 1) + (size_t)n1 * (iw + 2 * (size_t)(k + 1))];
+}
+struct FileCloser {
+    FILE *f;
+    ~FileCloser() { if (f) fclose(f); }
+};
+}  // namespace
+
+extern "C" {
+
+int dfdm_write_snapshot(dfdm_ctx *c, const char *path) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (!path) return fail(DFDM_ERR_INVALID, "null path");
+    const size_t nU = (size_t)c->nx * c->nyg * c->nzg, nV = (size_t)c->nxg * c->ny * c->nzg;
+    const size_t nW = (size_t)c->nxg * c->nyg * c->nz, nP = (size_t)c->nxg * c->nyg * c->nzg;
+    std::vector<double> U(nU), V(nV), W(nW), P(nP), NU;
+    int rc = dfdm_get_state(c, U.data(), V.data(), W.data(), P.data());
+    if (rc) return rc;
+    if (c->les) {
+        NU.resize(nP);
+        if ((rc = dfdm_get_nu_t(c, NU.data()))) return rc;
+    }
+    FileCloser fc{fopen(path, "wb")};
+    if (!fc.f) return fail(DFDM_ERR_INVALID, std::string("cannot open ") + path + " for writing");
+    bool ok = true;
+    for (const std::vector<double> &m : mesh_arrays(c)) {
+        const int32_t n = (int32_t)m.size();
+        ok = ok && fwrite(&n, sizeof(n), 1, fc.f) == 1 && fwrite(m.data(), sizeof(double), m.size(), fc.f) == m.size();
+    }
+    ok = ok && put_block(fc.f, U.data(), c->nx, c->nyg, c->nzg) && put_block(fc.f, V.data(), c->nxg, c->ny, c->nzg) &&
+         put_block(fc.f, W.data(), c->nxg, c->nyg, c->nz) && put_block(fc.f, P.data(), c->nxg, c->nyg, c->nzg);
+    if (c->les) ok = ok && put_block(fc.f, NU.data(), c->nxg, c->nyg, c->nzg);
+    if (!ok || fclose(fc.f) != 0) { fc.f = nullptr; return fail(DFDM_ERR_INVALID, std::string("write to ") + path + " failed"); }
+    fc.f = nullptr;
+    if (!(c->wm && c->wm_filter_mode == 1 && c->wmf_seeded)) return DFDM_OK;
+    // write_wm_filter_state
+    const size_t np = (size_t)2 * c->d.Nz * c->d.Nx;
+    double *planes[6] = {c->wsd.ux, c->wsd.wx, c->wsd.tx, c->wsd.uz, c->wsd.wz, c->wsd.tz};
+    FileCloser fw{fopen((std::string(path) + ".wmf").c_str(), "wb")};
+    if (!fw.f) return fail(DFDM_ERR_INVALID, std::string("cannot open ") + path + ".wmf for writing");
+    std::vector<double> dev(np), ref;
+    for (int q = 0; q < 6; ++q) {
+        CK(cudaMemcpyAsync(dev.data(), planes[q], np * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        const bool xf = q < 3;
+        wmf_to_ref(c, dev, xf, ref);
+        ok = ok && put_block(fw.f, ref.data(), xf ? c->nx : c->nxg, 2, xf ? c->nzg : c->nz);
+    }
+    if (!ok || fclose(fw.f) != 0) { fw.f = nullptr; return fail(DFDM_ERR_INVALID, std::string("write to ") + path + ".wmf failed"); }
+    fw.f = nullptr;
+    return DFDM_OK;
+}
+
+int dfdm_read_snapshot(dfdm_ctx *c, const char *path) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (!path) return fail(DFDM_ERR_INVALID, "null path");
+    FileCloser fc{fopen(path, "rb")};
+    if (!fc.f) return fail(DFDM_ERR_INVALID, std::string("cannot open restart file ") + path);
+    int32_t first = 0;
+    if (fread(&first, sizeof(first), 1, fc.f) != 1) return fail(DFDM_ERR_INVALID, "restart file is empty");
+    if (first == SNAP_MAGIC)
+        return fail(DFDM_ERR_INVALID, "the file is a cell-centred/chunked box snapshot and cannot be used for restart");
+    // size check of read_input_data: the mesh, then U, V, W and P
+    const std::vector<std::vector<double>> mesh = mesh_arrays(c);
+    long long expect = 6 * 4;
+    for (const auto &m : mesh) expect += 8LL * (long long)m.size();
+    expect += 4 * 12 + 8LL * ((long long)c->nx * c->nyg * c->nzg + (long long)c->nxg * c->ny * c->nzg +
+                              (long long)c->nxg * c->nyg * c->nz + (long long)c->nxg * c->nyg * c->nzg);
+    fseek(fc.f, 0, SEEK_END);
+    const long long have = ftell(fc.f);
+    if (have < expect)
+        return fail(DFDM_ERR_INVALID, "restart file is smaller than expected for this grid: " + std::to_string(have) +
+                                          " < " + std::to_string(expect) + " bytes");
+    fseek(fc.f, 0, SEEK_SET);
+    const char *names[6] = {"nx", "ny", "nz", "nxm", "nym", "nzm"};
+    for (int a = 0; a < 6; ++a) {
+        int32_t n = 0;
+        if (fread(&n, sizeof(n), 1, fc.f) != 1) return fail(DFDM_ERR_INVALID, "restart file header truncated");
+        if (n != (int32_t)mesh[a].size())
+            return fail(DFDM_ERR_INVALID, std::string("restart file ") + names[a] + " = " + std::to_string(n) +
+                                              " but the grid gives " + std::to_string(mesh[a].size()));
+        std::vector<double> f(n);
+        if (fread(f.data(), sizeof(double), n, fc.f) != (size_t)n) return fail(DFDM_ERR_INVALID, "restart file header truncated");
+        double scale = 1.0;
+        for (double v : mesh[a]) scale = std::max(scale, std::fabs(v));
+        for (int i = 0; i < n; ++i)
+            if (std::fabs(f[i] - mesh[a][i]) > 1e-12 * scale)
+                return fail(DFDM_ERR_INVALID, std::string("restart file coordinates (") + names[a] + ") differ from the grid");
+    }
+    std::vector<double> U, V, W, P;
+    int rc;
+    if ((rc = get_block(fc.f, U, c->nx, c->nyg, c->nzg, "U"))) return rc;
+    if ((rc = get_block(fc.f, V, c->nxg, c->ny, c->nzg, "V"))) return rc;
+    if ((rc = get_block(fc.f, W, c->nxg, c->nyg, c->nz, "W"))) return rc;
+    if ((rc = get_block(fc.f, P, c->nxg, c->nyg, c->nzg, "P"))) return rc;
+    if ((rc = dfdm_set_state(c, U.data(), V.data(), W.data(), P.data()))) return rc;
+    c->wmf_seeded = false;
+    if (!(c->wm && c->wm_filter_mode == 1)) return DFDM_OK;
+    FileCloser fw{fopen((std::string(path) + ".wmf").c_str(), "rb")};
+    if (!fw.f) return DFDM_OK;   // no filter file: the filter re-seeds on the next step
+    const size_t np = (size_t)2 * c->d.Nz * c->d.Nx;
+    double *planes[6] = {c->wsd.ux, c->wsd.wx, c->wsd.tx, c->wsd.uz, c->wsd.wz, c->wsd.tz};
+    const char *wn[6] = {"wmf_ux", "wmf_wx", "wmf_tx", "wmf_uz", "wmf_wz", "wmf_tz"};
+    std::vector<double> ref, dev;
+    for (int q = 0; q < 6; ++q) {
+        const bool xf = q < 3;
+        if ((rc = get_block(fw.f, ref, xf ? c->nx : c->nxg, 2, xf ? c->nzg : c->nz, wn[q]))) return rc;
+        wmf_from_ref(c, ref, xf, dev);
+        CK(cudaMemcpyAsync(planes[q], dev.data(), np * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    c->wmf_seeded = true;
     return DFDM_OK;
 }
 

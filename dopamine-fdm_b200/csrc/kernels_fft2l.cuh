@@ -1,11 +1,11 @@
 // kernels_fft2l.cuh -- the Poisson transforms for lengths with a two-level split (fft_reg.cuh).
 //
 // Same operations, inputs, outputs and rounding points as the Stockham kernels of kernels_poisson.cuh
-// (k_fwd_x, k_col_fft, k_inv_x): only the transform itself is organised differently.  Step 1 of every transform
-// reads its operands straight from global memory (and, in the x kernels, forms them there: the divergence of u*
-// or the packed half-length spectrum), step 2 of the z transforms and of the inverse x transform writes straight
-// to global memory, so a line crosses shared memory once (twice for the forward x transform, whose real-to-
-// complex unpacking pairs elements k and M-k).
+// (k_fwd_x, k_col_fft, k_inv_x): only the transform itself is organised differently.  Step 1 of the z transforms
+// and of the inverse x transform reads its operands straight from global memory (the inverse x kernel forms the
+// packed half-length spectrum there), and their step 2 writes straight to global memory, so a line crosses shared
+// memory once.  The forward x transform first forms the divergence pairs in shared memory with coalesced loads,
+// and its real-to-complex unpacking pairs elements k and M-k through shared memory once more.
 #pragma once
 
 #include "fft_reg.cuh"
@@ -13,7 +13,13 @@
 
 namespace dfdm {
 
+template <typename T> struct Vec2;
+template <> struct Vec2<float> { typedef float2 type; };
+template <> struct Vec2<double> { typedef double2 type; };
+
 // ---- div u* (or a real field) + forward real-to-complex x transform, line length Nx = 2M ----------------------
+// Phase A forms the packed half-length line z_n = x_2n + i x_2n+1 in shared memory with consecutive threads on
+// consecutive pairs (coalesced 8-byte loads of the velocity pairs); the two register steps follow.
 template <typename T, bool FROM_DIV, int M>
 __global__ void __launch_bounds__(256) k_fwd_x2(PoissonArgs<T> a, int lx, const T *__restrict__ U, const T *__restrict__ V,
                                                 const T *__restrict__ W, const T *__restrict__ src,
@@ -21,6 +27,7 @@ __global__ void __launch_bounds__(256) k_fwd_x2(PoissonArgs<T> a, int lx, const 
                                                 const typename cplx_t<T>::type *__restrict__ tw,
                                                 const typename cplx_t<T>::type *__restrict__ twr) {
     typedef typename cplx_t<T>::type C;
+    typedef typename Vec2<T>::type T2;
     typedef Arith<T> A;
     constexpr int N1 = Split<M>::N1, N2 = Split<M>::N2, Nx = 2 * M;
     constexpr int LDA = RowLayout<M>::LDA, LDT = RowLayout<M>::LDT;
@@ -30,37 +37,41 @@ __global__ void __launch_bounds__(256) k_fwd_x2(PoissonArgs<T> a, int lx, const 
     const int Ny = d.Ny, Nz = d.Nz, plane = Nx * Ny;
     const int line0 = blockIdx.x * lx;
     const int nl = min(lx, Ny * Nz - line0);
-    for (int b = threadIdx.x; b < nl * N2; b += blockDim.x) {
-        const int ll = b / N2, n2 = b - ll * N2;
+    for (int e = threadIdx.x; e < nl * M; e += blockDim.x) {
+        const int ll = e / M, n = e - ll * M;
         const int line = line0 + ll;
-        C v[N1];
+        C z;
         if (FROM_DIV) {
             const int k = (int)fdiv((unsigned)line, a.fNy), j = line - k * Ny;
-            const int ob = k * plane + j * Nx;
+            const int ob = k * plane + j * Nx, i = 2 * n, o = ob + i;
             const int dkm = (k == 0) ? (Nz - 1) * plane : -plane;
             const int djm = (j > 0) ? -Nx : (Ny - 1) * Nx;
             const bool vzero = (j == 0) && !d.yper;
             const T inv_dyj = A::inv(a.my.dc, a.my.idc, j), inv_dzk = A::inv(a.mz.dc, a.mz.idc, k);
-#pragma unroll
-            for (int n1 = 0; n1 < N1; ++n1) {
-                const int i = 2 * (n1 * N2 + n2);
-                const int o = ob + i;
-                const T um = __ldg(U + (i == 0 ? ob + Nx - 1 : o - 1)), u0 = __ldg(U + o), u1 = __ldg(U + o + 1);
-                const T v0 = __ldg(V + o), v1 = __ldg(V + o + 1);
-                const T vm0 = vzero ? T(0) : __ldg(V + o + djm), vm1 = vzero ? T(0) : __ldg(V + o + 1 + djm);
-                const T w0 = __ldg(W + o), w1 = __ldg(W + o + 1), wm0 = __ldg(W + o + dkm), wm1 = __ldg(W + o + 1 + dkm);
-                v[n1].x = (u0 - um) * a.inv_dx + (v0 - vm0) * inv_dyj + (w0 - wm0) * inv_dzk;
-                v[n1].y = (u1 - u0) * a.inv_dx + (v1 - vm1) * inv_dyj + (w1 - wm1) * inv_dzk;
-            }
+            const T2 u = *reinterpret_cast<const T2 *>(U + o);
+            const T um = __ldg(U + (i == 0 ? ob + Nx - 1 : o - 1));
+            const T2 v = *reinterpret_cast<const T2 *>(V + o);
+            T2 vm;
+            if (vzero) { vm.x = T(0); vm.y = T(0); }
+            else vm = *reinterpret_cast<const T2 *>(V + o + djm);
+            const T2 w = *reinterpret_cast<const T2 *>(W + o);
+            const T2 wm = *reinterpret_cast<const T2 *>(W + o + dkm);
+            z.x = (u.x - um) * a.inv_dx + (v.x - vm.x) * inv_dyj + (w.x - wm.x) * inv_dzk;
+            z.y = (u.y - u.x) * a.inv_dx + (v.y - vm.y) * inv_dyj + (w.y - wm.y) * inv_dzk;
         } else {
-            const T *s = src + (size_t)line * Nx;
-#pragma unroll
-            for (int n1 = 0; n1 < N1; ++n1) {
-                const int i = 2 * (n1 * N2 + n2);
-                v[n1].x = s[i];
-                v[n1].y = s[i + 1];
-            }
+            const T2 p = *reinterpret_cast<const T2 *>(src + (size_t)line * Nx + 2 * n);
+            z.x = p.x;
+            z.y = p.y;
         }
+        ba[ll * LDA + n] = z;
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < nl * N2; b += blockDim.x) {
+        const int ll = b / N2, n2 = b - ll * N2;
+        C v[N1];
+        const C *al = ba + ll * LDA + n2;
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) v[n1] = al[n1 * N2];
         row_step1<T, false, M>(v, bt + ll * LDT, n2, tw);
     }
     __syncthreads();
@@ -94,10 +105,6 @@ __global__ void __launch_bounds__(256) k_fwd_x2(PoissonArgs<T> a, int lx, const 
 }
 
 // ---- inverse complex-to-real x transform, writes phi = x / (nxp*nzp) -----------------------------------------
-template <typename T> struct Vec2;
-template <> struct Vec2<float> { typedef float2 type; };
-template <> struct Vec2<double> { typedef double2 type; };
-
 template <typename T, int M>
 __global__ void __launch_bounds__(256) k_inv_x2(PoissonArgs<T> a, int lx, const typename cplx_t<T>::type *__restrict__ spec,
                                                 T *__restrict__ phi, const typename cplx_t<T>::type *__restrict__ tw,

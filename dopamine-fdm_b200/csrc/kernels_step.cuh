@@ -173,15 +173,54 @@ __global__ void k_wall_model(StepArgs<T> a, WallState ws, const T *__restrict__ 
 }
 
 // ---------------------------------------------------------------------------------------------------------------
+// Metric values around one index p of an axis: weights of faces p-1 and p, widths and spacings at p-1, p, p+1.
+// FP32 reads them once per thread (y) or once per plane (z) and keeps them in registers; FP64 reads them where
+// they are used (its registers are taken by the double-precision stencil) and divides exactly, as Arith does.
+template <typename T> struct AxisLocal;
+template <> struct AxisLocal<float> {
+    float w0m_, w1m_, w0_, w1_, idc_, idcp_, idfm_, idf_;
+    __device__ __forceinline__ void load(const Metric1D<float> &m, int p) {
+        w0m_ = __ldg(m.w0 + p - 1); w1m_ = __ldg(m.w1 + p - 1); w0_ = __ldg(m.w0 + p); w1_ = __ldg(m.w1 + p);
+        idc_ = __ldg(m.idc + p); idcp_ = __ldg(m.idc + p + 1); idfm_ = __ldg(m.idf + p - 1); idf_ = __ldg(m.idf + p);
+    }
+    __device__ __forceinline__ float w0m() const { return w0m_; }
+    __device__ __forceinline__ float w1m() const { return w1m_; }
+    __device__ __forceinline__ float w0() const { return w0_; }
+    __device__ __forceinline__ float w1() const { return w1_; }
+    __device__ __forceinline__ float divc(float x) const { return x * idc_; }
+    __device__ __forceinline__ float divf(float x) const { return x * idf_; }
+    __device__ __forceinline__ float divfm(float x) const { return x * idfm_; }
+    __device__ __forceinline__ float invc() const { return idc_; }
+    __device__ __forceinline__ float invcp() const { return idcp_; }
+    __device__ __forceinline__ float invf() const { return idf_; }
+    __device__ __forceinline__ float invfm() const { return idfm_; }
+};
+template <> struct AxisLocal<double> {
+    const Metric1D<double> *m;   // the kernel argument's metric (stays in the parameter bank once inlined)
+    int p;
+    __device__ __forceinline__ void load(const Metric1D<double> &m_, int p_) { m = &m_; p = p_; }
+    __device__ __forceinline__ double w0m() const { return m->w0[p - 1]; }
+    __device__ __forceinline__ double w1m() const { return m->w1[p - 1]; }
+    __device__ __forceinline__ double w0() const { return m->w0[p]; }
+    __device__ __forceinline__ double w1() const { return m->w1[p]; }
+    __device__ __forceinline__ double divc(double x) const { return x / m->dc[p]; }
+    __device__ __forceinline__ double divf(double x) const { return x / m->df[p]; }
+    __device__ __forceinline__ double divfm(double x) const { return x / m->df[p - 1]; }
+    __device__ __forceinline__ double invc() const { return 1.0 / m->dc[p]; }
+    __device__ __forceinline__ double invcp() const { return 1.0 / m->dc[p + 1]; }
+    __device__ __forceinline__ double invf() const { return 1.0 / m->df[p]; }
+    __device__ __forceinline__ double invfm() const { return 1.0 / m->df[p - 1]; }
+};
+
 // Right-hand sides (src/equations.f90), evaluated in the reference's expression order at one index (i,j,k).
 // `q` is a neighbourhood accessor: q.U(di,dj,dk) is U at (i+di, j+dj, k+dk) with every boundary rule already
 // applied (periodic wraps, no-slip mirror, zero wall faces, zero nu_t ghosts), so the formulas below see the
 // same values the reference reads from its ghosted arrays.
 template <typename T, bool LES, typename Q>
-__device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Q &q, const double *__restrict__ tau_x, int i, int j, int k) {
+__device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Q &q, const AxisLocal<T> &Y, const AxisLocal<T> &Z,
+                                    const double *__restrict__ tau_x, int i, int j, int k) {
     const Dims &d = a.d;
     typedef Arith<T> A;
-    const Metric1D<T> &my = a.my, &mz = a.mz;
     T Uc = q.U(0, 0, 0), Uim = q.U(-1, 0, 0), Uip = q.U(1, 0, 0);
     T Ujm = q.U(0, -1, 0), Ujp = q.U(0, 1, 0), Ukm = q.U(0, 0, -1), Ukp = q.U(0, 0, 1);
     bool wm_band = a.wm && (j + 2 <= 1 + a.nwl || j + 2 >= d.Ny + 2 - a.nwl);
@@ -200,39 +239,39 @@ __device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Q &q, const do
     // -d(uv)/dy: u at y faces j-1, j (weighted), v at x faces (plain average)
     T V00 = q.V(0, 0, 0), V10 = q.V(1, 0, 0), V0m = q.V(0, -1, 0), V1m = q.V(1, -1, 0);
     {
-        T u1 = my.w0[j] * Uc + my.w1[j] * Ujp, u0 = my.w0[j - 1] * Ujm + my.w1[j - 1] * Uc;
+        T u1 = Y.w0() * Uc + Y.w1() * Ujp, u0 = Y.w0m() * Ujm + Y.w1m() * Uc;
         T v1 = T(0.5) * (V00 + V10), v0 = T(0.5) * (V0m + V1m);
-        r = r - A::div(wd * (u1 * v1 - u0 * v0) + wa * T(0.5) * (v0 + v1) * (u1 - u0), my.dc, my.idc, j);
+        r = r - Y.divc(wd * (u1 * v1 - u0 * v0) + wa * T(0.5) * (v0 + v1) * (u1 - u0));
     }
     // -d(uw)/dz
     T W00 = q.W(0, 0, 0), W10 = q.W(1, 0, 0), W0m = q.W(0, 0, -1), W1m = q.W(1, 0, -1);
     {
-        T u1 = mz.w0[k] * Uc + mz.w1[k] * Ukp, u0 = mz.w0[k - 1] * Ukm + mz.w1[k - 1] * Uc;
+        T u1 = Z.w0() * Uc + Z.w1() * Ukp, u0 = Z.w0m() * Ukm + Z.w1m() * Uc;
         T w1 = T(0.5) * (W00 + W10), w0 = T(0.5) * (W0m + W1m);
         if constexpr (sizeof(T) == 4) {
             // u1 w1 - u0 w0 = u1 (w1 - w0) + w0 (u1 - u0); u1 - u0 from deviations (same row: the profile cancels)
             T Udc = q.Ud(0, 0, 0);
-            T du = (mz.w0[k] * Udc + mz.w1[k] * q.Ud(0, 0, 1)) - (mz.w0[k - 1] * q.Ud(0, 0, -1) + mz.w1[k - 1] * Udc);
-            r = r - A::div(wd * (u1 * (w1 - w0) + w0 * du) + wa * T(0.5) * (w0 + w1) * du, mz.dc, mz.idc, k);
+            T du = (Z.w0() * Udc + Z.w1() * q.Ud(0, 0, 1)) - (Z.w0m() * q.Ud(0, 0, -1) + Z.w1m() * Udc);
+            r = r - Z.divc(wd * (u1 * (w1 - w0) + w0 * du) + wa * T(0.5) * (w0 + w1) * du);
         } else {
-            r = r - A::div(wd * (u1 * w1 - u0 * w0) + wa * T(0.5) * (w0 + w1) * (u1 - u0), mz.dc, mz.idc, k);
+            r = r - Z.divc(wd * (u1 * w1 - u0 * w0) + wa * T(0.5) * (w0 + w1) * (u1 - u0));
         }
     }
     // viscous: d(2 nu_x du/dx)/dx + d(nu_y (du/dy + dv/dx))/dy + d(nu_z (du/dz + dw/dx))/dz + dPdx
-    T inv_dz3 = A::inv(mz.dc, mz.idc, k), inv_dy3 = A::inv(my.dc, my.idc, j);
+    T inv_dz3 = Z.invc(), inv_dy3 = Y.invc();
     T nu = a.nu;
     T nu_x1 = nu, nu_x2 = nu, nu_y1 = nu, nu_y2 = nu, nu_z1 = nu, nu_z2 = nu;
     if (LES) {
         T n_c = q.N(0, 0, 0), n_p = q.N(1, 0, 0);
         nu_x1 = nu + n_c; nu_x2 = nu + n_p;
         if (!(d.yper == 0 && j == 0))
-            nu_y1 = nu + T(0.5) * (my.w0[j - 1] * q.N(0, -1, 0) + my.w1[j - 1] * n_c + my.w0[j - 1] * q.N(1, -1, 0) + my.w1[j - 1] * n_p);
+            nu_y1 = nu + T(0.5) * (Y.w0m() * q.N(0, -1, 0) + Y.w1m() * n_c + Y.w0m() * q.N(1, -1, 0) + Y.w1m() * n_p);
         if (!(d.yper == 0 && j == d.Ny - 1))
-            nu_y2 = nu + T(0.5) * (my.w0[j] * n_c + my.w1[j] * q.N(0, 1, 0) + my.w0[j] * n_p + my.w1[j] * q.N(1, 1, 0));
-        nu_z1 = nu + T(0.5) * (mz.w0[k - 1] * (q.N(0, 0, -1) + q.N(1, 0, -1)) + mz.w1[k - 1] * (n_c + n_p));
-        nu_z2 = nu + T(0.5) * (mz.w0[k] * (n_c + n_p) + mz.w1[k] * (q.N(0, 0, 1) + q.N(1, 0, 1)));
+            nu_y2 = nu + T(0.5) * (Y.w0() * n_c + Y.w1() * q.N(0, 1, 0) + Y.w0() * n_p + Y.w1() * q.N(1, 1, 0));
+        nu_z1 = nu + T(0.5) * (Z.w0m() * (q.N(0, 0, -1) + q.N(1, 0, -1)) + Z.w1m() * (n_c + n_p));
+        nu_z2 = nu + T(0.5) * (Z.w0() * (n_c + n_p) + Z.w1() * (q.N(0, 0, 1) + q.N(1, 0, 1)));
     }
-    T tj = A::div(Ujp - Uc, my.df, my.idf, j), tjm = A::div(Uc - Ujm, my.df, my.idf, j - 1);
+    T tj = Y.divf(Ujp - Uc), tjm = Y.divfm(Uc - Ujm);
     T fy2 = nu_y2 * (tj + (V10 - V00) * a.inv_dx);
     T fy1 = nu_y1 * (tjm + (V1m - V0m) * a.inv_dx);
     if (a.wm) {
@@ -245,7 +284,7 @@ __device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Q &q, const do
         dUkp = q.Ud(0, 0, 1) - Udc; dUkm = Udc - q.Ud(0, 0, -1);
         dUip = q.Ud(1, 0, 0) - Udc; dUim = Udc - q.Ud(-1, 0, 0);
     }
-    T tk = A::div(dUkp, mz.df, mz.idf, k), tkm = A::div(dUkm, mz.df, mz.idf, k - 1);
+    T tk = Z.divf(dUkp), tkm = Z.divfm(dUkm);
     T fz2 = nu_z2 * (tk + (W10 - W00) * a.inv_dx);
     T fz1 = nu_z1 * (tkm + (W1m - W0m) * a.inv_dx);
     r = r + T(2) * a.inv_dx2 * (nu_x2 * dUip - nu_x1 * dUim) + inv_dy3 * (fy2 - fy1) + inv_dz3 * (fz2 - fz1) + a.dPdx;
@@ -253,24 +292,23 @@ __device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Q &q, const do
 }
 
 template <typename T, bool LES, typename Q>
-__device__ __forceinline__ T rhs_v_at(const StepArgs<T> &a, const Q &q, int i, int j, int k) {
+__device__ __forceinline__ T rhs_v_at(const StepArgs<T> &a, const Q &q, const AxisLocal<T> &Y, const AxisLocal<T> &Z, int i, int j, int k) {
     const Dims &d = a.d;
     typedef Arith<T> A;
-    const Metric1D<T> &my = a.my, &mz = a.mz;
     (void)i; (void)d;
     T wa = a.w_adv, wd = T(1) - wa;
     T Vc = q.V(0, 0, 0), Vjm = q.V(0, -1, 0), Vjp = q.V(0, 1, 0);
     T Vim = q.V(-1, 0, 0), Vip = q.V(1, 0, 0), Vkm = q.V(0, 0, -1), Vkp = q.V(0, 0, 1);
     // -d(vv)/dy
     T t1 = T(0.5) * (Vc + Vjp), t0 = T(0.5) * (Vjm + Vc);
-    T r = -A::div(wd * (t1 * t1 - t0 * t0) + wa * Vc * (t1 - t0), my.df, my.idf, j);
+    T r = -Y.divf(wd * (t1 * t1 - t0 * t0) + wa * Vc * (t1 - t0));
     // -d(uv)/dx: u at y face j (weighted), v at x faces
     T Uc = q.U(0, 0, 0), Um = q.U(-1, 0, 0), Ucp = q.U(0, 1, 0), Ump = q.U(-1, 1, 0);
     {
-        T u1 = my.w0[j] * Uc + my.w1[j] * Ucp, u0 = my.w0[j] * Um + my.w1[j] * Ump;
+        T u1 = Y.w0() * Uc + Y.w1() * Ucp, u0 = Y.w0() * Um + Y.w1() * Ump;
         T v1 = T(0.5) * (Vc + Vip), v0 = T(0.5) * (Vim + Vc);
         if constexpr (sizeof(T) == 4) {   // u1 v1 - u0 v0 = u1 (v1 - v0) + v0 (u1 - u0), u1 - u0 from deviations
-            T du = my.w0[j] * (q.Ud(0, 0, 0) - q.Ud(-1, 0, 0)) + my.w1[j] * (q.Ud(0, 1, 0) - q.Ud(-1, 1, 0));
+            T du = Y.w0() * (q.Ud(0, 0, 0) - q.Ud(-1, 0, 0)) + Y.w1() * (q.Ud(0, 1, 0) - q.Ud(-1, 1, 0));
             r = r - (wd * (u1 * (v1 - v0) + v0 * du) + wa * T(0.5) * (u0 + u1) * (v1 - v0)) * a.inv_dx;
         } else {
             r = r - (wd * (u1 * v1 - u0 * v0) + wa * T(0.5) * (u0 + u1) * (v1 - v0)) * a.inv_dx;
@@ -279,26 +317,26 @@ __device__ __forceinline__ T rhs_v_at(const StepArgs<T> &a, const Q &q, int i, i
     // -d(vw)/dz: v at z faces (weighted), w at y face j (weighted)
     T Wc = q.W(0, 0, 0), Wjp = q.W(0, 1, 0), Wkm = q.W(0, 0, -1), Wkmjp = q.W(0, 1, -1);
     {
-        T v1 = mz.w0[k] * Vc + mz.w1[k] * Vkp, v0 = mz.w0[k - 1] * Vkm + mz.w1[k - 1] * Vc;
-        T w1 = my.w0[j] * Wc + my.w1[j] * Wjp, w0 = my.w0[j] * Wkm + my.w1[j] * Wkmjp;
-        r = r - A::div(wd * (v1 * w1 - v0 * w0) + wa * T(0.5) * (w0 + w1) * (v1 - v0), mz.dc, mz.idc, k);
+        T v1 = Z.w0() * Vc + Z.w1() * Vkp, v0 = Z.w0m() * Vkm + Z.w1m() * Vc;
+        T w1 = Y.w0() * Wc + Y.w1() * Wjp, w0 = Y.w0() * Wkm + Y.w1() * Wkmjp;
+        r = r - Z.divc(wd * (v1 * w1 - v0 * w0) + wa * T(0.5) * (w0 + w1) * (v1 - v0));
     }
     // viscous
-    T inv_dz3 = A::inv(mz.dc, mz.idc, k);
-    T inv_dzg1 = A::inv(mz.df, mz.idf, k - 1), inv_dzg2 = A::inv(mz.df, mz.idf, k);
-    T inv_dy1 = A::inv(my.dc, my.idc, j), inv_dy2 = A::inv(my.dc, my.idc, j + 1), inv_dy3 = A::inv(my.df, my.idf, j);
+    T inv_dz3 = Z.invc();
+    T inv_dzg1 = Z.invfm(), inv_dzg2 = Z.invf();
+    T inv_dy1 = Y.invc(), inv_dy2 = Y.invcp(), inv_dy3 = Y.invf();
     T two_inv_dy3 = T(2) * inv_dy3;
     T nu = a.nu;
     T nu_x1 = nu, nu_x2 = nu, nu_y1 = nu, nu_y2 = nu, nu_z1 = nu, nu_z2 = nu;
     if (LES) {
         T n_c = q.N(0, 0, 0), n_jp = q.N(0, 1, 0);
-        T w0 = my.w0[j], w1 = my.w1[j];
+        T w0 = Y.w0(), w1 = Y.w1();
         nu_x1 = nu + T(0.5) * (w0 * q.N(-1, 0, 0) + w1 * q.N(-1, 1, 0) + w0 * n_c + w1 * n_jp);
         nu_x2 = nu + T(0.5) * (w0 * n_c + w1 * n_jp + w0 * q.N(1, 0, 0) + w1 * q.N(1, 1, 0));
         nu_y1 = nu + n_c;
         nu_y2 = nu + n_jp;
-        nu_z1 = nu + mz.w0[k - 1] * (w0 * q.N(0, 0, -1) + w1 * q.N(0, 1, -1)) + mz.w1[k - 1] * (w0 * n_c + w1 * n_jp);
-        nu_z2 = nu + mz.w0[k] * (w0 * n_c + w1 * n_jp) + mz.w1[k] * (w0 * q.N(0, 0, 1) + w1 * q.N(0, 1, 1));
+        nu_z1 = nu + Z.w0m() * (w0 * q.N(0, 0, -1) + w1 * q.N(0, 1, -1)) + Z.w1m() * (w0 * n_c + w1 * n_jp);
+        nu_z2 = nu + Z.w0() * (w0 * n_c + w1 * n_jp) + Z.w1() * (w0 * q.N(0, 0, 1) + w1 * q.N(0, 1, 1));
     }
     T fx2 = nu_x2 * ((Vip - Vc) * a.inv_dx + (Ucp - Uc) * inv_dy3);
     T fx1 = nu_x1 * ((Vc - Vim) * a.inv_dx + (Ump - Um) * inv_dy3);
@@ -309,24 +347,24 @@ __device__ __forceinline__ T rhs_v_at(const StepArgs<T> &a, const Q &q, int i, i
 }
 
 template <typename T, bool LES, typename Q>
-__device__ __forceinline__ T rhs_w_at(const StepArgs<T> &a, const Q &q, const double *__restrict__ tau_z, int i, int j, int k) {
+__device__ __forceinline__ T rhs_w_at(const StepArgs<T> &a, const Q &q, const AxisLocal<T> &Y, const AxisLocal<T> &Z,
+                                    const double *__restrict__ tau_z, int i, int j, int k) {
     const Dims &d = a.d;
     typedef Arith<T> A;
-    const Metric1D<T> &my = a.my, &mz = a.mz;
     bool wm_band = a.wm && (j + 2 <= 1 + a.nwl || j + 2 >= d.Ny + 2 - a.nwl);
     T wa = wm_band ? T(0) : a.w_adv, wd = T(1) - wa;
     T Wc = q.W(0, 0, 0), Wkm = q.W(0, 0, -1), Wkp = q.W(0, 0, 1);
     T Wim = q.W(-1, 0, 0), Wip = q.W(1, 0, 0), Wjm = q.W(0, -1, 0), Wjp = q.W(0, 1, 0);
     // -d(ww)/dz
     T t1 = T(0.5) * (Wc + Wkp), t0 = T(0.5) * (Wkm + Wc);
-    T r = -A::div(wd * (t1 * t1 - t0 * t0) + wa * Wc * (t1 - t0), mz.df, mz.idf, k);
+    T r = -Z.divf(wd * (t1 * t1 - t0 * t0) + wa * Wc * (t1 - t0));
     // -d(uw)/dx: u at z face k (weighted), w at x faces
     T Uc = q.U(0, 0, 0), Um = q.U(-1, 0, 0), Ukp = q.U(0, 0, 1), Umkp = q.U(-1, 0, 1);
     {
-        T u1 = mz.w0[k] * Uc + mz.w1[k] * Ukp, u0 = mz.w0[k] * Um + mz.w1[k] * Umkp;
+        T u1 = Z.w0() * Uc + Z.w1() * Ukp, u0 = Z.w0() * Um + Z.w1() * Umkp;
         T w1 = T(0.5) * (Wc + Wip), w0 = T(0.5) * (Wim + Wc);
         if constexpr (sizeof(T) == 4) {   // u1 w1 - u0 w0 = u1 (w1 - w0) + w0 (u1 - u0), u1 - u0 from deviations
-            T du = mz.w0[k] * (q.Ud(0, 0, 0) - q.Ud(-1, 0, 0)) + mz.w1[k] * (q.Ud(0, 0, 1) - q.Ud(-1, 0, 1));
+            T du = Z.w0() * (q.Ud(0, 0, 0) - q.Ud(-1, 0, 0)) + Z.w1() * (q.Ud(0, 0, 1) - q.Ud(-1, 0, 1));
             r = r - (wd * (u1 * (w1 - w0) + w0 * du) + wa * T(0.5) * (u0 + u1) * (w1 - w0)) * a.inv_dx;
         } else {
             r = r - (wd * (u1 * w1 - u0 * w0) + wa * T(0.5) * (u0 + u1) * (w1 - w0)) * a.inv_dx;
@@ -335,29 +373,29 @@ __device__ __forceinline__ T rhs_w_at(const StepArgs<T> &a, const Q &q, const do
     // -d(vw)/dy: v at z face k (weighted), w at y faces (weighted)
     T Vc = q.V(0, 0, 0), Vkp = q.V(0, 0, 1), Vjm = q.V(0, -1, 0), Vjmkp = q.V(0, -1, 1);
     {
-        T v1 = mz.w0[k] * Vc + mz.w1[k] * Vkp, v0 = mz.w0[k] * Vjm + mz.w1[k] * Vjmkp;
-        T w1 = my.w0[j] * Wc + my.w1[j] * Wjp, w0 = my.w0[j - 1] * Wjm + my.w1[j - 1] * Wc;
-        r = r - A::div(wd * (v1 * w1 - v0 * w0) + wa * T(0.5) * (v0 + v1) * (w1 - w0), my.dc, my.idc, j);
+        T v1 = Z.w0() * Vc + Z.w1() * Vkp, v0 = Z.w0() * Vjm + Z.w1() * Vjmkp;
+        T w1 = Y.w0() * Wc + Y.w1() * Wjp, w0 = Y.w0m() * Wjm + Y.w1m() * Wc;
+        r = r - Y.divc(wd * (v1 * w1 - v0 * w0) + wa * T(0.5) * (v0 + v1) * (w1 - w0));
     }
     // viscous
-    T inv_dz1 = A::inv(mz.dc, mz.idc, k), inv_dz2 = A::inv(mz.dc, mz.idc, k + 1), inv_dz3 = A::inv(mz.df, mz.idf, k);
+    T inv_dz1 = Z.invc(), inv_dz2 = Z.invcp(), inv_dz3 = Z.invf();
     T two_inv_dz3 = T(2) * inv_dz3;
-    T inv_dy3 = A::inv(my.dc, my.idc, j);
+    T inv_dy3 = Y.invc();
     T nu = a.nu;
     T nu_x1 = nu, nu_x2 = nu, nu_y1 = nu, nu_y2 = nu, nu_z1 = nu, nu_z2 = nu;
     if (LES) {
         T n_c = q.N(0, 0, 0), n_kp = q.N(0, 0, 1);
-        T z0 = mz.w0[k], z1 = mz.w1[k];
+        T z0 = Z.w0(), z1 = Z.w1();
         nu_x1 = nu + T(0.5) * (z0 * (n_c + q.N(-1, 0, 0)) + z1 * (n_kp + q.N(-1, 0, 1)));
         nu_x2 = nu + T(0.5) * (z0 * (n_c + q.N(1, 0, 0)) + z1 * (n_kp + q.N(1, 0, 1)));
         if (!(d.yper == 0 && j == 0))
-            nu_y1 = nu + z0 * (my.w0[j - 1] * q.N(0, -1, 0) + my.w1[j - 1] * n_c) + z1 * (my.w0[j - 1] * q.N(0, -1, 1) + my.w1[j - 1] * n_kp);
+            nu_y1 = nu + z0 * (Y.w0m() * q.N(0, -1, 0) + Y.w1m() * n_c) + z1 * (Y.w0m() * q.N(0, -1, 1) + Y.w1m() * n_kp);
         if (!(d.yper == 0 && j == d.Ny - 1))
-            nu_y2 = nu + z0 * (my.w0[j] * n_c + my.w1[j] * q.N(0, 1, 0)) + z1 * (my.w0[j] * n_kp + my.w1[j] * q.N(0, 1, 1));
+            nu_y2 = nu + z0 * (Y.w0() * n_c + Y.w1() * q.N(0, 1, 0)) + z1 * (Y.w0() * n_kp + Y.w1() * q.N(0, 1, 1));
         nu_z1 = nu + n_c;
         nu_z2 = nu + n_kp;
     }
-    T tj = A::div(Wjp - Wc, my.df, my.idf, j), tjm = A::div(Wc - Wjm, my.df, my.idf, j - 1);
+    T tj = Y.divf(Wjp - Wc), tjm = Y.divfm(Wc - Wjm);
     T fy2 = nu_y2 * (tj + (Vkp - Vc) * inv_dz3);
     T fy1 = nu_y1 * (tjm + (Vjmkp - Vjm) * inv_dz3);
     if (a.wm) {
@@ -494,6 +532,9 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
         ubr[dj + 1] = sgn * __ldg(a.ub + gj);
     }
 
+    AxisLocal<T> Y;   // this thread's y metrics (FP32: read here once for every plane)
+    Y.load(a.my, min(j, Ny - 1));
+
     // planes k0-1, k0, k0+1 into slots 0, 1, 2; plane k lives in slot (k - k0 + 1) & 3
     issue(0, k0 - 1); issue(1, k0); issue(2, k0 + 1);
     cp_async_commit();
@@ -527,9 +568,11 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
                     fu = f1u[p]; fw = f1w[p];
                     if (vrow) fv = f1v[p];
                 }
-                T ru = rhs_u_at<T, LES>(a, q, tau_x, i, j, k);
-                T rw = rhs_w_at<T, LES>(a, q, tau_z, i, j, k);
-                T rv = vrow ? rhs_v_at<T, LES>(a, q, i, j, k) : T(0);
+                AxisLocal<T> Z;
+                Z.load(a.mz, k);
+                T ru = rhs_u_at<T, LES>(a, q, Y, Z, tau_x, i, j, k);
+                T rw = rhs_w_at<T, LES>(a, q, Y, Z, tau_z, i, j, k);
+                T rv = vrow ? rhs_v_at<T, LES>(a, q, Y, Z, i, j, k) : T(0);
                 if (rhs_only) {
                     rhs_only[p] = ru; rhs_only[d.cells + p] = rv; rhs_only[2 * d.cells + p] = rw;
                 } else if (sc.stage == 1) {

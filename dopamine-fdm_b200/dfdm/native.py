@@ -30,7 +30,7 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_compute_wall_model", "dfdm_apply_boundary_conditions", "dfdm_compute_projection_step",
            "dfdm_solve_poisson", "dfdm_compute_bulk_velocity", "dfdm_check_divergence", "dfdm_kinetic_energy",
            "dfdm_check_finite", "dfdm_pad_field", "dfdm_launch_kernel_async", "dfdm_kernel_bytes",
-           "dfdm_launch_count", "dfdm_solve_poisson_noalloc"]
+           "dfdm_launch_count", "dfdm_solve_poisson_noalloc", "dfdm_write_snapshot", "dfdm_read_snapshot"]
 
 
 class DfdmError(RuntimeError):
@@ -87,6 +87,9 @@ def load(build_if_missing: bool = True):
         "dfdm_launch_kernel_async": (c_int, [c_void_p, c_int, c_int]),
         "dfdm_kernel_bytes": (c_int, [c_void_p, c_int, P]),
         "dfdm_launch_count": (c_int, [c_void_p, POINTER(ctypes.c_longlong)]),
+        "dfdm_solve_poisson_noalloc": (c_int, [c_void_p, P, P]),
+        "dfdm_write_snapshot": (c_int, [c_void_p, c_char_p]),
+        "dfdm_read_snapshot": (c_int, [c_void_p, c_char_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -234,6 +237,14 @@ class Solver:
         out = np.zeros_like(a, order="F")
         _check(load().dfdm_solve_poisson_noalloc(self.h, dptr(a), dptr(out)))
         return out
+
+    def write_snapshot(self, path: str) -> None:
+        """The reference's restart file (and <path>.wmf with a seeded wall-model filter)."""
+        _check(load().dfdm_write_snapshot(self.h, os.fsencode(path)))
+
+    def read_snapshot(self, path: str) -> None:
+        """U, V, W, P (and the wall-model filter from <path>.wmf) from a restart file of this grid."""
+        _check(load().dfdm_read_snapshot(self.h, os.fsencode(path)))
 
     def compute_bulk_velocity(self) -> float:
         v = c_double(0.0)

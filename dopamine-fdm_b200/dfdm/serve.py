@@ -303,3 +303,43 @@ def run_isolated(executor, requests: List[Request], keep_state: bool = False) ->
         out.append(Result(r.rid, a, a, executor.now() - t0, r.nsteps, r.cells, state, summary))
     executor.reclaim()
     return out
+
+
+def measure_stream(executor, requests: List[Request], rank: int, world: int, gather, budget_bytes: float = 150e9,
+                   saturated: int = 48) -> Dict[str, object]:
+    """The serving measurement on one rank of `world` replicas: rank r serves requests r::world of the stream.
+
+    Returns the whole job's figures on every rank: p50/p99 latency from arrival to the result on the host over all
+    ranks' requests, the stream's throughput, and the loop's throughput when saturated (the rank's first
+    `saturated` requests all arriving at once) against the same requests run alone back to back.  `gather(obj)`
+    returns the list of every rank's obj (all_gather_object under torch.distributed, [obj] alone)."""
+    mine = requests[rank::world]
+    sch = Scheduler(executor, budget_bytes)
+    t0 = executor.now()
+    res = sch.run(mine)
+    wall = executor.now() - t0
+    sub = [Request(r.rid, r.case, r.nsteps, 0.0, r.precision) for r in mine[:saturated]]
+    iso = run_isolated(executor, sub)
+    iso_wall = iso[-1].finished if iso else float("nan")
+    t0 = executor.now()
+    Scheduler(executor, budget_bytes).run(sub)
+    sat_wall = executor.now() - t0
+    work_sub = float(sum(r.work for r in sub))
+    parts = gather({"rids": [r.rid for r in res], "lat": [r.latency for r in res],
+                    "work": float(sum(r.work for r in mine)), "wall": wall,
+                    "iso": work_sub / iso_wall if iso else 0.0, "sat": work_sub / sat_wall if sub else 0.0,
+                    "n_sub": len(sub), "finite": all(r.summary.get("finite", 1.0) == 1.0 for r in res),
+                    "peak_active": sch.peak_active, "peak_bytes": sch.peak_bytes})
+    lat = [x for p in parts for x in p["lat"]]
+    rids = sorted(x for p in parts for x in p["rids"])
+    iso_thr = sum(p["iso"] for p in parts)
+    sat_thr = sum(p["sat"] for p in parts)
+    wall_max = max(p["wall"] for p in parts)
+    return {"requests": len(lat), "rids": rids, "p50_latency_s": percentile(lat, 50),
+            "p99_latency_s": percentile(lat, 99), "max_latency_s": max(lat) if lat else None,
+            "stream_wall_s": wall_max, "stream_throughput_cell_steps_per_s": sum(p["work"] for p in parts) / wall_max,
+            "saturated_requests": sum(p["n_sub"] for p in parts), "saturated_throughput_cell_steps_per_s": sat_thr,
+            "isolated_throughput_cell_steps_per_s": iso_thr,
+            "saturated_over_isolated": sat_thr / iso_thr if iso_thr > 0 else None,
+            "all_finite": all(p["finite"] for p in parts), "peak_active": max(p["peak_active"] for p in parts),
+            "peak_admitted_bytes": max(p["peak_bytes"] for p in parts), "admission_budget_bytes": budget_bytes}

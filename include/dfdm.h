@@ -149,6 +149,17 @@ int dfdm_solve_poisson(dfdm_ctx *ctx, const double *rhs_p_in, double *phi_out);
  *    threads) race on the array: serialise them. */
 #define DFDM_NOALLOC_MAX_POINTS 2097152
 int dfdm_solve_poisson_noalloc(dfdm_ctx *ctx, const double *rhs_p_in, double *phi_out);
+/* ---- snapshots in the reference's restart format ----
+ * output_data's staggered full snapshot (src/input_output.f90:1782-1880): a little-endian stream holding the mesh
+ * (int32 n and n doubles for x, y, z and the centres xm, ym, zm) and then U, V, W, P and, with an SGS model, nu_t,
+ * each as int32 n1, n2, n3 and the ghosted array in Fortran order. With the wall-model filter seeded
+ * (wm_filter_mode = 1), write_wm_filter_state (:1990-2009) adds <path>.wmf with the six filter planes. */
+int dfdm_write_snapshot(dfdm_ctx *ctx, const char *path);
+/* read_input_data (src/input_output.f90:1225-1341) with the pressure block of read_pressure_restart (:1972-1977)
+ * and read_wm_filter_state (:2011-2031): loads U, V, W and P from a restart file of this grid (DFDM_ERR_INVALID
+ * for a chunked/cell-centred snapshot, a short file, other face counts, other coordinates or a block of another
+ * shape) and the filter planes from <path>.wmf when it exists; without it the filter re-seeds on the next step. */
+int dfdm_read_snapshot(dfdm_ctx *ctx, const char *path);
 /* compute_bulk_velocity (src/monitor.f90:463-523), FP64 compensated sum. */
 int dfdm_compute_bulk_velocity(dfdm_ctx *ctx, double *Ub);
 /* check_divergence (src/projection.f90:607-639): max |div u| over the interior. */

@@ -52,7 +52,8 @@ def test_footprint_scales_with_precision():
     c = cases.chan550()
     b64 = native.footprint_bytes(c, "fp64")
     b32 = native.footprint_bytes(c, "fp32")
-    assert 1.9 < b64 / b32 < 2.05
+    # the fields and the spectrum halve in FP32; the FP64 pivot table and the FP64 host staging do not
+    assert 1.75 < b64 / b32 < 2.0
     assert b32 < 2e9   # the 13M-cell throughput case fits easily in 180 GB
 
 

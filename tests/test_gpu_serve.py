@@ -19,3 +19,27 @@ def test_results_alone_equal_results_in_the_mix():
         for x, y in zip(a.state, b.state):
             assert np.array_equal(x, y), a.rid
         assert a.summary["kinetic_energy"] == b.summary["kinetic_energy"]
+
+
+@pytest.mark.parametrize("name,prec", [("chan180", "fp32"), ("chan180", "fp64"), ("tgv64", "fp32"), ("les395", "fp32")])
+def test_footprint_bounds_the_device_memory_of_a_context(name, prec):
+    """Admission relies on dfdm_footprint_bytes being an upper bound of what a stepping context holds."""
+    import torch
+    from dfdm import cases
+    from dfdm.native import Solver, footprint_bytes
+    warm = Solver(cases.get("chan_small"), "fp32")   # module and runtime set-up outside the measurement
+    c = cases.get(name)
+    U, V, W, P = cases.initial_condition(c)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    s = Solver(c, prec, graphs=True)
+    s.set_state(U, V, W, P)
+    s.compute_time_step_RK3(2)
+    s.get_state()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    used = free0 - free1
+    fp = footprint_bytes(c, prec)
+    s.close()
+    warm.close()
+    assert 0 < used <= 1.02 * fp + (8 << 20), (name, prec, used, fp)
