@@ -316,13 +316,15 @@ def main():
         b = s32.kernel_bytes(fam)
         kt[fam] = {"ms": ms, "alg_bytes": b, "GBps": b / (ms * 1e-3) / 1e9, "frac": b / (ms * 1e-3) / 1e9 / peak}
     dom = max(kt, key=lambda k: kt[k]["ms"])
+    # DRAM bytes (read + write) per launch of each kernel family from the committed ncu capture:
+    # lines "<config> <family> <bytes>" in profiles/traffic.txt
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    tfile = os.path.join(ROOT, "profiles", "traffic.txt")
     if os.path.exists(tfile):
-        try:
-            traffic = json.load(open(tfile)).get(c.name, {}).get(dom)
-        except Exception:
-            traffic = None
+        for line in open(tfile):
+            f = line.split()
+            if len(f) >= 3 and not line.startswith("#") and f[0] == c.name and f[1] == dom:
+                traffic = float(f[2])
     out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": kt[dom]["GBps"], "peak": peak, "unit": "GB/s",
                        "frac": kt[dom]["GBps"] / peak, "traffic": traffic, "peak_kind": peak_kind,
                        "alg_bytes_per_launch": kt[dom]["alg_bytes"], "avg_launch_ms": kt[dom]["ms"]}

@@ -88,6 +88,7 @@ struct dfdm_ctx {
     double *red_part = nullptr, *red_out = nullptr;
     int red_blocks = 0;
     unsigned long long *d_maxdiv = nullptr;
+    unsigned long long *d_cfl = nullptr;        // convective and viscous CFL maxima (bit patterns)
     int *d_flag = nullptr;
     double *staging = nullptr;
     size_t staging_n = 0;
@@ -97,7 +98,7 @@ struct dfdm_ctx {
     size_t smem_x = 0, smem_z = 0, smem_y = 0;
     // two-level register transforms (fft_reg.cuh) where the length has a split; Stockham otherwise
     bool x2 = false, z2 = false, y2 = false;
-    int lx2 = 1, thr_z2 = 256, thr_y2 = 256;
+    int lx2 = 1, lxi2 = 1, thr_z2 = 256, thr_y2 = 256;   // x lines per block: forward, inverse
     size_t smem_x2 = 0, smem_xi2 = 0, smem_z2 = 0, smem_y2 = 0;
     cudaStream_t own_stream = nullptr, stream = nullptr;
     double t = 0.0;
@@ -278,9 +279,10 @@ template <typename T> struct Impl {
         c->x2 = with_fft2l(d.Nx / 2, [&](auto n) {
             constexpr int N = decltype(n)::value;
             const size_t perline = (size_t)(RowLayout<N>::LDA + RowLayout<N>::LDT) * sizeof(C);
-            c->lx2 = (int)std::max<size_t>(1, std::min<size_t>(64, 73728 / perline));   // <= 72 KB: 3 blocks per SM
+            c->lx2 = RowLines<T, N>::value;   // the forward kernel's loop bound assumes exactly this
             c->smem_x2 = (size_t)c->lx2 * perline;
-            c->smem_xi2 = (size_t)c->lx2 * RowLayout<N>::LDT * sizeof(C);
+            c->lxi2 = (int)std::max<size_t>(1, std::min<size_t>(64, 73728 / perline));   // measured best for the inverse
+            c->smem_xi2 = (size_t)c->lxi2 * RowLayout<N>::LDT * sizeof(C);
             setattr((const void *)k_fwd_x2<T, true, N>, c->smem_x2);
             setattr((const void *)k_fwd_x2<T, false, N>, c->smem_x2);
             setattr((const void *)k_inv_x2<T, N>, c->smem_xi2);
@@ -350,10 +352,18 @@ template <typename T> struct Impl {
         int dev = 0, nsm = 148, occ = 1;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        if (c->les) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tiled<T, true, TILE_X, TILE_Y, 0>, TILE_X * TILE_Y, 0));
-        else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tiled<T, false, TILE_X, TILE_Y, 0>, TILE_X * TILE_Y, 0));
+        const void *stage_fn;
+        if constexpr (sizeof(T) == 8)
+            stage_fn = c->les ? (const void *)k_tiled<T, true, true, TILE_X, TILE_Y, 0>
+                              : (const void *)k_tiled<T, false, true, TILE_X, TILE_Y, 0>;
+        else
+            stage_fn = c->les ? (c->wm ? (const void *)k_tiled<T, true, true, TILE_X, TILE_Y, 0>
+                                       : (const void *)k_tiled<T, true, false, TILE_X, TILE_Y, 0>)
+                              : (c->wm ? (const void *)k_tiled<T, false, true, TILE_X, TILE_Y, 0>
+                                       : (const void *)k_tiled<T, false, false, TILE_X, TILE_Y, 0>);
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, stage_fn, TILE_X * TILE_Y, 0));
         c->kc_stage = choose_kc(d, occ, nsm);
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tiled<T, false, TILE_X, TILE_Y, 1>, TILE_X * TILE_Y, 0));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tiled<T, false, false, TILE_X, TILE_Y, 1>, TILE_X * TILE_Y, 0));
         c->kc_sgs = choose_kc(d, occ, nsm);
         return setup_fft2l(c);
     }
@@ -367,17 +377,21 @@ template <typename T> struct Impl {
         return sizeof(T) == 4 && s == 3 && c->projected && !c->unit_projection;
     }
 
+    template <bool LES, bool WM> static void stage_launch(dfdm_ctx *c, dim3 g, const StageCoef &sc, T *rhs_only) {
+        k_tiled<T, LES, WM, TILE_X, TILE_Y, 0><<<g, TILE_X * TILE_Y, 0, c->stream>>>(step_args<T>(c), f(c->u), f(c->v),
+            f(c->w), LES ? f(c->nut) : nullptr, c->wsd.tau_x, c->wsd.tau_z, sc, c->kc_stage, f(c->uo), f(c->vo), f(c->wo),
+            f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf), rhs_only, nullptr);
+    }
+
     static int stage_kernel(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
         const Dims &d = c->d;
         dim3 g = tile_grid(d, c->kc_stage);
-        if (c->les)
-            k_tiled<T, true, TILE_X, TILE_Y, 0><<<g, TILE_X * TILE_Y, 0, c->stream>>>(step_args<T>(c), f(c->u), f(c->v),
-                f(c->w), f(c->nut), c->wsd.tau_x, c->wsd.tau_z, sc, c->kc_stage, f(c->uo), f(c->vo), f(c->wo), f(c->f1u),
-                f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf), rhs_only, nullptr);
-        else
-            k_tiled<T, false, TILE_X, TILE_Y, 0><<<g, TILE_X * TILE_Y, 0, c->stream>>>(step_args<T>(c), f(c->u), f(c->v),
-                f(c->w), nullptr, c->wsd.tau_x, c->wsd.tau_z, sc, c->kc_stage, f(c->uo), f(c->vo), f(c->wo), f(c->f1u),
-                f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf), rhs_only, nullptr);
+        if constexpr (sizeof(T) == 8) {   // FP64 keeps the runtime wall-model flag
+            if (c->les) stage_launch<true, true>(c, g, sc, rhs_only); else stage_launch<false, true>(c, g, sc, rhs_only);
+        } else {
+            if (c->les) { if (c->wm) stage_launch<true, true>(c, g, sc, rhs_only); else stage_launch<true, false>(c, g, sc, rhs_only); }
+            else { if (c->wm) stage_launch<false, true>(c, g, sc, rhs_only); else stage_launch<false, false>(c, g, sc, rhs_only); }
+        }
         CKL();
         return DFDM_OK;
     }
@@ -390,7 +404,7 @@ template <typename T> struct Impl {
         case 0: {   // SGS
             if (!c->les) return DFDM_OK;
             StageCoef sc{1, 0.0, 0.0, 0.0, 0.0, 0};
-            k_tiled<T, false, TILE_X, TILE_Y, 1><<<tile_grid(d, c->kc_sgs), TILE_X * TILE_Y, 0, st>>>(
+            k_tiled<T, false, false, TILE_X, TILE_Y, 1><<<tile_grid(d, c->kc_sgs), TILE_X * TILE_Y, 0, st>>>(
                 step_args<T>(c), f(c->u), f(c->v), f(c->w), nullptr, nullptr, nullptr, sc, c->kc_sgs, nullptr, nullptr,
                 nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, f(c->nut));
             CKL();
@@ -467,10 +481,10 @@ template <typename T> struct Impl {
         case 6: {   // inverse x
             long long lines = (long long)d.Ny * d.Nz;
             if (c->x2) {
-                int nb = (int)((lines + c->lx2 - 1) / c->lx2);
+                int nb = (int)((lines + c->lxi2 - 1) / c->lxi2);
                 with_fft2l(d.Nx / 2, [&](auto n) {
                     constexpr int N = decltype(n)::value;
-                    k_inv_x2<T, N><<<nb, 256, c->smem_xi2, st>>>(poisson_args<T>(c), c->lx2, (const C *)c->spec, f(c->phi),
+                    k_inv_x2<T, N><<<nb, 256, c->smem_xi2, st>>>(poisson_args<T>(c), c->lxi2, (const C *)c->spec, f(c->phi),
                                                                   (const C *)c->tw_x, (const C *)c->twr_x);
                 });
             } else {
@@ -502,7 +516,7 @@ template <typename T> struct Impl {
             if (c->prm.flow_forcing_mode != 1) return DFDM_OK;
             k_bulk_partial<T><<<c->red_blocks, 256, 0, st>>>(d, f(c->u), c->d_dyc, c->d_dzc, c->d_ubd, c->red_part);
             CKL();
-            k_bulk_final<<<1, 32, 0, st>>>(c->red_blocks, c->red_part, c->prm.Ub_target, c->red_out);
+            k_bulk_final<<<1, 256, 0, st>>>(c->red_blocks, c->red_part, c->prm.Ub_target, c->red_out);
             CKL();
             k_shift<T><<<c->red_blocks, 256, 0, st>>>(d, f(c->u), c->red_out);
             CKL();
@@ -858,6 +872,8 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
     c->red_out = (double *)tmp;
     if ((rc = dalloc(c, &tmp, sizeof(unsigned long long)))) return bail(rc);
     c->d_maxdiv = (unsigned long long *)tmp;
+    if ((rc = dalloc(c, &tmp, 2 * sizeof(unsigned long long)))) return bail(rc);
+    c->d_cfl = (unsigned long long *)tmp;
     if ((rc = dalloc(c, &tmp, sizeof(int)))) return bail(rc);
     c->d_flag = (int *)tmp;
     c->in_create = false;   // later buffers (host staging, the unit RHS output) are separate allocations
@@ -1434,7 +1450,7 @@ int dfdm_compute_bulk_velocity(dfdm_ctx *c, double *Ub) {
         typedef typename std::remove_pointer<decltype(I::f(nullptr))>::type T;
         k_bulk_partial<T><<<c->red_blocks, 256, 0, c->stream>>>(c->d, I::f(c->u), c->d_dyc, c->d_dzc, c->d_ubd, c->red_part);
         CKL();
-        k_bulk_final<<<1, 32, 0, c->stream>>>(c->red_blocks, c->red_part, 0.0, c->red_out);
+        k_bulk_final<<<1, 256, 0, c->stream>>>(c->red_blocks, c->red_part, 0.0, c->red_out);
         CKL();
         return DFDM_OK;
     });
@@ -1462,6 +1478,30 @@ int dfdm_check_divergence(dfdm_ctx *c, double *max_div) {
     CK(cudaMemcpyAsync(&bits, c->d_maxdiv, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     std::memcpy(max_div, &bits, sizeof(double));
+    return DFDM_OK;
+}
+
+int dfdm_compute_cfl(dfdm_ctx *c, double *cfl_conv, double *cfl_visc) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (!cfl_conv || !cfl_visc) return fail(DFDM_ERR_INVALID, "null output");
+    CK(cudaMemsetAsync(c->d_cfl, 0, 2 * sizeof(unsigned long long), c->stream));
+    int rc = dispatch(c, [&](auto impl) {
+        typedef decltype(impl) I;
+        k_cfl<typename std::remove_pointer<decltype(I::f(nullptr))>::type><<<c->red_blocks, 256, 0, c->stream>>>(
+            c->d, I::f(c->u), I::f(c->v), I::f(c->w), c->les ? I::f(c->nut) : nullptr, c->d_ubd, 1.0 / c->dx, c->d_dyc,
+            c->d_dzc, c->prm.nu, c->d_cfl);
+        CKL();
+        return DFDM_OK;
+    });
+    if (rc) return rc;
+    unsigned long long bits[2] = {0, 0};
+    CK(cudaMemcpyAsync(bits, c->d_cfl, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    double m[2];
+    std::memcpy(m, bits, sizeof(m));
+    *cfl_conv = m[0] * c->prm.dt;
+    *cfl_visc = m[1] * c->prm.dt;
     return DFDM_OK;
 }
 

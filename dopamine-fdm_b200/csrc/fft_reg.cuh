@@ -123,6 +123,12 @@ template <int N> struct RowLayout {
     static constexpr int LDT = pad8(N1 * (N2 + 1));
 };
 
+// x lines per block of the row transforms: as many as fit in 56 KB of shared memory (4 blocks of 256 threads per SM)
+template <typename T, int N> struct RowLines {
+    static constexpr int bytes = (RowLayout<N>::LDA + RowLayout<N>::LDT) * 2 * (int)sizeof(T);
+    static constexpr int value = (57344 / bytes) < 1 ? 1 : ((57344 / bytes) > 64 ? 64 : (57344 / bytes));
+};
+
 // Step 1 of a row transform for one (line, n2) item: v holds x[n1*N2 + n2], n1 = 0..N1-1, on entry; the twiddled
 // step-1 outputs go to t (layout LDT).
 template <typename T, bool INV, int N>

@@ -40,32 +40,41 @@ __device__ __forceinline__ void block_sum2(double a, double b, double *out) {
 }
 
 // compute_bulk_velocity (src/monitor.f90:463-523): sum of 0.5 (U_i + U_{i-1}) dy_j dz_k over the independent
-// cells and of the weights dy_j dz_k, one partial pair per block (deterministic, no atomics).
+// cells and of the weights dy_j dz_k, one partial pair per block (deterministic, no atomics).  A block walks whole
+// x-rows (row = k*Ny + j, uniform over the block), so no per-cell index division is needed.
 template <typename T>
 __global__ void __launch_bounds__(256) k_bulk_partial(Dims d, const T *__restrict__ U, const double *__restrict__ dyc,
                                                       const double *__restrict__ dzc, const double *__restrict__ ubd,
                                                       double *__restrict__ part) {
     Kahan s, w; s.init(); w.init();
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x) {
-        int i = (int)(p % d.Nx);
-        long long q = p / d.Nx;
-        int j = (int)(q % d.Ny), k = (int)(q / d.Ny);
-        double a = dyc[j] * dzc[k];
-        double u0 = (double)U[p] + ubd[j], um = (double)U[idx3(d, wrap(i - 1, d.Nx), j, k)] + ubd[j];
-        s.add(0.5 * (u0 + um) * a);
-        w.add(a);
+    const int rows = d.Ny * d.Nz, Nx = d.Nx;
+    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int k = row / d.Ny, j = row - k * d.Ny;
+        const double a = dyc[j] * dzc[k], ub = ubd[j];
+        const T *Ur = U + (size_t)row * Nx;
+        for (int i = threadIdx.x; i < Nx; i += blockDim.x) {
+            const double u0 = (double)Ur[i] + ub, um = (double)Ur[i == 0 ? Nx - 1 : i - 1] + ub;
+            s.add(0.5 * (u0 + um) * a);
+            w.add(a);
+        }
     }
     block_sum2(s.s, w.s, part);
 }
 
-// Final pass over the block partials in a fixed order; writes Ub and the shift Ub_target - Ub.
-__global__ void k_bulk_final(int nparts, const double *__restrict__ part, double Ub_target, double *__restrict__ out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// Final pass over the block partials (one block): compensated per-thread sums in a fixed order, then a fixed tree;
+// writes Ub and the shift Ub_target - Ub.
+__global__ void __launch_bounds__(256) k_bulk_final(int nparts, const double *__restrict__ part, double Ub_target,
+                                                    double *__restrict__ out) {
+    __shared__ double tot[2];
     Kahan s, w; s.init(); w.init();
-    for (int b = 0; b < nparts; ++b) { s.add(part[2 * b]); w.add(part[2 * b + 1]); }
-    double Ub = s.s / fmax(w.s, 1e-14);
-    out[0] = Ub;
-    out[1] = Ub_target - Ub;
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x) { s.add(part[2 * b]); w.add(part[2 * b + 1]); }
+    block_sum2(s.s, w.s, tot);   // gridDim.x == 1: writes tot[0], tot[1]
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double Ub = tot[0] / fmax(tot[1], 1e-14);
+        out[0] = Ub;
+        out[1] = Ub_target - Ub;
+    }
 }
 
 // U += (Ub_target - Ub) on every independent U face (src/time_integration.f90:581-583).
@@ -96,6 +105,39 @@ __global__ void __launch_bounds__(256) k_maxdiv(Dims d, const T *__restrict__ U,
     }
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// compute_cfl (src/monitor.f90:304-424) without its IBM, buoyancy, rotation and actuator terms: the maxima over the
+// centres of |u_c|/dx + |v_c|/dy_j + |w_c|/dz_k (face velocities averaged to the centre) and of
+// (nu + nu_t) 2 (1/dx^2 + 1/dy_j^2 + 1/dz_k^2), in double, as exact integer maxima of their bit patterns.
+template <typename T>
+__global__ void __launch_bounds__(256) k_cfl(Dims d, const T *__restrict__ U, const T *__restrict__ V,
+                                             const T *__restrict__ W, const T *__restrict__ NU,
+                                             const double *__restrict__ ubd, double inv_dx, const double *__restrict__ dyc,
+                                             const double *__restrict__ dzc, double nu, unsigned long long *__restrict__ out) {
+    double mc = 0.0, mv = 0.0;
+    const double idx2 = inv_dx * inv_dx;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(p % d.Nx);
+        long long q = p / d.Nx;
+        int j = (int)(q % d.Ny), k = (int)(q / d.Ny);
+        const double ub = ubd[j];
+        const double uc = 0.5 * (((double)U[p] + ub) + ((double)U[idx3(d, wrap(i - 1, d.Nx), j, k)] + ub));
+        const double vc = 0.5 * ((double)ld_yf(V, d, i, j, k) + (double)ld_yf(V, d, i, j - 1, k));
+        const double wc = 0.5 * ((double)W[p] + (double)W[idx3(d, i, j, wrap(k - 1, d.Nz))]);
+        const double idy = 1.0 / fmax(dyc[j], 1e-14), idz = 1.0 / fmax(dzc[k], 1e-14);
+        mc = fmax(mc, fabs(uc) * inv_dx + fabs(vc) * idy + fabs(wc) * idz);
+        const double nt = NU ? (double)NU[p] : 0.0;
+        mv = fmax(mv, (nu + nt) * 2.0 * (idx2 + idy * idy + idz * idz));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mc = fmax(mc, __shfl_down_sync(0xffffffffu, mc, o));
+        mv = fmax(mv, __shfl_down_sync(0xffffffffu, mv, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(out, (unsigned long long)__double_as_longlong(mc));
+        atomicMax(out + 1, (unsigned long long)__double_as_longlong(mv));
+    }
 }
 
 // Volume-weighted kinetic energy 0.5 <u.u> with face velocities averaged to the centres (compensated sums).

@@ -37,7 +37,11 @@ __global__ void __launch_bounds__(256) k_fwd_x2(PoissonArgs<T> a, int lx, const 
     const int Ny = d.Ny, Nz = d.Nz, plane = Nx * Ny;
     const int line0 = blockIdx.x * lx;
     const int nl = min(lx, Ny * Nz - line0);
-    for (int e = threadIdx.x; e < nl * M; e += blockDim.x) {
+    constexpr int ITEMS = RowLines<T, M>::value * M;   // lx == RowLines<T, M>::value, blockDim.x == 256
+#pragma unroll 4
+    for (int e0 = 0; e0 < ITEMS; e0 += 256) {
+        const int e = e0 + threadIdx.x;
+        if (e >= nl * M) break;
         const int ll = e / M, n = e - ll * M;
         const int line = line0 + ll;
         C z;

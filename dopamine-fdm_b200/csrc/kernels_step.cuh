@@ -216,14 +216,14 @@ template <> struct AxisLocal<double> {
 // `q` is a neighbourhood accessor: q.U(di,dj,dk) is U at (i+di, j+dj, k+dk) with every boundary rule already
 // applied (periodic wraps, no-slip mirror, zero wall faces, zero nu_t ghosts), so the formulas below see the
 // same values the reference reads from its ghosted arrays.
-template <typename T, bool LES, typename Q>
+template <typename T, bool LES, bool WM, typename Q>
 __device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Q &q, const AxisLocal<T> &Y, const AxisLocal<T> &Z,
                                     const double *__restrict__ tau_x, int i, int j, int k) {
     const Dims &d = a.d;
     typedef Arith<T> A;
     T Uc = q.U(0, 0, 0), Uim = q.U(-1, 0, 0), Uip = q.U(1, 0, 0);
     T Ujm = q.U(0, -1, 0), Ujp = q.U(0, 1, 0), Ukm = q.U(0, 0, -1), Ukp = q.U(0, 0, 1);
-    bool wm_band = a.wm && (j + 2 <= 1 + a.nwl || j + 2 >= d.Ny + 2 - a.nwl);
+    bool wm_band = WM && a.wm && (j + 2 <= 1 + a.nwl || j + 2 >= d.Ny + 2 - a.nwl);
     T wa = wm_band ? T(0) : a.w_adv, wd = T(1) - wa;
     // -d(uu)/dx
     T r;
@@ -274,7 +274,7 @@ __device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Q &q, const Ax
     T tj = Y.divf(Ujp - Uc), tjm = Y.divfm(Uc - Ujm);
     T fy2 = nu_y2 * (tj + (V10 - V00) * a.inv_dx);
     T fy1 = nu_y1 * (tjm + (V1m - V0m) * a.inv_dx);
-    if (a.wm) {
+    if (WM && a.wm) {
         if (j == 0) fy1 = (T)tau_x[k * d.Nx + i];
         if (j == d.Ny - 1) fy2 = (T)tau_x[(d.Nz + k) * d.Nx + i];
     }
@@ -291,7 +291,7 @@ __device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Q &q, const Ax
     return r;
 }
 
-template <typename T, bool LES, typename Q>
+template <typename T, bool LES, bool WM, typename Q>
 __device__ __forceinline__ T rhs_v_at(const StepArgs<T> &a, const Q &q, const AxisLocal<T> &Y, const AxisLocal<T> &Z, int i, int j, int k) {
     const Dims &d = a.d;
     typedef Arith<T> A;
@@ -346,12 +346,12 @@ __device__ __forceinline__ T rhs_v_at(const StepArgs<T> &a, const Q &q, const Ax
     return r;
 }
 
-template <typename T, bool LES, typename Q>
+template <typename T, bool LES, bool WM, typename Q>
 __device__ __forceinline__ T rhs_w_at(const StepArgs<T> &a, const Q &q, const AxisLocal<T> &Y, const AxisLocal<T> &Z,
                                     const double *__restrict__ tau_z, int i, int j, int k) {
     const Dims &d = a.d;
     typedef Arith<T> A;
-    bool wm_band = a.wm && (j + 2 <= 1 + a.nwl || j + 2 >= d.Ny + 2 - a.nwl);
+    bool wm_band = WM && a.wm && (j + 2 <= 1 + a.nwl || j + 2 >= d.Ny + 2 - a.nwl);
     T wa = wm_band ? T(0) : a.w_adv, wd = T(1) - wa;
     T Wc = q.W(0, 0, 0), Wkm = q.W(0, 0, -1), Wkp = q.W(0, 0, 1);
     T Wim = q.W(-1, 0, 0), Wip = q.W(1, 0, 0), Wjm = q.W(0, -1, 0), Wjp = q.W(0, 1, 0);
@@ -398,7 +398,7 @@ __device__ __forceinline__ T rhs_w_at(const StepArgs<T> &a, const Q &q, const Ax
     T tj = Y.divf(Wjp - Wc), tjm = Y.divfm(Wc - Wjm);
     T fy2 = nu_y2 * (tj + (Vkp - Vc) * inv_dz3);
     T fy1 = nu_y1 * (tjm + (Vjmkp - Vjm) * inv_dz3);
-    if (a.wm) {
+    if (WM && a.wm) {
         if (j == 0) fy1 = (T)tau_z[k * d.Nx + i];
         if (j == d.Ny - 1) fy2 = (T)tau_z[(d.Nz + k) * d.Nx + i];
     }
@@ -451,7 +451,9 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // rules (no-slip mirror of U and W, zero V and nu_t on the ghost rows).  Every thread then evaluates the three
 // right-hand sides of its cell from shared memory and writes the RK3 update (or, with rhs_only, the right-hand
 // sides themselves for the unit entry point; with KIND 1, nu_t).
-template <typename T, bool LES, int TX, int TY, int KIND>
+// WM = false compiles the flat-wall model out; with WM = true the runtime flag StepArgs::wm decides (the FP64 form
+// always takes that variant: without the branches its register allocation spills).
+template <typename T, bool LES, bool WM, int TX, int TY, int KIND>
 __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepArgs<T> a, const T *__restrict__ U, const T *__restrict__ V,
                                                   const T *__restrict__ W, const T *__restrict__ NU,
                                                   const double *__restrict__ tau_x, const double *__restrict__ tau_z,
@@ -570,9 +572,9 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
                 }
                 AxisLocal<T> Z;
                 Z.load(a.mz, k);
-                T ru = rhs_u_at<T, LES>(a, q, Y, Z, tau_x, i, j, k);
-                T rw = rhs_w_at<T, LES>(a, q, Y, Z, tau_z, i, j, k);
-                T rv = vrow ? rhs_v_at<T, LES>(a, q, Y, Z, i, j, k) : T(0);
+                T ru = rhs_u_at<T, LES, WM>(a, q, Y, Z, tau_x, i, j, k);
+                T rw = rhs_w_at<T, LES, WM>(a, q, Y, Z, tau_z, i, j, k);
+                T rv = vrow ? rhs_v_at<T, LES, WM>(a, q, Y, Z, i, j, k) : T(0);
                 if (rhs_only) {
                     rhs_only[p] = ru; rhs_only[d.cells + p] = rv; rhs_only[2 * d.cells + p] = rw;
                 } else if (sc.stage == 1) {

@@ -30,7 +30,8 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_compute_wall_model", "dfdm_apply_boundary_conditions", "dfdm_compute_projection_step",
            "dfdm_solve_poisson", "dfdm_compute_bulk_velocity", "dfdm_check_divergence", "dfdm_kinetic_energy",
            "dfdm_check_finite", "dfdm_pad_field", "dfdm_launch_kernel_async", "dfdm_kernel_bytes",
-           "dfdm_launch_count", "dfdm_solve_poisson_noalloc", "dfdm_write_snapshot", "dfdm_read_snapshot"]
+           "dfdm_launch_count", "dfdm_solve_poisson_noalloc", "dfdm_write_snapshot", "dfdm_read_snapshot",
+           "dfdm_compute_cfl"]
 
 
 class DfdmError(RuntimeError):
@@ -90,6 +91,7 @@ def load(build_if_missing: bool = True):
         "dfdm_solve_poisson_noalloc": (c_int, [c_void_p, P, P]),
         "dfdm_write_snapshot": (c_int, [c_void_p, c_char_p]),
         "dfdm_read_snapshot": (c_int, [c_void_p, c_char_p]),
+        "dfdm_compute_cfl": (c_int, [c_void_p, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -255,6 +257,12 @@ class Solver:
         v = c_double(0.0)
         _check(load().dfdm_check_divergence(self.h, ctypes.byref(v)))
         return v.value
+
+    def compute_cfl(self):
+        """(convective, viscous) CFL numbers of the resident state, as compute_cfl (src/monitor.f90:304)."""
+        a, b = c_double(0.0), c_double(0.0)
+        _check(load().dfdm_compute_cfl(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
     def kinetic_energy(self) -> float:
         v = c_double(0.0)

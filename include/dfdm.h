@@ -164,6 +164,9 @@ int dfdm_read_snapshot(dfdm_ctx *ctx, const char *path);
 int dfdm_compute_bulk_velocity(dfdm_ctx *ctx, double *Ub);
 /* check_divergence (src/projection.f90:607-639): max |div u| over the interior. */
 int dfdm_check_divergence(dfdm_ctx *ctx, double *max_div);
+/* compute_cfl (src/monitor.f90:304-424) for the single-phase path: dt * max over the centres of
+ * |u_c|/dx + |v_c|/dy + |w_c|/dz (convective) and of (nu + nu_t) * 2 * (1/dx^2 + 1/dy^2 + 1/dz^2) (viscous). */
+int dfdm_compute_cfl(dfdm_ctx *ctx, double *cfl_conv, double *cfl_visc);
 /* Kinetic energy 0.5*<u.u> (volume-weighted, compensated sum) -- diagnostic with no reference counterpart. */
 int dfdm_kinetic_energy(dfdm_ctx *ctx, double *ke);
 /* Monitor guard of output_monitor (src/monitor.f90:32-52): DFDM_ERR_NOT_FINITE if any velocity is NaN/Inf or
