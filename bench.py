@@ -271,13 +271,16 @@ def main():
         return s, max_over_ranks(ms), clocks, launches
 
     s32, ms32, clocks, launches = timed_run("fp32", sample_clocks=True)
+    variant, ms_one, ms_pairs = s32.stage_variant()
     value = ws * c.n_cells * args.steps / (ms32 / 1e3)
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "fp32-mixed (FP32 fields/stencils/FFTs, FP64 y-solves and reductions)",
            "data": "synthetic: seeded laminar Poiseuille + 10% uniform noise, no dataset",
            "config": config_dict(c, {"parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"}),
-           "clocks": clocks, "gpu_launches": launches}
+           "clocks": clocks, "gpu_launches": launches,
+           "tuning": {"stage_kernel": ["one cell per thread", "packed FP32x2 pairs"][variant],
+                      "stage_ms_one_cell": ms_one, "stage_ms_packed_pairs": ms_pairs}}
 
     # ---- plain FP64 form and the FP32-vs-FP64 error after warmup + K steps from the same state ----
     if not args.no_fp64:

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
+#include <map>
 #include <cmath>
 #include <cstdio>
 #include <cstdint>
@@ -26,6 +28,13 @@ namespace {
 
 thread_local std::string g_err;
 thread_local long long g_launches = 0;   // kernels enqueued by this thread (read back into the context)
+
+struct TuneEntry {
+    int variant;
+    double ms[2];
+};
+std::mutex g_tune_mu;
+std::map<std::array<int, 6>, TuneEntry> g_tune;   // stage-kernel choice per (device, Nx, Ny, Nz, LES, wall model)
 
 int fail(int code, const std::string &msg) {
     g_err = msg;
@@ -95,6 +104,9 @@ struct dfdm_ctx {
     // launch geometry
     int lx = 8, tzx = 8;
     int kc_stage = 8, kc_sgs = 8;               // z-planes per block of the tiled kernels
+    int kc_stage2 = 8;                          // the same for the packed FP32 stage kernel
+    int stage_variant = 0;                      // FP32 stage kernel in use: 0 one cell per thread, 1 packed pairs
+    double stage_ms[2] = {-1.0, -1.0};          // autotuner timings of the two variants (ms per launch), -1 = not timed
     size_t smem_x = 0, smem_z = 0, smem_y = 0;
     // two-level register transforms (fft_reg.cuh) where the length has a split; Stockham otherwise
     bool x2 = false, z2 = false, y2 = false;
@@ -250,10 +262,11 @@ template <typename T> PoissonArgs<T> poisson_args(dfdm_ctx *c) {
 dim3 cell_grid(const Dims &d) { return dim3((d.Nx + 31) / 32, (d.Ny + 7) / 8, d.Nz); }
 const dim3 CELL_BLOCK(32, 8, 1);
 constexpr int TILE_X = 32, TILE_Y = 8;   // (i,j) tile of the 2.5-D blocked kernels
-dim3 tile_grid(const Dims &d, int kc) { return dim3((d.Nx + TILE_X - 1) / TILE_X, (d.Ny + TILE_Y - 1) / TILE_Y, (d.Nz + kc - 1) / kc); }
+const int TILE_X2 = 64;   // x cells per block of the packed FP32 stage kernel (32 threads x 2 cells)
+dim3 tile_grid(const Dims &d, int kc, int tx = TILE_X) { return dim3((d.Nx + tx - 1) / tx, (d.Ny + TILE_Y - 1) / TILE_Y, (d.Nz + kc - 1) / kc); }
 // z-planes per block: enough blocks for about four waves at the measured occupancy, at most 32 planes
-int choose_kc(const Dims &d, int blocks_per_sm, int nsm) {
-    long long cols = (long long)((d.Nx + TILE_X - 1) / TILE_X) * ((d.Ny + TILE_Y - 1) / TILE_Y);
+int choose_kc(const Dims &d, int blocks_per_sm, int nsm, int tx = TILE_X) {
+    long long cols = (long long)((d.Nx + tx - 1) / tx) * ((d.Ny + TILE_Y - 1) / TILE_Y);
     long long want = 4LL * nsm * std::max(1, blocks_per_sm);
     long long chunks = std::max(1LL, (want + cols - 1) / cols);
     int kc = (int)((d.Nz + chunks - 1) / chunks);
@@ -363,6 +376,13 @@ template <typename T> struct Impl {
                                        : (const void *)k_tiled<T, false, false, TILE_X, TILE_Y, 0>);
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, stage_fn, TILE_X * TILE_Y, 0));
         c->kc_stage = choose_kc(d, occ, nsm);
+        if constexpr (sizeof(T) == 4) {
+            const void *fn2 = c->les ? (c->wm ? (const void *)k_tiled2<true, true> : (const void *)k_tiled2<true, false>)
+                                     : (c->wm ? (const void *)k_tiled2<false, true> : (const void *)k_tiled2<false, false>);
+            int occ2 = 1;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, fn2, 256, 0));
+            c->kc_stage2 = choose_kc(d, occ2, nsm, TILE_X2);
+        }
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tiled<T, false, false, TILE_X, TILE_Y, 1>, TILE_X * TILE_Y, 0));
         c->kc_sgs = choose_kc(d, occ, nsm);
         return setup_fft2l(c);
@@ -377,22 +397,73 @@ template <typename T> struct Impl {
         return sizeof(T) == 4 && s == 3 && c->projected && !c->unit_projection;
     }
 
-    template <bool LES, bool WM> static void stage_launch(dfdm_ctx *c, dim3 g, const StageCoef &sc, T *rhs_only) {
-        k_tiled<T, LES, WM, TILE_X, TILE_Y, 0><<<g, TILE_X * TILE_Y, 0, c->stream>>>(step_args<T>(c), f(c->u), f(c->v),
-            f(c->w), LES ? f(c->nut) : nullptr, c->wsd.tau_x, c->wsd.tau_z, sc, c->kc_stage, f(c->uo), f(c->vo), f(c->wo),
-            f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf), rhs_only, nullptr);
+    template <bool LES, bool WM> static void stage_launch(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
+        const Dims &d = c->d;
+        if constexpr (sizeof(T) == 4) {
+            if (c->stage_variant == 1) {
+                k_tiled2<LES, WM><<<tile_grid(d, c->kc_stage2, TILE_X2), 256, 0, c->stream>>>(step_args<T>(c), f(c->u),
+                    f(c->v), f(c->w), LES ? f(c->nut) : nullptr, c->wsd.tau_x, c->wsd.tau_z, sc, c->kc_stage2, f(c->uo),
+                    f(c->vo), f(c->wo), f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf), rhs_only);
+                return;
+            }
+        }
+        k_tiled<T, LES, WM, TILE_X, TILE_Y, 0><<<tile_grid(d, c->kc_stage), TILE_X * TILE_Y, 0, c->stream>>>(
+            step_args<T>(c), f(c->u), f(c->v), f(c->w), LES ? f(c->nut) : nullptr, c->wsd.tau_x, c->wsd.tau_z, sc,
+            c->kc_stage, f(c->uo), f(c->vo), f(c->wo), f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf),
+            rhs_only, nullptr);
     }
 
     static int stage_kernel(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
-        const Dims &d = c->d;
-        dim3 g = tile_grid(d, c->kc_stage);
         if constexpr (sizeof(T) == 8) {   // FP64 keeps the runtime wall-model flag
-            if (c->les) stage_launch<true, true>(c, g, sc, rhs_only); else stage_launch<false, true>(c, g, sc, rhs_only);
+            if (c->les) stage_launch<true, true>(c, sc, rhs_only); else stage_launch<false, true>(c, sc, rhs_only);
         } else {
-            if (c->les) { if (c->wm) stage_launch<true, true>(c, g, sc, rhs_only); else stage_launch<true, false>(c, g, sc, rhs_only); }
-            else { if (c->wm) stage_launch<false, true>(c, g, sc, rhs_only); else stage_launch<false, false>(c, g, sc, rhs_only); }
+            if (c->les) { if (c->wm) stage_launch<true, true>(c, sc, rhs_only); else stage_launch<true, false>(c, sc, rhs_only); }
+            else { if (c->wm) stage_launch<false, true>(c, sc, rhs_only); else stage_launch<false, false>(c, sc, rhs_only); }
         }
         CKL();
+        return DFDM_OK;
+    }
+
+    // Autotuner of the FP32 stage kernel: times both variants on this grid (a stage-2 launch, 2 warm-up + 5 timed)
+    // and keeps the faster.  The choice is cached per device, grid shape and model flags for the process, so a
+    // serving loop that opens many contexts of one shape pays the timing once.
+    static int tune_stage(dfdm_ctx *c, bool force) {
+        if constexpr (sizeof(T) == 8) { (void)force; c->stage_variant = 0; return DFDM_OK; }
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        const std::array<int, 6> key = {dev, c->d.Nx, c->d.Ny, c->d.Nz, c->les, c->wm};
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            auto it = g_tune.find(key);
+            if (it != g_tune.end() && !force) {
+                c->stage_variant = it->second.variant;
+                c->stage_ms[0] = it->second.ms[0]; c->stage_ms[1] = it->second.ms[1];
+                return DFDM_OK;
+            }
+        }
+        StageCoef sc{2, 0.0, c->prm.dt, 0.25, 5.0 / 12.0, 0};
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        int rc = DFDM_OK;
+        for (int v = 0; v < 2 && !rc; ++v) {
+            c->stage_variant = v;
+            for (int r = 0; r < 2 && !rc; ++r) rc = stage_kernel(c, sc, nullptr);
+            if (rc) break;
+            cudaEventRecord(e0, c->stream);
+            for (int r = 0; r < 5 && !rc; ++r) rc = stage_kernel(c, sc, nullptr);
+            cudaEventRecord(e1, c->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail(DFDM_ERR_CUDA, "stage-kernel tuning failed");
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            c->stage_ms[v] = ms / 5.0;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (rc) return rc;
+        c->stage_variant = c->stage_ms[1] < c->stage_ms[0] ? 1 : 0;
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune[key] = TuneEntry{c->stage_variant, {c->stage_ms[0], c->stage_ms[1]}};
         return DFDM_OK;
     }
 
@@ -879,6 +950,8 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
     c->in_create = false;   // later buffers (host staging, the unit RHS output) are separate allocations
 
     rc = dispatch(c, [&](auto impl) { return decltype(impl)::setup_kernels(c); });
+    if (rc) return bail(rc);
+    rc = dispatch(c, [&](auto impl) { return decltype(impl)::tune_stage(c, false); });   // on the zeroed fields
     if (rc) return bail(rc);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(DFDM_ERR_CUDA, "set-up synchronisation failed"));
     *out = c;
@@ -1560,6 +1633,25 @@ int dfdm_launch_kernel_async(dfdm_ctx *c, int which, int rk_stage) {
     int rc = dispatch(c, [&](auto impl) { return decltype(impl)::launch(c, which, rk_stage); });
     c->launches += g_launches - before;
     return rc;
+}
+
+int dfdm_set_stage_variant(dfdm_ctx *c, int variant) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (variant < -1 || variant > 1) return fail(DFDM_ERR_INVALID, "stage variant must be -1, 0 or 1");
+    if (variant == 1 && c->prec == DFDM_FP64) return fail(DFDM_ERR_UNSUPPORTED, "the packed stage kernel is FP32 only");
+    CK(cudaStreamSynchronize(c->stream));
+    destroy_graph(c);   // the captured step holds the previous kernel
+    if (variant >= 0) { c->stage_variant = variant; return DFDM_OK; }
+    return dispatch(c, [&](auto impl) { return decltype(impl)::tune_stage(c, true); });
+}
+
+int dfdm_get_stage_variant(dfdm_ctx *c, int *variant, double *ms_one, double *ms_pairs) {
+    if (int rc = check_ctx(c)) return rc;
+    if (variant) *variant = c->stage_variant;
+    if (ms_one) *ms_one = c->stage_ms[0];
+    if (ms_pairs) *ms_pairs = c->stage_ms[1];
+    return DFDM_OK;
 }
 
 int dfdm_launch_count(dfdm_ctx *c, long long *count) {

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "dfdm_common.cuh"
+#include "f32x2.cuh"
 
 namespace dfdm {
 
@@ -195,6 +196,24 @@ template <> struct AxisLocal<float> {
     __device__ __forceinline__ float invf() const { return idf_; }
     __device__ __forceinline__ float invfm() const { return idfm_; }
 };
+template <> struct AxisLocal<F2> {   // packed pairs: the same metrics broadcast to both lanes, read once
+    F2 w0m_, w1m_, w0_, w1_, idc_, idcp_, idfm_, idf_;
+    __device__ __forceinline__ void load(const Metric1D<float> &m, int p) {
+        w0m_ = F2(__ldg(m.w0 + p - 1)); w1m_ = F2(__ldg(m.w1 + p - 1)); w0_ = F2(__ldg(m.w0 + p)); w1_ = F2(__ldg(m.w1 + p));
+        idc_ = F2(__ldg(m.idc + p)); idcp_ = F2(__ldg(m.idc + p + 1)); idfm_ = F2(__ldg(m.idf + p - 1)); idf_ = F2(__ldg(m.idf + p));
+    }
+    __device__ __forceinline__ F2 w0m() const { return w0m_; }
+    __device__ __forceinline__ F2 w1m() const { return w1m_; }
+    __device__ __forceinline__ F2 w0() const { return w0_; }
+    __device__ __forceinline__ F2 w1() const { return w1_; }
+    __device__ __forceinline__ P2 divc(F2 x) const { return x * idc_; }
+    __device__ __forceinline__ P2 divf(F2 x) const { return x * idf_; }
+    __device__ __forceinline__ P2 divfm(F2 x) const { return x * idfm_; }
+    __device__ __forceinline__ F2 invc() const { return idc_; }
+    __device__ __forceinline__ F2 invcp() const { return idcp_; }
+    __device__ __forceinline__ F2 invf() const { return idf_; }
+    __device__ __forceinline__ F2 invfm() const { return idfm_; }
+};
 template <> struct AxisLocal<double> {
     const Metric1D<double> *m;   // the kernel argument's metric (stays in the parameter bank once inlined)
     int p;
@@ -212,22 +231,25 @@ template <> struct AxisLocal<double> {
     __device__ __forceinline__ double invfm() const { return 1.0 / m->df[p - 1]; }
 };
 
+// Wall-model flux of the cell at t (plain types) or of the cells at t and t+1 (packed pairs), from double.
+template <typename T> __device__ __forceinline__ T wall_flux(const double *t) { return (T)t[0]; }
+template <> __device__ __forceinline__ F2 wall_flux<F2>(const double *t) { return F2::pair((float)t[0], (float)t[1]); }
+
 // Right-hand sides (src/equations.f90), evaluated in the reference's expression order at one index (i,j,k).
 // `q` is a neighbourhood accessor: q.U(di,dj,dk) is U at (i+di, j+dj, k+dk) with every boundary rule already
 // applied (periodic wraps, no-slip mirror, zero wall faces, zero nu_t ghosts), so the formulas below see the
 // same values the reference reads from its ghosted arrays.
-template <typename T, bool LES, bool WM, typename Q>
-__device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Q &q, const AxisLocal<T> &Y, const AxisLocal<T> &Z,
+template <typename T, bool LES, bool WM, typename Q, typename SA>
+__device__ __forceinline__ T rhs_u_at(const SA &a, const Q &q, const AxisLocal<T> &Y, const AxisLocal<T> &Z,
                                     const double *__restrict__ tau_x, int i, int j, int k) {
     const Dims &d = a.d;
-    typedef Arith<T> A;
     T Uc = q.U(0, 0, 0), Uim = q.U(-1, 0, 0), Uip = q.U(1, 0, 0);
     T Ujm = q.U(0, -1, 0), Ujp = q.U(0, 1, 0), Ukm = q.U(0, 0, -1), Ukp = q.U(0, 0, 1);
     bool wm_band = WM && a.wm && (j + 2 <= 1 + a.nwl || j + 2 >= d.Ny + 2 - a.nwl);
     T wa = wm_band ? T(0) : a.w_adv, wd = T(1) - wa;
     // -d(uu)/dx
     T r;
-    if constexpr (sizeof(T) == 4) {
+    if constexpr (Fp32Forms<T>::value) {
         // FP32: t1^2 - t0^2 = (t1 - t0)(t1 + t0) with t1 - t0 from the stored deviations (no cancellation)
         T dlt = T(0.5) * (q.Ud(1, 0, 0) - q.Ud(-1, 0, 0));
         T sum = T(0.5) * (Uip + Uim) + Uc;
@@ -248,7 +270,7 @@ __device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Q &q, const Ax
     {
         T u1 = Z.w0() * Uc + Z.w1() * Ukp, u0 = Z.w0m() * Ukm + Z.w1m() * Uc;
         T w1 = T(0.5) * (W00 + W10), w0 = T(0.5) * (W0m + W1m);
-        if constexpr (sizeof(T) == 4) {
+        if constexpr (Fp32Forms<T>::value) {
             // u1 w1 - u0 w0 = u1 (w1 - w0) + w0 (u1 - u0); u1 - u0 from deviations (same row: the profile cancels)
             T Udc = q.Ud(0, 0, 0);
             T du = (Z.w0() * Udc + Z.w1() * q.Ud(0, 0, 1)) - (Z.w0m() * q.Ud(0, 0, -1) + Z.w1m() * Udc);
@@ -275,11 +297,11 @@ __device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Q &q, const Ax
     T fy2 = nu_y2 * (tj + (V10 - V00) * a.inv_dx);
     T fy1 = nu_y1 * (tjm + (V1m - V0m) * a.inv_dx);
     if (WM && a.wm) {
-        if (j == 0) fy1 = (T)tau_x[k * d.Nx + i];
-        if (j == d.Ny - 1) fy2 = (T)tau_x[(d.Nz + k) * d.Nx + i];
+        if (j == 0) fy1 = wall_flux<T>(tau_x + k * d.Nx + i);
+        if (j == d.Ny - 1) fy2 = wall_flux<T>(tau_x + (d.Nz + k) * d.Nx + i);
     }
     T dUkp = Ukp - Uc, dUkm = Uc - Ukm, dUip = Uip - Uc, dUim = Uc - Uim;
-    if constexpr (sizeof(T) == 4) {   // x and z differences of U from the deviations
+    if constexpr (Fp32Forms<T>::value) {   // x and z differences of U from the deviations
         T Udc = q.Ud(0, 0, 0);
         dUkp = q.Ud(0, 0, 1) - Udc; dUkm = Udc - q.Ud(0, 0, -1);
         dUip = q.Ud(1, 0, 0) - Udc; dUim = Udc - q.Ud(-1, 0, 0);
@@ -291,10 +313,9 @@ __device__ __forceinline__ T rhs_u_at(const StepArgs<T> &a, const Q &q, const Ax
     return r;
 }
 
-template <typename T, bool LES, bool WM, typename Q>
-__device__ __forceinline__ T rhs_v_at(const StepArgs<T> &a, const Q &q, const AxisLocal<T> &Y, const AxisLocal<T> &Z, int i, int j, int k) {
+template <typename T, bool LES, bool WM, typename Q, typename SA>
+__device__ __forceinline__ T rhs_v_at(const SA &a, const Q &q, const AxisLocal<T> &Y, const AxisLocal<T> &Z, int i, int j, int k) {
     const Dims &d = a.d;
-    typedef Arith<T> A;
     (void)i; (void)d;
     T wa = a.w_adv, wd = T(1) - wa;
     T Vc = q.V(0, 0, 0), Vjm = q.V(0, -1, 0), Vjp = q.V(0, 1, 0);
@@ -307,7 +328,7 @@ __device__ __forceinline__ T rhs_v_at(const StepArgs<T> &a, const Q &q, const Ax
     {
         T u1 = Y.w0() * Uc + Y.w1() * Ucp, u0 = Y.w0() * Um + Y.w1() * Ump;
         T v1 = T(0.5) * (Vc + Vip), v0 = T(0.5) * (Vim + Vc);
-        if constexpr (sizeof(T) == 4) {   // u1 v1 - u0 v0 = u1 (v1 - v0) + v0 (u1 - u0), u1 - u0 from deviations
+        if constexpr (Fp32Forms<T>::value) {   // u1 v1 - u0 v0 = u1 (v1 - v0) + v0 (u1 - u0), u1 - u0 from deviations
             T du = Y.w0() * (q.Ud(0, 0, 0) - q.Ud(-1, 0, 0)) + Y.w1() * (q.Ud(0, 1, 0) - q.Ud(-1, 1, 0));
             r = r - (wd * (u1 * (v1 - v0) + v0 * du) + wa * T(0.5) * (u0 + u1) * (v1 - v0)) * a.inv_dx;
         } else {
@@ -346,11 +367,10 @@ __device__ __forceinline__ T rhs_v_at(const StepArgs<T> &a, const Q &q, const Ax
     return r;
 }
 
-template <typename T, bool LES, bool WM, typename Q>
-__device__ __forceinline__ T rhs_w_at(const StepArgs<T> &a, const Q &q, const AxisLocal<T> &Y, const AxisLocal<T> &Z,
+template <typename T, bool LES, bool WM, typename Q, typename SA>
+__device__ __forceinline__ T rhs_w_at(const SA &a, const Q &q, const AxisLocal<T> &Y, const AxisLocal<T> &Z,
                                     const double *__restrict__ tau_z, int i, int j, int k) {
     const Dims &d = a.d;
-    typedef Arith<T> A;
     bool wm_band = WM && a.wm && (j + 2 <= 1 + a.nwl || j + 2 >= d.Ny + 2 - a.nwl);
     T wa = wm_band ? T(0) : a.w_adv, wd = T(1) - wa;
     T Wc = q.W(0, 0, 0), Wkm = q.W(0, 0, -1), Wkp = q.W(0, 0, 1);
@@ -363,7 +383,7 @@ __device__ __forceinline__ T rhs_w_at(const StepArgs<T> &a, const Q &q, const Ax
     {
         T u1 = Z.w0() * Uc + Z.w1() * Ukp, u0 = Z.w0() * Um + Z.w1() * Umkp;
         T w1 = T(0.5) * (Wc + Wip), w0 = T(0.5) * (Wim + Wc);
-        if constexpr (sizeof(T) == 4) {   // u1 w1 - u0 w0 = u1 (w1 - w0) + w0 (u1 - u0), u1 - u0 from deviations
+        if constexpr (Fp32Forms<T>::value) {   // u1 w1 - u0 w0 = u1 (w1 - w0) + w0 (u1 - u0), u1 - u0 from deviations
             T du = Z.w0() * (q.Ud(0, 0, 0) - q.Ud(-1, 0, 0)) + Z.w1() * (q.Ud(0, 0, 1) - q.Ud(-1, 0, 1));
             r = r - (wd * (u1 * (w1 - w0) + w0 * du) + wa * T(0.5) * (u0 + u1) * (w1 - w0)) * a.inv_dx;
         } else {
@@ -399,8 +419,8 @@ __device__ __forceinline__ T rhs_w_at(const StepArgs<T> &a, const Q &q, const Ax
     T fy2 = nu_y2 * (tj + (Vkp - Vc) * inv_dz3);
     T fy1 = nu_y1 * (tjm + (Vjmkp - Vjm) * inv_dz3);
     if (WM && a.wm) {
-        if (j == 0) fy1 = (T)tau_z[k * d.Nx + i];
-        if (j == d.Ny - 1) fy2 = (T)tau_z[(d.Nz + k) * d.Nx + i];
+        if (j == 0) fy1 = wall_flux<T>(tau_z + k * d.Nx + i);
+        if (j == d.Ny - 1) fy2 = wall_flux<T>(tau_z + (d.Nz + k) * d.Nx + i);
     }
     T fx2 = nu_x2 * ((Wip - Wc) * a.inv_dx + (Ukp - Uc) * inv_dz3);
     T fx1 = nu_x1 * ((Wc - Wim) * a.inv_dx + (Umkp - Um) * inv_dz3);
@@ -433,6 +453,23 @@ template <typename T, int PX> struct TileQ {
     __device__ __forceinline__ T V(int di, int dj, int dk) const { return v[dk + 1][c + dj * PX + di]; }
     __device__ __forceinline__ T W(int di, int dj, int dk) const { return w[dk + 1][c + dj * PX + di]; }
     __device__ __forceinline__ T N(int di, int dj, int dk) const { return n[dk + 1][c + dj * PX + di]; }
+};
+
+// The same neighbourhood for a pair of x-neighbour cells (c, c+1) in FP32 shared planes; c is even and so is the
+// row pitch PX, so a pair at an even x-offset is one 8-byte shared load.
+template <int PX> struct TileQ2 {
+    const float *u[3], *v[3], *w[3], *n[3];
+    int c;
+    F2 ub[3];
+    static __device__ __forceinline__ F2 ld(const float *pl, int off) {
+        if ((off & 1) == 0) return F2(*reinterpret_cast<const float2 *>(pl + off));
+        return F2::pair(pl[off], pl[off + 1]);
+    }
+    __device__ __forceinline__ F2 U(int di, int dj, int dk) const { return ld(u[dk + 1] + c, dj * PX + di) + ub[dj + 1]; }
+    __device__ __forceinline__ F2 Ud(int di, int dj, int dk) const { return ld(u[dk + 1] + c, dj * PX + di); }
+    __device__ __forceinline__ F2 V(int di, int dj, int dk) const { return ld(v[dk + 1] + c, dj * PX + di); }
+    __device__ __forceinline__ F2 W(int di, int dj, int dk) const { return ld(w[dk + 1] + c, dj * PX + di); }
+    __device__ __forceinline__ F2 N(int di, int dj, int dk) const { return ld(n[dk + 1] + c, dj * PX + di); }
 };
 
 // Asynchronous global -> shared copies (cp.async, 4 or 8 bytes per element).
@@ -589,6 +626,149 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
                     wsf[p] = ow + dtt * (c1 * fw + c2 * rw);
                     if (vrow) vs[p] = ov + dtt * (c1 * fv + c2 * rv);
                 }
+            }
+        }
+        cp_async_wait_all();
+        if (more) fix(snext);
+        __syncthreads();
+    }
+}
+
+
+// FP32 stage kernel with two x-neighbour cells per thread, computed with the packed FP32x2 instructions (F2).  Same
+// loader, ghost rules and RK3 epilogue as k_tiled<float, LES, WM, ..., 0>; a block owns 64 x 8 cells, one warp
+// per row of 32 cell pairs.  Shared rows hold cells i0-2 .. i0+65 (pitch 68), so every pair starts at an even index.
+template <bool LES, bool WM>
+__global__ void __launch_bounds__(256, 2) k_tiled2(StepArgs<float> a, const float *__restrict__ U, const float *__restrict__ V,
+                                                   const float *__restrict__ W, const float *__restrict__ NU,
+                                                   const double *__restrict__ tau_x, const double *__restrict__ tau_z,
+                                                   StageCoef sc, int kc, float *__restrict__ uo, float *__restrict__ vo,
+                                                   float *__restrict__ wo, float *__restrict__ f1u, float *__restrict__ f1v,
+                                                   float *__restrict__ f1w, float *__restrict__ us, float *__restrict__ vs,
+                                                   float *__restrict__ wsf, float *__restrict__ rhs_only) {
+    constexpr int TXC = 64, TY = 8, NT = 256;
+    constexpr int PX = TXC + 4, PY = TY + 2, PS = PX * PY;
+    constexpr int NF = LES ? 4 : 3;
+    constexpr int PER = (PS + NT - 1) / NT;
+    __shared__ __align__(16) float sm[NF][4][PS];
+    const Dims &d = a.d;
+    const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
+    const int i0 = blockIdx.x * TXC, j0 = blockIdx.y * TY;
+    const int k0 = blockIdx.z * kc, kend = min(k0 + kc, Nz);
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int i = i0 + 2 * tx, j = j0 + ty;
+    const bool active = i < Nx && j < Ny;   // Nx is even: the pair's second cell is in range too
+    const int plane = Nx * Ny;
+
+    int off[PER];
+    bool ghost[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        int e = threadIdx.x + q * NT;
+        off[q] = -1; ghost[q] = false;
+        if (e < PS) {
+            int jj = e / PX, ii = e - jj * PX;
+            int gi = i0 - 2 + ii;
+            gi = gi < 0 ? gi + Nx : gi;
+            while (gi >= Nx) gi -= Nx;
+            int gj = j0 - 1 + jj, g;
+            if (d.yper) {
+                g = gj < 0 ? gj + Ny : gj;
+                while (g >= Ny) g -= Ny;
+            } else {
+                g = gj < 0 ? 0 : (gj >= Ny ? Ny - 1 : gj);
+                ghost[q] = (gj < 0 || gj >= Ny);
+            }
+            off[q] = g * Nx + gi;
+        }
+    }
+    auto issue = [&](int slot, int k) {
+        int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k);
+        const int kb = kw * plane;
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            if (off[q] < 0) continue;
+            const int o = kb + off[q], e = threadIdx.x + q * NT;
+            cp_async<4>(&sm[0][slot][e], U + o);
+            cp_async<4>(&sm[2][slot][e], W + o);
+            if (!ghost[q]) {
+                cp_async<4>(&sm[1][slot][e], V + o);
+                if (LES) cp_async<4>(&sm[NF - 1][slot][e], NU + o);
+            }
+        }
+    };
+    auto fix = [&](int slot) {
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            if (off[q] < 0 || !ghost[q]) continue;
+            const int e = threadIdx.x + q * NT;
+            sm[0][slot][e] = -sm[0][slot][e];
+            sm[2][slot][e] = -sm[2][slot][e];
+            sm[1][slot][e] = 0.0f;
+            if (LES) sm[NF - 1][slot][e] = 0.0f;
+        }
+    };
+    F2 ubr[3];
+#pragma unroll
+    for (int dj = -1; dj <= 1; ++dj) {
+        int gj = min(j, Ny - 1) + dj;
+        float sgn = 1.0f;
+        if (d.yper) { gj = gj < 0 ? gj + Ny : (gj >= Ny ? gj - Ny : gj); }
+        else if (gj < 0 || gj >= Ny) { gj = gj < 0 ? 0 : Ny - 1; sgn = -1.0f; }
+        ubr[dj + 1] = F2(sgn * __ldg(a.ub + gj));
+    }
+    AxisLocal<F2> Y;
+    Y.load(a.my, min(j, Ny - 1));
+
+    issue(0, k0 - 1); issue(1, k0); issue(2, k0 + 1);
+    cp_async_commit();
+    cp_async_wait_all();
+    fix(0); fix(1); fix(2);
+    __syncthreads();
+    const int cloc = (ty + 1) * PX + 2 + 2 * tx;
+    for (int k = k0; k < kend; ++k) {
+        const bool more = k + 2 <= kend;
+        const int snext = (k - k0 + 3) & 3;
+        if (more) issue(snext, k + 2);
+        cp_async_commit();
+        const int sm_ = (k - k0) & 3, s0 = (k - k0 + 1) & 3, sp = (k - k0 + 2) & 3;
+        if (active) {
+            const int p = k * plane + j * Nx + i;
+            TileQ2<PX> q;
+            q.c = cloc;
+            q.ub[0] = ubr[0]; q.ub[1] = ubr[1]; q.ub[2] = ubr[2];
+            q.u[0] = sm[0][sm_]; q.u[1] = sm[0][s0]; q.u[2] = sm[0][sp];
+            q.v[0] = sm[1][sm_]; q.v[1] = sm[1][s0]; q.v[2] = sm[1][sp];
+            q.w[0] = sm[2][sm_]; q.w[1] = sm[2][s0]; q.w[2] = sm[2][sp];
+            q.n[0] = sm[NF - 1][sm_]; q.n[1] = sm[NF - 1][s0]; q.n[2] = sm[NF - 1][sp];
+            const bool vrow = j < d.NyV;
+            const bool upd = !rhs_only && sc.stage != 1;
+            auto ld2 = [&](const float *b) { return F2(*reinterpret_cast<const float2 *>(b + p)); };
+            auto st2 = [&](float *b, F2 x) { *reinterpret_cast<float2 *>(b + p) = x.v; };
+            F2 ou(0.0f), ov(0.0f), ow(0.0f), fu(0.0f), fv(0.0f), fw(0.0f);
+            if (upd) {
+                if (!sc.incr) { ou = ld2(uo); ow = ld2(wo); if (vrow) ov = ld2(vo); }
+                fu = ld2(f1u); fw = ld2(f1w);
+                if (vrow) fv = ld2(f1v);
+            }
+            AxisLocal<F2> Z;
+            Z.load(a.mz, k);
+            F2 ru = rhs_u_at<F2, LES, WM>(a, q, Y, Z, tau_x, i, j, k);
+            F2 rw = rhs_w_at<F2, LES, WM>(a, q, Y, Z, tau_z, i, j, k);
+            F2 rv = vrow ? rhs_v_at<F2, LES, WM>(a, q, Y, Z, i, j, k) : F2(0.0f);
+            if (rhs_only) {
+                st2(rhs_only, ru); st2(rhs_only + d.cells, rv); st2(rhs_only + 2 * d.cells, rw);
+            } else if (sc.stage == 1) {
+                const F2 c = F2(sc.dt_a11);
+                F2 u0 = q.Ud(0, 0, 0), w0 = q.W(0, 0, 0);
+                st2(uo, u0); st2(f1u, ru); st2(us, u0 + c * ru);
+                st2(wo, w0); st2(f1w, rw); st2(wsf, w0 + c * rw);
+                if (vrow) { F2 v0 = q.V(0, 0, 0); st2(vo, v0); st2(f1v, rv); st2(vs, v0 + c * rv); }
+            } else {
+                const F2 c1 = F2(sc.c1), c2 = F2(sc.c2), dtt = F2(sc.dt);
+                st2(us, ou + dtt * (c1 * fu + c2 * ru));
+                st2(wsf, ow + dtt * (c1 * fw + c2 * rw));
+                if (vrow) st2(vs, ov + dtt * (c1 * fv + c2 * rv));
             }
         }
         cp_async_wait_all();

@@ -31,7 +31,7 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_solve_poisson", "dfdm_compute_bulk_velocity", "dfdm_check_divergence", "dfdm_kinetic_energy",
            "dfdm_check_finite", "dfdm_pad_field", "dfdm_launch_kernel_async", "dfdm_kernel_bytes",
            "dfdm_launch_count", "dfdm_solve_poisson_noalloc", "dfdm_write_snapshot", "dfdm_read_snapshot",
-           "dfdm_compute_cfl"]
+           "dfdm_compute_cfl", "dfdm_set_stage_variant", "dfdm_get_stage_variant"]
 
 
 class DfdmError(RuntimeError):
@@ -92,6 +92,8 @@ def load(build_if_missing: bool = True):
         "dfdm_write_snapshot": (c_int, [c_void_p, c_char_p]),
         "dfdm_read_snapshot": (c_int, [c_void_p, c_char_p]),
         "dfdm_compute_cfl": (c_int, [c_void_p, P, P]),
+        "dfdm_set_stage_variant": (c_int, [c_void_p, c_int]),
+        "dfdm_get_stage_variant": (c_int, [c_void_p, POINTER(ctypes.c_int), P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -257,6 +259,16 @@ class Solver:
         v = c_double(0.0)
         _check(load().dfdm_check_divergence(self.h, ctypes.byref(v)))
         return v.value
+
+    def set_stage_variant(self, variant: int) -> None:
+        """FP32 stage kernel: 0 one cell per thread, 1 packed pairs, -1 re-time both and keep the faster."""
+        _check(load().dfdm_set_stage_variant(self.h, int(variant)))
+
+    def stage_variant(self):
+        """(variant in use, ms per launch of variant 0, of variant 1) from the set-up timing (-1 = not timed)."""
+        v, a, b = ctypes.c_int(0), c_double(0.0), c_double(0.0)
+        _check(load().dfdm_get_stage_variant(self.h, ctypes.byref(v), ctypes.byref(a), ctypes.byref(b)))
+        return v.value, a.value, b.value
 
     def compute_cfl(self):
         """(convective, viscous) CFL numbers of the resident state, as compute_cfl (src/monitor.f90:304)."""

@@ -149,6 +149,16 @@ int dfdm_solve_poisson(dfdm_ctx *ctx, const double *rhs_p_in, double *phi_out);
  *    threads) race on the array: serialise them. */
 #define DFDM_NOALLOC_MAX_POINTS 2097152
 int dfdm_solve_poisson_noalloc(dfdm_ctx *ctx, const double *rhs_p_in, double *phi_out);
+/* ---- tuning (no counterpart in the reference) ----
+ * The FP32 stage kernel (RHS + RK3 update) has two variants: 0 computes one cell per thread on 32 x 8 tiles,
+ * 1 computes two x-neighbour cells per thread with the packed FP32x2 instructions on 64 x 8 tiles. dfdm_create
+ * times both on the context's grid and keeps the faster; the choice is cached per device and grid shape for the
+ * process. set_stage_variant forces 0 or 1, or re-times with -1 (FP64 contexts have variant 0 only); a change drops
+ * the context's captured step graph. get_stage_variant returns the variant in use and the timings (ms per launch,
+ * -1 where not timed); any output pointer may be NULL. */
+int dfdm_set_stage_variant(dfdm_ctx *ctx, int variant);
+int dfdm_get_stage_variant(dfdm_ctx *ctx, int *variant, double *ms_one, double *ms_pairs);
+
 /* ---- snapshots in the reference's restart format ----
  * output_data's staggered full snapshot (src/input_output.f90:1782-1880): a little-endian stream holding the mesh
  * (int32 n and n doubles for x, y, z and the centres xm, ym, zm) and then U, V, W, P and, with an SGS model, nu_t,

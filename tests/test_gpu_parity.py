@@ -193,3 +193,46 @@ def test_cfl_matches_the_reference_formula(name, prec, tol):
     got = s.compute_cfl()
     for g, w in zip(got, want):
         assert abs(g - w) <= tol * w, (got, want)
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("name", SMALL)
+def test_fp32_stage_variants_match_the_oracle(oracle_mod, name, variant):
+    """Both FP32 stage kernels (one cell per thread; packed FP32x2 pairs) against the FP64 oracle after 5 steps."""
+    c, o, s = _pair(oracle_mod, name, "fp32")
+    s.set_stage_variant(variant)
+    assert s.stage_variant()[0] == variant
+    o.step(5)
+    s.compute_time_step_RK3(5)
+    for key, a, b in zip("UVWP", s.get_state(), o.get_state()):
+        assert rel_l2(a, b) <= TOL32, (key, rel_l2(a, b))
+
+
+@pytest.mark.parametrize("name", ["chan_les_amd_small", "tgv_small", "chan_small"])
+def test_fp32_stage_variants_agree(name):
+    c = cases.get(name)
+    state = cases.initial_condition(c)
+    out = []
+    for variant in (0, 1):
+        s = Solver(c, "fp32", graphs=True)
+        s.set_stage_variant(variant)
+        s.set_state(*state)
+        s.compute_time_step_RK3(20)
+        out.append(s.get_state())
+    for key, a, b in zip("UVWP", *out):
+        assert rel_l2(a, b) <= 1e-6, (key, rel_l2(a, b))
+
+
+def test_stage_variant_tuning_is_reported():
+    c = cases.chan_small()
+    s = Solver(c, "fp32")
+    v, ms0, ms1 = s.stage_variant()
+    assert v in (0, 1) and ms0 > 0 and ms1 > 0 and (ms1 < ms0) == (v == 1)
+    s.set_stage_variant(-1)
+    assert s.stage_variant()[1] > 0
+    d = Solver(c, "fp64")
+    assert d.stage_variant() == (0, -1.0, -1.0)
+    from dfdm.native import DfdmError
+    with pytest.raises(DfdmError) as e:
+        d.set_stage_variant(1)
+    assert e.value.code == 4
