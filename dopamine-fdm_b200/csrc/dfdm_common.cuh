@@ -84,4 +84,12 @@ template <> struct Arith<float> {
     static __device__ __forceinline__ float inv(const float *, const float *id, int j) { return id[j]; }
 };
 
+// Asynchronous global -> shared copies (cp.async, 4 or 8 bytes per element).
+template <int B> __device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(B));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
 }  // namespace dfdm

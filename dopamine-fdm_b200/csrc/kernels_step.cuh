@@ -472,13 +472,7 @@ template <int PX> struct TileQ2 {
     __device__ __forceinline__ F2 N(int di, int dj, int dk) const { return ld(n[dk + 1] + c, dj * PX + di); }
 };
 
-// Asynchronous global -> shared copies (cp.async, 4 or 8 bytes per element).
-template <int B> __device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
-    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(B));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
 
 // Tiled kernels (KIND 0: fused stage, KIND 1: eddy viscosity), 2.5-D blocked: a block owns a TX x TY column of
 // (i,j) cells and marches through a chunk of kc z-planes.  Each z-plane of U, V, W (and nu_t) is copied from HBM
@@ -636,17 +630,18 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
 
 
 // FP32 stage kernel with two x-neighbour cells per thread, computed with the packed FP32x2 instructions (F2).  Same
-// loader, ghost rules and RK3 epilogue as k_tiled<float, LES, WM, ..., 0>; a block owns 64 x 8 cells, one warp
-// per row of 32 cell pairs.  Shared rows hold cells i0-2 .. i0+65 (pitch 68), so every pair starts at an even index.
-template <bool LES, bool WM>
-__global__ void __launch_bounds__(256, 2) k_tiled2(StepArgs<float> a, const float *__restrict__ U, const float *__restrict__ V,
+// loader, ghost rules and RK3 epilogue as k_tiled<float, LES, WM, ..., 0>; a block owns 64 x TY cells, one warp
+// per row of 32 cell pairs.  It needs ~118 registers: capping it at 96 or 80 (for more resident warps) spills
+// 170-300 bytes, so it runs 2 blocks of 256 threads per SM.  Shared rows hold cells i0-2 .. i0+65 (pitch 68), so every pair starts at an even index.
+template <bool LES, bool WM, int TY = 8>
+__global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<float> a, const float *__restrict__ U, const float *__restrict__ V,
                                                    const float *__restrict__ W, const float *__restrict__ NU,
                                                    const double *__restrict__ tau_x, const double *__restrict__ tau_z,
                                                    StageCoef sc, int kc, float *__restrict__ uo, float *__restrict__ vo,
                                                    float *__restrict__ wo, float *__restrict__ f1u, float *__restrict__ f1v,
                                                    float *__restrict__ f1w, float *__restrict__ us, float *__restrict__ vs,
                                                    float *__restrict__ wsf, float *__restrict__ rhs_only) {
-    constexpr int TXC = 64, TY = 8, NT = 256;
+    constexpr int TXC = 64, NT = 32 * TY;
     constexpr int PX = TXC + 4, PY = TY + 2, PS = PX * PY;
     constexpr int NF = LES ? 4 : 3;
     constexpr int PER = (PS + NT - 1) / NT;

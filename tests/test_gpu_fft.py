@@ -67,3 +67,20 @@ def test_poisson_x_and_z_lengths(oracle_mod, n):
 def test_poisson_periodic_y_lengths(oracle_mod, n):
     """Periodic y of length n (the y transform, the k^2 division and the (0,0,0) pin)."""
     _check(oracle_mod, _case(16, n, 8, yper=True), 200 + n)
+
+
+@pytest.mark.parametrize("n", TWO_LEVEL + STOCKHAM)
+def test_projection_x_lengths(oracle_mod, n):
+    """The projection (divergence fused with the forward x transform, the solve and the correction) at x
+    half-length n, FP64 against the oracle."""
+    c = _case(2 * n, 8, 16, yper=False)
+    state = _random_state(c, 300 + n)
+    o = oracle_mod.Oracle(c)
+    o.set_state(*state)
+    o.compute_projection_step(save_p=True)
+    o.apply_boundary_conditions()
+    s = Solver(c, "fp64")
+    s.set_state(*state)
+    s.compute_projection_step(save_p=True)
+    for key, a, b in zip("UVW", s.get_state()[:3], o.get_state()[:3]):
+        assert rel_l2(a, b) <= 1e-12, (n, key, rel_l2(a, b))
