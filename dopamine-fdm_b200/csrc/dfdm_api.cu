@@ -110,9 +110,6 @@ struct dfdm_ctx {
     size_t smem_x = 0, smem_z = 0, smem_y = 0;
     // two-level register transforms (fft_reg.cuh) where the length has a split; Stockham otherwise
     bool x2 = false, z2 = false, y2 = false;
-    bool x3 = false;                 // pipelined divergence + forward x (k_fwd_x3)
-    int grid_x3 = 1;
-    size_t smem_x3 = 0;
     int lx2 = 1, lxi2 = 1, thr_z2 = 256, thr_y2 = 256;   // x lines per block: forward, inverse
     size_t smem_x2 = 0, smem_xi2 = 0, smem_z2 = 0, smem_y2 = 0;
     cudaStream_t own_stream = nullptr, stream = nullptr;
@@ -302,17 +299,6 @@ template <typename T> struct Impl {
             setattr((const void *)k_fwd_x2<T, true, N>, c->smem_x2);
             setattr((const void *)k_fwd_x2<T, false, N>, c->smem_x2);
             setattr((const void *)k_inv_x2<T, N>, c->smem_xi2);
-            c->x3 = d.Nx % (16 / (int)sizeof(T)) == 0;
-            if (c->x3) {
-                constexpr int LB = FwdBatch<T>::LB;
-                c->smem_x3 = (size_t)LB * 5 * d.Nx * sizeof(T) + (size_t)LB * (RowLayout<N>::LDA + RowLayout<N>::LDT) * sizeof(C);
-                setattr((const void *)k_fwd_x3<T, N>, c->smem_x3);
-                int occ = 1, dev = 0, nsm = 148;
-                if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fwd_x3<T, N>, 256, c->smem_x3) != cudaSuccess) occ = 1;
-                const long long nbatch = ((long long)d.Ny * d.Nz + LB - 1) / LB;
-                c->grid_x3 = (int)std::max(1LL, std::min(nbatch, (long long)nsm * std::max(1, occ)));
-            }
         });
         c->z2 = with_fft2l(d.Nz, [&](auto n) {
             constexpr int N = decltype(n)::value;
@@ -335,13 +321,7 @@ template <typename T> struct Impl {
         const Dims &d = c->d;
         cudaStream_t st = c->stream;
         const long long lines = (long long)d.Ny * d.Nz;
-        if (c->x3 && from_div) {
-            with_fft2l(d.Nx / 2, [&](auto n) {
-                constexpr int N = decltype(n)::value;
-                k_fwd_x3<T, N><<<c->grid_x3, 256, c->smem_x3, st>>>(poisson_args<T>(c), f(c->us), f(c->vs), f(c->wsf),
-                                                                   (C *)c->spec, (const C *)c->tw_x, (const C *)c->twr_x);
-            });
-        } else if (c->x2) {
+        if (c->x2) {
             const int nb = (int)((lines + c->lx2 - 1) / c->lx2);
             with_fft2l(d.Nx / 2, [&](auto n) {
                 constexpr int N = decltype(n)::value;

@@ -108,124 +108,6 @@ __global__ void __launch_bounds__(256) k_fwd_x2(PoissonArgs<T> a, int lx, const 
     }
 }
 
-// ---- the same transform of div u*, pipelined: persistent blocks over batches of LB x-lines -------------------
-// For every line of a batch the five rows the divergence reads (U; V and the V row below it in j; W and the W row
-// of the plane below in k) are staged in shared memory with 16-byte cp.async.  The copies of the next batch are
-// issued as soon as the divergence pass has read the staging, so they overlap the register transform and the
-// unpacking of the current batch.  Needs Nx % 4 == 0 (16-byte rows).
-template <typename T> struct FwdBatch { static constexpr int LB = sizeof(T) == 4 ? 8 : 4; };
-
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
-}
-
-template <typename T, int M>
-__global__ void __launch_bounds__(256) k_fwd_x3(PoissonArgs<T> a, const T *__restrict__ U, const T *__restrict__ V,
-                                                const T *__restrict__ W, typename cplx_t<T>::type *__restrict__ spec,
-                                                const typename cplx_t<T>::type *__restrict__ tw,
-                                                const typename cplx_t<T>::type *__restrict__ twr) {
-    typedef typename cplx_t<T>::type C;
-    typedef typename Vec2<T>::type T2;
-    typedef Arith<T> A;
-    constexpr int N1 = Split<M>::N1, N2 = Split<M>::N2, Nx = 2 * M;
-    constexpr int LDA = RowLayout<M>::LDA, LDT = RowLayout<M>::LDT;
-    constexpr int LB = FwdBatch<T>::LB;
-    constexpr int CH = 16 / (int)sizeof(T);              // elements per 16-byte chunk
-    constexpr int ROWCH = Nx / CH;                       // chunks per row
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *stage = (T *)smem_raw;                            // [LB][5][Nx]: U, V, Vjm, W, Wkm
-    C *bt = (C *)(stage + LB * 5 * Nx), *ba = bt + LB * LDT;
-    const Dims &d = a.d;
-    const int Ny = d.Ny, Nz = d.Nz, plane = Nx * Ny;
-    const int lines = Ny * Nz, nbatch = (lines + LB - 1) / LB;
-    auto issue = [&](int batch) {
-        const int line0 = batch * LB;
-        for (int q = threadIdx.x; q < LB * 5 * ROWCH; q += blockDim.x) {
-            const int ll = q / (5 * ROWCH), rest = q - ll * 5 * ROWCH, r = rest / ROWCH, ch = rest - r * ROWCH;
-            const int line = min(line0 + ll, lines - 1);
-            const int k = (int)fdiv((unsigned)line, a.fNy), j = line - k * Ny;
-            const int ob = k * plane + j * Nx;
-            const T *src;
-            if (r == 0) src = U + ob;
-            else if (r == 1) src = V + ob;
-            else if (r == 2) src = V + ob + ((j > 0) ? -Nx : (Ny - 1) * Nx);   // zero at a wall: see vzero below
-            else if (r == 3) src = W + ob;
-            else src = W + ob + ((k == 0) ? (Nz - 1) * plane : -plane);
-            cp_async16(stage + (ll * 5 + r) * Nx + ch * CH, src + ch * CH);
-        }
-        cp_async_commit();
-    };
-    int b = blockIdx.x;
-    if (b < nbatch) issue(b);
-    for (; b < nbatch; b += gridDim.x) {
-        const int line0 = b * LB;
-        const int nl = min(LB, lines - line0);
-        cp_async_wait_all();
-        __syncthreads();
-        for (int e = threadIdx.x; e < nl * M; e += blockDim.x) {
-            const int ll = e / M, n = e - ll * M;
-            const int line = line0 + ll;
-            const int k = (int)fdiv((unsigned)line, a.fNy), j = line - k * Ny;
-            const bool vzero = (j == 0) && !d.yper;
-            const T inv_dyj = A::inv(a.my.dc, a.my.idc, j), inv_dzk = A::inv(a.mz.dc, a.mz.idc, k);
-            const T *sl = stage + ll * 5 * Nx;
-            const int i = 2 * n;
-            const T2 u = *reinterpret_cast<const T2 *>(sl + i);
-            const T um = sl[i == 0 ? Nx - 1 : i - 1];
-            const T2 v = *reinterpret_cast<const T2 *>(sl + Nx + i);
-            T2 vm = *reinterpret_cast<const T2 *>(sl + 2 * Nx + i);
-            if (vzero) { vm.x = T(0); vm.y = T(0); }
-            const T2 w = *reinterpret_cast<const T2 *>(sl + 3 * Nx + i);
-            const T2 wm = *reinterpret_cast<const T2 *>(sl + 4 * Nx + i);
-            C z;
-            z.x = (u.x - um) * a.inv_dx + (v.x - vm.x) * inv_dyj + (w.x - wm.x) * inv_dzk;
-            z.y = (u.y - u.x) * a.inv_dx + (v.y - vm.y) * inv_dyj + (w.y - wm.y) * inv_dzk;
-            ba[ll * LDA + n] = z;
-        }
-        __syncthreads();
-        if (b + (int)gridDim.x < nbatch) issue(b + gridDim.x);   // staging is free: overlap the next batch's loads
-        for (int q = threadIdx.x; q < nl * N2; q += blockDim.x) {
-            const int ll = q / N2, n2 = q - ll * N2;
-            C v[N1];
-            const C *al = ba + ll * LDA + n2;
-#pragma unroll
-            for (int n1 = 0; n1 < N1; ++n1) v[n1] = al[n1 * N2];
-            row_step1<T, false, M>(v, bt + ll * LDT, n2, tw);
-        }
-        __syncthreads();
-        for (int q = threadIdx.x; q < nl * N1; q += blockDim.x) {
-            const int ll = q / N1, k1 = q - ll * N1;
-            C v[N2];
-            const C *tl = bt + ll * LDT + k1 * (N2 + 1);
-#pragma unroll
-            for (int n2 = 0; n2 < N2; ++n2) v[n2] = tl[n2];
-            Codelet<T, false, N2>::run(v);
-            C *al = ba + ll * LDA;
-#pragma unroll
-            for (int k2 = 0; k2 < N2; ++k2) al[k1 + N1 * k2] = v[k2];
-        }
-        __syncthreads();
-        const int Nxc = d.Nxc;
-        for (int e = threadIdx.x; e < nl * (M + 1); e += blockDim.x) {
-            const int ll = e / (M + 1), kx = e - ll * (M + 1);
-            const C *res = ba + ll * LDA;
-            C Zk = res[kx == M ? 0 : kx];
-            C Zm = res[kx == 0 ? 0 : M - kx];
-            T Er = T(0.5) * (Zk.x + Zm.x), Ei = T(0.5) * (Zk.y - Zm.y);
-            T Dr = T(0.5) * (Zk.x - Zm.x), Di = T(0.5) * (Zk.y + Zm.y);
-            T Or = Di, Oi = -Dr;
-            C wv = __ldg(twr + kx);
-            C X;
-            X.x = Er + (wv.x * Or - wv.y * Oi);
-            X.y = Ei + (wv.x * Oi + wv.y * Or);
-            spec[(size_t)(line0 + ll) * Nxc + kx] = X;
-        }
-        __syncthreads();   // ba is reused by the next batch's divergence pass
-    }
-    cp_async_wait_all();
-}
-
 // ---- inverse complex-to-real x transform, writes phi = x / (nxp*nzp) -----------------------------------------
 template <typename T, int M>
 __global__ void __launch_bounds__(256) k_inv_x2(PoissonArgs<T> a, int lx, const typename cplx_t<T>::type *__restrict__ spec,
