@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--no-kernels", action="store_true", help="skip the per-kernel roofline timings")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream measurement")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-vs-FP64 report of the other configs")
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-rate", type=float, default=4.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--serve-saturated", type=int, default=48,
@@ -371,6 +372,33 @@ def main():
                       "d2h_bytes_per_step": bo, "steps": ne,
                       "path": "dfdm_set_state(U,V,W) + dfdm_compute_time_step_rk3(1) + dfdm_get_state(U,V,W,P) "
                               "per step, FP64 ghosted host arrays in pinned memory"}
+
+    # ---- every other config at its stated step count: FP32-mixed against the FP64 form (the oracle's arithmetic) ----
+    if not args.no_accuracy and rank == 0:
+        acc = {}
+        for name in ("tgv64", "chan180", "les395"):
+            cc = cases.get(name)
+            st = cases.initial_condition(cc)
+            res = {}
+            for prec in ("fp32", "fp64"):
+                sv = Solver(cc, prec, graphs=True)
+                sv.set_stream(sh)
+                sv.set_state(*st)
+                torch.cuda.synchronize()
+                a0 = torch.cuda.Event(enable_timing=True)
+                a1 = torch.cuda.Event(enable_timing=True)
+                a0.record(stream)
+                sv.compute_time_step_RK3_async(cc.nsteps)
+                a1.record(stream)
+                a1.synchronize()
+                res[prec] = (sv.get_state(), cc.n_cells * cc.nsteps / (a0.elapsed_time(a1) * 1e-3))
+                sv.close()
+            rel = {k: float(np.linalg.norm((x - y).ravel()) / max(np.linalg.norm(y.ravel()), 1e-300))
+                   for k, x, y in zip("UVWP", res["fp32"][0], res["fp64"][0])}
+            acc[name] = {"steps": cc.nsteps, "cells": cc.n_cells, "rel_l2_fp32_vs_fp64": rel,
+                         "fp32_cell_steps_per_s": res["fp32"][1], "fp64_cell_steps_per_s": res["fp64"][1],
+                         "note": "timing includes the first (ungraphed) step and the graph capture"}
+        out["accuracy"] = acc
 
     # ---- serving stream ----
     if not args.no_serve:

@@ -210,6 +210,89 @@ __global__ void __launch_bounds__(64) k_ysolve(Dims d, typename cplx_t<T>::type 
     }
 }
 
+// The same solve with the memory latency hidden: each sweep keeps two register buffers of CH rows and issues the
+// loads of the next chunk before the recurrence of the current one runs, and the per-row coefficients DL and DU
+// are read from shared memory.  Arithmetic and rounding are those of k_ysolve.
+template <typename T, int CH>
+__global__ void __launch_bounds__(64) k_ysolve2(Dims d, typename cplx_t<T>::type *__restrict__ spec,
+                                                const double *__restrict__ rpiv, const double *__restrict__ lo,
+                                                const double *__restrict__ up) {
+    typedef typename cplx_t<T>::type C;
+    extern __shared__ double sco[];   // DL at [0, n), DU at [n, 2n)
+    const int Nxc = d.Nxc, n = d.Ny;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) { sco[r] = lo[r]; sco[n + r] = up[r]; }
+    __syncthreads();
+    const int kx = blockIdx.x * blockDim.x + threadIdx.x, kz = blockIdx.y;
+    if (kx >= Nxc) return;
+    C *col = spec + kz * n * Nxc + kx;
+    const double *rp = rpiv + kz * n * Nxc + kx;
+    const double *slo = sco, *sup = sco + n;
+    C va[CH], vb[CH];
+    double ra[CH], rb[CH];
+    auto fload = [&](C *v, double *rv, int r0) {
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            const int r = r0 + q;
+            if (r < n) { v[q] = col[r * Nxc]; rv[q] = __ldg(rp + r * Nxc); }
+        }
+    };
+    C v0 = col[0];
+    double br = (double)v0.x, bi = (double)v0.y, rprev = __ldg(rp);
+    auto fproc = [&](const C *v, const double *rv, int r0) {
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            const int r = r0 + q;
+            if (r < n) {
+                const double m = slo[r] * rprev;
+                br = (double)v[q].x - m * br;
+                bi = (double)v[q].y - m * bi;
+                if (r < n - 1) { C o; o.x = (T)br; o.y = (T)bi; col[r * Nxc] = o; }
+                rprev = rv[q];
+            }
+        }
+    };
+    fload(va, ra, 1);
+    for (int r0 = 1; r0 < n; r0 += 2 * CH) {
+        if (r0 + CH < n) fload(vb, rb, r0 + CH);
+        fproc(va, ra, r0);
+        if (r0 + CH >= n) break;
+        if (r0 + 2 * CH < n) fload(va, ra, r0 + 2 * CH);
+        fproc(vb, rb, r0 + CH);
+    }
+    double xr = br * rprev, xi = bi * rprev;
+    {
+        C o; o.x = (T)xr; o.y = (T)xi;
+        col[(n - 1) * Nxc] = o;
+    }
+    auto bload = [&](C *v, double *rv, int r0) {
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            const int r = r0 - q;
+            if (r >= 0) { v[q] = col[r * Nxc]; rv[q] = __ldg(rp + r * Nxc); }
+        }
+    };
+    auto bproc = [&](const C *v, const double *rv, int r0) {
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            const int r = r0 - q;
+            if (r >= 0) {
+                xr = ((double)v[q].x - sup[r] * xr) * rv[q];
+                xi = ((double)v[q].y - sup[r] * xi) * rv[q];
+                C o; o.x = (T)xr; o.y = (T)xi;
+                col[r * Nxc] = o;
+            }
+        }
+    };
+    bload(va, ra, n - 2);
+    for (int r0 = n - 2; r0 >= 0; r0 -= 2 * CH) {
+        if (r0 - CH >= 0) bload(vb, rb, r0 - CH);
+        bproc(va, ra, r0);
+        if (r0 - CH < 0) break;
+        if (r0 - 2 * CH >= 0) bload(va, ra, r0 - 2 * CH);
+        bproc(vb, rb, r0 - CH);
+    }
+}
+
 // ---- 4. inverse complex-to-real x transform, writes the pseudo-pressure phi ----------------------------------
 //   Z_k = (X_k + conj X_{M-k}) + i (X_k - conj X_{M-k}) conj(W_Nx^k),  z = IFFT_M(Z),  x_2n = Re z_n, x_2n+1 = Im z_n
 // (unnormalised like cufftExecZ2D); the imaginary parts of X_0 and X_M are dropped, as the real part of the
