@@ -432,14 +432,14 @@ template <typename T> struct Impl {
         int dev = 0;
         CK(cudaGetDevice(&dev));
         const std::array<int, 6> key = {dev, c->d.Nx, c->d.Ny, c->d.Nz, c->les, c->wm};
-        {
-            std::lock_guard<std::mutex> lk(g_tune_mu);
-            auto it = g_tune.find(key);
-            if (it != g_tune.end() && !force) {
-                c->stage_variant = it->second.variant;
-                c->stage_ms[0] = it->second.ms[0]; c->stage_ms[1] = it->second.ms[1];
-                return DFDM_OK;
-            }
+        // held through the timing: contexts of one shape created at the same time all take the first one's choice,
+        // so every context of a shape in the process runs the same kernel (the variants round differently)
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end() && !force) {
+            c->stage_variant = it->second.variant;
+            c->stage_ms[0] = it->second.ms[0]; c->stage_ms[1] = it->second.ms[1];
+            return DFDM_OK;
         }
         StageCoef sc{2, 0.0, c->prm.dt, 0.25, 5.0 / 12.0, 0};
         cudaEvent_t e0, e1;
@@ -462,7 +462,6 @@ template <typename T> struct Impl {
         cudaEventDestroy(e1);
         if (rc) return rc;
         c->stage_variant = c->stage_ms[1] < c->stage_ms[0] ? 1 : 0;
-        std::lock_guard<std::mutex> lk(g_tune_mu);
         g_tune[key] = TuneEntry{c->stage_variant, {c->stage_ms[0], c->stage_ms[1]}};
         return DFDM_OK;
     }
