@@ -791,7 +791,38 @@ struct Oracle {
         periodic_z(nu_t, 4);
     }
 
-    double dt() const { return prm.dt; }
+    // time step: fixed (prm.dt) or adaptive (cfl_adaptive = 1; src/global.f90:472-478)
+    double dt_cur = -1.0;
+    int cfl_adaptive = 0;
+    double cfl_target = 0.5, cfl_safety = 0.9, dt_min = 1e-10, dt_max = 1e10;
+    double dt() const { return dt_cur > 0.0 ? dt_cur : prm.dt; }
+
+    // compute_cfl (src/monitor.f90:304-424) without the IBM, buoyancy, rotation and actuator terms
+    void compute_cfl(double &conv_out, double &visc_out) {
+        double conv = 0.0, visc = 0.0;
+        const double inv_dx = 1.0 / dx, inv_dx2 = inv_dx * inv_dx;
+        for (int k = 2; k <= nzg - 1; ++k)
+            for (int j = 2; j <= nyg - 1; ++j) {
+                const double inv_dy = 1.0 / std::max(y[j] - y[j - 1], 1e-14), inv_dy2 = inv_dy * inv_dy;
+                const double inv_dz = 1.0 / std::max(z[k] - z[k - 1], 1e-14), inv_dz2 = inv_dz * inv_dz;
+                for (int i = 2; i <= nxg - 1; ++i) {
+                    const double c = std::fabs(0.5 * (U(i, j, k) + U(i - 1, j, k))) * inv_dx +
+                                     std::fabs(0.5 * (V(i, j, k) + V(i, j - 1, k))) * inv_dy +
+                                     std::fabs(0.5 * (W(i, j, k) + W(i, j, k - 1))) * inv_dz;
+                    conv = std::max(conv, c);
+                    visc = std::max(visc, (prm.nu + nu_t(i, j, k)) * 2.0 * (inv_dx2 + inv_dy2 + inv_dz2));
+                }
+            }
+        conv_out = conv * dt();
+        visc_out = visc * dt();
+    }
+    // select_dt (src/monitor.f90:429-444) without the output-landing adjustments
+    void select_dt() {
+        double conv = 0.0, visc = 0.0;
+        compute_cfl(conv, visc);
+        const double cfl_now = std::max(conv, visc);
+        if (cfl_adaptive == 1 && cfl_now > 0.0) dt_cur = std::max(dt_min, std::min(dt_max, dt() * cfl_target / cfl_now * cfl_safety));
+    }
 
     // ---- projection (src/projection.f90) ----
     void compute_pseudo_pressure_rhs() {   // :37-63
@@ -992,6 +1023,7 @@ struct Oracle {
     }
     void step() {
         compute_sgs_model();
+        if (cfl_adaptive == 1) select_dt();   // from the start-of-step velocity, after nu_t (src/time_integration.f90:146-160)
         double to = t;
         Uo.d = U.d; Vo.d = V.d; Wo.d = W.d;
         if (prm.flow_forcing_mode == 0) { dPdx = prm.dPdx; dPdz = prm.dPdz; } else { dPdx = 0.0; dPdz = prm.dPdz; }
@@ -1058,6 +1090,14 @@ void orc_set_nu_t(void *h, const double *nu_t) { copy_in(((Oracle *)h)->nu_t, nu
 void orc_apply_bc(void *h) { ((Oracle *)h)->apply_boundary_conditions(); }
 void orc_step(void *h, int nsteps) { for (int n = 0; n < nsteps; ++n) ((Oracle *)h)->step(); }
 double orc_time(void *h) { return ((Oracle *)h)->t; }
+double orc_dt(void *h) { return ((Oracle *)h)->dt(); }
+void orc_set_adaptive(void *h, int enable, double target, double safety, double dtmin, double dtmax) {
+    Oracle *o = (Oracle *)h;
+    o->cfl_adaptive = enable ? 1 : 0;
+    o->cfl_target = target; o->cfl_safety = safety; o->dt_min = dtmin; o->dt_max = dtmax;
+    if (!enable) o->dt_cur = -1.0;
+}
+void orc_cfl(void *h, double *conv, double *visc) { ((Oracle *)h)->compute_cfl(*conv, *visc); }
 void orc_compute_sgs(void *h) { ((Oracle *)h)->compute_sgs_model(); }
 void orc_wall_model(void *h, int update_filter, double *tau_x, double *tau_z) {
     Oracle *o = (Oracle *)h;

@@ -67,6 +67,10 @@ def lib():
         L.orc_fft.argtypes = [c_int, POINTER(c_double), c_int]
         L.orc_zgtsv.restype = c_int
         L.orc_zgtsv.argtypes = [c_int] + [POINTER(c_double)] * 4
+        L.orc_dt.restype = c_double
+        L.orc_dt.argtypes = [c_void_p]
+        L.orc_set_adaptive.argtypes = [c_void_p, c_int, c_double, c_double, c_double, c_double]
+        L.orc_cfl.argtypes = [c_void_p, POINTER(c_double), POINTER(c_double)]
         L.orc_set_threads.argtypes = [c_int]
         L.orc_get_threads.restype = c_int
         _lib = L
@@ -133,6 +137,19 @@ class Oracle:
     @property
     def t(self) -> float:
         return float(lib().orc_time(self.h))
+
+    @property
+    def dt(self) -> float:
+        return float(lib().orc_dt(self.h))
+
+    def set_adaptive_dt(self, enable=True, cfl_target=0.5, cfl_safety=0.9, dt_min=1e-10, dt_max=1e10):
+        """cfl_adaptive = 1: dt from the CFL number at every step start (select_dt, src/monitor.f90:429)."""
+        lib().orc_set_adaptive(self.h, int(enable), cfl_target, cfl_safety, dt_min, dt_max)
+
+    def compute_cfl(self):
+        a, b = c_double(0.0), c_double(0.0)
+        lib().orc_cfl(self.h, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
 
     def compute_sgs_model(self):
         lib().orc_compute_sgs(self.h)

@@ -54,3 +54,25 @@ def oracle_mod():
     import oracle as O
     O.build()
     return O
+
+
+def cfl_reference(c, U, V, W, nu_t, dt=None):
+    """compute_cfl (src/monitor.f90:304-424) on the ghosted 1-based arrays: i = 2..nxg-1, j = 2..nyg-1,
+    k = 2..nzg-1, written out in numpy (0-based slices)."""
+    from dfdm import cases
+    x, y, z = cases.faces(c)
+    dx = np.diff(cases.centres(x)).min()
+    idx = 1.0 / dx
+    idy = 1.0 / np.maximum(y[1:] - y[:-1], 1e-14)      # index j-2 holds 1/(y(j) - y(j-1)) for j = 2..ny
+    idz = 1.0 / np.maximum(z[1:] - z[:-1], 1e-14)
+    nxg, nyg, nzg = c.nxg, c.nyg, c.nzg
+    I, J, K = slice(1, nxg - 1), slice(1, nyg - 1), slice(1, nzg - 1)
+    uc = 0.5 * (U[1:nxg - 1, J, K] + U[0:nxg - 2, J, K])
+    vc = 0.5 * (V[I, 1:nyg - 1, K] + V[I, 0:nyg - 2, K])
+    wc = 0.5 * (W[I, J, 1:nzg - 1] + W[I, J, 0:nzg - 2])
+    iy = idy[0:nyg - 2][None, :, None]
+    iz = idz[0:nzg - 2][None, None, :]
+    conv = (np.abs(uc) * idx + np.abs(vc) * iy + np.abs(wc) * iz).max()
+    visc = ((c.nu + nu_t[I, J, K]) * 2.0 * (idx * idx + iy * iy + iz * iz)).max()
+    dt = c.dt if dt is None else dt
+    return conv * dt, visc * dt

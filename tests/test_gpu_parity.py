@@ -6,7 +6,7 @@ the FP64 oracle; max |div u| after a projection 1e-12 relative to |u|/dy_min.
 import numpy as np
 import pytest
 
-from conftest import interior, rel_l2
+from conftest import cfl_reference, interior, rel_l2
 from dfdm import cases
 from dfdm.native import Solver
 
@@ -158,26 +158,6 @@ def test_not_finite_guard(oracle_mod):
     assert e.value.code == 5
 
 
-def _cfl_reference(c, U, V, W, nu_t):
-    """compute_cfl (src/monitor.f90:304-424) on the ghosted 1-based arrays: i = 2..nxg-1, j = 2..nyg-1,
-    k = 2..nzg-1, written out in numpy (0-based slices)."""
-    x, y, z = cases.faces(c)
-    dx = np.diff(cases.centres(x)).min()
-    idx = 1.0 / dx
-    idy = 1.0 / np.maximum(y[1:] - y[:-1], 1e-14)      # index j-2 holds 1/(y(j) - y(j-1)) for j = 2..ny
-    idz = 1.0 / np.maximum(z[1:] - z[:-1], 1e-14)
-    nxg, nyg, nzg = c.nxg, c.nyg, c.nzg
-    I, J, K = slice(1, nxg - 1), slice(1, nyg - 1), slice(1, nzg - 1)
-    uc = 0.5 * (U[1:nxg - 1, J, K] + U[0:nxg - 2, J, K])
-    vc = 0.5 * (V[I, 1:nyg - 1, K] + V[I, 0:nyg - 2, K])
-    wc = 0.5 * (W[I, J, 1:nzg - 1] + W[I, J, 0:nzg - 2])
-    iy = idy[0:nyg - 2][None, :, None]
-    iz = idz[0:nzg - 2][None, None, :]
-    conv = (np.abs(uc) * idx + np.abs(vc) * iy + np.abs(wc) * iz).max()
-    visc = ((c.nu + nu_t[I, J, K]) * 2.0 * (idx * idx + iy * iy + iz * iz)).max()
-    return conv * c.dt, visc * c.dt
-
-
 @pytest.mark.parametrize("name,prec,tol", [("chan_small", "fp64", 1e-13), ("chan_les_amd_small", "fp64", 1e-13),
                                            ("tgv_small", "fp64", 1e-13), ("chan_small", "fp32", 1e-6)])
 def test_cfl_matches_the_reference_formula(name, prec, tol):
@@ -189,7 +169,7 @@ def test_cfl_matches_the_reference_formula(name, prec, tol):
         s.compute_sgs_model()
     U, V, W, P = s.get_state()
     nut = s.get_nu_t() if c.sgs_model else np.zeros_like(P)
-    want = _cfl_reference(c, U, V, W, nut)
+    want = cfl_reference(c, U, V, W, nut)
     got = s.compute_cfl()
     for g, w in zip(got, want):
         assert abs(g - w) <= tol * w, (got, want)

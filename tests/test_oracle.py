@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 import scipy.linalg.lapack as lapack
 
-from conftest import interior, rel_l2
+from conftest import cfl_reference, interior, rel_l2
 from dfdm import cases
 
 
@@ -165,3 +165,42 @@ def test_golden_fixture_regression(oracle_mod):
         U, V, W, P = o.get_state()
         for key, arr in (("U", U), ("V", V), ("W", W), ("P", P)):
             assert rel_l2(arr, data[f"{name}_{key}"]) <= 1e-13, (name, key)
+
+
+@pytest.mark.parametrize("name", ["chan_small", "chan_les_amd_small", "tgv_small"])
+def test_cfl_matches_the_formula(oracle_mod, name):
+    """The oracle's compute_cfl against the numpy restatement of src/monitor.f90:304-424."""
+    c = cases.get(name)
+    o = _with_ic(oracle_mod, c)
+    o.step(2)
+    o.compute_sgs_model()
+    U, V, W, P = o.get_state()
+    nut = o.get_nu_t() if c.sgs_model else np.zeros_like(P)
+    want = cfl_reference(c, U, V, W, nut)
+    got = o.compute_cfl()
+    for g, w in zip(got, want):
+        assert abs(g - w) <= 1e-14 * w, (got, want)
+
+
+@pytest.mark.parametrize("name,target,dt_max", [("chan_les_amd_small", 0.5, 1e10), ("chan_small", 0.8, 1e10),
+                                                 ("tgv_small", 0.5, 1e-3)])
+def test_adaptive_dt_follows_select_dt(oracle_mod, name, target, dt_max):
+    """cfl_adaptive = 1: every step takes dt = max(dt_min, min(dt_max, dt*cfl_target/cfl*cfl_safety)) from the
+    start-of-step CFL number, after nu_t (src/time_integration.f90:146-160, src/monitor.f90:429-444)."""
+    c = cases.get(name)
+    o = _with_ic(oracle_mod, c)
+    o.set_adaptive_dt(True, target, 0.9, 1e-10, dt_max)
+    dt = c.dt
+    for _ in range(4):
+        o.compute_sgs_model()
+        U, V, W, P = o.get_state()
+        nut = o.get_nu_t() if c.sgs_model else np.zeros_like(P)
+        cfl = max(cfl_reference(c, U, V, W, nut, dt))
+        want = max(1e-10, min(dt_max, dt * target / cfl * 0.9))
+        t0 = o.t
+        o.step(1)
+        assert abs(o.dt - want) <= 1e-13 * want, (o.dt, want)
+        assert abs(o.t - (t0 + want)) <= 1e-13 * (t0 + want)
+        dt = want
+    if dt_max < 1.0:
+        assert o.dt == dt_max
