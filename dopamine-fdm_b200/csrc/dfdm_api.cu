@@ -98,6 +98,11 @@ struct dfdm_ctx {
     int red_blocks = 0;
     unsigned long long *d_maxdiv = nullptr;
     unsigned long long *d_cfl = nullptr;        // convective and viscous CFL maxima (bit patterns)
+    // adaptive time step (cfl_adaptive = 1): dt and t live on the device, {dt, t} in d_dtt, chosen by k_select_dt
+    // at every step start, so a run of steps (or its graph) needs no host round trip
+    double *d_dtt = nullptr;
+    bool adaptive = false;
+    double cfl_target = 0.5, cfl_safety = 0.9, dt_min = 1e-10, dt_max = 1e10;
     int *d_flag = nullptr;
     double *staging = nullptr;
     size_t staging_n = 0;
@@ -252,6 +257,7 @@ template <typename T> PoissonArgs<T> poisson_args(dfdm_ctx *c) {
     a.inv_dx = (T)(1.0 / c->dx);
     a.norm = (double)((long long)c->d.Nx * (long long)c->d.Nz);
     a.pdiv = c->prm.dt * (3.0 / 4.0);
+    a.dtp = c->adaptive ? c->d_dtt : nullptr;
     a.fNx = make_fastdiv((unsigned)c->d.Nx);
     a.fNy = make_fastdiv((unsigned)c->d.Ny);
     a.fM = make_fastdiv((unsigned)(c->d.Nx / 2));
@@ -486,7 +492,7 @@ template <typename T> struct Impl {
             int filt = c->wm_filter_mode == 1;
             if (s == 1 && filt) {
                 k_wm_filter<T><<<g, 128, 0, st>>>(step_args<T>(c), c->wsd, f(c->u), f(c->w), c->wmf_seeded ? 0 : 1,
-                                                 c->prm.dt, c->prm.wm_filter_Tf_fac);
+                                                 c->prm.dt, c->adaptive ? c->d_dtt : nullptr, c->prm.wm_filter_Tf_fac);
                 CKL();
                 c->wmf_seeded = true;
             }
@@ -504,6 +510,7 @@ template <typename T> struct Impl {
             sc.c1 = 1.0 / 4.0;
             sc.c2 = (s == 2) ? 5.0 / 12.0 : 3.0 / 4.0;
             sc.incr = incr_form(c, s);
+            sc.dtp = c->adaptive ? c->d_dtt : nullptr;
             return stage_kernel(c, sc, nullptr);
         }
         case 2:   // div + forward x
@@ -604,10 +611,26 @@ template <typename T> struct Impl {
     }
 
     // compute_time_step_RK3, single-phase flag set (src/time_integration.f90:120-713)
+    // the CFL maxima of the resident state into d_cfl (zeroed first)
+    static int cfl_maxima(dfdm_ctx *c) {
+        CK(cudaMemsetAsync(c->d_cfl, 0, 2 * sizeof(unsigned long long), c->stream));
+        k_cfl<T><<<c->red_blocks, 256, 0, c->stream>>>(c->d, f(c->u), f(c->v), f(c->w), c->les ? f(c->nut) : nullptr,
+                                                        c->d_ubd, 1.0 / c->dx, c->d_dyc, c->d_dzc, c->prm.nu, c->d_cfl);
+        CKL();
+        return DFDM_OK;
+    }
+    static int select_dt(dfdm_ctx *c) {
+        if (int rc = cfl_maxima(c)) return rc;
+        k_select_dt<<<1, 32, 0, c->stream>>>(c->d_cfl, c->d_dtt, c->cfl_target, c->cfl_safety, c->dt_min, c->dt_max);
+        CKL();
+        return DFDM_OK;
+    }
+
     static int step_enqueue(dfdm_ctx *c) {
         int rc;
         for (int s = 1; s <= 3; ++s) {
             if ((rc = launch(c, 0, s))) return rc;   // SGS (step start, then stages 2 and 3)
+            if (s == 1 && c->adaptive && (rc = select_dt(c))) return rc;   // dt from the start-of-step CFL, after nu_t
             if ((rc = launch(c, 8, s))) return rc;   // wall model
             if ((rc = launch(c, 1, s))) return rc;   // RHS + RK update
             if ((rc = poisson_chain(c, s))) return rc;
@@ -944,6 +967,8 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
     c->d_maxdiv = (unsigned long long *)tmp;
     if ((rc = dalloc(c, &tmp, 2 * sizeof(unsigned long long)))) return bail(rc);
     c->d_cfl = (unsigned long long *)tmp;
+    if ((rc = dalloc(c, &tmp, 2 * sizeof(double)))) return bail(rc);
+    c->d_dtt = (double *)tmp;
     if ((rc = dalloc(c, &tmp, sizeof(int)))) return bail(rc);
     c->d_flag = (int *)tmp;
     c->in_create = false;   // later buffers (host staging, the unit RHS output) are separate allocations
@@ -1073,16 +1098,62 @@ int dfdm_set_nu_t(dfdm_ctx *c, const double *nu_t) {
     return DFDM_OK;
 }
 
+// {dt, t} of the adaptive time step between the device and the host copies (c->t; dt into *dt)
+static int pull_dtt(dfdm_ctx *c, double *dt) {
+    double v[2] = {c->prm.dt, c->t};
+    if (c->adaptive) {
+        CK(cudaMemcpyAsync(v, c->d_dtt, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        c->t = v[1];
+    }
+    if (dt) *dt = v[0];
+    return DFDM_OK;
+}
+static int push_dtt(dfdm_ctx *c, double dt) {
+    const double v[2] = {dt, c->t};
+    CK(cudaMemcpyAsync(c->d_dtt, v, sizeof(v), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DFDM_OK;
+}
+
 int dfdm_set_time(dfdm_ctx *c, double t) {
     if (int rc = check_ctx(c)) return rc;
+    if (!c->adaptive) { c->t = t; return DFDM_OK; }
+    double dt = 0.0;
+    if (int rc = pull_dtt(c, &dt)) return rc;
     c->t = t;
-    return DFDM_OK;
+    return push_dtt(c, dt);
 }
 
 int dfdm_get_time(dfdm_ctx *c, double *t) {
     if (int rc = check_ctx(c)) return rc;
+    if (int rc = pull_dtt(c, nullptr)) return rc;
     if (t) *t = c->t;
     return DFDM_OK;
+}
+
+int dfdm_get_dt(dfdm_ctx *c, double *dt) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (!dt) return fail(DFDM_ERR_INVALID, "null output");
+    return pull_dtt(c, dt);
+}
+
+int dfdm_set_adaptive_dt(dfdm_ctx *c, int enable, double cfl_target, double cfl_safety, double dt_min, double dt_max) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (enable) {
+        if (!(cfl_target > 0.0) || !(cfl_safety > 0.0)) return fail(DFDM_ERR_INVALID, "cfl_target and cfl_safety must be > 0");
+        if (!(dt_min > 0.0) || !(dt_max >= dt_min)) return fail(DFDM_ERR_INVALID, "need 0 < dt_min <= dt_max");
+    }
+    double dt = c->prm.dt;
+    if (int rc = pull_dtt(c, &dt)) return rc;   // the current time (and dt, when it was adaptive already)
+    CK(cudaStreamSynchronize(c->stream));
+    destroy_graph(c);   // the captured kernels read dt from the host value or from d_dtt
+    if (!enable) { c->adaptive = false; return DFDM_OK; }   // back to the fixed dt of the parameters
+    c->cfl_target = cfl_target; c->cfl_safety = cfl_safety; c->dt_min = dt_min; c->dt_max = dt_max;
+    c->adaptive = true;
+    return push_dtt(c, dt);
 }
 
 // ---- the step ----
@@ -1113,7 +1184,7 @@ static int step_n(dfdm_ctx *c, int nsteps) {
             c->launches += g_launches - before;
             if (rc) return rc;
         }
-        c->t = to + 1.0 * c->prm.dt;   // t = to + rk_t(3)*dt
+        if (!c->adaptive) c->t = to + 1.0 * c->prm.dt;   // t = to + rk_t(3)*dt (adaptive: k_select_dt advances t)
         c->projected = true;
     }
     return DFDM_OK;
@@ -1130,6 +1201,7 @@ int dfdm_compute_time_step_rk3(dfdm_ctx *c, int nsteps, double *t) {
     int rc = dfdm_compute_time_step_rk3_async(c, nsteps);
     if (rc) return rc;
     CK(cudaStreamSynchronize(c->stream));
+    if (int rc2 = pull_dtt(c, nullptr)) return rc2;
     if (t) *t = c->t;
     return DFDM_OK;
 }
@@ -1557,23 +1629,16 @@ int dfdm_compute_cfl(dfdm_ctx *c, double *cfl_conv, double *cfl_visc) {
     g_err.clear();
     if (int rc = check_ctx(c)) return rc;
     if (!cfl_conv || !cfl_visc) return fail(DFDM_ERR_INVALID, "null output");
-    CK(cudaMemsetAsync(c->d_cfl, 0, 2 * sizeof(unsigned long long), c->stream));
-    int rc = dispatch(c, [&](auto impl) {
-        typedef decltype(impl) I;
-        k_cfl<typename std::remove_pointer<decltype(I::f(nullptr))>::type><<<c->red_blocks, 256, 0, c->stream>>>(
-            c->d, I::f(c->u), I::f(c->v), I::f(c->w), c->les ? I::f(c->nut) : nullptr, c->d_ubd, 1.0 / c->dx, c->d_dyc,
-            c->d_dzc, c->prm.nu, c->d_cfl);
-        CKL();
-        return DFDM_OK;
-    });
+    int rc = dispatch(c, [&](auto impl) { return decltype(impl)::cfl_maxima(c); });
     if (rc) return rc;
     unsigned long long bits[2] = {0, 0};
     CK(cudaMemcpyAsync(bits, c->d_cfl, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    double m[2];
+    double m[2], dt = c->prm.dt;
     std::memcpy(m, bits, sizeof(m));
-    *cfl_conv = m[0] * c->prm.dt;
-    *cfl_visc = m[1] * c->prm.dt;
+    if ((rc = pull_dtt(c, &dt))) return rc;   // the CFL numbers of the current dt
+    *cfl_conv = m[0] * dt;
+    *cfl_visc = m[1] * dt;
     return DFDM_OK;
 }
 

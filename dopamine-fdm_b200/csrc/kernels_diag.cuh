@@ -129,20 +129,30 @@ __global__ void __launch_bounds__(256) k_cfl(Dims d, const T *__restrict__ U, co
                                              const T *__restrict__ W, const T *__restrict__ NU,
                                              const double *__restrict__ ubd, double inv_dx, const double *__restrict__ dyc,
                                              const double *__restrict__ dzc, double nu, unsigned long long *__restrict__ out) {
+    // whole x-rows (row = k*Ny + j) per block, as k_bulk_partial: no per-cell index division
     double mc = 0.0, mv = 0.0;
     const double idx2 = inv_dx * inv_dx;
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x) {
-        int i = (int)(p % d.Nx);
-        long long q = p / d.Nx;
-        int j = (int)(q % d.Ny), k = (int)(q / d.Ny);
+    const int rows = d.Ny * d.Nz, Nx = d.Nx;
+#pragma unroll 2
+    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int k = row / d.Ny, j = row - k * d.Ny;
         const double ub = ubd[j];
-        const double uc = 0.5 * (((double)U[p] + ub) + ((double)U[idx3(d, wrap(i - 1, d.Nx), j, k)] + ub));
-        const double vc = 0.5 * ((double)ld_yf(V, d, i, j, k) + (double)ld_yf(V, d, i, j - 1, k));
-        const double wc = 0.5 * ((double)W[p] + (double)W[idx3(d, i, j, wrap(k - 1, d.Nz))]);
         const double idy = 1.0 / fmax(dyc[j], 1e-14), idz = 1.0 / fmax(dzc[k], 1e-14);
-        mc = fmax(mc, fabs(uc) * inv_dx + fabs(vc) * idy + fabs(wc) * idz);
-        const double nt = NU ? (double)NU[p] : 0.0;
-        mv = fmax(mv, (nu + nt) * 2.0 * (idx2 + idy * idy + idz * idz));
+        const double lap = idx2 + idy * idy + idz * idz;
+        const T *Ur = U + (size_t)row * Nx, *Vr = V + (size_t)row * Nx, *Wr = W + (size_t)row * Nx;
+        // V at j-1 (periodic wrap, or the zero wall value below the first row) and W at k-1 (periodic)
+        const int jm = j - 1 < 0 ? (d.yper ? d.Ny - 1 : -1) : j - 1;
+        const T *Vm = jm < 0 ? nullptr : V + ((size_t)k * d.Ny + jm) * Nx;
+        const T *Wm = W + ((size_t)(k == 0 ? d.Nz - 1 : k - 1) * d.Ny + j) * Nx;
+        const T *Nr = NU ? NU + (size_t)row * Nx : nullptr;
+        for (int i = threadIdx.x; i < Nx; i += blockDim.x) {
+            const double uc = 0.5 * (((double)Ur[i] + ub) + ((double)Ur[i == 0 ? Nx - 1 : i - 1] + ub));
+            const double vc = 0.5 * ((double)Vr[i] + (Vm ? (double)Vm[i] : 0.0));
+            const double wc = 0.5 * ((double)Wr[i] + (double)Wm[i]);
+            mc = fmax(mc, fabs(uc) * inv_dx + fabs(vc) * idy + fabs(wc) * idz);
+            const double nt = Nr ? (double)Nr[i] : 0.0;
+            mv = fmax(mv, (nu + nt) * 2.0 * lap);
+        }
     }
     for (int o = 16; o > 0; o >>= 1) {
         mc = fmax(mc, __shfl_down_sync(0xffffffffu, mc, o));
@@ -152,6 +162,20 @@ __global__ void __launch_bounds__(256) k_cfl(Dims d, const T *__restrict__ U, co
         atomicMax(out, (unsigned long long)__double_as_longlong(mc));
         atomicMax(out + 1, (unsigned long long)__double_as_longlong(mv));
     }
+}
+
+// select_dt with cfl_adaptive = 1 (src/monitor.f90:429-444): the CFL maxima of k_cfl times the current dt give
+// cfl_now = max(cfl_conv, cfl_visc); dt = max(dt_min, min(dt_max, dt*cfl_target/cfl_now*cfl_safety)) when
+// cfl_now > 0; then t += dt, the time at the end of the coming step.  dtt = {dt, t}; one thread.
+__global__ void k_select_dt(const unsigned long long *__restrict__ cfl, double *__restrict__ dtt, double cfl_target,
+                            double cfl_safety, double dt_min, double dt_max) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double dt = dtt[0];
+    const double conv = __longlong_as_double((long long)cfl[0]) * dt, visc = __longlong_as_double((long long)cfl[1]) * dt;
+    const double now = fmax(conv, visc);
+    if (now > 0.0) dt = fmax(dt_min, fmin(dt_max, dt * cfl_target / now * cfl_safety));
+    dtt[0] = dt;
+    dtt[1] += dt;
 }
 
 // Volume-weighted kinetic energy 0.5 <u.u> with face velocities averaged to the centres (compensated sums).

@@ -17,6 +17,7 @@ template <typename T> struct PoissonArgs {
     T inv_dx;
     double norm;              // nxp*nzp
     double pdiv;              // dt*rk_coef(3,3)
+    const double *dtp;        // adaptive time step: pdiv = dtp[0]*rk_coef(3,3) from device memory (null: fixed dt)
     FastDiv fNx, fNy, fM, fM1;   // division by Nx, Ny, Nx/2, Nx/2+1
 };
 
@@ -363,8 +364,9 @@ __global__ void __launch_bounds__(256) k_correct(PoissonArgs<T> a, const T *__re
         V[p] = sv - (pyp - pc) * A::inv(a.my.df, a.my.idf, j);
     }
     if (P) {
-        if (sizeof(T) == 8) P[p] = (T)((double)pc / a.pdiv);
-        else P[p] = pc * (T)(1.0 / a.pdiv);
+        const double pdiv = a.dtp ? *a.dtp * (3.0 / 4.0) : a.pdiv;
+        if (sizeof(T) == 8) P[p] = (T)((double)pc / pdiv);
+        else P[p] = pc * (T)(1.0 / pdiv);
     }
 }
 
@@ -418,11 +420,12 @@ __global__ void __launch_bounds__(256) k_correct4(PoissonArgs<T> a, const T *__r
     }
     if (P) {
         V4 o;
+        const double pdiv = a.dtp ? *a.dtp * (3.0 / 4.0) : a.pdiv;
         if (sizeof(T) == 8) {
-            o.x = (T)((double)pc.x / a.pdiv); o.y = (T)((double)pc.y / a.pdiv);
-            o.z = (T)((double)pc.z / a.pdiv); o.w = (T)((double)pc.w / a.pdiv);
+            o.x = (T)((double)pc.x / pdiv); o.y = (T)((double)pc.y / pdiv);
+            o.z = (T)((double)pc.z / pdiv); o.w = (T)((double)pc.w / pdiv);
         } else {
-            const T r = (T)(1.0 / a.pdiv);
+            const T r = (T)(1.0 / pdiv);
             o.x = pc.x * r; o.y = pc.y * r; o.z = pc.z * r; o.w = pc.w * r;
         }
         *reinterpret_cast<V4 *>(P + p) = o;

@@ -118,8 +118,9 @@ struct WallState {
 // update_wm_filter (src/wallmodel.f90:397-439): one thread per (i,k), both walls, U-face and W-face sets.
 template <typename T>
 __global__ void k_wm_filter(StepArgs<T> a, WallState ws, const T *__restrict__ U, const T *__restrict__ W, int seed,
-                            double dt, double Tf_fac) {
+                            double dt_fixed, const double *__restrict__ dtp, double Tf_fac) {
     const Dims &d = a.d;
+    const double dt = dtp ? *dtp : dt_fixed;   // adaptive time step: from device memory
     int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
     if (i >= d.Nx) return;
     const double kap = 0.41;
@@ -439,6 +440,7 @@ struct StageCoef {
     double dt;       // dt, stages 2 and 3
     double c1, c2;   // rk_coef(s,1) and rk_coef(s,s), stages 2 and 3
     int incr;        // store the increment du = dt (c1 F1 + c2 rhs) instead of u* = uo + du; uo is not read
+    const double *dtp = nullptr;   // adaptive time step: dt is dtp[0] (device memory) and dt_a11, dt are not used
 };
 
 // Shared-memory neighbourhood of one thread: three z-planes (k-1, k, k+1) of each field, each plane a
@@ -609,13 +611,13 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
                 if (rhs_only) {
                     rhs_only[p] = ru; rhs_only[d.cells + p] = rv; rhs_only[2 * d.cells + p] = rw;
                 } else if (sc.stage == 1) {
-                    T c = (T)sc.dt_a11;
+                    T c = (T)(sc.dtp ? *sc.dtp * (8.0 / 15.0) : sc.dt_a11);
                     T u0 = q.Ud(0, 0, 0), w0 = q.W(0, 0, 0);   // U as stored (deviation from the base profile)
                     uo[p] = u0; f1u[p] = ru; us[p] = u0 + c * ru;
                     wo[p] = w0; f1w[p] = rw; wsf[p] = w0 + c * rw;
                     if (vrow) { T v0 = q.V(0, 0, 0); vo[p] = v0; f1v[p] = rv; vs[p] = v0 + c * rv; }
                 } else {
-                    T c1 = (T)sc.c1, c2 = (T)sc.c2, dtt = (T)sc.dt;   // with sc.incr the base stays zero: du
+                    T c1 = (T)sc.c1, c2 = (T)sc.c2, dtt = (T)(sc.dtp ? *sc.dtp : sc.dt);   // with sc.incr the base stays zero: du
                     us[p] = ou + dtt * (c1 * fu + c2 * ru);
                     wsf[p] = ow + dtt * (c1 * fw + c2 * rw);
                     if (vrow) vs[p] = ov + dtt * (c1 * fv + c2 * rv);
@@ -754,13 +756,13 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
             if (rhs_only) {
                 st2(rhs_only, ru); st2(rhs_only + d.cells, rv); st2(rhs_only + 2 * d.cells, rw);
             } else if (sc.stage == 1) {
-                const F2 c = F2(sc.dt_a11);
+                const F2 c = F2(sc.dtp ? *sc.dtp * (8.0 / 15.0) : sc.dt_a11);
                 F2 u0 = q.Ud(0, 0, 0), w0 = q.W(0, 0, 0);
                 st2(uo, u0); st2(f1u, ru); st2(us, u0 + c * ru);
                 st2(wo, w0); st2(f1w, rw); st2(wsf, w0 + c * rw);
                 if (vrow) { F2 v0 = q.V(0, 0, 0); st2(vo, v0); st2(f1v, rv); st2(vs, v0 + c * rv); }
             } else {
-                const F2 c1 = F2(sc.c1), c2 = F2(sc.c2), dtt = F2(sc.dt);
+                const F2 c1 = F2(sc.c1), c2 = F2(sc.c2), dtt = F2(sc.dtp ? *sc.dtp : sc.dt);
                 st2(us, ou + dtt * (c1 * fu + c2 * ru));
                 st2(wsf, ow + dtt * (c1 * fw + c2 * rw));
                 if (vrow) st2(vs, ov + dtt * (c1 * fv + c2 * rv));

@@ -31,7 +31,8 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_solve_poisson", "dfdm_compute_bulk_velocity", "dfdm_check_divergence", "dfdm_kinetic_energy",
            "dfdm_check_finite", "dfdm_pad_field", "dfdm_launch_kernel_async", "dfdm_kernel_bytes",
            "dfdm_launch_count", "dfdm_solve_poisson_noalloc", "dfdm_write_snapshot", "dfdm_read_snapshot",
-           "dfdm_compute_cfl", "dfdm_set_stage_variant", "dfdm_get_stage_variant"]
+           "dfdm_compute_cfl", "dfdm_set_stage_variant", "dfdm_get_stage_variant", "dfdm_set_adaptive_dt",
+           "dfdm_get_dt"]
 
 
 class DfdmError(RuntimeError):
@@ -94,6 +95,8 @@ def load(build_if_missing: bool = True):
         "dfdm_compute_cfl": (c_int, [c_void_p, P, P]),
         "dfdm_set_stage_variant": (c_int, [c_void_p, c_int]),
         "dfdm_get_stage_variant": (c_int, [c_void_p, POINTER(ctypes.c_int), P, P]),
+        "dfdm_set_adaptive_dt": (c_int, [c_void_p, c_int, c_double, c_double, c_double, c_double]),
+        "dfdm_get_dt": (c_int, [c_void_p, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -194,6 +197,9 @@ class Solver:
         a = np.asfortranarray(a, dtype=np.float64)
         _check(load().dfdm_set_nu_t(self.h, dptr(a)))
 
+    def set_time(self, t: float):
+        _check(load().dfdm_set_time(self.h, float(t)))
+
     @property
     def t(self) -> float:
         v = c_double(0.0)
@@ -275,6 +281,17 @@ class Solver:
         a, b = c_double(0.0), c_double(0.0)
         _check(load().dfdm_compute_cfl(self.h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def set_adaptive_dt(self, enable=True, cfl_target=0.5, cfl_safety=0.9, dt_min=1e-10, dt_max=1e10):
+        """cfl_adaptive = 1: dt chosen on the device from the start-of-step CFL number at every step
+        (select_dt, src/monitor.f90:429-444)."""
+        _check(load().dfdm_set_adaptive_dt(self.h, int(enable), cfl_target, cfl_safety, dt_min, dt_max))
+
+    @property
+    def dt(self) -> float:
+        v = c_double(0.0)
+        _check(load().dfdm_get_dt(self.h, ctypes.byref(v)))
+        return v.value
 
     def kinetic_energy(self) -> float:
         v = c_double(0.0)

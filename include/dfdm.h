@@ -177,6 +177,16 @@ int dfdm_check_divergence(dfdm_ctx *ctx, double *max_div);
 /* compute_cfl (src/monitor.f90:304-424) for the single-phase path: dt * max over the centres of
  * |u_c|/dx + |v_c|/dy + |w_c|/dz (convective) and of (nu + nu_t) * 2 * (1/dx^2 + 1/dy^2 + 1/dz^2) (viscous). */
 int dfdm_compute_cfl(dfdm_ctx *ctx, double *cfl_conv, double *cfl_visc);
+/* Adaptive time step, cfl_adaptive = 1 of &TIME (src/global.f90:472-478): with enable != 0 every step starts, after
+ * the SGS eddy viscosity, with select_dt (src/monitor.f90:429-444; src/time_integration.f90:146-160):
+ * dt = max(dt_min, min(dt_max, dt * cfl_target / cfl * cfl_safety)) from cfl = max(cfl_conv, cfl_visc) of the
+ * start-of-step velocity and the previous dt (the &NUMERICS dt before the first step).  dt and t stay on the device,
+ * so steps and their graph replays need no host synchronisation; dfdm_get_dt / dfdm_get_time read them.  The
+ * output-landing shrink of select_dt (nsave < 0, nsteps < 0) belongs to the driver's output loop and is not
+ * applied.  enable = 0 returns to the fixed dt.  Requires cfl_target, cfl_safety > 0 and 0 < dt_min <= dt_max. */
+int dfdm_set_adaptive_dt(dfdm_ctx *ctx, int enable, double cfl_target, double cfl_safety, double dt_min, double dt_max);
+/* The dt of the last step taken (adaptive) or the fixed dt. */
+int dfdm_get_dt(dfdm_ctx *ctx, double *dt);
 /* Kinetic energy 0.5*<u.u> (volume-weighted, compensated sum) -- diagnostic with no reference counterpart. */
 int dfdm_kinetic_energy(dfdm_ctx *ctx, double *ke);
 /* Monitor guard of output_monitor (src/monitor.f90:32-52): DFDM_ERR_NOT_FINITE if any velocity is NaN/Inf or
