@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--no-kernels", action="store_true", help="skip the per-kernel roofline timings")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream measurement")
+    ap.add_argument("--no-adaptive", action="store_true", help="skip the adaptive-time-step run")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-vs-FP64 report of the other configs")
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-rate", type=float, default=4.0, help="Poisson arrival rate, requests/s")
@@ -249,10 +250,12 @@ def main():
 
     U, V, W, P = cases.initial_condition(c)
 
-    def timed_run(prec, sample_clocks=False):
+    def timed_run(prec, sample_clocks=False, adaptive=False):
         s = Solver(c, prec, graphs=True)
         s.set_stream(sh)
         s.set_state(U, V, W, P)
+        if adaptive:
+            s.set_adaptive_dt(True, 0.5, 0.9)
         s.compute_time_step_RK3(args.warmup)
         barrier_sync()
         l0 = s.launch_count()
@@ -295,6 +298,14 @@ def main():
                        "fp32_speedup": value / v64,
                        "rel_l2_fp32_vs_fp64": rel, "steps_compared": args.warmup + args.steps}
         s64.close()
+
+    # ---- the same step with the adaptive time step (cfl_adaptive = 1): CFL maxima and dt choice on the device ----
+    if not args.no_adaptive:
+        sa, msa, _, la = timed_run("fp32", adaptive=True)
+        out["adaptive_dt"] = {"value": ws * c.n_cells * args.steps / (msa / 1e3), "ms_per_step": msa / args.steps,
+                              "overhead_ms_per_step": (msa - ms32) / args.steps, "gpu_launches": la,
+                              "dt_last": sa.dt, "cfl_target": 0.5, "cfl_safety": 0.9}
+        sa.close()
 
     # ---- roofline: per-kernel-family device time of one stage, dominant family against HBM peak ----
     peak, peak_kind = measured_peaks()

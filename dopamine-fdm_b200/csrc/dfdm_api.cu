@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <array>
+#include <limits>
 #include <map>
 #include <cmath>
 #include <cstdio>
@@ -98,11 +99,14 @@ struct dfdm_ctx {
     int red_blocks = 0;
     unsigned long long *d_maxdiv = nullptr;
     unsigned long long *d_cfl = nullptr;        // convective and viscous CFL maxima (bit patterns)
-    // adaptive time step (cfl_adaptive = 1): dt and t live on the device, {dt, t} in d_dtt, chosen by k_select_dt
-    // at every step start, so a run of steps (or its graph) needs no host round trip
+    // device time step: with the adaptive time step (cfl_adaptive = 1) or an output-landing target, dt and t live on
+    // the device in d_dtt = {dt of the step, t, landing target, dt before landing}, set by k_select_dt at every step
+    // start, so a run of steps (or its graph) needs no host round trip
     double *d_dtt = nullptr;
-    bool adaptive = false;
+    bool adaptive = false, landing = false;
     double cfl_target = 0.5, cfl_safety = 0.9, dt_min = 1e-10, dt_max = 1e10;
+    double t_land = std::numeric_limits<double>::quiet_NaN();
+    bool dev_dt() const { return adaptive || landing; }
     int *d_flag = nullptr;
     double *staging = nullptr;
     size_t staging_n = 0;
@@ -257,7 +261,7 @@ template <typename T> PoissonArgs<T> poisson_args(dfdm_ctx *c) {
     a.inv_dx = (T)(1.0 / c->dx);
     a.norm = (double)((long long)c->d.Nx * (long long)c->d.Nz);
     a.pdiv = c->prm.dt * (3.0 / 4.0);
-    a.dtp = c->adaptive ? c->d_dtt : nullptr;
+    a.dtp = c->dev_dt() ? c->d_dtt : nullptr;
     a.fNx = make_fastdiv((unsigned)c->d.Nx);
     a.fNy = make_fastdiv((unsigned)c->d.Ny);
     a.fM = make_fastdiv((unsigned)(c->d.Nx / 2));
@@ -492,7 +496,7 @@ template <typename T> struct Impl {
             int filt = c->wm_filter_mode == 1;
             if (s == 1 && filt) {
                 k_wm_filter<T><<<g, 128, 0, st>>>(step_args<T>(c), c->wsd, f(c->u), f(c->w), c->wmf_seeded ? 0 : 1,
-                                                 c->prm.dt, c->adaptive ? c->d_dtt : nullptr, c->prm.wm_filter_Tf_fac);
+                                                 c->prm.dt, c->dev_dt() ? c->d_dtt : nullptr, c->prm.wm_filter_Tf_fac);
                 CKL();
                 c->wmf_seeded = true;
             }
@@ -510,7 +514,7 @@ template <typename T> struct Impl {
             sc.c1 = 1.0 / 4.0;
             sc.c2 = (s == 2) ? 5.0 / 12.0 : 3.0 / 4.0;
             sc.incr = incr_form(c, s);
-            sc.dtp = c->adaptive ? c->d_dtt : nullptr;
+            sc.dtp = c->dev_dt() ? c->d_dtt : nullptr;
             return stage_kernel(c, sc, nullptr);
         }
         case 2:   // div + forward x
@@ -620,8 +624,10 @@ template <typename T> struct Impl {
         return DFDM_OK;
     }
     static int select_dt(dfdm_ctx *c) {
-        if (int rc = cfl_maxima(c)) return rc;
-        k_select_dt<<<1, 32, 0, c->stream>>>(c->d_cfl, c->d_dtt, c->cfl_target, c->cfl_safety, c->dt_min, c->dt_max);
+        if (c->adaptive)
+            if (int rc = cfl_maxima(c)) return rc;
+        k_select_dt<<<1, 32, 0, c->stream>>>(c->d_cfl, c->d_dtt, c->adaptive ? 1 : 0, c->cfl_target, c->cfl_safety,
+                                             c->dt_min, c->dt_max);
         CKL();
         return DFDM_OK;
     }
@@ -630,7 +636,7 @@ template <typename T> struct Impl {
         int rc;
         for (int s = 1; s <= 3; ++s) {
             if ((rc = launch(c, 0, s))) return rc;   // SGS (step start, then stages 2 and 3)
-            if (s == 1 && c->adaptive && (rc = select_dt(c))) return rc;   // dt from the start-of-step CFL, after nu_t
+            if (s == 1 && c->dev_dt() && (rc = select_dt(c))) return rc;   // dt from the start-of-step CFL, after nu_t
             if ((rc = launch(c, 8, s))) return rc;   // wall model
             if ((rc = launch(c, 1, s))) return rc;   // RHS + RK update
             if ((rc = poisson_chain(c, s))) return rc;
@@ -967,7 +973,7 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
     c->d_maxdiv = (unsigned long long *)tmp;
     if ((rc = dalloc(c, &tmp, 2 * sizeof(unsigned long long)))) return bail(rc);
     c->d_cfl = (unsigned long long *)tmp;
-    if ((rc = dalloc(c, &tmp, 2 * sizeof(double)))) return bail(rc);
+    if ((rc = dalloc(c, &tmp, 4 * sizeof(double)))) return bail(rc);
     c->d_dtt = (double *)tmp;
     if ((rc = dalloc(c, &tmp, sizeof(int)))) return bail(rc);
     c->d_flag = (int *)tmp;
@@ -1098,19 +1104,20 @@ int dfdm_set_nu_t(dfdm_ctx *c, const double *nu_t) {
     return DFDM_OK;
 }
 
-// {dt, t} of the adaptive time step between the device and the host copies (c->t; dt into *dt)
+// the device time step: d_dtt = {dt of the last step, t, landing target, dt} to the host (c->t, c->t_land; the dt
+// before landing into *dt) and back
 static int pull_dtt(dfdm_ctx *c, double *dt) {
-    double v[2] = {c->prm.dt, c->t};
-    if (c->adaptive) {
+    double v[4] = {c->prm.dt, c->t, c->t_land, c->prm.dt};
+    if (c->dev_dt()) {
         CK(cudaMemcpyAsync(v, c->d_dtt, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
         c->t = v[1];
     }
-    if (dt) *dt = v[0];
+    if (dt) *dt = v[3];
     return DFDM_OK;
 }
 static int push_dtt(dfdm_ctx *c, double dt) {
-    const double v[2] = {dt, c->t};
+    const double v[4] = {dt, c->t, c->t_land, dt};
     CK(cudaMemcpyAsync(c->d_dtt, v, sizeof(v), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return DFDM_OK;
@@ -1118,7 +1125,7 @@ static int push_dtt(dfdm_ctx *c, double dt) {
 
 int dfdm_set_time(dfdm_ctx *c, double t) {
     if (int rc = check_ctx(c)) return rc;
-    if (!c->adaptive) { c->t = t; return DFDM_OK; }
+    if (!c->dev_dt()) { c->t = t; return DFDM_OK; }
     double dt = 0.0;
     if (int rc = pull_dtt(c, &dt)) return rc;
     c->t = t;
@@ -1147,13 +1154,29 @@ int dfdm_set_adaptive_dt(dfdm_ctx *c, int enable, double cfl_target, double cfl_
         if (!(dt_min > 0.0) || !(dt_max >= dt_min)) return fail(DFDM_ERR_INVALID, "need 0 < dt_min <= dt_max");
     }
     double dt = c->prm.dt;
-    if (int rc = pull_dtt(c, &dt)) return rc;   // the current time (and dt, when it was adaptive already)
+    if (int rc = pull_dtt(c, &dt)) return rc;   // the current time (and dt, when it was on the device already)
     CK(cudaStreamSynchronize(c->stream));
     destroy_graph(c);   // the captured kernels read dt from the host value or from d_dtt
-    if (!enable) { c->adaptive = false; return DFDM_OK; }   // back to the fixed dt of the parameters
+    if (!enable) {
+        c->adaptive = false;   // back to the fixed dt of the parameters
+        return c->landing ? push_dtt(c, c->prm.dt) : DFDM_OK;
+    }
     c->cfl_target = cfl_target; c->cfl_safety = cfl_safety; c->dt_min = dt_min; c->dt_max = dt_max;
     c->adaptive = true;
     return push_dtt(c, dt);
+}
+
+int dfdm_set_landing_time(dfdm_ctx *c, int enable, double t_land) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (enable && !std::isfinite(t_land)) return fail(DFDM_ERR_INVALID, "the landing time must be finite");
+    double dt = c->prm.dt;
+    if (int rc = pull_dtt(c, &dt)) return rc;
+    const bool was = c->dev_dt();
+    c->landing = enable != 0;
+    c->t_land = enable ? t_land : std::nan("");
+    if (was != c->dev_dt()) destroy_graph(c);   // a new target alone keeps the graph: it is read from d_dtt
+    return c->dev_dt() ? push_dtt(c, dt) : DFDM_OK;
 }
 
 // ---- the step ----
@@ -1184,7 +1207,7 @@ static int step_n(dfdm_ctx *c, int nsteps) {
             c->launches += g_launches - before;
             if (rc) return rc;
         }
-        if (!c->adaptive) c->t = to + 1.0 * c->prm.dt;   // t = to + rk_t(3)*dt (adaptive: k_select_dt advances t)
+        if (!c->dev_dt()) c->t = to + 1.0 * c->prm.dt;   // t = to + rk_t(3)*dt (device dt: k_select_dt advances t)
         c->projected = true;
     }
     return DFDM_OK;

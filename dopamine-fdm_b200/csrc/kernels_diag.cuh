@@ -164,16 +164,25 @@ __global__ void __launch_bounds__(256) k_cfl(Dims d, const T *__restrict__ U, co
     }
 }
 
-// select_dt with cfl_adaptive = 1 (src/monitor.f90:429-444): the CFL maxima of k_cfl times the current dt give
-// cfl_now = max(cfl_conv, cfl_visc); dt = max(dt_min, min(dt_max, dt*cfl_target/cfl_now*cfl_safety)) when
-// cfl_now > 0; then t += dt, the time at the end of the coming step.  dtt = {dt, t}; one thread.
-__global__ void k_select_dt(const unsigned long long *__restrict__ cfl, double *__restrict__ dtt, double cfl_target,
-                            double cfl_safety, double dt_min, double dt_max) {
+// select_dt (src/monitor.f90:429-458) at a step start.  dtt = {dt of the coming step, t, landing target, dt}:
+// with `adaptive`, the CFL maxima of k_cfl times dt give cfl_now = max(cfl_conv, cfl_visc) and
+// dt = max(dt_min, min(dt_max, dt*cfl_target/cfl_now*cfl_safety)) when cfl_now > 0 (kept in dtt[3], the
+// reference's dt_presnap); then landing_dt shrinks the step so that t lands on dtt[2] (NaN: no target; a target
+// within 1e-10 counts as reached): a remainder below 2 dt in one step, one between dt and 2 dt in two halves.
+// t += the step.  One thread.
+__global__ void k_select_dt(const unsigned long long *__restrict__ cfl, double *__restrict__ dtt, int adaptive,
+                            double cfl_target, double cfl_safety, double dt_min, double dt_max) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double dt = dtt[0];
-    const double conv = __longlong_as_double((long long)cfl[0]) * dt, visc = __longlong_as_double((long long)cfl[1]) * dt;
-    const double now = fmax(conv, visc);
-    if (now > 0.0) dt = fmax(dt_min, fmin(dt_max, dt * cfl_target / now * cfl_safety));
+    double dt = dtt[3];
+    if (adaptive) {
+        const double conv = __longlong_as_double((long long)cfl[0]) * dt;
+        const double visc = __longlong_as_double((long long)cfl[1]) * dt;
+        const double now = fmax(conv, visc);
+        if (now > 0.0) dt = fmax(dt_min, fmin(dt_max, dt * cfl_target / now * cfl_safety));
+    }
+    dtt[3] = dt;
+    const double rem = dtt[2] - dtt[1];
+    if (rem > 1e-10 && rem < 2.0 * dt) dt = rem > dt ? 0.5 * rem : rem;
     dtt[0] = dt;
     dtt[1] += dt;
 }

@@ -32,7 +32,7 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_check_finite", "dfdm_pad_field", "dfdm_launch_kernel_async", "dfdm_kernel_bytes",
            "dfdm_launch_count", "dfdm_solve_poisson_noalloc", "dfdm_write_snapshot", "dfdm_read_snapshot",
            "dfdm_compute_cfl", "dfdm_set_stage_variant", "dfdm_get_stage_variant", "dfdm_set_adaptive_dt",
-           "dfdm_get_dt"]
+           "dfdm_get_dt", "dfdm_set_landing_time"]
 
 
 class DfdmError(RuntimeError):
@@ -97,6 +97,7 @@ def load(build_if_missing: bool = True):
         "dfdm_get_stage_variant": (c_int, [c_void_p, POINTER(ctypes.c_int), P, P]),
         "dfdm_set_adaptive_dt": (c_int, [c_void_p, c_int, c_double, c_double, c_double, c_double]),
         "dfdm_get_dt": (c_int, [c_void_p, P]),
+        "dfdm_set_landing_time": (c_int, [c_void_p, c_int, c_double]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -286,6 +287,10 @@ class Solver:
         """cfl_adaptive = 1: dt chosen on the device from the start-of-step CFL number at every step
         (select_dt, src/monitor.f90:429-444)."""
         _check(load().dfdm_set_adaptive_dt(self.h, int(enable), cfl_target, cfl_safety, dt_min, dt_max))
+
+    def set_landing_time(self, t_land=None):
+        """Shrink the coming steps so that t lands on t_land (landing_dt, src/monitor.f90:436-458); None: no target."""
+        _check(load().dfdm_set_landing_time(self.h, 0 if t_land is None else 1, 0.0 if t_land is None else float(t_land)))
 
     @property
     def dt(self) -> float:

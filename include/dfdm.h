@@ -181,11 +181,16 @@ int dfdm_compute_cfl(dfdm_ctx *ctx, double *cfl_conv, double *cfl_visc);
  * the SGS eddy viscosity, with select_dt (src/monitor.f90:429-444; src/time_integration.f90:146-160):
  * dt = max(dt_min, min(dt_max, dt * cfl_target / cfl * cfl_safety)) from cfl = max(cfl_conv, cfl_visc) of the
  * start-of-step velocity and the previous dt (the &NUMERICS dt before the first step).  dt and t stay on the device,
- * so steps and their graph replays need no host synchronisation; dfdm_get_dt / dfdm_get_time read them.  The
- * output-landing shrink of select_dt (nsave < 0, nsteps < 0) belongs to the driver's output loop and is not
- * applied.  enable = 0 returns to the fixed dt.  Requires cfl_target, cfl_safety > 0 and 0 < dt_min <= dt_max. */
+ * so steps and their graph replays need no host synchronisation; dfdm_get_dt / dfdm_get_time read them.
+ * enable = 0 returns to the fixed dt.  Requires cfl_target, cfl_safety > 0 and 0 < dt_min <= dt_max. */
 int dfdm_set_adaptive_dt(dfdm_ctx *ctx, int enable, double cfl_target, double cfl_safety, double dt_min, double dt_max);
-/* The dt of the last step taken (adaptive) or the fixed dt. */
+/* Output landing of select_dt (nsave < 0, nsteps < 0; src/monitor.f90:436-458): with enable != 0 the coming steps
+ * are shrunk by landing_dt so that t lands on t_land (a remainder below 2 dt in one step, one between dt and 2 dt in
+ * two equal halves); dt returns to its value before the shrink after the step (src/time_integration.f90:711).
+ * A target within 1e-10 of t counts as reached; the caller then sets the next one (a new target keeps the captured
+ * step graph).  Works with the fixed and with the adaptive dt.  t_land must be finite. */
+int dfdm_set_landing_time(dfdm_ctx *ctx, int enable, double t_land);
+/* The reference's dt between steps: the fixed dt, or the adaptive dt of the last step before any landing shrink. */
 int dfdm_get_dt(dfdm_ctx *ctx, double *dt);
 /* Kinetic energy 0.5*<u.u> (volume-weighted, compensated sum) -- diagnostic with no reference counterpart. */
 int dfdm_kinetic_energy(dfdm_ctx *ctx, double *ke);

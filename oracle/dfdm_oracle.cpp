@@ -816,12 +816,31 @@ struct Oracle {
         conv_out = conv * dt();
         visc_out = visc * dt();
     }
-    // select_dt (src/monitor.f90:429-444) without the output-landing adjustments
+    // output landing (nsave < 0 / nsteps < 0): the step is shrunk so that t lands on t_land; NaN: no target.  A
+    // target within 1e-10 of t counts as reached (the tolerance of src/time_integration.f90:597 and
+    // src/main.f90:90-91), and the caller moves it on.
+    double t_land = std::nan("");
+    double dt_presnap = -1.0;
+    // landing_dt (src/monitor.f90:450-458): a remainder below 2 dt is taken in one step, or in two equal halves
+    // when it is above dt
+    static double landing_dt(double dt_now, double rem) {
+        double r = dt_now;
+        if (rem < 2.0 * dt_now) {
+            r = rem;
+            if (rem > dt_now) r = 0.5 * rem;
+        }
+        return r;
+    }
+    // select_dt (src/monitor.f90:429-444), one landing target
     void select_dt() {
-        double conv = 0.0, visc = 0.0;
-        compute_cfl(conv, visc);
-        const double cfl_now = std::max(conv, visc);
-        if (cfl_adaptive == 1 && cfl_now > 0.0) dt_cur = std::max(dt_min, std::min(dt_max, dt() * cfl_target / cfl_now * cfl_safety));
+        if (cfl_adaptive == 1) {
+            double conv = 0.0, visc = 0.0;
+            compute_cfl(conv, visc);
+            const double cfl_now = std::max(conv, visc);
+            if (cfl_now > 0.0) dt_cur = std::max(dt_min, std::min(dt_max, dt() * cfl_target / cfl_now * cfl_safety));
+        }
+        dt_presnap = dt();
+        if (t_land - t > 1e-10) dt_cur = landing_dt(dt(), t_land - t);
     }
 
     // ---- projection (src/projection.f90) ----
@@ -1023,7 +1042,9 @@ struct Oracle {
     }
     void step() {
         compute_sgs_model();
-        if (cfl_adaptive == 1) select_dt();   // from the start-of-step velocity, after nu_t (src/time_integration.f90:146-160)
+        // dt from the start-of-step velocity, after nu_t (src/time_integration.f90:146-160)
+        const bool sel = cfl_adaptive == 1 || !std::isnan(t_land);
+        if (sel) select_dt();
         double to = t;
         Uo.d = U.d; Vo.d = V.d; Wo.d = W.d;
         if (prm.flow_forcing_mode == 0) { dPdx = prm.dPdx; dPdz = prm.dPdz; } else { dPdx = 0.0; dPdz = prm.dPdz; }
@@ -1046,6 +1067,7 @@ struct Oracle {
                     for (int i = 2; i <= nx - 1; ++i) U(i, j, k) = U(i, j, k) + dU;
             apply_boundary_conditions();
         }
+        if (sel) dt_cur = dt_presnap;   // dt = dt_presnap (src/time_integration.f90:711)
     }
 };
 
@@ -1097,6 +1119,7 @@ void orc_set_adaptive(void *h, int enable, double target, double safety, double 
     o->cfl_target = target; o->cfl_safety = safety; o->dt_min = dtmin; o->dt_max = dtmax;
     if (!enable) o->dt_cur = -1.0;
 }
+void orc_set_landing(void *h, double t_land) { ((Oracle *)h)->t_land = t_land; }
 void orc_cfl(void *h, double *conv, double *visc) { ((Oracle *)h)->compute_cfl(*conv, *visc); }
 void orc_compute_sgs(void *h) { ((Oracle *)h)->compute_sgs_model(); }
 void orc_wall_model(void *h, int update_filter, double *tau_x, double *tau_z) {

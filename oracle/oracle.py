@@ -71,6 +71,7 @@ def lib():
         L.orc_dt.argtypes = [c_void_p]
         L.orc_set_adaptive.argtypes = [c_void_p, c_int, c_double, c_double, c_double, c_double]
         L.orc_cfl.argtypes = [c_void_p, POINTER(c_double), POINTER(c_double)]
+        L.orc_set_landing.argtypes = [c_void_p, c_double]
         L.orc_set_threads.argtypes = [c_int]
         L.orc_get_threads.restype = c_int
         _lib = L
@@ -145,6 +146,10 @@ class Oracle:
     def set_adaptive_dt(self, enable=True, cfl_target=0.5, cfl_safety=0.9, dt_min=1e-10, dt_max=1e10):
         """cfl_adaptive = 1: dt from the CFL number at every step start (select_dt, src/monitor.f90:429)."""
         lib().orc_set_adaptive(self.h, int(enable), cfl_target, cfl_safety, dt_min, dt_max)
+
+    def set_landing_time(self, t_land=None):
+        """Shrink the coming steps so that t lands on t_land (landing_dt, src/monitor.f90:436-458); None: no target."""
+        lib().orc_set_landing(self.h, float("nan") if t_land is None else float(t_land))
 
     def compute_cfl(self):
         a, b = c_double(0.0), c_double(0.0)

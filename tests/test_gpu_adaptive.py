@@ -98,3 +98,35 @@ def test_adaptive_dt_rejects_bad_parameters(args):
     with pytest.raises(DfdmError):
         s.set_adaptive_dt(True, *args)
     s.close()
+
+
+@pytest.mark.parametrize("adaptive", [False, True])
+def test_landing_matches_the_oracle(oracle_mod, adaptive):
+    """Output landing (landing_dt) with the fixed and with the adaptive dt: the same times and states as the oracle;
+    a new target between steps keeps the captured graph (graphs on)."""
+    c = cases.get("chan_les_amd_small")
+    U, V, W, P = cases.initial_condition(c)
+    o = oracle_mod.Oracle(c)
+    o.set_state(U, V, W, P)
+    s = Solver(c, "fp64")
+    s.set_state(U, V, W, P)
+    s.enable_graphs(True)
+    if adaptive:
+        o.set_adaptive_dt(True, 0.6, 0.9)
+        s.set_adaptive_dt(True, 0.6, 0.9)
+    target = 3.7 * c.dt
+    o.set_landing_time(target)
+    s.set_landing_time(target)
+    for n in range(8):
+        if n == 5:
+            target = o.t + 2.5 * c.dt
+            o.set_landing_time(target)
+            s.set_landing_time(target)
+        o.step(1)
+        t = s.compute_time_step_RK3(1)
+        assert abs(t - o.t) <= 1e-13 * o.t, (n, t, o.t)
+        assert abs(s.dt - o.dt) <= 1e-13 * o.dt, (n, s.dt, o.dt)
+    assert abs(o.t - target) <= 1e-12 * target or o.t > target
+    for key, a, b in zip("UVWP", s.get_state(), o.get_state()):
+        assert rel_l2(a, b) <= 1e-12, (key, rel_l2(a, b))
+    s.close()

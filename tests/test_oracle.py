@@ -204,3 +204,22 @@ def test_adaptive_dt_follows_select_dt(oracle_mod, name, target, dt_max):
         dt = want
     if dt_max < 1.0:
         assert o.dt == dt_max
+
+
+def test_landing_dt_lands_on_the_target(oracle_mod):
+    """landing_dt (src/monitor.f90:450-458): a remainder below 2 dt is one step, one between dt and 2 dt is two
+    equal halves; dt is restored after the shrunk step (src/time_integration.f90:711)."""
+    c = cases.get("chan_small")
+    o = _with_ic(oracle_mod, c)
+    dt = c.dt
+    target = 3.7 * dt
+    o.set_landing_time(target)
+    ts = []
+    for _ in range(5):
+        o.step(1)
+        ts.append(o.t)
+        assert o.dt == dt
+    # steps: dt, dt, then 1.7 dt is split in two halves 0.85 dt, then the target is reached and the rest are dt
+    want = [dt, 2 * dt, 2 * dt + 0.85 * dt, target, target + dt]
+    for got, w in zip(ts, want):
+        assert abs(got - w) <= 1e-12 * target, (ts, want)
