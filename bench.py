@@ -314,7 +314,9 @@ def main():
         if rank == 0:
             print(json.dumps(out), flush=True)
         return
-    fams = ["stage", "fwd_x", "fwd_z", "y_solve", "inv_z", "inv_x", "correct"]
+    fams = ["stage", "fwd_x", "fwd_z", "y_solve", "inv_z", "inv_x", "correct", "cfl"]
+    if c.flow_forcing_mode == 1:
+        fams.append("flux_shift")
     iters = 20
     kt = {}
     for fam in fams:

@@ -97,6 +97,7 @@ struct dfdm_ctx {
     WallState wsd{};
     double *red_part = nullptr, *red_out = nullptr;
     int red_blocks = 0;
+    int cfl_blocks = 1;
     unsigned long long *d_maxdiv = nullptr;
     unsigned long long *d_cfl = nullptr;        // convective and viscous CFL maxima (bit patterns)
     // device time step: with the adaptive time step (cfl_adaptive = 1) or an output-landing target, dt and t live on
@@ -395,6 +396,9 @@ template <typename T> struct Impl {
         }
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tiled<T, false, false, TILE_X, TILE_Y, 1>, TILE_X * TILE_Y, 0));
         c->kc_sgs = choose_kc(d, occ, nsm);
+        // the CFL maxima: one wave of resident blocks, at most one warp per x-row
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cfl<T, true>, 256, 0));
+        c->cfl_blocks = (int)std::max(1LL, std::min((long long)std::max(1, occ) * nsm, ((long long)d.Ny * d.Nz + 7) / 8));
         return setup_fft2l(c);
     }
 
@@ -595,7 +599,7 @@ template <typename T> struct Impl {
         }
         case 9: {   // constant-flux shift
             if (c->prm.flow_forcing_mode != 1) return DFDM_OK;
-            k_bulk_partial<T><<<c->red_blocks, 256, 0, st>>>(d, f(c->u), c->d_dyc, c->d_dzc, c->d_ubd, c->red_part);
+            bulk_partial(c);
             CKL();
             k_bulk_final<<<1, 256, 0, st>>>(c->red_blocks, c->red_part, c->prm.Ub_target, c->red_out);
             CKL();
@@ -603,6 +607,8 @@ template <typename T> struct Impl {
             CKL();
             return DFDM_OK;
         }
+        case 10:   // CFL maxima (the step-start part of the adaptive time step)
+            return cfl_maxima(c);
         }
         return fail(DFDM_ERR_INVALID, "unknown kernel family");
     }
@@ -614,11 +620,17 @@ template <typename T> struct Impl {
         return DFDM_OK;
     }
 
-    // compute_time_step_RK3, single-phase flag set (src/time_integration.f90:120-713)
+    // rows of 16-byte chunks (Nx * sizeof(T) a multiple of 16): the row reductions load whole chunks
+    static bool row_chunks(const dfdm_ctx *c) { return c->d.Nx % (16 / (int)sizeof(T)) == 0; }
+    static void bulk_partial(dfdm_ctx *c) {
+        auto fn = row_chunks(c) ? k_bulk_partial<T, true> : k_bulk_partial<T, false>;
+        fn<<<c->red_blocks, 256, 0, c->stream>>>(c->d, f(c->u), c->d_dyc, c->d_dzc, c->d_ubd, c->red_part);
+    }
     // the CFL maxima of the resident state into d_cfl (zeroed first)
     static int cfl_maxima(dfdm_ctx *c) {
         CK(cudaMemsetAsync(c->d_cfl, 0, 2 * sizeof(unsigned long long), c->stream));
-        k_cfl<T><<<c->red_blocks, 256, 0, c->stream>>>(c->d, f(c->u), f(c->v), f(c->w), c->les ? f(c->nut) : nullptr,
+        auto fn = row_chunks(c) ? k_cfl<T, true> : k_cfl<T, false>;
+        fn<<<c->cfl_blocks, 256, 0, c->stream>>>(c->d, f(c->u), f(c->v), f(c->w), c->les ? f(c->nut) : nullptr,
                                                         c->d_ubd, 1.0 / c->dx, c->d_dyc, c->d_dzc, c->prm.nu, c->d_cfl);
         CKL();
         return DFDM_OK;
@@ -632,6 +644,7 @@ template <typename T> struct Impl {
         return DFDM_OK;
     }
 
+    // compute_time_step_RK3, single-phase flag set (src/time_integration.f90:120-713)
     static int step_enqueue(dfdm_ctx *c) {
         int rc;
         for (int s = 1; s <= 3; ++s) {
@@ -1614,8 +1627,7 @@ int dfdm_compute_bulk_velocity(dfdm_ctx *c, double *Ub) {
     if (!Ub) return fail(DFDM_ERR_INVALID, "null output");
     int rc = dispatch(c, [&](auto impl) {
         typedef decltype(impl) I;
-        typedef typename std::remove_pointer<decltype(I::f(nullptr))>::type T;
-        k_bulk_partial<T><<<c->red_blocks, 256, 0, c->stream>>>(c->d, I::f(c->u), c->d_dyc, c->d_dzc, c->d_ubd, c->red_part);
+        I::bulk_partial(c);
         CKL();
         k_bulk_final<<<1, 256, 0, c->stream>>>(c->red_blocks, c->red_part, 0.0, c->red_out);
         CKL();
@@ -1715,7 +1727,7 @@ int dfdm_pad_field(dfdm_ctx *c, int field, int extra_planes, double *out) {
 int dfdm_launch_kernel_async(dfdm_ctx *c, int which, int rk_stage) {
     g_err.clear();
     if (int rc = check_ctx(c)) return rc;
-    if (which < 0 || which > 9 || rk_stage < 1 || rk_stage > 3) return fail(DFDM_ERR_INVALID, "bad kernel id or stage");
+    if (which < 0 || which > 10 || rk_stage < 1 || rk_stage > 3) return fail(DFDM_ERR_INVALID, "bad kernel id or stage");
     long long before = g_launches;
     int rc = dispatch(c, [&](auto impl) { return decltype(impl)::launch(c, which, rk_stage); });
     c->launches += g_launches - before;
@@ -1762,6 +1774,8 @@ int dfdm_kernel_bytes(dfdm_ctx *c, int which, double *bytes) {
     case 3: case 4: case 5: b = 2.0 * spec; break;                // read + write spectrum
     case 6: b = spec + cell; break;                               // read spectrum, write phi
     case 7: b = 7.0 * cell; break;                                // read phi, u*; write u (+P at stage 3)
+    case 9: b = c->prm.flow_forcing_mode == 1 ? 3.0 * cell : 0.0; break;   // bulk sum reads U; the shift reads + writes U
+    case 10: b = 3.0 * cell + (c->les ? cell : 0.0); break;       // read U, V, W (+ nu_t)
     default: return fail(DFDM_ERR_INVALID, "bad kernel id");
     }
     *bytes = b;

@@ -39,25 +39,90 @@ __device__ __forceinline__ void block_sum2(double a, double b, double *out) {
     }
 }
 
-// compute_bulk_velocity (src/monitor.f90:463-523): sum of 0.5 (U_i + U_{i-1}) dy_j dz_k over the independent
-// cells and of the weights dy_j dz_k, one partial pair per block (deterministic, no atomics).  A block walks whole
-// x-rows (row = k*Ny + j, uniform over the block), so no per-cell index division is needed.
-template <typename T>
+// Block maximum of two non-negative doubles, then one atomicMax of each bit pattern per block (non-negative
+// doubles order as their bit patterns); one atomic pair per block keeps the two addresses uncontended.
+__device__ __forceinline__ void block_max2_atomic(double a, double b, unsigned long long *out) {
+    __shared__ double sa[32], sb[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        a = fmax(a, __shfl_down_sync(0xffffffffu, a, o));
+        b = fmax(b, __shfl_down_sync(0xffffffffu, b, o));
+    }
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { sa[wid] = a; sb[wid] = b; }
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        a = lane < nw ? sa[lane] : 0.0;
+        b = lane < nw ? sb[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            a = fmax(a, __shfl_down_sync(0xffffffffu, a, o));
+            b = fmax(b, __shfl_down_sync(0xffffffffu, b, o));
+        }
+        if (lane == 0) {
+            atomicMax(out, (unsigned long long)__double_as_longlong(a));
+            atomicMax(out + 1, (unsigned long long)__double_as_longlong(b));
+        }
+    }
+}
+
+// 16-byte row chunks: NV = 16 / sizeof(T) consecutive cells in one load (rows start 16-byte aligned when Nx*sizeof(T)
+// is a multiple of 16: the fields are 256-byte aligned)
+template <typename T> struct Chunk {
+    static constexpr int NV = 16 / sizeof(T);
+    T x[NV];
+    __device__ __forceinline__ void load(const T *p) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(p));
+        if constexpr (sizeof(T) == 4) {
+            x[0] = __uint_as_float(v.x); x[1] = __uint_as_float(v.y); x[2] = __uint_as_float(v.z); x[3] = __uint_as_float(v.w);
+        } else {
+            x[0] = __hiloint2double((int)v.y, (int)v.x); x[1] = __hiloint2double((int)v.w, (int)v.z);
+        }
+    }
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int c = 0; c < NV; ++c) x[c] = T(0);
+    }
+};
+
+// compute_bulk_velocity (src/monitor.f90:463-523): sum of 0.5 (U_i + U_{i-1}) dy_j dz_k over the independent cells
+// and of the weights dy_j dz_k, one partial pair per block (deterministic, no atomics).  Over a periodic x-row the
+// face averages telescope, sum_i 0.5 (U_i + U_{i-1}) = sum_i U_i, so a row contributes dy_j dz_k (sum_i u_i + Nx ub_j)
+// (u the stored field, ub the base profile).  A warp walks whole x-rows (row = k*Ny + j): the row's metrics are
+// loaded once, with no per-cell index division, and a lane reads its cells in 16-byte chunks (VEC: Nx a multiple of
+// the chunk; otherwise one cell at a time).
+template <typename T, bool VEC>
 __global__ void __launch_bounds__(256) k_bulk_partial(Dims d, const T *__restrict__ U, const double *__restrict__ dyc,
                                                       const double *__restrict__ dzc, const double *__restrict__ ubd,
                                                       double *__restrict__ part) {
+    typedef Chunk<T> Ch;
     Kahan s, w; s.init(); w.init();
-    const int rows = d.Ny * d.Nz, Nx = d.Nx;
-#pragma unroll 4
-    for (int row = blockIdx.x; row < rows; row += gridDim.x) {   // unrolled: four rows' loads in flight at once
+    const int rows = d.Ny * d.Nz, Nx = d.Nx, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < rows; row += gridDim.x * wpb) {
         const int k = row / d.Ny, j = row - k * d.Ny;
         const double a = dyc[j] * dzc[k], ub = ubd[j];
         const T *Ur = U + (size_t)row * Nx;
-        for (int i = threadIdx.x; i < Nx; i += blockDim.x) {
-            const double u0 = (double)Ur[i] + ub, um = (double)Ur[i == 0 ? Nx - 1 : i - 1] + ub;
-            s.add(0.5 * (u0 + um) * a);
-            w.add(a);
+        double t = 0.0;
+        int n = 0;
+        if constexpr (VEC) {
+            const int nq = Nx / Ch::NV;
+            constexpr int CH = 2;   // chunks per lane loaded before any is summed
+            for (int q0 = lane; q0 < nq; q0 += 32 * CH) {
+                Ch u[CH];
+#pragma unroll
+                for (int m = 0; m < CH; ++m)
+                    if (q0 + 32 * m < nq) u[m].load(Ur + (size_t)(q0 + 32 * m) * Ch::NV); else u[m].zero();
+#pragma unroll
+                for (int m = 0; m < CH; ++m) {
+#pragma unroll
+                    for (int c = 0; c < Ch::NV; ++c) t += (double)u[m].x[c];
+                    if (q0 + 32 * m < nq) n += Ch::NV;
+                }
+            }
+        } else {
+            for (int i = lane; i < Nx; i += 32) { t += (double)Ur[i]; ++n; }
         }
+        s.add((t + n * ub) * a);
+        w.add(n * a);
     }
     block_sum2(s.s, w.s, part);
 }
@@ -123,45 +188,78 @@ __global__ void __launch_bounds__(256) k_maxdiv(Dims d, const T *__restrict__ U,
 
 // compute_cfl (src/monitor.f90:304-424) without its IBM, buoyancy, rotation and actuator terms: the maxima over the
 // centres of |u_c|/dx + |v_c|/dy_j + |w_c|/dz_k (face velocities averaged to the centre) and of
-// (nu + nu_t) 2 (1/dx^2 + 1/dy_j^2 + 1/dz_k^2), in double, as exact integer maxima of their bit patterns.
-template <typename T>
+// (nu + nu_t) 2 (1/dx^2 + 1/dy_j^2 + 1/dz_k^2), as exact integer maxima of their bit patterns.  The convective term
+// is computed in the storage type (double in the FP64 form, float in the FP32-mixed form, whose velocities carry
+// float rounding already) as |u_i + u_{i-1} + 2 ub| (dx^-1/2) + ..., the halving moved onto the metric (exact); the
+// viscous term is in double from the row maximum of nu_t (exact: the term grows monotonically with nu_t).  A warp
+// walks whole x-rows (row = k*Ny + j) with no per-cell index division; a lane reads 16-byte chunks of cells and takes
+// U_{i-1} of its first cell from the lane before (the warp's last lane carries it to the next batch); without VEC
+// (Nx not a multiple of the chunk) one cell at a time.
+template <typename T, bool VEC>
 __global__ void __launch_bounds__(256) k_cfl(Dims d, const T *__restrict__ U, const T *__restrict__ V,
                                              const T *__restrict__ W, const T *__restrict__ NU,
                                              const double *__restrict__ ubd, double inv_dx, const double *__restrict__ dyc,
                                              const double *__restrict__ dzc, double nu, unsigned long long *__restrict__ out) {
-    // whole x-rows (row = k*Ny + j) per block, as k_bulk_partial: no per-cell index division
-    double mc = 0.0, mv = 0.0;
+    typedef Chunk<T> Ch;
+    constexpr int NV = Ch::NV;
+    double mv = 0.0;
+    T mc = T(0);
     const double idx2 = inv_dx * inv_dx;
-    const int rows = d.Ny * d.Nz, Nx = d.Nx;
-#pragma unroll 2
-    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+    const T hx = (T)(0.5 * inv_dx);
+    const int rows = d.Ny * d.Nz, Nx = d.Nx, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < rows; row += gridDim.x * wpb) {
         const int k = row / d.Ny, j = row - k * d.Ny;
-        const double ub = ubd[j];
         const double idy = 1.0 / fmax(dyc[j], 1e-14), idz = 1.0 / fmax(dzc[k], 1e-14);
-        const double lap = idx2 + idy * idy + idz * idz;
+        const T ub2 = (T)(2.0 * ubd[j]), hy = (T)(0.5 * idy), hz = (T)(0.5 * idz);
         const T *Ur = U + (size_t)row * Nx, *Vr = V + (size_t)row * Nx, *Wr = W + (size_t)row * Nx;
         // V at j-1 (periodic wrap, or the zero wall value below the first row) and W at k-1 (periodic)
         const int jm = j - 1 < 0 ? (d.yper ? d.Ny - 1 : -1) : j - 1;
         const T *Vm = jm < 0 ? nullptr : V + ((size_t)k * d.Ny + jm) * Nx;
         const T *Wm = W + ((size_t)(k == 0 ? d.Nz - 1 : k - 1) * d.Ny + j) * Nx;
         const T *Nr = NU ? NU + (size_t)row * Nx : nullptr;
-        for (int i = threadIdx.x; i < Nx; i += blockDim.x) {
-            const double uc = 0.5 * (((double)Ur[i] + ub) + ((double)Ur[i == 0 ? Nx - 1 : i - 1] + ub));
-            const double vc = 0.5 * ((double)Vr[i] + (Vm ? (double)Vm[i] : 0.0));
-            const double wc = 0.5 * ((double)Wr[i] + (double)Wm[i]);
-            mc = fmax(mc, fabs(uc) * inv_dx + fabs(vc) * idy + fabs(wc) * idz);
-            const double nt = Nr ? (double)Nr[i] : 0.0;
-            mv = fmax(mv, (nu + nt) * 2.0 * lap);
+        T nmax = T(0);
+        auto cell = [&](T u0, T um, T v0, T vm, T w0, T wm, T nt) {
+            mc = max(mc, fabs(u0 + um + ub2) * hx + fabs(v0 + vm) * hy + fabs(w0 + wm) * hz);
+            nmax = max(nmax, nt);
+        };
+        if constexpr (VEC) {
+            const int nq = Nx / NV;
+            constexpr int CH = 2;                        // chunks per lane loaded before any is used
+            T carry = Ur[Nx - 1];                        // U_{i-1} of the row's first cell (periodic)
+            for (int q0 = 0; q0 < nq; q0 += 32 * CH) {   // warp-uniform: every lane takes part in the shuffles
+                Ch u[CH], v[CH], vm[CH], w[CH], wm[CH], n[CH];
+#pragma unroll
+                for (int m = 0; m < CH; ++m) {
+                    const int q = q0 + lane + 32 * m;
+                    if (q < nq) {
+                        const size_t o = (size_t)q * NV;
+                        u[m].load(Ur + o); v[m].load(Vr + o); w[m].load(Wr + o); wm[m].load(Wm + o);
+                        if (Vm) vm[m].load(Vm + o); else vm[m].zero();
+                        if (Nr) n[m].load(Nr + o); else n[m].zero();
+                    } else {
+                        u[m].zero(); v[m].zero(); vm[m].zero(); w[m].zero(); wm[m].zero(); n[m].zero();
+                    }
+                }
+#pragma unroll
+                for (int m = 0; m < CH; ++m) {
+                    const T up = __shfl_up_sync(0xffffffffu, u[m].x[NV - 1], 1);
+                    const T um0 = lane == 0 ? carry : up;
+                    carry = __shfl_sync(0xffffffffu, u[m].x[NV - 1], 31);
+                    if (q0 + lane + 32 * m < nq) {
+                        cell(u[m].x[0], um0, v[m].x[0], vm[m].x[0], w[m].x[0], wm[m].x[0], n[m].x[0]);
+#pragma unroll
+                        for (int c = 1; c < NV; ++c)
+                            cell(u[m].x[c], u[m].x[c - 1], v[m].x[c], vm[m].x[c], w[m].x[c], wm[m].x[c], n[m].x[c]);
+                    }
+                }
+            }
+        } else {
+            for (int i = lane; i < Nx; i += 32)
+                cell(Ur[i], Ur[i == 0 ? Nx - 1 : i - 1], Vr[i], Vm ? Vm[i] : T(0), Wr[i], Wm[i], Nr ? Nr[i] : T(0));
         }
+        mv = fmax(mv, (nu + (double)nmax) * 2.0 * (idx2 + idy * idy + idz * idz));
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        mc = fmax(mc, __shfl_down_sync(0xffffffffu, mc, o));
-        mv = fmax(mv, __shfl_down_sync(0xffffffffu, mv, o));
-    }
-    if ((threadIdx.x & 31) == 0) {
-        atomicMax(out, (unsigned long long)__double_as_longlong(mc));
-        atomicMax(out + 1, (unsigned long long)__double_as_longlong(mv));
-    }
+    block_max2_atomic((double)mc, mv, out);
 }
 
 // select_dt (src/monitor.f90:429-458) at a step start.  dtt = {dt of the coming step, t, landing target, dt}:
