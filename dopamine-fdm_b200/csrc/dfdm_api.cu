@@ -98,7 +98,9 @@ struct dfdm_ctx {
     double *red_part = nullptr, *red_out = nullptr;
     int red_blocks = 0;
     int cfl_blocks = 1;
-    unsigned long long *d_maxdiv = nullptr;
+    // monitor block: [0],[1] CFL maxima, [2] max |div u|, [3] max |U| (bit patterns), [4] guard flag (int),
+    // [5],[6] wall u_tau sums (double), [8..17] the dfdm_monitor values
+    unsigned long long *d_mon = nullptr;
     unsigned long long *d_cfl = nullptr;        // convective and viscous CFL maxima (bit patterns)
     // device time step: with the adaptive time step (cfl_adaptive = 1) or an output-landing target, dt and t live on
     // the device in d_dtt = {dt of the step, t, landing target, dt before landing}, set by k_select_dt at every step
@@ -108,7 +110,6 @@ struct dfdm_ctx {
     double cfl_target = 0.5, cfl_safety = 0.9, dt_min = 1e-10, dt_max = 1e10;
     double t_land = std::numeric_limits<double>::quiet_NaN();
     bool dev_dt() const { return adaptive || landing; }
-    int *d_flag = nullptr;
     double *staging = nullptr;
     size_t staging_n = 0;
     // launch geometry
@@ -635,6 +636,38 @@ template <typename T> struct Impl {
         CKL();
         return DFDM_OK;
     }
+    // max |div u|, max |U| and the finite guard into d_mon[2], [3], [4] (zeroed first)
+    static int monitor_rows(dfdm_ctx *c) {
+        CK(cudaMemsetAsync(c->d_mon + 2, 0, 3 * sizeof(unsigned long long), c->stream));
+        k_monitor_rows<T><<<c->cfl_blocks, 256, 0, c->stream>>>(c->d, f(c->u), f(c->v), f(c->w), c->d_ubd, c->d_dxc,
+                                                                 c->d_dyc, c->d_dzc, c->d_mon + 2, (int *)(c->d_mon + 4));
+        CKL();
+        return DFDM_OK;
+    }
+    // output_monitor: every value into d_mon[8..17] (the dfdm_monitor layout), no host synchronisation
+    static int monitor(dfdm_ctx *c) {
+        CK(cudaMemsetAsync(c->d_mon, 0, 2 * sizeof(unsigned long long), c->stream));
+        auto fn = row_chunks(c) ? k_cfl<T, true> : k_cfl<T, false>;
+        fn<<<c->cfl_blocks, 256, 0, c->stream>>>(c->d, f(c->u), f(c->v), f(c->w), c->les ? f(c->nut) : nullptr,
+                                                 c->d_ubd, 1.0 / c->dx, c->d_dyc, c->d_dzc, c->prm.nu, c->d_mon);
+        CKL();
+        if (int rc = monitor_rows(c)) return rc;
+        bulk_partial(c);
+        CKL();
+        k_bulk_final<<<1, 256, 0, c->stream>>>(c->red_blocks, c->red_part, 0.0, c->red_out);
+        CKL();
+        const int ncol = c->d.Nx * c->d.Nz;
+        double *wsum = c->wm ? (double *)(c->d_mon + 5) : nullptr;
+        if (wsum) {
+            k_wall_diag<<<1, 256, 0, c->stream>>>(ncol, c->wsd.tx, wsum);
+            CKL();
+        }
+        k_monitor_final<<<1, 32, 0, c->stream>>>(c->d_mon, (const int *)(c->d_mon + 4), c->red_out, wsum, ncol,
+                                                 c->dev_dt() ? c->d_dtt : nullptr, c->t, c->prm.dt,
+                                                 (double *)(c->d_mon + 8));
+        CKL();
+        return DFDM_OK;
+    }
     static int select_dt(dfdm_ctx *c) {
         if (c->adaptive)
             if (int rc = cfl_maxima(c)) return rc;
@@ -982,14 +1015,12 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
     c->red_part = (double *)tmp;
     if ((rc = dalloc(c, &tmp, 4 * sizeof(double)))) return bail(rc);
     c->red_out = (double *)tmp;
-    if ((rc = dalloc(c, &tmp, sizeof(unsigned long long)))) return bail(rc);
-    c->d_maxdiv = (unsigned long long *)tmp;
+    if ((rc = dalloc(c, &tmp, 32 * sizeof(unsigned long long)))) return bail(rc);
+    c->d_mon = (unsigned long long *)tmp;
     if ((rc = dalloc(c, &tmp, 2 * sizeof(unsigned long long)))) return bail(rc);
     c->d_cfl = (unsigned long long *)tmp;
     if ((rc = dalloc(c, &tmp, 4 * sizeof(double)))) return bail(rc);
     c->d_dtt = (double *)tmp;
-    if ((rc = dalloc(c, &tmp, sizeof(int)))) return bail(rc);
-    c->d_flag = (int *)tmp;
     c->in_create = false;   // later buffers (host staging, the unit RHS output) are separate allocations
 
     rc = dispatch(c, [&](auto impl) { return decltype(impl)::setup_kernels(c); });
@@ -1643,20 +1674,35 @@ int dfdm_check_divergence(dfdm_ctx *c, double *max_div) {
     g_err.clear();
     if (int rc = check_ctx(c)) return rc;
     if (!max_div) return fail(DFDM_ERR_INVALID, "null output");
-    CK(cudaMemsetAsync(c->d_maxdiv, 0, sizeof(unsigned long long), c->stream));
-    int rc = dispatch(c, [&](auto impl) {
-        typedef decltype(impl) I;
-        typedef typename std::remove_pointer<decltype(I::f(nullptr))>::type T;
-        k_maxdiv<T><<<c->red_blocks, 256, 0, c->stream>>>(c->d, I::f(c->u), I::f(c->v), I::f(c->w), c->d_dxc, c->d_dyc,
-                                                          c->d_dzc, c->d_maxdiv);
-        CKL();
-        return DFDM_OK;
-    });
+    int rc = dispatch(c, [&](auto impl) { return decltype(impl)::monitor_rows(c); });
     if (rc) return rc;
     unsigned long long bits = 0;
-    CK(cudaMemcpyAsync(&bits, c->d_maxdiv, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&bits, c->d_mon + 2, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     std::memcpy(max_div, &bits, sizeof(double));
+    return DFDM_OK;
+}
+
+int dfdm_output_monitor_async(dfdm_ctx *c, dfdm_monitor *out) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (!out) return fail(DFDM_ERR_INVALID, "null output");
+    static_assert(sizeof(dfdm_monitor) == 10 * sizeof(double), "dfdm_monitor is ten doubles");
+    long long before = g_launches;
+    int rc = dispatch(c, [&](auto impl) { return decltype(impl)::monitor(c); });
+    c->launches += g_launches - before;
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(out, c->d_mon + 8, sizeof(dfdm_monitor), cudaMemcpyDefault, c->stream));
+    return DFDM_OK;
+}
+
+int dfdm_output_monitor(dfdm_ctx *c, dfdm_monitor *out) {
+    if (!out) return fail(DFDM_ERR_INVALID, "null output");
+    dfdm_monitor m;
+    if (int rc = dfdm_output_monitor_async(c, &m)) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    *out = m;
+    if (m.nan_flag != 0.0) return fail(DFDM_ERR_NOT_FINITE, "NaN, Inf or |u| > 1e8 in the velocity field");
     return DFDM_OK;
 }
 
@@ -1700,17 +1746,10 @@ int dfdm_kinetic_energy(dfdm_ctx *c, double *ke) {
 int dfdm_check_finite(dfdm_ctx *c) {
     g_err.clear();
     if (int rc = check_ctx(c)) return rc;
-    CK(cudaMemsetAsync(c->d_flag, 0, sizeof(int), c->stream));
-    int rc = dispatch(c, [&](auto impl) {
-        typedef decltype(impl) I;
-        typedef typename std::remove_pointer<decltype(I::f(nullptr))>::type T;
-        k_finite<T><<<c->red_blocks, 256, 0, c->stream>>>(c->d.cells, I::f(c->u), I::f(c->v), I::f(c->w), c->d_flag);
-        CKL();
-        return DFDM_OK;
-    });
+    int rc = dispatch(c, [&](auto impl) { return decltype(impl)::monitor_rows(c); });
     if (rc) return rc;
     int flag = 0;
-    CK(cudaMemcpyAsync(&flag, c->d_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&flag, c->d_mon + 4, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     if (flag) return fail(DFDM_ERR_NOT_FINITE, "NaN, Inf or |U| > 1e8 in the velocity field");
     return DFDM_OK;

@@ -164,26 +164,83 @@ __global__ void __launch_bounds__(256) k_shift(Dims d, T *__restrict__ U, const 
     for (long long p = first; p < d.cells; p += stride) U[p] = U[p] + s;
 }
 
-// check_divergence (src/projection.f90:607-639): max |div u| over the independent centres, in double.
-// The maximum of non-negative doubles is taken with an integer atomicMax on their bit patterns (exact).
+// check_divergence (src/projection.f90:607-639), max |U| over the U faces and the NaN / |u| > 1e8 guard of
+// output_monitor (src/monitor.f90:32-58) in one pass: out[0] = max |div u|, out[1] = max |U| (bit patterns, atomicMax
+// per block), flag |= 1 when the guard trips.  div u = (U_i - U_{i-1})/dx_i + (V_j - V_{j-1})/dy_j +
+// (W_k - W_{k-1})/dz_k in double, divided as the reference divides; U is the stored field plus the base profile.
+// A warp walks whole x-rows (row = k*Ny + j), four cells per lane loaded before any is used.
 template <typename T>
-__global__ void __launch_bounds__(256) k_maxdiv(Dims d, const T *__restrict__ U, const T *__restrict__ V,
-                                                const T *__restrict__ W, const double *__restrict__ dxc,
-                                                const double *__restrict__ dyc, const double *__restrict__ dzc,
-                                                unsigned long long *__restrict__ out) {
-    double m = 0.0;
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x) {
-        int i = (int)(p % d.Nx);
-        long long q = p / d.Nx;
-        int j = (int)(q % d.Ny), k = (int)(q / d.Ny);
-        double du = (double)U[p] - (double)U[idx3(d, wrap(i - 1, d.Nx), j, k)];
-        double dv = (double)ld_yf(V, d, i, j, k) - (double)ld_yf(V, d, i, j - 1, k);
-        double dw = (double)W[p] - (double)W[idx3(d, i, j, wrap(k - 1, d.Nz))];
-        double dv_ = fabs(du / dxc[i] + dv / dyc[j] + dw / dzc[k]);
-        m = fmax(m, dv_);
+__global__ void __launch_bounds__(256) k_monitor_rows(Dims d, const T *__restrict__ U, const T *__restrict__ V,
+                                                      const T *__restrict__ W, const double *__restrict__ ubd,
+                                                      const double *__restrict__ dxc, const double *__restrict__ dyc,
+                                                      const double *__restrict__ dzc, unsigned long long *__restrict__ out,
+                                                      int *__restrict__ flag) {
+    double mdiv = 0.0, mu = 0.0;
+    int bad = 0;
+    const int rows = d.Ny * d.Nz, Nx = d.Nx, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < rows; row += gridDim.x * wpb) {
+        const int k = row / d.Ny, j = row - k * d.Ny;
+        const double ub = ubd[j], dy = dyc[j], dz = dzc[k];
+        const T *Ur = U + (size_t)row * Nx, *Vr = V + (size_t)row * Nx, *Wr = W + (size_t)row * Nx;
+        const int jm = j - 1 < 0 ? (d.yper ? d.Ny - 1 : -1) : j - 1;
+        const T *Vm = jm < 0 ? nullptr : V + ((size_t)k * d.Ny + jm) * Nx;
+        const T *Wm = W + ((size_t)(k == 0 ? d.Nz - 1 : k - 1) * d.Ny + j) * Nx;
+        constexpr int CH = 4;
+        for (int i0 = lane; i0 < Nx; i0 += 32 * CH) {
+            T u0[CH], um[CH], v0[CH], vm[CH], w0[CH], wm[CH];
+#pragma unroll
+            for (int m = 0; m < CH; ++m) {
+                const int i = i0 + 32 * m;
+                if (i < Nx) {
+                    u0[m] = Ur[i]; um[m] = Ur[i == 0 ? Nx - 1 : i - 1];
+                    v0[m] = Vr[i]; vm[m] = Vm ? Vm[i] : T(0);
+                    w0[m] = Wr[i]; wm[m] = Wm[i];
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < CH; ++m) {
+                const int i = i0 + 32 * m;
+                if (i < Nx) {
+                    const double du = (double)u0[m] - (double)um[m], dv = (double)v0[m] - (double)vm[m];
+                    const double dw = (double)w0[m] - (double)wm[m];
+                    mdiv = fmax(mdiv, fabs(du / dxc[i] + dv / dy + dw / dz));
+                    const double ut = (double)u0[m] + ub;
+                    mu = fmax(mu, fabs(ut));
+                    if (!(fabs(ut) <= 1e8) || !(fabs((double)v0[m]) <= 1e8) || !(fabs((double)w0[m]) <= 1e8)) bad = 1;
+                }
+            }
+        }
     }
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+    block_max2_atomic(mdiv, mu, out);
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
+// wall_diag_sums (src/wallmodel.f90:700-723): the sums over the wall-parallel columns of the wall model's u_tau
+// (the filter state tx, both walls) into out[0], out[1]; one block, compensated per-thread sums then a fixed tree.
+__global__ void __launch_bounds__(256) k_wall_diag(int ncol, const double *__restrict__ tx, double *__restrict__ out) {
+    Kahan s, w; s.init(); w.init();
+    for (int p = threadIdx.x; p < ncol; p += blockDim.x) { s.add(tx[p]); w.add(tx[ncol + p]); }
+    block_sum2(s.s, w.s, out);   // gridDim.x == 1
+}
+
+// The monitor values (the layout of dfdm_monitor): t, dt, mean U, max |U|, max |div u|, CFL conv, CFL visc, mean
+// u_tau of the lower and upper wall, NaN flag.  dtt = {dt of the step, t, landing target, dt} when the time step
+// lives on the device, else null and the host's t and dt are used.  One thread.
+__global__ void k_monitor_final(const unsigned long long *__restrict__ bits, const int *__restrict__ flag,
+                                const double *__restrict__ bulk, const double *__restrict__ wsum, int ncol,
+                                const double *__restrict__ dtt, double t_host, double dt_host, double *__restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double dt = dtt ? dtt[3] : dt_host, t = dtt ? dtt[1] : t_host;
+    out[0] = t;
+    out[1] = dt;
+    out[2] = bulk[0];
+    out[3] = __longlong_as_double((long long)bits[3]);
+    out[4] = __longlong_as_double((long long)bits[2]);
+    out[5] = __longlong_as_double((long long)bits[0]) * dt;
+    out[6] = __longlong_as_double((long long)bits[1]) * dt;
+    out[7] = wsum ? wsum[0] / (double)ncol : 0.0;
+    out[8] = wsum ? wsum[1] / (double)ncol : 0.0;
+    out[9] = *flag ? 1.0 : 0.0;
 }
 
 // compute_cfl (src/monitor.f90:304-424) without its IBM, buoyancy, rotation and actuator terms: the maxima over the
@@ -313,17 +370,6 @@ __global__ void k_ratio_final(int nparts, const double *__restrict__ part, doubl
     out[0] = s.s / w.s;
 }
 
-// NaN / Inf / |U| > 1e8 guard of output_monitor (src/monitor.f90:32-52).
-template <typename T>
-__global__ void __launch_bounds__(256) k_finite(long long n, const T *__restrict__ a, const T *__restrict__ b,
-                                                const T *__restrict__ c, int *__restrict__ flag) {
-    int bad = 0;
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-        double x = (double)a[p], y = (double)b[p], z = (double)c[p];
-        if (!(fabs(x) <= 1e8) || !(fabs(y) <= 1e8) || !(fabs(z) <= 1e8)) bad = 1;
-    }
-    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
-}
 
 // ---- state transfer ---------------------------------------------------------------------------------------------
 // Field kinds of the ghosted reference arrays.

@@ -32,7 +32,7 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_check_finite", "dfdm_pad_field", "dfdm_launch_kernel_async", "dfdm_kernel_bytes",
            "dfdm_launch_count", "dfdm_solve_poisson_noalloc", "dfdm_write_snapshot", "dfdm_read_snapshot",
            "dfdm_compute_cfl", "dfdm_set_stage_variant", "dfdm_get_stage_variant", "dfdm_set_adaptive_dt",
-           "dfdm_get_dt", "dfdm_set_landing_time"]
+           "dfdm_get_dt", "dfdm_set_landing_time", "dfdm_output_monitor", "dfdm_output_monitor_async"]
 
 
 class DfdmError(RuntimeError):
@@ -98,6 +98,8 @@ def load(build_if_missing: bool = True):
         "dfdm_set_adaptive_dt": (c_int, [c_void_p, c_int, c_double, c_double, c_double, c_double]),
         "dfdm_get_dt": (c_int, [c_void_p, P]),
         "dfdm_set_landing_time": (c_int, [c_void_p, c_int, c_double]),
+        "dfdm_output_monitor": (c_int, [c_void_p, P]),
+        "dfdm_output_monitor_async": (c_int, [c_void_p, c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -297,6 +299,19 @@ class Solver:
         v = c_double(0.0)
         _check(load().dfdm_get_dt(self.h, ctypes.byref(v)))
         return v.value
+
+    MONITOR_KEYS = ("t", "dt", "mean_u", "max_u", "max_div", "cfl_conv", "cfl_visc", "u_tau_lo", "u_tau_hi", "nan_flag")
+
+    def output_monitor(self) -> dict:
+        """The values output_monitor prints (src/monitor.f90:21-102), from one device pass; raises DfdmError
+        (DFDM_ERR_NOT_FINITE) when the NaN / |u| > 1e8 guard trips."""
+        out = (c_double * 10)()
+        _check(load().dfdm_output_monitor(self.h, out))
+        return dict(zip(self.MONITOR_KEYS, list(out)))
+
+    def output_monitor_async(self, out_ptr: int) -> None:
+        """Enqueue the monitor into ten doubles at out_ptr (pinned host or device memory)."""
+        _check(load().dfdm_output_monitor_async(self.h, ctypes.c_void_p(out_ptr)))
 
     def kinetic_energy(self) -> float:
         v = c_double(0.0)

@@ -192,6 +192,26 @@ int dfdm_set_adaptive_dt(dfdm_ctx *ctx, int enable, double cfl_target, double cf
 int dfdm_set_landing_time(dfdm_ctx *ctx, int enable, double t_land);
 /* The reference's dt between steps: the fixed dt, or the adaptive dt of the last step before any landing shrink. */
 int dfdm_get_dt(dfdm_ctx *ctx, double *dt);
+/* The values output_monitor prints (src/monitor.f90:21-102), computed on the device. */
+typedef struct dfdm_monitor {
+    double t;          /* time */
+    double dt;         /* the reference's dt between steps */
+    double mean_u;     /* compute_bulk_velocity (meanU) */
+    double max_u;      /* max |U| over the independent U faces (maxU) */
+    double max_div;    /* check_divergence (max_divergence) */
+    double cfl_conv;   /* compute_cfl of the current state, convective */
+    double cfl_visc;   /* compute_cfl of the current state, viscous */
+    double u_tau_lo;   /* wall_diag_sums (src/wallmodel.f90:700-723): mean u_tau of the lower wall; 0 without the y-wall model */
+    double u_tau_hi;   /* the same for the upper wall */
+    double nan_flag;   /* 1 when the guard of output_monitor trips (a NaN or Inf, or |u| > 1e8), else 0 */
+} dfdm_monitor;
+/* output_monitor: all of dfdm_monitor in one device pass and one copy.  Returns DFDM_ERR_NOT_FINITE, with *out filled,
+ * when the guard trips (where the reference aborts the run).  The CFL numbers are those of the current state (the
+ * reference prints those of the start of the step just taken). */
+int dfdm_output_monitor(dfdm_ctx *ctx, dfdm_monitor *out);
+/* Same, enqueued on the context's stream with no host synchronisation: *out (pinned host or device memory) is
+ * written when the stream reaches it, after the steps enqueued before; check nan_flag there. */
+int dfdm_output_monitor_async(dfdm_ctx *ctx, dfdm_monitor *out);
 /* Kinetic energy 0.5*<u.u> (volume-weighted, compensated sum) -- diagnostic with no reference counterpart. */
 int dfdm_kinetic_energy(dfdm_ctx *ctx, double *ke);
 /* Monitor guard of output_monitor (src/monitor.f90:32-52): DFDM_ERR_NOT_FINITE if any velocity is NaN/Inf or

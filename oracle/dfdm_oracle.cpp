@@ -994,6 +994,35 @@ struct Oracle {
                                                   (W(i, j, k) - W(i, j, k - 1)) / (z[k] - z[k - 1])));
         return div;
     }
+    // output_monitor (src/monitor.f90:21-102) for one rank, without its printing: out = {t, dt, meanU, maxU,
+    // max_divergence, cfl_conv, cfl_visc, mean u_tau lower wall, upper wall (wall_diag_sums, src/wallmodel.f90:700-723;
+    // 0 without the y-wall model), NaN flag}.  The CFL numbers are those of the current state.
+    void output_monitor(double *out) {
+        int bad = 0;
+        auto chk = [&](double v) { if (v != v || std::fabs(v) > 1e8) bad = 1; };
+        double maxU = 0.0;
+        for (int k = 2; k <= nzg - 1; ++k)
+            for (int j = 2; j <= nyg - 1; ++j)
+                for (int i = 2; i <= nx - 1; ++i) { chk(U(i, j, k)); maxU = std::max(maxU, std::fabs(U(i, j, k))); }
+        for (int k = 2; k <= nzg - 1; ++k)
+            for (int j = 2; j <= ny - 1; ++j)
+                for (int i = 2; i <= nxg - 1; ++i) chk(V(i, j, k));
+        for (int k = 2; k <= nz - 1; ++k)
+            for (int j = 2; j <= nyg - 1; ++j)
+                for (int i = 2; i <= nxg - 1; ++i) chk(W(i, j, k));
+        double conv = 0.0, visc = 0.0;
+        compute_cfl(conv, visc);
+        double s1 = 0.0, s2 = 0.0;
+        if (y_bc_type == 1 && prm.flat_wall_model_flag > 0) {
+            for (int k = 2; k <= nzg - 1; ++k)
+                for (int i = 2; i <= nx - 1; ++i) { s1 += wmf_tx(i, 1, k); s2 += wmf_tx(i, 2, k); }
+            const double cols = (double)((nx - 2) * (nzg - 2));
+            s1 /= cols; s2 /= cols;
+        }
+        const double vals[10] = {t, dt(), compute_bulk_velocity(), maxU, check_divergence(), conv, visc, s1, s2,
+                                 (double)bad};
+        for (int q = 0; q < 10; ++q) out[q] = vals[q];
+    }
     // volume-weighted 0.5*<|u|^2> over the independent cells with face velocities averaged to centres
     double kinetic_energy() {
         int ihi = nxg - 2, jhi = (y_bc_type == 0) ? nyg - 2 : nyg - 1, khi = nzg - 2;
@@ -1119,6 +1148,7 @@ void orc_set_adaptive(void *h, int enable, double target, double safety, double 
     o->cfl_target = target; o->cfl_safety = safety; o->dt_min = dtmin; o->dt_max = dtmax;
     if (!enable) o->dt_cur = -1.0;
 }
+void orc_output_monitor(void *h, double *out) { ((Oracle *)h)->output_monitor(out); }
 void orc_set_landing(void *h, double t_land) { ((Oracle *)h)->t_land = t_land; }
 void orc_cfl(void *h, double *conv, double *visc) { ((Oracle *)h)->compute_cfl(*conv, *visc); }
 void orc_compute_sgs(void *h) { ((Oracle *)h)->compute_sgs_model(); }

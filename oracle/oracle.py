@@ -72,6 +72,7 @@ def lib():
         L.orc_set_adaptive.argtypes = [c_void_p, c_int, c_double, c_double, c_double, c_double]
         L.orc_cfl.argtypes = [c_void_p, POINTER(c_double), POINTER(c_double)]
         L.orc_set_landing.argtypes = [c_void_p, c_double]
+        L.orc_output_monitor.argtypes = [c_void_p, POINTER(c_double)]
         L.orc_set_threads.argtypes = [c_int]
         L.orc_get_threads.restype = c_int
         _lib = L
@@ -150,6 +151,14 @@ class Oracle:
     def set_landing_time(self, t_land=None):
         """Shrink the coming steps so that t lands on t_land (landing_dt, src/monitor.f90:436-458); None: no target."""
         lib().orc_set_landing(self.h, float("nan") if t_land is None else float(t_land))
+
+    MONITOR_KEYS = ("t", "dt", "mean_u", "max_u", "max_div", "cfl_conv", "cfl_visc", "u_tau_lo", "u_tau_hi", "nan_flag")
+
+    def output_monitor(self) -> dict:
+        """The values output_monitor prints (src/monitor.f90:21-102), CFL numbers of the current state."""
+        out = np.zeros(10)
+        lib().orc_output_monitor(self.h, dptr(out))
+        return dict(zip(self.MONITOR_KEYS, out.tolist()))
 
     def compute_cfl(self):
         a, b = c_double(0.0), c_double(0.0)

@@ -223,3 +223,18 @@ def test_landing_dt_lands_on_the_target(oracle_mod):
     want = [dt, 2 * dt, 2 * dt + 0.85 * dt, target, target + dt]
     for got, w in zip(ts, want):
         assert abs(got - w) <= 1e-12 * target, (ts, want)
+
+
+def test_output_monitor_restatement(oracle_mod):
+    """The oracle's output_monitor values against numpy on its own state."""
+    c = cases.get("chan_les_amd_small")
+    o = _with_ic(oracle_mod, c)
+    o.step(2)
+    m = o.output_monitor()
+    U, V, W, P = o.get_state()
+    nx, nyg, nzg = c.nx, c.nyg, c.nzg
+    assert m["max_u"] == np.abs(U[1:nx - 1, 1:nyg - 1, 1:nzg - 1]).max()
+    assert m["mean_u"] == o.bulk_velocity() and m["max_div"] == o.max_divergence()
+    assert (m["cfl_conv"], m["cfl_visc"]) == o.compute_cfl()
+    assert m["t"] == o.t and m["dt"] == o.dt and m["nan_flag"] == 0.0
+    assert 0.5 < m["u_tau_lo"] < 2.0 and 0.5 < m["u_tau_hi"] < 2.0
