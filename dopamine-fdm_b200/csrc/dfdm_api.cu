@@ -656,10 +656,10 @@ template <typename T> struct Impl {
         CKL();
         k_bulk_final<<<1, 256, 0, c->stream>>>(c->red_blocks, c->red_part, 0.0, c->red_out);
         CKL();
-        const int ncol = c->d.Nx * c->d.Nz;
+        const int ncol = c->d.Nx * (c->d.Nz + 1);   // the reference's (nx-2)*(nzg-2) columns
         double *wsum = c->wm ? (double *)(c->d_mon + 5) : nullptr;
         if (wsum) {
-            k_wall_diag<<<1, 256, 0, c->stream>>>(ncol, c->wsd.tx, wsum);
+            k_wall_diag<<<1, 256, 0, c->stream>>>(c->d.Nx, c->d.Nz, c->wsd.tx, wsum);
             CKL();
         }
         k_monitor_final<<<1, 32, 0, c->stream>>>(c->d_mon, (const int *)(c->d_mon + 4), c->red_out, wsum, ncol,

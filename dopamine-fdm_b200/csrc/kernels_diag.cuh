@@ -215,11 +215,19 @@ __global__ void __launch_bounds__(256) k_monitor_rows(Dims d, const T *__restric
     if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
 }
 
-// wall_diag_sums (src/wallmodel.f90:700-723): the sums over the wall-parallel columns of the wall model's u_tau
-// (the filter state tx, both walls) into out[0], out[1]; one block, compensated per-thread sums then a fixed tree.
-__global__ void __launch_bounds__(256) k_wall_diag(int ncol, const double *__restrict__ tx, double *__restrict__ out) {
+// wall_diag_sums (src/wallmodel.f90:700-723): the sums of the wall model's u_tau (tx, planes (wall, k, i)) over the
+// reference's columns i = 2..nx-1, k = 2..nzg-1 into out[0], out[1].  Those are the Nx*Nz independent columns plus
+// the periodic duplicate k = nzg-1 of the first z-plane, so plane k = 0 counts twice and the column count is
+// Nx*(Nz+1).  One block, compensated per-thread sums then a fixed tree.
+__global__ void __launch_bounds__(256) k_wall_diag(int Nx, int Nz, const double *__restrict__ tx,
+                                                   double *__restrict__ out) {
     Kahan s, w; s.init(); w.init();
-    for (int p = threadIdx.x; p < ncol; p += blockDim.x) { s.add(tx[p]); w.add(tx[ncol + p]); }
+    const int plane = Nx * Nz;
+    for (int q = threadIdx.x; q < plane + Nx; q += blockDim.x) {
+        const int p = q < plane ? q : q - plane;
+        s.add(tx[p]);
+        w.add(tx[plane + p]);
+    }
     block_sum2(s.s, w.s, out);   // gridDim.x == 1
 }
 

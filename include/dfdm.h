@@ -201,7 +201,8 @@ typedef struct dfdm_monitor {
     double max_div;    /* check_divergence (max_divergence) */
     double cfl_conv;   /* compute_cfl of the current state, convective */
     double cfl_visc;   /* compute_cfl of the current state, viscous */
-    double u_tau_lo;   /* wall_diag_sums (src/wallmodel.f90:700-723): mean u_tau of the lower wall; 0 without the y-wall model */
+    double u_tau_lo;   /* wall_diag_sums (src/wallmodel.f90:700-723): mean u_tau of the lower wall over the reference's
+                          (nx-2)*(nzg-2) columns (the periodic duplicate z-plane included); 0 without the y-wall model */
     double u_tau_hi;   /* the same for the upper wall */
     double nan_flag;   /* 1 when the guard of output_monitor trips (a NaN or Inf, or |u| > 1e8), else 0 */
 } dfdm_monitor;
