@@ -22,6 +22,7 @@
 #include "kernels_fft2l.cuh"
 #include "kernels_poisson.cuh"
 #include "kernels_step.cuh"
+#include "kernels_hybrid.cuh"
 
 using namespace dfdm;
 
@@ -109,6 +110,7 @@ struct dfdm_ctx {
     bool adaptive = false, landing = false;
     double cfl_target = 0.5, cfl_safety = 0.9, dt_min = 1e-10, dt_max = 1e10;
     double t_land = std::numeric_limits<double>::quiet_NaN();
+    void *adv = nullptr;   // advection_scheme = 2: the dissipative terms, 3 fields of the storage type
     bool dev_dt() const { return adaptive || landing; }
     double *staging = nullptr;
     size_t staging_n = 0;
@@ -252,6 +254,7 @@ template <typename T> StepArgs<T> step_args(dfdm_ctx *c) {
     a.ygtop = c->Ly - c->yg[c->nyg - 1];
     a.ub = (const T *)c->d_ub;
     a.ubd = c->d_ubd;
+    a.adv = (const T *)c->adv;
     return a;
 }
 
@@ -610,6 +613,22 @@ template <typename T> struct Impl {
         }
         case 10:   // CFL maxima (the step-start part of the adaptive time step)
             return cfl_maxima(c);
+        case 11: {   // advection_scheme = 2: the dissipative terms of the coming stage kernel
+            if (!c->adv) return DFDM_OK;
+            HybArgs<T> h;
+            h.d = d;
+            h.beta = (T)c->prm.adv_beta0;
+            h.inv_dx = (T)(1.0 / c->dx);
+            h.my = metric_view<T>(c->my_t, d.Ny);
+            h.mz = metric_view<T>(c->mz_t, d.Nz);
+            h.ub = (const T *)c->d_ub;
+            if (c->prm.adv_order == 5)
+                k_adv_hybrid<T, 5><<<cell_grid(d), CELL_BLOCK, 0, st>>>(h, f(c->u), f(c->v), f(c->w), f(c->adv));
+            else
+                k_adv_hybrid<T, 3><<<cell_grid(d), CELL_BLOCK, 0, st>>>(h, f(c->u), f(c->v), f(c->w), f(c->adv));
+            CKL();
+            return DFDM_OK;
+        }
         }
         return fail(DFDM_ERR_INVALID, "unknown kernel family");
     }
@@ -684,6 +703,7 @@ template <typename T> struct Impl {
             if ((rc = launch(c, 0, s))) return rc;   // SGS (step start, then stages 2 and 3)
             if (s == 1 && c->dev_dt() && (rc = select_dt(c))) return rc;   // dt from the start-of-step CFL, after nu_t
             if ((rc = launch(c, 8, s))) return rc;   // wall model
+            if ((rc = launch(c, 11, s))) return rc;  // hybrid-scheme dissipation (advection_scheme = 2)
             if ((rc = launch(c, 1, s))) return rc;   // RHS + RK update
             if ((rc = poisson_chain(c, s))) return rc;
         }
@@ -742,8 +762,13 @@ int validate(const dfdm_grid *g, const dfdm_params *p) {
     if (p->flat_wall_model_flag < 0 || p->flat_wall_model_flag > 1)
         return fail(DFDM_ERR_UNSUPPORTED, "flat_wall_model_flag must be 0 or 1 (the rough-wall law is off the path)");
     if (p->flat_wall_model_flag == 1 && g->y_bc_type != 1) return fail(DFDM_ERR_INVALID, "the flat-wall model needs y walls");
-    if (p->advection_scheme != 0 && p->advection_scheme != 1)
-        return fail(DFDM_ERR_UNSUPPORTED, "advection_scheme must be 0 or 1 (the hybrid upwind scheme is off the path)");
+    if (p->advection_scheme < 0 || p->advection_scheme > 2)
+        return fail(DFDM_ERR_INVALID, "ERROR: advection_scheme must be 0 (skew-symmetric), 1 (divergence-form central) or 2 "
+                                      "(skew-symmetric + upwind-biased dissipation)");
+    if (p->advection_scheme == 2) {
+        if (p->adv_order != 3 && p->adv_order != 5) return fail(DFDM_ERR_INVALID, "ERROR: adv_order must be 3 or 5");
+        if (!(p->adv_beta0 >= 0.0)) return fail(DFDM_ERR_INVALID, "ERROR: adv_beta0 and adv_beta_ibm must be >= 0");
+    }
     if (!(p->dt > 0.0)) return fail(DFDM_ERR_INVALID, "ERROR: &NUMERICS dt must be > 0");
     if (!(p->nu >= 0.0)) return fail(DFDM_ERR_INVALID, "ERROR: &PHYSICS nu must be set");
     if (p->precision != DFDM_FP64 && p->precision != DFDM_FP32_MIXED) return fail(DFDM_ERR_INVALID, "unknown precision");
@@ -768,7 +793,8 @@ size_t arena_bytes(const dfdm_grid *g, const dfdm_params *p) {
     size_t ts = p->precision == DFDM_FP64 ? 8 : 4;
     size_t Nx = g->nx - 2, Nz = g->nz - 2, Ny = g->y_bc_type == 0 ? g->ny - 2 : g->ny - 1;
     size_t cells = Nx * Ny * Nz, spec = (Nx / 2 + 1) * Ny * Nz;
-    size_t n = cells * ts * (3 /*u*/ + 3 /*uo*/ + 3 /*F1*/ + 3 /*u**/ + 1 /*P*/ + 1 /*phi*/ + (p->sgs_model ? 1 : 0));
+    size_t n = cells * ts * (3 /*u*/ + 3 /*uo*/ + 3 /*F1*/ + 3 /*u**/ + 1 /*P*/ + 1 /*phi*/ + (p->sgs_model ? 1 : 0) +
+                             (p->advection_scheme == 2 ? 3 /*hybrid-scheme terms*/ : 0));
     n += spec * 2 * ts;
     if (g->y_bc_type != 0) n += (Nx / 2 + 1) * Ny * Nz * 8;   // pivot table of the y solves
     n += 8 * Nx * Nz * 2 * 8;   // wall planes
@@ -798,6 +824,8 @@ void dfdm_default_params(dfdm_params *p) {
     p->C_amd = 1.0 / 3.0;        // :307
     p->flat_wall_model_flag = 0; // :312
     p->advection_scheme = 0;
+    p->adv_order = 3;
+    p->adv_beta0 = 0.05;
     p->adv_wall_layers = -1;
     p->wm_filter_mode = -1;
     p->wm_filter_Tf_fac = 1.0;
@@ -1021,6 +1049,10 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
     c->d_cfl = (unsigned long long *)tmp;
     if ((rc = dalloc(c, &tmp, 4 * sizeof(double)))) return bail(rc);
     c->d_dtt = (double *)tmp;
+    if (prm->advection_scheme == 2) {   // the dissipative terms of the hybrid scheme
+        if ((rc = dalloc(c, &c->adv, (size_t)3 * d.cells * c->ts))) return bail(rc);
+        CK(cudaMemsetAsync(c->adv, 0, (size_t)3 * d.cells * c->ts, c->stream));
+    }
     c->in_create = false;   // later buffers (host staging, the unit RHS output) are separate allocations
 
     rc = dispatch(c, [&](auto impl) { return decltype(impl)::setup_kernels(c); });
@@ -1328,6 +1360,7 @@ int dfdm_compute_rhs(dfdm_ctx *c, double *rhs_u, double *rhs_v, double *rhs_w) {
     int rc = dispatch(c, [&](auto impl) {
         typedef decltype(impl) I;
         StageCoef sc{1, 0.0, 0.0, 0.0, 0.0, 0};
+        if (int rc2 = I::launch(c, 11, 1)) return rc2;   // the hybrid scheme's dissipation of the resident state
         return I::stage_kernel(c, sc, I::f(c->rhs3));
     });
     if (rc) return rc;
@@ -1766,7 +1799,7 @@ int dfdm_pad_field(dfdm_ctx *c, int field, int extra_planes, double *out) {
 int dfdm_launch_kernel_async(dfdm_ctx *c, int which, int rk_stage) {
     g_err.clear();
     if (int rc = check_ctx(c)) return rc;
-    if (which < 0 || which > 10 || rk_stage < 1 || rk_stage > 3) return fail(DFDM_ERR_INVALID, "bad kernel id or stage");
+    if (which < 0 || which > 11 || rk_stage < 1 || rk_stage > 3) return fail(DFDM_ERR_INVALID, "bad kernel id or stage");
     long long before = g_launches;
     int rc = dispatch(c, [&](auto impl) { return decltype(impl)::launch(c, which, rk_stage); });
     c->launches += g_launches - before;
@@ -1815,6 +1848,7 @@ int dfdm_kernel_bytes(dfdm_ctx *c, int which, double *bytes) {
     case 7: b = 7.0 * cell; break;                                // read phi, u*; write u (+P at stage 3)
     case 9: b = c->prm.flow_forcing_mode == 1 ? 3.0 * cell : 0.0; break;   // bulk sum reads U; the shift reads + writes U
     case 10: b = 3.0 * cell + (c->les ? cell : 0.0); break;       // read U, V, W (+ nu_t)
+    case 11: b = c->adv ? 6.0 * cell : 0.0; break;                // read U, V, W; write the three terms
     default: return fail(DFDM_ERR_INVALID, "bad kernel id");
     }
     *bytes = b;

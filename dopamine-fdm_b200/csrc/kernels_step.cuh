@@ -23,6 +23,9 @@ template <typename T> struct StepArgs {
     // representable in the storage type; ubd is the same profile in double.
     const T *ub;
     const double *ubd;
+    // advection_scheme = 2: the dissipative terms of k_adv_hybrid (u, v, w blocks of `cells`), added to the
+    // right-hand sides; null otherwise
+    const T *adv;
 };
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -608,6 +611,10 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
                 T ru = rhs_u_at<T, LES, WM>(a, q, Y, Z, tau_x, i, j, k);
                 T rw = rhs_w_at<T, LES, WM>(a, q, Y, Z, tau_z, i, j, k);
                 T rv = vrow ? rhs_v_at<T, LES, WM>(a, q, Y, Z, i, j, k) : T(0);
+                if (a.adv) {
+                    ru = ru + a.adv[p]; rw = rw + a.adv[2 * d.cells + p];
+                    if (vrow) rv = rv + a.adv[d.cells + p];
+                }
                 if (rhs_only) {
                     rhs_only[p] = ru; rhs_only[d.cells + p] = rv; rhs_only[2 * d.cells + p] = rw;
                 } else if (sc.stage == 1) {
@@ -753,6 +760,10 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
             F2 ru = rhs_u_at<F2, LES, WM>(a, q, Y, Z, tau_x, i, j, k);
             F2 rw = rhs_w_at<F2, LES, WM>(a, q, Y, Z, tau_z, i, j, k);
             F2 rv = vrow ? rhs_v_at<F2, LES, WM>(a, q, Y, Z, i, j, k) : F2(0.0f);
+            if (a.adv) {
+                ru = ru + ld2(a.adv); rw = rw + ld2(a.adv + 2 * d.cells);
+                if (vrow) rv = rv + ld2(a.adv + d.cells);
+            }
             if (rhs_only) {
                 st2(rhs_only, ru); st2(rhs_only + d.cells, rv); st2(rhs_only + 2 * d.cells, rw);
             } else if (sc.stage == 1) {

@@ -34,7 +34,7 @@ class DfdmParams(ctypes.Structure):
                 ("sgs_model", c_int), ("Cs_vreman", c_double), ("C_amd", c_double),
                 ("flat_wall_model_flag", c_int), ("advection_scheme", c_int), ("adv_wall_layers", c_int),
                 ("wm_filter_mode", c_int), ("wm_filter_Tf_fac", c_double), ("flow_forcing_mode", c_int),
-                ("Ub_target", c_double), ("precision", c_int)]
+                ("Ub_target", c_double), ("precision", c_int), ("adv_order", c_int), ("adv_beta0", c_double)]
 
 
 def dptr(a: np.ndarray):
@@ -57,4 +57,5 @@ class GridHolder:
 def make_params(case: Case, precision: int = DFDM_FP64) -> DfdmParams:
     return DfdmParams(case.nu, case.dt, case.dPdx, case.dPdz, case.sgs_model, case.Cs_vreman, case.C_amd,
                       case.flat_wall_model_flag, case.advection_scheme, case.adv_wall_layers, case.wm_filter_mode,
-                      case.wm_filter_Tf_fac, case.flow_forcing_mode, case.Ub_target, int(precision))
+                      case.wm_filter_Tf_fac, case.flow_forcing_mode, case.Ub_target, int(precision),
+                      case.adv_order, case.adv_beta0)

@@ -42,7 +42,9 @@ class Case:
     Cs_vreman: float = 0.17
     C_amd: float = 1.0 / 3.0
     flat_wall_model_flag: int = 0
-    advection_scheme: int = 0
+    advection_scheme: int = 0    # 0 skew-symmetric, 1 divergence form, 2 skew + upwind-biased dissipation
+    adv_order: int = 3           # advection_scheme = 2: dissipation order (3 or 5)
+    adv_beta0: float = 0.05      # advection_scheme = 2: dissipation coefficient
     adv_wall_layers: int = -1
     wm_filter_mode: int = -1
     wm_filter_Tf_fac: float = 1.0

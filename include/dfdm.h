@@ -68,13 +68,17 @@ typedef struct dfdm_params {
     double Cs_vreman;          /* Vreman constant (0.17) */
     double C_amd;              /* AMD constant (1/3) */
     int    flat_wall_model_flag; /* 0 no-slip walls, 1 smooth Reichardt EQWM */
-    int    advection_scheme;   /* 0 skew-symmetric blend, 1 divergence form */
+    int    advection_scheme;   /* 0 skew-symmetric blend, 1 divergence form, 2 skew-symmetric + upwind-biased
+                                  dissipation (src/adv_hybrid.f90) */
     int    adv_wall_layers;    /* -1 automatic */
     int    wm_filter_mode;     /* -1 automatic, 0 raw, 1 temporal filter */
     double wm_filter_Tf_fac;   /* filter time-scale factor (1.0) */
     int    flow_forcing_mode;  /* 0 prescribed dPdx, 1 constant flux */
     double Ub_target;          /* bulk velocity target of the constant-flux forcing */
     int    precision;          /* DFDM_FP64 or DFDM_FP32_MIXED */
+    int    adv_order;          /* advection_scheme = 2: order of the dissipation, 3 or 5 (default 3) */
+    double adv_beta0;          /* advection_scheme = 2: its coefficient beta, >= 0 (default 0.05); with no immersed
+                                  body beta = adv_beta0 everywhere (src/adv_hybrid.f90:22-74) */
 } dfdm_params;
 
 typedef struct dfdm_ctx dfdm_ctx;

@@ -395,6 +395,77 @@ struct Oracle {
     bool wall_hi() const { return y_bc_type == 1 && bc_face_yhi == 1; }
 
     // ---- compute_rhs_u (src/equations.f90:25-257) ----
+    // ---- advection_scheme = 2: upwind-biased dissipation (src/adv_hybrid.f90), beta = adv_beta0 (no solid) ----
+    // adv_wsel (:88-103): stencil weights of the dissipative flux for s(-2:3)
+    static void adv_wsel(int o, double w[6]) {
+        static const double w5[6] = {1.0, -5.0, 10.0, -10.0, 5.0, -1.0}, w3[6] = {0.0, -1.0, 3.0, -3.0, 1.0, 0.0};
+        for (int q = 0; q < 6; ++q) w[q] = (o == 5) ? w5[q] / 60.0 : (o == 3) ? w3[q] / 12.0 : 0.0;
+    }
+    // adv_dflux (:106-117)
+    static double adv_dflux(double a, double b, double c, double d, double e, double f, double uc, double beta,
+                            const double w[6]) {
+        return beta * std::fabs(uc) * (w[0] * a + w[1] * b + w[2] * c + w[3] * d + w[4] * e + w[5] * f);
+    }
+    // adv_ord_y (:120-133): order usable for the face between rows m and m+1 of 1..n
+    static int adv_ord_y(int m, int n, int ord) {
+        if (ord == 5 && m - 2 >= 1 && m + 3 <= n) return 5;
+        if (m - 1 >= 1 && m + 2 <= n) return 3;
+        return 0;
+    }
+    // the padded copies of pad_field_dev (src/halo_pad.f90:185-240) on one rank: x and z extended periodically
+    double pad(const A3 &F, int i, int j, int k) const {
+        const int Nc = nx - 2, Nzc = nz - 2;
+        const int iw = 2 + (((i - 2) % Nc) + Nc) % Nc, kw = 2 + (((k - 2) % Nzc) + Nzc) % Nzc;
+        return F(iw, j, kw);
+    }
+    // adv_add_u / adv_add_v / adv_add_w (:136-282): rhs += -d/dx_j of the dissipative fluxes.  `comp` 0 u, 1 v, 2 w.
+    void adv_add(int comp, A3 &rhs) {
+        const int n = prm.adv_order;
+        double wx[6], wy[6];
+        adv_wsel(n, wx);
+        const double inv_dx = 1.0 / dx, bt = prm.adv_beta0;
+        const A3 &F = comp == 0 ? U : comp == 1 ? V : W;
+        const int ihi = comp == 0 ? nx - 1 : nxg - 1, jhi = comp == 1 ? ny - 1 : nyg - 1, khi = comp == 2 ? nz - 1 : nzg - 1;
+        const int ny_f = comp == 1 ? ny : nyg;   // rows of the advected field
+#pragma omp parallel for
+        for (int k = 2; k <= khi; ++k)
+            for (int j = 2; j <= jhi; ++j)
+                for (int i = 2; i <= ihi; ++i) {
+                    double dyj, dzk;
+                    if (comp == 1) dyj = 1.0 / (yg[j + 1] - yg[j]); else dyj = 1.0 / (y[j] - y[j - 1]);
+                    if (comp == 2) dzk = 1.0 / (zg[k + 1] - zg[k]); else dzk = 1.0 / (z[k] - z[k - 1]);
+                    double r = 0.0;
+                    for (int m = 0; m <= 1; ++m) {
+                        const double sg = 2.0 * m - 1.0;
+                        const int ii = i - 1 + m, jj = j - 1 + m, kk = k - 1 + m;
+                        // the convecting velocity at the face, at the advected field's position
+                        double ucx, ucy, ucz;
+                        if (comp == 0) {
+                            ucx = 0.5 * (pad(U, ii, j, k) + pad(U, ii + 1, j, k));
+                            ucy = 0.5 * (pad(V, i, jj, k) + pad(V, i + 1, jj, k));
+                            ucz = 0.5 * (pad(W, i, j, kk) + pad(W, i + 1, j, kk));
+                        } else if (comp == 1) {
+                            ucx = 0.5 * (pad(U, ii, j, k) + pad(U, ii, j + 1, k));
+                            ucy = 0.5 * (pad(V, i, jj, k) + pad(V, i, jj + 1, k));
+                            ucz = 0.5 * (pad(W, i, j, kk) + pad(W, i, j + 1, kk));
+                        } else {
+                            ucx = 0.5 * (pad(U, ii, j, k) + pad(U, ii, j, k + 1));
+                            ucy = 0.5 * (pad(V, i, jj, k) + pad(V, i, jj, k + 1));
+                            ucz = 0.5 * (pad(W, i, j, kk) + pad(W, i, j, kk + 1));
+                        }
+                        r = r - sg * adv_dflux(pad(F, ii - 2, j, k), pad(F, ii - 1, j, k), pad(F, ii, j, k), pad(F, ii + 1, j, k),
+                                               pad(F, ii + 2, j, k), pad(F, ii + 3, j, k), ucx, bt, wx) * inv_dx;
+                        adv_wsel(adv_ord_y(jj, ny_f, n), wy);
+                        r = r - sg * adv_dflux(pad(F, i, std::max(jj - 2, 1), k), pad(F, i, std::max(jj - 1, 1), k), pad(F, i, jj, k),
+                                               pad(F, i, jj + 1, k), pad(F, i, std::min(jj + 2, ny_f), k),
+                                               pad(F, i, std::min(jj + 3, ny_f), k), ucy, bt, wy) * dyj;
+                        r = r - sg * adv_dflux(pad(F, i, j, kk - 2), pad(F, i, j, kk - 1), pad(F, i, j, kk), pad(F, i, j, kk + 1),
+                                               pad(F, i, j, kk + 2), pad(F, i, j, kk + 3), ucz, bt, wx) * dzk;
+                    }
+                    rhs(i, j, k) = rhs(i, j, k) + r;
+                }
+    }
+
     void compute_rhs_u(A3 &rhs_u) {
         bool wlo = wall_lo(), whi = wall_hi();
         bool wm_lo = wlo && prm.flat_wall_model_flag > 0, wm_hi = whi && prm.flat_wall_model_flag > 0;
@@ -435,6 +506,7 @@ struct Oracle {
                                                        wa * 0.5 * (term_2(i, j, k - 1) + term_2(i, j, k)) * (term_1(i, j, k) - term_1(i, j, k - 1))) /
                                                           (z[k] - z[k - 1]);
             }
+        if (prm.advection_scheme == 2) adv_add(0, rhs_u);   // src/equations.f90:149
         // viscous terms
 #pragma omp parallel for
         for (int k = 1; k <= nzg; ++k)
@@ -508,6 +580,7 @@ struct Oracle {
                     rhs_v(i, j, k) = rhs_v(i, j, k) - (wd * (term_1(i, j, k) * term_2(i, j, k) - term_1(i, j, k - 1) * term_2(i, j, k - 1)) +
                                                        wa * 0.5 * (term_2(i, j, k - 1) + term_2(i, j, k)) * (term_1(i, j, k) - term_1(i, j, k - 1))) /
                                                           (z[k] - z[k - 1]);
+        if (prm.advection_scheme == 2) adv_add(1, rhs_v);   // src/equations.f90:373
 #pragma omp parallel for
         for (int k = 2; k <= nzg - 1; ++k)
             for (int j = 2; j <= ny - 1; ++j) {
@@ -578,6 +651,7 @@ struct Oracle {
                                                        wa * 0.5 * (term_1(i, j - 1, k) + term_1(i, j, k)) * (term_2(i, j, k) - term_2(i, j - 1, k))) /
                                                           (y[j] - y[j - 1]);
             }
+        if (prm.advection_scheme == 2) adv_add(2, rhs_w);   // src/equations.f90:602
 #pragma omp parallel for
         for (int k = 1; k <= nz; ++k)
             for (int j = 1; j <= nyg - 1; ++j)

@@ -32,12 +32,15 @@ def test_default_params_match_reference_defaults():
     L.dfdm_default_params(ctypes.byref(p))
     assert p.sgs_model == 2 and abs(p.Cs_vreman - 0.17) < 1e-15 and abs(p.C_amd - 1.0 / 3.0) < 1e-15
     assert p.adv_wall_layers == -1 and p.wm_filter_mode == -1 and p.flat_wall_model_flag == 0
+    assert p.advection_scheme == 0 and p.adv_order == 3 and abs(p.adv_beta0 - 0.05) < 1e-15   # src/global.f90:71-72
 
 
 @pytest.mark.parametrize("mutate,code,msg", [
     (dict(nx=17), 1, "even"),
     (dict(sgs_model=3), 1, "sgs_model"),
-    (dict(advection_scheme=2), 4, "hybrid"),
+    (dict(advection_scheme=3), 1, "advection_scheme"),
+    (dict(advection_scheme=2, adv_order=4), 1, "adv_order"),
+    (dict(advection_scheme=2, adv_beta0=-1.0), 1, "adv_beta0"),
     (dict(flat_wall_model_flag=2), 4, "rough"),
     (dict(dt=0.0), 1, "dt"),
 ])

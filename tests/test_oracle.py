@@ -238,3 +238,34 @@ def test_output_monitor_restatement(oracle_mod):
     assert (m["cfl_conv"], m["cfl_visc"]) == o.compute_cfl()
     assert m["t"] == o.t and m["dt"] == o.dt and m["nan_flag"] == 0.0
     assert 0.5 < m["u_tau_lo"] < 2.0 and 0.5 < m["u_tau_hi"] < 2.0
+
+
+@pytest.mark.parametrize("order,factor,power", [(3, 4.0 / 3.0, 4), (5, 16.0 / 15.0, 6)])
+def test_hybrid_dissipation_symbol(oracle_mod, order, factor, power):
+    """advection_scheme = 2 (src/adv_hybrid.f90) on a pure x-mode W = a cos(theta (i-2)) convected by a uniform
+    U = u0 > 0 (fully periodic box): the added rhs_w is the known symbol of the dissipation,
+    -(4/3) beta u0/dx sin^4(theta/2) W for order 3 and -(16/15) beta u0/dx sin^6(theta/2) W for order 5."""
+    base = cases.get("tgv_small")
+    Nx = base.cells[0]
+    theta, a, u0, beta = 2.0 * math.pi * 3 / Nx, 0.1, 1.0, 0.3
+    U, V, W, P = (np.zeros(base.shapes()[k], order="F") for k in "UVWP")
+    U[...] = u0
+    i = np.arange(W.shape[0])
+    W[...] = (a * np.cos(theta * (i - 1)))[:, None, None]   # 0-based index i is the reference's i+1
+    out = {}
+    for scheme in (0, 2):
+        c = base.with_(advection_scheme=scheme, adv_order=order, adv_beta0=beta)
+        o = oracle_mod.Oracle(c)
+        o.set_state(U, V, W, P)
+        out[scheme] = o.compute_rhs()[2]
+    dw = out[2] - out[0]
+    dx = (cases.faces(base)[0][1] - cases.faces(base)[0][0])
+    iw = np.arange(dw.shape[0])   # rhs arrays start at the reference's i = 2
+    want = -factor * beta * u0 / dx * math.sin(theta / 2) ** power * (a * np.cos(theta * iw))[:, None, None]
+    want = np.broadcast_to(want, dw.shape)
+    assert np.abs(dw - want).max() <= 1e-10 * np.abs(want).max()
+    # beta = 0 is advection_scheme = 0 (the reference's statement, src/adv_hybrid.f90:4-5)
+    c = base.with_(advection_scheme=2, adv_order=order, adv_beta0=0.0)
+    o = oracle_mod.Oracle(c)
+    o.set_state(U, V, W, P)
+    assert np.array_equal(o.compute_rhs()[2], out[0])
