@@ -421,7 +421,7 @@ struct Oracle {
     // adv_add_u / adv_add_v / adv_add_w (:136-282): rhs += -d/dx_j of the dissipative fluxes.  `comp` 0 u, 1 v, 2 w.
     void adv_add(int comp, A3 &rhs) {
         const int n = prm.adv_order;
-        double wx[6], wy[6];
+        double wx[6];
         adv_wsel(n, wx);
         const double inv_dx = 1.0 / dx, bt = prm.adv_beta0;
         const A3 &F = comp == 0 ? U : comp == 1 ? V : W;
@@ -434,7 +434,7 @@ struct Oracle {
                     double dyj, dzk;
                     if (comp == 1) dyj = 1.0 / (yg[j + 1] - yg[j]); else dyj = 1.0 / (y[j] - y[j - 1]);
                     if (comp == 2) dzk = 1.0 / (zg[k + 1] - zg[k]); else dzk = 1.0 / (z[k] - z[k - 1]);
-                    double r = 0.0;
+                    double r = 0.0, wy[6];   // per thread: the y order changes near the ends
                     for (int m = 0; m <= 1; ++m) {
                         const double sg = 2.0 * m - 1.0;
                         const int ii = i - 1 + m, jj = j - 1 + m, kk = k - 1 + m;
