@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream measurement")
     ap.add_argument("--no-adaptive", action="store_true", help="skip the adaptive-time-step run")
+    ap.add_argument("--no-hybrid", action="store_true", help="skip the advection_scheme = 2 runs")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-vs-FP64 report of the other configs")
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-rate", type=float, default=4.0, help="Poisson arrival rate, requests/s")
@@ -250,8 +251,8 @@ def main():
 
     U, V, W, P = cases.initial_condition(c)
 
-    def timed_run(prec, sample_clocks=False, adaptive=False):
-        s = Solver(c, prec, graphs=True)
+    def timed_run(prec, sample_clocks=False, adaptive=False, case=None):
+        s = Solver(case or c, prec, graphs=True)
         s.set_stream(sh)
         s.set_state(U, V, W, P)
         if adaptive:
@@ -306,6 +307,29 @@ def main():
                               "overhead_ms_per_step": (msa - ms32) / args.steps, "gpu_launches": la,
                               "dt_last": sa.dt, "cfl_target": 0.5, "cfl_safety": 0.9}
         sa.close()
+
+    # ---- the same step with advection_scheme = 2 (upwind-biased dissipation, orders 3 and 5) ----
+    if not args.no_hybrid:
+        hyb = {}
+        for order in (3, 5):
+            ch = c.with_(advection_scheme=2, adv_order=order, adv_beta0=0.05)
+            sh_, msh, _, lh = timed_run("fp32", case=ch)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            for _ in range(3):
+                sh_.launch_kernel_async("hybrid", 2)
+            e0.record(stream)
+            for _ in range(20):
+                sh_.launch_kernel_async("hybrid", 2)
+            e1.record(stream)
+            e1.synchronize()
+            kms = e0.elapsed_time(e1) / 20
+            kb = sh_.kernel_bytes("hybrid")
+            hyb[f"order{order}"] = {"value": ws * c.n_cells * args.steps / (msh / 1e3), "ms_per_step": msh / args.steps,
+                                    "gpu_launches": lh, "k_adv_hybrid_ms": kms,
+                                    "k_adv_hybrid_GBps": kb / (kms * 1e-3) / 1e9}
+            sh_.close()
+        out["hybrid_scheme"] = hyb
 
     # ---- roofline: per-kernel-family device time of one stage, dominant family against HBM peak ----
     peak, peak_kind = measured_peaks()

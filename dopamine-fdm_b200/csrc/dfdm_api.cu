@@ -415,29 +415,35 @@ template <typename T> struct Impl {
         return sizeof(T) == 4 && s == 3 && c->projected && !c->unit_projection;
     }
 
-    template <bool LES, bool WM> static void stage_launch(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
+    template <bool LES, bool WM, bool HYB> static void stage_launch(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
         const Dims &d = c->d;
         if constexpr (sizeof(T) == 4) {
             if (c->stage_variant == 1) {
-                k_tiled2<LES, WM><<<tile_grid(d, c->kc_stage2, TILE_X2), 256, 0, c->stream>>>(step_args<T>(c), f(c->u),
-                    f(c->v), f(c->w), LES ? f(c->nut) : nullptr, c->wsd.tau_x, c->wsd.tau_z, sc, c->kc_stage2, f(c->uo),
-                    f(c->vo), f(c->wo), f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf), rhs_only);
+                k_tiled2<LES, WM, 8, HYB><<<tile_grid(d, c->kc_stage2, TILE_X2), 256, 0, c->stream>>>(step_args<T>(c),
+                    f(c->u), f(c->v), f(c->w), LES ? f(c->nut) : nullptr, c->wsd.tau_x, c->wsd.tau_z, sc, c->kc_stage2,
+                    f(c->uo), f(c->vo), f(c->wo), f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf), rhs_only);
                 return;
             }
         }
-        k_tiled<T, LES, WM, TILE_X, TILE_Y, 0><<<tile_grid(d, c->kc_stage), TILE_X * TILE_Y, 0, c->stream>>>(
+        k_tiled<T, LES, WM, TILE_X, TILE_Y, HYB ? 2 : 0><<<tile_grid(d, c->kc_stage), TILE_X * TILE_Y, 0, c->stream>>>(
             step_args<T>(c), f(c->u), f(c->v), f(c->w), LES ? f(c->nut) : nullptr, c->wsd.tau_x, c->wsd.tau_z, sc,
             c->kc_stage, f(c->uo), f(c->vo), f(c->wo), f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf),
             rhs_only, nullptr);
     }
+    template <bool HYB> static void stage_dispatch(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
+        if constexpr (sizeof(T) == 8) {   // FP64 keeps the runtime wall-model flag
+            if (c->les) stage_launch<true, true, HYB>(c, sc, rhs_only); else stage_launch<false, true, HYB>(c, sc, rhs_only);
+        } else {
+            if (c->les) {
+                if (c->wm) stage_launch<true, true, HYB>(c, sc, rhs_only); else stage_launch<true, false, HYB>(c, sc, rhs_only);
+            } else {
+                if (c->wm) stage_launch<false, true, HYB>(c, sc, rhs_only); else stage_launch<false, false, HYB>(c, sc, rhs_only);
+            }
+        }
+    }
 
     static int stage_kernel(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
-        if constexpr (sizeof(T) == 8) {   // FP64 keeps the runtime wall-model flag
-            if (c->les) stage_launch<true, true>(c, sc, rhs_only); else stage_launch<false, true>(c, sc, rhs_only);
-        } else {
-            if (c->les) { if (c->wm) stage_launch<true, true>(c, sc, rhs_only); else stage_launch<true, false>(c, sc, rhs_only); }
-            else { if (c->wm) stage_launch<false, true>(c, sc, rhs_only); else stage_launch<false, false>(c, sc, rhs_only); }
-        }
+        if (c->adv) stage_dispatch<true>(c, sc, rhs_only); else stage_dispatch<false>(c, sc, rhs_only);
         CKL();
         return DFDM_OK;
     }

@@ -479,7 +479,8 @@ template <int PX> struct TileQ2 {
 
 
 
-// Tiled kernels (KIND 0: fused stage, KIND 1: eddy viscosity), 2.5-D blocked: a block owns a TX x TY column of
+// Tiled kernels (KIND 0: fused stage, KIND 1: eddy viscosity, KIND 2: fused stage adding the dissipative terms of
+// advection_scheme = 2 from StepArgs::adv), 2.5-D blocked: a block owns a TX x TY column of
 // (i,j) cells and marches through a chunk of kc z-planes.  Each z-plane of U, V, W (and nu_t) is copied from HBM
 // once per block, with its one-cell halo, into one of four rotating shared planes by cp.async: the copies of
 // plane k+2 are in flight while the cells of plane k are evaluated, and one barrier per plane suffices.  After
@@ -611,7 +612,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
                 T ru = rhs_u_at<T, LES, WM>(a, q, Y, Z, tau_x, i, j, k);
                 T rw = rhs_w_at<T, LES, WM>(a, q, Y, Z, tau_z, i, j, k);
                 T rv = vrow ? rhs_v_at<T, LES, WM>(a, q, Y, Z, i, j, k) : T(0);
-                if (a.adv) {
+                if constexpr (KIND == 2) {
                     ru = ru + a.adv[p]; rw = rw + a.adv[2 * d.cells + p];
                     if (vrow) rv = rv + a.adv[d.cells + p];
                 }
@@ -640,9 +641,9 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
 
 // FP32 stage kernel with two x-neighbour cells per thread, computed with the packed FP32x2 instructions (F2).  Same
 // loader, ghost rules and RK3 epilogue as k_tiled<float, LES, WM, ..., 0>; a block owns 64 x TY cells, one warp
-// per row of 32 cell pairs.  It needs ~118 registers: capping it at 96 or 80 (for more resident warps) spills
+// per row of 32 cell pairs; HYB adds the dissipative terms of advection_scheme = 2 (StepArgs::adv).  It needs ~118 registers: capping it at 96 or 80 (for more resident warps) spills
 // 170-300 bytes, so it runs 2 blocks of 256 threads per SM.  Shared rows hold cells i0-2 .. i0+65 (pitch 68), so every pair starts at an even index.
-template <bool LES, bool WM, int TY = 8>
+template <bool LES, bool WM, int TY = 8, bool HYB = false>
 __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<float> a, const float *__restrict__ U, const float *__restrict__ V,
                                                    const float *__restrict__ W, const float *__restrict__ NU,
                                                    const double *__restrict__ tau_x, const double *__restrict__ tau_z,
@@ -760,7 +761,7 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
             F2 ru = rhs_u_at<F2, LES, WM>(a, q, Y, Z, tau_x, i, j, k);
             F2 rw = rhs_w_at<F2, LES, WM>(a, q, Y, Z, tau_z, i, j, k);
             F2 rv = vrow ? rhs_v_at<F2, LES, WM>(a, q, Y, Z, i, j, k) : F2(0.0f);
-            if (a.adv) {
+            if constexpr (HYB) {
                 ru = ru + ld2(a.adv); rw = rw + ld2(a.adv + 2 * d.cells);
                 if (vrow) rv = rv + ld2(a.adv + d.cells);
             }

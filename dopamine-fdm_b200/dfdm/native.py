@@ -20,7 +20,7 @@ from .cases import Case
 _lib = None
 
 KERNELS = {"sgs": 0, "stage": 1, "fwd_x": 2, "fwd_z": 3, "y_solve": 4, "inv_z": 5, "inv_x": 6, "correct": 7,
-           "wall_model": 8, "flux_shift": 9, "cfl": 10}
+           "wall_model": 8, "flux_shift": 9, "cfl": 10, "hybrid": 11}
 
 # Every exported symbol of include/dfdm.h (checked by the CPU test suite).
 EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_create", "dfdm_destroy",

@@ -229,7 +229,7 @@ int dfdm_pad_field(dfdm_ctx *ctx, int field, int extra_planes, double *out);
 /* ---- profiling hooks: launch one kernel family of one RK stage on the context's stream, no sync ----
  * which: 0 SGS, 1 stage (RHS + RK update), 2 div + forward x-FFT, 3 forward z-FFT, 4 y solve,
  *        5 inverse z-FFT, 6 inverse x-FFT, 7 velocity correction, 8 wall model, 9 constant-flux bulk sum + shift,
- *        10 CFL maxima */
+ *        10 CFL maxima, 11 the dissipative terms of advection_scheme = 2 */
 int dfdm_launch_kernel_async(dfdm_ctx *ctx, int which, int rk_stage);
 /* Algorithmic HBM bytes one launch of that kernel family moves (the roofline numerator). */
 int dfdm_kernel_bytes(dfdm_ctx *ctx, int which, double *bytes);
