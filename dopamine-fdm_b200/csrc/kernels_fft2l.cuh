@@ -21,7 +21,7 @@ template <> struct Vec2<double> { typedef double2 type; };
 // Phase A forms the packed half-length line z_n = x_2n + i x_2n+1 in shared memory with consecutive threads on
 // consecutive pairs (coalesced 8-byte loads of the velocity pairs); the two register steps follow.
 template <typename T, bool FROM_DIV, int M>
-__global__ void __launch_bounds__(256) k_fwd_x2(PoissonArgs<T> a, int lx, const T *__restrict__ U, const T *__restrict__ V,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_fwd_x2(PoissonArgs<T> a, int lx, const T *__restrict__ U, const T *__restrict__ V,
                                                 const T *__restrict__ W, const T *__restrict__ src,
                                                 typename cplx_t<T>::type *__restrict__ spec,
                                                 const typename cplx_t<T>::type *__restrict__ tw,
@@ -38,36 +38,56 @@ __global__ void __launch_bounds__(256) k_fwd_x2(PoissonArgs<T> a, int lx, const 
     const int line0 = blockIdx.x * lx;
     const int nl = min(lx, Ny * Nz - line0);
     constexpr int ITEMS = RowLines<T, M>::value * M;   // lx == RowLines<T, M>::value, blockDim.x == 256
-#pragma unroll 4
-    for (int e0 = 0; e0 < ITEMS; e0 += 256) {
-        const int e = e0 + threadIdx.x;
-        if (e >= nl * M) break;
-        const int ll = e / M, n = e - ll * M;
-        const int line = line0 + ll;
-        C z;
-        if (FROM_DIV) {
-            const int k = (int)fdiv((unsigned)line, a.fNy), j = line - k * Ny;
-            const int ob = k * plane + j * Nx, i = 2 * n, o = ob + i;
-            const int dkm = (k == 0) ? (Nz - 1) * plane : -plane;
-            const int djm = (j > 0) ? -Nx : (Ny - 1) * Nx;
-            const bool vzero = (j == 0) && !d.yper;
-            const T inv_dyj = A::inv(a.my.dc, a.my.idc, j), inv_dzk = A::inv(a.mz.dc, a.mz.idc, k);
-            const T2 u = *reinterpret_cast<const T2 *>(U + o);
-            const T um = __ldg(U + (i == 0 ? ob + Nx - 1 : o - 1));
-            const T2 v = *reinterpret_cast<const T2 *>(V + o);
-            T2 vm;
-            if (vzero) { vm.x = T(0); vm.y = T(0); }
-            else vm = *reinterpret_cast<const T2 *>(V + o + djm);
-            const T2 w = *reinterpret_cast<const T2 *>(W + o);
-            const T2 wm = *reinterpret_cast<const T2 *>(W + o + dkm);
-            z.x = (u.x - um) * a.inv_dx + (v.x - vm.x) * inv_dyj + (w.x - wm.x) * inv_dzk;
-            z.y = (u.y - u.x) * a.inv_dx + (v.y - vm.y) * inv_dyj + (w.y - wm.y) * inv_dzk;
-        } else {
-            const T2 p = *reinterpret_cast<const T2 *>(src + (size_t)line * Nx + 2 * n);
-            z.x = p.x;
-            z.y = p.y;
+    constexpr int PER = (ITEMS + 255) / 256, UNR = sizeof(T) == 4 ? 4 : 2;   // items per thread; items loaded together
+    const int lim = nl * M;
+#pragma unroll 1
+    for (int b0 = 0; b0 < PER; b0 += UNR) {
+        // all loads of UNR items first (predicated, no early exit), then their arithmetic
+        T2 ru[UNR], rv[UNR], rvm[UNR], rw[UNR], rwm[UNR];
+        T rum[UNR], riy[UNR], riz[UNR];
+#pragma unroll
+        for (int q = 0; q < UNR; ++q) {
+            const int e = (b0 + q) * 256 + threadIdx.x;
+            if (b0 + q < PER && e < lim) {
+                const int ll = e / M, n = e - ll * M;
+                const int line = line0 + ll;
+                if (FROM_DIV) {
+                    const int k = (int)fdiv((unsigned)line, a.fNy), j = line - k * Ny;
+                    const int ob = k * plane + j * Nx, i = 2 * n, o = ob + i;
+                    const int dkm = (k == 0) ? (Nz - 1) * plane : -plane;
+                    const int djm = (j > 0) ? -Nx : (Ny - 1) * Nx;
+                    const bool vzero = (j == 0) && !d.yper;
+                    riy[q] = A::inv(a.my.dc, a.my.idc, j);
+                    riz[q] = A::inv(a.mz.dc, a.mz.idc, k);
+                    ru[q] = *reinterpret_cast<const T2 *>(U + o);
+                    rum[q] = __ldg(U + (i == 0 ? ob + Nx - 1 : o - 1));
+                    rv[q] = *reinterpret_cast<const T2 *>(V + o);
+                    if (vzero) { rvm[q].x = T(0); rvm[q].y = T(0); }
+                    else rvm[q] = *reinterpret_cast<const T2 *>(V + o + djm);
+                    rw[q] = *reinterpret_cast<const T2 *>(W + o);
+                    rwm[q] = *reinterpret_cast<const T2 *>(W + o + dkm);
+                } else {
+                    ru[q] = *reinterpret_cast<const T2 *>(src + (size_t)line * Nx + 2 * n);
+                }
+            }
         }
-        ba[ll * LDA + n] = z;
+#pragma unroll
+        for (int q = 0; q < UNR; ++q) {
+            const int e = (b0 + q) * 256 + threadIdx.x;
+            if (b0 + q < PER && e < lim) {
+                const int ll = e / M, n = e - ll * M;
+                C z;
+                if (FROM_DIV) {
+                    const T2 u = ru[q], v = rv[q], vm = rvm[q], w = rw[q], wm = rwm[q];
+                    z.x = (u.x - rum[q]) * a.inv_dx + (v.x - vm.x) * riy[q] + (w.x - wm.x) * riz[q];
+                    z.y = (u.y - u.x) * a.inv_dx + (v.y - vm.y) * riy[q] + (w.y - wm.y) * riz[q];
+                } else {
+                    z.x = ru[q].x;
+                    z.y = ru[q].y;
+                }
+                ba[ll * LDA + n] = z;
+            }
+        }
     }
     __syncthreads();
     for (int b = threadIdx.x; b < nl * N2; b += blockDim.x) {
