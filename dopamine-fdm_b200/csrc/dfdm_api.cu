@@ -84,6 +84,13 @@ struct dfdm_ctx {
     bool in_create = false;
     void *u = nullptr, *v = nullptr, *w = nullptr, *uo = nullptr, *vo = nullptr, *wo = nullptr;
     void *f1u = nullptr, *f1v = nullptr, *f1w = nullptr, *us = nullptr, *vs = nullptr, *wsf = nullptr;
+    // Fused corrections (DNS or filtered wall model, no hybrid scheme: the stage kernel is the only reader of the
+    // corrected velocity at stages 2 and 3): the stage-1 and stage-2 corrections run inside the next stage kernel's
+    // loader instead of k_correct, U keeps the step-start velocity until the stage-3 correction (so it also serves
+    // as uo), and u* alternates between us/vs/wsf and us2/vs2/ws2 so that a stage kernel reads the previous u*
+    // while it writes its own.
+    void *us2 = nullptr, *vs2 = nullptr, *ws2 = nullptr;
+    bool fuse_ok = false, fused = false;
     void *nut = nullptr, *p = nullptr, *phi = nullptr, *spec = nullptr, *rhs3 = nullptr;
     void *my_t = nullptr, *mz_t = nullptr;      // 6 metric arrays each, storage type
     double *my_d = nullptr, *mz_d = nullptr;    // same in double
@@ -255,6 +262,7 @@ template <typename T> StepArgs<T> step_args(dfdm_ctx *c) {
     a.ub = (const T *)c->d_ub;
     a.ubd = c->d_ubd;
     a.adv = (const T *)c->adv;
+    a.phi = (const T *)c->phi;
     return a;
 }
 
@@ -415,31 +423,42 @@ template <typename T> struct Impl {
         return sizeof(T) == 4 && s == 3 && c->projected && !c->unit_projection;
     }
 
-    template <bool LES, bool WM, bool HYB> static void stage_launch(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
+    // CORR: the input planes are the previous stage's u* (us2/vs2/ws2 after the swap in step_enqueue), corrected in
+    // the loader; with fused corrections the step-start velocity U doubles as uo
+    template <bool LES, bool WM, bool HYB, bool CORR> static void stage_launch(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
         const Dims &d = c->d;
+        const T *iu = CORR ? f(c->us2) : f(c->u), *iv = CORR ? f(c->vs2) : f(c->v), *iw = CORR ? f(c->ws2) : f(c->w);
+        T *uo = c->fused && !rhs_only ? f(c->u) : f(c->uo), *vo = c->fused && !rhs_only ? f(c->v) : f(c->vo);
+        T *wo = c->fused && !rhs_only ? f(c->w) : f(c->wo);
         if constexpr (sizeof(T) == 4) {
             if (c->stage_variant == 1) {
-                k_tiled2<LES, WM, 8, HYB><<<tile_grid(d, c->kc_stage2, TILE_X2), 256, 0, c->stream>>>(step_args<T>(c),
-                    f(c->u), f(c->v), f(c->w), LES ? f(c->nut) : nullptr, c->wsd.tau_x, c->wsd.tau_z, sc, c->kc_stage2,
-                    f(c->uo), f(c->vo), f(c->wo), f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf), rhs_only);
+                k_tiled2<LES, WM, 8, HYB, CORR><<<tile_grid(d, c->kc_stage2, TILE_X2), 256, 0, c->stream>>>(step_args<T>(c),
+                    iu, iv, iw, LES ? f(c->nut) : nullptr, c->wsd.tau_x, c->wsd.tau_z, sc, c->kc_stage2,
+                    uo, vo, wo, f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf), rhs_only);
                 return;
             }
         }
-        k_tiled<T, LES, WM, TILE_X, TILE_Y, HYB ? 2 : 0><<<tile_grid(d, c->kc_stage), TILE_X * TILE_Y, 0, c->stream>>>(
-            step_args<T>(c), f(c->u), f(c->v), f(c->w), LES ? f(c->nut) : nullptr, c->wsd.tau_x, c->wsd.tau_z, sc,
-            c->kc_stage, f(c->uo), f(c->vo), f(c->wo), f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf),
+        k_tiled<T, LES, WM, TILE_X, TILE_Y, HYB ? 2 : 0, CORR><<<tile_grid(d, c->kc_stage), TILE_X * TILE_Y, 0, c->stream>>>(
+            step_args<T>(c), iu, iv, iw, LES ? f(c->nut) : nullptr, c->wsd.tau_x, c->wsd.tau_z, sc,
+            c->kc_stage, uo, vo, wo, f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf),
             rhs_only, nullptr);
     }
     template <bool HYB> static void stage_dispatch(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
         if constexpr (sizeof(T) == 8) {   // FP64 keeps the runtime wall-model flag
-            if (c->les) stage_launch<true, true, HYB>(c, sc, rhs_only); else stage_launch<false, true, HYB>(c, sc, rhs_only);
+            if (c->les) stage_launch<true, true, HYB, false>(c, sc, rhs_only); else stage_launch<false, true, HYB, false>(c, sc, rhs_only);
         } else {
             if (c->les) {
-                if (c->wm) stage_launch<true, true, HYB>(c, sc, rhs_only); else stage_launch<true, false, HYB>(c, sc, rhs_only);
+                if (c->wm) stage_launch<true, true, HYB, false>(c, sc, rhs_only); else stage_launch<true, false, HYB, false>(c, sc, rhs_only);
             } else {
-                if (c->wm) stage_launch<false, true, HYB>(c, sc, rhs_only); else stage_launch<false, false, HYB>(c, sc, rhs_only);
+                if (c->wm) stage_launch<false, true, HYB, false>(c, sc, rhs_only); else stage_launch<false, false, HYB, false>(c, sc, rhs_only);
             }
         }
+    }
+    // stages 2 and 3 with the fused correction (no LES, no hybrid scheme: fuse_eligible)
+    static void stage_dispatch_corr(dfdm_ctx *c, const StageCoef &sc) {
+        if constexpr (sizeof(T) == 8) stage_launch<false, true, false, true>(c, sc, nullptr);
+        else if (c->wm) stage_launch<false, true, false, true>(c, sc, nullptr);
+        else stage_launch<false, false, false, true>(c, sc, nullptr);
     }
 
     static int stage_kernel(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
@@ -529,6 +548,12 @@ template <typename T> struct Impl {
             sc.c2 = (s == 2) ? 5.0 / 12.0 : 3.0 / 4.0;
             sc.incr = incr_form(c, s);
             sc.dtp = c->dev_dt() ? c->d_dtt : nullptr;
+            sc.no_uo = c->fused ? 1 : 0;
+            if (c->fused && s >= 2) {
+                stage_dispatch_corr(c, sc);
+                CKL();
+                return DFDM_OK;
+            }
             return stage_kernel(c, sc, nullptr);
         }
         case 2:   // div + forward x
@@ -592,17 +617,18 @@ template <typename T> struct Impl {
         }
         case 7: {   // correction (+ P at stage 3)
             bool inc = incr_form(c, s);
+            void *pu = c->fused ? c->u : c->uo, *pv = c->fused ? c->v : c->vo, *pw = c->fused ? c->w : c->wo;
             if (d.Nx % 4 == 0) {
                 dim3 g((d.Nx / 4 + 63) / 64, (d.Ny + 3) / 4, d.Nz);
                 k_correct4<T><<<g, dim3(64, 4, 1), 0, st>>>(poisson_args<T>(c), f(c->phi), f(c->us), f(c->vs), f(c->wsf),
                                                             f(c->u), f(c->v), f(c->w), s == 3 ? f(c->p) : nullptr,
-                                                            inc ? f(c->uo) : nullptr, inc ? f(c->vo) : nullptr,
-                                                            inc ? f(c->wo) : nullptr);
+                                                            inc ? f(pu) : nullptr, inc ? f(pv) : nullptr,
+                                                            inc ? f(pw) : nullptr);
             } else {
                 k_correct<T><<<cell_grid(d), CELL_BLOCK, 0, st>>>(poisson_args<T>(c), f(c->phi), f(c->us), f(c->vs), f(c->wsf),
                                                                   f(c->u), f(c->v), f(c->w), s == 3 ? f(c->p) : nullptr,
-                                                                  inc ? f(c->uo) : nullptr, inc ? f(c->vo) : nullptr,
-                                                                  inc ? f(c->wo) : nullptr);
+                                                                  inc ? f(pu) : nullptr, inc ? f(pv) : nullptr,
+                                                                  inc ? f(pw) : nullptr);
             }
             CKL();
             return DFDM_OK;
@@ -641,8 +667,10 @@ template <typename T> struct Impl {
 
     static int poisson_chain(dfdm_ctx *c, int s) {
         int rc;
-        for (int k = 2; k <= 7; ++k)
+        for (int k = 2; k <= 7; ++k) {
+            if (k == 7 && c->fused && s < 3 && !c->unit_projection) break;   // the next stage kernel applies it
             if ((rc = launch(c, k, s))) return rc;
+        }
         return DFDM_OK;
     }
 
@@ -710,6 +738,9 @@ template <typename T> struct Impl {
             if (s == 1 && c->dev_dt() && (rc = select_dt(c))) return rc;   // dt from the start-of-step CFL, after nu_t
             if ((rc = launch(c, 8, s))) return rc;   // wall model
             if ((rc = launch(c, 11, s))) return rc;  // hybrid-scheme dissipation (advection_scheme = 2)
+            if (c->fused && s >= 2) {   // the previous u* becomes this stage kernel's input; it writes the other set
+                std::swap(c->us, c->us2); std::swap(c->vs, c->vs2); std::swap(c->wsf, c->ws2);
+            }
             if ((rc = launch(c, 1, s))) return rc;   // RHS + RK update
             if ((rc = poisson_chain(c, s))) return rc;
         }
@@ -794,13 +825,20 @@ int validate(const dfdm_grid *g, const dfdm_params *p) {
     return DFDM_OK;
 }
 
+// The fused-correction step applies (see dfdm_ctx::fused): no SGS model, the wall model only with its temporal
+// filter (automatic with periodic z), and not the hybrid advection scheme.
+bool fuse_eligible(const dfdm_params *p) {
+    return p->sgs_model == 0 && (p->flat_wall_model_flag == 0 || p->wm_filter_mode != 0) && p->advection_scheme != 2;
+}
+
 // Bytes of the buffers dfdm_create carves from the context's arena (every sub-allocation 256-byte aligned).
 size_t arena_bytes(const dfdm_grid *g, const dfdm_params *p) {
     size_t ts = p->precision == DFDM_FP64 ? 8 : 4;
     size_t Nx = g->nx - 2, Nz = g->nz - 2, Ny = g->y_bc_type == 0 ? g->ny - 2 : g->ny - 1;
     size_t cells = Nx * Ny * Nz, spec = (Nx / 2 + 1) * Ny * Nz;
     size_t n = cells * ts * (3 /*u*/ + 3 /*uo*/ + 3 /*F1*/ + 3 /*u**/ + 1 /*P*/ + 1 /*phi*/ + (p->sgs_model ? 1 : 0) +
-                             (p->advection_scheme == 2 ? 3 /*hybrid-scheme terms*/ : 0));
+                             (p->advection_scheme == 2 ? 3 /*hybrid-scheme terms*/ : 0) +
+                             (fuse_eligible(p) ? 3 /*second u* set*/ : 0));
     n += spec * 2 * ts;
     if (g->y_bc_type != 0) n += (Nx / 2 + 1) * Ny * Nz * 8;   // pivot table of the y solves
     n += 8 * Nx * Nz * 2 * 8;   // wall planes
@@ -923,6 +961,12 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
                        &c->us, &c->vs, &c->wsf, &c->p, &c->phi};
     for (void **fp : fields)
         if ((rc = dalloc(c, fp, F))) return bail(rc);
+    if (fuse_eligible(prm)) {
+        void **alt[] = {&c->us2, &c->vs2, &c->ws2};
+        for (void **fp : alt)
+            if ((rc = dalloc(c, fp, F))) return bail(rc);
+        c->fuse_ok = c->fused = true;
+    }
     if ((rc = dalloc(c, &c->nut, c->les ? F : c->ts))) return bail(rc);
     if ((rc = dalloc(c, &c->spec, (size_t)d.Nxc * d.Ny * d.Nz * 2 * c->ts))) return bail(rc);
 
@@ -1812,6 +1856,24 @@ int dfdm_launch_kernel_async(dfdm_ctx *c, int which, int rk_stage) {
     return rc;
 }
 
+int dfdm_set_fused_correction(dfdm_ctx *c, int enable) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (enable && !c->fuse_ok)
+        return fail(DFDM_ERR_UNSUPPORTED, "fused corrections need a DNS or filtered-wall-model case without the hybrid scheme");
+    CK(cudaStreamSynchronize(c->stream));
+    destroy_graph(c);   // the captured step holds the other launch sequence
+    c->fused = enable != 0;
+    return DFDM_OK;
+}
+
+int dfdm_get_fused_correction(dfdm_ctx *c, int *enabled) {
+    if (int rc = check_ctx(c)) return rc;
+    if (!enabled) return fail(DFDM_ERR_INVALID, "null output");
+    *enabled = c->fused ? 1 : 0;
+    return DFDM_OK;
+}
+
 int dfdm_set_stage_variant(dfdm_ctx *c, int variant) {
     g_err.clear();
     if (int rc = check_ctx(c)) return rc;
@@ -1847,7 +1909,8 @@ int dfdm_kernel_bytes(dfdm_ctx *c, int which, double *bytes) {
     double b = 0.0;
     switch (which) {
     case 0: b = c->les ? 4.0 * cell : 0.0; break;                 // read U,V,W; write nu_t
-    case 1: b = 12.0 * cell + (c->les ? cell : 0.0); break;       // stage 1: 3 in, 9 out; stages 2/3: 9 in, 3 out
+    case 1: b = 12.0 * cell + (c->les ? cell : 0.0) + (c->fused ? cell : 0.0); break;   // stage 1: 3 in, 9 out; stages 2/3:
+                                                                  // 9 in, 3 out (fused corrections: + phi)
     case 2: b = 3.0 * cell + spec; break;                         // read u*, write spectrum
     case 3: case 4: case 5: b = 2.0 * spec; break;                // read + write spectrum
     case 6: b = spec + cell; break;                               // read spectrum, write phi

@@ -26,6 +26,9 @@ template <typename T> struct StepArgs {
     // advection_scheme = 2: the dissipative terms of k_adv_hybrid (u, v, w blocks of `cells`), added to the
     // right-hand sides; null otherwise
     const T *adv;
+    // fused correction of the previous stage (CORR kernels): its potential phi; the plane loads then hold u* and
+    // the loader forms u = u* - grad(phi) exactly as k_correct does
+    const T *phi;
 };
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -444,6 +447,7 @@ struct StageCoef {
     double c1, c2;   // rk_coef(s,1) and rk_coef(s,s), stages 2 and 3
     int incr;        // store the increment du = dt (c1 F1 + c2 rhs) instead of u* = uo + du; uo is not read
     const double *dtp = nullptr;   // adaptive time step: dt is dtp[0] (device memory) and dt_a11, dt are not used
+    int no_uo = 0;                 // stage 1: the step-start velocity stays in U (fused corrections), uo is not written
 };
 
 // Shared-memory neighbourhood of one thread: three z-planes (k-1, k, k+1) of each field, each plane a
@@ -490,7 +494,12 @@ template <int PX> struct TileQ2 {
 // sides themselves for the unit entry point; with KIND 1, nu_t).
 // WM = false compiles the flat-wall model out; with WM = true the runtime flag StepArgs::wm decides (the FP64 form
 // always takes that variant: without the branches its register allocation spills).
-template <typename T, bool LES, bool WM, int TX, int TY, int KIND>
+// CORR (stages 2 and 3 of a step whose stage kernel is the only reader of the corrected velocity): U, V, W are the
+// previous stage's u*, and the loader applies that stage's projection, u = u* - grad(phi) with StepArgs::phi, to
+// every plane element it copies, before the wall rules -- the arithmetic of k_correct, so the values are the ones
+// k_correct would have stored.  phi planes k-1 .. k+3 rotate through four more shared planes, one plane ahead of
+// the velocity planes (a plane's w correction needs phi of the plane above).
+template <typename T, bool LES, bool WM, int TX, int TY, int KIND, bool CORR = false>
 __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepArgs<T> a, const T *__restrict__ U, const T *__restrict__ V,
                                                   const T *__restrict__ W, const T *__restrict__ NU,
                                                   const double *__restrict__ tau_x, const double *__restrict__ tau_z,
@@ -502,6 +511,8 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
     constexpr int NF = LES ? 4 : 3;
     constexpr int PER = (PS + NT - 1) / NT;   // plane elements per thread
     __shared__ __align__(16) T sm[NF][4][PS];
+    constexpr int PXP = PX + 1, PSP = PXP * (PY + 1), PERP = (PSP + NT - 1) / NT;   // phi tile: one more column, row
+    __shared__ __align__(16) T smp[CORR ? 4 : 1][CORR ? PSP : 1];
     const Dims &d = a.d;
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
     const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
@@ -514,6 +525,8 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
     // This thread's share of a plane: offsets within the plane (or -1), the wall rule and the base profile.
     int off[PER];
     bool ghost[PER];   // wall ghost row: mirror U/W, zero V/nu_t
+    int pix[CORR ? PER : 1];    // CORR: phi-tile index of the element
+    T iyq[CORR ? PER : 1];      // CORR: 1/(centre spacing) of its row for the v correction, 0 where v is not corrected
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
         int e = threadIdx.x + q * NT;
@@ -532,8 +545,38 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
                 ghost[q] = (gj < 0 || gj >= Ny);
             }
             off[q] = g * Nx + gi;
+            if constexpr (CORR) {
+                pix[q] = jj * PXP + ii;
+                iyq[q] = (ghost[q] || g >= d.NyV) ? T(0) : Arith<T>::inv(a.my.df, a.my.idf, g);
+            }
         }
     }
+    int offp[CORR ? PERP : 1];   // CORR: this thread's share of a phi plane (same row and column rules)
+    if constexpr (CORR) {
+#pragma unroll
+        for (int q = 0; q < PERP; ++q) {
+            int e = threadIdx.x + q * NT;
+            offp[q] = -1;
+            if (e < PSP) {
+                int jj = e / PXP, ii = e - jj * PXP;
+                int gi = i0 - 1 + ii;
+                gi = gi < 0 ? gi + Nx : gi;
+                while (gi >= Nx) gi -= Nx;
+                int gj = j0 - 1 + jj, g;
+                if (d.yper) { g = gj < 0 ? gj + Ny : gj; while (g >= Ny) g -= Ny; }
+                else g = gj < 0 ? 0 : (gj >= Ny ? Ny - 1 : gj);
+                offp[q] = g * Nx + gi;
+            }
+        }
+    }
+    auto issue_phi = [&](int k) {   // phi plane k into phi slot (k - k0 + 1) & 3
+        if constexpr (CORR) {
+            const int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k), slot = (k - k0 + 1) & 3;
+#pragma unroll
+            for (int q = 0; q < PERP; ++q)
+                if (offp[q] >= 0) cp_async<sizeof(T)>(&smp[slot][threadIdx.x + q * NT], a.phi + kw * plane + offp[q]);
+        }
+    };
     auto issue = [&](int slot, int k) {
         int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k);
         const int kb = kw * plane;
@@ -549,9 +592,23 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
             }
         }
     };
-    auto fix = [&](int slot) {   // after this thread's copies have landed: wall ghost rows
+    auto fix = [&](int slot, int k) {   // after the copies of plane k (and, CORR, phi k and k+1) have landed
+        if constexpr (CORR) {   // project_velocity of the previous stage (k_correct's arithmetic)
+            const int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k);
+            const int p0 = (k - k0 + 1) & 3, p1 = (k - k0 + 2) & 3;
+            const T iz = Arith<T>::inv(a.mz.df, a.mz.idf, kw);
 #pragma unroll
-        for (int q = 0; q < PER; ++q) {
+            for (int q = 0; q < PER; ++q) {
+                if (off[q] < 0) continue;
+                const int e = threadIdx.x + q * NT;
+                const T pc = smp[p0][pix[q]], pxp = smp[p0][pix[q] + 1], pzp = smp[p1][pix[q]];
+                sm[0][slot][e] = sm[0][slot][e] - (pxp - pc) * a.inv_dx;
+                sm[2][slot][e] = sm[2][slot][e] - (pzp - pc) * iz;
+                if (iyq[q] != T(0)) sm[1][slot][e] = sm[1][slot][e] - (smp[p0][pix[q] + PXP] - pc) * iyq[q];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {   // wall ghost rows
             if (off[q] < 0 || !ghost[q]) continue;
             const int e = threadIdx.x + q * NT;
             sm[0][slot][e] = -sm[0][slot][e];   // deviation mirrored; the row profile is mirrored in TileQ::ub
@@ -574,17 +631,19 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
     AxisLocal<T> Y;   // this thread's y metrics (FP32: read here once for every plane)
     Y.load(a.my, min(j, Ny - 1));
 
-    // planes k0-1, k0, k0+1 into slots 0, 1, 2; plane k lives in slot (k - k0 + 1) & 3
+    // planes k0-1, k0, k0+1 into slots 0, 1, 2; plane k lives in slot (k - k0 + 1) & 3 (CORR: phi k0-1 .. k0+2)
     issue(0, k0 - 1); issue(1, k0); issue(2, k0 + 1);
+    issue_phi(k0 - 1); issue_phi(k0); issue_phi(k0 + 1); issue_phi(k0 + 2);
     cp_async_commit();
     cp_async_wait_all();
-    fix(0); fix(1); fix(2);
+    if (CORR) __syncthreads();   // phi elements copied by other threads
+    fix(0, k0 - 1); fix(1, k0); fix(2, k0 + 1);
     __syncthreads();
     const int cloc = (ty + 1) * PX + tx + 1;
     for (int k = k0; k < kend; ++k) {
         const bool more = k + 2 <= kend;
         const int snext = (k - k0 + 3) & 3;
-        if (more) issue(snext, k + 2);
+        if (more) { issue(snext, k + 2); issue_phi(k + 3); }
         cp_async_commit();
         const int sm_ = (k - k0) & 3, s0 = (k - k0 + 1) & 3, sp = (k - k0 + 2) & 3;
         if (active) {
@@ -621,9 +680,14 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
                 } else if (sc.stage == 1) {
                     T c = (T)(sc.dtp ? *sc.dtp * (8.0 / 15.0) : sc.dt_a11);
                     T u0 = q.Ud(0, 0, 0), w0 = q.W(0, 0, 0);   // U as stored (deviation from the base profile)
-                    uo[p] = u0; f1u[p] = ru; us[p] = u0 + c * ru;
-                    wo[p] = w0; f1w[p] = rw; wsf[p] = w0 + c * rw;
-                    if (vrow) { T v0 = q.V(0, 0, 0); vo[p] = v0; f1v[p] = rv; vs[p] = v0 + c * rv; }
+                    f1u[p] = ru; us[p] = u0 + c * ru;
+                    f1w[p] = rw; wsf[p] = w0 + c * rw;
+                    if (!sc.no_uo) { uo[p] = u0; wo[p] = w0; }
+                    if (vrow) {
+                        T v0 = q.V(0, 0, 0);
+                        f1v[p] = rv; vs[p] = v0 + c * rv;
+                        if (!sc.no_uo) vo[p] = v0;
+                    }
                 } else {
                     T c1 = (T)sc.c1, c2 = (T)sc.c2, dtt = (T)(sc.dtp ? *sc.dtp : sc.dt);   // with sc.incr the base stays zero: du
                     us[p] = ou + dtt * (c1 * fu + c2 * ru);
@@ -633,7 +697,8 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
             }
         }
         cp_async_wait_all();
-        if (more) fix(snext);
+        if (CORR) __syncthreads();   // phi k+3 copied by other threads before any thread corrects plane k+2
+        if (more) fix(snext, k + 2);
         __syncthreads();
     }
 }
@@ -641,9 +706,10 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
 
 // FP32 stage kernel with two x-neighbour cells per thread, computed with the packed FP32x2 instructions (F2).  Same
 // loader, ghost rules and RK3 epilogue as k_tiled<float, LES, WM, ..., 0>; a block owns 64 x TY cells, one warp
-// per row of 32 cell pairs; HYB adds the dissipative terms of advection_scheme = 2 (StepArgs::adv).  It needs ~118 registers: capping it at 96 or 80 (for more resident warps) spills
+// per row of 32 cell pairs; HYB adds the dissipative terms of advection_scheme = 2 (StepArgs::adv); CORR fuses
+// the previous stage's correction into the loader as k_tiled does.  It needs ~118 registers: capping it at 96 or 80 (for more resident warps) spills
 // 170-300 bytes, so it runs 2 blocks of 256 threads per SM.  Shared rows hold cells i0-2 .. i0+65 (pitch 68), so every pair starts at an even index.
-template <bool LES, bool WM, int TY = 8, bool HYB = false>
+template <bool LES, bool WM, int TY = 8, bool HYB = false, bool CORR = false>
 __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<float> a, const float *__restrict__ U, const float *__restrict__ V,
                                                    const float *__restrict__ W, const float *__restrict__ NU,
                                                    const double *__restrict__ tau_x, const double *__restrict__ tau_z,
@@ -656,6 +722,8 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
     constexpr int NF = LES ? 4 : 3;
     constexpr int PER = (PS + NT - 1) / NT;
     __shared__ __align__(16) float sm[NF][4][PS];
+    constexpr int PXP = PX + 1, PSP = PXP * (PY + 1), PERP = (PSP + NT - 1) / NT;   // phi tile: one more column, row
+    __shared__ __align__(16) float smp[CORR ? 4 : 1][CORR ? PSP : 1];
     const Dims &d = a.d;
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
     const int i0 = blockIdx.x * TXC, j0 = blockIdx.y * TY;
@@ -667,6 +735,8 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
 
     int off[PER];
     bool ghost[PER];
+    int pix[CORR ? PER : 1];      // CORR: phi-tile index of the element
+    float iyq[CORR ? PER : 1];    // CORR: 1/(centre spacing) of its row for the v correction, 0 where v is not corrected
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
         int e = threadIdx.x + q * NT;
@@ -685,8 +755,38 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
                 ghost[q] = (gj < 0 || gj >= Ny);
             }
             off[q] = g * Nx + gi;
+            if constexpr (CORR) {
+                pix[q] = jj * PXP + ii;
+                iyq[q] = (ghost[q] || g >= d.NyV) ? 0.0f : Arith<float>::inv(a.my.df, a.my.idf, g);
+            }
         }
     }
+    int offp[CORR ? PERP : 1];   // CORR: this thread's share of a phi plane (same row and column rules)
+    if constexpr (CORR) {
+#pragma unroll
+        for (int q = 0; q < PERP; ++q) {
+            int e = threadIdx.x + q * NT;
+            offp[q] = -1;
+            if (e < PSP) {
+                int jj = e / PXP, ii = e - jj * PXP;
+                int gi = i0 - 2 + ii;
+                gi = gi < 0 ? gi + Nx : gi;
+                while (gi >= Nx) gi -= Nx;
+                int gj = j0 - 1 + jj, g;
+                if (d.yper) { g = gj < 0 ? gj + Ny : gj; while (g >= Ny) g -= Ny; }
+                else g = gj < 0 ? 0 : (gj >= Ny ? Ny - 1 : gj);
+                offp[q] = g * Nx + gi;
+            }
+        }
+    }
+    auto issue_phi = [&](int k) {   // phi plane k into phi slot (k - k0 + 1) & 3
+        if constexpr (CORR) {
+            const int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k), slot = (k - k0 + 1) & 3;
+#pragma unroll
+            for (int q = 0; q < PERP; ++q)
+                if (offp[q] >= 0) cp_async<4>(&smp[slot][threadIdx.x + q * NT], a.phi + kw * plane + offp[q]);
+        }
+    };
     auto issue = [&](int slot, int k) {
         int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k);
         const int kb = kw * plane;
@@ -702,7 +802,21 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
             }
         }
     };
-    auto fix = [&](int slot) {
+    auto fix = [&](int slot, int k) {
+        if constexpr (CORR) {   // project_velocity of the previous stage (k_correct's arithmetic)
+            const int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k);
+            const int p0 = (k - k0 + 1) & 3, p1 = (k - k0 + 2) & 3;
+            const float iz = Arith<float>::inv(a.mz.df, a.mz.idf, kw);
+#pragma unroll
+            for (int q = 0; q < PER; ++q) {
+                if (off[q] < 0) continue;
+                const int e = threadIdx.x + q * NT;
+                const float pc = smp[p0][pix[q]], pxp = smp[p0][pix[q] + 1], pzp = smp[p1][pix[q]];
+                sm[0][slot][e] = sm[0][slot][e] - (pxp - pc) * a.inv_dx;
+                sm[2][slot][e] = sm[2][slot][e] - (pzp - pc) * iz;
+                if (iyq[q] != 0.0f) sm[1][slot][e] = sm[1][slot][e] - (smp[p0][pix[q] + PXP] - pc) * iyq[q];
+            }
+        }
 #pragma unroll
         for (int q = 0; q < PER; ++q) {
             if (off[q] < 0 || !ghost[q]) continue;
@@ -726,15 +840,17 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
     Y.load(a.my, min(j, Ny - 1));
 
     issue(0, k0 - 1); issue(1, k0); issue(2, k0 + 1);
+    issue_phi(k0 - 1); issue_phi(k0); issue_phi(k0 + 1); issue_phi(k0 + 2);
     cp_async_commit();
     cp_async_wait_all();
-    fix(0); fix(1); fix(2);
+    if (CORR) __syncthreads();   // phi elements copied by other threads
+    fix(0, k0 - 1); fix(1, k0); fix(2, k0 + 1);
     __syncthreads();
     const int cloc = (ty + 1) * PX + 2 + 2 * tx;
     for (int k = k0; k < kend; ++k) {
         const bool more = k + 2 <= kend;
         const int snext = (k - k0 + 3) & 3;
-        if (more) issue(snext, k + 2);
+        if (more) { issue(snext, k + 2); issue_phi(k + 3); }
         cp_async_commit();
         const int sm_ = (k - k0) & 3, s0 = (k - k0 + 1) & 3, sp = (k - k0 + 2) & 3;
         if (active) {
@@ -770,9 +886,14 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
             } else if (sc.stage == 1) {
                 const F2 c = F2(sc.dtp ? *sc.dtp * (8.0 / 15.0) : sc.dt_a11);
                 F2 u0 = q.Ud(0, 0, 0), w0 = q.W(0, 0, 0);
-                st2(uo, u0); st2(f1u, ru); st2(us, u0 + c * ru);
-                st2(wo, w0); st2(f1w, rw); st2(wsf, w0 + c * rw);
-                if (vrow) { F2 v0 = q.V(0, 0, 0); st2(vo, v0); st2(f1v, rv); st2(vs, v0 + c * rv); }
+                st2(f1u, ru); st2(us, u0 + c * ru);
+                st2(f1w, rw); st2(wsf, w0 + c * rw);
+                if (!sc.no_uo) { st2(uo, u0); st2(wo, w0); }
+                if (vrow) {
+                    F2 v0 = q.V(0, 0, 0);
+                    st2(f1v, rv); st2(vs, v0 + c * rv);
+                    if (!sc.no_uo) st2(vo, v0);
+                }
             } else {
                 const F2 c1 = F2(sc.c1), c2 = F2(sc.c2), dtt = F2(sc.dtp ? *sc.dtp : sc.dt);
                 st2(us, ou + dtt * (c1 * fu + c2 * ru));
@@ -781,7 +902,8 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
             }
         }
         cp_async_wait_all();
-        if (more) fix(snext);
+        if (CORR) __syncthreads();   // phi k+3 copied by other threads before any thread corrects plane k+2
+        if (more) fix(snext, k + 2);
         __syncthreads();
     }
 }

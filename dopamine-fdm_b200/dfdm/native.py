@@ -32,7 +32,8 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_check_finite", "dfdm_pad_field", "dfdm_launch_kernel_async", "dfdm_kernel_bytes",
            "dfdm_launch_count", "dfdm_solve_poisson_noalloc", "dfdm_write_snapshot", "dfdm_read_snapshot",
            "dfdm_compute_cfl", "dfdm_set_stage_variant", "dfdm_get_stage_variant", "dfdm_set_adaptive_dt",
-           "dfdm_get_dt", "dfdm_set_landing_time", "dfdm_output_monitor", "dfdm_output_monitor_async"]
+           "dfdm_get_dt", "dfdm_set_landing_time", "dfdm_output_monitor", "dfdm_output_monitor_async",
+           "dfdm_set_fused_correction", "dfdm_get_fused_correction"]
 
 
 class DfdmError(RuntimeError):
@@ -100,6 +101,8 @@ def load(build_if_missing: bool = True):
         "dfdm_set_landing_time": (c_int, [c_void_p, c_int, c_double]),
         "dfdm_output_monitor": (c_int, [c_void_p, P]),
         "dfdm_output_monitor_async": (c_int, [c_void_p, c_void_p]),
+        "dfdm_set_fused_correction": (c_int, [c_void_p, c_int]),
+        "dfdm_get_fused_correction": (c_int, [c_void_p, POINTER(ctypes.c_int)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -268,6 +271,16 @@ class Solver:
         v = c_double(0.0)
         _check(load().dfdm_check_divergence(self.h, ctypes.byref(v)))
         return v.value
+
+    def set_fused_correction(self, enable: bool = True):
+        """Stage-1/2 projections inside the next stage kernel (on by default where it applies)."""
+        _check(load().dfdm_set_fused_correction(self.h, int(enable)))
+
+    @property
+    def fused_correction(self) -> bool:
+        v = ctypes.c_int(0)
+        _check(load().dfdm_get_fused_correction(self.h, ctypes.byref(v)))
+        return bool(v.value)
 
     def set_stage_variant(self, variant: int) -> None:
         """FP32 stage kernel: 0 one cell per thread, 1 packed pairs, -1 re-time both and keep the faster."""

@@ -231,6 +231,13 @@ int dfdm_pad_field(dfdm_ctx *ctx, int field, int extra_planes, double *out);
  *        5 inverse z-FFT, 6 inverse x-FFT, 7 velocity correction, 8 wall model, 9 constant-flux bulk sum + shift,
  *        10 CFL maxima, 11 the dissipative terms of advection_scheme = 2 */
 int dfdm_launch_kernel_async(dfdm_ctx *ctx, int which, int rk_stage);
+/* Fused corrections (on by default where they apply: no SGS model, the wall model only with its temporal filter, no
+ * hybrid advection scheme).  The projections of RK stages 1 and 2 then run inside the next stage kernel's loader
+ * instead of as separate launches, and the step-start velocity stays in place as the RK base state: two launches and
+ * 17 words per cell fewer per step, the same arithmetic.  No counterpart in the reference; enable = 0 restores the
+ * separate corrections (DFDM_ERR_UNSUPPORTED for enable = 1 where they do not apply). */
+int dfdm_set_fused_correction(dfdm_ctx *ctx, int enable);
+int dfdm_get_fused_correction(dfdm_ctx *ctx, int *enabled);
 /* Algorithmic HBM bytes one launch of that kernel family moves (the roofline numerator). */
 int dfdm_kernel_bytes(dfdm_ctx *ctx, int which, double *bytes);
 /* Number of the library's own kernels enqueued by this context so far (graph replays included). */
