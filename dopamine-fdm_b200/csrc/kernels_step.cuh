@@ -497,8 +497,9 @@ template <int PX> struct TileQ2 {
 // CORR (stages 2 and 3 of a step whose stage kernel is the only reader of the corrected velocity): U, V, W are the
 // previous stage's u*, and the loader applies that stage's projection, u = u* - grad(phi) with StepArgs::phi, to
 // every plane element it copies, before the wall rules -- the arithmetic of k_correct, so the values are the ones
-// k_correct would have stored.  phi planes k-1 .. k+3 rotate through four more shared planes, one plane ahead of
-// the velocity planes (a plane's w correction needs phi of the plane above).
+// k_correct would have stored.  phi planes rotate through five more shared planes and are copied two planes ahead
+// of the velocity planes (a plane's w correction needs phi of the plane above), so they have landed, and passed a
+// barrier, before the plane that needs them is corrected.
 template <typename T, bool LES, bool WM, int TX, int TY, int KIND, bool CORR = false>
 __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepArgs<T> a, const T *__restrict__ U, const T *__restrict__ V,
                                                   const T *__restrict__ W, const T *__restrict__ NU,
@@ -512,7 +513,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
     constexpr int PER = (PS + NT - 1) / NT;   // plane elements per thread
     __shared__ __align__(16) T sm[NF][4][PS];
     constexpr int PXP = PX + 1, PSP = PXP * (PY + 1), PERP = (PSP + NT - 1) / NT;   // phi tile: one more column, row
-    __shared__ __align__(16) T smp[CORR ? 4 : 1][CORR ? PSP : 1];
+    __shared__ __align__(16) T smp[CORR ? 5 : 1][CORR ? PSP : 1];
     const Dims &d = a.d;
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
     const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
@@ -569,9 +570,9 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
             }
         }
     }
-    auto issue_phi = [&](int k) {   // phi plane k into phi slot (k - k0 + 1) & 3
+    auto issue_phi = [&](int k) {   // phi plane k into phi slot (k - k0 + 1) % 5
         if constexpr (CORR) {
-            const int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k), slot = (k - k0 + 1) & 3;
+            const int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k), slot = (k - k0 + 1) % 5;
 #pragma unroll
             for (int q = 0; q < PERP; ++q)
                 if (offp[q] >= 0) cp_async<sizeof(T)>(&smp[slot][threadIdx.x + q * NT], a.phi + kw * plane + offp[q]);
@@ -595,7 +596,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
     auto fix = [&](int slot, int k) {   // after the copies of plane k (and, CORR, phi k and k+1) have landed
         if constexpr (CORR) {   // project_velocity of the previous stage (k_correct's arithmetic)
             const int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k);
-            const int p0 = (k - k0 + 1) & 3, p1 = (k - k0 + 2) & 3;
+            const int p0 = (k - k0 + 1) % 5, p1 = (k - k0 + 2) % 5;
             const T iz = Arith<T>::inv(a.mz.df, a.mz.idf, kw);
 #pragma unroll
             for (int q = 0; q < PER; ++q) {
@@ -633,7 +634,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
 
     // planes k0-1, k0, k0+1 into slots 0, 1, 2; plane k lives in slot (k - k0 + 1) & 3 (CORR: phi k0-1 .. k0+2)
     issue(0, k0 - 1); issue(1, k0); issue(2, k0 + 1);
-    issue_phi(k0 - 1); issue_phi(k0); issue_phi(k0 + 1); issue_phi(k0 + 2);
+    issue_phi(k0 - 1); issue_phi(k0); issue_phi(k0 + 1); issue_phi(k0 + 2); issue_phi(k0 + 3);
     cp_async_commit();
     cp_async_wait_all();
     if (CORR) __syncthreads();   // phi elements copied by other threads
@@ -643,7 +644,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
     for (int k = k0; k < kend; ++k) {
         const bool more = k + 2 <= kend;
         const int snext = (k - k0 + 3) & 3;
-        if (more) { issue(snext, k + 2); issue_phi(k + 3); }
+        if (more) { issue(snext, k + 2); issue_phi(k + 4); }
         cp_async_commit();
         const int sm_ = (k - k0) & 3, s0 = (k - k0 + 1) & 3, sp = (k - k0 + 2) & 3;
         if (active) {
@@ -697,8 +698,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
             }
         }
         cp_async_wait_all();
-        if (CORR) __syncthreads();   // phi k+3 copied by other threads before any thread corrects plane k+2
-        if (more) fix(snext, k + 2);
+        if (more) fix(snext, k + 2);   // CORR: phi k+2 and k+3 were copied one and two iterations ago
         __syncthreads();
     }
 }
@@ -723,7 +723,7 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
     constexpr int PER = (PS + NT - 1) / NT;
     __shared__ __align__(16) float sm[NF][4][PS];
     constexpr int PXP = PX + 1, PSP = PXP * (PY + 1), PERP = (PSP + NT - 1) / NT;   // phi tile: one more column, row
-    __shared__ __align__(16) float smp[CORR ? 4 : 1][CORR ? PSP : 1];
+    __shared__ __align__(16) float smp[CORR ? 5 : 1][CORR ? PSP : 1];
     const Dims &d = a.d;
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
     const int i0 = blockIdx.x * TXC, j0 = blockIdx.y * TY;
@@ -779,9 +779,9 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
             }
         }
     }
-    auto issue_phi = [&](int k) {   // phi plane k into phi slot (k - k0 + 1) & 3
+    auto issue_phi = [&](int k) {   // phi plane k into phi slot (k - k0 + 1) % 5
         if constexpr (CORR) {
-            const int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k), slot = (k - k0 + 1) & 3;
+            const int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k), slot = (k - k0 + 1) % 5;
 #pragma unroll
             for (int q = 0; q < PERP; ++q)
                 if (offp[q] >= 0) cp_async<4>(&smp[slot][threadIdx.x + q * NT], a.phi + kw * plane + offp[q]);
@@ -805,7 +805,7 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
     auto fix = [&](int slot, int k) {
         if constexpr (CORR) {   // project_velocity of the previous stage (k_correct's arithmetic)
             const int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k);
-            const int p0 = (k - k0 + 1) & 3, p1 = (k - k0 + 2) & 3;
+            const int p0 = (k - k0 + 1) % 5, p1 = (k - k0 + 2) % 5;
             const float iz = Arith<float>::inv(a.mz.df, a.mz.idf, kw);
 #pragma unroll
             for (int q = 0; q < PER; ++q) {
@@ -840,7 +840,7 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
     Y.load(a.my, min(j, Ny - 1));
 
     issue(0, k0 - 1); issue(1, k0); issue(2, k0 + 1);
-    issue_phi(k0 - 1); issue_phi(k0); issue_phi(k0 + 1); issue_phi(k0 + 2);
+    issue_phi(k0 - 1); issue_phi(k0); issue_phi(k0 + 1); issue_phi(k0 + 2); issue_phi(k0 + 3);
     cp_async_commit();
     cp_async_wait_all();
     if (CORR) __syncthreads();   // phi elements copied by other threads
@@ -850,7 +850,7 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
     for (int k = k0; k < kend; ++k) {
         const bool more = k + 2 <= kend;
         const int snext = (k - k0 + 3) & 3;
-        if (more) { issue(snext, k + 2); issue_phi(k + 3); }
+        if (more) { issue(snext, k + 2); issue_phi(k + 4); }
         cp_async_commit();
         const int sm_ = (k - k0) & 3, s0 = (k - k0 + 1) & 3, sp = (k - k0 + 2) & 3;
         if (active) {
@@ -902,8 +902,7 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
             }
         }
         cp_async_wait_all();
-        if (CORR) __syncthreads();   // phi k+3 copied by other threads before any thread corrects plane k+2
-        if (more) fix(snext, k + 2);
+        if (more) fix(snext, k + 2);   // CORR: phi k+2 and k+3 were copied one and two iterations ago
         __syncthreads();
     }
 }
