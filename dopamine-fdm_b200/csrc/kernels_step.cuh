@@ -720,10 +720,12 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
     constexpr int TXC = 64, NT = 32 * TY;
     constexpr int PX = TXC + 4, PY = TY + 2, PS = PX * PY;
     constexpr int NF = LES ? 4 : 3;
-    constexpr int PER = (PS + NT - 1) / NT;
+    // the loader moves element pairs (columns 2m, 2m+1 of a tile row: even global x, so one 8-byte copy)
+    constexpr int PS2 = PS / 2, PER = (PS2 + NT - 1) / NT;
     __shared__ __align__(16) float sm[NF][4][PS];
-    constexpr int PXP = PX + 1, PSP = PXP * (PY + 1), PERP = (PSP + NT - 1) / NT;   // phi tile: one more column, row
-    __shared__ __align__(16) float smp[CORR ? 5 : 1][CORR ? PSP : 1];
+    // CORR phi tile: two more columns (an even pitch keeps pairs aligned) and one more row
+    constexpr int PXP = PX + 2, PSP2 = PXP * (PY + 1) / 2, PERP = (PSP2 + NT - 1) / NT;
+    __shared__ __align__(16) float smp[CORR ? 5 : 1][CORR ? 2 * PSP2 : 2];
     const Dims &d = a.d;
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
     const int i0 = blockIdx.x * TXC, j0 = blockIdx.y * TY;
@@ -733,16 +735,16 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
     const bool active = i < Nx && j < Ny;   // Nx is even: the pair's second cell is in range too
     const int plane = Nx * Ny;
 
-    int off[PER];
+    int off[PER];       // global offset of the pair's first element within a plane, or -1
     bool ghost[PER];
-    int pix[CORR ? PER : 1];      // CORR: phi-tile index of the element
+    int pix[CORR ? PER : 1];      // CORR: phi-tile index of the pair
     float iyq[CORR ? PER : 1];    // CORR: 1/(centre spacing) of its row for the v correction, 0 where v is not corrected
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
-        int e = threadIdx.x + q * NT;
+        int e2 = threadIdx.x + q * NT;
         off[q] = -1; ghost[q] = false;
-        if (e < PS) {
-            int jj = e / PX, ii = e - jj * PX;
+        if (e2 < PS2) {
+            int jj = e2 / (PX / 2), ii = 2 * (e2 - jj * (PX / 2));
             int gi = i0 - 2 + ii;
             gi = gi < 0 ? gi + Nx : gi;
             while (gi >= Nx) gi -= Nx;
@@ -761,14 +763,14 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
             }
         }
     }
-    int offp[CORR ? PERP : 1];   // CORR: this thread's share of a phi plane (same row and column rules)
+    int offp[CORR ? PERP : 1];   // CORR: this thread's pairs of a phi plane (same row and column rules)
     if constexpr (CORR) {
 #pragma unroll
         for (int q = 0; q < PERP; ++q) {
-            int e = threadIdx.x + q * NT;
+            int e2 = threadIdx.x + q * NT;
             offp[q] = -1;
-            if (e < PSP) {
-                int jj = e / PXP, ii = e - jj * PXP;
+            if (e2 < PSP2) {
+                int jj = e2 / (PXP / 2), ii = 2 * (e2 - jj * (PXP / 2));
                 int gi = i0 - 2 + ii;
                 gi = gi < 0 ? gi + Nx : gi;
                 while (gi >= Nx) gi -= Nx;
@@ -784,7 +786,7 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
             const int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k), slot = (k - k0 + 1) % 5;
 #pragma unroll
             for (int q = 0; q < PERP; ++q)
-                if (offp[q] >= 0) cp_async<4>(&smp[slot][threadIdx.x + q * NT], a.phi + kw * plane + offp[q]);
+                if (offp[q] >= 0) cp_async<8>(&smp[slot][2 * (threadIdx.x + q * NT)], a.phi + kw * plane + offp[q]);
         }
     };
     auto issue = [&](int slot, int k) {
@@ -793,38 +795,51 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
 #pragma unroll
         for (int q = 0; q < PER; ++q) {
             if (off[q] < 0) continue;
-            const int o = kb + off[q], e = threadIdx.x + q * NT;
-            cp_async<4>(&sm[0][slot][e], U + o);
-            cp_async<4>(&sm[2][slot][e], W + o);
+            const int o = kb + off[q], e = 2 * (threadIdx.x + q * NT);
+            cp_async<8>(&sm[0][slot][e], U + o);
+            cp_async<8>(&sm[2][slot][e], W + o);
             if (!ghost[q]) {
-                cp_async<4>(&sm[1][slot][e], V + o);
-                if (LES) cp_async<4>(&sm[NF - 1][slot][e], NU + o);
+                cp_async<8>(&sm[1][slot][e], V + o);
+                if (LES) cp_async<8>(&sm[NF - 1][slot][e], NU + o);
             }
         }
     };
     auto fix = [&](int slot, int k) {
-        if constexpr (CORR) {   // project_velocity of the previous stage (k_correct's arithmetic)
+        if constexpr (CORR) {   // project_velocity of the previous stage (k_correct's arithmetic, lane by lane)
             const int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k);
             const int p0 = (k - k0 + 1) % 5, p1 = (k - k0 + 2) % 5;
             const float iz = Arith<float>::inv(a.mz.df, a.mz.idf, kw);
 #pragma unroll
             for (int q = 0; q < PER; ++q) {
                 if (off[q] < 0) continue;
-                const int e = threadIdx.x + q * NT;
-                const float pc = smp[p0][pix[q]], pxp = smp[p0][pix[q] + 1], pzp = smp[p1][pix[q]];
-                sm[0][slot][e] = sm[0][slot][e] - (pxp - pc) * a.inv_dx;
-                sm[2][slot][e] = sm[2][slot][e] - (pzp - pc) * iz;
-                if (iyq[q] != 0.0f) sm[1][slot][e] = sm[1][slot][e] - (smp[p0][pix[q] + PXP] - pc) * iyq[q];
+                const int e = 2 * (threadIdx.x + q * NT);
+                const float2 pc = *reinterpret_cast<const float2 *>(&smp[p0][pix[q]]);
+                const float pn = smp[p0][pix[q] + 2];
+                const float2 pz = *reinterpret_cast<const float2 *>(&smp[p1][pix[q]]);
+                float2 *u2 = reinterpret_cast<float2 *>(&sm[0][slot][e]), *w2 = reinterpret_cast<float2 *>(&sm[2][slot][e]);
+                float2 u = *u2, w = *w2;
+                u.x = u.x - (pc.y - pc.x) * a.inv_dx; u.y = u.y - (pn - pc.y) * a.inv_dx;
+                w.x = w.x - (pz.x - pc.x) * iz; w.y = w.y - (pz.y - pc.y) * iz;
+                *u2 = u; *w2 = w;
+                if (iyq[q] != 0.0f) {
+                    const float2 py = *reinterpret_cast<const float2 *>(&smp[p0][pix[q] + PXP]);
+                    float2 *v2 = reinterpret_cast<float2 *>(&sm[1][slot][e]);
+                    float2 v = *v2;
+                    v.x = v.x - (py.x - pc.x) * iyq[q]; v.y = v.y - (py.y - pc.y) * iyq[q];
+                    *v2 = v;
+                }
             }
         }
 #pragma unroll
         for (int q = 0; q < PER; ++q) {
             if (off[q] < 0 || !ghost[q]) continue;
-            const int e = threadIdx.x + q * NT;
-            sm[0][slot][e] = -sm[0][slot][e];
-            sm[2][slot][e] = -sm[2][slot][e];
-            sm[1][slot][e] = 0.0f;
-            if (LES) sm[NF - 1][slot][e] = 0.0f;
+            const int e = 2 * (threadIdx.x + q * NT);
+            float2 *u2 = reinterpret_cast<float2 *>(&sm[0][slot][e]), *w2 = reinterpret_cast<float2 *>(&sm[2][slot][e]);
+            const float2 u = *u2, w = *w2;
+            *u2 = make_float2(-u.x, -u.y);
+            *w2 = make_float2(-w.x, -w.y);
+            *reinterpret_cast<float2 *>(&sm[1][slot][e]) = make_float2(0.0f, 0.0f);
+            if (LES) *reinterpret_cast<float2 *>(&sm[NF - 1][slot][e]) = make_float2(0.0f, 0.0f);
         }
     };
     F2 ubr[3];
