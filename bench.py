@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream measurement")
     ap.add_argument("--no-adaptive", action="store_true", help="skip the adaptive-time-step run")
     ap.add_argument("--no-hybrid", action="store_true", help="skip the advection_scheme = 2 runs")
+    ap.add_argument("--stage-kernel", choices=["auto", "one-cell", "pairs"], default="auto",
+                    help="FP32 stage kernel: the autotuner's choice (default) or a fixed one (profiling runs, where the "
+                         "serialised launches under a profiler skew the autotuner's timing)")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-vs-FP64 report of the other configs")
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-rate", type=float, default=4.0, help="Poisson arrival rate, requests/s")
@@ -254,6 +257,8 @@ def main():
     def timed_run(prec, sample_clocks=False, adaptive=False, case=None):
         s = Solver(case or c, prec, graphs=True)
         s.set_stream(sh)
+        if prec == "fp32" and args.stage_kernel != "auto":
+            s.set_stage_variant(0 if args.stage_kernel == "one-cell" else 1)
         s.set_state(U, V, W, P)
         if adaptive:
             s.set_adaptive_dt(True, 0.5, 0.9)
