@@ -368,6 +368,10 @@ template <typename T> struct Impl {
         return DFDM_OK;
     }
 
+    // the tiled hybrid-scheme kernel: z-planes per block and dynamic shared memory (3 fields x 8 planes of 38 x 14)
+    static constexpr int HYB_KC = 32;
+    static constexpr size_t hyb_smem_bytes() { return (size_t)3 * 8 * 38 * 14 * sizeof(T); }
+
     static int setup_kernels(dfdm_ctx *c) {
         const Dims &d = c->d;
         const int M = d.Nx / 2;
@@ -411,6 +415,10 @@ template <typename T> struct Impl {
         // the CFL maxima: one wave of resident blocks, at most one warp per x-row
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cfl<T, true>, 256, 0));
         c->cfl_blocks = (int)std::max(1LL, std::min((long long)std::max(1, occ) * nsm, ((long long)d.Ny * d.Nz + 7) / 8));
+        if (c->prm.advection_scheme == 2) {
+            CK(cudaFuncSetAttribute(k_adv_hybrid_tiled<T, 3, HYB_KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hyb_smem_bytes()));
+            CK(cudaFuncSetAttribute(k_adv_hybrid_tiled<T, 5, HYB_KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hyb_smem_bytes()));
+        }
         return setup_fft2l(c);
     }
 
@@ -654,10 +662,11 @@ template <typename T> struct Impl {
             h.my = metric_view<T>(c->my_t, d.Ny);
             h.mz = metric_view<T>(c->mz_t, d.Nz);
             h.ub = (const T *)c->d_ub;
+            const dim3 g((d.Nx + 31) / 32, (d.Ny + 7) / 8, (d.Nz + HYB_KC - 1) / HYB_KC);
             if (c->prm.adv_order == 5)
-                k_adv_hybrid<T, 5><<<cell_grid(d), CELL_BLOCK, 0, st>>>(h, f(c->u), f(c->v), f(c->w), f(c->adv));
+                k_adv_hybrid_tiled<T, 5, HYB_KC><<<g, 256, hyb_smem_bytes(), st>>>(h, f(c->u), f(c->v), f(c->w), f(c->adv));
             else
-                k_adv_hybrid<T, 3><<<cell_grid(d), CELL_BLOCK, 0, st>>>(h, f(c->u), f(c->v), f(c->w), f(c->adv));
+                k_adv_hybrid_tiled<T, 3, HYB_KC><<<g, 256, hyb_smem_bytes(), st>>>(h, f(c->u), f(c->v), f(c->w), f(c->adv));
             CKL();
             return DFDM_OK;
         }

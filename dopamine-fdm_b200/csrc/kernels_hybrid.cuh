@@ -3,7 +3,7 @@
 // The skew-symmetric central convection of the stage kernels is kept and beta |u_c| D is added as a conservative flux
 // difference, D the third difference / 12 (order 3) or minus the fifth difference / 60 (order 5) of the advected
 // velocity across the face, with the face's convecting velocity u_c.  With no immersed body beta = adv_beta0
-// everywhere.  One thread per cell computes the three components into out[0..cells), [cells..2 cells),
+// everywhere.  k_adv_hybrid_tiled computes the three components into out[0..cells), [cells..2 cells),
 // [2 cells..3 cells); the stage kernels add them to their right-hand sides.
 //
 // Index conventions: device cell (i, j, k) is the reference's (i+2, j+2, k+2).  x and z are periodic (the padded
@@ -24,16 +24,19 @@ template <typename T> struct HybArgs {
     const T *ub;          // streamwise base profile by row (zeros in FP64)
 };
 
+// the stencil weights of adv_wsel (src/adv_hybrid.f90:88-103), divided as the reference divides them (in double),
+// applied to s(-2:3) = a..f as sum(w*s); the zero weights of order 3 are skipped
 template <int ORD> struct HybW;
 template <> struct HybW<3> {
     template <typename T> static __device__ __forceinline__ T sum(T a, T b, T c, T d, T e, T f) {
         (void)a; (void)f;
-        return (T(-1) * b + T(3) * c + T(-3) * d + T(1) * e) / T(12);
+        return T(-1.0 / 12.0) * b + T(3.0 / 12.0) * c + T(-3.0 / 12.0) * d + T(1.0 / 12.0) * e;
     }
 };
 template <> struct HybW<5> {
     template <typename T> static __device__ __forceinline__ T sum(T a, T b, T c, T d, T e, T f) {
-        return (T(1) * a + T(-5) * b + T(10) * c + T(-10) * d + T(5) * e + T(-1) * f) / T(60);
+        return T(1.0 / 60.0) * a + T(-5.0 / 60.0) * b + T(10.0 / 60.0) * c + T(-10.0 / 60.0) * d + T(5.0 / 60.0) * e +
+               T(-1.0 / 60.0) * f;
     }
 };
 
@@ -51,117 +54,171 @@ __device__ __forceinline__ T hyb_wsum(int o, T a, T b, T c, T d, T e, T f) {
     return T(0);
 }
 
-template <typename T, int ORD>
-__global__ void __launch_bounds__(256) k_adv_hybrid(HybArgs<T> h, const T *__restrict__ U, const T *__restrict__ V,
-                                                    const T *__restrict__ W, T *__restrict__ out) {
+// A block owns a 32 x 8 column of cells and marches through KC z-planes; the
+// planes k-3 .. k+3 of U, V, W, each a (32+6) x (8+6) tile with a 3-cell halo in x and y, rotate through eight
+// shared planes filled by cp.async four planes ahead.  After a plane's copies land, each thread turns the
+// elements it copied into the values the reference reads: U (plus the base profile) and W mirrored and V zero on
+// wall rows, rows beyond a wall holding the clamped row's value (Max(jj-2,1), Min(jj+3,nyg)), periodic rows
+// wrapped.  Totals throughout (the x and z differences then carry the base profile's rounding: the terms are small).
+template <typename T, int ORD, int KC>
+__global__ void __launch_bounds__(256) k_adv_hybrid_tiled(HybArgs<T> h, const T *__restrict__ U, const T *__restrict__ V,
+                                                          const T *__restrict__ W, T *__restrict__ out) {
+    constexpr int TX = 32, TY = 8, H = 3, PX = TX + 2 * H, PY = TY + 2 * H, PS = PX * PY, NT = TX * TY;
+    constexpr int NP = 8, PER = (PS + NT - 1) / NT;
+    extern __shared__ __align__(16) unsigned char hyb_smem[];
+    T *sm = reinterpret_cast<T *>(hyb_smem);   // [3][NP][PS]
     const Dims &d = h.d;
-    const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
-    if (i >= Nx || j >= Ny) return;
-    const int nyg = d.yper ? Ny + 3 : Ny + 2, ny = d.yper ? Ny + 2 : Ny + 1;   // the reference's row counts
-    // device row of reference row J for a y-centred field, with the wall mirror sign
-    auto crow = [&](int J, T &sgn) -> int {
-        sgn = T(1);
-        if (d.yper) return wrap(J - 2, Ny);
-        if (J <= 1) { sgn = T(-1); return 0; }
-        if (J >= Ny + 2) { sgn = T(-1); return Ny - 1; }
-        return J - 2;
+    const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz, plane = Nx * Ny;
+    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k0 = blockIdx.z * KC, kend = min(k0 + KC, Nz);
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool active = i < Nx && j < Ny;
+    // this thread's plane elements: global offset (row, column), the row's sign for U/W (-1: mirror), V zero,
+    // and the base profile of the row
+    int off[PER];
+    T sg[PER], ubq[PER];
+    bool vz[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int e = threadIdx.x + q * NT;
+        off[q] = -1; sg[q] = T(1); ubq[q] = T(0); vz[q] = false;
+        if (e < PS) {
+            const int jj = e / PX, ii = e - jj * PX;
+            int gi = i0 - H + ii;
+            gi = gi < 0 ? gi + Nx : gi;
+            while (gi >= Nx) gi -= Nx;
+            const int gj = j0 - H + jj;   // device row; the reference's J = gj + 2
+            int g;
+            if (d.yper) {
+                g = gj % Ny; if (g < 0) g += Ny;
+            } else if (gj < 0) {
+                g = 0; sg[q] = T(-1); vz[q] = true;                 // J <= 1: the bottom ghost (V: the wall face)
+            } else if (gj >= Ny) {
+                g = Ny - 1; sg[q] = T(-1); vz[q] = true;            // J >= nyg: the top ghost
+            } else {
+                g = gj;
+                vz[q] = gj >= Ny - 1;                               // V row Ny-1 (J = ny) is the top wall face
+            }
+            off[q] = g * Nx + gi;
+            ubq[q] = h.ub[g];
+        }
+    }
+    auto slot = [&](int k) { return (k - k0 + H) & (NP - 1); };
+    auto issue = [&](int k) {
+        const int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k), sl = slot(k);
+        const size_t kb = (size_t)kw * plane;
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            if (off[q] < 0) continue;
+            const int e = threadIdx.x + q * NT;
+            cp_async<sizeof(T)>(&sm[(0 * NP + sl) * PS + e], U + kb + off[q]);
+            cp_async<sizeof(T)>(&sm[(1 * NP + sl) * PS + e], V + kb + off[q]);
+            cp_async<sizeof(T)>(&sm[(2 * NP + sl) * PS + e], W + kb + off[q]);
+        }
     };
-    auto at = [&](const T *F, int x, int r, int z) -> T {
-        return __ldg(F + ((size_t)wrap(z, Nz) * Ny + r) * Nx + wrap(x, Nx));
+    auto fix = [&](int k) {
+        const int sl = slot(k);
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            if (off[q] < 0) continue;
+            const int e = threadIdx.x + q * NT;
+            T &u = sm[(0 * NP + sl) * PS + e], &v = sm[(1 * NP + sl) * PS + e], &w = sm[(2 * NP + sl) * PS + e];
+            u = sg[q] * (u + ubq[q]);
+            w = sg[q] * w;
+            if (vz[q]) v = T(0);
+        }
     };
-    // total U and W at reference row J (device x, z), the base profile added back and the ghost rules applied
-    auto Ut = [&](int x, int J, int z) -> T {
-        T s;
-        const int r = crow(J, s);
-        return s * (at(U, x, r, z) + h.ub[r]);
-    };
-    auto Wt = [&](int x, int J, int z) -> T {
-        T s;
-        const int r = crow(J, s);
-        return s * at(W, x, r, z);
-    };
-    // V at reference face row J (1..ny): zero on the wall faces
-    auto Vf = [&](int x, int J, int z) -> T {
-        if (d.yper) return at(V, x, wrap(J - 2, Ny), z);
-        if (J <= 1 || J >= Ny + 1) return T(0);
-        return at(V, x, J - 2, z);
-    };
+    const int nyg = d.yper ? Ny + 3 : Ny + 2, ny = d.yper ? Ny + 2 : Ny + 1;
     const int J = j + 2;
     const T beta = h.beta, idx = h.inv_dx;
-    const size_t p = ((size_t)k * Ny + j) * Nx + i;
-
-    // ---- u (adv_add_u, :136-176): stored deviations in x and z (the profile cancels), totals in y ----
-    {
-        const T dyj = h.my.idc[j], dzk = h.mz.idc[k];
-        const T ubj = h.ub[j];
-        T r = T(0);
+    const T dyU = h.my.idc[min(j, Ny - 1)], dyV = h.my.idf[min(j, Ny - 1)];
+    for (int k = k0 - H; k <= k0 + H; ++k) issue(k);
+    cp_async_commit();
+    cp_async_wait_all();
+    for (int k = k0 - H; k <= k0 + H; ++k) fix(k);
+    __syncthreads();
+    for (int k = k0; k < kend; ++k) {
+        const bool more = k + 1 < kend;
+        if (more) issue(k + H + 1);
+        cp_async_commit();
+        if (active) {
+            // value of field f at this thread's cell offset by (dx, dy, dz)
+            auto S = [&](int f, int dx, int dy, int dz) -> T {
+                return sm[(f * NP + slot(k + dz)) * PS + (ty + H + dy) * PX + (tx + H + dx)];
+            };
+            // the clamped y rows of the reference, as offsets from this thread's row (J = j + 2)
+            auto yo = [&](int Jr, int n) -> int { return max(1, min(n, Jr)) - J; };
+            const T dzU = h.mz.idc[k], dzW = h.mz.idf[k];
+            const size_t p = ((size_t)k * Ny + j) * Nx + i;
+            // ---- u ----
+            T r = T(0);
 #pragma unroll
-        for (int m = 0; m <= 1; ++m) {
-            const T sg = T(2 * m - 1);
-            const int ii = i - 1 + m, jj = J - 1 + m, kk = k - 1 + m;
-            T uc = T(0.5) * ((at(U, ii, j, k) + ubj) + (at(U, ii + 1, j, k) + ubj));
-            T s = HybW<ORD>::sum(at(U, ii - 2, j, k), at(U, ii - 1, j, k), at(U, ii, j, k), at(U, ii + 1, j, k),
-                                 at(U, ii + 2, j, k), at(U, ii + 3, j, k));
-            r = r - sg * (beta * fabs(uc) * s) * idx;
-            uc = T(0.5) * (Vf(i, jj, k) + Vf(i + 1, jj, k));
-            s = hyb_wsum(hyb_ord_y(jj, nyg, ORD), Ut(i, max(jj - 2, 1), k), Ut(i, max(jj - 1, 1), k), Ut(i, jj, k),
-                         Ut(i, jj + 1, k), Ut(i, min(jj + 2, nyg), k), Ut(i, min(jj + 3, nyg), k));
-            r = r - sg * (beta * fabs(uc) * s) * dyj;
-            uc = T(0.5) * (at(W, i, j, kk) + at(W, i + 1, j, kk));
-            s = HybW<ORD>::sum(at(U, i, j, kk - 2), at(U, i, j, kk - 1), at(U, i, j, kk), at(U, i, j, kk + 1),
-                               at(U, i, j, kk + 2), at(U, i, j, kk + 3));
-            r = r - sg * (beta * fabs(uc) * s) * dzk;
-        }
-        out[p] = r;
-    }
-    // ---- v (adv_add_v, :179-219) ----
-    if (j < d.NyV) {
-        const T dyj = h.my.idf[j], dzk = h.mz.idc[k];
-        T r = T(0);
+            for (int m = 0; m <= 1; ++m) {
+                const T sgm = T(2 * m - 1);
+                const int a = m - 1;   // ii - i, jj - J, kk - k
+                T uc = T(0.5) * (S(0, a, 0, 0) + S(0, a + 1, 0, 0));
+                T s = HybW<ORD>::sum(S(0, a - 2, 0, 0), S(0, a - 1, 0, 0), S(0, a, 0, 0), S(0, a + 1, 0, 0),
+                                     S(0, a + 2, 0, 0), S(0, a + 3, 0, 0));
+                r = r - sgm * (beta * fabs(uc) * s) * idx;
+                const int jj = J + a;
+                uc = T(0.5) * (S(1, 0, a, 0) + S(1, 1, a, 0));
+                s = hyb_wsum(hyb_ord_y(jj, nyg, ORD), S(0, 0, yo(jj - 2, nyg), 0), S(0, 0, yo(jj - 1, nyg), 0),
+                             S(0, 0, a, 0), S(0, 0, a + 1, 0), S(0, 0, yo(jj + 2, nyg), 0), S(0, 0, yo(jj + 3, nyg), 0));
+                r = r - sgm * (beta * fabs(uc) * s) * dyU;
+                uc = T(0.5) * (S(2, 0, 0, a) + S(2, 1, 0, a));
+                s = HybW<ORD>::sum(S(0, 0, 0, a - 2), S(0, 0, 0, a - 1), S(0, 0, 0, a), S(0, 0, 0, a + 1),
+                                   S(0, 0, 0, a + 2), S(0, 0, 0, a + 3));
+                r = r - sgm * (beta * fabs(uc) * s) * dzU;
+            }
+            out[p] = r;
+            // ---- v ----
+            r = T(0);
+            if (j < d.NyV) {
 #pragma unroll
-        for (int m = 0; m <= 1; ++m) {
-            const T sg = T(2 * m - 1);
-            const int ii = i - 1 + m, jj = J - 1 + m, kk = k - 1 + m;
-            T uc = T(0.5) * (Ut(ii, J, k) + Ut(ii, J + 1, k));
-            T s = HybW<ORD>::sum(at(V, ii - 2, j, k), at(V, ii - 1, j, k), at(V, ii, j, k), at(V, ii + 1, j, k),
-                                 at(V, ii + 2, j, k), at(V, ii + 3, j, k));
-            r = r - sg * (beta * fabs(uc) * s) * idx;
-            uc = T(0.5) * (Vf(i, jj, k) + Vf(i, jj + 1, k));
-            s = hyb_wsum(hyb_ord_y(jj, ny, ORD), Vf(i, max(jj - 2, 1), k), Vf(i, max(jj - 1, 1), k), Vf(i, jj, k),
-                         Vf(i, jj + 1, k), Vf(i, min(jj + 2, ny), k), Vf(i, min(jj + 3, ny), k));
-            r = r - sg * (beta * fabs(uc) * s) * dyj;
-            uc = T(0.5) * (Wt(i, J, kk) + Wt(i, J + 1, kk));
-            s = HybW<ORD>::sum(at(V, i, j, kk - 2), at(V, i, j, kk - 1), at(V, i, j, kk), at(V, i, j, kk + 1),
-                               at(V, i, j, kk + 2), at(V, i, j, kk + 3));
-            r = r - sg * (beta * fabs(uc) * s) * dzk;
-        }
-        out[d.cells + p] = r;
-    } else {
-        out[d.cells + p] = T(0);
-    }
-    // ---- w (adv_add_w, :222-262) ----
-    {
-        const T dyj = h.my.idc[j], dzk = h.mz.idf[k];
-        T r = T(0);
+                for (int m = 0; m <= 1; ++m) {
+                    const T sgm = T(2 * m - 1);
+                    const int a = m - 1;
+                    T uc = T(0.5) * (S(0, a, 0, 0) + S(0, a, 1, 0));
+                    T s = HybW<ORD>::sum(S(1, a - 2, 0, 0), S(1, a - 1, 0, 0), S(1, a, 0, 0), S(1, a + 1, 0, 0),
+                                         S(1, a + 2, 0, 0), S(1, a + 3, 0, 0));
+                    r = r - sgm * (beta * fabs(uc) * s) * idx;
+                    const int jj = J + a;
+                    uc = T(0.5) * (S(1, 0, a, 0) + S(1, 0, a + 1, 0));
+                    s = hyb_wsum(hyb_ord_y(jj, ny, ORD), S(1, 0, yo(jj - 2, ny), 0), S(1, 0, yo(jj - 1, ny), 0),
+                                 S(1, 0, a, 0), S(1, 0, a + 1, 0), S(1, 0, yo(jj + 2, ny), 0), S(1, 0, yo(jj + 3, ny), 0));
+                    r = r - sgm * (beta * fabs(uc) * s) * dyV;
+                    uc = T(0.5) * (S(2, 0, 0, a) + S(2, 0, 1, a));
+                    s = HybW<ORD>::sum(S(1, 0, 0, a - 2), S(1, 0, 0, a - 1), S(1, 0, 0, a), S(1, 0, 0, a + 1),
+                                       S(1, 0, 0, a + 2), S(1, 0, 0, a + 3));
+                    r = r - sgm * (beta * fabs(uc) * s) * dzU;
+                }
+            }
+            out[d.cells + p] = r;
+            // ---- w ----
+            r = T(0);
 #pragma unroll
-        for (int m = 0; m <= 1; ++m) {
-            const T sg = T(2 * m - 1);
-            const int ii = i - 1 + m, jj = J - 1 + m, kk = k - 1 + m;
-            T uc = T(0.5) * (Ut(ii, J, k) + Ut(ii, J, k + 1));
-            T s = HybW<ORD>::sum(at(W, ii - 2, j, k), at(W, ii - 1, j, k), at(W, ii, j, k), at(W, ii + 1, j, k),
-                                 at(W, ii + 2, j, k), at(W, ii + 3, j, k));
-            r = r - sg * (beta * fabs(uc) * s) * idx;
-            uc = T(0.5) * (Vf(i, jj, k) + Vf(i, jj, k + 1));
-            s = hyb_wsum(hyb_ord_y(jj, nyg, ORD), Wt(i, max(jj - 2, 1), k), Wt(i, max(jj - 1, 1), k), Wt(i, jj, k),
-                         Wt(i, jj + 1, k), Wt(i, min(jj + 2, nyg), k), Wt(i, min(jj + 3, nyg), k));
-            r = r - sg * (beta * fabs(uc) * s) * dyj;
-            uc = T(0.5) * (at(W, i, j, kk) + at(W, i, j, kk + 1));
-            s = HybW<ORD>::sum(at(W, i, j, kk - 2), at(W, i, j, kk - 1), at(W, i, j, kk), at(W, i, j, kk + 1),
-                               at(W, i, j, kk + 2), at(W, i, j, kk + 3));
-            r = r - sg * (beta * fabs(uc) * s) * dzk;
+            for (int m = 0; m <= 1; ++m) {
+                const T sgm = T(2 * m - 1);
+                const int a = m - 1;
+                T uc = T(0.5) * (S(0, a, 0, 0) + S(0, a, 0, 1));
+                T s = HybW<ORD>::sum(S(2, a - 2, 0, 0), S(2, a - 1, 0, 0), S(2, a, 0, 0), S(2, a + 1, 0, 0),
+                                     S(2, a + 2, 0, 0), S(2, a + 3, 0, 0));
+                r = r - sgm * (beta * fabs(uc) * s) * idx;
+                const int jj = J + a;
+                uc = T(0.5) * (S(1, 0, a, 0) + S(1, 0, a, 1));
+                s = hyb_wsum(hyb_ord_y(jj, nyg, ORD), S(2, 0, yo(jj - 2, nyg), 0), S(2, 0, yo(jj - 1, nyg), 0),
+                             S(2, 0, a, 0), S(2, 0, a + 1, 0), S(2, 0, yo(jj + 2, nyg), 0), S(2, 0, yo(jj + 3, nyg), 0));
+                r = r - sgm * (beta * fabs(uc) * s) * dyU;
+                uc = T(0.5) * (S(2, 0, 0, a) + S(2, 0, 0, a + 1));
+                s = HybW<ORD>::sum(S(2, 0, 0, a - 2), S(2, 0, 0, a - 1), S(2, 0, 0, a), S(2, 0, 0, a + 1),
+                                   S(2, 0, 0, a + 2), S(2, 0, 0, a + 3));
+                r = r - sgm * (beta * fabs(uc) * s) * dzW;
+            }
+            out[2 * d.cells + p] = r;
         }
-        out[2 * d.cells + p] = r;
+        cp_async_wait_all();
+        if (more) fix(k + H + 1);
+        __syncthreads();
     }
 }
 
