@@ -35,7 +35,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_fwd_x2(PoissonA
     C *bt = (C *)smem_raw, *ba = bt + lx * LDT;
     const Dims &d = a.d;
     const int Ny = d.Ny, Nz = d.Nz, plane = Nx * Ny;
-    const int line0 = blockIdx.x * lx;
+    // blocks run roughly in index order: the first take the highest lines (top z planes), which the stage kernel
+    // wrote last and which are the likeliest to still be in L2
+    const int line0 = (gridDim.x - 1 - blockIdx.x) * lx;
     const int nl = min(lx, Ny * Nz - line0);
     constexpr int ITEMS = RowLines<T, M>::value * M;   // lx == RowLines<T, M>::value, blockDim.x == 256
     constexpr int PER = (ITEMS + 255) / 256, UNR = sizeof(T) == 4 ? 4 : 2;   // items per thread; items loaded together
