@@ -133,6 +133,12 @@ struct dfdm_ctx {
     int lx2 = 1, lxi2 = 1, thr_z2 = 256, thr_y2 = 256;   // x lines per block: forward, inverse
     size_t smem_x2 = 0, smem_xi2 = 0, smem_z2 = 0, smem_y2 = 0;
     cudaStream_t own_stream = nullptr, stream = nullptr;
+    // asynchronous state transfer (dfdm_set_state_async / dfdm_get_state_async): one copy stream per direction, one
+    // FP64 staging buffer per field and direction, and events that keep a buffer from being refilled before its
+    // last reader is done.  Made on first use, outside the footprint.
+    cudaStream_t cin = nullptr, cout = nullptr;
+    double *stage_in[4] = {nullptr, nullptr, nullptr, nullptr}, *stage_out[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_in[4] = {}, ev_unpacked[4] = {}, ev_packed[4] = {}, ev_out[4] = {};
     double t = 0.0;
     bool wmf_seeded = false;
     // graphs
@@ -1126,6 +1132,15 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
 int dfdm_destroy(dfdm_ctx *c) {
     if (!c) return DFDM_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->cin) cudaStreamSynchronize(c->cin);
+    if (c->cout) cudaStreamSynchronize(c->cout);
+    for (int q = 0; q < 4; ++q) {
+        cudaEvent_t *evs[4] = {&c->ev_in[q], &c->ev_unpacked[q], &c->ev_packed[q], &c->ev_out[q]};
+        for (cudaEvent_t *e : evs)
+            if (*e) cudaEventDestroy(*e);
+    }
+    if (c->cin) cudaStreamDestroy(c->cin);
+    if (c->cout) cudaStreamDestroy(c->cout);
     destroy_graph(c);
     for (void *p : c->allocs) cudaFree(p);
     c->allocs.clear();
@@ -1145,6 +1160,29 @@ int dfdm_set_stream(dfdm_ctx *c, void *s) {
 int dfdm_synchronize(dfdm_ctx *c) {
     if (int rc = check_ctx(c)) return rc;
     CK(cudaStreamSynchronize(c->stream));
+    if (c->cin) CK(cudaStreamSynchronize(c->cin));
+    if (c->cout) CK(cudaStreamSynchronize(c->cout));
+    return DFDM_OK;
+}
+
+// copy streams, staging buffers and events of the asynchronous transfers
+static int ensure_async(dfdm_ctx *c) {
+    if (c->cin) return DFDM_OK;
+    const size_t n = (size_t)(c->nxg) * c->nyg * c->nzg;   // the largest ghosted shape
+    for (int q = 0; q < 4; ++q) {
+        void *a = nullptr, *b = nullptr;
+        if (int rc = dalloc(c, &a, n * sizeof(double))) return rc;
+        if (int rc = dalloc(c, &b, n * sizeof(double))) return rc;
+        c->stage_in[q] = (double *)a;
+        c->stage_out[q] = (double *)b;
+        cudaEvent_t *evs[4] = {&c->ev_in[q], &c->ev_unpacked[q], &c->ev_packed[q], &c->ev_out[q]};
+        for (cudaEvent_t *e : evs) CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+        // a first wait on an event that was never recorded is a no-op: record them once on the compute stream
+        CK(cudaEventRecord(c->ev_unpacked[q], c->stream));
+        CK(cudaEventRecord(c->ev_out[q], c->stream));
+    }
+    CK(cudaStreamCreateWithFlags(&c->cin, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->cout, cudaStreamNonBlocking));
     return DFDM_OK;
 }
 
@@ -1215,6 +1253,60 @@ int dfdm_get_state(dfdm_ctx *c, double *U, double *V, double *W, double *P) {
     if (V) { if ((rc = get_field(c, FK_V, c->v, V, c->nxg, c->ny, c->nzg))) return rc; CK(cudaStreamSynchronize(c->stream)); }
     if (W) { if ((rc = get_field(c, FK_W, c->w, W, c->nxg, c->nyg, c->nz))) return rc; CK(cudaStreamSynchronize(c->stream)); }
     if (P) { if ((rc = get_field(c, FK_P, c->p, P, c->nxg, c->nyg, c->nzg))) return rc; CK(cudaStreamSynchronize(c->stream)); }
+    return DFDM_OK;
+}
+
+int dfdm_set_state_async(dfdm_ctx *c, const double *U, const double *V, const double *W, const double *P) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (!U || !V || !W) return fail(DFDM_ERR_INVALID, "U, V and W must not be NULL");
+    if (c->prec == DFDM_FP32_MIXED && !c->ub_set)   // the first state fixes the base profile (host work): synchronous
+        return dfdm_set_state(c, U, V, W, P);
+    if (int rc = ensure_async(c)) return rc;
+    struct { const double *h; int kind; void *dst; int n1, n2, n3; } f[4] = {
+        {U, FK_U, c->u, c->nx, c->nyg, c->nzg}, {V, FK_V, c->v, c->nxg, c->ny, c->nzg},
+        {W, FK_W, c->w, c->nxg, c->nyg, c->nz}, {P, FK_P, c->p, c->nxg, c->nyg, c->nzg}};
+    const int gb = reduce_grid(c->d);
+    for (int q = 0; q < 4; ++q) {
+        if (!f[q].h) continue;
+        const size_t n = (size_t)f[q].n1 * f[q].n2 * f[q].n3;
+        CK(cudaStreamWaitEvent(c->cin, c->ev_unpacked[q], 0));   // the buffer's previous contents are unpacked
+        CK(cudaMemcpyAsync(c->stage_in[q], f[q].h, n * sizeof(double), cudaMemcpyHostToDevice, c->cin));
+        CK(cudaEventRecord(c->ev_in[q], c->cin));
+        CK(cudaStreamWaitEvent(c->stream, c->ev_in[q], 0));
+        if (c->prec == DFDM_FP64)
+            k_unpack<double><<<gb, 256, 0, c->stream>>>(c->d, f[q].kind, f[q].n1, f[q].n2, c->stage_in[q], c->d_ubd, (double *)f[q].dst);
+        else
+            k_unpack<float><<<gb, 256, 0, c->stream>>>(c->d, f[q].kind, f[q].n1, f[q].n2, c->stage_in[q], c->d_ubd, (float *)f[q].dst);
+        CKL();
+        CK(cudaEventRecord(c->ev_unpacked[q], c->stream));
+    }
+    c->projected = false;
+    return DFDM_OK;
+}
+
+int dfdm_get_state_async(dfdm_ctx *c, double *U, double *V, double *W, double *P) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (int rc = ensure_async(c)) return rc;
+    struct { double *h; int kind; const void *src; int n1, n2, n3; } f[4] = {
+        {U, FK_U, c->u, c->nx, c->nyg, c->nzg}, {V, FK_V, c->v, c->nxg, c->ny, c->nzg},
+        {W, FK_W, c->w, c->nxg, c->nyg, c->nz}, {P, FK_P, c->p, c->nxg, c->nyg, c->nzg}};
+    for (int q = 0; q < 4; ++q) {
+        if (!f[q].h) continue;
+        const size_t n = (size_t)f[q].n1 * f[q].n2 * f[q].n3;
+        const int gb = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
+        CK(cudaStreamWaitEvent(c->stream, c->ev_out[q], 0));   // the buffer's previous contents are downloaded
+        if (c->prec == DFDM_FP64)
+            k_pack<double><<<gb, 256, 0, c->stream>>>(c->d, f[q].kind, f[q].n1, f[q].n2, f[q].n3, (const double *)f[q].src, c->d_ubd, c->stage_out[q]);
+        else
+            k_pack<float><<<gb, 256, 0, c->stream>>>(c->d, f[q].kind, f[q].n1, f[q].n2, f[q].n3, (const float *)f[q].src, c->d_ubd, c->stage_out[q]);
+        CKL();
+        CK(cudaEventRecord(c->ev_packed[q], c->stream));
+        CK(cudaStreamWaitEvent(c->cout, c->ev_packed[q], 0));
+        CK(cudaMemcpyAsync(f[q].h, c->stage_out[q], n * sizeof(double), cudaMemcpyDeviceToHost, c->cout));
+        CK(cudaEventRecord(c->ev_out[q], c->cout));
+    }
     return DFDM_OK;
 }
 

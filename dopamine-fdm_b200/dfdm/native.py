@@ -33,7 +33,7 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_launch_count", "dfdm_solve_poisson_noalloc", "dfdm_write_snapshot", "dfdm_read_snapshot",
            "dfdm_compute_cfl", "dfdm_set_stage_variant", "dfdm_get_stage_variant", "dfdm_set_adaptive_dt",
            "dfdm_get_dt", "dfdm_set_landing_time", "dfdm_output_monitor", "dfdm_output_monitor_async",
-           "dfdm_set_fused_correction", "dfdm_get_fused_correction"]
+           "dfdm_set_fused_correction", "dfdm_get_fused_correction", "dfdm_set_state_async", "dfdm_get_state_async"]
 
 
 class DfdmError(RuntimeError):
@@ -69,6 +69,8 @@ def load(build_if_missing: bool = True):
         "dfdm_synchronize": (c_int, [c_void_p]),
         "dfdm_set_state": (c_int, [c_void_p, P, P, P, P]),
         "dfdm_get_state": (c_int, [c_void_p, P, P, P, P]),
+        "dfdm_set_state_async": (c_int, [c_void_p, P, P, P, P]),
+        "dfdm_get_state_async": (c_int, [c_void_p, P, P, P, P]),
         "dfdm_get_nu_t": (c_int, [c_void_p, P]),
         "dfdm_set_nu_t": (c_int, [c_void_p, P]),
         "dfdm_set_time": (c_int, [c_void_p, c_double]),
@@ -176,6 +178,7 @@ class Solver:
 
     def synchronize(self):
         _check(load().dfdm_synchronize(self.h))
+        self._pending = []
 
     def enable_graphs(self, on: bool = True):
         _check(load().dfdm_enable_graphs(self.h, int(on)))
@@ -193,6 +196,27 @@ class Solver:
         U, V, W, P = out if out is not None else (self._arr("U"), self._arr("V"), self._arr("W"), self._arr("P"))
         _check(load().dfdm_get_state(self.h, dptr(U), dptr(V), dptr(W), dptr(P)))
         return U, V, W, P
+
+    @staticmethod
+    def _async_arg(a):
+        """An array an asynchronous copy may use in place: Fortran-ordered float64 (no temporary copy)."""
+        if a is None:
+            return None
+        if a.dtype != np.float64 or not a.flags.f_contiguous:
+            raise ValueError("asynchronous transfers need Fortran-ordered float64 arrays (ideally pinned memory)")
+        return a
+
+    def set_state_async(self, U, V, W, P=None):
+        """Enqueue the upload; the arrays must stay untouched until synchronize()."""
+        args = [self._async_arg(a) for a in (U, V, W, P)]
+        self._pending = getattr(self, "_pending", []) + args
+        _check(load().dfdm_set_state_async(self.h, *[dptr(a) for a in args]))
+
+    def get_state_async(self, out):
+        """Enqueue the download into out = (U, V, W, P) (P may be None); valid after synchronize()."""
+        args = [self._async_arg(a) for a in out]
+        self._pending = getattr(self, "_pending", []) + args
+        _check(load().dfdm_get_state_async(self.h, *[dptr(a) for a in args]))
 
     def get_nu_t(self):
         a = self._arr("P")

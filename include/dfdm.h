@@ -101,12 +101,19 @@ int dfdm_footprint_bytes(const dfdm_grid *grid, const dfdm_params *params, size_
 /* Run the context's work on an externally owned CUDA stream (cudaStream_t passed as void*); NULL restores the
  * context's own stream. */
 int dfdm_set_stream(dfdm_ctx *ctx, void *cuda_stream);
-int dfdm_synchronize(dfdm_ctx *ctx);
+int dfdm_synchronize(dfdm_ctx *ctx);   /* waits for the context's stream and its copy streams */
 
 /* ---- state transfer: the reference's U, V, W, P, nu_t module arrays (src/global.f90:139,300) ----
  * set_state reads the interior (independent) cells; ghosts are implied. P may be NULL. */
 int dfdm_set_state(dfdm_ctx *ctx, const double *U, const double *V, const double *W, const double *P);
 int dfdm_get_state(dfdm_ctx *ctx, double *U, double *V, double *W, double *P);
+/* The same transfers, enqueued without a host synchronisation: uploads run on a copy stream of their own, downloads
+ * on another, the unpack/pack kernels on the context's stream in order with the steps.  A host loop of set_async,
+ * step_async, get_async therefore overlaps one step's download with the next step's upload.  The host arrays must
+ * stay untouched until dfdm_synchronize (pinned memory makes the copies asynchronous; pageable memory works but
+ * copies synchronously).  The context's first FP32-mixed set_state fixes its base profile and is synchronous. */
+int dfdm_set_state_async(dfdm_ctx *ctx, const double *U, const double *V, const double *W, const double *P);
+int dfdm_get_state_async(dfdm_ctx *ctx, double *U, double *V, double *W, double *P);
 int dfdm_get_nu_t(dfdm_ctx *ctx, double *nu_t);
 int dfdm_set_nu_t(dfdm_ctx *ctx, const double *nu_t);
 int dfdm_set_time(dfdm_ctx *ctx, double t);
