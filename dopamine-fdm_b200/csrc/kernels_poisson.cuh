@@ -150,70 +150,9 @@ __global__ void __launch_bounds__(256) k_col_fft(Dims d, typename cplx_t<T>::typ
 //   x(n-1) = b'(n-1)/D(n-1),  x(r) = (b'(r) - DU(r) x(r+1))/D(r)  (backward)
 // The pressure operator is similar to a symmetric negative-definite matrix once the null mode is pinned, so
 // elimination without interchanges is stable.  One thread owns one (kx,kz) column and a warp covers 32
-// consecutive kx, so every row access is coalesced.  Each sweep works in chunks of CH rows: the chunk's loads
-// are all issued before its recurrence runs, so one memory latency is paid per CH rows.
-template <typename T, int CH>
-__global__ void __launch_bounds__(64) k_ysolve(Dims d, typename cplx_t<T>::type *__restrict__ spec,
-                                               const double *__restrict__ rpiv, const double *__restrict__ lo,
-                                               const double *__restrict__ up) {
-    typedef typename cplx_t<T>::type C;
-    const int Nxc = d.Nxc;
-    const int kx = blockIdx.x * blockDim.x + threadIdx.x, kz = blockIdx.y;
-    if (kx >= Nxc) return;
-    const int n = d.Ny;
-    C *col = spec + kz * n * Nxc + kx;
-    const double *rp = rpiv + kz * n * Nxc + kx;
-    C v0 = col[0];
-    double br = (double)v0.x, bi = (double)v0.y, rprev = __ldg(rp);
-    for (int r0 = 1; r0 < n; r0 += CH) {
-        C v[CH];
-        double rv[CH], lv[CH];
-#pragma unroll
-        for (int q = 0; q < CH; ++q) {
-            const int r = r0 + q;
-            if (r < n) { v[q] = col[r * Nxc]; rv[q] = __ldg(rp + r * Nxc); lv[q] = __ldg(lo + r); }
-        }
-#pragma unroll
-        for (int q = 0; q < CH; ++q) {
-            const int r = r0 + q;
-            if (r < n) {
-                const double m = lv[q] * rprev;
-                br = (double)v[q].x - m * br;
-                bi = (double)v[q].y - m * bi;
-                if (r < n - 1) { C o; o.x = (T)br; o.y = (T)bi; col[r * Nxc] = o; }
-                rprev = rv[q];
-            }
-        }
-    }
-    double xr = br * rprev, xi = bi * rprev;
-    {
-        C o; o.x = (T)xr; o.y = (T)xi;
-        col[(n - 1) * Nxc] = o;
-    }
-    for (int r0 = n - 2; r0 >= 0; r0 -= CH) {
-        C v[CH];
-        double rv[CH], uv[CH];
-#pragma unroll
-        for (int q = 0; q < CH; ++q) {
-            const int r = r0 - q;
-            if (r >= 0) { v[q] = col[r * Nxc]; rv[q] = __ldg(rp + r * Nxc); uv[q] = __ldg(up + r); }
-        }
-#pragma unroll
-        for (int q = 0; q < CH; ++q) {
-            const int r = r0 - q;
-            if (r >= 0) {
-                xr = ((double)v[q].x - uv[q] * xr) * rv[q];
-                xi = ((double)v[q].y - uv[q] * xi) * rv[q];
-                C o; o.x = (T)xr; o.y = (T)xi;
-                col[r * Nxc] = o;
-            }
-        }
-    }
-}
-
-// The same solve with the memory latency hidden: each sweep keeps two register buffers of CH rows and issues the
-// loads of the next chunk before the recurrence of the current one runs, and the per-row coefficients DL and DU
-// are read from shared memory.  Arithmetic and rounding are those of k_ysolve.
+// consecutive kx, so every row access is coalesced.  Each sweep keeps two register buffers of CH rows and issues
+// the loads of the next chunk before the recurrence of the current one runs, and the per-row coefficients DL and
+// DU are read from shared memory.
 template <typename T, int CH>
 __global__ void __launch_bounds__(64) k_ysolve2(Dims d, typename cplx_t<T>::type *__restrict__ spec,
                                                 const double *__restrict__ rpiv, const double *__restrict__ lo,
