@@ -374,9 +374,8 @@ template <typename T> struct Impl {
         return DFDM_OK;
     }
 
-    // the tiled hybrid-scheme kernel: z-planes per block and dynamic shared memory (3 fields x 8 planes of 38 x 14)
+    // the hybrid-scheme kernel: z-planes per block (its shared memory: hyb_faces_smem_bytes)
     static constexpr int HYB_KC = 32;
-    static constexpr size_t hyb_smem_bytes() { return (size_t)3 * 8 * 38 * 14 * sizeof(T); }
 
     static int setup_kernels(dfdm_ctx *c) {
         const Dims &d = c->d;
@@ -422,8 +421,16 @@ template <typename T> struct Impl {
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cfl<T, true>, 256, 0));
         c->cfl_blocks = (int)std::max(1LL, std::min((long long)std::max(1, occ) * nsm, ((long long)d.Ny * d.Nz + 7) / 8));
         if (c->prm.advection_scheme == 2) {
-            CK(cudaFuncSetAttribute(k_adv_hybrid_tiled<T, 3, HYB_KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hyb_smem_bytes()));
-            CK(cudaFuncSetAttribute(k_adv_hybrid_tiled<T, 5, HYB_KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hyb_smem_bytes()));
+            CK(cudaFuncSetAttribute(k_adv_hybrid_faces<T, 3, HYB_KC, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)hyb_faces_smem_bytes<T, 3>()));
+            CK(cudaFuncSetAttribute(k_adv_hybrid_faces<T, 5, HYB_KC, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)hyb_faces_smem_bytes<T, 5>()));
+            if constexpr (sizeof(T) == 4) {
+                CK(cudaFuncSetAttribute(k_adv_hybrid_faces<T, 3, HYB_KC, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)hyb_faces_smem_bytes<T, 3>()));
+                CK(cudaFuncSetAttribute(k_adv_hybrid_faces<T, 5, HYB_KC, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)hyb_faces_smem_bytes<T, 5>()));
+            }
         }
         return setup_fft2l(c);
     }
@@ -669,10 +676,16 @@ template <typename T> struct Impl {
             h.mz = metric_view<T>(c->mz_t, d.Nz);
             h.ub = (const T *)c->d_ub;
             const dim3 g((d.Nx + 31) / 32, (d.Ny + 7) / 8, (d.Nz + HYB_KC - 1) / HYB_KC);
-            if (c->prm.adv_order == 5)
-                k_adv_hybrid_tiled<T, 5, HYB_KC><<<g, 256, hyb_smem_bytes(), st>>>(h, f(c->u), f(c->v), f(c->w), f(c->adv));
-            else
-                k_adv_hybrid_tiled<T, 3, HYB_KC><<<g, 256, hyb_smem_bytes(), st>>>(h, f(c->u), f(c->v), f(c->w), f(c->adv));
+            // 16-byte row copies in FP32 when Nx % 4 == 0, else 8-byte pairs (Nx is even)
+            const bool quads = sizeof(T) == 4 && d.Nx % 4 == 0;
+            const size_t sb = c->prm.adv_order == 5 ? hyb_faces_smem_bytes<T, 5>() : hyb_faces_smem_bytes<T, 3>();
+            if (c->prm.adv_order == 5) {
+                if (quads) k_adv_hybrid_faces<T, 5, HYB_KC, 16 / sizeof(T)><<<g, 256, sb, st>>>(h, f(c->u), f(c->v), f(c->w), f(c->adv));
+                else k_adv_hybrid_faces<T, 5, HYB_KC, 2><<<g, 256, sb, st>>>(h, f(c->u), f(c->v), f(c->w), f(c->adv));
+            } else {
+                if (quads) k_adv_hybrid_faces<T, 3, HYB_KC, 16 / sizeof(T)><<<g, 256, sb, st>>>(h, f(c->u), f(c->v), f(c->w), f(c->adv));
+                else k_adv_hybrid_faces<T, 3, HYB_KC, 2><<<g, 256, sb, st>>>(h, f(c->u), f(c->v), f(c->w), f(c->adv));
+            }
             CKL();
             return DFDM_OK;
         }

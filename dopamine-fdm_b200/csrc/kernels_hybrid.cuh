@@ -3,7 +3,7 @@
 // The skew-symmetric central convection of the stage kernels is kept and beta |u_c| D is added as a conservative flux
 // difference, D the third difference / 12 (order 3) or minus the fifth difference / 60 (order 5) of the advected
 // velocity across the face, with the face's convecting velocity u_c.  With no immersed body beta = adv_beta0
-// everywhere.  k_adv_hybrid_tiled computes the three components into out[0..cells), [cells..2 cells),
+// everywhere.  k_adv_hybrid_faces computes the three components into out[0..cells), [cells..2 cells),
 // [2 cells..3 cells); the stage kernels add them to their right-hand sides.
 //
 // Index conventions: device cell (i, j, k) is the reference's (i+2, j+2, k+2).  x and z are periodic (the padded
@@ -54,27 +54,51 @@ __device__ __forceinline__ T hyb_wsum(int o, T a, T b, T c, T d, T e, T f) {
     return T(0);
 }
 
-// A block owns a 32 x 8 column of cells and marches through KC z-planes; the
-// planes k-3 .. k+3 of U, V, W, each a (32+6) x (8+6) tile with a 3-cell halo in x and y, rotate through eight
-// shared planes filled by cp.async four planes ahead.  After a plane's copies land, each thread turns the
-// elements it copied into the values the reference reads: U (plus the base profile) and W mirrored and V zero on
-// wall rows, rows beyond a wall holding the clamped row's value (Max(jj-2,1), Min(jj+3,nyg)), periodic rows
-// wrapped.  Totals throughout (the x and z differences then carry the base profile's rounding: the terms are small).
-template <typename T, int ORD, int KC>
-__global__ void __launch_bounds__(256) k_adv_hybrid_tiled(HybArgs<T> h, const T *__restrict__ U, const T *__restrict__ V,
-                                                          const T *__restrict__ W, T *__restrict__ out) {
-    constexpr int TX = 32, TY = 8, H = 3, PX = TX + 2 * H, PY = TY + 2 * H, PS = PX * PY, NT = TX * TY;
-    constexpr int NP = 8, PER = (PS + NT - 1) / NT;
+// Shared memory of k_adv_hybrid_faces: the ring of 8 planes of U, V, W, each a 40 x (8 + 2H) tile (a 4-cell x halo,
+// so that tile rows start on 16-byte boundaries; H = 2 rows for order 3, 3 for order 5), then the x faces [3][8][33]
+// and the y faces [3][9][32] of the current plane.
+template <typename T, int ORD> constexpr size_t hyb_faces_smem_bytes() {
+    return ((size_t)3 * 8 * 40 * (8 + 2 * (ORD == 5 ? 3 : 2)) + 3 * 8 * 33 + 3 * 9 * 32) * sizeof(T);
+}
+
+// A block owns a 32 x 8 column of cells and marches through KC z-planes; the planes of U, V, W rotate through eight
+// shared tiles filled by cp.async H+1 planes ahead (y halo H = 2 rows for order 3, 3 for order 5; x halo 4 cells).
+// After a plane's copies land, each thread turns the vectors it copied into the values the reference reads: U (plus
+// the base profile) and W mirrored and V zero on wall rows, rows beyond a wall holding the clamped row's value
+// (Max(jj-2,1), Min(jj+3,nyg)), periodic rows wrapped.  Totals throughout (the x and z differences then carry the
+// base profile's rounding: the terms are small).
+// Each face flux is evaluated once.  The flux through a face, beta |u_c| D (without the cell's metric), depends
+// only on the face, so a cell's two faces per direction are shared with its neighbours:
+//   x: each thread evaluates the face on its left, lanes 0..7 of warp 0 the right-hand faces of the tile's rows;
+//   y: each thread the face below its row, warp 7 the faces above the tile;
+//   z: each thread the face above its cell, carried in registers to the next plane as the face below; the cell's
+//      own column of each field (the z stencil) is a register queue that takes one new plane per step.
+// x and y faces pass through shared memory (a barrier between their stores and the reads).  The cell then assembles
+//   r = -(-1)Fx(-) dx' - (-1)Fy(-) dy' - (-1)Fz(-) dz' - Fx(+) dx' - Fy(+) dy' - Fz(+) dz'
+// in the order of adv_dflux (src/adv_hybrid.f90:136-210): the lower faces, then the upper faces, x, y, z.  y rows
+// are clamped to the reference's ranges by absolute row.
+template <typename T, int ORD, int KC, int VW>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? (ORD == 5 ? 3 : 4) : (ORD == 5 ? 1 : 2))
+    k_adv_hybrid_faces(HybArgs<T> h, const T *__restrict__ U, const T *__restrict__ V, const T *__restrict__ W,
+                       T *__restrict__ out) {
+    constexpr int TX = 32, TY = 8, H = ORD == 5 ? 3 : 2, HX = 4, PX = TX + 2 * HX, PY = TY + 2 * H, PS = PX * PY;
+    constexpr int NT = TX * TY, NP = 8;
+    // the loader copies VW consecutive x cells at a time (VW = 4 in FP32 when Nx % 4 == 0, else 2): every vector
+    // starts at a column that is a multiple of VW, so it never straddles the periodic seam
+    constexpr int VB = VW * (int)sizeof(T), RV = PX / VW, NV = PY * RV, PER = (NV + NT - 1) / NT;
+    static_assert(VB == 8 || VB == 16, "8- or 16-byte copies");
+    struct alignas(VB) Vec { T v[VW]; };
+    constexpr int FXP = TX + 1;   // pitch of the x-face rows
     extern __shared__ __align__(16) unsigned char hyb_smem[];
     T *sm = reinterpret_cast<T *>(hyb_smem);   // [3][NP][PS]
+    T *fx = sm + 3 * NP * PS;                  // [3][TY][TX + 1]: face between columns c-1 and c at [row][c]
+    T *fy = fx + 3 * TY * FXP;                 // [3][TY + 1][TX]: face between rows r-1 and r at [r][col]
     const Dims &d = h.d;
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz, plane = Nx * Ny;
     const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k0 = blockIdx.z * KC, kend = min(k0 + KC, Nz);
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int i = i0 + tx, j = j0 + ty;
     const bool active = i < Nx && j < Ny;
-    // this thread's plane elements: global offset (row, column), the row's sign for U/W (-1: mirror), V zero,
-    // and the base profile of the row
     int off[PER];
     T sg[PER], ubq[PER];
     bool vz[PER];
@@ -82,140 +106,189 @@ __global__ void __launch_bounds__(256) k_adv_hybrid_tiled(HybArgs<T> h, const T 
     for (int q = 0; q < PER; ++q) {
         const int e = threadIdx.x + q * NT;
         off[q] = -1; sg[q] = T(1); ubq[q] = T(0); vz[q] = false;
-        if (e < PS) {
-            const int jj = e / PX, ii = e - jj * PX;
-            int gi = i0 - H + ii;
+        if (e < NV) {
+            const int jj = e / RV, vc = e - jj * RV;
+            int gi = i0 - HX + vc * VW;
             gi = gi < 0 ? gi + Nx : gi;
             while (gi >= Nx) gi -= Nx;
-            const int gj = j0 - H + jj;   // device row; the reference's J = gj + 2
+            const int gj = j0 - H + jj;
             int g;
             if (d.yper) {
                 g = gj % Ny; if (g < 0) g += Ny;
             } else if (gj < 0) {
-                g = 0; sg[q] = T(-1); vz[q] = true;                 // J <= 1: the bottom ghost (V: the wall face)
+                g = 0; sg[q] = T(-1); vz[q] = true;
             } else if (gj >= Ny) {
-                g = Ny - 1; sg[q] = T(-1); vz[q] = true;            // J >= nyg: the top ghost
+                g = Ny - 1; sg[q] = T(-1); vz[q] = true;
             } else {
                 g = gj;
-                vz[q] = gj >= Ny - 1;                               // V row Ny-1 (J = ny) is the top wall face
+                vz[q] = gj >= Ny - 1;
             }
             off[q] = g * Nx + gi;
             ubq[q] = h.ub[g];
         }
     }
-    auto slot = [&](int k) { return (k - k0 + H) & (NP - 1); };
     auto issue = [&](int k) {
-        const int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k), sl = slot(k);
-        const size_t kb = (size_t)kw * plane;
+        const int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k), sl = (k - k0 + H) & (NP - 1);
+        const int kb = kw * plane;   // 3 x cells < 2^31 (checked at context creation)
 #pragma unroll
         for (int q = 0; q < PER; ++q) {
             if (off[q] < 0) continue;
-            const int e = threadIdx.x + q * NT;
-            cp_async<sizeof(T)>(&sm[(0 * NP + sl) * PS + e], U + kb + off[q]);
-            cp_async<sizeof(T)>(&sm[(1 * NP + sl) * PS + e], V + kb + off[q]);
-            cp_async<sizeof(T)>(&sm[(2 * NP + sl) * PS + e], W + kb + off[q]);
+            const int e = (threadIdx.x + q * NT) * VW;
+            cp_async<VB>(&sm[(0 * NP + sl) * PS + e], U + kb + off[q]);
+            cp_async<VB>(&sm[(1 * NP + sl) * PS + e], V + kb + off[q]);
+            cp_async<VB>(&sm[(2 * NP + sl) * PS + e], W + kb + off[q]);
         }
     };
     auto fix = [&](int k) {
-        const int sl = slot(k);
+        const int sl = (k - k0 + H) & (NP - 1);
 #pragma unroll
         for (int q = 0; q < PER; ++q) {
             if (off[q] < 0) continue;
-            const int e = threadIdx.x + q * NT;
-            T &u = sm[(0 * NP + sl) * PS + e], &v = sm[(1 * NP + sl) * PS + e], &w = sm[(2 * NP + sl) * PS + e];
-            u = sg[q] * (u + ubq[q]);
-            w = sg[q] * w;
-            if (vz[q]) v = T(0);
+            const int e = (threadIdx.x + q * NT) * VW;
+            Vec *pu = reinterpret_cast<Vec *>(&sm[(0 * NP + sl) * PS + e]);
+            Vec *pv = reinterpret_cast<Vec *>(&sm[(1 * NP + sl) * PS + e]);
+            Vec *pw = reinterpret_cast<Vec *>(&sm[(2 * NP + sl) * PS + e]);
+            Vec u = *pu, w = *pw;
+#pragma unroll
+            for (int m = 0; m < VW; ++m) { u.v[m] = sg[q] * (u.v[m] + ubq[q]); w.v[m] = sg[q] * w.v[m]; }
+            *pu = u; *pw = w;
+            if (vz[q]) {
+                Vec z;
+#pragma unroll
+                for (int m = 0; m < VW; ++m) z.v[m] = T(0);
+                *pv = z;
+            }
         }
     };
+    // field f at tile row r, column c (0-based within the tile, -H .. TY+H-1 / -HX .. TX+HX-1), plane kk
+    auto A = [&](int f, int r, int c, int kk) -> T {
+        return sm[(f * NP + ((kk - k0 + H) & (NP - 1))) * PS + (r + H) * PX + (c + HX)];
+    };
     const int nyg = d.yper ? Ny + 3 : Ny + 2, ny = d.yper ? Ny + 2 : Ny + 1;
-    const int J = j + 2;
-    const T beta = h.beta, idx = h.inv_dx;
+    // beta * |0.5 (a + b)| = (0.5 beta) |a + b| exactly (scaling by a power of two)
+    const T bh = T(0.5) * h.beta;
+    // the tile row of the reference's (clamped) row Jr: device row Jr - 2
+    auto yrow = [&](int Jr, int n) -> int { return max(1, min(n, Jr)) - 2 - j0; };
+    // y-face rows: the face between tile rows r-1 and r is the reference's face jj = J(r) - 1 (adv_ord_y, the
+    // clamped stencil rows jj-2 .. jj+3 for U and W (n = nyg) and for V (n = ny))
+    struct YRows { int o, m2, m1, p2, p3; };
+    auto yrows = [&](int r, int n) -> YRows {
+        const int jj = j0 + r + 2 - 1;
+        return YRows{hyb_ord_y(jj, n, ORD), yrow(jj - 2, n), yrow(jj - 1, n), yrow(jj + 2, n), yrow(jj + 3, n)};
+    };
+    auto xface = [&](int comp, int r, int c, int kk) -> T {   // between columns c-1 and c
+        T uc;
+        if (comp == 0) uc = A(0, r, c - 1, kk) + A(0, r, c, kk);
+        else if (comp == 1) uc = A(0, r, c - 1, kk) + A(0, r + 1, c - 1, kk);
+        else uc = A(0, r, c - 1, kk) + A(0, r, c - 1, kk + 1);
+        T s;
+        if constexpr (ORD == 5)
+            s = HybW<5>::sum(A(comp, r, c - 3, kk), A(comp, r, c - 2, kk), A(comp, r, c - 1, kk), A(comp, r, c, kk),
+                             A(comp, r, c + 1, kk), A(comp, r, c + 2, kk));
+        else   // order 3 reads s(-1:2) only
+            s = HybW<3>::sum(T(0), A(comp, r, c - 2, kk), A(comp, r, c - 1, kk), A(comp, r, c, kk),
+                             A(comp, r, c + 1, kk), T(0));
+        return bh * fabs(uc) * s;
+    };
+    auto yface = [&](int comp, int r, int c, int kk, const YRows &y) -> T {   // between rows r-1 and r
+        T uc;
+        if (comp == 0) uc = A(1, r - 1, c, kk) + A(1, r - 1, c + 1, kk);
+        else if (comp == 1) uc = A(1, r - 1, c, kk) + A(1, r, c, kk);
+        else uc = A(1, r - 1, c, kk) + A(1, r - 1, c, kk + 1);
+        T s;
+        if constexpr (ORD == 5)
+            s = hyb_wsum(y.o, A(comp, y.m2, c, kk), A(comp, y.m1, c, kk), A(comp, r - 1, c, kk), A(comp, r, c, kk),
+                         A(comp, y.p2, c, kk), A(comp, y.p3, c, kk));
+        else
+            s = hyb_wsum(y.o, T(0), A(comp, y.m1, c, kk), A(comp, r - 1, c, kk), A(comp, r, c, kk),
+                         A(comp, y.p2, c, kk), T(0));
+        return bh * fabs(uc) * s;
+    };
+    // this cell's own column of each field in registers: q[f][m] is plane k - (NQ/2 - 1) + m, the planes of the
+    // stencil of the face between k and k+1; each plane adds one shared-memory read per field
+    constexpr int NQ = ORD == 5 ? 6 : 4, QC = NQ / 2 - 1;   // q[f][QC] is plane k
+    T q[3][NQ];
+    auto zface = [&](int comp, int kk) -> T {   // between planes kk and kk+1, from the queue of plane kk
+        T uc;
+        if (comp == 0) uc = q[2][QC] + A(2, ty, tx + 1, kk);
+        else if (comp == 1) uc = q[2][QC] + A(2, ty + 1, tx, kk);
+        else uc = q[2][QC] + q[2][QC + 1];
+        T s;
+        if constexpr (ORD == 5) s = HybW<5>::sum(q[comp][0], q[comp][1], q[comp][2], q[comp][3], q[comp][4], q[comp][5]);
+        else s = HybW<3>::sum(T(0), q[comp][0], q[comp][1], q[comp][2], q[comp][3], T(0));
+        return bh * fabs(uc) * s;
+    };
+    const YRows yg = yrows(ty, nyg), yv = yrows(ty, ny);          // this thread's face below its row
+    const YRows ygt = yrows(TY, nyg), yvt = yrows(TY, ny);        // warp TY-1: the faces above the tile
+    const T idx = h.inv_dx;
     const T dyU = h.my.idc[min(j, Ny - 1)], dyV = h.my.idf[min(j, Ny - 1)];
     for (int k = k0 - H; k <= k0 + H; ++k) issue(k);
     cp_async_commit();
     cp_async_wait_all();
     for (int k = k0 - H; k <= k0 + H; ++k) fix(k);
     __syncthreads();
+    T zb[3];   // the face below this cell (between planes k-1 and k)
+#pragma unroll
+    for (int f = 0; f < 3; ++f)
+#pragma unroll
+        for (int m = 0; m < NQ; ++m) q[f][m] = A(f, ty, tx, k0 - 1 - QC + m);
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) zb[comp] = zface(comp, k0 - 1);
     for (int k = k0; k < kend; ++k) {
         const bool more = k + 1 < kend;
         if (more) issue(k + H + 1);
         cp_async_commit();
-        if (active) {
-            // value of field f at this thread's cell offset by (dx, dy, dz)
-            auto S = [&](int f, int dx, int dy, int dz) -> T {
-                return sm[(f * NP + slot(k + dz)) * PS + (ty + H + dy) * PX + (tx + H + dx)];
-            };
-            // the clamped y rows of the reference, as offsets from this thread's row (J = j + 2)
-            auto yo = [&](int Jr, int n) -> int { return max(1, min(n, Jr)) - J; };
-            const T dzU = h.mz.idc[k], dzW = h.mz.idf[k];
-            const size_t p = ((size_t)k * Ny + j) * Nx + i;
-            // ---- u ----
-            T r = T(0);
 #pragma unroll
-            for (int m = 0; m <= 1; ++m) {
-                const T sgm = T(2 * m - 1);
-                const int a = m - 1;   // ii - i, jj - J, kk - k
-                T uc = T(0.5) * (S(0, a, 0, 0) + S(0, a + 1, 0, 0));
-                T s = HybW<ORD>::sum(S(0, a - 2, 0, 0), S(0, a - 1, 0, 0), S(0, a, 0, 0), S(0, a + 1, 0, 0),
-                                     S(0, a + 2, 0, 0), S(0, a + 3, 0, 0));
-                r = r - sgm * (beta * fabs(uc) * s) * idx;
-                const int jj = J + a;
-                uc = T(0.5) * (S(1, 0, a, 0) + S(1, 1, a, 0));
-                s = hyb_wsum(hyb_ord_y(jj, nyg, ORD), S(0, 0, yo(jj - 2, nyg), 0), S(0, 0, yo(jj - 1, nyg), 0),
-                             S(0, 0, a, 0), S(0, 0, a + 1, 0), S(0, 0, yo(jj + 2, nyg), 0), S(0, 0, yo(jj + 3, nyg), 0));
-                r = r - sgm * (beta * fabs(uc) * s) * dyU;
-                uc = T(0.5) * (S(2, 0, 0, a) + S(2, 1, 0, a));
-                s = HybW<ORD>::sum(S(0, 0, 0, a - 2), S(0, 0, 0, a - 1), S(0, 0, 0, a), S(0, 0, 0, a + 1),
-                                   S(0, 0, 0, a + 2), S(0, 0, 0, a + 3));
-                r = r - sgm * (beta * fabs(uc) * s) * dzU;
-            }
-            out[p] = r;
-            // ---- v ----
-            r = T(0);
-            if (j < d.NyV) {
+        for (int f = 0; f < 3; ++f) {
 #pragma unroll
-                for (int m = 0; m <= 1; ++m) {
-                    const T sgm = T(2 * m - 1);
-                    const int a = m - 1;
-                    T uc = T(0.5) * (S(0, a, 0, 0) + S(0, a, 1, 0));
-                    T s = HybW<ORD>::sum(S(1, a - 2, 0, 0), S(1, a - 1, 0, 0), S(1, a, 0, 0), S(1, a + 1, 0, 0),
-                                         S(1, a + 2, 0, 0), S(1, a + 3, 0, 0));
-                    r = r - sgm * (beta * fabs(uc) * s) * idx;
-                    const int jj = J + a;
-                    uc = T(0.5) * (S(1, 0, a, 0) + S(1, 0, a + 1, 0));
-                    s = hyb_wsum(hyb_ord_y(jj, ny, ORD), S(1, 0, yo(jj - 2, ny), 0), S(1, 0, yo(jj - 1, ny), 0),
-                                 S(1, 0, a, 0), S(1, 0, a + 1, 0), S(1, 0, yo(jj + 2, ny), 0), S(1, 0, yo(jj + 3, ny), 0));
-                    r = r - sgm * (beta * fabs(uc) * s) * dyV;
-                    uc = T(0.5) * (S(2, 0, 0, a) + S(2, 0, 1, a));
-                    s = HybW<ORD>::sum(S(1, 0, 0, a - 2), S(1, 0, 0, a - 1), S(1, 0, 0, a), S(1, 0, 0, a + 1),
-                                       S(1, 0, 0, a + 2), S(1, 0, 0, a + 3));
-                    r = r - sgm * (beta * fabs(uc) * s) * dzU;
-                }
-            }
-            out[d.cells + p] = r;
-            // ---- w ----
-            r = T(0);
-#pragma unroll
-            for (int m = 0; m <= 1; ++m) {
-                const T sgm = T(2 * m - 1);
-                const int a = m - 1;
-                T uc = T(0.5) * (S(0, a, 0, 0) + S(0, a, 0, 1));
-                T s = HybW<ORD>::sum(S(2, a - 2, 0, 0), S(2, a - 1, 0, 0), S(2, a, 0, 0), S(2, a + 1, 0, 0),
-                                     S(2, a + 2, 0, 0), S(2, a + 3, 0, 0));
-                r = r - sgm * (beta * fabs(uc) * s) * idx;
-                const int jj = J + a;
-                uc = T(0.5) * (S(1, 0, a, 0) + S(1, 0, a, 1));
-                s = hyb_wsum(hyb_ord_y(jj, nyg, ORD), S(2, 0, yo(jj - 2, nyg), 0), S(2, 0, yo(jj - 1, nyg), 0),
-                             S(2, 0, a, 0), S(2, 0, a + 1, 0), S(2, 0, yo(jj + 2, nyg), 0), S(2, 0, yo(jj + 3, nyg), 0));
-                r = r - sgm * (beta * fabs(uc) * s) * dyU;
-                uc = T(0.5) * (S(2, 0, 0, a) + S(2, 0, 0, a + 1));
-                s = HybW<ORD>::sum(S(2, 0, 0, a - 2), S(2, 0, 0, a - 1), S(2, 0, 0, a), S(2, 0, 0, a + 1),
-                                   S(2, 0, 0, a + 2), S(2, 0, 0, a + 3));
-                r = r - sgm * (beta * fabs(uc) * s) * dzW;
-            }
-            out[2 * d.cells + p] = r;
+            for (int m = 0; m + 1 < NQ; ++m) q[f][m] = q[f][m + 1];
+            q[f][NQ - 1] = A(f, ty, tx, k + NQ - 1 - QC);
         }
+        // every face value first (no shared store between the stencil reads), then the stores
+        T xb[3], yb[3], za[3], xe[3], ye[3];
+#pragma unroll
+        for (int comp = 0; comp < 3; ++comp) {
+            xb[comp] = xface(comp, ty, tx, k);
+            yb[comp] = yface(comp, ty, tx, k, comp == 1 ? yv : yg);
+            za[comp] = zface(comp, k);
+        }
+        const bool xedge = ty == 0 && tx < TY, yedge = ty == TY - 1;
+        if (xedge) {   // the right-hand x faces of the tile's rows (row tx)
+#pragma unroll
+            for (int comp = 0; comp < 3; ++comp) xe[comp] = xface(comp, tx, TX, k);
+        }
+        if (yedge) {   // the y faces above the tile
+#pragma unroll
+            for (int comp = 0; comp < 3; ++comp) ye[comp] = yface(comp, TY, tx, k, comp == 1 ? yvt : ygt);
+        }
+#pragma unroll
+        for (int comp = 0; comp < 3; ++comp) {
+            fx[(comp * TY + ty) * FXP + tx] = xb[comp];
+            fy[(comp * (TY + 1) + ty) * TX + tx] = yb[comp];
+            if (xedge) fx[(comp * TY + tx) * FXP + TX] = xe[comp];
+            if (yedge) fy[(comp * (TY + 1) + TY) * TX + tx] = ye[comp];
+        }
+        __syncthreads();
+        if (active) {
+            const T dzU = h.mz.idc[k], dzW = h.mz.idf[k];
+            const int p = (k * Ny + j) * Nx + i;
+#pragma unroll
+            for (int comp = 0; comp < 3; ++comp) {
+                const T dy = comp == 1 ? dyV : dyU, dz = comp == 2 ? dzW : dzU;
+                const T xa = fx[(comp * TY + ty) * FXP + tx + 1], ya = fy[(comp * (TY + 1) + ty + 1) * TX + tx];
+                T r = T(0);
+                r = r - T(-1) * xb[comp] * idx;
+                r = r - T(-1) * yb[comp] * dy;
+                r = r - T(-1) * zb[comp] * dz;
+                r = r - T(1) * xa * idx;
+                r = r - T(1) * ya * dy;
+                r = r - T(1) * za[comp] * dz;
+                if (comp == 1 && j >= d.NyV) r = T(0);   // v rows beyond the last interior face
+                out[comp * (int)d.cells + p] = r;
+            }
+        }
+#pragma unroll
+        for (int comp = 0; comp < 3; ++comp) zb[comp] = za[comp];
         cp_async_wait_all();
         if (more) fix(k + H + 1);
         __syncthreads();

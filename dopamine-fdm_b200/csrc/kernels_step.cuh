@@ -23,7 +23,7 @@ template <typename T> struct StepArgs {
     // representable in the storage type; ubd is the same profile in double.
     const T *ub;
     const double *ubd;
-    // advection_scheme = 2: the dissipative terms of k_adv_hybrid_tiled (u, v, w blocks of `cells`), added to the
+    // advection_scheme = 2: the dissipative terms of k_adv_hybrid_faces (u, v, w blocks of `cells`), added to the
     // right-hand sides; null otherwise
     const T *adv;
     // fused correction of the previous stage (CORR kernels): its potential phi; the plane loads then hold u* and
