@@ -125,6 +125,7 @@ struct dfdm_ctx {
     int lx = 8, tzx = 8;
     int kc_stage = 8, kc_sgs = 8;               // z-planes per block of the tiled kernels
     int kc_stage2 = 8;                          // the same for the packed FP32 stage kernel
+    int kc_hyb = 32;                            // the same for the hybrid-scheme kernel
     int stage_variant = 0;                      // FP32 stage kernel in use: 0 one cell per thread, 1 packed pairs
     double stage_ms[2] = {-1.0, -1.0};          // autotuner timings of the two variants (ms per launch), -1 = not timed
     size_t smem_x = 0, smem_z = 0, smem_y = 0;
@@ -294,12 +295,29 @@ constexpr int TILE_X = 32, TILE_Y = 8;   // (i,j) tile of the 2.5-D blocked kern
 const int TILE_X2 = 64;   // x cells per block of the packed FP32 stage kernel (32 threads x 2 cells)
 dim3 tile_grid(const Dims &d, int kc, int tx = TILE_X) { return dim3((d.Nx + tx - 1) / tx, (d.Ny + TILE_Y - 1) / TILE_Y, (d.Nz + kc - 1) / kc); }
 // z-planes per block: enough blocks for about four waves at the measured occupancy, at most 32 planes
-int choose_kc(const Dims &d, int blocks_per_sm, int nsm, int tx = TILE_X) {
-    long long cols = (long long)((d.Nx + tx - 1) / tx) * ((d.Ny + TILE_Y - 1) / TILE_Y);
-    long long want = 4LL * nsm * std::max(1, blocks_per_sm);
-    long long chunks = std::max(1LL, (want + cols - 1) / cols);
-    int kc = (int)((d.Nz + chunks - 1) / chunks);
-    return std::max(2, std::min(32, kc));
+// z-planes per block of the 2.5-D tiled kernels.  A block of a (tx x ty) column runs kc planes after loading `halo`
+// extra planes; blocks_per_sm of them share an SM.  The chunking minimises (kc + halo) x g, g the waves the launch
+// takes: full waves of blocks_per_sm x nsm blocks, then a last wave as long as its most loaded SM (its blocks over
+// blocks_per_sm) but never shorter than 0.6 of a wave (a lone block hides little latency).  Measured at 256 x 192 x
+// 256 cells: the packed stage kernel and the order-3 hybrid kernel are fastest with 3 chunks of 86 planes (one
+// wave), the order-5 hybrid kernel (3 blocks per SM) with 6 chunks of 43; the earlier fixed four-wave target (13
+// chunks of 20 planes, 4.2 waves) cost about 1.5 % of a step.
+int choose_kc(const Dims &d, int blocks_per_sm, int nsm, int tx = TILE_X, int ty = TILE_Y, int halo = 2) {
+    const long long cols = (long long)((d.Nx + tx - 1) / tx) * ((d.Ny + ty - 1) / ty);
+    const int bps = std::max(1, blocks_per_sm), sms = std::max(1, nsm);
+    const long long cap = (long long)bps * sms;
+    double best = -1.0;
+    int best_kc = d.Nz;
+    for (int chunks = 1; chunks <= d.Nz; ++chunks) {
+        const int kc = (d.Nz + chunks - 1) / chunks;
+        if (kc < 2 && d.Nz >= 2) break;
+        const long long blocks = cols * ((d.Nz + kc - 1) / kc), rem = blocks % cap;
+        double g = (double)(blocks / cap);
+        if (rem) g += std::max(0.6, (double)((rem + sms - 1) / sms) / bps);
+        const double cost = g * (kc + halo);
+        if (best < 0.0 || cost < best - 1e-9) { best = cost; best_kc = kc; }
+    }
+    return std::max(1, best_kc);
 }
 
 template <typename T> struct Impl {
@@ -374,8 +392,6 @@ template <typename T> struct Impl {
         return DFDM_OK;
     }
 
-    // the hybrid-scheme kernel: z-planes per block (its shared memory: hyb_faces_smem_bytes)
-    static constexpr int HYB_KC = 32;
 
     static int setup_kernels(dfdm_ctx *c) {
         const Dims &d = c->d;
@@ -421,16 +437,21 @@ template <typename T> struct Impl {
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cfl<T, true>, 256, 0));
         c->cfl_blocks = (int)std::max(1LL, std::min((long long)std::max(1, occ) * nsm, ((long long)d.Ny * d.Nz + 7) / 8));
         if (c->prm.advection_scheme == 2) {
-            CK(cudaFuncSetAttribute(k_adv_hybrid_faces<T, 3, HYB_KC, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)hyb_faces_smem_bytes<T, 3>()));
-            CK(cudaFuncSetAttribute(k_adv_hybrid_faces<T, 5, HYB_KC, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)hyb_faces_smem_bytes<T, 5>()));
-            if constexpr (sizeof(T) == 4) {
-                CK(cudaFuncSetAttribute(k_adv_hybrid_faces<T, 3, HYB_KC, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)hyb_faces_smem_bytes<T, 3>()));
-                CK(cudaFuncSetAttribute(k_adv_hybrid_faces<T, 5, HYB_KC, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)hyb_faces_smem_bytes<T, 5>()));
-            }
+            const bool quads = sizeof(T) == 4 && d.Nx % 4 == 0;
+            const void *fn = nullptr;
+            auto attr = [&](const void *k, size_t bytes) {
+                CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+                return DFDM_OK;
+            };
+            if (int rc = attr((const void *)k_adv_hybrid_faces<T, 3, 2>, hyb_faces_smem_bytes<T, 3>())) return rc;
+            if (int rc = attr((const void *)k_adv_hybrid_faces<T, 5, 2>, hyb_faces_smem_bytes<T, 5>())) return rc;
+            if (int rc = attr((const void *)k_adv_hybrid_faces<T, 3, 16 / sizeof(T)>, hyb_faces_smem_bytes<T, 3>())) return rc;
+            if (int rc = attr((const void *)k_adv_hybrid_faces<T, 5, 16 / sizeof(T)>, hyb_faces_smem_bytes<T, 5>())) return rc;
+            const bool o5 = c->prm.adv_order == 5;
+            fn = o5 ? (quads ? (const void *)k_adv_hybrid_faces<T, 5, 16 / sizeof(T)> : (const void *)k_adv_hybrid_faces<T, 5, 2>)
+                    : (quads ? (const void *)k_adv_hybrid_faces<T, 3, 16 / sizeof(T)> : (const void *)k_adv_hybrid_faces<T, 3, 2>);
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, o5 ? hyb_faces_smem_bytes<T, 5>() : hyb_faces_smem_bytes<T, 3>()));
+            c->kc_hyb = choose_kc(d, occ, nsm, 32, 8, o5 ? 6 : 4);
         }
         return setup_fft2l(c);
     }
@@ -675,16 +696,17 @@ template <typename T> struct Impl {
             h.my = metric_view<T>(c->my_t, d.Ny);
             h.mz = metric_view<T>(c->mz_t, d.Nz);
             h.ub = (const T *)c->d_ub;
-            const dim3 g((d.Nx + 31) / 32, (d.Ny + 7) / 8, (d.Nz + HYB_KC - 1) / HYB_KC);
+            const int kc = c->kc_hyb;
+            const dim3 g((d.Nx + 31) / 32, (d.Ny + 7) / 8, (d.Nz + kc - 1) / kc);
             // 16-byte row copies in FP32 when Nx % 4 == 0, else 8-byte pairs (Nx is even)
             const bool quads = sizeof(T) == 4 && d.Nx % 4 == 0;
             const size_t sb = c->prm.adv_order == 5 ? hyb_faces_smem_bytes<T, 5>() : hyb_faces_smem_bytes<T, 3>();
             if (c->prm.adv_order == 5) {
-                if (quads) k_adv_hybrid_faces<T, 5, HYB_KC, 16 / sizeof(T)><<<g, 256, sb, st>>>(h, f(c->u), f(c->v), f(c->w), f(c->adv));
-                else k_adv_hybrid_faces<T, 5, HYB_KC, 2><<<g, 256, sb, st>>>(h, f(c->u), f(c->v), f(c->w), f(c->adv));
+                if (quads) k_adv_hybrid_faces<T, 5, 16 / sizeof(T)><<<g, 256, sb, st>>>(h, kc, f(c->u), f(c->v), f(c->w), f(c->adv));
+                else k_adv_hybrid_faces<T, 5, 2><<<g, 256, sb, st>>>(h, kc, f(c->u), f(c->v), f(c->w), f(c->adv));
             } else {
-                if (quads) k_adv_hybrid_faces<T, 3, HYB_KC, 16 / sizeof(T)><<<g, 256, sb, st>>>(h, f(c->u), f(c->v), f(c->w), f(c->adv));
-                else k_adv_hybrid_faces<T, 3, HYB_KC, 2><<<g, 256, sb, st>>>(h, f(c->u), f(c->v), f(c->w), f(c->adv));
+                if (quads) k_adv_hybrid_faces<T, 3, 16 / sizeof(T)><<<g, 256, sb, st>>>(h, kc, f(c->u), f(c->v), f(c->w), f(c->adv));
+                else k_adv_hybrid_faces<T, 3, 2><<<g, 256, sb, st>>>(h, kc, f(c->u), f(c->v), f(c->w), f(c->adv));
             }
             CKL();
             return DFDM_OK;

@@ -61,7 +61,7 @@ template <typename T, int ORD> constexpr size_t hyb_faces_smem_bytes() {
     return ((size_t)3 * 8 * 40 * (8 + 2 * (ORD == 5 ? 3 : 2)) + 3 * 8 * 33 + 3 * 9 * 32) * sizeof(T);
 }
 
-// A block owns a 32 x 8 column of cells and marches through KC z-planes; the planes of U, V, W rotate through eight
+// A block owns a 32 x 8 column of cells and marches through kc z-planes; the planes of U, V, W rotate through eight
 // shared tiles filled by cp.async H+1 planes ahead (y halo H = 2 rows for order 3, 3 for order 5; x halo 4 cells).
 // After a plane's copies land, each thread turns the vectors it copied into the values the reference reads: U (plus
 // the base profile) and W mirrored and V zero on wall rows, rows beyond a wall holding the clamped row's value
@@ -77,9 +77,9 @@ template <typename T, int ORD> constexpr size_t hyb_faces_smem_bytes() {
 //   r = -(-1)Fx(-) dx' - (-1)Fy(-) dy' - (-1)Fz(-) dz' - Fx(+) dx' - Fy(+) dy' - Fz(+) dz'
 // in the order of adv_dflux (src/adv_hybrid.f90:136-210): the lower faces, then the upper faces, x, y, z.  y rows
 // are clamped to the reference's ranges by absolute row.
-template <typename T, int ORD, int KC, int VW>
+template <typename T, int ORD, int VW>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (ORD == 5 ? 3 : 4) : (ORD == 5 ? 1 : 2))
-    k_adv_hybrid_faces(HybArgs<T> h, const T *__restrict__ U, const T *__restrict__ V, const T *__restrict__ W,
+    k_adv_hybrid_faces(HybArgs<T> h, int kc, const T *__restrict__ U, const T *__restrict__ V, const T *__restrict__ W,
                        T *__restrict__ out) {
     constexpr int TX = 32, TY = 8, H = ORD == 5 ? 3 : 2, HX = 4, PX = TX + 2 * HX, PY = TY + 2 * H, PS = PX * PY;
     constexpr int NT = TX * TY, NP = 8;
@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (ORD == 5 ? 3 : 4) : (OR
     T *fy = fx + 3 * TY * FXP;                 // [3][TY + 1][TX]: face between rows r-1 and r at [r][col]
     const Dims &d = h.d;
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz, plane = Nx * Ny;
-    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k0 = blockIdx.z * KC, kend = min(k0 + KC, Nz);
+    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k0 = blockIdx.z * kc, kend = min(k0 + kc, Nz);
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int i = i0 + tx, j = j0 + ty;
     const bool active = i < Nx && j < Ny;
