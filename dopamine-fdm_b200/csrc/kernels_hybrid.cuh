@@ -69,8 +69,8 @@ template <typename T, int ORD> constexpr size_t hyb_faces_smem_bytes() {
 // base profile's rounding: the terms are small).
 // Each face flux is evaluated once.  The flux through a face, beta |u_c| D (without the cell's metric), depends
 // only on the face, so a cell's two faces per direction are shared with its neighbours:
-//   x: each thread evaluates the face on its left, lanes 0..7 of warp 0 the right-hand faces of the tile's rows;
-//   y: each thread the face below its row, warp 7 the faces above the tile;
+//   x: each thread evaluates the face on its left; y: each thread the face below its row; the tile's right-hand x
+//      faces and its top y faces are spread over warps 0..5, one face per thread;
 //   z: each thread the face above its cell, carried in registers to the next plane as the face below; the cell's
 //      own column of each field (the z stencil) is a register queue that takes one new plane per step.
 // x and y faces pass through shared memory (a barrier between their stores and the reads).  The cell then assembles
@@ -245,29 +245,25 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (ORD == 5 ? 3 : 4) : (OR
             q[f][NQ - 1] = A(f, ty, tx, k + NQ - 1 - QC);
         }
         // every face value first (no shared store between the stencil reads), then the stores
-        T xb[3], yb[3], za[3], xe[3], ye[3];
+        T xb[3], yb[3], za[3];
 #pragma unroll
         for (int comp = 0; comp < 3; ++comp) {
             xb[comp] = xface(comp, ty, tx, k);
             yb[comp] = yface(comp, ty, tx, k, comp == 1 ? yv : yg);
             za[comp] = zface(comp, k);
         }
-        const bool xedge = ty == 0 && tx < TY, yedge = ty == TY - 1;
-        if (xedge) {   // the right-hand x faces of the tile's rows (row tx)
-#pragma unroll
-            for (int comp = 0; comp < 3; ++comp) xe[comp] = xface(comp, tx, TX, k);
-        }
-        if (yedge) {   // the y faces above the tile
-#pragma unroll
-            for (int comp = 0; comp < 3; ++comp) ye[comp] = yface(comp, TY, tx, k, comp == 1 ? yvt : ygt);
-        }
+        // the tile's edge faces, one per thread of warps 0..5: warp c < 3 the y faces above the tile of component c,
+        // lanes 0..7 of warp 3 + c the right-hand x faces of the tile's rows (row = lane) of component c
+        T ex = T(0);
+        if (ty < 3) ex = yface(ty, TY, tx, k, ty == 1 ? yvt : ygt);
+        else if (ty < 6 && tx < TY) ex = xface(ty - 3, tx, TX, k);
 #pragma unroll
         for (int comp = 0; comp < 3; ++comp) {
             fx[(comp * TY + ty) * FXP + tx] = xb[comp];
             fy[(comp * (TY + 1) + ty) * TX + tx] = yb[comp];
-            if (xedge) fx[(comp * TY + tx) * FXP + TX] = xe[comp];
-            if (yedge) fy[(comp * (TY + 1) + TY) * TX + tx] = ye[comp];
         }
+        if (ty < 3) fy[(ty * (TY + 1) + TY) * TX + tx] = ex;
+        else if (ty < 6 && tx < TY) fx[((ty - 3) * TY + tx) * FXP + TX] = ex;
         __syncthreads();
         if (active) {
             const T dzU = h.mz.idc[k], dzW = h.mz.idf[k];
