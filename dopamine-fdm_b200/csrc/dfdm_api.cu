@@ -1808,6 +1808,92 @@ int dfdm_write_snapshot(dfdm_ctx *c, const char *path) {
     return DFDM_OK;
 }
 
+// write_box_snapshot (src/input_output.f90:1699-1767) of a one-rank run: field_box (:1586-1598) gives each field's
+// stagger flags st and global range gl:gh over the face box f1:f2 (a staggered direction holds faces f1..f2, a centred
+// one cells f1..f2-1); fill_box_block (:1623-1659) maps global index g to the ghosted array index g + 1 - st, and with
+// location 1 averages each velocity to the cell centres over the two faces of its own direction.
+int dfdm_write_box_snapshot(dfdm_ctx *c, const char *path, const int32_t f1[3], const int32_t f2[3], int location,
+                            int32_t step) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (!path || !f1 || !f2) return fail(DFDM_ERR_INVALID, "null argument");
+    if (location != 0 && location != 1)
+        return fail(DFDM_ERR_INVALID, "snapshot_location must be 0 (staggered) or 1 (cell-centred)");
+    const int nf3[3] = {c->nx, c->ny, c->nz};
+    for (int a = 0; a < 3; ++a)
+        if (!(f1[a] >= 1 && f2[a] <= nf3[a] && f1[a] < f2[a]))
+            return fail(DFDM_ERR_INVALID, "chunk box is empty or outside the domain in direction " + std::to_string(a + 1));
+    const size_t nU = (size_t)c->nx * c->nyg * c->nzg, nV = (size_t)c->nxg * c->ny * c->nzg;
+    const size_t nW = (size_t)c->nxg * c->nyg * c->nz, nP = (size_t)c->nxg * c->nyg * c->nzg;
+    std::vector<double> U(nU), V(nV), W(nW), P(nP), NU;
+    int rc = dfdm_get_state(c, U.data(), V.data(), W.data(), P.data());
+    if (rc) return rc;
+    if (c->les) {   // sgs_model /= 0
+        NU.resize(nP);
+        if ((rc = dfdm_get_nu_t(c, NU.data()))) return rc;
+    }
+    double t = 0.0;
+    if ((rc = dfdm_get_time(c, &t))) return rc;
+    struct Field { const char *name; const double *a; int ic, n1, n2; };
+    std::vector<Field> fields = {{"U", U.data(), 1, c->nx, c->nyg}, {"V", V.data(), 2, c->nxg, c->ny},
+                                 {"W", W.data(), 3, c->nxg, c->nyg}, {"P", P.data(), 0, c->nxg, c->nyg}};
+    if (c->les) fields.push_back({"nu_t", NU.data(), 0, c->nxg, c->nyg});
+    auto box = [&](int ic, int32_t st[3], int32_t gl[3], int32_t gh[3]) {
+        for (int a = 0; a < 3; ++a) st[a] = (location == 0 && ic == a + 1) ? 1 : 0;
+        for (int a = 0; a < 3; ++a) { gl[a] = f1[a]; gh[a] = f2[a] - 1 + st[a]; }
+    };
+    FileCloser fc{fopen(path, "wb")};
+    if (!fc.f) return fail(DFDM_ERR_INVALID, std::string("cannot open ") + path + " for writing");
+    bool ok = true;
+    auto put = [&](const void *p, size_t sz, size_t n) { ok = ok && fwrite(p, sz, n, fc.f) == n; };
+    const int32_t head[4] = {SNAP_MAGIC, (int32_t)location, step, (int32_t)fields.size()};
+    put(head, sizeof(int32_t), 4);
+    put(&t, sizeof(double), 1);
+    put(f1, sizeof(int32_t), 3);
+    put(f2, sizeof(int32_t), 3);
+    const std::vector<std::vector<double>> mesh = mesh_arrays(c);   // x, y, z, xm, ym, zm
+    for (int a = 0; a < 3; ++a) {
+        put(mesh[a].data() + (f1[a] - 1), sizeof(double), (size_t)(f2[a] - f1[a] + 1));
+        put(mesh[3 + a].data() + (f1[a] - 1), sizeof(double), (size_t)(f2[a] - f1[a]));
+    }
+    for (const Field &fl : fields) {
+        char name[8];
+        std::memset(name, ' ', sizeof(name));
+        std::memcpy(name, fl.name, std::strlen(fl.name));
+        int32_t st[3], gl[3], gh[3];
+        box(fl.ic, st, gl, gh);
+        put(name, 1, 8);
+        put(st, sizeof(int32_t), 3);
+        put(gl, sizeof(int32_t), 3);
+        put(gh, sizeof(int32_t), 3);
+    }
+    for (const Field &fl : fields) {
+        int32_t st[3], gl[3], gh[3];
+        box(fl.ic, st, gl, gh);
+        const bool centred = location == 1 && fl.ic > 0;
+        std::vector<double> buf;
+        buf.reserve((size_t)(gh[0] - gl[0] + 1) * (gh[1] - gl[1] + 1) * (gh[2] - gl[2] + 1));
+        auto at = [&](int i, int j, int k) {   // 1-based ghosted indices
+            return fl.a[((size_t)(k - 1) * fl.n2 + (j - 1)) * fl.n1 + (i - 1)];
+        };
+        for (int k = gl[2]; k <= gh[2]; ++k)
+            for (int j = gl[1]; j <= gh[1]; ++j)
+                for (int i = gl[0]; i <= gh[0]; ++i) {
+                    const int ia = i + 1 - st[0], ja = j + 1 - st[1], ka = k + 1 - st[2];
+                    double v;
+                    if (centred && fl.ic == 1) v = 0.5 * (at(ia - 1, ja, ka) + at(ia, ja, ka));
+                    else if (centred && fl.ic == 2) v = 0.5 * (at(ia, ja - 1, ka) + at(ia, ja, ka));
+                    else if (centred && fl.ic == 3) v = 0.5 * (at(ia, ja, ka - 1) + at(ia, ja, ka));
+                    else v = at(ia, ja, ka);
+                    buf.push_back(v);
+                }
+        put(buf.data(), sizeof(double), buf.size());
+    }
+    if (!ok || fclose(fc.f) != 0) { fc.f = nullptr; return fail(DFDM_ERR_INVALID, std::string("write to ") + path + " failed"); }
+    fc.f = nullptr;
+    return DFDM_OK;
+}
+
 int dfdm_read_snapshot(dfdm_ctx *c, const char *path) {
     g_err.clear();
     if (int rc = check_ctx(c)) return rc;

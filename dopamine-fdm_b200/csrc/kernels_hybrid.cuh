@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (ORD == 5 ? 3 : 4) : (OR
     // this cell's own column of each field in registers: q[f][m] is plane k - (NQ/2 - 1) + m, the planes of the
     // stencil of the face between k and k+1; each plane adds one shared-memory read per field
     constexpr int NQ = ORD == 5 ? 6 : 4, QC = NQ / 2 - 1;   // q[f][QC] is plane k
-    T q[3][NQ];
+    T q[3][NQ] = {};   // filled from shared memory once the first planes have landed
     auto zface = [&](int comp, int kk) -> T {   // between planes kk and kk+1, from the queue of plane kk
         T uc;
         if (comp == 0) uc = q[2][QC] + A(2, ty, tx + 1, kk);

@@ -33,7 +33,8 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_launch_count", "dfdm_solve_poisson_noalloc", "dfdm_write_snapshot", "dfdm_read_snapshot",
            "dfdm_compute_cfl", "dfdm_set_stage_variant", "dfdm_get_stage_variant", "dfdm_set_adaptive_dt",
            "dfdm_get_dt", "dfdm_set_landing_time", "dfdm_output_monitor", "dfdm_output_monitor_async",
-           "dfdm_set_fused_correction", "dfdm_get_fused_correction", "dfdm_set_state_async", "dfdm_get_state_async"]
+           "dfdm_set_fused_correction", "dfdm_get_fused_correction", "dfdm_set_state_async", "dfdm_get_state_async",
+           "dfdm_write_box_snapshot"]
 
 
 class DfdmError(RuntimeError):
@@ -95,6 +96,8 @@ def load(build_if_missing: bool = True):
         "dfdm_solve_poisson_noalloc": (c_int, [c_void_p, P, P]),
         "dfdm_write_snapshot": (c_int, [c_void_p, c_char_p]),
         "dfdm_read_snapshot": (c_int, [c_void_p, c_char_p]),
+        "dfdm_write_box_snapshot": (c_int, [c_void_p, c_char_p, POINTER(ctypes.c_int32), POINTER(ctypes.c_int32), c_int,
+                                            ctypes.c_int32]),
         "dfdm_compute_cfl": (c_int, [c_void_p, P, P]),
         "dfdm_set_stage_variant": (c_int, [c_void_p, c_int]),
         "dfdm_get_stage_variant": (c_int, [c_void_p, POINTER(ctypes.c_int), P, P]),
@@ -285,6 +288,13 @@ class Solver:
     def read_snapshot(self, path: str) -> None:
         """U, V, W, P (and the wall-model filter from <path>.wmf) from a restart file of this grid."""
         _check(load().dfdm_read_snapshot(self.h, os.fsencode(path)))
+
+    def write_box_snapshot(self, path: str, f1, f2, location: int = 0, step: int = 0) -> None:
+        """The reference's chunked / cell-centred box snapshot (write_box_snapshot) of the face box f1..f2 (1-based
+        faces per direction; dfdm.snapshot.resolve_chunk_box turns the &IO chunk inputs into f1, f2)."""
+        a = (ctypes.c_int32 * 3)(*[int(v) for v in f1])
+        b = (ctypes.c_int32 * 3)(*[int(v) for v in f2])
+        _check(load().dfdm_write_box_snapshot(self.h, os.fsencode(path), a, b, int(location), int(step)))
 
     def compute_bulk_velocity(self) -> float:
         v = c_double(0.0)

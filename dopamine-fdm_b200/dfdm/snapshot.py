@@ -10,6 +10,17 @@ a little-endian stream with no record markers:
 (The mesh blocks come in the order x, y, z, xm, ym, zm.)  A file that starts with -4242 is a cell-centred/chunked
 box snapshot, which cannot serve as a restart.
 
+The box snapshot (write_box_snapshot, :1699-1767) holds the face box f1..f2 (1-based faces) of every field:
+  int32 -4242, snapshot_location, step, nfields; float64 t; int32 f1(3), f2(3);
+  per direction float64 faces x(f1:f2) and centres xm(f1:f2-1);
+  per field char name(8) (blank-padded), int32 st(3), gl(3), gh(3);
+  then each field's box gl:gh as float64 in Fortran order.
+field_box (:1586-1598): st(a) = 1 for the velocity of direction a when snapshot_location = 0, else 0; gl = f1,
+gh = f2 - 1 + st.  fill_box_block (:1623-1659) reads global index g of a one-rank run at ghosted index g + 1 - st and,
+with snapshot_location = 1, averages each velocity over the two faces of its own direction.  The reference writes it
+for chunked_snapshot (the box resolve_chunk_box gives, :1538-1583) and for a cell-centred full snapshot
+(snapshot_location = 1, f1 = 1, f2 = n).
+
 The wall-model filter state goes next to it as <file>.wmf (write_wm_filter_state, :1990-2009): six blocks
 wmf_ux, wmf_wx, wmf_tx (nx,2,nzg) and wmf_uz, wmf_wz, wmf_tz (nxg,2,nz), with the x/z ghost planes written as zero.
 """
@@ -125,4 +136,124 @@ def read_wmf(path: str, case: Case) -> Optional[Dict[str, np.ndarray]]:
             out[key] = _read_block(fh, (nx, 2, nzg), "wmf_" + key)
         for key in ("uz", "wz", "tz"):
             out[key] = _read_block(fh, (nxg, 2, nz), "wmf_" + key)
+    return out
+
+
+def coordinate_face_range(xf: np.ndarray, s: float, e: float) -> Tuple[int, int, bool]:
+    """coordinate_face_range (src/input_output.f90:1517-1535): the faces nearest the clamped start and end
+    coordinates (1-based, first of equal distances), widened to one cell when they coincide."""
+    nf = xf.size
+    ok = (s <= e) and (e >= xf[0]) and (s <= xf[nf - 1])
+    f1 = int(np.argmin(np.abs(xf - min(max(s, xf[0]), xf[nf - 1])))) + 1
+    f2 = int(np.argmin(np.abs(xf - min(max(e, xf[0]), xf[nf - 1])))) + 1
+    if f2 <= f1:
+        if f1 < nf:
+            f2 = f1 + 1
+        else:
+            f1 = f2 - 1
+    return f1, f2, ok
+
+
+def resolve_chunk_box(case: Case, x_start: float, x_end: float, y_start: float, y_end: float, z_start: float,
+                      z_end: float) -> Tuple[Tuple[int, int, int], Tuple[int, int, int]]:
+    """check_snapshot_inputs and resolve_chunk_box (src/input_output.f90:913-925, 1538-1583): the &IO chunk box as
+    1-based face indices f1, f2.  All six inputs negative: index mode, -v is the 1-based face (0 <= -v-1 < n);
+    none negative: coordinates, mapped by coordinate_face_range.  Raises ValueError where the reference aborts."""
+    vals = [x_start, x_end, y_start, y_end, z_start, z_end]
+    nneg = sum(1 for v in vals if v < 0.0)
+    if nneg not in (0, 6):
+        raise ValueError("chunk box x/y/z_start/end must be all lengths (>= 0) or all negative face indices")
+    faces_ = cases.faces(case)
+    nf = (case.nx, case.ny, case.nz)
+    index_mode = x_start < 0.0
+    f1, f2 = [0, 0, 0], [0, 0, 0]
+    for a, (st, en) in enumerate(((x_start, x_end), (y_start, y_end), (z_start, z_end))):
+        if index_mode:
+            n1 = int(round(-st)) - 1
+            n2 = int(round(-en)) - 1
+            ok = n1 >= 0 and n2 <= nf[a] - 1 and n1 < n2
+            f1[a], f2[a] = n1 + 1, n2 + 1
+        else:
+            f1[a], f2[a], ok = coordinate_face_range(faces_[a], st, en)
+        if not ok:
+            raise ValueError(f"chunk box is empty or outside the domain in direction {a + 1}")
+    return (f1[0], f1[1], f1[2]), (f2[0], f2[1], f2[2])
+
+
+def field_box(ic: int, f1, f2, location: int) -> Tuple[Tuple[int, ...], Tuple[int, ...], Tuple[int, ...]]:
+    """field_box: stagger flags and the global index range gl:gh of field kind ic (0 scalar, 1/2/3 = U/V/W)."""
+    st = [0, 0, 0]
+    if location == 0 and ic > 0:
+        st[ic - 1] = 1
+    gl = tuple(int(v) for v in f1)
+    gh = tuple(int(f2[a]) - 1 + st[a] for a in range(3))
+    return tuple(st), gl, gh
+
+
+def box_block(A: np.ndarray, ic: int, f1, f2, location: int) -> np.ndarray:
+    """fill_box_block of a one-rank run: the box gl:gh of the ghosted array A (reference shape, Fortran order)."""
+    st, gl, gh = field_box(ic, f1, f2, location)
+    sl = tuple(slice(gl[a] - st[a], gh[a] - st[a] + 1) for a in range(3))   # 0-based ghosted index g - st
+    if location == 1 and ic > 0:
+        a = ic - 1
+        lo = list(sl)
+        lo[a] = slice(sl[a].start - 1, sl[a].stop - 1)
+        return 0.5 * (A[tuple(lo)] + A[sl])
+    return np.array(A[sl], dtype=np.float64)
+
+
+def write_box(path: str, case: Case, f1, f2, U, V, W, P, nu_t=None, location: int = 0, step: int = 0,
+              t: float = 0.0) -> None:
+    """write_box_snapshot of a one-rank run (the restatement that the library's dfdm_write_box_snapshot is checked
+    against)."""
+    if location not in (0, 1):
+        raise ValueError("snapshot_location must be 0 (staggered) or 1 (cell-centred)")
+    fields = [("U", U, 1), ("V", V, 2), ("W", W, 3), ("P", P, 0)]
+    if nu_t is not None:
+        fields.append(("nu_t", nu_t, 0))
+    faces_ = cases.faces(case)
+    with open(path, "wb") as fh:
+        np.asarray([SNAP_MAGIC, location, step, len(fields)], dtype="<i4").tofile(fh)
+        np.asarray([t], dtype="<f8").tofile(fh)
+        np.asarray(list(f1) + list(f2), dtype="<i4").tofile(fh)
+        for a in range(3):
+            f = faces_[a]
+            np.asarray(f[f1[a] - 1:f2[a]], dtype="<f8").tofile(fh)
+            np.asarray(_centres(f)[f1[a] - 1:f2[a] - 1], dtype="<f8").tofile(fh)
+        for name, _, ic in fields:
+            fh.write(name.ljust(8).encode("ascii"))
+            st, gl, gh = field_box(ic, f1, f2, location)
+            np.asarray(list(st) + list(gl) + list(gh), dtype="<i4").tofile(fh)
+        for _, A, ic in fields:
+            fh.write(np.asfortranarray(box_block(np.asarray(A), ic, f1, f2, location), dtype="<f8").tobytes(order="F"))
+
+
+def read_box(path: str) -> Dict[str, object]:
+    """A box snapshot: its header (location, step, t, f1, f2, the face and centre coordinates) and fields by name."""
+    with open(path, "rb") as fh:
+        head = np.fromfile(fh, dtype="<i4", count=4)
+        if head.size != 4 or int(head[0]) != SNAP_MAGIC:
+            raise ValueError("not a box snapshot (no -4242 magic)")
+        out: Dict[str, object] = {"location": int(head[1]), "step": int(head[2])}
+        nf = int(head[3])
+        out["t"] = float(np.fromfile(fh, dtype="<f8", count=1)[0])
+        ff = np.fromfile(fh, dtype="<i4", count=6)
+        f1, f2 = tuple(int(v) for v in ff[:3]), tuple(int(v) for v in ff[3:])
+        out["f1"], out["f2"] = f1, f2
+        for a, key in enumerate("xyz"):
+            out[key] = np.fromfile(fh, dtype="<f8", count=f2[a] - f1[a] + 1)
+            out[key + "m"] = np.fromfile(fh, dtype="<f8", count=f2[a] - f1[a])
+        heads = []
+        for _ in range(nf):
+            name = fh.read(8).decode("ascii").rstrip()
+            v = np.fromfile(fh, dtype="<i4", count=9)
+            heads.append((name, tuple(int(x) for x in v[:3]), tuple(int(x) for x in v[3:6]), tuple(int(x) for x in v[6:])))
+        out["fields"] = {}
+        for name, st, gl, gh in heads:
+            shape = tuple(gh[a] - gl[a] + 1 for a in range(3))
+            n = int(np.prod(shape))
+            data = np.fromfile(fh, dtype="<f8", count=n)
+            if data.size != n:
+                raise ValueError(f"box snapshot ends inside the {name} block")
+            out["fields"][name] = {"st": st, "gl": gl, "gh": gh, "data": data.reshape(shape, order="F")}
     return out

@@ -24,6 +24,7 @@
 #define DFDM_H
 
 #include <stddef.h>
+#include <stdint.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -176,6 +177,16 @@ int dfdm_get_stage_variant(dfdm_ctx *ctx, int *variant, double *ms_one, double *
  * each as int32 n1, n2, n3 and the ghosted array in Fortran order. With the wall-model filter seeded
  * (wm_filter_mode = 1), write_wm_filter_state (:1990-2009) adds <path>.wmf with the six filter planes. */
 int dfdm_write_snapshot(dfdm_ctx *ctx, const char *path);
+/* write_box_snapshot (src/input_output.f90:1699-1767, field_box :1586-1598, fill_box_block :1623-1659): the
+ * chunked or cell-centred box snapshot of the face box f1..f2 (1-based faces, f1 < f2 <= nx/ny/nz), which the reference
+ * writes for chunked_snapshot and for snapshot_location = 1 (then over the whole domain, f1 = 1, f2 = n). Little-endian
+ * stream: int32 -4242, location, step, nfields; float64 t; int32 f1(3), f2(3); per direction float64 faces
+ * x(f1:f2) and centres xm(f1:f2-1); per field char name(8) (blank-padded U, V, W, P and, with an SGS model, nu_t),
+ * int32 st(3), gl(3), gh(3); then each field's box gl:gh in Fortran order. location 0 keeps the velocities on their
+ * faces (st = 1 in their own direction); location 1 averages them to the cell centres. step is the reference's
+ * istep + nstep_init. Box snapshots cannot be read back as a restart. */
+int dfdm_write_box_snapshot(dfdm_ctx *ctx, const char *path, const int32_t f1[3], const int32_t f2[3], int location,
+                            int32_t step);
 /* read_input_data (src/input_output.f90:1225-1341) with the pressure block of read_pressure_restart (:1972-1977)
  * and read_wm_filter_state (:2011-2031): loads U, V, W and P from a restart file of this grid (DFDM_ERR_INVALID
  * for a chunked/cell-centred snapshot, a short file, other face counts, other coordinates or a block of another

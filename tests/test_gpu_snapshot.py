@@ -49,3 +49,36 @@ def test_library_reads_the_host_written_restart(tmp_path):
     with pytest.raises(DfdmError) as e:
         other.read_snapshot(f)
     assert e.value.code == 1 and "coordinates" in str(e.value)
+
+
+@pytest.mark.parametrize("name", ["chan_les_amd_small", "tgv_small"])
+@pytest.mark.parametrize("location", [0, 1])
+def test_box_snapshot_equals_the_host_restatement(tmp_path, name, location):
+    """dfdm_write_box_snapshot writes, byte for byte, what the host restatement of write_box_snapshot writes from
+    the same state, time and step: a sub-box and the whole domain (the cell-centred full snapshot at location 1)."""
+    c = cases.get(name)
+    s = Solver(c, "fp64")
+    s.set_state(*cases.initial_condition(c))
+    s.compute_time_step_RK3(2)
+    U, V, W, P = s.get_state()
+    nut = s.get_nu_t() if c.sgs_model else None
+    for f1, f2 in (((2, 3, 2), (c.nx - 2, c.ny - 1, c.nz - 3)), ((1, 1, 1), (c.nx, c.ny, c.nz))):
+        a, b = str(tmp_path / "lib"), str(tmp_path / "host")
+        s.write_box_snapshot(a, f1, f2, location=location, step=7)
+        snapshot.write_box(b, c, f1, f2, U, V, W, P, nut, location=location, step=7, t=s.t)
+        assert open(a, "rb").read() == open(b, "rb").read(), (f1, f2)
+    s.close()
+
+
+def test_box_snapshot_rejections(tmp_path):
+    c = cases.chan_small()
+    s = Solver(c, "fp64")
+    s.set_state(*cases.initial_condition(c))
+    f = str(tmp_path / "box")
+    for f1, f2, loc in (((1, 1, 1), (c.nx + 1, 3, 3), 0), ((2, 2, 2), (2, 5, 5), 0), ((1, 1, 1), (3, 3, 3), 2)):
+        with pytest.raises(DfdmError):
+            s.write_box_snapshot(f, f1, f2, location=loc)
+    s.write_box_snapshot(f, (1, 1, 1), (3, 3, 3))
+    with pytest.raises(DfdmError, match="cannot be used for restart"):
+        s.read_snapshot(f)
+    s.close()
