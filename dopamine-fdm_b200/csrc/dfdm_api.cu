@@ -111,12 +111,13 @@ struct dfdm_ctx {
     unsigned long long *d_mon = nullptr;
     unsigned long long *d_cfl = nullptr;        // convective and viscous CFL maxima (bit patterns)
     // device time step: with the adaptive time step (cfl_adaptive = 1) or an output-landing target, dt and t live on
-    // the device in d_dtt = {dt of the step, t, landing target, dt before landing}, set by k_select_dt at every step
-    // start, so a run of steps (or its graph) needs no host round trip
+    // the device in d_dtt = {dt of the step, t, dt before landing, landing targets[5]}, set by k_select_dt at every
+    // step start, so a run of steps (or its graph) needs no host round trip
     double *d_dtt = nullptr;
     bool adaptive = false, landing = false;
     double cfl_target = 0.5, cfl_safety = 0.9, dt_min = 1e-10, dt_max = 1e10;
-    double t_land = std::numeric_limits<double>::quiet_NaN();
+    // landing targets in select_dt's order: tsave_next, chunk_tsave_next, slice_tnext, line_tnext, sim_end_time
+    double t_land[5] = {NAN, NAN, NAN, NAN, NAN};
     void *adv = nullptr;   // advection_scheme = 2: the dissipative terms, 3 fields of the storage type
     bool dev_dt() const { return adaptive || landing; }
     double *staging = nullptr;
@@ -1147,7 +1148,7 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
     c->d_mon = (unsigned long long *)tmp;
     if ((rc = dalloc(c, &tmp, 2 * sizeof(unsigned long long)))) return bail(rc);
     c->d_cfl = (unsigned long long *)tmp;
-    if ((rc = dalloc(c, &tmp, 4 * sizeof(double)))) return bail(rc);
+    if ((rc = dalloc(c, &tmp, 8 * sizeof(double)))) return bail(rc);
     c->d_dtt = (double *)tmp;
     if (prm->advection_scheme == 2) {   // the dissipative terms of the hybrid scheme
         if ((rc = dalloc(c, &c->adv, (size_t)3 * d.cells * c->ts))) return bail(rc);
@@ -1366,20 +1367,21 @@ int dfdm_set_nu_t(dfdm_ctx *c, const double *nu_t) {
     return DFDM_OK;
 }
 
-// the device time step: d_dtt = {dt of the last step, t, landing target, dt} to the host (c->t, c->t_land; the dt
-// before landing into *dt) and back
+// the device time step: d_dtt = {dt of the last step, t, dt before landing, landing targets[5]} to the host (c->t;
+// the dt before landing into *dt) and back (with c->t_land)
 static int pull_dtt(dfdm_ctx *c, double *dt) {
-    double v[4] = {c->prm.dt, c->t, c->t_land, c->prm.dt};
+    double v[8] = {c->prm.dt, c->t, c->prm.dt, NAN, NAN, NAN, NAN, NAN};
     if (c->dev_dt()) {
         CK(cudaMemcpyAsync(v, c->d_dtt, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
         c->t = v[1];
     }
-    if (dt) *dt = v[3];
+    if (dt) *dt = v[2];
     return DFDM_OK;
 }
 static int push_dtt(dfdm_ctx *c, double dt) {
-    const double v[4] = {dt, c->t, c->t_land, dt};
+    double v[8] = {dt, c->t, dt, 0, 0, 0, 0, 0};
+    for (int q = 0; q < 5; ++q) v[3 + q] = c->t_land[q];
     CK(cudaMemcpyAsync(c->d_dtt, v, sizeof(v), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return DFDM_OK;
@@ -1428,17 +1430,39 @@ int dfdm_set_adaptive_dt(dfdm_ctx *c, int enable, double cfl_target, double cfl_
     return push_dtt(c, dt);
 }
 
+// the landing targets of the coming steps (NaN: a slot without a target)
+static int set_landings(dfdm_ctx *c, const double tl[5]) {
+    double dt = c->prm.dt;
+    if (int rc = pull_dtt(c, &dt)) return rc;
+    const bool was = c->dev_dt();
+    c->landing = false;
+    for (int q = 0; q < 5; ++q) {
+        c->t_land[q] = tl[q];
+        c->landing = c->landing || !std::isnan(tl[q]);
+    }
+    if (was != c->dev_dt()) destroy_graph(c);   // new targets alone keep the graph: they are read from d_dtt
+    return c->dev_dt() ? push_dtt(c, dt) : DFDM_OK;
+}
+
 int dfdm_set_landing_time(dfdm_ctx *c, int enable, double t_land) {
     g_err.clear();
     if (int rc = check_ctx(c)) return rc;
     if (enable && !std::isfinite(t_land)) return fail(DFDM_ERR_INVALID, "the landing time must be finite");
-    double dt = c->prm.dt;
-    if (int rc = pull_dtt(c, &dt)) return rc;
-    const bool was = c->dev_dt();
-    c->landing = enable != 0;
-    c->t_land = enable ? t_land : std::nan("");
-    if (was != c->dev_dt()) destroy_graph(c);   // a new target alone keeps the graph: it is read from d_dtt
-    return c->dev_dt() ? push_dtt(c, dt) : DFDM_OK;
+    const double tl[5] = {enable ? t_land : NAN, NAN, NAN, NAN, NAN};
+    return set_landings(c, tl);
+}
+
+int dfdm_set_landing_times(dfdm_ctx *c, int n, const double *t_land) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (n < 0 || n > 5) return fail(DFDM_ERR_INVALID, "between 0 and 5 landing targets");
+    if (n > 0 && !t_land) return fail(DFDM_ERR_INVALID, "null landing targets");
+    double tl[5] = {NAN, NAN, NAN, NAN, NAN};
+    for (int q = 0; q < n; ++q) {
+        if (std::isinf(t_land[q])) return fail(DFDM_ERR_INVALID, "a landing time must be finite (NaN: no target)");
+        tl[q] = t_land[q];
+    }
+    return set_landings(c, tl);
 }
 
 // ---- the step ----

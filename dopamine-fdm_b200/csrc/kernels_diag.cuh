@@ -232,13 +232,13 @@ __global__ void __launch_bounds__(256) k_wall_diag(int Nx, int Nz, const double 
 }
 
 // The monitor values (the layout of dfdm_monitor): t, dt, mean U, max |U|, max |div u|, CFL conv, CFL visc, mean
-// u_tau of the lower and upper wall, NaN flag.  dtt = {dt of the step, t, landing target, dt} when the time step
-// lives on the device, else null and the host's t and dt are used.  One thread.
+// u_tau of the lower and upper wall, NaN flag.  dtt = {dt of the step, t, dt before landing, landing targets} when
+// the time step lives on the device, else null and the host's t and dt are used.  One thread.
 __global__ void k_monitor_final(const unsigned long long *__restrict__ bits, const int *__restrict__ flag,
                                 const double *__restrict__ bulk, const double *__restrict__ wsum, int ncol,
                                 const double *__restrict__ dtt, double t_host, double dt_host, double *__restrict__ out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const double dt = dtt ? dtt[3] : dt_host, t = dtt ? dtt[1] : t_host;
+    const double dt = dtt ? dtt[2] : dt_host, t = dtt ? dtt[1] : t_host;
     out[0] = t;
     out[1] = dt;
     out[2] = bulk[0];
@@ -327,25 +327,27 @@ __global__ void __launch_bounds__(256) k_cfl(Dims d, const T *__restrict__ U, co
     block_max2_atomic((double)mc, mv, out);
 }
 
-// select_dt (src/monitor.f90:429-458) at a step start.  dtt = {dt of the coming step, t, landing target, dt}:
-// with `adaptive`, the CFL maxima of k_cfl times dt give cfl_now = max(cfl_conv, cfl_visc) and
-// dt = max(dt_min, min(dt_max, dt*cfl_target/cfl_now*cfl_safety)) when cfl_now > 0 (kept in dtt[3], the
-// reference's dt_presnap); then landing_dt shrinks the step so that t lands on dtt[2] (NaN: no target; a target
-// within 1e-10 counts as reached): a remainder below 2 dt in one step, one between dt and 2 dt in two halves.
-// t += the step.  One thread.
+// select_dt (src/monitor.f90:429-444) and landing_dt (:450-458) on the device, one thread.  dtt = {dt of the
+// step, t, dt before landing, landing targets [3..7]}: the adaptive dt from the CFL maxima (bit patterns of
+// non-negative doubles per unit dt), kept in dtt[2] as the dt between steps; then, for each target in select_dt's
+// order (tsave_next, chunk_tsave_next, slice_tnext, line_tnext, sim_end_time; NaN: none), a remainder below 2 dt
+// is taken in one step and one between dt and 2 dt in two halves.  A target within 1e-10 of t counts as reached.
+// The step's dt goes to dtt[0] and t advances.
 __global__ void k_select_dt(const unsigned long long *__restrict__ cfl, double *__restrict__ dtt, int adaptive,
                             double cfl_target, double cfl_safety, double dt_min, double dt_max) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double dt = dtt[3];
+    double dt = dtt[2];
     if (adaptive) {
         const double conv = __longlong_as_double((long long)cfl[0]) * dt;
         const double visc = __longlong_as_double((long long)cfl[1]) * dt;
         const double now = fmax(conv, visc);
         if (now > 0.0) dt = fmax(dt_min, fmin(dt_max, dt * cfl_target / now * cfl_safety));
     }
-    dtt[3] = dt;
-    const double rem = dtt[2] - dtt[1];
-    if (rem > 1e-10 && rem < 2.0 * dt) dt = rem > dt ? 0.5 * rem : rem;
+    dtt[2] = dt;
+    for (int q = 0; q < 5; ++q) {
+        const double rem = dtt[3 + q] - dtt[1];   // NaN: no target
+        if (rem > 1e-10 && rem < 2.0 * dt) dt = rem > dt ? 0.5 * rem : rem;
+    }
     dtt[0] = dt;
     dtt[1] += dt;
 }

@@ -34,7 +34,7 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_compute_cfl", "dfdm_set_stage_variant", "dfdm_get_stage_variant", "dfdm_set_adaptive_dt",
            "dfdm_get_dt", "dfdm_set_landing_time", "dfdm_output_monitor", "dfdm_output_monitor_async",
            "dfdm_set_fused_correction", "dfdm_get_fused_correction", "dfdm_set_state_async", "dfdm_get_state_async",
-           "dfdm_write_box_snapshot"]
+           "dfdm_write_box_snapshot", "dfdm_set_landing_times"]
 
 
 class DfdmError(RuntimeError):
@@ -104,6 +104,7 @@ def load(build_if_missing: bool = True):
         "dfdm_set_adaptive_dt": (c_int, [c_void_p, c_int, c_double, c_double, c_double, c_double]),
         "dfdm_get_dt": (c_int, [c_void_p, P]),
         "dfdm_set_landing_time": (c_int, [c_void_p, c_int, c_double]),
+        "dfdm_set_landing_times": (c_int, [c_void_p, c_int, P]),
         "dfdm_output_monitor": (c_int, [c_void_p, P]),
         "dfdm_output_monitor_async": (c_int, [c_void_p, c_void_p]),
         "dfdm_set_fused_correction": (c_int, [c_void_p, c_int]),
@@ -340,6 +341,16 @@ class Solver:
     def set_landing_time(self, t_land=None):
         """Shrink the coming steps so that t lands on t_land (landing_dt, src/monitor.f90:436-458); None: no target."""
         _check(load().dfdm_set_landing_time(self.h, 0 if t_land is None else 1, 0.0 if t_land is None else float(t_land)))
+
+    def set_landing_times(self, targets=()):
+        """Up to five landing targets in select_dt's order (tsave_next, chunk_tsave_next, slice_tnext, line_tnext,
+        sim_end_time), applied in turn; None entries are slots without a target (dfdm.output.OutputSchedule keeps
+        them)."""
+        vals = [float("nan") if v is None else float(v) for v in targets]
+        if len(vals) > 5:
+            raise ValueError("at most five landing targets")
+        arr = (c_double * max(1, len(vals)))(*vals)
+        _check(load().dfdm_set_landing_times(self.h, len(vals), arr))
 
     @property
     def dt(self) -> float:

@@ -212,6 +212,11 @@ int dfdm_set_adaptive_dt(dfdm_ctx *ctx, int enable, double cfl_target, double cf
  * A target within 1e-10 of t counts as reached; the caller then sets the next one (a new target keeps the captured
  * step graph).  Works with the fixed and with the adaptive dt.  t_land must be finite. */
 int dfdm_set_landing_time(dfdm_ctx *ctx, int enable, double t_land);
+/* All of select_dt's landing targets (src/monitor.f90:436-440), applied in turn in this order: tsave_next
+ * (nsave < 0), chunk_tsave_next (chunked_snapshot with chunk_nsave < 0), slice_tnext (slice_freq < 0), line_tnext
+ * (line_freq < 0), sim_end_time (nsteps < 0). t_land[q] for q < n, NaN for a slot without a target; 0 <= n <= 5, n = 0
+ * removes every target. dfdm_set_landing_time(ctx, 1, t) is the single target {t}. */
+int dfdm_set_landing_times(dfdm_ctx *ctx, int n, const double *t_land);
 /* The reference's dt between steps: the fixed dt, or the adaptive dt of the last step before any landing shrink. */
 int dfdm_get_dt(dfdm_ctx *ctx, double *dt);
 /* The values output_monitor prints (src/monitor.f90:21-102), computed on the device. */

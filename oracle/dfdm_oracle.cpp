@@ -890,10 +890,17 @@ struct Oracle {
         conv_out = conv * dt();
         visc_out = visc * dt();
     }
-    // output landing (nsave < 0 / nsteps < 0): the step is shrunk so that t lands on t_land; NaN: no target.  A
-    // target within 1e-10 of t counts as reached (the tolerance of src/time_integration.f90:597 and
-    // src/main.f90:90-91), and the caller moves it on.
-    double t_land = std::nan("");
+    // output landing (nsave < 0, chunk_nsave < 0, slice_freq < 0, line_freq < 0, nsteps < 0): the step is shrunk
+    // in turn for each target, in select_dt's order tsave_next, chunk_tsave_next, slice_tnext, line_tnext,
+    // sim_end_time; NaN: no target in that slot.  A target within 1e-10 of t counts as reached (the tolerance of
+    // src/time_integration.f90:597 and src/main.f90:90-91), and the caller moves it on.
+    static constexpr int NLAND = 5;
+    double t_land[NLAND] = {NAN, NAN, NAN, NAN, NAN};
+    bool landing() const {
+        for (double v : t_land)
+            if (!std::isnan(v)) return true;
+        return false;
+    }
     double dt_presnap = -1.0;
     // landing_dt (src/monitor.f90:450-458): a remainder below 2 dt is taken in one step, or in two equal halves
     // when it is above dt
@@ -905,7 +912,7 @@ struct Oracle {
         }
         return r;
     }
-    // select_dt (src/monitor.f90:429-444), one landing target
+    // select_dt (src/monitor.f90:429-444)
     void select_dt() {
         if (cfl_adaptive == 1) {
             double conv = 0.0, visc = 0.0;
@@ -914,7 +921,8 @@ struct Oracle {
             if (cfl_now > 0.0) dt_cur = std::max(dt_min, std::min(dt_max, dt() * cfl_target / cfl_now * cfl_safety));
         }
         dt_presnap = dt();
-        if (t_land - t > 1e-10) dt_cur = landing_dt(dt(), t_land - t);
+        for (double tl : t_land)
+            if (tl - t > 1e-10) dt_cur = landing_dt(dt(), tl - t);
     }
 
     // ---- projection (src/projection.f90) ----
@@ -1146,7 +1154,7 @@ struct Oracle {
     void step() {
         compute_sgs_model();
         // dt from the start-of-step velocity, after nu_t (src/time_integration.f90:146-160)
-        const bool sel = cfl_adaptive == 1 || !std::isnan(t_land);
+        const bool sel = cfl_adaptive == 1 || landing();
         if (sel) select_dt();
         double to = t;
         Uo.d = U.d; Vo.d = V.d; Wo.d = W.d;
@@ -1223,7 +1231,15 @@ void orc_set_adaptive(void *h, int enable, double target, double safety, double 
     if (!enable) o->dt_cur = -1.0;
 }
 void orc_output_monitor(void *h, double *out) { ((Oracle *)h)->output_monitor(out); }
-void orc_set_landing(void *h, double t_land) { ((Oracle *)h)->t_land = t_land; }
+void orc_set_landing(void *h, double t_land) {
+    Oracle *o = (Oracle *)h;
+    for (double &v : o->t_land) v = NAN;
+    o->t_land[0] = t_land;
+}
+void orc_set_landings(void *h, int n, const double *t_land) {
+    Oracle *o = (Oracle *)h;
+    for (int q = 0; q < Oracle::NLAND; ++q) o->t_land[q] = q < n ? t_land[q] : NAN;
+}
 void orc_cfl(void *h, double *conv, double *visc) { ((Oracle *)h)->compute_cfl(*conv, *visc); }
 void orc_compute_sgs(void *h) { ((Oracle *)h)->compute_sgs_model(); }
 void orc_wall_model(void *h, int update_filter, double *tau_x, double *tau_z) {

@@ -72,6 +72,7 @@ def lib():
         L.orc_set_adaptive.argtypes = [c_void_p, c_int, c_double, c_double, c_double, c_double]
         L.orc_cfl.argtypes = [c_void_p, POINTER(c_double), POINTER(c_double)]
         L.orc_set_landing.argtypes = [c_void_p, c_double]
+        L.orc_set_landings.argtypes = [c_void_p, c_int, POINTER(c_double)]
         L.orc_output_monitor.argtypes = [c_void_p, POINTER(c_double)]
         L.orc_set_threads.argtypes = [c_int]
         L.orc_get_threads.restype = c_int
@@ -151,6 +152,15 @@ class Oracle:
     def set_landing_time(self, t_land=None):
         """Shrink the coming steps so that t lands on t_land (landing_dt, src/monitor.f90:436-458); None: no target."""
         lib().orc_set_landing(self.h, float("nan") if t_land is None else float(t_land))
+
+    def set_landing_times(self, targets=()):
+        """Up to five landing targets in select_dt's order (tsave_next, chunk_tsave_next, slice_tnext, line_tnext,
+        sim_end_time; src/monitor.f90:436-440), each applied in turn; None entries are slots without a target."""
+        vals = [float("nan") if v is None else float(v) for v in targets]
+        if len(vals) > 5:
+            raise ValueError("at most five landing targets")
+        arr = (c_double * max(1, len(vals)))(*vals)
+        lib().orc_set_landings(self.h, len(vals), arr)
 
     MONITOR_KEYS = ("t", "dt", "mean_u", "max_u", "max_div", "cfl_conv", "cfl_visc", "u_tau_lo", "u_tau_hi", "nan_flag")
 

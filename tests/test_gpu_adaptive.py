@@ -130,3 +130,50 @@ def test_landing_matches_the_oracle(oracle_mod, adaptive):
     for key, a, b in zip("UVWP", s.get_state(), o.get_state()):
         assert rel_l2(a, b) <= 1e-12, (key, rel_l2(a, b))
     s.close()
+
+
+@pytest.mark.parametrize("adaptive", [False, True])
+def test_several_landing_targets_match_the_oracle(oracle_mod, adaptive):
+    """select_dt with three time targets at once (full snapshots, slices, the end time), the targets moved on by
+    the host output cadence (dfdm.output.OutputSchedule) after every step: the same times, dt and states as the
+    oracle, with the step graph kept across new targets."""
+    from dfdm.output import OutputSchedule
+    c = cases.get("chan_les_amd_small")
+    U, V, W, P = cases.initial_condition(c)
+    o = oracle_mod.Oracle(c)
+    o.set_state(U, V, W, P)
+    s = Solver(c, "fp64")
+    s.set_state(U, V, W, P)
+    s.enable_graphs(True)
+    if adaptive:
+        o.set_adaptive_dt(True, 0.6, 0.9)
+        s.set_adaptive_dt(True, 0.6, 0.9)
+
+    def sched():
+        return OutputSchedule(nsteps=-1, sim_end_time=11.3 * c.dt, nsave=-1, tsave=2.6 * c.dt, n_slices=1,
+                              slice_freq=-1, slice_interval=3.7 * c.dt)
+    so, ss = sched(), sched()
+    istep = 0
+    while True:
+        istep += 1
+        o.set_landing_times(so.targets())
+        s.set_landing_times(ss.targets())
+        o.step(1)
+        t = s.compute_time_step_RK3(1)
+        assert abs(t - o.t) <= 1e-13 * o.t, (istep, t, o.t)
+        assert abs(s.dt - o.dt) <= 1e-13 * o.dt, (istep, s.dt, o.dt)
+        assert ss.after_step(istep, t) == so.after_step(istep, o.t)
+        if so.done(istep, o.t):
+            assert ss.done(istep, t)
+            break
+        assert istep < 200
+    assert abs(o.t - 11.3 * c.dt) <= 1e-12
+    for key, a, b in zip("UVWP", s.get_state(), o.get_state()):
+        assert rel_l2(a, b) <= 1e-12, (key, rel_l2(a, b))
+    import ctypes
+    from dfdm.native import load
+    six = (ctypes.c_double * 6)(*([1.0] * 6))
+    assert load().dfdm_set_landing_times(s.h, 6, six) != 0        # at most five targets
+    inf = (ctypes.c_double * 1)(float("inf"))
+    assert load().dfdm_set_landing_times(s.h, 1, inf) != 0        # NaN marks a free slot; inf is an error
+    s.close()
