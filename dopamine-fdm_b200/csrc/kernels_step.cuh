@@ -209,6 +209,24 @@ template <> struct AxisLocal<F2> {   // packed pairs: the same metrics broadcast
         w0m_ = F2(__ldg(m.w0 + p - 1)); w1m_ = F2(__ldg(m.w1 + p - 1)); w0_ = F2(__ldg(m.w0 + p)); w1_ = F2(__ldg(m.w1 + p));
         idc_ = F2(__ldg(m.idc + p)); idcp_ = F2(__ldg(m.idc + p + 1)); idfm_ = F2(__ldg(m.idf + p - 1)); idf_ = F2(__ldg(m.idf + p));
     }
+    // the same eight values staged by metric_src (w0, w1 at p-1 and p; idc at p, p+1; idf at p-1, p)
+    __device__ __forceinline__ void load8(const float *z) {
+        w0m_ = F2(z[0]); w1m_ = F2(z[1]); w0_ = F2(z[2]); w1_ = F2(z[3]);
+        idc_ = F2(z[4]); idcp_ = F2(z[5]); idfm_ = F2(z[6]); idf_ = F2(z[7]);
+    }
+    // the address of staged value t (0..7) of point p, in the order of load8
+    static __device__ __forceinline__ const float *metric_src(const Metric1D<float> &m, int p, int t) {
+        switch (t) {
+        case 0: return m.w0 + p - 1;
+        case 1: return m.w1 + p - 1;
+        case 2: return m.w0 + p;
+        case 3: return m.w1 + p;
+        case 4: return m.idc + p;
+        case 5: return m.idc + p + 1;
+        case 6: return m.idf + p - 1;
+        default: return m.idf + p;
+        }
+    }
     __device__ __forceinline__ F2 w0m() const { return w0m_; }
     __device__ __forceinline__ F2 w1m() const { return w1m_; }
     __device__ __forceinline__ F2 w0() const { return w0_; }
@@ -726,6 +744,9 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
     // CORR phi tile: two more columns (an even pitch keeps pairs aligned) and one more row
     constexpr int PXP = PX + 2, PSP2 = PXP * (PY + 1) / 2, PERP = (PSP2 + NT - 1) / NT;
     __shared__ __align__(16) float smp[CORR ? 5 : 1][CORR ? 2 * PSP2 : 2];
+    // the z metrics of planes k .. k+2 (AxisLocal<F2>::load8 order), copied with the planes: under the streaming
+    // tile copies the metric tables do not stay in L1, and every thread needs them at the start of its plane
+    __shared__ float zmr[4][8];
     const Dims &d = a.d;
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
     const int i0 = blockIdx.x * TXC, j0 = blockIdx.y * TY;
@@ -788,6 +809,9 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
             for (int q = 0; q < PERP; ++q)
                 if (offp[q] >= 0) cp_async<8>(&smp[slot][2 * (threadIdx.x + q * NT)], a.phi + kw * plane + offp[q]);
         }
+    };
+    auto issue_z = [&](int k) {   // the z metrics of plane k (k0 <= k < kend) into zmr[(k - k0) & 3]
+        if (threadIdx.x < 8) cp_async<4>(&zmr[(k - k0) & 3][threadIdx.x], AxisLocal<F2>::metric_src(a.mz, k, threadIdx.x));
     };
     auto issue = [&](int slot, int k) {
         int kw = k < 0 ? k + Nz : (k >= Nz ? k - Nz : k);
@@ -856,6 +880,8 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
 
     issue(0, k0 - 1); issue(1, k0); issue(2, k0 + 1);
     issue_phi(k0 - 1); issue_phi(k0); issue_phi(k0 + 1); issue_phi(k0 + 2); issue_phi(k0 + 3);
+    issue_z(k0);
+    if (k0 + 1 < kend) issue_z(k0 + 1);
     cp_async_commit();
     cp_async_wait_all();
     if (CORR) __syncthreads();   // phi elements copied by other threads
@@ -866,6 +892,7 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
         const bool more = k + 2 <= kend;
         const int snext = (k - k0 + 3) & 3;
         if (more) { issue(snext, k + 2); issue_phi(k + 4); }
+        if (k + 2 < kend) issue_z(k + 2);
         cp_async_commit();
         const int sm_ = (k - k0) & 3, s0 = (k - k0 + 1) & 3, sp = (k - k0 + 2) & 3;
         if (active) {
@@ -888,7 +915,7 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
                 if (vrow) fv = ld2(f1v);
             }
             AxisLocal<F2> Z;
-            Z.load(a.mz, k);
+            Z.load8(zmr[(k - k0) & 3]);
             F2 ru = rhs_u_at<F2, LES, WM>(a, q, Y, Z, tau_x, i, j, k);
             F2 rw = rhs_w_at<F2, LES, WM>(a, q, Y, Z, tau_z, i, j, k);
             F2 rv = vrow ? rhs_v_at<F2, LES, WM>(a, q, Y, Z, i, j, k) : F2(0.0f);
