@@ -210,7 +210,8 @@ int dfdm_set_adaptive_dt(dfdm_ctx *ctx, int enable, double cfl_target, double cf
  * are shrunk by landing_dt so that t lands on t_land (a remainder below 2 dt in one step, one between dt and 2 dt in
  * two equal halves); dt returns to its value before the shrink after the step (src/time_integration.f90:711).
  * A target within 1e-10 of t counts as reached; the caller then sets the next one (a new target keeps the captured
- * step graph).  Works with the fixed and with the adaptive dt.  t_land must be finite. */
+ * step graph).  Works with the fixed and with the adaptive dt.  t_land must be finite.  It replaces every target set
+ * through dfdm_set_landing_times (enable = 0 removes them all). */
 int dfdm_set_landing_time(dfdm_ctx *ctx, int enable, double t_land);
 /* All of select_dt's landing targets (src/monitor.f90:436-440), applied in turn in this order: tsave_next
  * (nsave < 0), chunk_tsave_next (chunked_snapshot with chunk_nsave < 0), slice_tnext (slice_freq < 0), line_tnext
