@@ -636,7 +636,7 @@ template <typename T> struct Impl {
                 k_col_fft<T, 2, CT><<<g, 256, c->smem_y, st>>>(d, (C *)c->spec, c->plan_y, (const C *)c->tw_y, c->d_kxx, c->d_kyy, c->d_kzz);
             } else {
                 dim3 g((d.Nxc + 63) / 64, d.Nz);
-                k_ysolve2<T, 8><<<g, 64, 2 * d.Ny * sizeof(double), st>>>(d, (C *)c->spec, c->d_rpiv, c->d_lo, c->d_up);
+                k_ysolve2<T, sizeof(T) == 4 ? 16 : 8><<<g, 64, 2 * d.Ny * sizeof(double), st>>>(d, (C *)c->spec, c->d_rpiv, c->d_lo, c->d_up);
             }
             CKL();
             return DFDM_OK;
