@@ -84,6 +84,14 @@ def workload_name(c):
     return f"{c.name}: {Nx}x{Ny}x{Nz} cells"
 
 
+def data_desc(c):
+    """The synthetic input of the workload: its seeded initial condition (there is no dataset)."""
+    return {"poiseuille_uniform": "synthetic: seeded laminar Poiseuille + 10% uniform noise, no dataset",
+            "reichardt_gauss": "synthetic: seeded Reichardt profile + Gaussian noise, no dataset",
+            "tgv": "synthetic: Taylor-Green vortex, no dataset",
+            "zero": "synthetic: fluid at rest, no dataset"}.get(c.ic, f"synthetic: initial condition {c.ic}, no dataset")
+
+
 def config_dict(c, extra=None):
     d = {"workload": workload_name(c), "grid_faces": [c.nx, c.ny, c.nz], "cells": c.n_cells,
          "y": "walls, tanh alpha=%g" % c.alpha_grid if c.y_bc_type == 1 else "periodic",
@@ -216,7 +224,7 @@ def run_reference(args, c):
     sample = f"{n} full RK3 steps of the {workload_name(c)} case after 1 warm-up step"
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": n, "warmup": 1,
             "ms_per_step": 1e3 * el / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (seeded Poiseuille + 10% uniform noise)",
+            "dtype": "f64", "data": data_desc(c),
             "config": config_dict(c), "impl": "reference",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": "port", "sample": sample,
                              "note": "reference Fortran/MPI build unavailable on this box; FP64 C++ restatement"},
@@ -331,7 +339,7 @@ def main():
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "fp32-mixed (FP32 fields/stencils/FFTs, FP64 y-solves and reductions)",
-           "data": "synthetic: seeded laminar Poiseuille + 10% uniform noise, no dataset",
+           "data": data_desc(c),
            "config": config_dict(c, {"parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"}),
            "clocks": clocks, "gpu_launches": launches,
            "tuning": {"stage_kernel": ["one cell per thread", "packed FP32x2 pairs"][variant],
