@@ -1725,25 +1725,61 @@ int dfdm_solve_poisson_noalloc(dfdm_ctx *c, const double *rhs_in, double *phi_ou
 }  // extern "C"
 
 namespace {
-// ---- the reference's restart format (one rank, little-endian stream) ----
+// ---- the reference's restart format (one rank, a stream of int32 and float64 words) ----
+// The staggered restart and its .wmf are opened without convert= (src/input_output.f90:1272,1842,1996,2019), so
+// they take the build's default byte order, which every compiler branch of the reference's CMakeLists.txt sets to
+// big-endian (:210 gfortran -fconvert=big-endian, Intel -convert big_endian, NVHPC -Mbyteswapio). Only the
+// box-snapshot magic probe (:1235) and the box snapshot itself (:1723) are explicitly little-endian.
 const int32_t SNAP_MAGIC = -4242;
+static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "the snapshot code assumes a little-endian host");
 
-bool put_block(FILE *f, const double *a, int n1, int n2, int n3) {
+inline int32_t bswap(int32_t v) { return (int32_t)__builtin_bswap32((uint32_t)v); }
+inline double bswap(double v) {
+    uint64_t u;
+    std::memcpy(&u, &v, 8);
+    u = __builtin_bswap64(u);
+    std::memcpy(&v, &u, 8);
+    return v;
+}
+// write n words, byte-swapped when `swap` (a big-endian file), through a bounded buffer
+template <class T> bool put_words(FILE *f, const T *p, size_t n, bool swap) {
+    if (!swap) return fwrite(p, sizeof(T), n, f) == n;
+    std::vector<T> buf(std::min(n, (size_t)65536));
+    for (size_t o = 0; o < n; o += buf.size()) {
+        const size_t m = std::min(buf.size(), n - o);
+        for (size_t i = 0; i < m; ++i) buf[i] = bswap(p[o + i]);
+        if (fwrite(buf.data(), sizeof(T), m, f) != m) return false;
+    }
+    return true;
+}
+template <class T> bool get_words(FILE *f, T *p, size_t n, bool swap) {
+    if (fread(p, sizeof(T), n, f) != n) return false;
+    if (swap) for (size_t i = 0; i < n; ++i) p[i] = bswap(p[i]);
+    return true;
+}
+bool put_block(FILE *f, const double *a, int n1, int n2, int n3, bool swap) {
     const int32_t h[3] = {n1, n2, n3};
     const size_t n = (size_t)n1 * n2 * n3;
-    return fwrite(h, sizeof(int32_t), 3, f) == 3 && fwrite(a, sizeof(double), n, f) == n;
+    return put_words(f, h, 3, swap) && put_words(f, a, n, swap);
 }
-int get_block(FILE *f, std::vector<double> &a, int n1, int n2, int n3, const char *what) {
+int get_block(FILE *f, std::vector<double> &a, int n1, int n2, int n3, const char *what, bool swap) {
     int32_t h[3];
-    if (fread(h, sizeof(int32_t), 3, f) != 3) return fail(DFDM_ERR_INVALID, std::string("restart file ends before ") + what);
+    if (!get_words(f, h, 3, swap)) return fail(DFDM_ERR_INVALID, std::string("restart file ends before ") + what);
     if (h[0] != n1 || h[1] != n2 || h[2] != n3)
         return fail(DFDM_ERR_INVALID, std::string("restart file field block size mismatch for ") + what + ": found " +
                                           std::to_string(h[0]) + " " + std::to_string(h[1]) + " " + std::to_string(h[2]) +
                                           " expected " + std::to_string(n1) + " " + std::to_string(n2) + " " + std::to_string(n3));
     a.resize((size_t)n1 * n2 * n3);
-    if (fread(a.data(), sizeof(double), a.size(), f) != a.size())
+    if (!get_words(f, a.data(), a.size(), swap))
         return fail(DFDM_ERR_INVALID, std::string("restart file ends inside the ") + what + " block");
     return DFDM_OK;
+}
+// Byte order of a restart or .wmf file from its first word, which is nx in both: big-endian when the word read
+// big-endian is nx, little-endian when the word read little-endian is. Returns 1 (big), 0 (little) or -1 (neither).
+int detect_order(int32_t first_le, int nx) {
+    if (bswap(first_le) == nx) return 1;
+    if (first_le == nx) return 0;
+    return -1;
 }
 // the six mesh arrays of the header: faces x, y, z (1-based host copies) and their centres
 std::vector<std::vector<double>> mesh_arrays(const dfdm_ctx *c) {
@@ -1788,10 +1824,15 @@ struct FileCloser {
 
 extern "C" {
 
-int dfdm_write_snapshot(dfdm_ctx *c, const char *path) {
+int dfdm_write_snapshot(dfdm_ctx *c, const char *path) { return dfdm_write_snapshot_ex(c, path, DFDM_BIG_ENDIAN); }
+
+int dfdm_write_snapshot_ex(dfdm_ctx *c, const char *path, int byte_order) {
     g_err.clear();
     if (int rc = check_ctx(c)) return rc;
     if (!path) return fail(DFDM_ERR_INVALID, "null path");
+    if (byte_order != DFDM_BIG_ENDIAN && byte_order != DFDM_LITTLE_ENDIAN)
+        return fail(DFDM_ERR_INVALID, "byte_order must be DFDM_BIG_ENDIAN or DFDM_LITTLE_ENDIAN");
+    const bool sw = byte_order == DFDM_BIG_ENDIAN;
     const size_t nU = (size_t)c->nx * c->nyg * c->nzg, nV = (size_t)c->nxg * c->ny * c->nzg;
     const size_t nW = (size_t)c->nxg * c->nyg * c->nz, nP = (size_t)c->nxg * c->nyg * c->nzg;
     std::vector<double> U(nU), V(nV), W(nW), P(nP), NU;
@@ -1806,11 +1847,11 @@ int dfdm_write_snapshot(dfdm_ctx *c, const char *path) {
     bool ok = true;
     for (const std::vector<double> &m : mesh_arrays(c)) {
         const int32_t n = (int32_t)m.size();
-        ok = ok && fwrite(&n, sizeof(n), 1, fc.f) == 1 && fwrite(m.data(), sizeof(double), m.size(), fc.f) == m.size();
+        ok = ok && put_words(fc.f, &n, 1, sw) && put_words(fc.f, m.data(), m.size(), sw);
     }
-    ok = ok && put_block(fc.f, U.data(), c->nx, c->nyg, c->nzg) && put_block(fc.f, V.data(), c->nxg, c->ny, c->nzg) &&
-         put_block(fc.f, W.data(), c->nxg, c->nyg, c->nz) && put_block(fc.f, P.data(), c->nxg, c->nyg, c->nzg);
-    if (c->les) ok = ok && put_block(fc.f, NU.data(), c->nxg, c->nyg, c->nzg);
+    ok = ok && put_block(fc.f, U.data(), c->nx, c->nyg, c->nzg, sw) && put_block(fc.f, V.data(), c->nxg, c->ny, c->nzg, sw) &&
+         put_block(fc.f, W.data(), c->nxg, c->nyg, c->nz, sw) && put_block(fc.f, P.data(), c->nxg, c->nyg, c->nzg, sw);
+    if (c->les) ok = ok && put_block(fc.f, NU.data(), c->nxg, c->nyg, c->nzg, sw);
     if (!ok || fclose(fc.f) != 0) { fc.f = nullptr; return fail(DFDM_ERR_INVALID, std::string("write to ") + path + " failed"); }
     fc.f = nullptr;
     if (!(c->wm && c->wm_filter_mode == 1 && c->wmf_seeded)) return DFDM_OK;
@@ -1825,7 +1866,7 @@ int dfdm_write_snapshot(dfdm_ctx *c, const char *path) {
         CK(cudaStreamSynchronize(c->stream));
         const bool xf = q < 3;
         wmf_to_ref(c, dev, xf, ref);
-        ok = ok && put_block(fw.f, ref.data(), xf ? c->nx : c->nxg, 2, xf ? c->nzg : c->nz);
+        ok = ok && put_block(fw.f, ref.data(), xf ? c->nx : c->nxg, 2, xf ? c->nzg : c->nz, sw);
     }
     if (!ok || fclose(fw.f) != 0) { fw.f = nullptr; return fail(DFDM_ERR_INVALID, std::string("write to ") + path + ".wmf failed"); }
     fw.f = nullptr;
@@ -1926,7 +1967,7 @@ int dfdm_read_snapshot(dfdm_ctx *c, const char *path) {
     if (!fc.f) return fail(DFDM_ERR_INVALID, std::string("cannot open restart file ") + path);
     int32_t first = 0;
     if (fread(&first, sizeof(first), 1, fc.f) != 1) return fail(DFDM_ERR_INVALID, "restart file is empty");
-    if (first == SNAP_MAGIC)
+    if (first == SNAP_MAGIC)   // the magic probe reads little-endian (src/input_output.f90:1235)
         return fail(DFDM_ERR_INVALID, "the file is a cell-centred/chunked box snapshot and cannot be used for restart");
     // size check of read_input_data: the mesh, then U, V, W and P
     const std::vector<std::vector<double>> mesh = mesh_arrays(c);
@@ -1939,16 +1980,21 @@ int dfdm_read_snapshot(dfdm_ctx *c, const char *path) {
     if (have < expect)
         return fail(DFDM_ERR_INVALID, "restart file is smaller than expected for this grid: " + std::to_string(have) +
                                           " < " + std::to_string(expect) + " bytes");
+    const int order = detect_order(first, c->nx);
+    if (order < 0)
+        return fail(DFDM_ERR_INVALID, "restart file nx = " + std::to_string(bswap(first)) + " (big-endian) or " +
+                                          std::to_string(first) + " (little-endian) but the grid gives " + std::to_string(c->nx));
+    const bool sw = order == 1;
     fseek(fc.f, 0, SEEK_SET);
     const char *names[6] = {"nx", "ny", "nz", "nxm", "nym", "nzm"};
     for (int a = 0; a < 6; ++a) {
         int32_t n = 0;
-        if (fread(&n, sizeof(n), 1, fc.f) != 1) return fail(DFDM_ERR_INVALID, "restart file header truncated");
+        if (!get_words(fc.f, &n, 1, sw)) return fail(DFDM_ERR_INVALID, "restart file header truncated");
         if (n != (int32_t)mesh[a].size())
             return fail(DFDM_ERR_INVALID, std::string("restart file ") + names[a] + " = " + std::to_string(n) +
                                               " but the grid gives " + std::to_string(mesh[a].size()));
         std::vector<double> f(n);
-        if (fread(f.data(), sizeof(double), n, fc.f) != (size_t)n) return fail(DFDM_ERR_INVALID, "restart file header truncated");
+        if (!get_words(fc.f, f.data(), (size_t)n, sw)) return fail(DFDM_ERR_INVALID, "restart file header truncated");
         double scale = 1.0;
         for (double v : mesh[a]) scale = std::max(scale, std::fabs(v));
         for (int i = 0; i < n; ++i)
@@ -1957,22 +2003,23 @@ int dfdm_read_snapshot(dfdm_ctx *c, const char *path) {
     }
     std::vector<double> U, V, W, P;
     int rc;
-    if ((rc = get_block(fc.f, U, c->nx, c->nyg, c->nzg, "U"))) return rc;
-    if ((rc = get_block(fc.f, V, c->nxg, c->ny, c->nzg, "V"))) return rc;
-    if ((rc = get_block(fc.f, W, c->nxg, c->nyg, c->nz, "W"))) return rc;
-    if ((rc = get_block(fc.f, P, c->nxg, c->nyg, c->nzg, "P"))) return rc;
+    if ((rc = get_block(fc.f, U, c->nx, c->nyg, c->nzg, "U", sw))) return rc;
+    if ((rc = get_block(fc.f, V, c->nxg, c->ny, c->nzg, "V", sw))) return rc;
+    if ((rc = get_block(fc.f, W, c->nxg, c->nyg, c->nz, "W", sw))) return rc;
+    if ((rc = get_block(fc.f, P, c->nxg, c->nyg, c->nzg, "P", sw))) return rc;
     if ((rc = dfdm_set_state(c, U.data(), V.data(), W.data(), P.data()))) return rc;
     c->wmf_seeded = false;
     if (!(c->wm && c->wm_filter_mode == 1)) return DFDM_OK;
     FileCloser fw{fopen((std::string(path) + ".wmf").c_str(), "rb")};
     if (!fw.f) return DFDM_OK;   // no filter file: the filter re-seeds on the next step
+    // the .wmf comes from the same build as the restart: the restart's byte order
     const size_t np = (size_t)2 * c->d.Nz * c->d.Nx;
     double *planes[6] = {c->wsd.ux, c->wsd.wx, c->wsd.tx, c->wsd.uz, c->wsd.wz, c->wsd.tz};
     const char *wn[6] = {"wmf_ux", "wmf_wx", "wmf_tx", "wmf_uz", "wmf_wz", "wmf_tz"};
     std::vector<double> ref, dev;
     for (int q = 0; q < 6; ++q) {
         const bool xf = q < 3;
-        if ((rc = get_block(fw.f, ref, xf ? c->nx : c->nxg, 2, xf ? c->nzg : c->nz, wn[q]))) return rc;
+        if ((rc = get_block(fw.f, ref, xf ? c->nx : c->nxg, 2, xf ? c->nzg : c->nz, wn[q], sw))) return rc;
         wmf_from_ref(c, ref, xf, dev);
         CK(cudaMemcpyAsync(planes[q], dev.data(), np * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         CK(cudaStreamSynchronize(c->stream));

@@ -322,8 +322,15 @@ def chan_les_amd_small() -> Case:
                 seed=18, nsteps=20)
 
 
+def chan_les_vreman_small() -> Case:
+    """The wall-modelled LES regression grid with the Vreman closure (sgs_model = 1, Cs_vreman = 0.17) in place of
+    AMD: the other eddy-viscosity branch of compute_vreman (src/sgs_model.f90:212-216)."""
+    return chan_les_amd_small().with_(name="chan_les_vreman_small", sgs_model=1)
+
+
 CONFIGS = {"tgv64": tgv, "chan180": chan180, "les395": les395, "chan550": chan550,
-           "tgv_small": tgv_small, "chan_small": chan_small, "chan_les_amd_small": chan_les_amd_small}
+           "tgv_small": tgv_small, "chan_small": chan_small, "chan_les_amd_small": chan_les_amd_small,
+           "chan_les_vreman_small": chan_les_vreman_small}
 
 
 def get(name: str, **kw) -> Case:

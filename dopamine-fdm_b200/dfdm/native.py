@@ -34,7 +34,7 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_compute_cfl", "dfdm_set_stage_variant", "dfdm_get_stage_variant", "dfdm_set_adaptive_dt",
            "dfdm_get_dt", "dfdm_set_landing_time", "dfdm_output_monitor", "dfdm_output_monitor_async",
            "dfdm_set_fused_correction", "dfdm_get_fused_correction", "dfdm_set_state_async", "dfdm_get_state_async",
-           "dfdm_write_box_snapshot", "dfdm_set_landing_times"]
+           "dfdm_write_box_snapshot", "dfdm_set_landing_times", "dfdm_write_snapshot_ex"]
 
 
 class DfdmError(RuntimeError):
@@ -95,6 +95,7 @@ def load(build_if_missing: bool = True):
         "dfdm_launch_count": (c_int, [c_void_p, POINTER(ctypes.c_longlong)]),
         "dfdm_solve_poisson_noalloc": (c_int, [c_void_p, P, P]),
         "dfdm_write_snapshot": (c_int, [c_void_p, c_char_p]),
+        "dfdm_write_snapshot_ex": (c_int, [c_void_p, c_char_p, c_int]),
         "dfdm_read_snapshot": (c_int, [c_void_p, c_char_p]),
         "dfdm_write_box_snapshot": (c_int, [c_void_p, c_char_p, POINTER(ctypes.c_int32), POINTER(ctypes.c_int32), c_int,
                                             ctypes.c_int32]),
@@ -282,12 +283,16 @@ class Solver:
         _check(load().dfdm_solve_poisson_noalloc(self.h, dptr(a), dptr(out)))
         return out
 
-    def write_snapshot(self, path: str) -> None:
-        """The reference's restart file (and <path>.wmf with a seeded wall-model filter)."""
-        _check(load().dfdm_write_snapshot(self.h, os.fsencode(path)))
+    def write_snapshot(self, path: str, byte_order: str = "big") -> None:
+        """The reference's restart file (and <path>.wmf with a seeded wall-model filter), big-endian as the
+        reference's builds write it, or little-endian with byte_order="little"."""
+        if byte_order not in ("big", "little"):
+            raise ValueError("byte_order must be 'big' or 'little'")
+        _check(load().dfdm_write_snapshot_ex(self.h, os.fsencode(path), 1 if byte_order == "big" else 0))
 
     def read_snapshot(self, path: str) -> None:
-        """U, V, W, P (and the wall-model filter from <path>.wmf) from a restart file of this grid."""
+        """U, V, W, P (and the wall-model filter from <path>.wmf) from a restart file of this grid, in the byte
+        order the file holds."""
         _check(load().dfdm_read_snapshot(self.h, os.fsencode(path)))
 
     def write_box_snapshot(self, path: str, f1, f2, location: int = 0, step: int = 0) -> None:

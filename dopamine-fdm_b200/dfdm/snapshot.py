@@ -1,14 +1,20 @@
 """The reference's staggered restart/snapshot format, on the host (numpy).
 
 Layout of a one-rank file (output_data, src/input_output.f90:1782-1880; read back by read_input_data, :1225-1341),
-a little-endian stream with no record markers:
+a stream with no record markers, big-endian by default:
   int32 nx,  float64 x(nx)        face coordinates        int32 nxm, float64 xm(nxm)   centres, nxm = nx-1
   int32 ny,  float64 y(ny)                                int32 nym, float64 ym(nym)
   int32 nz,  float64 z(nz)                                int32 nzm, float64 zm(nzm)
   then one block per field: int32 n1, n2, n3 and n1*n2*n3 float64 in Fortran order:
   U(nx,nyg,nzg), V(nxg,ny,nzg), W(nxg,nyg,nz), P(nxg,nyg,nzg) and, with an SGS model, nu_t(nxg,nyg,nzg).
-(The mesh blocks come in the order x, y, z, xm, ym, zm.)  A file that starts with -4242 is a cell-centred/chunked
-box snapshot, which cannot serve as a restart.
+(The mesh blocks come in the order x, y, z, xm, ym, zm.)  A file that starts with -4242 (read little-endian, as the
+reference's probe at :1235 reads it) is a cell-centred/chunked box snapshot, which cannot serve as a restart.
+
+Byte order: output_data and read_input_data open the restart without convert= (:1272, :1842), and so do the .wmf
+writer and reader (:1996, :2019), so these files take the build's default byte order, which the reference's
+CMakeLists.txt:210 sets to big-endian for gfortran (-fconvert=big-endian), Intel (-convert big_endian) and NVHPC
+(-Mbyteswapio).  They are written big-endian here unless byte_order="little" is asked for, and read in the order
+their first word (nx) shows.  The box snapshot is explicitly little-endian (:1723) and stays so.
 
 The box snapshot (write_box_snapshot, :1699-1767) holds the face box f1..f2 (1-based faces) of every field:
   int32 -4242, snapshot_location, step, nfields; float64 t; int32 f1(3), f2(3);
@@ -41,21 +47,41 @@ def _centres(f: np.ndarray) -> np.ndarray:
     return 0.5 * (f[:-1] + f[1:])
 
 
-def _write_block(fh, a: np.ndarray) -> None:
-    a = np.asfortranarray(a, dtype="<f8")
-    np.asarray(a.shape, dtype="<i4").tofile(fh)
+def _prefix(byte_order: str) -> str:
+    if byte_order not in ("big", "little"):
+        raise ValueError("byte_order must be 'big' or 'little'")
+    return ">" if byte_order == "big" else "<"
+
+
+def detect_byte_order(path: str, nx: int) -> str:
+    """'big' or 'little': the order in which the file's first word reads as nx (a restart starts with nx, a .wmf
+    with its first block's n1 = nx); ValueError when it reads as nx in neither."""
+    raw = open(path, "rb").read(4)
+    if len(raw) < 4:
+        raise ValueError("restart file is empty")
+    be, le = int(np.frombuffer(raw, ">i4")[0]), int(np.frombuffer(raw, "<i4")[0])
+    if be == nx:
+        return "big"
+    if le == nx:
+        return "little"
+    raise ValueError(f"restart file nx = {be} (big-endian) or {le} (little-endian) but the grid gives {nx}")
+
+
+def _write_block(fh, a: np.ndarray, e: str = ">") -> None:
+    a = np.asfortranarray(a, dtype=e + "f8")
+    np.asarray(a.shape, dtype=e + "i4").tofile(fh)
     fh.write(a.tobytes(order="F"))
 
 
-def _read_block(fh, shape: Tuple[int, int, int], what: str) -> np.ndarray:
-    nn = np.fromfile(fh, dtype="<i4", count=3)
+def _read_block(fh, shape: Tuple[int, int, int], what: str, e: str = ">") -> np.ndarray:
+    nn = np.fromfile(fh, dtype=e + "i4", count=3)
     if nn.size != 3 or tuple(int(v) for v in nn) != tuple(shape):
         raise ValueError(f"restart file field block size mismatch for {what}: found {tuple(nn)} expected {shape}")
     n = int(np.prod(shape))
-    data = np.fromfile(fh, dtype="<f8", count=n)
+    data = np.fromfile(fh, dtype=e + "f8", count=n)
     if data.size != n:
         raise ValueError(f"restart file ends inside the {what} block")
-    return data.reshape(shape, order="F")
+    return data.reshape(shape, order="F").astype(np.float64)
 
 
 def expected_size(case: Case, with_p: bool = True, with_nut: bool = False) -> int:
@@ -67,23 +93,25 @@ def expected_size(case: Case, with_p: bool = True, with_nut: bool = False) -> in
     return n
 
 
-def write_restart(path: str, case: Case, U, V, W, P, nu_t=None) -> None:
-    """The staggered full snapshot (snapshot_location = 0) of one rank."""
+def write_restart(path: str, case: Case, U, V, W, P, nu_t=None, byte_order: str = "big") -> None:
+    """The staggered full snapshot (snapshot_location = 0) of one rank, big-endian as the reference's builds
+    write it (byte_order="little" for a build without the CMakeLists.txt:210 flags)."""
+    e = _prefix(byte_order)
     x, y, z = cases.faces(case)
     with open(path, "wb") as fh:
         for f in (x, y, z, _centres(x), _centres(y), _centres(z)):
-            np.asarray([f.size], dtype="<i4").tofile(fh)
-            np.asarray(f, dtype="<f8").tofile(fh)
+            np.asarray([f.size], dtype=e + "i4").tofile(fh)
+            np.asarray(f, dtype=e + "f8").tofile(fh)
         for a in (U, V, W, P):
-            _write_block(fh, a)
+            _write_block(fh, a, e)
         if nu_t is not None:
-            _write_block(fh, nu_t)
+            _write_block(fh, nu_t, e)
 
 
 def read_restart(path: str, case: Case, read_nut: bool = False, rtol: float = 1e-12) -> Dict[str, np.ndarray]:
-    """U, V, W, P (and nu_t) of a restart file written for this case's grid; raises ValueError as the reference
-    aborts: chunked snapshot, short file, face-count mismatch, block-shape mismatch, or (here) coordinates that do
-    not match the case's grid."""
+    """U, V, W, P (and nu_t) of a restart file written for this case's grid, in the byte order its first word shows;
+    raises ValueError as the reference aborts: chunked snapshot, short file, face-count mismatch, block-shape
+    mismatch, or (here) coordinates that do not match the case's grid."""
     with open(path, "rb") as fh:
         first = np.fromfile(fh, dtype="<i4", count=1)
         if first.size == 1 and int(first[0]) == SNAP_MAGIC:
@@ -92,29 +120,31 @@ def read_restart(path: str, case: Case, read_nut: bool = False, rtol: float = 1e
     need = expected_size(case, with_p=True)
     if size < need:
         raise ValueError(f"restart file is smaller than expected for the grid: {size} < {need} bytes")
+    e = _prefix(detect_byte_order(path, case.nx))
     x, y, z = cases.faces(case)
     want = [("nx", x), ("ny", y), ("nz", z), ("nxm", _centres(x)), ("nym", _centres(y)), ("nzm", _centres(z))]
     out: Dict[str, np.ndarray] = {}
     sh = case.shapes()
     with open(path, "rb") as fh:
         for name, ref in want:
-            n = int(np.fromfile(fh, dtype="<i4", count=1)[0])
+            n = int(np.fromfile(fh, dtype=e + "i4", count=1)[0])
             if n != ref.size:
                 raise ValueError(f"restart file {name} = {n} but the grid gives {ref.size}")
-            f = np.fromfile(fh, dtype="<f8", count=n)
+            f = np.fromfile(fh, dtype=e + "f8", count=n)
             scale = max(1.0, float(np.abs(ref).max()))
             if np.abs(f - ref).max() > rtol * scale:
                 raise ValueError(f"restart file coordinates ({name}) differ from the grid")
         for key in ("U", "V", "W", "P"):
-            out[key] = _read_block(fh, sh[key], key)
+            out[key] = _read_block(fh, sh[key], key, e)
         if read_nut:
-            out["nu_t"] = _read_block(fh, sh["P"], "nu_t")
+            out["nu_t"] = _read_block(fh, sh["P"], "nu_t", e)
     return out
 
 
-def write_wmf(path: str, case: Case, planes: Dict[str, np.ndarray]) -> None:
+def write_wmf(path: str, case: Case, planes: Dict[str, np.ndarray], byte_order: str = "big") -> None:
     """<snapshot>.wmf from the filter planes in the reference shapes (ux/wx/tx (nx,2,nzg), uz/wz/tz (nxg,2,nz));
     the x/z ghost planes are written as zero, as write_distributed_field_block(..., interior_only) leaves them."""
+    e = _prefix(byte_order)
     with open(path, "wb") as fh:
         for key in ("ux", "wx", "tx", "uz", "wz", "tz"):
             a = np.array(planes[key], dtype=np.float64, order="F", copy=True)
@@ -122,20 +152,22 @@ def write_wmf(path: str, case: Case, planes: Dict[str, np.ndarray]) -> None:
             a[-1, :, :] = 0.0
             a[:, :, 0] = 0.0
             a[:, :, -1] = 0.0
-            _write_block(fh, a)
+            _write_block(fh, a, e)
 
 
 def read_wmf(path: str, case: Case) -> Optional[Dict[str, np.ndarray]]:
-    """The filter planes of <snapshot>.wmf, or None when the file does not exist (the filter then re-seeds)."""
+    """The filter planes of <snapshot>.wmf, or None when the file does not exist (the filter then re-seeds); read in
+    the byte order its first word shows."""
     if not os.path.exists(path):
         return None
     nx, nz, nxg, nzg = case.nx, case.nz, case.nxg, case.nzg
+    e = _prefix(detect_byte_order(path, nx))
     out = {}
     with open(path, "rb") as fh:
         for key in ("ux", "wx", "tx"):
-            out[key] = _read_block(fh, (nx, 2, nzg), "wmf_" + key)
+            out[key] = _read_block(fh, (nx, 2, nzg), "wmf_" + key, e)
         for key in ("uz", "wz", "tz"):
-            out[key] = _read_block(fh, (nxg, 2, nz), "wmf_" + key)
+            out[key] = _read_block(fh, (nxg, 2, nz), "wmf_" + key, e)
     return out
 
 

@@ -172,11 +172,18 @@ int dfdm_set_stage_variant(dfdm_ctx *ctx, int variant);
 int dfdm_get_stage_variant(dfdm_ctx *ctx, int *variant, double *ms_one, double *ms_pairs);
 
 /* ---- snapshots in the reference's restart format ----
- * output_data's staggered full snapshot (src/input_output.f90:1782-1880): a little-endian stream holding the mesh
- * (int32 n and n doubles for x, y, z and the centres xm, ym, zm) and then U, V, W, P and, with an SGS model, nu_t,
- * each as int32 n1, n2, n3 and the ghosted array in Fortran order. With the wall-model filter seeded
- * (wm_filter_mode = 1), write_wm_filter_state (:1990-2009) adds <path>.wmf with the six filter planes. */
+ * output_data's staggered full snapshot (src/input_output.f90:1782-1880): a stream holding the mesh (int32 n and n
+ * doubles for x, y, z and the centres xm, ym, zm) and then U, V, W, P and, with an SGS model, nu_t, each as int32 n1,
+ * n2, n3 and the ghosted array in Fortran order. With the wall-model filter seeded (wm_filter_mode = 1),
+ * write_wm_filter_state (:1990-2009) adds <path>.wmf with the six filter planes. The reference opens both files
+ * without convert= (:1842, :1996), so they take its build's default byte order, which its CMakeLists.txt:210
+ * sets to big-endian for every compiler (gfortran -fconvert=big-endian, Intel -convert big_endian, NVHPC
+ * -Mbyteswapio). dfdm_write_snapshot therefore writes big-endian; dfdm_write_snapshot_ex takes the byte order
+ * (DFDM_BIG_ENDIAN or DFDM_LITTLE_ENDIAN, the latter for a reference build without those flags). */
+#define DFDM_LITTLE_ENDIAN 0
+#define DFDM_BIG_ENDIAN    1
 int dfdm_write_snapshot(dfdm_ctx *ctx, const char *path);
+int dfdm_write_snapshot_ex(dfdm_ctx *ctx, const char *path, int byte_order);
 /* write_box_snapshot (src/input_output.f90:1699-1767, field_box :1586-1598, fill_box_block :1623-1659): the
  * chunked or cell-centred box snapshot of the face box f1..f2 (1-based faces, f1 < f2 <= nx/ny/nz), which the reference
  * writes for chunked_snapshot and for snapshot_location = 1 (then over the whole domain, f1 = 1, f2 = n). Little-endian
@@ -190,7 +197,10 @@ int dfdm_write_box_snapshot(dfdm_ctx *ctx, const char *path, const int32_t f1[3]
 /* read_input_data (src/input_output.f90:1225-1341) with the pressure block of read_pressure_restart (:1972-1977)
  * and read_wm_filter_state (:2011-2031): loads U, V, W and P from a restart file of this grid (DFDM_ERR_INVALID
  * for a chunked/cell-centred snapshot, a short file, other face counts, other coordinates or a block of another
- * shape) and the filter planes from <path>.wmf when it exists; without it the filter re-seeds on the next step. */
+ * shape) and the filter planes from <path>.wmf when it exists; without it the filter re-seeds on the next step.
+ * The byte order is taken from the file: big-endian when its first word read big-endian is nx, little-endian
+ * when read little-endian it is (the reference reads only its build's order); the .wmf is read in the same order.
+ * A first word of -4242 read little-endian marks a box snapshot, as the reference's probe (:1235) reads it. */
 int dfdm_read_snapshot(dfdm_ctx *ctx, const char *path);
 /* compute_bulk_velocity (src/monitor.f90:463-523), FP64 compensated sum. */
 int dfdm_compute_bulk_velocity(dfdm_ctx *ctx, double *Ub);

@@ -68,6 +68,10 @@ struct FFTPlan {
     int n = 0;
     std::vector<int> factors;
     std::vector<cplx> tw;  // exp(-2 pi i k / n), k = 0..n-1
+    // Per recursion level fi (sub-length len = n / twstride, radix r, m = len / r): the table entries the
+    // butterflies use, gathered once so that the inner loops index without a modulo. tw1[fi][q*m + k] =
+    // tw[(q k twstride) mod n] (twiddles), tw2[fi][q*r + s] = tw[(q s m twstride) mod n] (the radix-r DFT).
+    std::vector<std::vector<cplx>> tw1, tw2;
     void init(int n_) {
         n = n_;
         factors.clear();
@@ -82,25 +86,43 @@ struct FFTPlan {
             double a = -2.0 * pi * (double)k / (double)n;
             tw[k] = cplx(std::cos(a), std::sin(a));
         }
+        tw1.assign(factors.size(), {});
+        tw2.assign(factors.size(), {});
+        long twstride = 1;
+        for (size_t fi = 0; fi < factors.size(); ++fi) {
+            int r = factors[fi];
+            long len = n / twstride, mm = len / r;
+            tw1[fi].resize((size_t)(r * mm));
+            tw2[fi].resize((size_t)(r * r));
+            for (int q = 0; q < r; ++q) {
+                for (long k = 0; k < mm; ++k) tw1[fi][(size_t)(q * mm + k)] = tw[(size_t)((long)q * k * twstride % n)];
+                for (int s2 = 0; s2 < r; ++s2) tw2[fi][(size_t)(q * r + s2)] = tw[(size_t)((long)q * s2 * mm * twstride % n)];
+            }
+            twstride *= r;
+        }
     }
     // recursive decimation in time on strided input
-    void rec(const cplx *in, long istride, cplx *out, int len, int fi, int twstride, bool inverse) const {
+    void rec(const cplx *in, long istride, cplx *out, int len, int fi, bool inverse) const {
         if (len == 1) { out[0] = in[0]; return; }
         int r = factors[fi];
         int m = len / r;
         for (int q = 0; q < r; ++q)
-            rec(in + q * istride, istride * r, out + q * m, m, fi + 1, twstride * r, inverse);
-        std::vector<cplx> tmp(r), res(r);
+            rec(in + q * istride, istride * r, out + q * m, m, fi + 1, inverse);
+        cplx tmp_s[16], res_s[16];
+        std::vector<cplx> tmp_v, res_v;
+        cplx *tmp = tmp_s, *res = res_s;
+        if (r > 16) { tmp_v.resize(r); res_v.resize(r); tmp = tmp_v.data(); res = res_v.data(); }
+        const cplx *t1 = tw1[fi].data(), *t2 = tw2[fi].data();
         for (int k = 0; k < m; ++k) {
             for (int q = 0; q < r; ++q) {
-                cplx w = tw[(size_t)((long)q * k * twstride % n)];
+                cplx w = t1[q * m + k];
                 if (inverse) w = std::conj(w);
                 tmp[q] = out[q * m + k] * w;
             }
             for (int s = 0; s < r; ++s) {
                 cplx acc(0.0, 0.0);
                 for (int q = 0; q < r; ++q) {
-                    cplx w = tw[(size_t)((long)q * s * m * twstride % n)];
+                    cplx w = t2[q * r + s];
                     if (inverse) w = std::conj(w);
                     acc += tmp[q] * w;
                 }
@@ -112,7 +134,7 @@ struct FFTPlan {
     void exec(cplx *data, long stride, bool inverse) const {
         std::vector<cplx> in(n), out(n);
         for (int i = 0; i < n; ++i) in[i] = data[i * stride];
-        rec(in.data(), 1, out.data(), n, 0, 1, inverse);
+        rec(in.data(), 1, out.data(), n, 0, inverse);
         for (int i = 0; i < n; ++i) data[i * stride] = out[i];
     }
 };

@@ -12,7 +12,7 @@ from dfdm.native import Solver
 
 pytestmark = pytest.mark.gpu
 
-SMALL = ["tgv_small", "chan_small", "chan_les_amd_small"]
+SMALL = ["tgv_small", "chan_small", "chan_les_amd_small", "chan_les_vreman_small"]
 TOL64 = 1e-12
 TOL32 = 1e-5
 
@@ -45,7 +45,7 @@ def test_rhs_parity(oracle_mod, name):
         assert rel_l2(a[:n1, :n2, :n3], b[:n1, :n2, :n3]) <= TOL64
 
 
-@pytest.mark.parametrize("name", ["chan_les_amd_small"])
+@pytest.mark.parametrize("name", ["chan_les_amd_small", "chan_les_vreman_small"])
 def test_sgs_parity(oracle_mod, name):
     c, o, s = _pair(oracle_mod, name)
     o.compute_sgs_model()
@@ -188,7 +188,7 @@ def test_fp32_stage_variants_match_the_oracle(oracle_mod, name, variant):
         assert rel_l2(a, b) <= TOL32, (key, rel_l2(a, b))
 
 
-@pytest.mark.parametrize("name", ["chan_les_amd_small", "tgv_small", "chan_small"])
+@pytest.mark.parametrize("name", ["chan_les_amd_small", "chan_les_vreman_small", "tgv_small", "chan_small"])
 def test_fp32_stage_variants_agree(name):
     c = cases.get(name)
     state = cases.initial_condition(c)

@@ -34,11 +34,12 @@ def test_restart_from_the_library_snapshot_continues_the_run(tmp_path):
         assert rel_l2(x, y) <= 1e-13
 
 
-def test_library_reads_the_host_written_restart(tmp_path):
+@pytest.mark.parametrize("order", ["big", "little"])
+def test_library_reads_the_host_written_restart(tmp_path, order):
     c = cases.chan_small()
     U, V, W, P = cases.initial_condition(c)
     f = str(tmp_path / "ic")
-    snapshot.write_restart(f, c, U, V, W, P)
+    snapshot.write_restart(f, c, U, V, W, P, byte_order=order)
     s = Solver(c, "fp64")
     s.read_snapshot(f)
     ref = Solver(c, "fp64")
@@ -49,6 +50,27 @@ def test_library_reads_the_host_written_restart(tmp_path):
     with pytest.raises(DfdmError) as e:
         other.read_snapshot(f)
     assert e.value.code == 1 and "coordinates" in str(e.value)
+
+
+@pytest.mark.parametrize("order", ["big", "little"])
+def test_library_writes_what_the_host_writer_writes(tmp_path, order):
+    """The library's restart and .wmf are byte for byte the host restatement's, big-endian by default (as the
+    reference's builds write them) and little-endian on request."""
+    c = cases.chan_les_amd_small()
+    s = Solver(c, "fp64")
+    s.set_state(*cases.initial_condition(c))
+    s.compute_time_step_RK3(2)
+    a, b = str(tmp_path / "lib"), str(tmp_path / "host")
+    if order == "big":
+        s.write_snapshot(a)
+    else:
+        s.write_snapshot(a, byte_order="little")
+    snapshot.write_restart(b, c, *s.get_state(), nu_t=s.get_nu_t(), byte_order=order)
+    assert open(a, "rb").read() == open(b, "rb").read()
+    assert snapshot.detect_byte_order(a + ".wmf", c.nx) == order
+    snapshot.write_wmf(b + ".wmf", c, snapshot.read_wmf(a + ".wmf", c), byte_order=order)
+    assert open(a + ".wmf", "rb").read() == open(b + ".wmf", "rb").read()
+    s.close()
 
 
 @pytest.mark.parametrize("name", ["chan_les_amd_small", "tgv_small"])

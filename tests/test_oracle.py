@@ -269,3 +269,30 @@ def test_hybrid_dissipation_symbol(oracle_mod, order, factor, power):
     o = oracle_mod.Oracle(c)
     o.set_state(U, V, W, P)
     assert np.array_equal(o.compute_rhs()[2], out[0])
+
+
+@pytest.mark.parametrize("model", [1, 2])
+def test_eddy_viscosity_of_a_two_component_shear(oracle_mod, model):
+    """Known answer of compute_vreman (src/sgs_model.f90:118-216) for u = s*y, v = r*x on a uniform grid, where
+    the only gradients are a21 = s and a12 = r:
+      Vreman: B_beta = (dx*r)^2 (dy*s)^2, alpha^2 = s^2 + r^2, nu_t = 2.5 Cs^2 sqrt(B_beta / alpha^2);
+      AMD: -beta:S = -(b12 (a12 + a21)) with b12 = dx^2 a11 a12 + dy^2 a21 a22 + dz^2 a31 a32 = 0, so nu_t = 0.
+    A single shear (r = 0) gives B_beta = 0, so Vreman also vanishes there (its design property)."""
+    c = cases.chan_small().with_(sgs_model=model, flat_wall_model_flag=0)
+    x, y, z = cases.faces(c)
+    xc, yc = cases.centres(x), cases.centres(y)
+    dx, dy = x[1] - x[0], y[1] - y[0]
+    for s, r in ((0.7, 0.3), (1.3, 0.0)):
+        U, V, W, P = cases.allocate_state(c)
+        U[:] = s * yc[None, :, None]           # U(i,j,k) sits at (x_i, yc_j, zc_k)
+        V[:] = r * xc[:, None, None]           # V(i,j,k) sits at (xc_i, y_j, zc_k)
+        o = oracle_mod.Oracle(c)
+        o.set_state(U, V, W, P)
+        o.compute_sgs_model()
+        nut = o.get_nu_t()[2:-2, 2:-2, 2:-2]   # away from every ghost
+        if model == 1:
+            want = 2.5 * c.Cs_vreman ** 2 * math.sqrt((dx * r) ** 2 * (dy * s) ** 2 / (s * s + r * r))
+        else:
+            want = 0.0
+        assert np.max(np.abs(nut - want)) <= 1e-13 * max(want, 1e-3), (model, s, r, nut.min(), nut.max(), want)
+        o.close()
