@@ -56,7 +56,11 @@ def parse():
     ap.add_argument("--stage-kernel", choices=["auto", "one-cell", "pairs"], default="auto",
                     help="FP32 stage kernel: the autotuner's choice (default) or a fixed one (profiling runs, where the "
                          "serialised launches under a profiler skew the autotuner's timing)")
-    ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-vs-FP64 report of the other configs")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the report of every config's FP32 and FP64 results against the FP64 oracle")
+    ap.add_argument("--oracle-steps", type=int, default=20,
+                    help="steps of the bench workload compared with the oracle in the accuracy report (the other "
+                         "configs use their own step counts; the full 120-step comparison is a GPU test)")
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-rate", type=float, default=4.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--serve-saturated", type=int, default=48,
@@ -209,8 +213,13 @@ def run_reference(args, c):
     U, V, W, P = cases.initial_condition(c)
     o.set_state(U, V, W, P)
     budget = 90.0
+    nwarm = max(1, args.warmup)
     t0 = time.perf_counter()
-    o.step(1)   # warm-up: first touch of every array
+    for w in range(nwarm):   # warm-up: first touch of every array, then as many as the run asks for
+        o.step(1)
+        if time.perf_counter() - t0 > budget / 3:
+            nwarm = w + 1
+            break
     t_first = time.perf_counter() - t0
     n = 0
     t0 = time.perf_counter()
@@ -221,8 +230,8 @@ def run_reference(args, c):
             break
     el = time.perf_counter() - t0
     value = c.n_cells * n / el
-    sample = f"{n} full RK3 steps of the {workload_name(c)} case after 1 warm-up step"
-    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": n, "warmup": 1,
+    sample = f"{n} full RK3 steps of the {workload_name(c)} case after {nwarm} warm-up step(s)"
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": n, "warmup": nwarm,
             "ms_per_step": 1e3 * el / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": data_desc(c),
             "config": config_dict(c), "impl": "reference",
@@ -340,7 +349,7 @@ def main():
            "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "fp32-mixed (FP32 fields/stencils/FFTs, FP64 y-solves and reductions)",
            "data": data_desc(c),
-           "config": config_dict(c, {"parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"}),
+           "config": config_dict(c), "replicas": ws,
            "clocks": clocks, "gpu_launches": launches,
            "tuning": {"stage_kernel": ["one cell per thread", "packed FP32x2 pairs"][variant],
                       "stage_ms_one_cell": ms_one, "stage_ms_packed_pairs": ms_pairs}}
@@ -479,11 +488,22 @@ def main():
                                             "path": "dfdm_set_state + dfdm_compute_time_step_rk3(1) + dfdm_get_state "
                                                     "per step"}}
 
-    # ---- every other config at its stated step count: FP32-mixed against the FP64 form (the oracle's arithmetic) ----
+    # ---- every config at its stated step count: FP32-mixed and FP64 against the FP64 oracle and each other ----
     if not args.no_accuracy and rank == 0:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        oracle.build()
+        oracle.set_threads(os.cpu_count() or 1)
+
+        def rel_l2(a, b):
+            return {k: float(np.linalg.norm((x - y).ravel()) / max(np.linalg.norm(y.ravel()), 1e-300))
+                    for k, x, y in zip("UVWP", a, b)}
+
         acc = {}
-        for name in ("tgv64", "chan180", "les395"):
+        runs = [("tgv64", None), ("chan180", None), ("les395", None), (args.config, args.oracle_steps)]
+        for name, nsteps in runs:
             cc = cases.get(name)
+            nsteps = cc.nsteps if nsteps is None else nsteps
             st = cases.initial_condition(cc)
             res = {}
             for prec in ("fp32", "fp64"):
@@ -494,16 +514,27 @@ def main():
                 a0 = torch.cuda.Event(enable_timing=True)
                 a1 = torch.cuda.Event(enable_timing=True)
                 a0.record(stream)
-                sv.compute_time_step_RK3_async(cc.nsteps)
+                sv.compute_time_step_RK3_async(nsteps)
                 a1.record(stream)
                 a1.synchronize()
-                res[prec] = (sv.get_state(), cc.n_cells * cc.nsteps / (a0.elapsed_time(a1) * 1e-3))
+                res[prec] = (sv.get_state(), cc.n_cells * nsteps / (a0.elapsed_time(a1) * 1e-3))
                 sv.close()
-            rel = {k: float(np.linalg.norm((x - y).ravel()) / max(np.linalg.norm(y.ravel()), 1e-300))
-                   for k, x, y in zip("UVWP", res["fp32"][0], res["fp64"][0])}
-            acc[name] = {"steps": cc.nsteps, "cells": cc.n_cells, "rel_l2_fp32_vs_fp64": rel,
+            o = oracle.Oracle(cc)
+            o.set_state(*st)
+            t0 = time.perf_counter()
+            o.step(nsteps)
+            t_oracle = time.perf_counter() - t0
+            want = o.get_state()
+            o.close()
+            acc[name] = {"steps": nsteps, "cells": cc.n_cells,
+                         "rel_l2_fp32_vs_oracle": rel_l2(res["fp32"][0], want),
+                         "rel_l2_fp64_vs_oracle": rel_l2(res["fp64"][0], want),
+                         "rel_l2_fp32_vs_fp64": rel_l2(res["fp32"][0], res["fp64"][0]),
                          "fp32_cell_steps_per_s": res["fp32"][1], "fp64_cell_steps_per_s": res["fp64"][1],
+                         "oracle_s": t_oracle,
                          "note": "timing includes the first (ungraphed) step and the graph capture"}
+        acc["bars"] = {"fp64_vs_oracle": 1e-12, "fp32_vs_oracle": 1e-5,
+                       "oracle": "FP64 C++ restatement of the reference, same grid, initial condition and dt"}
         out["accuracy"] = acc
 
     # ---- serving stream ----

@@ -21,7 +21,7 @@
 //   src/boundary_conditions.f90:186-804 apply_boundary_conditions and the periodic / Robin rules
 //   src/projection.f90:21-639         divergence, solve_poisson_equation (CPU chain), projection, P save
 //   src/initialization.f90:243-274,326-345,417-539,629-660  centres, dx, kxx/kzz/kyy, Dyy, weights, RK
-//   src/monitor.f90:463-523           compute_bulk_velocity
+//   src/monitor.f90:463-523           compute_bulk_velocity (compensated sums: the reference's order is unspecified)
 // Third-party arithmetic restated from its published algorithm: FFTW3's complex DFT (here a mixed-radix
 // Cooley-Tukey FFT) and LAPACK zgtsv (Gaussian elimination with partial pivoting, LAPACK 3.x).
 
@@ -1073,16 +1073,27 @@ struct Oracle {
     }
 
     // ---- compute_bulk_velocity (src/monitor.f90:463-523) ----
+    // The reference accumulates the two sums in an unspecified order (an !$acc parallel loop reduction(+:...), then
+    // MPI_Allreduce over the ranks), so no one rounding of them is the reference's. This restatement evaluates each
+    // sum with Kahan compensation, within a few ulps of its exact value: a sequential sum carries O(sqrt(N) eps)
+    // relative error, which the constant-flux shift feeds back into U at every step (on the 128 x 96 x 128 channel
+    // a sequential and a compensated oracle differ by 9e-12 relative L2 in V and W after 200 steps).
     double compute_bulk_velocity() {
         int ihi = nxg - 2, jhi = nyg - 1, khi = nzg - 2;
         if (y_bc_type == 0) jhi = nyg - 2;
-        double local_sum = 0.0, local_wgt = 0.0;
+        double local_sum = 0.0, local_wgt = 0.0, c_sum = 0.0, c_wgt = 0.0;
         for (int k = 2; k <= khi; ++k)
             for (int j = 2; j <= jhi; ++j) {
                 double dy_j = (y[j] - y[j - 1]) * (z[k] - z[k - 1]);
                 for (int i = 2; i <= ihi; ++i) {
-                    local_sum = local_sum + 0.5 * (U(i, j, k) + U(i - 1, j, k)) * dy_j;
-                    local_wgt = local_wgt + dy_j;
+                    const double xs = 0.5 * (U(i, j, k) + U(i - 1, j, k)) * dy_j - c_sum;
+                    const double ts = local_sum + xs;
+                    c_sum = (ts - local_sum) - xs;
+                    local_sum = ts;
+                    const double xw = dy_j - c_wgt;
+                    const double tw = local_wgt + xw;
+                    c_wgt = (tw - local_wgt) - xw;
+                    local_wgt = tw;
                 }
             }
         return local_sum / std::max(local_wgt, 1e-14);

@@ -20,6 +20,7 @@ def test_reference_arm_json_line():
         assert key in d, key
     assert d["impl"] == "reference" and d["metric"] == "cell-RK3-steps/s" and d["higher_is_better"] is True
     assert d["value"] > 0 and 1 <= d["steps"] <= 2 and d["config"]["workload"].startswith("tgv64")
+    assert d["warmup"] == 1 and "parallelism" not in d["config"]
     assert "Taylor-Green" in d["data"]
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and cb["sample"]
