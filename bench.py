@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream measurement")
     ap.add_argument("--no-adaptive", action="store_true", help="skip the adaptive-time-step run")
     ap.add_argument("--no-hybrid", action="store_true", help="skip the advection_scheme = 2 runs")
-    ap.add_argument("--stage-kernel", choices=["auto", "one-cell", "pairs"], default="auto",
+    ap.add_argument("--stage-kernel", choices=["auto", "one-cell", "pairs", "tma"], default="auto",
                     help="FP32 stage kernel: the autotuner's choice (default) or a fixed one (profiling runs, where the "
                          "serialised launches under a profiler skew the autotuner's timing)")
     ap.add_argument("--no-accuracy", action="store_true",
@@ -320,7 +320,7 @@ def main():
         s = Solver(case or c, prec, graphs=True)
         s.set_stream(sh)
         if prec == "fp32" and args.stage_kernel != "auto":
-            s.set_stage_variant(0 if args.stage_kernel == "one-cell" else 1)
+            s.set_stage_variant({"one-cell": 0, "pairs": 1, "tma": 2}[args.stage_kernel])
         s.set_state(U, V, W, P)
         if adaptive:
             s.set_adaptive_dt(True, 0.5, 0.9)
@@ -351,8 +351,10 @@ def main():
            "data": data_desc(c),
            "config": config_dict(c), "replicas": ws,
            "clocks": clocks, "gpu_launches": launches,
-           "tuning": {"stage_kernel": ["one cell per thread", "packed FP32x2 pairs"][variant],
-                      "stage_ms_one_cell": ms_one, "stage_ms_packed_pairs": ms_pairs}}
+           "tuning": {"stage_kernel": ["one cell per thread", "packed FP32x2 pairs",
+                                       "packed FP32x2 pairs, TMA plane tiles"][variant],
+                      "stage_ms_one_cell": ms_one, "stage_ms_packed_pairs": ms_pairs,
+                      "stage_ms_tma": s32.stage_timing(2)}}
 
     # ---- plain FP64 form and the FP32-vs-FP64 error after warmup + K steps from the same state ----
     if not args.no_fp64:

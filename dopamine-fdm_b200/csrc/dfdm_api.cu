@@ -1,5 +1,6 @@
 // dfdm_api.cu -- the C ABI (include/dfdm.h): context set-up, the RK3 step driver, state transfer and the unit
 // entry points that mirror the reference's Fortran subroutines.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -23,6 +24,7 @@
 #include "kernels_poisson.cuh"
 #include "kernels_step.cuh"
 #include "kernels_hybrid.cuh"
+#include "kernels_tma.cuh"
 
 using namespace dfdm;
 
@@ -33,7 +35,7 @@ thread_local long long g_launches = 0;   // kernels enqueued by this thread (rea
 
 struct TuneEntry {
     int variant;
-    double ms[2];
+    double ms[3];
 };
 std::mutex g_tune_mu;
 std::map<std::array<int, 6>, TuneEntry> g_tune;   // stage-kernel choice per (device, Nx, Ny, Nz, LES, wall model)
@@ -60,6 +62,23 @@ int fail(int code, const std::string &msg) {
     } while (0)
 
 const double PI = 4.0 * std::atan(1.0);   // pi = 4d0*datan(1d0)
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point, so the library loads where no driver is present
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    });
+    return fn;
+}
 const int MAX_NY = 1024;                  // longest y line of the shared-memory y transform
 
 }  // namespace
@@ -93,6 +112,7 @@ struct dfdm_ctx {
     bool fuse_ok = false, fused = false;
     void *nut = nullptr, *p = nullptr, *phi = nullptr, *spec = nullptr, *rhs3 = nullptr;
     void *my_t = nullptr, *mz_t = nullptr;      // 6 metric arrays each, storage type
+    void *zm8 = nullptr;                        // FP32: the z metrics of each plane in load8 order (StepArgs::zm8)
     double *my_d = nullptr, *mz_d = nullptr;    // same in double
     void *tw_x = nullptr, *twr_x = nullptr, *tw_z = nullptr, *tw_y = nullptr;
     FFTPlan plan_x{}, plan_z{}, plan_y{};
@@ -127,8 +147,16 @@ struct dfdm_ctx {
     int kc_stage = 8, kc_sgs = 8;               // z-planes per block of the tiled kernels
     int kc_stage2 = 8;                          // the same for the packed FP32 stage kernel
     int kc_hyb = 32;                            // the same for the hybrid-scheme kernel
-    int stage_variant = 0;                      // FP32 stage kernel in use: 0 one cell per thread, 1 packed pairs
-    double stage_ms[2] = {-1.0, -1.0};          // autotuner timings of the two variants (ms per launch), -1 = not timed
+    int stage_variant = 0;                      // FP32 stage kernel in use: 0 one cell per thread, 1 packed pairs,
+                                                // 2 packed pairs with TMA plane tiles
+    double stage_ms[3] = {-1.0, -1.0, -1.0};    // autotuner timings of the variants (ms per launch), -1 = not timed
+    // TMA stage kernel (variant 2): eligible with FP32, walls in y and Nx a multiple of 4.  Tensor maps of each input
+    // buffer (main box and x-wrap patch box), encoded on first use; a host-mapped flag that a bounded mbarrier wait
+    // sets when it gives up.
+    bool tma_ok = false;
+    int kc_tma = 8;
+    std::map<std::pair<const void *, int>, std::array<CUtensorMap, 2>> tmaps;
+    int *h_err = nullptr, *d_err = nullptr;
     size_t smem_x = 0, smem_z = 0, smem_y = 0;
     // two-level register transforms (fft_reg.cuh) where the length has a split; Stockham otherwise
     bool x2 = false, z2 = false, y2 = false;
@@ -271,6 +299,7 @@ template <typename T> StepArgs<T> step_args(dfdm_ctx *c) {
     a.ubd = c->d_ubd;
     a.adv = (const T *)c->adv;
     a.phi = (const T *)c->phi;
+    a.zm8 = (const float *)c->zm8;
     return a;
 }
 
@@ -431,6 +460,7 @@ template <typename T> struct Impl {
             int occ2 = 1;
             CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, fn2, 256, 0));
             c->kc_stage2 = choose_kc(d, occ2, nsm, TILE_X2);
+            if (int rc = setup_tma(c, nsm)) return rc;
         }
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tiled<T, false, false, TILE_X, TILE_Y, 1>, TILE_X * TILE_Y, 0));
         c->kc_sgs = choose_kc(d, occ, nsm);
@@ -457,7 +487,75 @@ template <typename T> struct Impl {
         return setup_fft2l(c);
     }
 
-    // FP32-mixed stage 3 carries the increment du = u* - uo through the Poisson solve once the resident velocity
+    // The TMA stage kernel (variant 2): eligible with walls in y and Nx a multiple of 4 (16-byte row strides and box
+    // origins), when the driver's tensor-map encoder is reachable.  Every instantiation a step can launch gets its
+    // dynamic shared memory; the error flag lives in host-mapped pinned memory.
+    template <bool LES, bool WM, bool HYB, bool CORR> static int tma_attr() {
+        if constexpr (sizeof(T) == 4) {
+            CK(cudaFuncSetAttribute(k_tma2<LES, WM, HYB, CORR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sizeof(TmaSmem<LES, CORR>)));
+        }
+        return DFDM_OK;
+    }
+    static int setup_tma(dfdm_ctx *c, int nsm) {
+        const Dims &d = c->d;
+        c->tma_ok = false;
+        if (d.yper || d.Nx % 4 != 0 || !encode_tiled()) return DFDM_OK;
+        int rc = DFDM_OK;
+        for (int les = 0; les < 2 && !rc; ++les)
+            for (int wm = 0; wm < 2 && !rc; ++wm)
+                for (int hyb = 0; hyb < 2 && !rc; ++hyb) {
+                    if (les) rc = wm ? (hyb ? tma_attr<true, true, true, false>() : tma_attr<true, true, false, false>())
+                                     : (hyb ? tma_attr<true, false, true, false>() : tma_attr<true, false, false, false>());
+                    else rc = wm ? (hyb ? tma_attr<false, true, true, false>() : tma_attr<false, true, false, false>())
+                                 : (hyb ? tma_attr<false, false, true, false>() : tma_attr<false, false, false, false>());
+                }
+        if (!rc) rc = tma_attr<false, true, false, true>();
+        if (!rc) rc = tma_attr<false, false, false, true>();
+        if (rc) return rc;
+        int occ = 1;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tma2<false, false, false, true>, 256,
+                                                         sizeof(TmaSmem<false, true>)));
+        c->kc_tma = choose_kc(d, std::max(1, occ), nsm, TILE_X2);
+        if (!c->h_err) {
+            void *h = nullptr, *dp = nullptr;
+            CK(cudaHostAlloc(&h, sizeof(int), cudaHostAllocMapped));
+            *(volatile int *)h = 0;
+            if (cudaHostGetDevicePointer(&dp, h, 0) != cudaSuccess) {
+                cudaFreeHost(h);
+                return fail(DFDM_ERR_CUDA, "cudaHostGetDevicePointer of the stage kernel's error flag failed");
+            }
+            c->h_err = (int *)h;
+            c->d_err = (int *)dp;
+        }
+        c->tma_ok = true;
+        return DFDM_OK;
+    }
+    // the main box (72 x rows x 1) and the x-wrap patch box (4 x rows x 1) of a field buffer, encoded once
+    static int tensor_maps(dfdm_ctx *c, const void *buf, int rows, CUtensorMap *main_box, CUtensorMap *patch_box) {
+        auto key = std::make_pair(buf, rows);
+        auto it = c->tmaps.find(key);
+        if (it == c->tmaps.end()) {
+            const Dims &d = c->d;
+            std::array<CUtensorMap, 2> m;
+            const cuuint64_t dims[3] = {(cuuint64_t)d.Nx, (cuuint64_t)d.Ny, (cuuint64_t)d.Nz};
+            const cuuint64_t strides[2] = {(cuuint64_t)d.Nx * sizeof(float), (cuuint64_t)d.Nx * d.Ny * sizeof(float)};
+            const cuuint32_t estr[3] = {1, 1, 1};
+            for (int b = 0; b < 2; ++b) {
+                const cuuint32_t box[3] = {b == 0 ? (cuuint32_t)tma::BX : (cuuint32_t)tma::PW, (cuuint32_t)rows, 1};
+                CUresult r = encode_tiled()(&m[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void *>(buf), dims,
+                                            strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                if (r != CUDA_SUCCESS) return fail(DFDM_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+            }
+            it = c->tmaps.emplace(key, m).first;
+        }
+        *main_box = it->second[0];
+        *patch_box = it->second[1];
+        return DFDM_OK;
+    }
+
+
     // is the output of a full step (so div uo vanishes up to the rounding of its storage).  Solving for div(du)
     // alone keeps that rounding noise, amplified by dx/dt, out of the saved pressure P = phi/(dt*3/4); the
     // correction forms u = uo + du - grad(phi).  Right after set_state (a field that need not be solenoidal), in
@@ -468,50 +566,64 @@ template <typename T> struct Impl {
 
     // CORR: the input planes are the previous stage's u* (us2/vs2/ws2 after the swap in step_enqueue), corrected in
     // the loader; with fused corrections the step-start velocity U doubles as uo
-    template <bool LES, bool WM, bool HYB, bool CORR> static void stage_launch(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
+    template <bool LES, bool WM, bool HYB, bool CORR> static int stage_launch(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
         const Dims &d = c->d;
         const T *iu = CORR ? f(c->us2) : f(c->u), *iv = CORR ? f(c->vs2) : f(c->v), *iw = CORR ? f(c->ws2) : f(c->w);
         T *uo = c->fused && !rhs_only ? f(c->u) : f(c->uo), *vo = c->fused && !rhs_only ? f(c->v) : f(c->vo);
         T *wo = c->fused && !rhs_only ? f(c->w) : f(c->wo);
         if constexpr (sizeof(T) == 4) {
+            if (c->stage_variant == 2 && c->tma_ok) {
+                TmaMaps tm;
+                std::memset(&tm, 0, sizeof(tm));
+                const void *in[4] = {iu, iv, iw, LES ? c->nut : iu};
+                for (int q = 0; q < 4; ++q)
+                    if (int rc = tensor_maps(c, in[q], tma::BY, &tm.f[q], &tm.fp[q])) return rc;
+                if (CORR)
+                    if (int rc = tensor_maps(c, c->phi, tma::BYP, &tm.phi, &tm.phip)) return rc;
+                k_tma2<LES, WM, HYB, CORR><<<tile_grid(d, c->kc_tma, TILE_X2), 256, sizeof(TmaSmem<LES, CORR>), c->stream>>>(
+                    step_args<T>(c), tm, c->wsd.tau_x, c->wsd.tau_z, sc, c->kc_tma, uo, vo, wo, f(c->f1u), f(c->f1v),
+                    f(c->f1w), f(c->us), f(c->vs), f(c->wsf), rhs_only, c->d_err);
+                return DFDM_OK;
+            }
             if (c->stage_variant == 1) {
                 k_tiled2<LES, WM, 8, HYB, CORR><<<tile_grid(d, c->kc_stage2, TILE_X2), 256, 0, c->stream>>>(step_args<T>(c),
                     iu, iv, iw, LES ? f(c->nut) : nullptr, c->wsd.tau_x, c->wsd.tau_z, sc, c->kc_stage2,
                     uo, vo, wo, f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf), rhs_only);
-                return;
+                return DFDM_OK;
             }
         }
         k_tiled<T, LES, WM, TILE_X, TILE_Y, HYB ? 2 : 0, CORR><<<tile_grid(d, c->kc_stage), TILE_X * TILE_Y, 0, c->stream>>>(
             step_args<T>(c), iu, iv, iw, LES ? f(c->nut) : nullptr, c->wsd.tau_x, c->wsd.tau_z, sc,
             c->kc_stage, uo, vo, wo, f(c->f1u), f(c->f1v), f(c->f1w), f(c->us), f(c->vs), f(c->wsf),
             rhs_only, nullptr);
+        return DFDM_OK;
     }
-    template <bool HYB> static void stage_dispatch(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
+    template <bool HYB> static int stage_dispatch(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
         if constexpr (sizeof(T) == 8) {   // FP64 keeps the runtime wall-model flag
-            if (c->les) stage_launch<true, true, HYB, false>(c, sc, rhs_only); else stage_launch<false, true, HYB, false>(c, sc, rhs_only);
+            return c->les ? stage_launch<true, true, HYB, false>(c, sc, rhs_only) : stage_launch<false, true, HYB, false>(c, sc, rhs_only);
         } else {
             if (c->les) {
-                if (c->wm) stage_launch<true, true, HYB, false>(c, sc, rhs_only); else stage_launch<true, false, HYB, false>(c, sc, rhs_only);
+                if (c->wm) return stage_launch<true, true, HYB, false>(c, sc, rhs_only); else return stage_launch<true, false, HYB, false>(c, sc, rhs_only);
             } else {
-                if (c->wm) stage_launch<false, true, HYB, false>(c, sc, rhs_only); else stage_launch<false, false, HYB, false>(c, sc, rhs_only);
+                if (c->wm) return stage_launch<false, true, HYB, false>(c, sc, rhs_only); else return stage_launch<false, false, HYB, false>(c, sc, rhs_only);
             }
         }
     }
     // stages 2 and 3 with the fused correction (no LES, no hybrid scheme: fuse_eligible)
-    static void stage_dispatch_corr(dfdm_ctx *c, const StageCoef &sc) {
-        if constexpr (sizeof(T) == 8) stage_launch<false, true, false, true>(c, sc, nullptr);
-        else if (c->wm) stage_launch<false, true, false, true>(c, sc, nullptr);
-        else stage_launch<false, false, false, true>(c, sc, nullptr);
+    static int stage_dispatch_corr(dfdm_ctx *c, const StageCoef &sc) {
+        if constexpr (sizeof(T) == 8) return stage_launch<false, true, false, true>(c, sc, nullptr);
+        else if (c->wm) return stage_launch<false, true, false, true>(c, sc, nullptr);
+        else return stage_launch<false, false, false, true>(c, sc, nullptr);
     }
 
     static int stage_kernel(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
-        if (c->adv) stage_dispatch<true>(c, sc, rhs_only); else stage_dispatch<false>(c, sc, rhs_only);
+        if (int rc = c->adv ? stage_dispatch<true>(c, sc, rhs_only) : stage_dispatch<false>(c, sc, rhs_only)) return rc;
         CKL();
         return DFDM_OK;
     }
 
-    // Autotuner of the FP32 stage kernel: times both variants on this grid (a stage-2 launch, 2 warm-up + 5 timed)
-    // and keeps the faster.  The choice is cached per device, grid shape and model flags for the process, so a
+    // Autotuner of the FP32 stage kernel: times the variants on this grid (a stage-2 launch, 2 warm-up + 5 timed;
+    // the TMA variant where the grid allows it) and keeps the fastest.  The choice is cached per device, grid shape and model flags for the process, so a
     // serving loop that opens many contexts of one shape pays the timing once.
     static int tune_stage(dfdm_ctx *c, bool force) {
         if constexpr (sizeof(T) == 8) { (void)force; c->stage_variant = 0; return DFDM_OK; }
@@ -524,7 +636,7 @@ template <typename T> struct Impl {
         auto it = g_tune.find(key);
         if (it != g_tune.end() && !force) {
             c->stage_variant = it->second.variant;
-            c->stage_ms[0] = it->second.ms[0]; c->stage_ms[1] = it->second.ms[1];
+            for (int v = 0; v < 3; ++v) c->stage_ms[v] = it->second.ms[v];
             return DFDM_OK;
         }
         StageCoef sc{2, 0.0, c->prm.dt, 0.25, 5.0 / 12.0, 0};
@@ -532,7 +644,7 @@ template <typename T> struct Impl {
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
         int rc = DFDM_OK;
-        for (int v = 0; v < 2 && !rc; ++v) {
+        for (int v = 0; v < (c->tma_ok ? 3 : 2) && !rc; ++v) {
             c->stage_variant = v;
             for (int r = 0; r < 2 && !rc; ++r) rc = stage_kernel(c, sc, nullptr);
             if (rc) break;
@@ -547,8 +659,10 @@ template <typename T> struct Impl {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         if (rc) return rc;
-        c->stage_variant = c->stage_ms[1] < c->stage_ms[0] ? 1 : 0;
-        g_tune[key] = TuneEntry{c->stage_variant, {c->stage_ms[0], c->stage_ms[1]}};
+        c->stage_variant = 0;
+        for (int v = 1; v < 3; ++v)
+            if (c->stage_ms[v] > 0.0 && c->stage_ms[v] < c->stage_ms[c->stage_variant]) c->stage_variant = v;
+        g_tune[key] = TuneEntry{c->stage_variant, {c->stage_ms[0], c->stage_ms[1], c->stage_ms[2]}};
         return DFDM_OK;
     }
 
@@ -593,7 +707,7 @@ template <typename T> struct Impl {
             sc.dtp = c->dev_dt() ? c->d_dtt : nullptr;
             sc.no_uo = c->fused ? 1 : 0;
             if (c->fused && s >= 2) {
-                stage_dispatch_corr(c, sc);
+                if (int rc = stage_dispatch_corr(c, sc)) return rc;
                 CKL();
                 return DFDM_OK;
             }
@@ -1034,6 +1148,15 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
     else {
         if ((rc = upload_as<float>(c, &c->my_t, my))) return bail(rc);
         if ((rc = upload_as<float>(c, &c->mz_t, mz))) return bail(rc);
+        // per plane k: w0(k-1), w1(k-1), w0(k), w1(k), idc(k), idc(k+1), idf(k-1), idf(k) of metric_view's layout
+        // (AxisLocal<F2>::metric_src), the same FP32 values as mz_t
+        const int L = d.Nz + 3;
+        std::vector<double> z8((size_t)d.Nz * 8);
+        for (int k = 0; k < d.Nz; ++k) {
+            const int src[8][2] = {{2, k - 1}, {3, k - 1}, {2, k}, {3, k}, {4, k}, {4, k + 1}, {5, k - 1}, {5, k}};
+            for (int t = 0; t < 8; ++t) z8[(size_t)k * 8 + t] = mz[(size_t)src[t][0] * L + 1 + src[t][1]];
+        }
+        if ((rc = upload_as<float>(c, &c->zm8, z8))) return bail(rc);
     }
     std::vector<double> dxc(d.Nx), dyc(d.Ny), dzc(d.Nz);
     for (int i = 0; i < d.Nx; ++i) dxc[i] = c->x[i + 2] - c->x[i + 1];
@@ -1180,6 +1303,7 @@ int dfdm_destroy(dfdm_ctx *c) {
     destroy_graph(c);
     for (void *p : c->allocs) cudaFree(p);
     c->allocs.clear();
+    if (c->h_err) cudaFreeHost(c->h_err);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return DFDM_OK;
@@ -1193,12 +1317,25 @@ int dfdm_set_stream(dfdm_ctx *c, void *s) {
     return DFDM_OK;
 }
 
+}  // extern "C"
+
+// the flag a bounded wait of the TMA stage kernel sets when it gives up (read after the stream has drained)
+static int check_err_flag(dfdm_ctx *c) {
+    if (c->h_err && *(volatile int *)c->h_err) {
+        *(volatile int *)c->h_err = 0;
+        return fail(DFDM_ERR_TIMEOUT, "a bounded wait of the stage kernel gave up: its tile copies did not arrive");
+    }
+    return DFDM_OK;
+}
+
+extern "C" {
+
 int dfdm_synchronize(dfdm_ctx *c) {
     if (int rc = check_ctx(c)) return rc;
     CK(cudaStreamSynchronize(c->stream));
     if (c->cin) CK(cudaStreamSynchronize(c->cin));
     if (c->cout) CK(cudaStreamSynchronize(c->cout));
-    return DFDM_OK;
+    return check_err_flag(c);
 }
 
 // copy streams, staging buffers and events of the asynchronous transfers
@@ -1510,6 +1647,7 @@ int dfdm_compute_time_step_rk3(dfdm_ctx *c, int nsteps, double *t) {
     int rc = dfdm_compute_time_step_rk3_async(c, nsteps);
     if (rc) return rc;
     CK(cudaStreamSynchronize(c->stream));
+    if (int rc1 = check_err_flag(c)) return rc1;
     if (int rc2 = pull_dtt(c, nullptr)) return rc2;
     if (t) *t = c->t;
     return DFDM_OK;
@@ -2170,8 +2308,10 @@ int dfdm_get_fused_correction(dfdm_ctx *c, int *enabled) {
 int dfdm_set_stage_variant(dfdm_ctx *c, int variant) {
     g_err.clear();
     if (int rc = check_ctx(c)) return rc;
-    if (variant < -1 || variant > 1) return fail(DFDM_ERR_INVALID, "stage variant must be -1, 0 or 1");
-    if (variant == 1 && c->prec == DFDM_FP64) return fail(DFDM_ERR_UNSUPPORTED, "the packed stage kernel is FP32 only");
+    if (variant < -1 || variant > 2) return fail(DFDM_ERR_INVALID, "stage variant must be -1, 0, 1 or 2");
+    if (variant >= 1 && c->prec == DFDM_FP64) return fail(DFDM_ERR_UNSUPPORTED, "the packed stage kernels are FP32 only");
+    if (variant == 2 && !c->tma_ok)
+        return fail(DFDM_ERR_UNSUPPORTED, "the TMA stage kernel needs walls in y and Nx a multiple of 4");
     CK(cudaStreamSynchronize(c->stream));
     destroy_graph(c);   // the captured step holds the previous kernel
     if (variant >= 0) { c->stage_variant = variant; return DFDM_OK; }
@@ -2183,6 +2323,14 @@ int dfdm_get_stage_variant(dfdm_ctx *c, int *variant, double *ms_one, double *ms
     if (variant) *variant = c->stage_variant;
     if (ms_one) *ms_one = c->stage_ms[0];
     if (ms_pairs) *ms_pairs = c->stage_ms[1];
+    return DFDM_OK;
+}
+
+int dfdm_get_stage_timing(dfdm_ctx *c, int variant, double *ms) {
+    if (int rc = check_ctx(c)) return rc;
+    if (variant < 0 || variant > 2) return fail(DFDM_ERR_INVALID, "stage variant must be 0, 1 or 2");
+    if (!ms) return fail(DFDM_ERR_INVALID, "null output");
+    *ms = c->stage_ms[variant];
     return DFDM_OK;
 }
 

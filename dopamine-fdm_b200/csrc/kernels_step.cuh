@@ -29,6 +29,9 @@ template <typename T> struct StepArgs {
     // fused correction of the previous stage (CORR kernels): its potential phi; the plane loads then hold u* and
     // the loader forms u = u* - grad(phi) exactly as k_correct does
     const T *phi;
+    // FP32: the eight z metrics of every plane in AxisLocal<F2>::load8 order, 8 consecutive values per plane (one
+    // 32-byte bulk copy per plane for the TMA stage kernel); null in FP64
+    const float *zm8;
 };
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -722,6 +725,59 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
 }
 
 
+// One thread's pair of cells (i, i+1) of plane k from the shared-memory neighbourhood q: the three right-hand sides
+// and the RK3 stage update (or, with rhs_only, the right-hand sides themselves).  zm holds the eight z metrics of
+// plane k (AxisLocal<F2>::load8 order).  Shared by the packed stage kernels.
+template <bool LES, bool WM, bool HYB, int PX>
+__device__ __forceinline__ void stage_pair(const StepArgs<float> &a, const TileQ2<PX> &q, const AxisLocal<F2> &Y,
+                                           const float *zm, const double *__restrict__ tau_x,
+                                           const double *__restrict__ tau_z, const StageCoef &sc, int i, int j, int k,
+                                           float *__restrict__ uo, float *__restrict__ vo, float *__restrict__ wo,
+                                           float *__restrict__ f1u, float *__restrict__ f1v, float *__restrict__ f1w,
+                                           float *__restrict__ us, float *__restrict__ vs, float *__restrict__ wsf,
+                                           float *__restrict__ rhs_only) {
+    const Dims &d = a.d;
+    const int p = k * (d.Nx * d.Ny) + j * d.Nx + i;
+    const bool vrow = j < d.NyV;
+    const bool upd = !rhs_only && sc.stage != 1;
+    auto ld2 = [&](const float *b) { return F2(*reinterpret_cast<const float2 *>(b + p)); };
+    auto st2 = [&](float *b, F2 x) { *reinterpret_cast<float2 *>(b + p) = x.v; };
+    F2 ou(0.0f), ov(0.0f), ow(0.0f), fu(0.0f), fv(0.0f), fw(0.0f);
+    if (upd) {
+        if (!sc.incr) { ou = ld2(uo); ow = ld2(wo); if (vrow) ov = ld2(vo); }
+        fu = ld2(f1u); fw = ld2(f1w);
+        if (vrow) fv = ld2(f1v);
+    }
+    AxisLocal<F2> Z;
+    Z.load8(zm);
+    F2 ru = rhs_u_at<F2, LES, WM>(a, q, Y, Z, tau_x, i, j, k);
+    F2 rw = rhs_w_at<F2, LES, WM>(a, q, Y, Z, tau_z, i, j, k);
+    F2 rv = vrow ? rhs_v_at<F2, LES, WM>(a, q, Y, Z, i, j, k) : F2(0.0f);
+    if constexpr (HYB) {
+        ru = ru + ld2(a.adv); rw = rw + ld2(a.adv + 2 * d.cells);
+        if (vrow) rv = rv + ld2(a.adv + d.cells);
+    }
+    if (rhs_only) {
+        st2(rhs_only, ru); st2(rhs_only + d.cells, rv); st2(rhs_only + 2 * d.cells, rw);
+    } else if (sc.stage == 1) {
+        const F2 c = F2(sc.dtp ? *sc.dtp * (8.0 / 15.0) : sc.dt_a11);
+        F2 u0 = q.Ud(0, 0, 0), w0 = q.W(0, 0, 0);
+        st2(f1u, ru); st2(us, u0 + c * ru);
+        st2(f1w, rw); st2(wsf, w0 + c * rw);
+        if (!sc.no_uo) { st2(uo, u0); st2(wo, w0); }
+        if (vrow) {
+            F2 v0 = q.V(0, 0, 0);
+            st2(f1v, rv); st2(vs, v0 + c * rv);
+            if (!sc.no_uo) st2(vo, v0);
+        }
+    } else {
+        const F2 c1 = F2(sc.c1), c2 = F2(sc.c2), dtt = F2(sc.dtp ? *sc.dtp : sc.dt);
+        st2(us, ou + dtt * (c1 * fu + c2 * ru));
+        st2(wsf, ow + dtt * (c1 * fw + c2 * rw));
+        if (vrow) st2(vs, ov + dtt * (c1 * fv + c2 * rv));
+    }
+}
+
 // FP32 stage kernel with two x-neighbour cells per thread, computed with the packed FP32x2 instructions (F2).  Same
 // loader, ghost rules and RK3 epilogue as k_tiled<float, LES, WM, ..., 0>; a block owns 64 x TY cells, one warp
 // per row of 32 cell pairs; HYB adds the dissipative terms of advection_scheme = 2 (StepArgs::adv); CORR fuses
@@ -896,7 +952,6 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
         cp_async_commit();
         const int sm_ = (k - k0) & 3, s0 = (k - k0 + 1) & 3, sp = (k - k0 + 2) & 3;
         if (active) {
-            const int p = k * plane + j * Nx + i;
             TileQ2<PX> q;
             q.c = cloc;
             q.ub[0] = ubr[0]; q.ub[1] = ubr[1]; q.ub[2] = ubr[2];
@@ -904,44 +959,8 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
             q.v[0] = sm[1][sm_]; q.v[1] = sm[1][s0]; q.v[2] = sm[1][sp];
             q.w[0] = sm[2][sm_]; q.w[1] = sm[2][s0]; q.w[2] = sm[2][sp];
             q.n[0] = sm[NF - 1][sm_]; q.n[1] = sm[NF - 1][s0]; q.n[2] = sm[NF - 1][sp];
-            const bool vrow = j < d.NyV;
-            const bool upd = !rhs_only && sc.stage != 1;
-            auto ld2 = [&](const float *b) { return F2(*reinterpret_cast<const float2 *>(b + p)); };
-            auto st2 = [&](float *b, F2 x) { *reinterpret_cast<float2 *>(b + p) = x.v; };
-            F2 ou(0.0f), ov(0.0f), ow(0.0f), fu(0.0f), fv(0.0f), fw(0.0f);
-            if (upd) {
-                if (!sc.incr) { ou = ld2(uo); ow = ld2(wo); if (vrow) ov = ld2(vo); }
-                fu = ld2(f1u); fw = ld2(f1w);
-                if (vrow) fv = ld2(f1v);
-            }
-            AxisLocal<F2> Z;
-            Z.load8(zmr[(k - k0) & 3]);
-            F2 ru = rhs_u_at<F2, LES, WM>(a, q, Y, Z, tau_x, i, j, k);
-            F2 rw = rhs_w_at<F2, LES, WM>(a, q, Y, Z, tau_z, i, j, k);
-            F2 rv = vrow ? rhs_v_at<F2, LES, WM>(a, q, Y, Z, i, j, k) : F2(0.0f);
-            if constexpr (HYB) {
-                ru = ru + ld2(a.adv); rw = rw + ld2(a.adv + 2 * d.cells);
-                if (vrow) rv = rv + ld2(a.adv + d.cells);
-            }
-            if (rhs_only) {
-                st2(rhs_only, ru); st2(rhs_only + d.cells, rv); st2(rhs_only + 2 * d.cells, rw);
-            } else if (sc.stage == 1) {
-                const F2 c = F2(sc.dtp ? *sc.dtp * (8.0 / 15.0) : sc.dt_a11);
-                F2 u0 = q.Ud(0, 0, 0), w0 = q.W(0, 0, 0);
-                st2(f1u, ru); st2(us, u0 + c * ru);
-                st2(f1w, rw); st2(wsf, w0 + c * rw);
-                if (!sc.no_uo) { st2(uo, u0); st2(wo, w0); }
-                if (vrow) {
-                    F2 v0 = q.V(0, 0, 0);
-                    st2(f1v, rv); st2(vs, v0 + c * rv);
-                    if (!sc.no_uo) st2(vo, v0);
-                }
-            } else {
-                const F2 c1 = F2(sc.c1), c2 = F2(sc.c2), dtt = F2(sc.dtp ? *sc.dtp : sc.dt);
-                st2(us, ou + dtt * (c1 * fu + c2 * ru));
-                st2(wsf, ow + dtt * (c1 * fw + c2 * rw));
-                if (vrow) st2(vs, ov + dtt * (c1 * fv + c2 * rv));
-            }
+            stage_pair<LES, WM, HYB>(a, q, Y, zmr[(k - k0) & 3], tau_x, tau_z, sc, i, j, k, uo, vo, wo, f1u, f1v, f1w,
+                                     us, vs, wsf, rhs_only);
         }
         cp_async_wait_all();
         if (more) fix(snext, k + 2);   // CORR: phi k+2 and k+3 were copied one and two iterations ago

@@ -34,7 +34,7 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_compute_cfl", "dfdm_set_stage_variant", "dfdm_get_stage_variant", "dfdm_set_adaptive_dt",
            "dfdm_get_dt", "dfdm_set_landing_time", "dfdm_output_monitor", "dfdm_output_monitor_async",
            "dfdm_set_fused_correction", "dfdm_get_fused_correction", "dfdm_set_state_async", "dfdm_get_state_async",
-           "dfdm_write_box_snapshot", "dfdm_set_landing_times", "dfdm_write_snapshot_ex"]
+           "dfdm_write_box_snapshot", "dfdm_set_landing_times", "dfdm_write_snapshot_ex", "dfdm_get_stage_timing"]
 
 
 class DfdmError(RuntimeError):
@@ -102,6 +102,7 @@ def load(build_if_missing: bool = True):
         "dfdm_compute_cfl": (c_int, [c_void_p, P, P]),
         "dfdm_set_stage_variant": (c_int, [c_void_p, c_int]),
         "dfdm_get_stage_variant": (c_int, [c_void_p, POINTER(ctypes.c_int), P, P]),
+        "dfdm_get_stage_timing": (c_int, [c_void_p, c_int, P]),
         "dfdm_set_adaptive_dt": (c_int, [c_void_p, c_int, c_double, c_double, c_double, c_double]),
         "dfdm_get_dt": (c_int, [c_void_p, P]),
         "dfdm_set_landing_time": (c_int, [c_void_p, c_int, c_double]),
@@ -323,8 +324,15 @@ class Solver:
         return bool(v.value)
 
     def set_stage_variant(self, variant: int) -> None:
-        """FP32 stage kernel: 0 one cell per thread, 1 packed pairs, -1 re-time both and keep the faster."""
+        """FP32 stage kernel: 0 one cell per thread, 1 packed pairs, 2 packed pairs with TMA plane tiles (walls in y,
+        Nx a multiple of 4), -1 re-time the eligible ones and keep the fastest."""
         _check(load().dfdm_set_stage_variant(self.h, int(variant)))
+
+    def stage_timing(self, variant: int) -> float:
+        """ms per launch of a stage-kernel variant from the set-up timing (-1 = not timed)."""
+        ms = c_double(0.0)
+        _check(load().dfdm_get_stage_timing(self.h, int(variant), ctypes.byref(ms)))
+        return ms.value
 
     def stage_variant(self):
         """(variant in use, ms per launch of variant 0, of variant 1) from the set-up timing (-1 = not timed)."""

@@ -162,14 +162,19 @@ int dfdm_solve_poisson(dfdm_ctx *ctx, const double *rhs_p_in, double *phi_out);
 #define DFDM_NOALLOC_MAX_POINTS 2097152
 int dfdm_solve_poisson_noalloc(dfdm_ctx *ctx, const double *rhs_p_in, double *phi_out);
 /* ---- tuning (no counterpart in the reference) ----
- * The FP32 stage kernel (RHS + RK3 update) has two variants: 0 computes one cell per thread on 32 x 8 tiles,
- * 1 computes two x-neighbour cells per thread with the packed FP32x2 instructions on 64 x 8 tiles. dfdm_create
- * times both on the context's grid and keeps the faster; the choice is cached per device and grid shape for the
- * process. set_stage_variant forces 0 or 1, or re-times with -1 (FP64 contexts have variant 0 only); a change drops
- * the context's captured step graph. get_stage_variant returns the variant in use and the timings (ms per launch,
- * -1 where not timed); any output pointer may be NULL. */
+ * The FP32 stage kernel (RHS + RK3 update) has three variants: 0 computes one cell per thread on 32 x 8 tiles,
+ * 1 computes two x-neighbour cells per thread with the packed FP32x2 instructions on 64 x 8 tiles, 2 is variant 1
+ * with its z-plane tiles brought in by the Tensor Memory Accelerator (3-D boxes completing on mbarriers, four planes
+ * in flight); variant 2 needs walls in y and Nx a multiple of 4. dfdm_create times the eligible variants on the
+ * context's grid and keeps the fastest; the choice is cached per device and grid shape for the process.
+ * set_stage_variant forces 0, 1 or 2 (DFDM_ERR_UNSUPPORTED where not eligible), or re-times with -1 (FP64
+ * contexts have variant 0 only); a change drops the context's captured step graph. get_stage_variant returns the
+ * variant in use and the timings of variants 0 and 1, get_stage_timing that of any variant (ms per launch, -1
+ * where not timed); any output pointer of get_stage_variant may be NULL. A bounded wait of variant 2 that gives up
+ * makes the next synchronising call (dfdm_compute_time_step_rk3, dfdm_synchronize) return DFDM_ERR_TIMEOUT. */
 int dfdm_set_stage_variant(dfdm_ctx *ctx, int variant);
 int dfdm_get_stage_variant(dfdm_ctx *ctx, int *variant, double *ms_one, double *ms_pairs);
+int dfdm_get_stage_timing(dfdm_ctx *ctx, int variant, double *ms);
 
 /* ---- snapshots in the reference's restart format ----
  * output_data's staggered full snapshot (src/input_output.f90:1782-1880): a stream holding the mesh (int32 n and n
