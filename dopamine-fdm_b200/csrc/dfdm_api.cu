@@ -1338,24 +1338,49 @@ int dfdm_synchronize(dfdm_ctx *c) {
     return check_err_flag(c);
 }
 
-// copy streams, staging buffers and events of the asynchronous transfers
+// copy streams, staging buffers and events of the asynchronous transfers, made together on first use: the context
+// publishes them only when all exist, and a failure part-way frees what it made (so a retry starts clean)
 static int ensure_async(dfdm_ctx *c) {
     if (c->cin) return DFDM_OK;
     const size_t n = (size_t)(c->nxg) * c->nyg * c->nzg;   // the largest ghosted shape
+    void *buf[8] = {};
+    cudaEvent_t ev[16] = {};
+    cudaStream_t sin = nullptr, sout = nullptr;
+    auto unwind = [&](int rc) {
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+        if (sin) cudaStreamDestroy(sin);
+        if (sout) cudaStreamDestroy(sout);
+        for (void *b : buf) {
+            if (!b) continue;
+            auto it = std::find(c->allocs.begin(), c->allocs.end(), b);
+            if (it != c->allocs.end()) c->allocs.erase(it);
+            cudaFree(b);
+        }
+        return rc;
+    };
+    for (int q = 0; q < 8; ++q)
+        if (int rc = dalloc(c, &buf[q], n * sizeof(double))) return unwind(rc);
+    for (int q = 0; q < 16; ++q)
+        if (cudaEventCreateWithFlags(&ev[q], cudaEventDisableTiming) != cudaSuccess)
+            return unwind(fail(DFDM_ERR_CUDA, "cudaEventCreateWithFlags of the transfer events failed"));
+    if (cudaStreamCreateWithFlags(&sin, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&sout, cudaStreamNonBlocking) != cudaSuccess)
+        return unwind(fail(DFDM_ERR_CUDA, "cudaStreamCreateWithFlags of the copy streams failed"));
+    // a first wait on an event that was never recorded is a no-op: record them once on the compute stream
+    for (int q = 0; q < 4; ++q)
+        if (cudaEventRecord(ev[4 * q + 1], c->stream) != cudaSuccess || cudaEventRecord(ev[4 * q + 3], c->stream) != cudaSuccess)
+            return unwind(fail(DFDM_ERR_CUDA, "cudaEventRecord of the transfer events failed"));
     for (int q = 0; q < 4; ++q) {
-        void *a = nullptr, *b = nullptr;
-        if (int rc = dalloc(c, &a, n * sizeof(double))) return rc;
-        if (int rc = dalloc(c, &b, n * sizeof(double))) return rc;
-        c->stage_in[q] = (double *)a;
-        c->stage_out[q] = (double *)b;
-        cudaEvent_t *evs[4] = {&c->ev_in[q], &c->ev_unpacked[q], &c->ev_packed[q], &c->ev_out[q]};
-        for (cudaEvent_t *e : evs) CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
-        // a first wait on an event that was never recorded is a no-op: record them once on the compute stream
-        CK(cudaEventRecord(c->ev_unpacked[q], c->stream));
-        CK(cudaEventRecord(c->ev_out[q], c->stream));
+        c->stage_in[q] = (double *)buf[2 * q];
+        c->stage_out[q] = (double *)buf[2 * q + 1];
+        c->ev_in[q] = ev[4 * q];
+        c->ev_unpacked[q] = ev[4 * q + 1];
+        c->ev_packed[q] = ev[4 * q + 2];
+        c->ev_out[q] = ev[4 * q + 3];
     }
-    CK(cudaStreamCreateWithFlags(&c->cin, cudaStreamNonBlocking));
-    CK(cudaStreamCreateWithFlags(&c->cout, cudaStreamNonBlocking));
+    c->cout = sout;
+    c->cin = sin;
     return DFDM_OK;
 }
 
@@ -1797,13 +1822,17 @@ const int NOALLOC_MAX_DEVICES = 64;
 std::mutex g_noalloc_mu;
 double *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
 
-// Address of the staging array on the current device, looked up on the first call for that device.
-int noalloc_scratch(double **out) {
+// Address of the staging array on the current device. It is looked up again on every call made outside a stream
+// capture, so a module reloaded after cudaDeviceReset is found at its new address; a call inside a capture uses the
+// address of the last call outside one (the first call on a device must therefore precede any capture).
+int noalloc_scratch(cudaStream_t stream, double **out) {
     int dev = -1;
     CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(DFDM_ERR_UNSUPPORTED, "device ordinal beyond 63");
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(stream, &cap));
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    if (!g_noalloc_ptr[dev] || cap == cudaStreamCaptureStatusNone) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
@@ -1830,7 +1859,7 @@ int dfdm_solve_poisson_noalloc(dfdm_ctx *c, const double *rhs_in, double *phi_ou
         return fail(DFDM_ERR_INVALID, "rhs_p has " + std::to_string(n) + " points; dfdm_solve_poisson_noalloc takes at most " +
                                           std::to_string(DFDM_NOALLOC_MAX_POINTS) + " (use dfdm_solve_poisson)");
     double *scratch = nullptr;
-    if (int rc = noalloc_scratch(&scratch)) return rc;
+    if (int rc = noalloc_scratch(c->stream, &scratch)) return rc;
     // The host copy fills scratch[0, n) before the unpack kernel reads it, and the pack kernel rewrites
     // scratch[0, n) before the copy back: nothing has to start at zero.
     CK(cudaMemcpyAsync(scratch, rhs_in, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));

@@ -58,6 +58,7 @@ class Result:
     cells: int
     state: Optional[tuple] = None
     summary: Dict[str, float] = field(default_factory=dict)
+    device_s: Optional[float] = None   # run_isolated: device time of the request's steps alone
 
     @property
     def latency(self) -> float:
@@ -260,8 +261,19 @@ class GpuExecutor:
         return True
 
     def enqueue(self, h, nsteps: int) -> None:
+        if "ev0" in h:
+            h["ev0"].record(h["st"])
         h["s"].compute_time_step_RK3_async(nsteps)
         h["ev"].record(h["st"])
+
+    def time_steps(self, h) -> None:
+        """Time the next enqueue on the device (CUDA events around its steps on the case's stream)."""
+        h["ev0"] = self.torch.cuda.Event(enable_timing=True)
+        h["ev"] = self.torch.cuda.Event(enable_timing=True)
+
+    def device_seconds(self, h) -> float:
+        h["ev"].synchronize()
+        return h["ev0"].elapsed_time(h["ev"]) * 1e-3
 
     def ready(self, h) -> bool:
         return h["ev"].query()
@@ -287,20 +299,25 @@ class GpuExecutor:
 
 def run_isolated(executor, requests: List[Request], keep_state: bool = False) -> List[Result]:
     """Every request alone, back to back (the isolated-run reference for the loop's throughput): set-up, steps,
-    result, in turn."""
+    result, in turn.  Each Result carries the device time of its steps alone (device_s: CUDA events around the
+    steps on the case's own stream, set-up and transfers excluded) where the executor can time them."""
     out = []
     t0 = executor.now()
+    timed = hasattr(executor, "time_steps")
     for r in requests:
         a = executor.now() - t0
         executor.prepare(r)
         h = executor.start(r)
         while not executor.can_enqueue(h):
             executor.idle(None)
+        if timed:
+            executor.time_steps(h)
         executor.enqueue(h, r.nsteps)
         while not executor.ready(h):
             executor.idle(None)
+        dev = executor.device_seconds(h) if timed else None
         state, summary = executor.finish(h, r, keep_state)
-        out.append(Result(r.rid, a, a, executor.now() - t0, r.nsteps, r.cells, state, summary))
+        out.append(Result(r.rid, a, a, executor.now() - t0, r.nsteps, r.cells, state, summary, dev))
     executor.reclaim()
     return out
 
@@ -321,18 +338,23 @@ def measure_stream(executor, requests: List[Request], rank: int, world: int, gat
     sub = [Request(r.rid, r.case, r.nsteps, 0.0, r.precision) for r in mine[:saturated]]
     iso = run_isolated(executor, sub)
     iso_wall = iso[-1].finished if iso else float("nan")
+    # the isolated reference is the device time of each request's steps alone (set-up, uploads and results
+    # excluded), so the ratio compares the loop against the device's throughput on one case at a time
+    iso_dev = sum(r.device_s for r in iso) if iso and all(r.device_s is not None for r in iso) else iso_wall
     t0 = executor.now()
     Scheduler(executor, budget_bytes).run(sub)
     sat_wall = executor.now() - t0
     work_sub = float(sum(r.work for r in sub))
     parts = gather({"rids": [r.rid for r in res], "lat": [r.latency for r in res],
                     "work": float(sum(r.work for r in mine)), "wall": wall,
-                    "iso": work_sub / iso_wall if iso else 0.0, "sat": work_sub / sat_wall if sub else 0.0,
+                    "iso": work_sub / iso_dev if iso else 0.0, "iso_wall": work_sub / iso_wall if iso else 0.0,
+                    "sat": work_sub / sat_wall if sub else 0.0,
                     "n_sub": len(sub), "finite": all(r.summary.get("finite", 1.0) == 1.0 for r in res),
                     "peak_active": sch.peak_active, "peak_bytes": sch.peak_bytes})
     lat = [x for p in parts for x in p["lat"]]
     rids = sorted(x for p in parts for x in p["rids"])
     iso_thr = sum(p["iso"] for p in parts)
+    iso_wall_thr = sum(p["iso_wall"] for p in parts)
     sat_thr = sum(p["sat"] for p in parts)
     wall_max = max(p["wall"] for p in parts)
     return {"requests": len(lat), "rids": rids, "p50_latency_s": percentile(lat, 50),
@@ -340,6 +362,8 @@ def measure_stream(executor, requests: List[Request], rank: int, world: int, gat
             "stream_wall_s": wall_max, "stream_throughput_cell_steps_per_s": sum(p["work"] for p in parts) / wall_max,
             "saturated_requests": sum(p["n_sub"] for p in parts), "saturated_throughput_cell_steps_per_s": sat_thr,
             "isolated_throughput_cell_steps_per_s": iso_thr,
+            "isolated_basis": "device time of each request's steps alone (CUDA events; set-up, transfers excluded)",
+            "isolated_wall_throughput_cell_steps_per_s": iso_wall_thr,
             "saturated_over_isolated": sat_thr / iso_thr if iso_thr > 0 else None,
             "all_finite": all(p["finite"] for p in parts), "peak_active": max(p["peak_active"] for p in parts),
             "peak_admitted_bytes": max(p["peak_bytes"] for p in parts), "admission_budget_bytes": budget_bytes}

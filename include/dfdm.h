@@ -261,8 +261,11 @@ int dfdm_kinetic_energy(dfdm_ctx *ctx, double *ke);
 /* Monitor guard of output_monitor (src/monitor.f90:32-52): DFDM_ERR_NOT_FINITE if any velocity is NaN/Inf or
  * |U| > 1e8. */
 int dfdm_check_finite(dfdm_ctx *ctx);
-/* pad_field_dev (src/halo_pad.f90:185-194) is called only by the hybrid advection scheme, the immersed
- * boundary and the particles, none of which is on the single-phase path: returns DFDM_ERR_UNSUPPORTED. */
+/* pad_field_dev (src/halo_pad.f90:185-194) builds copies of a field with extra x/z planes for wide stencils. Its
+ * callers are the hybrid advection scheme (advection_scheme = 2), the immersed boundary and the particles. On one
+ * GPU the hybrid scheme reads its +-3 x/z neighbours with periodic index wraps instead of padded copies
+ * (k_adv_hybrid_faces), and the other two callers are not on the single-phase path, so no padded copy is ever
+ * needed: this entry point returns DFDM_ERR_UNSUPPORTED. */
 int dfdm_pad_field(dfdm_ctx *ctx, int field, int extra_planes, double *out);
 
 /* ---- profiling hooks: launch one kernel family of one RK stage on the context's stream, no sync ----

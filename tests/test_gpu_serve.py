@@ -7,13 +7,21 @@ from dfdm import serve
 pytestmark = pytest.mark.gpu
 
 
-def test_results_alone_equal_results_in_the_mix():
-    reqs = serve.make_stream(8, rate=200.0, seed=21, grids=(32, 48), steps=(20, 60))
+@pytest.mark.parametrize("seed,grids,n", [(21, (32, 48), 8), (1, (48, 64, 96, 128), 10)])
+def test_results_alone_equal_results_in_the_mix(seed, grids, n):
+    """Each result is bit-identical alone and in the mix: small grids, and a mix that reaches 96^3 and 128^3 with
+    several channel and Taylor-Green cases."""
+    reqs = serve.make_stream(n, rate=200.0, seed=seed, grids=grids, steps=(20, 60))
+    kinds = {r.case.name[:3] for r in reqs}
+    assert kinds == {"tgv", "cha"}
+    if max(grids) >= 96:
+        assert {96, 128} <= {r.case.cells[0] for r in reqs}
     mix = serve.Scheduler(serve.GpuExecutor(), 150e9, chunk_cell_steps=2e5, keep_state=True)
     got = mix.run(reqs)
     assert mix.peak_active > 1
     alone = serve.run_isolated(serve.GpuExecutor(), reqs, keep_state=True)
     assert [r.rid for r in got] == [r.rid for r in alone]
+    assert all(r.device_s is not None and r.device_s > 0 for r in alone)
     for a, b in zip(got, alone):
         assert a.summary["finite"] == 1.0
         for x, y in zip(a.state, b.state):
