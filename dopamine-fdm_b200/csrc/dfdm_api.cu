@@ -25,6 +25,7 @@
 #include "kernels_step.cuh"
 #include "kernels_hybrid.cuh"
 #include "kernels_tma.cuh"
+#include "kernels_les.cuh"
 
 using namespace dfdm;
 
@@ -113,6 +114,7 @@ struct dfdm_ctx {
     void *nut = nullptr, *p = nullptr, *phi = nullptr, *spec = nullptr, *rhs3 = nullptr;
     void *my_t = nullptr, *mz_t = nullptr;      // 6 metric arrays each, storage type
     void *zm8 = nullptr;                        // FP32: the z metrics of each plane in load8 order (StepArgs::zm8)
+    double *d_wfac = nullptr;                   // LES + wall model: wall factors of the eddy viscosity (k_wall_sgs)
     double *my_d = nullptr, *mz_d = nullptr;    // same in double
     void *tw_x = nullptr, *twr_x = nullptr, *tw_z = nullptr, *tw_y = nullptr;
     FFTPlan plan_x{}, plan_z{}, plan_y{};
@@ -146,6 +148,10 @@ struct dfdm_ctx {
     int lx = 8, tzx = 8;
     int kc_stage = 8, kc_sgs = 8;               // z-planes per block of the tiled kernels
     int kc_stage2 = 8;                          // the same for the packed FP32 stage kernel
+    int kc_les = 8;                             // the same for the LES stage kernel with in-tile eddy viscosity
+    // LES: the stage kernels compute the eddy viscosity in their tiles (k_les) instead of reading it from a
+    // separate pass (dfdm_set_sgs_in_tile; the pass is the default)
+    bool sgs_tile = false;
     int kc_hyb = 32;                            // the same for the hybrid-scheme kernel
     int stage_variant = 0;                      // FP32 stage kernel in use: 0 one cell per thread, 1 packed pairs,
                                                 // 2 packed pairs with TMA plane tiles
@@ -300,6 +306,7 @@ template <typename T> StepArgs<T> step_args(dfdm_ctx *c) {
     a.adv = (const T *)c->adv;
     a.phi = (const T *)c->phi;
     a.zm8 = (const float *)c->zm8;
+    a.wfac = c->d_wfac;
     return a;
 }
 
@@ -464,6 +471,20 @@ template <typename T> struct Impl {
         }
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tiled<T, false, false, TILE_X, TILE_Y, 1>, TILE_X * TILE_Y, 0));
         c->kc_sgs = choose_kc(d, occ, nsm);
+        if (c->les) {
+            const int b0 = (int)les::smem_bytes<T>(false), b1 = (int)les::smem_bytes<T>(true);
+            CK(cudaFuncSetAttribute(k_les<T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b0));
+            CK(cudaFuncSetAttribute(k_les<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b1));
+            CK(cudaFuncSetAttribute(k_les<T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b0));
+            CK(cudaFuncSetAttribute(k_les<T, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b1));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_les<T, true, true>, les::NT, b1));
+            c->kc_les = choose_kc(d, std::max(1, occ), nsm, les::TX, les::TY, 4);
+            // measured on the Re_tau 395 LES grid (96 x 64 x 96, one B200): the separate pass plus the stage kernel
+            // take 0.254 ms per FP32 step against 0.326 ms in the tile, so the pass is the default and fused
+            // corrections (which need the in-tile form) start off
+            c->sgs_tile = false;
+            c->fused = false;
+        }
         // the CFL maxima: one wave of resident blocks, at most one warp per x-row
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cfl<T, true>, 256, 0));
         c->cfl_blocks = (int)std::max(1LL, std::min((long long)std::max(1, occ) * nsm, ((long long)d.Ny * d.Nz + 7) / 8));
@@ -598,6 +619,30 @@ template <typename T> struct Impl {
             rhs_only, nullptr);
         return DFDM_OK;
     }
+    // the eddy viscosity's wall factors (wall model only) from the velocity it is about to be computed from
+    template <bool CORR> static int wall_factors(dfdm_ctx *c, const T *u, const T *w) {
+        if (!c->d_wfac) return DFDM_OK;
+        const Dims &d = c->d;
+        k_wall_sgs<T, CORR><<<dim3((d.Nx + 127) / 128, d.Nz), 128, 0, c->stream>>>(step_args<T>(c), u, w,
+                                                                                   CORR ? f(c->phi) : nullptr, c->d_wfac);
+        CKL();
+        return DFDM_OK;
+    }
+    // LES stage with the eddy viscosity computed in the tile (stage 3 also stores it in nu_t)
+    template <bool WM, bool CORR> static int les_launch(dfdm_ctx *c, const StageCoef &sc) {
+        const Dims &d = c->d;
+        const T *iu = CORR ? f(c->us2) : f(c->u), *iv = CORR ? f(c->vs2) : f(c->v), *iw = CORR ? f(c->ws2) : f(c->w);
+        if (int rc = wall_factors<CORR>(c, iu, iw)) return rc;
+        T *uo = c->fused ? f(c->u) : f(c->uo), *vo = c->fused ? f(c->v) : f(c->vo), *wo = c->fused ? f(c->w) : f(c->wo);
+        k_les<T, WM, CORR><<<tile_grid(d, c->kc_les), les::NT, les::smem_bytes<T>(CORR), c->stream>>>(
+            step_args<T>(c), iu, iv, iw, c->wsd.tau_x, c->wsd.tau_z, sc, c->kc_les, uo, vo, wo, f(c->f1u), f(c->f1v),
+            f(c->f1w), f(c->us), f(c->vs), f(c->wsf), sc.stage == 3 ? f(c->nut) : nullptr);
+        return DFDM_OK;
+    }
+    template <bool CORR> static int les_dispatch(dfdm_ctx *c, const StageCoef &sc) {
+        if constexpr (sizeof(T) == 8) return les_launch<true, CORR>(c, sc);   // FP64 keeps the runtime flag
+        else return c->wm ? les_launch<true, CORR>(c, sc) : les_launch<false, CORR>(c, sc);
+    }
     template <bool HYB> static int stage_dispatch(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
         if constexpr (sizeof(T) == 8) {   // FP64 keeps the runtime wall-model flag
             return c->les ? stage_launch<true, true, HYB, false>(c, sc, rhs_only) : stage_launch<false, true, HYB, false>(c, sc, rhs_only);
@@ -609,7 +654,7 @@ template <typename T> struct Impl {
             }
         }
     }
-    // stages 2 and 3 with the fused correction (no LES, no hybrid scheme: fuse_eligible)
+    // stages 2 and 3 with the fused correction (no hybrid scheme: fuse_eligible; LES goes through les_dispatch)
     static int stage_dispatch_corr(dfdm_ctx *c, const StageCoef &sc) {
         if constexpr (sizeof(T) == 8) return stage_launch<false, true, false, true>(c, sc, nullptr);
         else if (c->wm) return stage_launch<false, true, false, true>(c, sc, nullptr);
@@ -617,6 +662,11 @@ template <typename T> struct Impl {
     }
 
     static int stage_kernel(dfdm_ctx *c, const StageCoef &sc, T *rhs_only) {
+        if (c->les && c->sgs_tile && !rhs_only && !c->adv) {
+            if (int rc = les_dispatch<false>(c, sc)) return rc;
+            CKL();
+            return DFDM_OK;
+        }
         if (int rc = c->adv ? stage_dispatch<true>(c, sc, rhs_only) : stage_dispatch<false>(c, sc, rhs_only)) return rc;
         CKL();
         return DFDM_OK;
@@ -640,6 +690,9 @@ template <typename T> struct Impl {
             return DFDM_OK;
         }
         StageCoef sc{2, 0.0, c->prm.dt, 0.25, 5.0 / 12.0, 0};
+        // the variants are those of the stage kernel that reads a stored eddy viscosity (k_les has one form)
+        struct Restore { dfdm_ctx *c; bool v; ~Restore() { c->sgs_tile = v; } } restore{c, c->sgs_tile};
+        c->sgs_tile = false;
         cudaEvent_t e0, e1;
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
@@ -674,6 +727,7 @@ template <typename T> struct Impl {
         case 0: {   // SGS
             if (!c->les) return DFDM_OK;
             StageCoef sc{1, 0.0, 0.0, 0.0, 0.0, 0};
+            if (int rc = wall_factors<false>(c, f(c->u), f(c->w))) return rc;
             k_tiled<T, false, false, TILE_X, TILE_Y, 1><<<tile_grid(d, c->kc_sgs), TILE_X * TILE_Y, 0, st>>>(
                 step_args<T>(c), f(c->u), f(c->v), f(c->w), nullptr, nullptr, nullptr, sc, c->kc_sgs, nullptr, nullptr,
                 nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, f(c->nut));
@@ -707,7 +761,7 @@ template <typename T> struct Impl {
             sc.dtp = c->dev_dt() ? c->d_dtt : nullptr;
             sc.no_uo = c->fused ? 1 : 0;
             if (c->fused && s >= 2) {
-                if (int rc = stage_dispatch_corr(c, sc)) return rc;
+                if (int rc = c->les ? les_dispatch<true>(c, sc) : stage_dispatch_corr(c, sc)) return rc;
                 CKL();
                 return DFDM_OK;
             }
@@ -899,7 +953,9 @@ template <typename T> struct Impl {
     static int step_enqueue(dfdm_ctx *c) {
         int rc;
         for (int s = 1; s <= 3; ++s) {
-            if ((rc = launch(c, 0, s))) return rc;   // SGS (step start, then stages 2 and 3)
+            // SGS (step start, then stages 2 and 3); with the eddy viscosity in the stage tiles only the adaptive
+            // step's start-of-step CFL needs the field
+            if ((!c->sgs_tile || (s == 1 && c->dev_dt())) && (rc = launch(c, 0, s))) return rc;
             if (s == 1 && c->dev_dt() && (rc = select_dt(c))) return rc;   // dt from the start-of-step CFL, after nu_t
             if ((rc = launch(c, 8, s))) return rc;   // wall model
             if ((rc = launch(c, 11, s))) return rc;  // hybrid-scheme dissipation (advection_scheme = 2)
@@ -992,8 +1048,11 @@ int validate(const dfdm_grid *g, const dfdm_params *p) {
 
 // The fused-correction step applies (see dfdm_ctx::fused): no SGS model, the wall model only with its temporal
 // filter (automatic with periodic z), and not the hybrid advection scheme.
+// The fused correction needs the stage kernel to be the only reader of the corrected velocity: no hybrid scheme,
+// the wall model only with its filter (its stage 2-3 inputs are the filtered planes), and LES only through the
+// in-tile eddy viscosity (no separate pass reading u).
 bool fuse_eligible(const dfdm_params *p) {
-    return p->sgs_model == 0 && (p->flat_wall_model_flag == 0 || p->wm_filter_mode != 0) && p->advection_scheme != 2;
+    return (p->flat_wall_model_flag == 0 || p->wm_filter_mode != 0) && p->advection_scheme != 2;
 }
 
 // Bytes of the buffers dfdm_create carves from the context's arena (every sub-allocation 256-byte aligned).
@@ -1006,7 +1065,7 @@ size_t arena_bytes(const dfdm_grid *g, const dfdm_params *p) {
                              (fuse_eligible(p) ? 3 /*second u* set*/ : 0));
     n += spec * 2 * ts;
     if (g->y_bc_type != 0) n += (Nx / 2 + 1) * Ny * Nz * 8;   // pivot table of the y solves
-    n += 8 * Nx * Nz * 2 * 8;   // wall planes
+    n += 9 * Nx * Nz * 2 * 8;   // wall planes (and the eddy viscosity's wall factors)
     n += 1 << 20;               // metrics, twiddles, reductions, alignment
     return n;
 }
@@ -1260,6 +1319,10 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
     double **wsp[] = {&c->wsd.tau_x, &c->wsd.tau_z, &c->wsd.ux, &c->wsd.wx, &c->wsd.tx, &c->wsd.uz, &c->wsd.wz, &c->wsd.tz};
     for (double **pp : wsp)
         if ((rc = dalloc(c, (void **)pp, wp))) return bail(rc);
+    if (c->les && c->wm) {   // the first-cell gradient factors of the eddy viscosity's wall override (k_wall_sgs)
+        if ((rc = dalloc(c, &tmp, wp))) return bail(rc);
+        c->d_wfac = (double *)tmp;
+    }
 
     // ---- reductions ----
     c->red_blocks = reduce_grid(d);
@@ -2321,9 +2384,30 @@ int dfdm_set_fused_correction(dfdm_ctx *c, int enable) {
     if (int rc = check_ctx(c)) return rc;
     if (enable && !c->fuse_ok)
         return fail(DFDM_ERR_UNSUPPORTED, "fused corrections need a DNS or filtered-wall-model case without the hybrid scheme");
+    if (enable && c->les && !c->sgs_tile)
+        return fail(DFDM_ERR_UNSUPPORTED, "fused corrections in LES need the eddy viscosity computed in the stage tiles");
     CK(cudaStreamSynchronize(c->stream));
     destroy_graph(c);   // the captured step holds the other launch sequence
     c->fused = enable != 0;
+    return DFDM_OK;
+}
+
+int dfdm_set_sgs_in_tile(dfdm_ctx *c, int enable) {
+    g_err.clear();
+    if (int rc = check_ctx(c)) return rc;
+    if (!c->les) return fail(DFDM_ERR_UNSUPPORTED, "the eddy viscosity is only computed for LES (sgs_model > 0)");
+    CK(cudaStreamSynchronize(c->stream));
+    destroy_graph(c);   // the captured step holds the other launch sequence
+    c->sgs_tile = enable != 0;
+    // the separate pass reads the corrected velocity from U; the in-tile form takes the fused corrections with it
+    c->fused = c->sgs_tile && c->fuse_ok;
+    return DFDM_OK;
+}
+
+int dfdm_get_sgs_in_tile(dfdm_ctx *c, int *enabled) {
+    if (int rc = check_ctx(c)) return rc;
+    if (!enabled) return fail(DFDM_ERR_INVALID, "null output");
+    *enabled = c->sgs_tile ? 1 : 0;
     return DFDM_OK;
 }
 

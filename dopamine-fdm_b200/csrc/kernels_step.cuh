@@ -32,6 +32,10 @@ template <typename T> struct StepArgs {
     // FP32: the eight z metrics of every plane in AxisLocal<F2>::load8 order, 8 consecutive values per plane (one
     // 32-byte bulk copy per plane for the TMA stage kernel); null in FP64
     const float *zm8;
+    // LES with the wall model: the first-cell gradient factor of every wall cell, (iw*Nz + k)*Nx + i, written by
+    // k_wall_sgs from the velocity the eddy viscosity is computed from (NaN where the override does not apply);
+    // null: nut_at solves for it in place
+    const double *wfac;
 };
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -60,12 +64,22 @@ __device__ __forceinline__ double solve_u_tau(double u_ref, double y_ref, double
     return u_tau;
 }
 
+// The wall-modelled first-cell gradient override of compute_vreman (src/sgs_model.f90:158-172): the factor
+// u_tau/(kappa y_w |u|) (signed by the wall) that replaces du/dy and dw/dy by fac*u_c and fac*w_c, with u_tau from the
+// Reichardt law at the first-cell velocity magnitude; NaN where |u| <= 1e-14 and the gradients are kept.
+__device__ __forceinline__ double wall_gradient_factor(double u_c, double w_c, bool lower, double y_w, double nu) {
+    double u_mag = sqrt(u_c * u_c + w_c * w_c);
+    if (!(u_mag > 1e-14)) return __longlong_as_double(0x7ff8000000000000LL);
+    double u_tau = solve_u_tau(u_mag, y_w, nu);
+    return (lower ? 1.0 : -1.0) * u_tau / (0.41 * y_w * u_mag);
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 // Eddy viscosity at one cell centre: compute_vreman pass 1 (src/sgs_model.f90:118-223) with the AMD
 // (Rozema et al. 2015) or Vreman (2004) closure and the wall-modelled first-cell gradient override (:158-172).
 // Ghost values come from the neighbourhood accessor (sgs_fill_ghosts' rules, :458-531).
 template <typename T, typename Q>
-__device__ __forceinline__ T nut_at(const StepArgs<T> &a, const Q &q, int j, int k) {
+__device__ __forceinline__ T nut_at(const StepArgs<T> &a, const Q &q, int i, int j, int k) {
     const Dims &d = a.d;
     typedef Arith<T> A;
     const Metric1D<T> &my = a.my, &mz = a.mz;
@@ -87,13 +101,15 @@ __device__ __forceinline__ T nut_at(const StepArgs<T> &a, const Q &q, int j, int
     T a23 = T(0.5) * ((Wc - q.W(0, -1, 0)) * inv_yg_jm + (q.W(0, 1, 0) - Wc) * inv_yg_jp);
     T a33 = (Wc - Wkm) * inv_dz_k;
     if (a.wm && (j == 0 || j == d.Ny - 1)) {
-        double y_w = (j == 0) ? a.yg2 : a.ygtop;
         double u_c = 0.5 * ((double)Um + (double)Uc);
         double w_c = 0.5 * ((double)Wkm + (double)Wc);
-        double u_mag = sqrt(u_c * u_c + w_c * w_c);
-        if (u_mag > 1e-14) {
-            double u_tau = solve_u_tau(u_mag, y_w, a.nu_d);
-            double fac_w = ((j == 0) ? 1.0 : -1.0) * u_tau / (0.41 * y_w * u_mag);
+        double fac_w;
+        if (a.wfac) {
+            fac_w = a.wfac[((j == 0 ? 0 : d.Nz) + k) * d.Nx + i];   // NaN: no override
+        } else {
+            fac_w = wall_gradient_factor(u_c, w_c, j == 0, (j == 0) ? a.yg2 : a.ygtop, a.nu_d);
+        }
+        if (!isnan(fac_w)) {
             a21 = (T)(fac_w * u_c);
             a23 = (T)(fac_w * w_c);
         }
@@ -258,6 +274,36 @@ template <> struct AxisLocal<double> {
     __device__ __forceinline__ double invf() const { return 1.0 / m->df[p]; }
     __device__ __forceinline__ double invfm() const { return 1.0 / m->df[p - 1]; }
 };
+
+// The gradient factor of the eddy viscosity's wall override for every wall cell (wall_gradient_factor), from the
+// velocity the eddy viscosity is then computed from: U and W as stored, or (CORR) the previous stage's u* with its
+// projection applied exactly as the stage kernels' loaders apply it.  One thread per (i, k) of both walls: the
+// Reichardt solve runs once per wall cell here instead of on the critical path of every tile that holds the cell.
+template <typename T, bool CORR>
+__global__ void k_wall_sgs(StepArgs<T> a, const T *__restrict__ U, const T *__restrict__ W, const T *__restrict__ phi,
+                           double *__restrict__ wfac) {
+    const Dims &d = a.d;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+    if (i >= d.Nx) return;
+    const int im = wrap(i - 1, d.Nx), ip = wrap(i + 1, d.Nx), km = wrap(k - 1, d.Nz), kp = wrap(k + 1, d.Nz);
+    for (int iw = 0; iw < 2; ++iw) {
+        const int j = iw ? d.Ny - 1 : 0;
+        T u0 = U[idx3(d, im, j, k)], u1 = U[idx3(d, i, j, k)], w0 = W[idx3(d, i, j, km)], w1 = W[idx3(d, i, j, k)];
+        if constexpr (CORR) {
+            const T pm = phi[idx3(d, im, j, k)], pc = phi[idx3(d, i, j, k)], pp = phi[idx3(d, ip, j, k)];
+            const T pkm = phi[idx3(d, i, j, km)], pkp = phi[idx3(d, i, j, kp)];
+            u0 = u0 - (pc - pm) * a.inv_dx;
+            u1 = u1 - (pp - pc) * a.inv_dx;
+            w0 = w0 - (pc - pkm) * Arith<T>::inv(a.mz.df, a.mz.idf, km);
+            w1 = w1 - (pkp - pc) * Arith<T>::inv(a.mz.df, a.mz.idf, k);
+        }
+        const T ubj = a.ub[j];
+        const T Um = u0 + ubj, Uc = u1 + ubj;   // as TileQ::U forms them
+        const double u_c = 0.5 * ((double)Um + (double)Uc);
+        const double w_c = 0.5 * ((double)w0 + (double)w1);
+        wfac[((long long)iw * d.Nz + k) * d.Nx + i] = wall_gradient_factor(u_c, w_c, iw == 0, iw ? a.ygtop : a.yg2, a.nu_d);
+    }
+}
 
 // Wall-model flux of the cell at t (plain types) or of the cells at t and t+1 (packed pairs), from double.
 template <typename T> __device__ __forceinline__ T wall_flux(const double *t) { return (T)t[0]; }
@@ -504,6 +550,55 @@ template <int PX> struct TileQ2 {
 
 
 
+// One thread's cell (i, j, k) from the shared-memory neighbourhood q: the three right-hand sides and the RK3 stage
+// update (or, with rhs_only, the right-hand sides themselves).  Shared by the one-cell stage kernels.
+template <typename T, bool LES, bool WM, bool HYB, typename Q>
+__device__ __forceinline__ void stage_cell(const StepArgs<T> &a, const Q &q, const AxisLocal<T> &Y,
+                                           const double *__restrict__ tau_x, const double *__restrict__ tau_z,
+                                           const StageCoef &sc, int i, int j, int k, T *__restrict__ uo,
+                                           T *__restrict__ vo, T *__restrict__ wo, T *__restrict__ f1u,
+                                           T *__restrict__ f1v, T *__restrict__ f1w, T *__restrict__ us,
+                                           T *__restrict__ vs, T *__restrict__ wsf, T *__restrict__ rhs_only) {
+    const Dims &d = a.d;
+    const int p = k * (d.Nx * d.Ny) + j * d.Nx + i;
+    const bool vrow = j < d.NyV;
+    const bool upd = !rhs_only && sc.stage != 1;
+    T ou = T(0), ov = T(0), ow = T(0), fu = T(0), fv = T(0), fw = T(0);
+    if (upd) {   // issue the base-state and F1 loads before the arithmetic
+        if (!sc.incr) { ou = uo[p]; ow = wo[p]; if (vrow) ov = vo[p]; }
+        fu = f1u[p]; fw = f1w[p];
+        if (vrow) fv = f1v[p];
+    }
+    AxisLocal<T> Z;
+    Z.load(a.mz, k);
+    T ru = rhs_u_at<T, LES, WM>(a, q, Y, Z, tau_x, i, j, k);
+    T rw = rhs_w_at<T, LES, WM>(a, q, Y, Z, tau_z, i, j, k);
+    T rv = vrow ? rhs_v_at<T, LES, WM>(a, q, Y, Z, i, j, k) : T(0);
+    if constexpr (HYB) {
+        ru = ru + a.adv[p]; rw = rw + a.adv[2 * d.cells + p];
+        if (vrow) rv = rv + a.adv[d.cells + p];
+    }
+    if (rhs_only) {
+        rhs_only[p] = ru; rhs_only[d.cells + p] = rv; rhs_only[2 * d.cells + p] = rw;
+    } else if (sc.stage == 1) {
+        T c = (T)(sc.dtp ? *sc.dtp * (8.0 / 15.0) : sc.dt_a11);
+        T u0 = q.Ud(0, 0, 0), w0 = q.W(0, 0, 0);   // U as stored (deviation from the base profile)
+        f1u[p] = ru; us[p] = u0 + c * ru;
+        f1w[p] = rw; wsf[p] = w0 + c * rw;
+        if (!sc.no_uo) { uo[p] = u0; wo[p] = w0; }
+        if (vrow) {
+            T v0 = q.V(0, 0, 0);
+            f1v[p] = rv; vs[p] = v0 + c * rv;
+            if (!sc.no_uo) vo[p] = v0;
+        }
+    } else {
+        T c1 = (T)sc.c1, c2 = (T)sc.c2, dtt = (T)(sc.dtp ? *sc.dtp : sc.dt);   // with sc.incr the base stays zero: du
+        us[p] = ou + dtt * (c1 * fu + c2 * ru);
+        wsf[p] = ow + dtt * (c1 * fw + c2 * rw);
+        if (vrow) vs[p] = ov + dtt * (c1 * fv + c2 * rv);
+    }
+}
+
 // Tiled kernels (KIND 0: fused stage, KIND 1: eddy viscosity, KIND 2: fused stage adding the dissipative terms of
 // advection_scheme = 2 from StepArgs::adv), 2.5-D blocked: a block owns a TX x TY column of
 // (i,j) cells and marches through a chunk of kc z-planes.  Each z-plane of U, V, W (and nu_t) is copied from HBM
@@ -678,44 +773,10 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
             q.w[0] = sm[2][sm_]; q.w[1] = sm[2][s0]; q.w[2] = sm[2][sp];
             q.n[0] = sm[NF - 1][sm_]; q.n[1] = sm[NF - 1][s0]; q.n[2] = sm[NF - 1][sp];
             if (KIND == 1) {
-                nut_out[p] = nut_at<T>(a, q, j, k);
+                nut_out[p] = nut_at<T>(a, q, i, j, k);
             } else {
-                const bool vrow = j < d.NyV;
-                const bool upd = !rhs_only && sc.stage != 1;
-                T ou = T(0), ov = T(0), ow = T(0), fu = T(0), fv = T(0), fw = T(0);
-                if (upd) {   // issue the base-state and F1 loads before the arithmetic
-                    if (!sc.incr) { ou = uo[p]; ow = wo[p]; if (vrow) ov = vo[p]; }
-                    fu = f1u[p]; fw = f1w[p];
-                    if (vrow) fv = f1v[p];
-                }
-                AxisLocal<T> Z;
-                Z.load(a.mz, k);
-                T ru = rhs_u_at<T, LES, WM>(a, q, Y, Z, tau_x, i, j, k);
-                T rw = rhs_w_at<T, LES, WM>(a, q, Y, Z, tau_z, i, j, k);
-                T rv = vrow ? rhs_v_at<T, LES, WM>(a, q, Y, Z, i, j, k) : T(0);
-                if constexpr (KIND == 2) {
-                    ru = ru + a.adv[p]; rw = rw + a.adv[2 * d.cells + p];
-                    if (vrow) rv = rv + a.adv[d.cells + p];
-                }
-                if (rhs_only) {
-                    rhs_only[p] = ru; rhs_only[d.cells + p] = rv; rhs_only[2 * d.cells + p] = rw;
-                } else if (sc.stage == 1) {
-                    T c = (T)(sc.dtp ? *sc.dtp * (8.0 / 15.0) : sc.dt_a11);
-                    T u0 = q.Ud(0, 0, 0), w0 = q.W(0, 0, 0);   // U as stored (deviation from the base profile)
-                    f1u[p] = ru; us[p] = u0 + c * ru;
-                    f1w[p] = rw; wsf[p] = w0 + c * rw;
-                    if (!sc.no_uo) { uo[p] = u0; wo[p] = w0; }
-                    if (vrow) {
-                        T v0 = q.V(0, 0, 0);
-                        f1v[p] = rv; vs[p] = v0 + c * rv;
-                        if (!sc.no_uo) vo[p] = v0;
-                    }
-                } else {
-                    T c1 = (T)sc.c1, c2 = (T)sc.c2, dtt = (T)(sc.dtp ? *sc.dtp : sc.dt);   // with sc.incr the base stays zero: du
-                    us[p] = ou + dtt * (c1 * fu + c2 * ru);
-                    wsf[p] = ow + dtt * (c1 * fw + c2 * rw);
-                    if (vrow) vs[p] = ov + dtt * (c1 * fv + c2 * rv);
-                }
+                stage_cell<T, LES, WM, KIND == 2>(a, q, Y, tau_x, tau_z, sc, i, j, k, uo, vo, wo, f1u, f1v, f1w, us, vs,
+                                                  wsf, rhs_only);
             }
         }
         cp_async_wait_all();

@@ -34,7 +34,8 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_compute_cfl", "dfdm_set_stage_variant", "dfdm_get_stage_variant", "dfdm_set_adaptive_dt",
            "dfdm_get_dt", "dfdm_set_landing_time", "dfdm_output_monitor", "dfdm_output_monitor_async",
            "dfdm_set_fused_correction", "dfdm_get_fused_correction", "dfdm_set_state_async", "dfdm_get_state_async",
-           "dfdm_write_box_snapshot", "dfdm_set_landing_times", "dfdm_write_snapshot_ex", "dfdm_get_stage_timing"]
+           "dfdm_write_box_snapshot", "dfdm_set_landing_times", "dfdm_write_snapshot_ex", "dfdm_get_stage_timing",
+           "dfdm_set_sgs_in_tile", "dfdm_get_sgs_in_tile"]
 
 
 class DfdmError(RuntimeError):
@@ -103,6 +104,8 @@ def load(build_if_missing: bool = True):
         "dfdm_set_stage_variant": (c_int, [c_void_p, c_int]),
         "dfdm_get_stage_variant": (c_int, [c_void_p, POINTER(ctypes.c_int), P, P]),
         "dfdm_get_stage_timing": (c_int, [c_void_p, c_int, P]),
+        "dfdm_set_sgs_in_tile": (c_int, [c_void_p, c_int]),
+        "dfdm_get_sgs_in_tile": (c_int, [c_void_p, POINTER(ctypes.c_int)]),
         "dfdm_set_adaptive_dt": (c_int, [c_void_p, c_int, c_double, c_double, c_double, c_double]),
         "dfdm_get_dt": (c_int, [c_void_p, P]),
         "dfdm_set_landing_time": (c_int, [c_void_p, c_int, c_double]),
@@ -327,6 +330,15 @@ class Solver:
         """FP32 stage kernel: 0 one cell per thread, 1 packed pairs, 2 packed pairs with TMA plane tiles (walls in y,
         Nx a multiple of 4), -1 re-time the eligible ones and keep the fastest."""
         _check(load().dfdm_set_stage_variant(self.h, int(variant)))
+
+    def set_sgs_in_tile(self, enable: bool = True) -> None:
+        """LES: eddy viscosity computed in the stage tiles (True, the default) or by the separate pass (False)."""
+        _check(load().dfdm_set_sgs_in_tile(self.h, int(bool(enable))))
+
+    def sgs_in_tile(self) -> bool:
+        v = ctypes.c_int(0)
+        _check(load().dfdm_get_sgs_in_tile(self.h, ctypes.byref(v)))
+        return bool(v.value)
 
     def stage_timing(self, variant: int) -> float:
         """ms per launch of a stage-kernel variant from the set-up timing (-1 = not timed)."""

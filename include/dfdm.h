@@ -273,13 +273,27 @@ int dfdm_pad_field(dfdm_ctx *ctx, int field, int extra_planes, double *out);
  *        5 inverse z-FFT, 6 inverse x-FFT, 7 velocity correction, 8 wall model, 9 constant-flux bulk sum + shift,
  *        10 CFL maxima, 11 the dissipative terms of advection_scheme = 2 */
 int dfdm_launch_kernel_async(dfdm_ctx *ctx, int which, int rk_stage);
-/* Fused corrections (on by default where they apply: no SGS model, the wall model only with its temporal filter, no
- * hybrid advection scheme).  The projections of RK stages 1 and 2 then run inside the next stage kernel's loader
- * instead of as separate launches, and the step-start velocity stays in place as the RK base state: two launches and
- * 17 words per cell fewer per step, the same arithmetic.  No counterpart in the reference; enable = 0 restores the
- * separate corrections (DFDM_ERR_UNSUPPORTED for enable = 1 where they do not apply). */
+/* Fused corrections (on by default where they apply: the wall model only with its temporal filter, no hybrid
+ * advection scheme; LES only with the eddy viscosity computed in the stage tiles, dfdm_set_sgs_in_tile).  The projections of RK stages 1
+ * and 2 then run inside the next stage kernel's loader instead of as separate launches, and the step-start velocity
+ * stays in place as the RK base state: two launches and 17 words per cell fewer per step, the same arithmetic.  No
+ * counterpart in the reference; enable = 0 restores the separate corrections (DFDM_ERR_UNSUPPORTED for enable = 1
+ * where they do not apply). */
 int dfdm_set_fused_correction(dfdm_ctx *ctx, int enable);
 int dfdm_get_fused_correction(dfdm_ctx *ctx, int *enabled);
+/* LES (sgs_model > 0): with enable = 1 the stage kernels compute the eddy viscosity of compute_vreman
+ * (src/sgs_model.f90:118-223) from their own shared-memory velocity tiles, on the tile and a one-cell halo, instead of
+ * reading the field a separate full-grid pass wrote at the step start and after the stage-1 and stage-2 projections
+ * (src/time_integration.f90:144,361,493), and the fused corrections come on with it (where they apply). The results
+ * agree with the separate pass to rounding; from one state the field is the same bit for bit. The stage-3 kernel
+ * stores its field, so dfdm_get_nu_t, the CFL numbers and snapshots after a step see the step's last nu_t as before;
+ * the adaptive time step still runs the pass at the step start for its CFL. enable = 0 (the default: on the Re_tau 395
+ * LES grid the separate pass measured faster, 0.254 against 0.326 ms per FP32 step) restores the pass and turns the
+ * fused corrections off, since the pass reads the corrected velocity. With the wall model, both forms read the
+ * first-cell gradient factor of the override from a per-wall-cell table that a small kernel fills from the same
+ * velocity before each evaluation. DFDM_ERR_UNSUPPORTED without an SGS model. No counterpart in the reference. */
+int dfdm_set_sgs_in_tile(dfdm_ctx *ctx, int enable);
+int dfdm_get_sgs_in_tile(dfdm_ctx *ctx, int *enabled);
 /* Algorithmic HBM bytes one launch of that kernel family moves (the roofline numerator). */
 int dfdm_kernel_bytes(dfdm_ctx *ctx, int which, double *bytes);
 /* Number of the library's own kernels enqueued by this context so far (graph replays included). */
