@@ -26,6 +26,7 @@
 #include "kernels_hybrid.cuh"
 #include "kernels_tma.cuh"
 #include "kernels_les.cuh"
+#include "kernels_group.cuh"
 
 using namespace dfdm;
 
@@ -2475,6 +2476,344 @@ int dfdm_kernel_bytes(dfdm_ctx *c, int which, double *bytes) {
     default: return fail(DFDM_ERR_INVALID, "bad kernel id");
     }
     *bytes = b;
+    return DFDM_OK;
+}
+
+}  // extern "C"
+
+// ================================================================================================================
+// Serving groups: the steady steps of several FP32-mixed contexts advanced together, one grouped launch per kernel
+// family (and transform length) for all of them.  See kernels_group.cuh.
+struct dfdm_group {
+    std::vector<dfdm_ctx *> cs;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    cudaEvent_t ev = nullptr;              // orders the members' own streams with the group's launches
+    long long launches = 0, graph_launches = 0;
+};
+
+namespace {
+
+// the per-job block counts and the launches of one family, GROUP_MAX jobs at a time
+template <class Job, class L> int launch_groups(const std::vector<Job> &jobs, L &&launch) {
+    for (size_t o = 0; o < jobs.size(); o += GROUP_MAX) {
+        GroupTable<Job> t;
+        const int n = (int)std::min<size_t>(GROUP_MAX, jobs.size() - o);
+        t.njobs = n;
+        int tot = 0;
+        for (int q = 0; q < n; ++q) {
+            t.start[q] = tot;
+            t.jobs[q] = jobs[o + q];
+            tot += (int)(jobs[o + q].grid.x * jobs[o + q].grid.y * jobs[o + q].grid.z);
+        }
+        for (int q = n; q <= GROUP_MAX; ++q) t.start[q] = tot;
+        launch(t, tot);
+        CKL();
+    }
+    return DFDM_OK;
+}
+
+// can this context step inside a group?  (FP32-mixed DNS with fused corrections, fixed dt, two-level transforms,
+// first step taken)
+int group_eligible(const dfdm_ctx *c) {
+    if (c->prec != DFDM_FP32_MIXED) return fail(DFDM_ERR_UNSUPPORTED, "serving groups take FP32-mixed contexts");
+    if (c->les || c->wm || c->adv) return fail(DFDM_ERR_UNSUPPORTED, "serving groups take DNS contexts (no SGS, wall model or hybrid scheme)");
+    if (!c->fused) return fail(DFDM_ERR_UNSUPPORTED, "serving groups need the fused corrections");
+    if (c->dev_dt()) return fail(DFDM_ERR_UNSUPPORTED, "serving groups take a fixed time step");
+    if (!c->x2 || !c->z2 || (c->yper && !c->y2)) return fail(DFDM_ERR_UNSUPPORTED, "serving groups need two-level transform lengths");
+    if (c->d.Nx % 4 != 0) return fail(DFDM_ERR_UNSUPPORTED, "serving groups need Nx a multiple of 4");
+    if (!c->projected) return fail(DFDM_ERR_INVALID, "take a context's first step before it joins a group");
+    return DFDM_OK;
+}
+
+// one step of every case of the group (the launch sequence of step_enqueue, family by family across the cases)
+int group_step_enqueue(dfdm_group *g) {
+    typedef Impl<float> I;
+    typedef float2 C;
+    cudaStream_t st = g->stream;
+    constexpr int NL = I::NL;
+    for (int s = 1; s <= 3; ++s) {
+        // ---- stage kernels ----
+        std::vector<StageJob> stage[2];   // [variant 0 one cell, variant 1 packed]
+        const bool corr = s >= 2;
+        for (dfdm_ctx *c : g->cs) {
+            if (corr) { std::swap(c->us, c->us2); std::swap(c->vs, c->vs2); std::swap(c->wsf, c->ws2); }
+            StageJob J;
+            // variant 2 is variant 1's arithmetic (the per-case launch falls back to variant 0 without TMA)
+            const int v = (c->stage_variant == 1 || (c->stage_variant == 2 && c->tma_ok)) ? 1 : 0;
+            J.kc = v ? c->kc_stage2 : c->kc_stage;
+            J.grid = v ? tile_grid(c->d, J.kc, TILE_X2) : tile_grid(c->d, J.kc);
+            J.a = step_args<float>(c);
+            J.U = corr ? (const float *)c->us2 : (const float *)c->u;
+            J.V = corr ? (const float *)c->vs2 : (const float *)c->v;
+            J.W = corr ? (const float *)c->ws2 : (const float *)c->w;
+            J.tau_x = c->wsd.tau_x; J.tau_z = c->wsd.tau_z;
+            StageCoef sc;
+            sc.stage = s;
+            sc.dt_a11 = c->prm.dt * (8.0 / 15.0);
+            sc.dt = c->prm.dt;
+            sc.c1 = 1.0 / 4.0;
+            sc.c2 = (s == 2) ? 5.0 / 12.0 : 3.0 / 4.0;
+            sc.incr = I::incr_form(c, s);
+            sc.dtp = nullptr;
+            sc.no_uo = 1;
+            J.sc = sc;
+            J.uo = (float *)c->u; J.vo = (float *)c->v; J.wo = (float *)c->w;   // fused: U is the RK base state
+            J.f1u = (float *)c->f1u; J.f1v = (float *)c->f1v; J.f1w = (float *)c->f1w;
+            J.us = (float *)c->us; J.vs = (float *)c->vs; J.wsf = (float *)c->wsf;
+            J.nu = nullptr; J.rhs_only = nullptr; J.nut_out = nullptr;
+            stage[v].push_back(J);
+        }
+        int rc;
+        if (corr) {
+            if ((rc = launch_groups(stage[1], [&](const GroupTable<StageJob> &t, int nb) { kg_stage2<true><<<nb, 256, 0, st>>>(t); }))) return rc;
+            if ((rc = launch_groups(stage[0], [&](const GroupTable<StageJob> &t, int nb) { kg_stage1<true><<<nb, 256, 0, st>>>(t); }))) return rc;
+        } else {
+            if ((rc = launch_groups(stage[1], [&](const GroupTable<StageJob> &t, int nb) { kg_stage2<false><<<nb, 256, 0, st>>>(t); }))) return rc;
+            if ((rc = launch_groups(stage[0], [&](const GroupTable<StageJob> &t, int nb) { kg_stage1<false><<<nb, 256, 0, st>>>(t); }))) return rc;
+        }
+        // ---- div u* + forward x, per length ----
+        std::map<int, std::vector<FwdXJob>> fx;
+        std::map<int, size_t> fx_smem;
+        for (dfdm_ctx *c : g->cs) {
+            FwdXJob J;
+            const long long lines = (long long)c->d.Ny * c->d.Nz;
+            J.grid = dim3((unsigned)((lines + c->lx2 - 1) / c->lx2), 1, 1);
+            J.a = poisson_args<float>(c); J.lx = c->lx2;
+            J.U = (const float *)c->us; J.V = (const float *)c->vs; J.W = (const float *)c->wsf; J.src = nullptr;
+            J.spec = (C *)c->spec; J.tw = (const C *)c->tw_x; J.twr = (const C *)c->twr_x;
+            fx[c->d.Nx / 2].push_back(J);
+            fx_smem[c->d.Nx / 2] = c->smem_x2;
+        }
+        for (auto &kv : fx) {
+            with_fft2l(kv.first, [&](auto n) {
+                constexpr int M = decltype(n)::value;
+                rc = launch_groups(kv.second, [&](const GroupTable<FwdXJob> &t, int nb) { kg_fwd_x<M><<<nb, 256, fx_smem[M], st>>>(t); });
+            });
+            if (rc) return rc;
+        }
+        // ---- z transforms and the y solve, per length ----
+        auto col_family = [&](int mode) -> int {
+            std::map<int, std::vector<ColJob>> jobs;
+            std::map<int, std::pair<int, size_t>> cfg;   // threads, shared bytes
+            for (dfdm_ctx *c : g->cs) {
+                if (mode == 2 && !c->yper) continue;
+                ColJob J;
+                const int L = mode == 2 ? c->d.Ny : c->d.Nz;
+                J.grid = dim3((unsigned)((c->d.Nxc + NL - 1) / NL), (unsigned)(mode == 2 ? c->d.Nz : c->d.Ny), 1);
+                J.d = c->d; J.spec = (C *)c->spec; J.tw = (const C *)(mode == 2 ? c->tw_y : c->tw_z);
+                J.kxx = c->d_kxx; J.kyy = c->d_kyy; J.kzz = c->d_kzz;
+                jobs[L].push_back(J);
+                cfg[L] = mode == 2 ? std::make_pair(c->thr_y2, c->smem_y2) : std::make_pair(c->thr_z2, c->smem_z2);
+            }
+            int r = DFDM_OK;
+            for (auto &kv : jobs) {
+                const int thr = cfg[kv.first].first;
+                const size_t sm = cfg[kv.first].second;
+                with_fft2l(kv.first, [&](auto n) {
+                    constexpr int L = decltype(n)::value;
+                    if (mode == 0) r = launch_groups(kv.second, [&](const GroupTable<ColJob> &t, int nb) { kg_col<0, L><<<nb, thr, sm, st>>>(t); });
+                    else if (mode == 1) r = launch_groups(kv.second, [&](const GroupTable<ColJob> &t, int nb) { kg_col<1, L><<<nb, thr, sm, st>>>(t); });
+                    else r = launch_groups(kv.second, [&](const GroupTable<ColJob> &t, int nb) { kg_col<2, L><<<nb, thr, sm, st>>>(t); });
+                });
+                if (r) return r;
+            }
+            return r;
+        };
+        if ((rc = col_family(0))) return rc;
+        {
+            std::vector<YJob> yj;
+            size_t ysm = 0;
+            for (dfdm_ctx *c : g->cs) {
+                if (c->yper) continue;
+                YJob J;
+                J.grid = dim3((unsigned)((c->d.Nxc + 63) / 64), (unsigned)c->d.Nz, 1);
+                J.d = c->d; J.spec = (C *)c->spec; J.rpiv = c->d_rpiv; J.lo = c->d_lo; J.up = c->d_up;
+                yj.push_back(J);
+                ysm = std::max(ysm, (size_t)2 * c->d.Ny * sizeof(double));
+            }
+            if ((rc = launch_groups(yj, [&](const GroupTable<YJob> &t, int nb) { kg_ysolve<<<nb, 64, ysm, st>>>(t); }))) return rc;
+        }
+        if ((rc = col_family(2))) return rc;
+        if ((rc = col_family(1))) return rc;
+        // ---- inverse x, per length ----
+        std::map<int, std::vector<InvXJob>> ix;
+        std::map<int, size_t> ix_smem;
+        for (dfdm_ctx *c : g->cs) {
+            InvXJob J;
+            const long long lines = (long long)c->d.Ny * c->d.Nz;
+            J.grid = dim3((unsigned)((lines + c->lxi2 - 1) / c->lxi2), 1, 1);
+            J.a = poisson_args<float>(c); J.lx = c->lxi2;
+            J.spec = (const C *)c->spec; J.phi = (float *)c->phi; J.tw = (const C *)c->tw_x; J.twr = (const C *)c->twr_x;
+            ix[c->d.Nx / 2].push_back(J);
+            ix_smem[c->d.Nx / 2] = c->smem_xi2;
+        }
+        for (auto &kv : ix) {
+            with_fft2l(kv.first, [&](auto n) {
+                constexpr int M = decltype(n)::value;
+                rc = launch_groups(kv.second, [&](const GroupTable<InvXJob> &t, int nb) { kg_inv_x<M><<<nb, 256, ix_smem[M], st>>>(t); });
+            });
+            if (rc) return rc;
+        }
+        // ---- stage 3: the correction (+ P); stages 1 and 2 are corrected in the next stage kernel's loader ----
+        if (s == 3) {
+            std::vector<CorrJob> cj;
+            for (dfdm_ctx *c : g->cs) {
+                const bool inc = I::incr_form(c, 3);
+                CorrJob J;
+                const Dims &d = c->d;
+                J.grid = dim3((unsigned)((d.Nx / 4 + 63) / 64), (unsigned)((d.Ny + 3) / 4), (unsigned)d.Nz);
+                J.a = poisson_args<float>(c);
+                J.phi = (const float *)c->phi; J.us = (const float *)c->us; J.vs = (const float *)c->vs; J.ws = (const float *)c->wsf;
+                J.U = (float *)c->u; J.V = (float *)c->v; J.W = (float *)c->w; J.P = (float *)c->p;
+                J.uo = inc ? (const float *)c->u : nullptr; J.vo = inc ? (const float *)c->v : nullptr;
+                J.wo = inc ? (const float *)c->w : nullptr;
+                cj.push_back(J);
+            }
+            if ((rc = launch_groups(cj, [&](const GroupTable<CorrJob> &t, int nb) { kg_correct4<<<nb, dim3(64, 4, 1), 0, st>>>(t); }))) return rc;
+        }
+    }
+    // ---- constant-flux shift of the channel cases ----
+    std::vector<BulkJob> bj;
+    std::vector<FinalJob> fj;
+    std::vector<ShiftJob> sj;
+    for (dfdm_ctx *c : g->cs) {
+        if (c->prm.flow_forcing_mode != 1) continue;
+        BulkJob B;
+        B.grid = dim3((unsigned)c->red_blocks, 1, 1);
+        B.d = c->d; B.U = (const float *)c->u; B.dyc = c->d_dyc; B.dzc = c->d_dzc; B.ubd = c->d_ubd; B.part = c->red_part;
+        bj.push_back(B);
+        FinalJob F;
+        F.grid = dim3(1, 1, 1);
+        F.nparts = c->red_blocks; F.part = c->red_part; F.Ub_target = c->prm.Ub_target; F.out = c->red_out;
+        fj.push_back(F);
+        ShiftJob S;
+        S.grid = dim3((unsigned)c->red_blocks, 1, 1);
+        S.d = c->d; S.U = (float *)c->u; S.dU = c->red_out;
+        sj.push_back(S);
+    }
+    int rc;
+    if ((rc = launch_groups(bj, [&](const GroupTable<BulkJob> &t, int nb) { kg_bulk_partial<<<nb, 256, 0, st>>>(t); }))) return rc;
+    if ((rc = launch_groups(fj, [&](const GroupTable<FinalJob> &t, int nb) { kg_bulk_final<<<nb, 256, 0, st>>>(t); }))) return rc;
+    if ((rc = launch_groups(sj, [&](const GroupTable<ShiftJob> &t, int nb) { kg_shift<<<nb, 256, 0, st>>>(t); }))) return rc;
+    return DFDM_OK;
+}
+
+void group_destroy_graph(dfdm_group *g) {
+    if (g->gexec) { cudaGraphExecDestroy(g->gexec); g->gexec = nullptr; }
+    if (g->graph) { cudaGraphDestroy(g->graph); g->graph = nullptr; }
+}
+
+// dynamic shared memory of every grouped transform instantiation the group launches
+int group_attributes(dfdm_group *g) {
+    int rc = DFDM_OK;
+    auto setattr = [&](const void *fn, size_t bytes) {
+        if (rc || bytes <= 48 * 1024) return;
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess) rc = fail(DFDM_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+    };
+    for (dfdm_ctx *c : g->cs) {
+        with_fft2l(c->d.Nx / 2, [&](auto n) {
+            constexpr int M = decltype(n)::value;
+            setattr((const void *)kg_fwd_x<M>, c->smem_x2);
+            setattr((const void *)kg_inv_x<M>, c->smem_xi2);
+        });
+        with_fft2l(c->d.Nz, [&](auto n) {
+            constexpr int L = decltype(n)::value;
+            setattr((const void *)kg_col<0, L>, c->smem_z2);
+            setattr((const void *)kg_col<1, L>, c->smem_z2);
+        });
+        if (c->yper)
+            with_fft2l(c->d.Ny, [&](auto n) {
+                constexpr int L = decltype(n)::value;
+                setattr((const void *)kg_col<2, L>, c->smem_y2);
+            });
+    }
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dfdm_group_create(dfdm_ctx *const *ctxs, int n, void *stream, dfdm_group **out) {
+    g_err.clear();
+    if (!out) return fail(DFDM_ERR_INVALID, "null output");
+    *out = nullptr;
+    if (n < 1 || !ctxs) return fail(DFDM_ERR_INVALID, "a group needs at least one context");
+    for (int q = 0; q < n; ++q) {
+        if (int rc = check_ctx(ctxs[q])) return rc;
+        if (int rc = group_eligible(ctxs[q])) return rc;
+        for (int r = 0; r < q; ++r)
+            if (ctxs[r] == ctxs[q]) return fail(DFDM_ERR_INVALID, "a context appears twice in the group");
+    }
+    dfdm_group *g = new dfdm_group;
+    g->cs.assign(ctxs, ctxs + n);
+    g->stream = stream ? (cudaStream_t)stream : ctxs[0]->stream;
+    if (int rc = group_attributes(g)) { delete g; return rc; }
+    if (cudaEventCreateWithFlags(&g->ev, cudaEventDisableTiming) != cudaSuccess) {
+        delete g;
+        return fail(DFDM_ERR_CUDA, "event creation failed");
+    }
+    *out = g;
+    return DFDM_OK;
+}
+
+int dfdm_group_step_async(dfdm_group *g, int nsteps) {
+    g_err.clear();
+    if (!g) return fail(DFDM_ERR_INVALID, "null group");
+    if (nsteps < 0) return fail(DFDM_ERR_INVALID, "nsteps must be >= 0");
+    if (nsteps == 0) return DFDM_OK;
+    // each member's earlier work on its own stream comes before the group's steps (and the members' later work,
+    // below, after them), without a host synchronisation
+    for (dfdm_ctx *c : g->cs)
+        if (c->stream != g->stream) {
+            CK(cudaEventRecord(g->ev, c->stream));
+            CK(cudaStreamWaitEvent(g->stream, g->ev, 0));
+        }
+    for (int n = 0; n < nsteps; ++n) {
+        if (!g->gexec) {   // one step of the whole group, captured once per group
+            CK(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+            long long before = g_launches;
+            int rc = group_step_enqueue(g);
+            g->graph_launches = g_launches - before;
+            g_launches = before;
+            cudaGraph_t gr = nullptr;
+            cudaError_t e = cudaStreamEndCapture(g->stream, &gr);
+            if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }
+            if (e != cudaSuccess) return fail(DFDM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            g->graph = gr;
+            CK(cudaGraphInstantiate(&g->gexec, g->graph, 0));
+        }
+        CK(cudaGraphLaunch(g->gexec, g->stream));
+        g->launches += g->graph_launches;
+        for (dfdm_ctx *c : g->cs) c->t += c->prm.dt;   // the group's kernels are counted on the group
+    }
+    CK(cudaEventRecord(g->ev, g->stream));
+    for (dfdm_ctx *c : g->cs)
+        if (c->stream != g->stream) CK(cudaStreamWaitEvent(c->stream, g->ev, 0));
+    return DFDM_OK;
+}
+
+int dfdm_group_synchronize(dfdm_group *g) {
+    if (!g) return fail(DFDM_ERR_INVALID, "null group");
+    CK(cudaStreamSynchronize(g->stream));
+    return DFDM_OK;
+}
+
+int dfdm_group_launch_count(dfdm_group *g, long long *count) {
+    if (!g || !count) return fail(DFDM_ERR_INVALID, "null argument");
+    *count = g->launches;
+    return DFDM_OK;
+}
+
+// no host wait: an executable graph and an event destroyed while in flight are released when the device is done
+int dfdm_group_destroy(dfdm_group *g) {
+    if (!g) return DFDM_OK;
+    group_destroy_graph(g);
+    if (g->ev) cudaEventDestroy(g->ev);
+    delete g;
     return DFDM_OK;
 }
 

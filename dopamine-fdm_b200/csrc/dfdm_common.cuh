@@ -17,6 +17,20 @@
 
 namespace dfdm {
 
+// Block coordinates of a kernel body.  A per-case kernel passes HwBlock, whose accessors read the hardware registers
+// at each use (the body then compiles as if it named blockIdx / gridDim itself); a grouped launch (kernels_group.cuh)
+// passes JobBlock, the block's coordinates in its own case's grid.
+struct HwBlock {
+    __device__ __forceinline__ uint3 idx() const { return blockIdx; }
+    __device__ __forceinline__ dim3 dim() const { return gridDim; }
+};
+struct JobBlock {
+    uint3 b;
+    dim3 g;
+    __device__ __forceinline__ uint3 idx() const { return b; }
+    __device__ __forceinline__ dim3 dim() const { return g; }
+};
+
 template <typename T> struct cplx_t;
 template <> struct cplx_t<double> { typedef double2 type; };
 template <> struct cplx_t<float> { typedef float2 type; };

@@ -17,8 +17,9 @@ struct Kahan {
     }
 };
 
-// Block reduction of two compensated sums; thread 0 writes the block's pair to out[2*blockIdx].
-__device__ __forceinline__ void block_sum2(double a, double b, double *out) {
+// Block reduction of two compensated sums; thread 0 writes the block's pair to out[2*blk] (blk: the block's index in
+// its own grid, which in a grouped launch is not blockIdx.x).
+__device__ __forceinline__ void block_sum2(double a, double b, double *out, int blk) {
     __shared__ double sa[32], sb[32];
     for (int o = 16; o > 0; o >>= 1) {
         a += __shfl_down_sync(0xffffffffu, a, o);
@@ -35,7 +36,7 @@ __device__ __forceinline__ void block_sum2(double a, double b, double *out) {
             a += __shfl_down_sync(0xffffffffu, a, o);
             b += __shfl_down_sync(0xffffffffu, b, o);
         }
-        if (lane == 0) { out[2 * blockIdx.x] = a; out[2 * blockIdx.x + 1] = b; }
+        if (lane == 0) { out[2 * blk] = a; out[2 * blk + 1] = b; }
     }
 }
 
@@ -90,14 +91,14 @@ template <typename T> struct Chunk {
 // (u the stored field, ub the base profile).  A warp walks whole x-rows (row = k*Ny + j): the row's metrics are
 // loaded once, with no per-cell index division, and a lane reads its cells in 16-byte chunks (VEC: Nx a multiple of
 // the chunk; otherwise one cell at a time).
-template <typename T, bool VEC>
-__global__ void __launch_bounds__(256) k_bulk_partial(Dims d, const T *__restrict__ U, const double *__restrict__ dyc,
+template <typename T, bool VEC, class BC>
+__device__ __forceinline__ void k_bulk_partial_body(const BC &bc, const Dims &d, const T *__restrict__ U, const double *__restrict__ dyc,
                                                       const double *__restrict__ dzc, const double *__restrict__ ubd,
                                                       double *__restrict__ part) {
     typedef Chunk<T> Ch;
     Kahan s, w; s.init(); w.init();
     const int rows = d.Ny * d.Nz, Nx = d.Nx, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-    for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < rows; row += gridDim.x * wpb) {
+    for (int row = bc.idx().x * wpb + (threadIdx.x >> 5); row < rows; row += bc.dim().x * wpb) {
         const int k = row / d.Ny, j = row - k * d.Ny;
         const double a = dyc[j] * dzc[k], ub = ubd[j];
         const T *Ur = U + (size_t)row * Nx;
@@ -124,17 +125,24 @@ __global__ void __launch_bounds__(256) k_bulk_partial(Dims d, const T *__restric
         s.add((t + n * ub) * a);
         w.add(n * a);
     }
-    block_sum2(s.s, w.s, part);
+    block_sum2(s.s, w.s, part, bc.idx().x);
+}
+template <typename T, bool VEC>
+__global__ void __launch_bounds__(256) k_bulk_partial(Dims d, const T *__restrict__ U, const double *__restrict__ dyc,
+                                                      const double *__restrict__ dzc, const double *__restrict__ ubd,
+                                                      double *__restrict__ part) {
+    k_bulk_partial_body<T, VEC>(HwBlock(), d, U, dyc, dzc, ubd, part);
 }
 
 // Final pass over the block partials (one block): compensated per-thread sums in a fixed order, then a fixed tree;
 // writes Ub and the shift Ub_target - Ub.
-__global__ void __launch_bounds__(256) k_bulk_final(int nparts, const double *__restrict__ part, double Ub_target,
+template <class BC>
+__device__ __forceinline__ void k_bulk_final_body(const BC &bc, int nparts, const double *__restrict__ part, double Ub_target,
                                                     double *__restrict__ out) {
     __shared__ double tot[2];
     Kahan s, w; s.init(); w.init();
     for (int b = threadIdx.x; b < nparts; b += blockDim.x) { s.add(part[2 * b]); w.add(part[2 * b + 1]); }
-    block_sum2(s.s, w.s, tot);   // gridDim.x == 1: writes tot[0], tot[1]
+    block_sum2(s.s, w.s, tot, 0);   // one block: tot[0], tot[1]
     __syncthreads();
     if (threadIdx.x == 0) {
         const double Ub = tot[0] / fmax(tot[1], 1e-14);
@@ -142,14 +150,18 @@ __global__ void __launch_bounds__(256) k_bulk_final(int nparts, const double *__
         out[1] = Ub_target - Ub;
     }
 }
+__global__ void __launch_bounds__(256) k_bulk_final(int nparts, const double *__restrict__ part, double Ub_target,
+                                                    double *__restrict__ out) {
+    k_bulk_final_body(HwBlock(), nparts, part, Ub_target, out);
+}
 
 // U += (Ub_target - Ub) on every independent U face (src/time_integration.f90:581-583); four faces per thread
 // when the cell count allows 16-byte (FP32) accesses.
-template <typename T>
-__global__ void __launch_bounds__(256) k_shift(Dims d, T *__restrict__ U, const double *__restrict__ dU) {
+template <typename T, class BC>
+__device__ __forceinline__ void k_shift_body(const BC &bc, const Dims &d, T *__restrict__ U, const double *__restrict__ dU) {
     const T s = (T)dU[1];
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    const long long first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long stride = (long long)bc.dim().x * blockDim.x;
+    const long long first = (long long)bc.idx().x * blockDim.x + threadIdx.x;
     if constexpr (sizeof(T) == 4) {
         if ((d.cells & 3) == 0) {
             float4 *U4 = reinterpret_cast<float4 *>(U);
@@ -162,6 +174,10 @@ __global__ void __launch_bounds__(256) k_shift(Dims d, T *__restrict__ U, const 
         }
     }
     for (long long p = first; p < d.cells; p += stride) U[p] = U[p] + s;
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_shift(Dims d, T *__restrict__ U, const double *__restrict__ dU) {
+    k_shift_body<T>(HwBlock(), d, U, dU);
 }
 
 // check_divergence (src/projection.f90:607-639), max |U| over the U faces and the NaN / |u| > 1e8 guard of
@@ -228,7 +244,7 @@ __global__ void __launch_bounds__(256) k_wall_diag(int Nx, int Nz, const double 
         s.add(tx[p]);
         w.add(tx[plane + p]);
     }
-    block_sum2(s.s, w.s, out);   // gridDim.x == 1
+    block_sum2(s.s, w.s, out, 0);   // one block
 }
 
 // The monitor values (the layout of dfdm_monitor): t, dt, mean U, max |U|, max |div u|, CFL conv, CFL visc, mean
@@ -370,7 +386,7 @@ __global__ void __launch_bounds__(256) k_ke_partial(Dims d, const T *__restrict_
         s.add(0.5 * (uc * uc + vc * vc + wc * wc) * vol);
         w.add(vol);
     }
-    block_sum2(s.s, w.s, part);
+    block_sum2(s.s, w.s, part, blockIdx.x);
 }
 
 __global__ void k_ratio_final(int nparts, const double *__restrict__ part, double *__restrict__ out) {

@@ -20,8 +20,8 @@ template <> struct Vec2<double> { typedef double2 type; };
 // ---- div u* (or a real field) + forward real-to-complex x transform, line length Nx = 2M ----------------------
 // Phase A forms the packed half-length line z_n = x_2n + i x_2n+1 in shared memory with consecutive threads on
 // consecutive pairs (coalesced 8-byte loads of the velocity pairs); the two register steps follow.
-template <typename T, bool FROM_DIV, int M>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_fwd_x2(PoissonArgs<T> a, int lx, const T *__restrict__ U, const T *__restrict__ V,
+template <typename T, bool FROM_DIV, int M, class BC>
+__device__ __forceinline__ void k_fwd_x2_body(const BC &bc, const PoissonArgs<T> &a, int lx, const T *__restrict__ U, const T *__restrict__ V,
                                                 const T *__restrict__ W, const T *__restrict__ src,
                                                 typename cplx_t<T>::type *__restrict__ spec,
                                                 const typename cplx_t<T>::type *__restrict__ tw,
@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_fwd_x2(PoissonA
     const int Ny = d.Ny, Nz = d.Nz, plane = Nx * Ny;
     // blocks run roughly in index order: the first take the highest lines (top z planes), which the stage kernel
     // wrote last and which are the likeliest to still be in L2
-    const int line0 = (gridDim.x - 1 - blockIdx.x) * lx;
+    const int line0 = (bc.dim().x - 1 - bc.idx().x) * lx;
     const int nl = min(lx, Ny * Nz - line0);
     constexpr int ITEMS = RowLines<T, M>::value * M;   // lx == RowLines<T, M>::value, blockDim.x == 256
     constexpr int PER = (ITEMS + 255) / 256, UNR = sizeof(T) == 4 ? 4 : 2;   // items per thread; items loaded together
@@ -129,10 +129,18 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_fwd_x2(PoissonA
         spec[(size_t)(line0 + ll) * Nxc + kx] = X;
     }
 }
+template <typename T, bool FROM_DIV, int M>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_fwd_x2(PoissonArgs<T> a, int lx, const T *__restrict__ U, const T *__restrict__ V,
+                                                const T *__restrict__ W, const T *__restrict__ src,
+                                                typename cplx_t<T>::type *__restrict__ spec,
+                                                const typename cplx_t<T>::type *__restrict__ tw,
+                                                const typename cplx_t<T>::type *__restrict__ twr) {
+    k_fwd_x2_body<T, FROM_DIV, M>(HwBlock(), a, lx, U, V, W, src, spec, tw, twr);
+}
 
 // ---- inverse complex-to-real x transform, writes phi = x / (nxp*nzp) -----------------------------------------
-template <typename T, int M>
-__global__ void __launch_bounds__(256) k_inv_x2(PoissonArgs<T> a, int lx, const typename cplx_t<T>::type *__restrict__ spec,
+template <typename T, int M, class BC>
+__device__ __forceinline__ void k_inv_x2_body(const BC &bc, const PoissonArgs<T> &a, int lx, const typename cplx_t<T>::type *__restrict__ spec,
                                                 T *__restrict__ phi, const typename cplx_t<T>::type *__restrict__ tw,
                                                 const typename cplx_t<T>::type *__restrict__ twr) {
     typedef typename cplx_t<T>::type C;
@@ -143,7 +151,7 @@ __global__ void __launch_bounds__(256) k_inv_x2(PoissonArgs<T> a, int lx, const 
     C *bt = (C *)smem_raw;
     const Dims &d = a.d;
     const int Nxc = d.Nxc;
-    const int line0 = blockIdx.x * lx;
+    const int line0 = bc.idx().x * lx;
     const int nl = min(lx, d.Ny * d.Nz - line0);
     for (int b = threadIdx.x; b < nl * N2; b += blockDim.x) {
         const int ll = b / N2, n2 = b - ll * N2;
@@ -181,6 +189,12 @@ __global__ void __launch_bounds__(256) k_inv_x2(PoissonArgs<T> a, int lx, const 
         }
     }
 }
+template <typename T, int M>
+__global__ void __launch_bounds__(256) k_inv_x2(PoissonArgs<T> a, int lx, const typename cplx_t<T>::type *__restrict__ spec,
+                                                T *__restrict__ phi, const typename cplx_t<T>::type *__restrict__ tw,
+                                                const typename cplx_t<T>::type *__restrict__ twr) {
+    k_inv_x2_body<T, M>(HwBlock(), a, lx, spec, phi, tw, twr);
+}
 
 // ---- z transforms (MODE 0 forward, 1 inverse) and the periodic-y solve (MODE 2) on tiles of NL kx columns ----
 // MODE 2: forward FFT along y, division by kxx+kyy+kzz with the (0,0,0) mode set to zero, inverse FFT, division
@@ -190,88 +204,9 @@ __global__ void __launch_bounds__(256) k_col2(Dims d, typename cplx_t<T>::type *
                                               const typename cplx_t<T>::type *__restrict__ tw,
                                               const double *__restrict__ kxx, const double *__restrict__ kyy,
                                               const double *__restrict__ kzz) {
-    typedef typename cplx_t<T>::type C;
-    constexpr int N1 = Split<L>::N1, N2 = Split<L>::N2;
-    constexpr bool INV1 = (MODE == 1);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *t = (C *)smem_raw;          // step-1 outputs, [e*NL + c]
-    C *nat = t + L * NL;           // MODE 2: natural-order spectrum between the two transforms
-    const int kx0 = blockIdx.x * NL;
-    const int other = blockIdx.y;
-    const int Nxc = d.Nxc;
-    size_t base;
-    int rowstride;
-    if (MODE == 2) { base = (size_t)other * d.Ny * Nxc; rowstride = Nxc; }
-    else { base = (size_t)other * Nxc; rowstride = d.Ny * Nxc; }
-    C *colbase = spec + base + kx0;
-    for (int b = threadIdx.x; b < NL * N2; b += blockDim.x) {
-        const int c = b % NL, n2 = b / NL;
-        const bool ok = kx0 + c < Nxc;
-        C v[N1];
-#pragma unroll
-        for (int n1 = 0; n1 < N1; ++n1) v[n1] = ok ? colbase[(size_t)(n1 * N2 + n2) * rowstride + c] : mkc<T>(T(0), T(0));
-        col_step1<T, INV1, L, NL>(v, t, c, n2, tw);
-    }
-    __syncthreads();
-    if (MODE != 2) {
-        for (int b = threadIdx.x; b < NL * N1; b += blockDim.x) {
-            const int c = b % NL, k1 = b / NL;
-            C v[N2];
-#pragma unroll
-            for (int n2 = 0; n2 < N2; ++n2) v[n2] = t[(k1 * N2 + n2) * NL + c];
-            Codelet<T, INV1, N2>::run(v);
-            if (kx0 + c < Nxc) {
-#pragma unroll
-                for (int k2 = 0; k2 < N2; ++k2) colbase[(size_t)(k1 + N1 * k2) * rowstride + c] = v[k2];
-            }
-        }
-        return;
-    }
-    // MODE 2: finish the forward transform, divide, write natural order
-    const int kz = other;
-    for (int b = threadIdx.x; b < NL * N1; b += blockDim.x) {
-        const int c = b % NL, k1 = b / NL, kx = kx0 + c;
-        C v[N2];
-#pragma unroll
-        for (int n2 = 0; n2 < N2; ++n2) v[n2] = t[(k1 * N2 + n2) * NL + c];
-        Codelet<T, false, N2>::run(v);
-#pragma unroll
-        for (int k2 = 0; k2 < N2; ++k2) {
-            const int j = k1 + N1 * k2;
-            C x = v[k2];
-            if (kx < Nxc) {
-                double wavenum_sum = kxx[kx] + kyy[j] + kzz[kz];
-                if (kx == 0 && j == 0 && kz == 0) { x.x = T(0); x.y = T(0); }
-                else { x.x = (T)((double)x.x / wavenum_sum); x.y = (T)((double)x.y / wavenum_sum); }
-            }
-            nat[j * NL + c] = x;
-        }
-    }
-    __syncthreads();
-    for (int b = threadIdx.x; b < NL * N2; b += blockDim.x) {
-        const int c = b % NL, n2 = b / NL;
-        C v[N1];
-#pragma unroll
-        for (int n1 = 0; n1 < N1; ++n1) v[n1] = nat[(n1 * N2 + n2) * NL + c];
-        col_step1<T, true, L, NL>(v, t, c, n2, tw);
-    }
-    __syncthreads();
-    const double nyp = (double)L;
-    for (int b = threadIdx.x; b < NL * N1; b += blockDim.x) {
-        const int c = b % NL, k1 = b / NL;
-        C v[N2];
-#pragma unroll
-        for (int n2 = 0; n2 < N2; ++n2) v[n2] = t[(k1 * N2 + n2) * NL + c];
-        Codelet<T, true, N2>::run(v);
-        if (kx0 + c < Nxc) {
-#pragma unroll
-            for (int k2 = 0; k2 < N2; ++k2) {
-                C x = v[k2];
-                x.x = (T)((double)x.x / nyp); x.y = (T)((double)x.y / nyp);
-                colbase[(size_t)(k1 + N1 * k2) * rowstride + c] = x;
-            }
-        }
-    }
+#define DFDM_BLOCK_IDX blockIdx
+#include "k_col2_body.inc"
+#undef DFDM_BLOCK_IDX
 }
 
 }  // namespace dfdm

@@ -153,8 +153,8 @@ __global__ void __launch_bounds__(256) k_col_fft(Dims d, typename cplx_t<T>::typ
 // consecutive kx, so every row access is coalesced.  Each sweep keeps two register buffers of CH rows and issues
 // the loads of the next chunk before the recurrence of the current one runs, and the per-row coefficients DL and
 // DU are read from shared memory.
-template <typename T, int CH>
-__global__ void __launch_bounds__(64) k_ysolve2(Dims d, typename cplx_t<T>::type *__restrict__ spec,
+template <typename T, int CH, class BC>
+__device__ __forceinline__ void k_ysolve2_body(const BC &bc, const Dims &d, typename cplx_t<T>::type *__restrict__ spec,
                                                 const double *__restrict__ rpiv, const double *__restrict__ lo,
                                                 const double *__restrict__ up) {
     typedef typename cplx_t<T>::type C;
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(64) k_ysolve2(Dims d, typename cplx_t<T>::type
     const int Nxc = d.Nxc, n = d.Ny;
     for (int r = threadIdx.x; r < n; r += blockDim.x) { sco[r] = lo[r]; sco[n + r] = up[r]; }
     __syncthreads();
-    const int kx = blockIdx.x * blockDim.x + threadIdx.x, kz = blockIdx.y;
+    const int kx = bc.idx().x * blockDim.x + threadIdx.x, kz = bc.idx().y;
     if (kx >= Nxc) return;
     C *col = spec + kz * n * Nxc + kx;
     const double *rp = rpiv + kz * n * Nxc + kx;
@@ -231,6 +231,12 @@ __global__ void __launch_bounds__(64) k_ysolve2(Dims d, typename cplx_t<T>::type
         if (r0 - 2 * CH >= 0) bload(va, ra, r0 - 2 * CH);
         bproc(vb, rb, r0 - CH);
     }
+}
+template <typename T, int CH>
+__global__ void __launch_bounds__(64) k_ysolve2(Dims d, typename cplx_t<T>::type *__restrict__ spec,
+                                                const double *__restrict__ rpiv, const double *__restrict__ lo,
+                                                const double *__restrict__ up) {
+    k_ysolve2_body<T, CH>(HwBlock(), d, spec, rpiv, lo, up);
 }
 
 // ---- 4. inverse complex-to-real x transform, writes the pseudo-pressure phi ----------------------------------
@@ -315,8 +321,8 @@ template <typename T> struct Vec4;
 template <> struct Vec4<float> { typedef float4 type; };
 template <> struct Vec4<double> { typedef double4 type; };
 
-template <typename T>
-__global__ void __launch_bounds__(256) k_correct4(PoissonArgs<T> a, const T *__restrict__ phi, const T *__restrict__ us,
+template <typename T, class BC>
+__device__ __forceinline__ void k_correct4_body(const BC &bc, const PoissonArgs<T> &a, const T *__restrict__ phi, const T *__restrict__ us,
                                                   const T *__restrict__ vs, const T *__restrict__ ws, T *__restrict__ U,
                                                   T *__restrict__ V, T *__restrict__ W, T *__restrict__ P,
                                                   const T *__restrict__ uo, const T *__restrict__ vo, const T *__restrict__ wo) {
@@ -324,8 +330,8 @@ __global__ void __launch_bounds__(256) k_correct4(PoissonArgs<T> a, const T *__r
     typedef Arith<T> A;
     const Dims &d = a.d;
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz, plane = Nx * Ny, nq = Nx >> 2;
-    const int iq = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    const int iq = bc.idx().x * blockDim.x + threadIdx.x;
+    const int j = bc.idx().y * blockDim.y + threadIdx.y, k = bc.idx().z;
     if (iq >= nq || j >= Ny) return;
     const int i = iq << 2;
     const int p = k * plane + j * Nx + i;
@@ -369,6 +375,13 @@ __global__ void __launch_bounds__(256) k_correct4(PoissonArgs<T> a, const T *__r
         }
         *reinterpret_cast<V4 *>(P + p) = o;
     }
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_correct4(PoissonArgs<T> a, const T *__restrict__ phi, const T *__restrict__ us,
+                                                  const T *__restrict__ vs, const T *__restrict__ ws, T *__restrict__ U,
+                                                  T *__restrict__ V, T *__restrict__ W, T *__restrict__ P,
+                                                  const T *__restrict__ uo, const T *__restrict__ vo, const T *__restrict__ wo) {
+    k_correct4_body<T>(HwBlock(), a, phi, us, vs, ws, U, V, W, P, uo, vo, wo);
 }
 
 }  // namespace dfdm

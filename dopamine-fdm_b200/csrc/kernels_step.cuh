@@ -616,11 +616,11 @@ __device__ __forceinline__ void stage_cell(const StepArgs<T> &a, const Q &q, con
 // k_correct would have stored.  phi planes rotate through five more shared planes and are copied two planes ahead
 // of the velocity planes (a plane's w correction needs phi of the plane above), so they have landed, and passed a
 // barrier, before the plane that needs them is corrected.
-template <typename T, bool LES, bool WM, int TX, int TY, int KIND, bool CORR = false>
-__global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepArgs<T> a, const T *__restrict__ U, const T *__restrict__ V,
+template <typename T, bool LES, bool WM, int TX, int TY, int KIND, bool CORR = false, class BC>
+__device__ __forceinline__ void k_tiled_body(const BC &bc, const StepArgs<T> &a, const T *__restrict__ U, const T *__restrict__ V,
                                                   const T *__restrict__ W, const T *__restrict__ NU,
                                                   const double *__restrict__ tau_x, const double *__restrict__ tau_z,
-                                                  StageCoef sc, int kc, T *__restrict__ uo, T *__restrict__ vo,
+                                                  const StageCoef &sc, const int kc, T *__restrict__ uo, T *__restrict__ vo,
                                                   T *__restrict__ wo, T *__restrict__ f1u, T *__restrict__ f1v,
                                                   T *__restrict__ f1w, T *__restrict__ us, T *__restrict__ vs,
                                                   T *__restrict__ wsf, T *__restrict__ rhs_only, T *__restrict__ nut_out) {
@@ -632,8 +632,8 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
     __shared__ __align__(16) T smp[CORR ? 5 : 1][CORR ? PSP : 1];
     const Dims &d = a.d;
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
-    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
-    const int k0 = blockIdx.z * kc, kend = min(k0 + kc, Nz);
+    const int i0 = bc.idx().x * TX, j0 = bc.idx().y * TY;
+    const int k0 = bc.idx().z * kc, kend = min(k0 + kc, Nz);
     const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
     const int i = i0 + tx, j = j0 + ty;
     const bool active = i < Nx && j < Ny;
@@ -784,6 +784,16 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
         __syncthreads();
     }
 }
+template <typename T, bool LES, bool WM, int TX, int TY, int KIND, bool CORR = false>
+__global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepArgs<T> a, const T *__restrict__ U, const T *__restrict__ V,
+                                                  const T *__restrict__ W, const T *__restrict__ NU,
+                                                  const double *__restrict__ tau_x, const double *__restrict__ tau_z,
+                                                  StageCoef sc, int kc, T *__restrict__ uo, T *__restrict__ vo,
+                                                  T *__restrict__ wo, T *__restrict__ f1u, T *__restrict__ f1v,
+                                                  T *__restrict__ f1w, T *__restrict__ us, T *__restrict__ vs,
+                                                  T *__restrict__ wsf, T *__restrict__ rhs_only, T *__restrict__ nut_out) {
+    k_tiled_body<T, LES, WM, TX, TY, KIND, CORR>(HwBlock(), a, U, V, W, NU, tau_x, tau_z, sc, kc, uo, vo, wo, f1u, f1v, f1w, us, vs, wsf, rhs_only, nut_out);
+}
 
 
 // One thread's pair of cells (i, i+1) of plane k from the shared-memory neighbourhood q: the three right-hand sides
@@ -844,11 +854,11 @@ __device__ __forceinline__ void stage_pair(const StepArgs<float> &a, const TileQ
 // per row of 32 cell pairs; HYB adds the dissipative terms of advection_scheme = 2 (StepArgs::adv); CORR fuses
 // the previous stage's correction into the loader as k_tiled does.  It needs ~118 registers: capping it at 96 or 80 (for more resident warps) spills
 // 170-300 bytes, so it runs 2 blocks of 256 threads per SM.  Shared rows hold cells i0-2 .. i0+65 (pitch 68), so every pair starts at an even index.
-template <bool LES, bool WM, int TY = 8, bool HYB = false, bool CORR = false>
-__global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<float> a, const float *__restrict__ U, const float *__restrict__ V,
+template <bool LES, bool WM, int TY = 8, bool HYB = false, bool CORR = false, class BC>
+__device__ __forceinline__ void k_tiled2_body(const BC &bc, const StepArgs<float> &a, const float *__restrict__ U, const float *__restrict__ V,
                                                    const float *__restrict__ W, const float *__restrict__ NU,
                                                    const double *__restrict__ tau_x, const double *__restrict__ tau_z,
-                                                   StageCoef sc, int kc, float *__restrict__ uo, float *__restrict__ vo,
+                                                   const StageCoef &sc, const int kc, float *__restrict__ uo, float *__restrict__ vo,
                                                    float *__restrict__ wo, float *__restrict__ f1u, float *__restrict__ f1v,
                                                    float *__restrict__ f1w, float *__restrict__ us, float *__restrict__ vs,
                                                    float *__restrict__ wsf, float *__restrict__ rhs_only) {
@@ -866,8 +876,8 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
     __shared__ float zmr[4][8];
     const Dims &d = a.d;
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz;
-    const int i0 = blockIdx.x * TXC, j0 = blockIdx.y * TY;
-    const int k0 = blockIdx.z * kc, kend = min(k0 + kc, Nz);
+    const int i0 = bc.idx().x * TXC, j0 = bc.idx().y * TY;
+    const int k0 = bc.idx().z * kc, kend = min(k0 + kc, Nz);
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int i = i0 + 2 * tx, j = j0 + ty;
     const bool active = i < Nx && j < Ny;   // Nx is even: the pair's second cell is in range too
@@ -1027,6 +1037,16 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
         if (more) fix(snext, k + 2);   // CORR: phi k+2 and k+3 were copied one and two iterations ago
         __syncthreads();
     }
+}
+template <bool LES, bool WM, int TY = 8, bool HYB = false, bool CORR = false>
+__global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<float> a, const float *__restrict__ U, const float *__restrict__ V,
+                                                   const float *__restrict__ W, const float *__restrict__ NU,
+                                                   const double *__restrict__ tau_x, const double *__restrict__ tau_z,
+                                                   StageCoef sc, int kc, float *__restrict__ uo, float *__restrict__ vo,
+                                                   float *__restrict__ wo, float *__restrict__ f1u, float *__restrict__ f1v,
+                                                   float *__restrict__ f1w, float *__restrict__ us, float *__restrict__ vs,
+                                                   float *__restrict__ wsf, float *__restrict__ rhs_only) {
+    k_tiled2_body<LES, WM, TY, HYB, CORR>(HwBlock(), a, U, V, W, NU, tau_x, tau_z, sc, kc, uo, vo, wo, f1u, f1v, f1w, us, vs, wsf, rhs_only);
 }
 
 }  // namespace dfdm

@@ -32,7 +32,8 @@ def sources():
 
 
 def deps():
-    return sources() + sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + [os.path.join(INCLUDE, "dfdm.h")]
+    return (sources() + sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + sorted(glob.glob(os.path.join(CSRC, "*.inc")))
+            + [os.path.join(INCLUDE, "dfdm.h")])
 
 
 def up_to_date() -> bool:

@@ -35,7 +35,8 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_get_dt", "dfdm_set_landing_time", "dfdm_output_monitor", "dfdm_output_monitor_async",
            "dfdm_set_fused_correction", "dfdm_get_fused_correction", "dfdm_set_state_async", "dfdm_get_state_async",
            "dfdm_write_box_snapshot", "dfdm_set_landing_times", "dfdm_write_snapshot_ex", "dfdm_get_stage_timing",
-           "dfdm_set_sgs_in_tile", "dfdm_get_sgs_in_tile"]
+           "dfdm_set_sgs_in_tile", "dfdm_get_sgs_in_tile", "dfdm_group_create", "dfdm_group_step_async",
+           "dfdm_group_synchronize", "dfdm_group_launch_count", "dfdm_group_destroy"]
 
 
 class DfdmError(RuntimeError):
@@ -114,6 +115,11 @@ def load(build_if_missing: bool = True):
         "dfdm_output_monitor_async": (c_int, [c_void_p, c_void_p]),
         "dfdm_set_fused_correction": (c_int, [c_void_p, c_int]),
         "dfdm_get_fused_correction": (c_int, [c_void_p, POINTER(ctypes.c_int)]),
+        "dfdm_group_create": (c_int, [POINTER(c_void_p), c_int, c_void_p, POINTER(c_void_p)]),
+        "dfdm_group_step_async": (c_int, [c_void_p, c_int]),
+        "dfdm_group_synchronize": (c_int, [c_void_p]),
+        "dfdm_group_launch_count": (c_int, [c_void_p, POINTER(ctypes.c_longlong)]),
+        "dfdm_group_destroy": (c_int, [c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -422,3 +428,49 @@ class Solver:
         v = c_double(0.0)
         _check(load().dfdm_kernel_bytes(self.h, int(which), ctypes.byref(v)))
         return v.value
+
+
+class Group:
+    """Several FP32-mixed DNS solvers stepped together: one grouped launch per kernel family for all members, one
+    CUDA graph per group step (dfdm_group_create).  A member's results do not depend on the other members (the same
+    case steps bit-identically in a group of one and in any mix); against compute_time_step_RK3 steps of the member
+    alone they agree to FP32 rounding.  Members must have taken a first step."""
+
+    def __init__(self, solvers, stream: Optional[int] = None):
+        self.solvers = list(solvers)
+        hs = (c_void_p * len(self.solvers))(*[s.h.value if isinstance(s.h, c_void_p) else s.h for s in self.solvers])
+        h = c_void_p()
+        _check(load().dfdm_group_create(hs, len(self.solvers), c_void_p(stream) if stream else None, ctypes.byref(h)))
+        self.h = h
+
+    def step_async(self, nsteps: int = 1) -> None:
+        _check(load().dfdm_group_step_async(self.h, int(nsteps)))
+
+    def step(self, nsteps: int = 1) -> None:
+        self.step_async(nsteps)
+        self.synchronize()
+
+    def synchronize(self) -> None:
+        _check(load().dfdm_group_synchronize(self.h))
+
+    def launch_count(self) -> int:
+        v = ctypes.c_longlong(0)
+        _check(load().dfdm_group_launch_count(self.h, ctypes.byref(v)))
+        return int(v.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().dfdm_group_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -297,6 +297,195 @@ class GpuExecutor:
         self.finished = []
 
 
+class GroupScheduler:
+    """FIFO admission by device footprint, as Scheduler; the admitted cases step TOGETHER, as one serving group.
+
+    A case takes its first step on its own (set-up and the first projection), then joins the group: every chunk of
+    steps is one group step of all joined cases (one grouped launch per kernel family, dfdm_group_create), k steps
+    at a time, k = chunk_cell_steps / (the group's cells), cut at the first member to finish.  The composition
+    changes when a case joins or finishes; the executor keeps one group (one captured graph) per composition.  Up
+    to `depth` chunks are in flight, so the device works on one while the host prepares the next.
+
+    executor protocol:
+      footprint(req) -> bytes        prepare(req)          start(req) -> handle        can_enqueue(handle) -> bool
+      first_step(handle) -> token    group_step([handle], k) -> token                  done(token) -> bool
+      finish(handle, req, keep_state) -> (state, summary)   reclaim()   now()   idle(seconds or None)
+      defers_free: bool
+    """
+
+    def __init__(self, executor, budget_bytes: float, chunk_cell_steps: float = 2.5e7, max_active: int = 256,
+                 keep_state: bool = False, depth: int = 2):
+        self.ex = executor
+        self.budget = float(budget_bytes)
+        self.chunk_cell_steps = float(chunk_cell_steps)
+        self.max_active = int(max_active)
+        self.keep_state = keep_state
+        self.depth = int(depth)
+        self.peak_bytes = 0.0
+        self.peak_active = 0
+        self.peak_group = 0
+        self.reclaims = 0
+        self.chunks = 0
+        self.compositions = 0
+
+    def chunk(self, members: List[dict]) -> int:
+        cells = sum(a["req"].cells for a in members)
+        k = int(max(1, round(self.chunk_cell_steps / max(1, cells))))
+        return min([k] + [a["req"].nsteps - a["done"] for a in members])
+
+    def run(self, requests: List[Request], t0: Optional[float] = None) -> List[Result]:
+        ex = self.ex
+        defers = getattr(ex, "defers_free", False)
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        waiting: deque = deque()
+        active: List[dict] = []
+        inflight: List[tuple] = []      # (token, [(case, steps)], is a group chunk)
+        results: List[Result] = []
+        used = 0.0
+        held = 0.0
+        last = None
+        start = ex.now() if t0 is None else t0
+        while pending or waiting or active:
+            now = ex.now() - start
+            while pending and pending[0].arrival <= now:
+                r = pending.popleft()
+                fp = ex.footprint(r)
+                if fp > self.budget:
+                    raise ValueError(f"request {r.rid} needs {fp} bytes, more than the whole budget")
+                ex.prepare(r)
+                waiting.append((r, fp))
+            while waiting and len(active) < self.max_active:
+                r, fp = waiting[0]
+                if used + held + fp > self.budget and held > 0:
+                    ex.reclaim()
+                    held = 0.0
+                    self.reclaims += 1
+                if used + held + fp > self.budget:
+                    break
+                waiting.popleft()
+                used += fp
+                active.append({"req": r, "h": ex.start(r), "fp": fp, "done": 0, "completed": 0, "joined": False,
+                               "admitted": ex.now() - start})
+            self.peak_bytes = max(self.peak_bytes, used + held)
+            self.peak_active = max(self.peak_active, len(active))
+            progressed = False
+            # completed chunks (the group's chunks complete in order; first steps on their own streams)
+            keep = []
+            for item in inflight:
+                if ex.done(item[0]):
+                    for a, k in item[1]:
+                        a["completed"] += k
+                    progressed = True
+                else:
+                    keep.append(item)
+            inflight = keep
+            for a in list(active):
+                r = a["req"]
+                if a["completed"] >= r.nsteps:
+                    state, summary = ex.finish(a["h"], r, self.keep_state)
+                    results.append(Result(r.rid, r.arrival, a["admitted"], ex.now() - start, r.nsteps, r.cells,
+                                          state, summary))
+                    used -= a["fp"]
+                    if defers:
+                        held += a["fp"]
+                    active.remove(a)
+                    progressed = True
+                elif not a["joined"] and ex.can_enqueue(a["h"]):
+                    inflight.append((ex.first_step(a["h"]), [(a, 1)], False))
+                    a["done"] = 1
+                    a["joined"] = True
+                    progressed = True
+            members = [a for a in active if a["joined"] and a["done"] < a["req"].nsteps]
+            if members and sum(1 for item in inflight if item[2]) < self.depth:
+                k = self.chunk(members)
+                key = tuple(a["req"].rid for a in members)
+                if key != last:
+                    self.compositions += 1
+                    last = key
+                inflight.append((ex.group_step([a["h"] for a in members], k), [(a, k) for a in members], True))
+                for a in members:
+                    a["done"] += k
+                self.chunks += 1
+                self.peak_group = max(self.peak_group, len(members))
+                progressed = True
+            if not progressed:
+                nxt = pending[0].arrival - (ex.now() - start) if pending else None
+                ex.idle(nxt)
+        ex.reclaim()
+        return sorted(results, key=lambda x: x.rid)
+
+
+class GroupGpuExecutor(GpuExecutor):
+    """GroupScheduler's executor on one GPU: one dfdm context and CUDA stream per admitted case (set-up, first step
+    and the result transfer run there), and the group steps on one stream of their own, with one dfdm group (one
+    captured graph per group step) per composition, kept while the composition lasts.
+
+    The same object runs run_isolated: a case alone is a group of one on the case's own stream, so every result is
+    bit-identical alone and in any mix."""
+
+    def __init__(self, device: int = 0, workers: int = 4):
+        super().__init__(device=device, graphs=False, workers=workers)
+        from .native import Group
+        self.Group = Group
+        self.gstream = self.torch.cuda.Stream(device=device)
+        self.groups: Dict[tuple, object] = {}
+        self.retired: List[tuple] = []     # (group, event of its last chunk)
+
+    def _event(self, stream):
+        ev = self.torch.cuda.Event()
+        ev.record(stream)
+        return ev
+
+    def first_step(self, h):
+        self.can_enqueue(h)
+        h["s"].compute_time_step_RK3_async(1)
+        return self._event(h["st"])
+
+    def _group(self, hs):
+        key = tuple(id(h) for h in hs)
+        g = self.groups.get(key)
+        if g is None:
+            # compositions not in use any more are released once their last chunk is done
+            for k2 in list(self.groups):
+                self.retired.append((self.groups.pop(k2), self._event(self.gstream)))
+            g = self.Group([h["s"] for h in hs], stream=self.gstream.cuda_stream)
+            self.groups[key] = g
+        still = []
+        for gr, ev in self.retired:
+            if ev.query():
+                gr.close()
+            else:
+                still.append((gr, ev))
+        self.retired = still
+        return g
+
+    def group_step(self, hs, k: int):
+        self._group(hs).step_async(k)
+        return self._event(self.gstream)
+
+    def done(self, token) -> bool:
+        return token.query()
+
+    # run_isolated: first step on the case's stream, then a group of one on the same stream
+    def enqueue(self, h, nsteps: int) -> None:
+        if "ev0" in h:
+            h["ev0"].record(h["st"])
+        h["s"].compute_time_step_RK3_async(1)
+        if nsteps > 1:
+            g = self.Group([h["s"]], stream=h["st"].cuda_stream)
+            g.step_async(nsteps - 1)
+            g.close()
+        h["ev"].record(h["st"])
+
+    def reclaim(self) -> None:
+        for key in list(self.groups):
+            self.groups.pop(key).close()
+        for g, _ in self.retired:
+            g.close()
+        self.retired = []
+        super().reclaim()
+
+
 def run_isolated(executor, requests: List[Request], keep_state: bool = False) -> List[Result]:
     """Every request alone, back to back (the isolated-run reference for the loop's throughput): set-up, steps,
     result, in turn.  Each Result carries the device time of its steps alone (device_s: CUDA events around the
@@ -323,15 +512,17 @@ def run_isolated(executor, requests: List[Request], keep_state: bool = False) ->
 
 
 def measure_stream(executor, requests: List[Request], rank: int, world: int, gather, budget_bytes: float = 150e9,
-                   saturated: int = 48) -> Dict[str, object]:
+                   saturated: int = 48, scheduler=None) -> Dict[str, object]:
     """The serving measurement on one rank of `world` replicas: rank r serves requests r::world of the stream.
 
     Returns the whole job's figures on every rank: p50/p99 latency from arrival to the result on the host over all
     ranks' requests, the stream's throughput, and the loop's throughput when saturated (the rank's first
     `saturated` requests all arriving at once) against the same requests run alone back to back.  `gather(obj)`
-    returns the list of every rank's obj (all_gather_object under torch.distributed, [obj] alone)."""
+    returns the list of every rank's obj (all_gather_object under torch.distributed, [obj] alone).  `scheduler` is
+    the loop's class (Scheduler, the default, or GroupScheduler with a GroupGpuExecutor)."""
+    scheduler = scheduler or Scheduler
     mine = requests[rank::world]
-    sch = Scheduler(executor, budget_bytes)
+    sch = scheduler(executor, budget_bytes)
     t0 = executor.now()
     res = sch.run(mine)
     wall = executor.now() - t0
@@ -342,7 +533,7 @@ def measure_stream(executor, requests: List[Request], rank: int, world: int, gat
     # excluded), so the ratio compares the loop against the device's throughput on one case at a time
     iso_dev = sum(r.device_s for r in iso) if iso and all(r.device_s is not None for r in iso) else iso_wall
     t0 = executor.now()
-    Scheduler(executor, budget_bytes).run(sub)
+    scheduler(executor, budget_bytes).run(sub)
     sat_wall = executor.now() - t0
     work_sub = float(sum(r.work for r in sub))
     parts = gather({"rids": [r.rid for r in res], "lat": [r.latency for r in res],
@@ -350,7 +541,8 @@ def measure_stream(executor, requests: List[Request], rank: int, world: int, gat
                     "iso": work_sub / iso_dev if iso else 0.0, "iso_wall": work_sub / iso_wall if iso else 0.0,
                     "sat": work_sub / sat_wall if sub else 0.0,
                     "n_sub": len(sub), "finite": all(r.summary.get("finite", 1.0) == 1.0 for r in res),
-                    "peak_active": sch.peak_active, "peak_bytes": sch.peak_bytes})
+                    "peak_active": sch.peak_active, "peak_bytes": sch.peak_bytes,
+                    "peak_group": getattr(sch, "peak_group", 0), "compositions": getattr(sch, "compositions", 0)})
     lat = [x for p in parts for x in p["lat"]]
     rids = sorted(x for p in parts for x in p["rids"])
     iso_thr = sum(p["iso"] for p in parts)
@@ -366,4 +558,5 @@ def measure_stream(executor, requests: List[Request], rank: int, world: int, gat
             "isolated_wall_throughput_cell_steps_per_s": iso_wall_thr,
             "saturated_over_isolated": sat_thr / iso_thr if iso_thr > 0 else None,
             "all_finite": all(p["finite"] for p in parts), "peak_active": max(p["peak_active"] for p in parts),
+            "peak_group": max(p["peak_group"] for p in parts), "group_compositions": sum(p["compositions"] for p in parts),
             "peak_admitted_bytes": max(p["peak_bytes"] for p in parts), "admission_budget_bytes": budget_bytes}

@@ -299,6 +299,35 @@ int dfdm_kernel_bytes(dfdm_ctx *ctx, int which, double *bytes);
 /* Number of the library's own kernels enqueued by this context so far (graph replays included). */
 int dfdm_launch_count(dfdm_ctx *ctx, long long *count);
 
+/* ---- serving groups (no counterpart in the reference) ----
+ * A host that serves many small cases on one GPU steps them one context at a time: per FP32 step a context enqueues
+ * 19 to 22 kernels, and on a 32^3 to 64^3 grid each kernel fills a few SMs for a few microseconds, so the GPU idles
+ * between launches however many streams run beside each other.  A group steps several contexts together: every
+ * kernel family of the step (stage kernel, div + forward x transform, z transforms, y solve, inverse x transform,
+ * stage-3 correction, constant-flux shift) is ONE launch for all members, whose blocks find their case in a job table
+ * and run the per-case kernel's code on it (transform families launch once per distinct length), and one group step
+ * is captured once as a CUDA graph.  A member's results do not depend on the other members: a case steps
+ * bit-identically in a group of one and in any mix, on any stream.  Against k dfdm_compute_time_step_rk3 steps of
+ * the same context they agree to FP32 rounding: the grouped kernels are a separate compilation of the per-case
+ * kernels' source, whose scalar multiply-add contractions may differ.
+ *  - Members: FP32-mixed contexts without SGS model, wall model or hybrid advection scheme, with the fused
+ *    corrections on, a fixed time step (no adaptive step or landing target), two-level transform lengths
+ *    (Nx/2, Nz and periodic Ny in {8,16,24,32,48,64,96,128,192,256}), Nx a multiple of 4, and a first step taken
+ *    (dfdm_compute_time_step_rk3 after set_state; the group runs the steady step).  Else DFDM_ERR_UNSUPPORTED or
+ *    DFDM_ERR_INVALID.  A context may belong to several groups; only one may step it at a time.
+ *  - stream: where the group's work runs (NULL: the first member's stream).  group_step_async orders itself after
+ *    the members' earlier work on their own streams and their later work after it, with events (no host wait),
+ *    and advances each member's time by nsteps * dt.  group_synchronize waits for the group's stream.
+ *  - The members must outlive the group's enqueued steps; destroying the group does not wait for them (its graph is
+ *    released when they are done) and leaves the members as they are. */
+typedef struct dfdm_group dfdm_group;
+int dfdm_group_create(dfdm_ctx *const *ctxs, int n, void *stream, dfdm_group **out);
+int dfdm_group_step_async(dfdm_group *group, int nsteps);
+int dfdm_group_synchronize(dfdm_group *group);
+/* Number of the library's kernels the group has enqueued (graph replays included). */
+int dfdm_group_launch_count(dfdm_group *group, long long *count);
+int dfdm_group_destroy(dfdm_group *group);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,7 +29,28 @@ def test_results_alone_equal_results_in_the_mix(seed, grids, n):
         assert a.summary["kinetic_energy"] == b.summary["kinetic_energy"]
 
 
-@pytest.mark.parametrize("name,prec", [("chan180", "fp32"), ("chan180", "fp64"), ("tgv64", "fp32"), ("les395", "fp32")])
+@pytest.mark.parametrize("seed,grids,n", [(21, (32, 48), 8), (1, (48, 64, 96, 128), 10)])
+def test_grouped_loop_results_alone_equal_results_in_the_mix(seed, grids, n):
+    """The grouped loop: each case steps inside serving groups whose composition changes as cases join and finish;
+    every result is bit-identical to the case alone (a group of one) and agrees with the per-context loop to FP32
+    rounding."""
+    reqs = serve.make_stream(n, rate=200.0, seed=seed, grids=grids, steps=(20, 60))
+    ex = serve.GroupGpuExecutor()
+    mix = serve.GroupScheduler(ex, 150e9, chunk_cell_steps=2e5, keep_state=True)
+    got = mix.run(reqs)
+    assert mix.peak_group > 1 and mix.compositions > 2
+    alone = serve.run_isolated(serve.GroupGpuExecutor(), reqs, keep_state=True)
+    per_ctx = serve.run_isolated(serve.GpuExecutor(), reqs, keep_state=True)
+    assert [r.rid for r in got] == [r.rid for r in alone] == [r.rid for r in per_ctx]
+    for a, b, c in zip(got, alone, per_ctx):
+        assert a.summary["finite"] == 1.0
+        for x, y, z in zip(a.state, b.state, c.state):
+            assert np.array_equal(x, y), a.rid
+            assert np.linalg.norm((x - z).ravel()) <= 1e-5 * np.linalg.norm(z.ravel()), a.rid
+        assert a.summary["t"] == c.summary["t"]
+
+
+@pytest.mark.parametrize("name,prec",[("chan180", "fp32"), ("chan180", "fp64"), ("tgv64", "fp32"), ("les395", "fp32")])
 def test_footprint_bounds_the_device_memory_of_a_context(name, prec):
     """Admission relies on dfdm_footprint_bytes being an upper bound of what a stepping context holds."""
     import torch

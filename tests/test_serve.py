@@ -69,6 +69,85 @@ class FakeExecutor:
         return None, {"steps": self.steps[req.rid]}
 
 
+class FakeGroupExecutor(FakeExecutor):
+    """Simulated device for GroupScheduler: first steps and group chunks queue on one device at `rate` cell-steps/s;
+    a group chunk of k steps costs k times the members' cells."""
+
+    def __init__(self, rate=5e9, bytes_per_cell=72.0):
+        super().__init__(rate, bytes_per_cell)
+        self.tokens = []
+        self.chunk_sizes = []
+        self.max_group_inflight = 0
+
+    def idle(self, until_next_arrival):
+        cands = [t["t_done"] for t in self.tokens if t["t_done"] > self.t]
+        if until_next_arrival is not None:
+            cands.append(self.t + max(until_next_arrival, 1e-9))
+        self.t = min(cands) if cands else self.t + 1e-3
+
+    def start(self, req):
+        h = super().start(req)
+        h["nsteps"] = req.nsteps
+        h["joined"] = False
+        return h
+
+    def _run(self, work, group):
+        t0 = max(self.t, self.busy_until)
+        self.busy_until = t0 + work / self.rate
+        tok = {"t_done": self.busy_until, "group": group}
+        self.tokens.append(tok)
+        return tok
+
+    def first_step(self, h):
+        assert not h["joined"] and self.steps[h["rid"]] == 0
+        h["joined"] = True
+        self.steps[h["rid"]] += 1
+        return self._run(h["cells"], False)
+
+    def group_step(self, hs, k):
+        assert k >= 1 and hs
+        for h in hs:
+            assert h["joined"]
+            self.steps[h["rid"]] += k
+            assert self.steps[h["rid"]] <= h["nsteps"]           # never past a member's last step
+        self.chunk_sizes.append(len(hs))
+        tok = self._run(k * sum(h["cells"] for h in hs), True)
+        live = sum(1 for t in self.tokens if t["group"] and t["t_done"] > self.t)
+        self.max_group_inflight = max(self.max_group_inflight, live)
+        return tok
+
+    def done(self, tok):
+        return tok["t_done"] <= self.t
+
+
+def test_group_scheduler_issues_every_step_once_within_budget_in_order():
+    reqs = serve.make_stream(64, 4.0, seed=11, steps=(1, 60))
+    ex = FakeGroupExecutor(rate=1e8)
+    budget = 3 * 128**3 * ex.bpc
+    sch = serve.GroupScheduler(ex, budget, chunk_cell_steps=1e6, depth=2)
+    out = sch.run(reqs)
+    assert [r.rid for r in out] == sorted(r.rid for r in reqs)
+    for r, q in zip(out, sorted(reqs, key=lambda x: x.rid)):
+        assert r.summary["steps"] == q.nsteps                      # first step + group chunks, each step once
+        assert r.finished >= r.admitted >= r.arrival - 1e-12
+    assert sch.peak_bytes <= budget
+    assert ex.started == sorted(ex.started, key=lambda rid: reqs[rid].arrival)
+    assert sch.peak_group > 1 and max(ex.chunk_sizes) == sch.peak_group   # cases step together
+    assert ex.max_group_inflight <= 2                                      # at most `depth` chunks queued
+    assert sch.compositions >= 2
+
+
+def test_group_scheduler_chunk_is_cut_at_the_first_member_to_finish():
+    reqs = [serve.Request(0, serve.serve_case("tgv", 32, 800.0, 1), 50, 0.0),
+            serve.Request(1, serve.serve_case("tgv", 48, 800.0, 2), 9, 0.0),
+            serve.Request(2, serve.serve_case("chan", 32, 0.0, 3), 30, 0.0)]
+    ex = FakeGroupExecutor(rate=1e9)
+    sch = serve.GroupScheduler(ex, 1e12, chunk_cell_steps=1e9)   # chunks limited only by the members' ends
+    out = sch.run(reqs)
+    assert [r.summary["steps"] for r in out] == [50, 9, 30]
+    assert ex.chunk_sizes[:3] == [3, 2, 1]                        # 3 together, then 2 after rid 1, then rid 0 alone
+
+
 def test_stream_is_seeded_and_matches_its_distribution():
     a = serve.make_stream(256, 4.0, seed=5)
     b = serve.make_stream(256, 4.0, seed=5)
