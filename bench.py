@@ -266,11 +266,12 @@ def cpu_baseline(c, seconds):
 # ---------------------------------------------------------------------------------------------------------------
 def serve_bench(args, local, rank, ws, gather):
     """The serving stream (256 requests, Poisson arrivals at 4/s, FP32-mixed, 150 GB admission budget) through the
-    grouped loop (serve.GroupScheduler: every admitted case steps inside one serving group, one grouped launch per
-    kernel family): p50/p99 latency from arrival to the result on the host, and the loop's throughput when saturated
-    against the same requests run alone back to back (device time of each alone, a group of one).  Beside it, the
-    per-context loop (serve.Scheduler: one context, stream and step graph per case) on the same saturated requests.
-    With N ranks each serves requests rank::N of the stream."""
+    grouped loop (serve.GroupScheduler: the admitted cases of each shape class step as one serving group, one grouped
+    launch per kernel family, the classes on streams of their own): p50/p99 latency from arrival to the result on the
+    host, and the loop's throughput when saturated (median of 3 runs) against the same requests run alone back to
+    back (device time of each alone, a group of one).  Beside it, the per-context loop (serve.Scheduler: one context,
+    stream and step graph per case) on the same saturated requests.  With N ranks each serves requests rank::N of
+    the stream."""
     from dfdm import serve
     warm = serve.make_stream(4, 100.0, seed=99, grids=(32, 48), steps=(10, 10))
     gex = serve.GroupGpuExecutor(device=local)
@@ -278,18 +279,15 @@ def serve_bench(args, local, rank, ws, gather):
     reqs = serve.make_stream(args.serve_requests, args.serve_rate, seed=5)
     out = serve.measure_stream(gex, reqs, rank, ws, gather, 150e9, args.serve_saturated, serve.GroupScheduler)
     out.pop("rids")
-    # the per-context loop on the same saturated requests (all arriving at once)
+    # the per-context loop on the same saturated requests (all arriving at once), repeated as the grouped loop's
     pex = serve.GpuExecutor(device=local)
     serve.Scheduler(pex, 150e9).run(warm)
-    mine = reqs[rank::ws][:args.serve_saturated]
-    sub = [serve.Request(r.rid, r.case, r.nsteps, 0.0, r.precision) for r in mine]
-    t0 = pex.now()
-    serve.Scheduler(pex, 150e9).run(sub)
-    wall = pex.now() - t0
-    per = sum(p for p in gather(float(sum(r.work for r in sub)) / wall))
-    out.update({"loop": "grouped (serve.GroupScheduler)", "arrival_rate_per_s": args.serve_rate,
+    runs = serve.saturated_throughput(pex, serve.Scheduler, reqs[rank::ws][:args.serve_saturated], 150e9)
+    per = sum(gather(float(np.median(runs))))
+    out.update({"loop": "grouped per shape class (serve.GroupScheduler)", "arrival_rate_per_s": args.serve_rate,
                 "precision": "fp32-mixed",
                 "per_context_saturated_throughput_cell_steps_per_s": per,
+                "per_context_saturated_runs_cell_steps_per_s": runs,
                 "grouped_over_per_context_saturated": out["saturated_throughput_cell_steps_per_s"] / per,
                 "stream": "seed 5: 50% Taylor-Green (Re log-uniform 400-3200), 50% Re_tau=180 channel domain; "
                           "N^3 cells, N in {32,48,64,96,128}; 200-2000 steps"})

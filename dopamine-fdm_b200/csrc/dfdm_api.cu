@@ -1373,6 +1373,13 @@ int dfdm_destroy(dfdm_ctx *c) {
     return DFDM_OK;
 }
 
+int dfdm_get_stream(dfdm_ctx *c, void **s) {
+    if (int rc = check_ctx(c)) return rc;
+    if (!s) return fail(DFDM_ERR_INVALID, "null output");
+    *s = (void *)c->stream;
+    return DFDM_OK;
+}
+
 int dfdm_set_stream(dfdm_ctx *c, void *s) {
     if (int rc = check_ctx(c)) return rc;
     CK(cudaStreamSynchronize(c->stream));
@@ -2489,7 +2496,11 @@ struct dfdm_group {
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
+    bool own_stream = false;               // created by dfdm_group_create (stream argument NULL)
     cudaEvent_t ev = nullptr;              // orders the members' own streams with the group's launches
+    // the branch streams and fork/join events of the step's capture, released once the capture has ended
+    std::vector<cudaStream_t> cap_streams;
+    std::vector<cudaEvent_t> cap_events;
     long long launches = 0, graph_launches = 0;
 };
 
@@ -2527,17 +2538,16 @@ int group_eligible(const dfdm_ctx *c) {
     return DFDM_OK;
 }
 
-// one step of every case of the group (the launch sequence of step_enqueue, family by family across the cases)
-int group_step_enqueue(dfdm_group *g) {
+// one step of the cases `cs` on stream st (the launch sequence of step_enqueue, family by family across the cases)
+int members_step_enqueue(const std::vector<dfdm_ctx *> &cs, cudaStream_t st) {
     typedef Impl<float> I;
     typedef float2 C;
-    cudaStream_t st = g->stream;
     constexpr int NL = I::NL;
     for (int s = 1; s <= 3; ++s) {
         // ---- stage kernels ----
         std::vector<StageJob> stage[2];   // [variant 0 one cell, variant 1 packed]
         const bool corr = s >= 2;
-        for (dfdm_ctx *c : g->cs) {
+        for (dfdm_ctx *c : cs) {
             if (corr) { std::swap(c->us, c->us2); std::swap(c->vs, c->vs2); std::swap(c->wsf, c->ws2); }
             StageJob J;
             // variant 2 is variant 1's arithmetic (the per-case launch falls back to variant 0 without TMA)
@@ -2576,7 +2586,7 @@ int group_step_enqueue(dfdm_group *g) {
         // ---- div u* + forward x, per length ----
         std::map<int, std::vector<FwdXJob>> fx;
         std::map<int, size_t> fx_smem;
-        for (dfdm_ctx *c : g->cs) {
+        for (dfdm_ctx *c : cs) {
             FwdXJob J;
             const long long lines = (long long)c->d.Ny * c->d.Nz;
             J.grid = dim3((unsigned)((lines + c->lx2 - 1) / c->lx2), 1, 1);
@@ -2597,7 +2607,7 @@ int group_step_enqueue(dfdm_group *g) {
         auto col_family = [&](int mode) -> int {
             std::map<int, std::vector<ColJob>> jobs;
             std::map<int, std::pair<int, size_t>> cfg;   // threads, shared bytes
-            for (dfdm_ctx *c : g->cs) {
+            for (dfdm_ctx *c : cs) {
                 if (mode == 2 && !c->yper) continue;
                 ColJob J;
                 const int L = mode == 2 ? c->d.Ny : c->d.Nz;
@@ -2625,7 +2635,7 @@ int group_step_enqueue(dfdm_group *g) {
         {
             std::vector<YJob> yj;
             size_t ysm = 0;
-            for (dfdm_ctx *c : g->cs) {
+            for (dfdm_ctx *c : cs) {
                 if (c->yper) continue;
                 YJob J;
                 J.grid = dim3((unsigned)((c->d.Nxc + 63) / 64), (unsigned)c->d.Nz, 1);
@@ -2640,7 +2650,7 @@ int group_step_enqueue(dfdm_group *g) {
         // ---- inverse x, per length ----
         std::map<int, std::vector<InvXJob>> ix;
         std::map<int, size_t> ix_smem;
-        for (dfdm_ctx *c : g->cs) {
+        for (dfdm_ctx *c : cs) {
             InvXJob J;
             const long long lines = (long long)c->d.Ny * c->d.Nz;
             J.grid = dim3((unsigned)((lines + c->lxi2 - 1) / c->lxi2), 1, 1);
@@ -2659,7 +2669,7 @@ int group_step_enqueue(dfdm_group *g) {
         // ---- stage 3: the correction (+ P); stages 1 and 2 are corrected in the next stage kernel's loader ----
         if (s == 3) {
             std::vector<CorrJob> cj;
-            for (dfdm_ctx *c : g->cs) {
+            for (dfdm_ctx *c : cs) {
                 const bool inc = I::incr_form(c, 3);
                 CorrJob J;
                 const Dims &d = c->d;
@@ -2678,7 +2688,7 @@ int group_step_enqueue(dfdm_group *g) {
     std::vector<BulkJob> bj;
     std::vector<FinalJob> fj;
     std::vector<ShiftJob> sj;
-    for (dfdm_ctx *c : g->cs) {
+    for (dfdm_ctx *c : cs) {
         if (c->prm.flow_forcing_mode != 1) continue;
         BulkJob B;
         B.grid = dim3((unsigned)c->red_blocks, 1, 1);
@@ -2698,6 +2708,50 @@ int group_step_enqueue(dfdm_group *g) {
     if ((rc = launch_groups(fj, [&](const GroupTable<FinalJob> &t, int nb) { kg_bulk_final<<<nb, 256, 0, st>>>(t); }))) return rc;
     if ((rc = launch_groups(sj, [&](const GroupTable<ShiftJob> &t, int nb) { kg_shift<<<nb, 256, 0, st>>>(t); }))) return rc;
     return DFDM_OK;
+}
+
+// A group's cases fall into shape classes: the same stage-kernel form, Nx, Nz and periodic Ny, so that every kernel
+// family of a class is one instantiation, i.e. one launch.  Each class is captured on a branch of its own (forked
+// from the group's stream and joined back), so the classes' launches overlap on the device as independent streams'
+// would, while the cases of a class share their launches.
+int group_step_enqueue(dfdm_group *g) {
+    std::map<std::array<int, 4>, std::vector<dfdm_ctx *>> classes;
+    for (dfdm_ctx *c : g->cs) {
+        const int v = (c->stage_variant == 1 || (c->stage_variant == 2 && c->tma_ok)) ? 1 : 0;
+        classes[{v, c->d.Nx, c->d.Nz, c->yper ? c->d.Ny : -1}].push_back(c);
+    }
+    if (classes.size() == 1) return members_step_enqueue(g->cs, g->stream);
+    cudaEvent_t fork = nullptr;
+    int rc = DFDM_OK;
+    auto check = [&](cudaError_t e, const char *what) {
+        if (!rc && e != cudaSuccess) rc = fail(DFDM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    };
+    check(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "fork event creation");
+    if (fork) g->cap_events.push_back(fork);
+    check(cudaEventRecord(fork, g->stream), "fork event record");
+    for (auto &kv : classes) {
+        if (rc) break;
+        cudaStream_t b = nullptr;
+        cudaEvent_t j = nullptr;
+        check(cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking), "branch stream creation");
+        if (b) g->cap_streams.push_back(b);
+        check(cudaEventCreateWithFlags(&j, cudaEventDisableTiming), "join event creation");
+        if (j) g->cap_events.push_back(j);
+        if (rc) break;
+        check(cudaStreamWaitEvent(b, fork, 0), "branch wait on the fork");
+        if (!rc) rc = members_step_enqueue(kv.second, b);
+        check(cudaEventRecord(j, b), "join event record");
+        check(cudaStreamWaitEvent(g->stream, j, 0), "wait on the join");
+    }
+    if (rc) g_err += " (" + std::to_string(classes.size()) + " shape classes)";
+    return rc;
+}
+
+void release_capture_objects(dfdm_group *g) {
+    for (cudaEvent_t e : g->cap_events) cudaEventDestroy(e);
+    for (cudaStream_t b : g->cap_streams) cudaStreamDestroy(b);
+    g->cap_events.clear();
+    g->cap_streams.clear();
 }
 
 void group_destroy_graph(dfdm_group *g) {
@@ -2750,11 +2804,20 @@ int dfdm_group_create(dfdm_ctx *const *ctxs, int n, void *stream, dfdm_group **o
     }
     dfdm_group *g = new dfdm_group;
     g->cs.assign(ctxs, ctxs + n);
-    g->stream = stream ? (cudaStream_t)stream : ctxs[0]->stream;
     if (int rc = group_attributes(g)) { delete g; return rc; }
     if (cudaEventCreateWithFlags(&g->ev, cudaEventDisableTiming) != cudaSuccess) {
         delete g;
         return fail(DFDM_ERR_CUDA, "event creation failed");
+    }
+    if (stream) {
+        g->stream = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaEventDestroy(g->ev);
+            delete g;
+            return fail(DFDM_ERR_CUDA, "stream creation failed");
+        }
+        g->own_stream = true;
     }
     *out = g;
     return DFDM_OK;
@@ -2781,6 +2844,7 @@ int dfdm_group_step_async(dfdm_group *g, int nsteps) {
             g_launches = before;
             cudaGraph_t gr = nullptr;
             cudaError_t e = cudaStreamEndCapture(g->stream, &gr);
+            release_capture_objects(g);
             if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }
             if (e != cudaSuccess) return fail(DFDM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
             g->graph = gr;
@@ -2802,6 +2866,12 @@ int dfdm_group_synchronize(dfdm_group *g) {
     return DFDM_OK;
 }
 
+int dfdm_group_get_stream(dfdm_group *g, void **stream) {
+    if (!g || !stream) return fail(DFDM_ERR_INVALID, "null argument");
+    *stream = (void *)g->stream;
+    return DFDM_OK;
+}
+
 int dfdm_group_launch_count(dfdm_group *g, long long *count) {
     if (!g || !count) return fail(DFDM_ERR_INVALID, "null argument");
     *count = g->launches;
@@ -2813,6 +2883,7 @@ int dfdm_group_destroy(dfdm_group *g) {
     if (!g) return DFDM_OK;
     group_destroy_graph(g);
     if (g->ev) cudaEventDestroy(g->ev);
+    if (g->own_stream) cudaStreamDestroy(g->stream);   // returns at once; released when its work is done
     delete g;
     return DFDM_OK;
 }

@@ -36,7 +36,8 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_set_fused_correction", "dfdm_get_fused_correction", "dfdm_set_state_async", "dfdm_get_state_async",
            "dfdm_write_box_snapshot", "dfdm_set_landing_times", "dfdm_write_snapshot_ex", "dfdm_get_stage_timing",
            "dfdm_set_sgs_in_tile", "dfdm_get_sgs_in_tile", "dfdm_group_create", "dfdm_group_step_async",
-           "dfdm_group_synchronize", "dfdm_group_launch_count", "dfdm_group_destroy"]
+           "dfdm_group_synchronize", "dfdm_group_launch_count", "dfdm_group_destroy", "dfdm_get_stream",
+           "dfdm_group_get_stream"]
 
 
 class DfdmError(RuntimeError):
@@ -120,6 +121,8 @@ def load(build_if_missing: bool = True):
         "dfdm_group_synchronize": (c_int, [c_void_p]),
         "dfdm_group_launch_count": (c_int, [c_void_p, POINTER(ctypes.c_longlong)]),
         "dfdm_group_destroy": (c_int, [c_void_p]),
+        "dfdm_get_stream": (c_int, [c_void_p, POINTER(c_void_p)]),
+        "dfdm_group_get_stream": (c_int, [c_void_p, POINTER(c_void_p)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -194,6 +197,13 @@ class Solver:
     def synchronize(self):
         _check(load().dfdm_synchronize(self.h))
         self._pending = []
+
+    @property
+    def stream_handle(self) -> int:
+        """The cudaStream_t the context runs on, as an integer (torch.cuda.ExternalStream wraps it)."""
+        v = c_void_p()
+        _check(load().dfdm_get_stream(self.h, ctypes.byref(v)))
+        return int(v.value or 0)
 
     def enable_graphs(self, on: bool = True):
         _check(load().dfdm_enable_graphs(self.h, int(on)))
@@ -452,6 +462,13 @@ class Group:
 
     def synchronize(self) -> None:
         _check(load().dfdm_group_synchronize(self.h))
+
+    @property
+    def stream_handle(self) -> int:
+        """The cudaStream_t the group runs on, as an integer."""
+        v = c_void_p()
+        _check(load().dfdm_group_get_stream(self.h, ctypes.byref(v)))
+        return int(v.value or 0)
 
     def launch_count(self) -> int:
         v = ctypes.c_longlong(0)

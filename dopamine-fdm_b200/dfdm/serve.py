@@ -204,6 +204,11 @@ def summarize(results: List[Result], wall: float) -> Dict[str, float]:
 class GpuExecutor:
     """Executor on one GPU: one dfdm context (CUDA-graph steps) and one CUDA stream per admitted request.
 
+    Each context runs on the non-blocking stream dfdm_create makes for it (wrapped in torch.cuda.ExternalStream for
+    the events); streams from torch's pool would not do, since the pool hands out a fixed set of streams in turn, so
+    that with more cases than the pool holds two contexts would share one stream and a set-up on a worker thread
+    could land inside another context's graph capture.
+
     The host-side initial condition of a request is built on worker threads from the moment it arrives (no device
     memory is touched before admission); at admission another worker creates the context and uploads the state, so
     the loop keeps feeding the device meanwhile.  Finished contexts are kept until reclaim(): releasing device
@@ -225,7 +230,6 @@ class GpuExecutor:
         self.setup_pool = ThreadPoolExecutor(max_workers=workers)
         self.ics: Dict[int, object] = {}
         self.finished: List = []
-        self.streams: List = []     # CUDA streams of released contexts, reused
 
     def now(self) -> float:
         return time.perf_counter()
@@ -239,9 +243,9 @@ class GpuExecutor:
     def prepare(self, req: Request) -> None:
         self.ics[req.rid] = self.ic_pool.submit(cases.initial_condition, req.case)
 
-    def _setup(self, req: Request, ic, st):
+    def _setup(self, req: Request, ic):
         self.torch.cuda.set_device(self.device)
-        s = self.Solver(req.case, req.precision, graphs=self.graphs, stream=st.cuda_stream)
+        s = self.Solver(req.case, req.precision, graphs=self.graphs)
         s.set_state(*ic.result())
         return s
 
@@ -249,8 +253,7 @@ class GpuExecutor:
         if req.rid not in self.ics:
             self.prepare(req)
         ic = self.ics.pop(req.rid)
-        st = self.streams.pop() if self.streams else self.torch.cuda.Stream(device=self.device)
-        return {"fut": self.setup_pool.submit(self._setup, req, ic, st), "s": None, "st": st,
+        return {"fut": self.setup_pool.submit(self._setup, req, ic), "s": None, "st": None,
                 "ev": self.torch.cuda.Event()}
 
     def can_enqueue(self, h) -> bool:
@@ -258,6 +261,7 @@ class GpuExecutor:
             if not h["fut"].done():
                 return False
             h["s"] = h["fut"].result()
+            h["st"] = self.torch.cuda.ExternalStream(h["s"].stream_handle, device=self.device)
         return True
 
     def enqueue(self, h, nsteps: int) -> None:
@@ -287,40 +291,43 @@ class GpuExecutor:
         except Exception:
             summary["finite"] = 0.0
         state = s.get_state() if keep_state else None
-        self.finished.append((s, h["st"]))
+        self.finished.append(s)
         return state, summary
 
     def reclaim(self) -> None:
-        for s, st in self.finished:
+        for s in self.finished:
             s.close()
-            self.streams.append(st)
         self.finished = []
 
 
 class GroupScheduler:
-    """FIFO admission by device footprint, as Scheduler; the admitted cases step TOGETHER, as one serving group.
+    """FIFO admission by device footprint, as Scheduler; the admitted cases step in serving groups.
 
-    A case takes its first step on its own (set-up and the first projection), then joins the group: every chunk of
-    steps is one group step of all joined cases (one grouped launch per kernel family, dfdm_group_create), k steps
-    at a time, k = chunk_cell_steps / (the group's cells), cut at the first member to finish.  The composition
-    changes when a case joins or finishes; the executor keeps one group (one captured graph) per composition.  Up
-    to `depth` chunks are in flight, so the device works on one while the host prepares the next.
+    A case takes its first step on its own (set-up and the first projection), then joins the group of its shape
+    class (grid and boundary type; executor.shape_class): every chunk of a class is one group step of all its joined
+    cases (one grouped launch per kernel family, dfdm_group_create), k steps at a time, k = chunk_cell_steps / (the
+    class's cells), cut at the class's first member to finish.  Each class steps on its own stream with up to `depth`
+    chunks in flight, so classes share the device in cell-steps as the per-context loop's cases do, while the cases
+    of a class share their launches.  by_class=False puts every joined case in one group instead.  A composition
+    changes when a case joins or finishes; the executor keeps one group (one captured graph) per composition.
 
     executor protocol:
       footprint(req) -> bytes        prepare(req)          start(req) -> handle        can_enqueue(handle) -> bool
-      first_step(handle) -> token    group_step([handle], k) -> token                  done(token) -> bool
+      shape_class(handle) -> key     first_step(handle) -> token
+      group_step([handle], k, key) -> token                 done(token) -> bool
       finish(handle, req, keep_state) -> (state, summary)   reclaim()   now()   idle(seconds or None)
       defers_free: bool
     """
 
     def __init__(self, executor, budget_bytes: float, chunk_cell_steps: float = 2.5e7, max_active: int = 256,
-                 keep_state: bool = False, depth: int = 2):
+                 keep_state: bool = False, depth: int = 2, by_class: bool = True):
         self.ex = executor
         self.budget = float(budget_bytes)
         self.chunk_cell_steps = float(chunk_cell_steps)
         self.max_active = int(max_active)
         self.keep_state = keep_state
         self.depth = int(depth)
+        self.by_class = by_class
         self.peak_bytes = 0.0
         self.peak_active = 0
         self.peak_group = 0
@@ -339,11 +346,11 @@ class GroupScheduler:
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         waiting: deque = deque()
         active: List[dict] = []
-        inflight: List[tuple] = []      # (token, [(case, steps)], is a group chunk)
+        inflight: List[tuple] = []      # (token, [(case, steps)], class key or None for a first step)
         results: List[Result] = []
         used = 0.0
         held = 0.0
-        last = None
+        last: Dict[object, tuple] = {}  # class -> its last composition
         start = ex.now() if t0 is None else t0
         while pending or waiting or active:
             now = ex.now() - start
@@ -369,7 +376,7 @@ class GroupScheduler:
             self.peak_bytes = max(self.peak_bytes, used + held)
             self.peak_active = max(self.peak_active, len(active))
             progressed = False
-            # completed chunks (the group's chunks complete in order; first steps on their own streams)
+            # completed chunks (a class's chunks complete in order; first steps on the cases' own streams)
             keep = []
             for item in inflight:
                 if ex.done(item[0]):
@@ -391,18 +398,28 @@ class GroupScheduler:
                     active.remove(a)
                     progressed = True
                 elif not a["joined"] and ex.can_enqueue(a["h"]):
-                    inflight.append((ex.first_step(a["h"]), [(a, 1)], False))
+                    inflight.append((ex.first_step(a["h"]), [(a, 1)], None))
                     a["done"] = 1
                     a["joined"] = True
+                    a["class"] = ex.shape_class(a["h"]) if self.by_class else 0
                     progressed = True
-            members = [a for a in active if a["joined"] and a["done"] < a["req"].nsteps]
-            if members and sum(1 for item in inflight if item[2]) < self.depth:
+            classes: Dict[object, List[dict]] = {}
+            for a in active:
+                if a["joined"] and a["done"] < a["req"].nsteps:
+                    classes.setdefault(a["class"], []).append(a)
+            busy: Dict[object, int] = {}
+            for item in inflight:
+                if item[2] is not None:
+                    busy[item[2]] = busy.get(item[2], 0) + 1
+            for key, members in classes.items():
+                if busy.get(key, 0) >= self.depth:
+                    continue
                 k = self.chunk(members)
-                key = tuple(a["req"].rid for a in members)
-                if key != last:
+                comp = tuple(a["req"].rid for a in members)
+                if last.get(key) != comp:
                     self.compositions += 1
-                    last = key
-                inflight.append((ex.group_step([a["h"] for a in members], k), [(a, k) for a in members], True))
+                    last[key] = comp
+                inflight.append((ex.group_step([a["h"] for a in members], k, key), [(a, k) for a in members], key))
                 for a in members:
                     a["done"] += k
                 self.chunks += 1
@@ -417,8 +434,8 @@ class GroupScheduler:
 
 class GroupGpuExecutor(GpuExecutor):
     """GroupScheduler's executor on one GPU: one dfdm context and CUDA stream per admitted case (set-up, first step
-    and the result transfer run there), and the group steps on one stream of their own, with one dfdm group (one
-    captured graph per group step) per composition, kept while the composition lasts.
+    and the result transfer run there); each shape class steps in one dfdm group per composition (one captured graph
+    per group step, on the group's own stream), kept while the composition lasts.
 
     The same object runs run_isolated: a case alone is a group of one on the case's own stream, so every result is
     bit-identical alone and in any mix."""
@@ -427,29 +444,31 @@ class GroupGpuExecutor(GpuExecutor):
         super().__init__(device=device, graphs=False, workers=workers)
         from .native import Group
         self.Group = Group
-        self.gstream = self.torch.cuda.Stream(device=device)
-        self.groups: Dict[tuple, object] = {}
-        self.retired: List[tuple] = []     # (group, event of its last chunk)
+        self.groups: Dict[object, tuple] = {}       # class -> (composition, group, its stream)
+        self.retired: List[tuple] = []              # (group, event after its last chunk)
 
     def _event(self, stream):
         ev = self.torch.cuda.Event()
         ev.record(stream)
         return ev
 
+    def shape_class(self, h):
+        c = h["s"].case
+        return (c.nx, c.ny, c.nz, c.y_bc_type)
+
     def first_step(self, h):
         self.can_enqueue(h)
         h["s"].compute_time_step_RK3_async(1)
         return self._event(h["st"])
 
-    def _group(self, hs):
-        key = tuple(id(h) for h in hs)
-        g = self.groups.get(key)
-        if g is None:
-            # compositions not in use any more are released once their last chunk is done
-            for k2 in list(self.groups):
-                self.retired.append((self.groups.pop(k2), self._event(self.gstream)))
-            g = self.Group([h["s"] for h in hs], stream=self.gstream.cuda_stream)
-            self.groups[key] = g
+    def _group(self, hs, key):
+        comp = tuple(id(h) for h in hs)
+        cur = self.groups.get(key)
+        if cur is None or cur[0] != comp:
+            if cur is not None:   # released once its last chunk is done
+                self.retired.append((cur[1], self._event(cur[2])))
+            g = self.Group([h["s"] for h in hs])
+            cur = self.groups[key] = (comp, g, self.torch.cuda.ExternalStream(g.stream_handle, device=self.device))
         still = []
         for gr, ev in self.retired:
             if ev.query():
@@ -457,11 +476,12 @@ class GroupGpuExecutor(GpuExecutor):
             else:
                 still.append((gr, ev))
         self.retired = still
-        return g
+        return cur[1], cur[2]
 
-    def group_step(self, hs, k: int):
-        self._group(hs).step_async(k)
-        return self._event(self.gstream)
+    def group_step(self, hs, k: int, key=0):
+        g, st = self._group(hs, key)
+        g.step_async(k)
+        return self._event(st)
 
     def done(self, token) -> bool:
         return token.query()
@@ -479,7 +499,7 @@ class GroupGpuExecutor(GpuExecutor):
 
     def reclaim(self) -> None:
         for key in list(self.groups):
-            self.groups.pop(key).close()
+            self.groups.pop(key)[1].close()
         for g, _ in self.retired:
             g.close()
         self.retired = []
@@ -511,15 +531,30 @@ def run_isolated(executor, requests: List[Request], keep_state: bool = False) ->
     return out
 
 
+def saturated_throughput(executor, scheduler, requests: List[Request], budget_bytes: float = 150e9,
+                         reps: int = 3) -> List[float]:
+    """Cell-steps/s of the loop with every request arriving at once, `reps` times (wall clock of each run)."""
+    sub = [Request(r.rid, r.case, r.nsteps, 0.0, r.precision) for r in requests]
+    work = float(sum(r.work for r in sub))
+    out = []
+    for _ in range(reps):
+        t0 = executor.now()
+        scheduler(executor, budget_bytes).run(sub)
+        out.append(work / (executor.now() - t0))
+    return out
+
+
 def measure_stream(executor, requests: List[Request], rank: int, world: int, gather, budget_bytes: float = 150e9,
-                   saturated: int = 48, scheduler=None) -> Dict[str, object]:
+                   saturated: int = 48, scheduler=None, reps: int = 3) -> Dict[str, object]:
     """The serving measurement on one rank of `world` replicas: rank r serves requests r::world of the stream.
 
     Returns the whole job's figures on every rank: p50/p99 latency from arrival to the result on the host over all
     ranks' requests, the stream's throughput, and the loop's throughput when saturated (the rank's first
     `saturated` requests all arriving at once) against the same requests run alone back to back.  `gather(obj)`
     returns the list of every rank's obj (all_gather_object under torch.distributed, [obj] alone).  `scheduler` is
-    the loop's class (Scheduler, the default, or GroupScheduler with a GroupGpuExecutor)."""
+    the loop's class (Scheduler, the default, or GroupScheduler with a GroupGpuExecutor).  The saturated run is
+    repeated `reps` times and its median reported: its wall time varies by some 20% from run to run with the order in
+    which the cases' set-ups complete."""
     scheduler = scheduler or Scheduler
     mine = requests[rank::world]
     sch = scheduler(executor, budget_bytes)
@@ -532,14 +567,12 @@ def measure_stream(executor, requests: List[Request], rank: int, world: int, gat
     # the isolated reference is the device time of each request's steps alone (set-up, uploads and results
     # excluded), so the ratio compares the loop against the device's throughput on one case at a time
     iso_dev = sum(r.device_s for r in iso) if iso and all(r.device_s is not None for r in iso) else iso_wall
-    t0 = executor.now()
-    scheduler(executor, budget_bytes).run(sub)
-    sat_wall = executor.now() - t0
+    sat_runs = saturated_throughput(executor, scheduler, sub, budget_bytes, reps) if sub else [0.0]
     work_sub = float(sum(r.work for r in sub))
     parts = gather({"rids": [r.rid for r in res], "lat": [r.latency for r in res],
                     "work": float(sum(r.work for r in mine)), "wall": wall,
                     "iso": work_sub / iso_dev if iso else 0.0, "iso_wall": work_sub / iso_wall if iso else 0.0,
-                    "sat": work_sub / sat_wall if sub else 0.0,
+                    "sat": float(np.median(sat_runs)), "sat_runs": sat_runs,
                     "n_sub": len(sub), "finite": all(r.summary.get("finite", 1.0) == 1.0 for r in res),
                     "peak_active": sch.peak_active, "peak_bytes": sch.peak_bytes,
                     "peak_group": getattr(sch, "peak_group", 0), "compositions": getattr(sch, "compositions", 0)})
@@ -553,6 +586,7 @@ def measure_stream(executor, requests: List[Request], rank: int, world: int, gat
             "p99_latency_s": percentile(lat, 99), "max_latency_s": max(lat) if lat else None,
             "stream_wall_s": wall_max, "stream_throughput_cell_steps_per_s": sum(p["work"] for p in parts) / wall_max,
             "saturated_requests": sum(p["n_sub"] for p in parts), "saturated_throughput_cell_steps_per_s": sat_thr,
+            "saturated_runs_cell_steps_per_s": [sum(x) for x in zip(*[p["sat_runs"] for p in parts])],
             "isolated_throughput_cell_steps_per_s": iso_thr,
             "isolated_basis": "device time of each request's steps alone (CUDA events; set-up, transfers excluded)",
             "isolated_wall_throughput_cell_steps_per_s": iso_wall_thr,

@@ -102,6 +102,8 @@ int dfdm_footprint_bytes(const dfdm_grid *grid, const dfdm_params *params, size_
 /* Run the context's work on an externally owned CUDA stream (cudaStream_t passed as void*); NULL restores the
  * context's own stream. */
 int dfdm_set_stream(dfdm_ctx *ctx, void *cuda_stream);
+/* The stream the context's work runs on (its own, created non-blocking by dfdm_create, or the one set). */
+int dfdm_get_stream(dfdm_ctx *ctx, void **cuda_stream);
 int dfdm_synchronize(dfdm_ctx *ctx);   /* waits for the context's stream and its copy streams */
 
 /* ---- state transfer: the reference's U, V, W, P, nu_t module arrays (src/global.f90:139,300) ----
@@ -302,11 +304,12 @@ int dfdm_launch_count(dfdm_ctx *ctx, long long *count);
 /* ---- serving groups (no counterpart in the reference) ----
  * A host that serves many small cases on one GPU steps them one context at a time: per FP32 step a context enqueues
  * 19 to 22 kernels, and on a 32^3 to 64^3 grid each kernel fills a few SMs for a few microseconds, so the GPU idles
- * between launches however many streams run beside each other.  A group steps several contexts together: every
- * kernel family of the step (stage kernel, div + forward x transform, z transforms, y solve, inverse x transform,
- * stage-3 correction, constant-flux shift) is ONE launch for all members, whose blocks find their case in a job table
- * and run the per-case kernel's code on it (transform families launch once per distinct length), and one group step
- * is captured once as a CUDA graph.  A member's results do not depend on the other members: a case steps
+ * between launches however many streams run beside each other.  A group steps several contexts together.  Its
+ * members fall into shape classes (stage-kernel form, Nx, Nz, periodic Ny); within a class every kernel family of the
+ * step (stage kernel, div + forward x transform, z transforms, y solve or periodic-y transform, inverse x transform,
+ * stage-3 correction, constant-flux sum and shift) is ONE launch for all the class's members, whose blocks find
+ * their case in a job table and run the per-case kernel's code on it.  One group step is captured once as a CUDA
+ * graph, each class on a branch of its own, so that the classes' launches overlap.  A member's results do not depend on the other members: a case steps
  * bit-identically in a group of one and in any mix, on any stream.  Against k dfdm_compute_time_step_rk3 steps of
  * the same context they agree to FP32 rounding: the grouped kernels are a separate compilation of the per-case
  * kernels' source, whose scalar multiply-add contractions may differ.
@@ -315,15 +318,17 @@ int dfdm_launch_count(dfdm_ctx *ctx, long long *count);
  *    (Nx/2, Nz and periodic Ny in {8,16,24,32,48,64,96,128,192,256}), Nx a multiple of 4, and a first step taken
  *    (dfdm_compute_time_step_rk3 after set_state; the group runs the steady step).  Else DFDM_ERR_UNSUPPORTED or
  *    DFDM_ERR_INVALID.  A context may belong to several groups; only one may step it at a time.
- *  - stream: where the group's work runs (NULL: the first member's stream).  group_step_async orders itself after
- *    the members' earlier work on their own streams and their later work after it, with events (no host wait),
- *    and advances each member's time by nsteps * dt.  group_synchronize waits for the group's stream.
+ *  - stream: where the group's work runs; NULL gives the group a non-blocking stream of its own (group_get_stream
+ *    returns it; destroyed with the group).  group_step_async orders itself after the members' earlier work on
+ *    their own streams and their later work after it, with events (no host wait), and advances each member's time
+ *    by nsteps * dt.  group_synchronize waits for the group's stream.
  *  - The members must outlive the group's enqueued steps; destroying the group does not wait for them (its graph is
  *    released when they are done) and leaves the members as they are. */
 typedef struct dfdm_group dfdm_group;
 int dfdm_group_create(dfdm_ctx *const *ctxs, int n, void *stream, dfdm_group **out);
 int dfdm_group_step_async(dfdm_group *group, int nsteps);
 int dfdm_group_synchronize(dfdm_group *group);
+int dfdm_group_get_stream(dfdm_group *group, void **cuda_stream);
 /* Number of the library's kernels the group has enqueued (graph replays included). */
 int dfdm_group_launch_count(dfdm_group *group, long long *count);
 int dfdm_group_destroy(dfdm_group *group);

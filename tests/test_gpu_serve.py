@@ -29,16 +29,19 @@ def test_results_alone_equal_results_in_the_mix(seed, grids, n):
         assert a.summary["kinetic_energy"] == b.summary["kinetic_energy"]
 
 
-@pytest.mark.parametrize("seed,grids,n", [(21, (32, 48), 8), (1, (48, 64, 96, 128), 10)])
-def test_grouped_loop_results_alone_equal_results_in_the_mix(seed, grids, n):
-    """The grouped loop: each case steps inside serving groups whose composition changes as cases join and finish;
-    every result is bit-identical to the case alone (a group of one) and agrees with the per-context loop to FP32
-    rounding."""
+@pytest.mark.parametrize("seed,grids,n,by_class", [(21, (32, 48), 8, True), (1, (48, 64, 96, 128), 10, True),
+                                                   (1, (48, 64, 96, 128), 10, False)])
+def test_grouped_loop_results_alone_equal_results_in_the_mix(seed, grids, n, by_class):
+    """The grouped loop (one group per shape class, or one group for all): each case steps inside serving groups
+    whose composition changes as cases join and finish; every result is bit-identical to the case alone (a group of
+    one) and agrees with the per-context loop to FP32 rounding."""
     reqs = serve.make_stream(n, rate=200.0, seed=seed, grids=grids, steps=(20, 60))
     ex = serve.GroupGpuExecutor()
-    mix = serve.GroupScheduler(ex, 150e9, chunk_cell_steps=2e5, keep_state=True)
+    mix = serve.GroupScheduler(ex, 150e9, chunk_cell_steps=2e5, keep_state=True, by_class=by_class)
     got = mix.run(reqs)
-    assert mix.peak_group > 1 and mix.compositions > 2
+    assert mix.compositions > 2
+    if not by_class:
+        assert mix.peak_group > 1
     alone = serve.run_isolated(serve.GroupGpuExecutor(), reqs, keep_state=True)
     per_ctx = serve.run_isolated(serve.GpuExecutor(), reqs, keep_state=True)
     assert [r.rid for r in got] == [r.rid for r in alone] == [r.rid for r in per_ctx]

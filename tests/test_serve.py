@@ -77,7 +77,9 @@ class FakeGroupExecutor(FakeExecutor):
         super().__init__(rate, bytes_per_cell)
         self.tokens = []
         self.chunk_sizes = []
+        self.chunk_keys = []
         self.max_group_inflight = 0
+        self.by_class = True
 
     def idle(self, until_next_arrival):
         cands = [t["t_done"] for t in self.tokens if t["t_done"] > self.t]
@@ -98,21 +100,27 @@ class FakeGroupExecutor(FakeExecutor):
         self.tokens.append(tok)
         return tok
 
+    def shape_class(self, h):
+        return h["cells"]
+
     def first_step(self, h):
         assert not h["joined"] and self.steps[h["rid"]] == 0
         h["joined"] = True
         self.steps[h["rid"]] += 1
         return self._run(h["cells"], False)
 
-    def group_step(self, hs, k):
+    def group_step(self, hs, k, key=0):
         assert k >= 1 and hs
         for h in hs:
             assert h["joined"]
+            assert self.by_class is False or h["cells"] == key      # one shape class per group
             self.steps[h["rid"]] += k
             assert self.steps[h["rid"]] <= h["nsteps"]           # never past a member's last step
         self.chunk_sizes.append(len(hs))
+        self.chunk_keys.append(key)
         tok = self._run(k * sum(h["cells"] for h in hs), True)
-        live = sum(1 for t in self.tokens if t["group"] and t["t_done"] > self.t)
+        tok["key"] = key
+        live = sum(1 for t in self.tokens if t["group"] and t.get("key") == key and t["t_done"] > self.t)
         self.max_group_inflight = max(self.max_group_inflight, live)
         return tok
 
@@ -120,11 +128,13 @@ class FakeGroupExecutor(FakeExecutor):
         return tok["t_done"] <= self.t
 
 
-def test_group_scheduler_issues_every_step_once_within_budget_in_order():
+@pytest.mark.parametrize("by_class", [True, False])
+def test_group_scheduler_issues_every_step_once_within_budget_in_order(by_class):
     reqs = serve.make_stream(64, 4.0, seed=11, steps=(1, 60))
     ex = FakeGroupExecutor(rate=1e8)
+    ex.by_class = by_class
     budget = 3 * 128**3 * ex.bpc
-    sch = serve.GroupScheduler(ex, budget, chunk_cell_steps=1e6, depth=2)
+    sch = serve.GroupScheduler(ex, budget, chunk_cell_steps=1e6, depth=2, by_class=by_class)
     out = sch.run(reqs)
     assert [r.rid for r in out] == sorted(r.rid for r in reqs)
     for r, q in zip(out, sorted(reqs, key=lambda x: x.rid)):
@@ -133,19 +143,22 @@ def test_group_scheduler_issues_every_step_once_within_budget_in_order():
     assert sch.peak_bytes <= budget
     assert ex.started == sorted(ex.started, key=lambda rid: reqs[rid].arrival)
     assert sch.peak_group > 1 and max(ex.chunk_sizes) == sch.peak_group   # cases step together
-    assert ex.max_group_inflight <= 2                                      # at most `depth` chunks queued
+    assert ex.max_group_inflight <= 2                                      # at most `depth` chunks per class queued
     assert sch.compositions >= 2
 
 
 def test_group_scheduler_chunk_is_cut_at_the_first_member_to_finish():
     reqs = [serve.Request(0, serve.serve_case("tgv", 32, 800.0, 1), 50, 0.0),
-            serve.Request(1, serve.serve_case("tgv", 48, 800.0, 2), 9, 0.0),
-            serve.Request(2, serve.serve_case("chan", 32, 0.0, 3), 30, 0.0)]
+            serve.Request(1, serve.serve_case("tgv", 32, 900.0, 2), 9, 0.0),
+            serve.Request(2, serve.serve_case("tgv", 32, 1000.0, 3), 30, 0.0),
+            serve.Request(3, serve.serve_case("chan", 48, 0.0, 4), 20, 0.0)]
     ex = FakeGroupExecutor(rate=1e9)
     sch = serve.GroupScheduler(ex, 1e12, chunk_cell_steps=1e9)   # chunks limited only by the members' ends
     out = sch.run(reqs)
-    assert [r.summary["steps"] for r in out] == [50, 9, 30]
-    assert ex.chunk_sizes[:3] == [3, 2, 1]                        # 3 together, then 2 after rid 1, then rid 0 alone
+    assert [r.summary["steps"] for r in out] == [50, 9, 30, 20]
+    sizes = [n for n, key in zip(ex.chunk_sizes, ex.chunk_keys) if key == 32**3]
+    assert sizes == [3, 2, 1]                     # the 32^3 class: 3 together, then 2 after rid 1, then rid 0 alone
+    assert [n for n, key in zip(ex.chunk_sizes, ex.chunk_keys) if key == 48**3] == [1]
 
 
 def test_stream_is_seeded_and_matches_its_distribution():
