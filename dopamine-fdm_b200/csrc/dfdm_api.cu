@@ -167,6 +167,7 @@ struct dfdm_ctx {
     size_t smem_x = 0, smem_z = 0, smem_y = 0;
     // two-level register transforms (fft_reg.cuh) where the length has a split; Stockham otherwise
     bool x2 = false, z2 = false, y2 = false;
+    bool ys3 = false;                           // walls in y: the staged-column y solve (k_ysolve3) fits
     int lx2 = 1, lxi2 = 1, thr_z2 = 256, thr_y2 = 256;   // x lines per block: forward, inverse
     size_t smem_x2 = 0, smem_xi2 = 0, smem_z2 = 0, smem_y2 = 0;
     cudaStream_t own_stream = nullptr, stream = nullptr;
@@ -441,13 +442,29 @@ template <typename T> struct Impl {
         c->smem_y = 2 * (size_t)d.Ny * c->tzx * sizeof(C);
         size_t maxs = std::max(c->smem_x, std::max(c->smem_z, c->smem_y));
         if (maxs > 227 * 1024) return fail(DFDM_ERR_UNSUPPORTED, "grid too large for the shared-memory transforms");
-        CK(cudaFuncSetAttribute(k_fwd_x<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_x));
-        CK(cudaFuncSetAttribute(k_fwd_x<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_x));
-        CK(cudaFuncSetAttribute(k_inv_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_x));
-        int cs = (int)std::max(c->smem_z, c->smem_y);
-        CK(cudaFuncSetAttribute(k_col_fft<T, 0, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs));
-        CK(cudaFuncSetAttribute(k_col_fft<T, 1, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs));
-        CK(cudaFuncSetAttribute(k_col_fft<T, 2, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs));
+        // The dynamic shared-memory cap is an attribute of the kernel for the whole process, not of a launch: for
+        // kernels whose shared memory depends on the grid it is set to the device's opt-in maximum, so that a
+        // context of a smaller grid cannot lower it under a larger context's launches (or its captured graphs).
+        int optin = 0, dev0 = 0;
+        CK(cudaGetDevice(&dev0));
+        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev0));
+        CK(cudaFuncSetAttribute(k_fwd_x<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        CK(cudaFuncSetAttribute(k_fwd_x<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        CK(cudaFuncSetAttribute(k_inv_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        CK(cudaFuncSetAttribute(k_col_fft<T, 0, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        CK(cudaFuncSetAttribute(k_col_fft<T, 1, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        CK(cudaFuncSetAttribute(k_col_fft<T, 2, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        // the staged-column y solve where at least three of its blocks fit on an SM: with fewer, too few columns
+        // sweep at a time (measured at Ny = 192, FP32: 101 us against 42 us for k_ysolve2; at Ny = 96 and 64 it
+        // is 15-30 % faster than k_ysolve2)
+        c->ys3 = false;
+        if (!d.yper && ysolve3_smem<T>(d.Ny) <= (size_t)optin) {
+            const int ysm = (int)ysolve3_smem<T>(d.Ny);
+            CK(cudaFuncSetAttribute(k_ysolve3<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+            int ys_occ = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ys_occ, k_ysolve3<T>, YS_COLS, ysm));
+            c->ys3 = ys_occ >= 3;
+        }
         int dev = 0, nsm = 148, occ = 1;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -803,6 +820,10 @@ template <typename T> struct Impl {
             } else if (d.yper) {
                 dim3 g((d.Nxc + c->tzx - 1) / c->tzx, d.Nz);
                 k_col_fft<T, 2, CT><<<g, 256, c->smem_y, st>>>(d, (C *)c->spec, c->plan_y, (const C *)c->tw_y, c->d_kxx, c->d_kyy, c->d_kzz);
+            } else if (c->ys3) {
+                const int ncol = d.Nxc * d.Nz;
+                k_ysolve3<T><<<(ncol + YS_COLS - 1) / YS_COLS, YS_COLS, ysolve3_smem<T>(d.Ny), st>>>(
+                    d, (C *)c->spec, c->d_rpiv, c->d_lo, c->d_up);
             } else {
                 dim3 g((d.Nxc + 63) / 64, d.Nz);
                 k_ysolve2<T, sizeof(T) == 4 ? 16 : 8><<<g, 64, 2 * d.Ny * sizeof(double), st>>>(d, (C *)c->spec, c->d_rpiv, c->d_lo, c->d_up);
@@ -2534,6 +2555,8 @@ int group_eligible(const dfdm_ctx *c) {
     if (c->dev_dt()) return fail(DFDM_ERR_UNSUPPORTED, "serving groups take a fixed time step");
     if (!c->x2 || !c->z2 || (c->yper && !c->y2)) return fail(DFDM_ERR_UNSUPPORTED, "serving groups need two-level transform lengths");
     if (c->d.Nx % 4 != 0) return fail(DFDM_ERR_UNSUPPORTED, "serving groups need Nx a multiple of 4");
+    if (!c->yper && ysolve3_smem<float>(c->d.Ny) > 227 * 1024)
+        return fail(DFDM_ERR_UNSUPPORTED, "serving groups need Ny <= 440 with walls");
     if (!c->projected) return fail(DFDM_ERR_INVALID, "take a context's first step before it joins a group");
     return DFDM_OK;
 }
@@ -2638,12 +2661,12 @@ int members_step_enqueue(const std::vector<dfdm_ctx *> &cs, cudaStream_t st) {
             for (dfdm_ctx *c : cs) {
                 if (c->yper) continue;
                 YJob J;
-                J.grid = dim3((unsigned)((c->d.Nxc + 63) / 64), (unsigned)c->d.Nz, 1);
+                J.grid = dim3((unsigned)((c->d.Nxc * c->d.Nz + YS_COLS - 1) / YS_COLS), 1, 1);
                 J.d = c->d; J.spec = (C *)c->spec; J.rpiv = c->d_rpiv; J.lo = c->d_lo; J.up = c->d_up;
                 yj.push_back(J);
-                ysm = std::max(ysm, (size_t)2 * c->d.Ny * sizeof(double));
+                ysm = std::max(ysm, ysolve3_smem<float>(c->d.Ny));
             }
-            if ((rc = launch_groups(yj, [&](const GroupTable<YJob> &t, int nb) { kg_ysolve<<<nb, 64, ysm, st>>>(t); }))) return rc;
+            if ((rc = launch_groups(yj, [&](const GroupTable<YJob> &t, int nb) { kg_ysolve<<<nb, YS_COLS, ysm, st>>>(t); }))) return rc;
         }
         if ((rc = col_family(2))) return rc;
         if ((rc = col_family(1))) return rc;
@@ -2767,6 +2790,12 @@ int group_attributes(dfdm_group *g) {
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         if (e != cudaSuccess) rc = fail(DFDM_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
     };
+    // the grouped y solve's shared memory depends on the members' Ny: its cap is the device's opt-in maximum (the
+    // attribute holds for the whole process; a group of smaller grids must not lower it under another's launches)
+    int optin = 0, dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+        return fail(DFDM_ERR_CUDA, "device attribute query failed");
+    setattr((const void *)kg_ysolve, (size_t)optin);
     for (dfdm_ctx *c : g->cs) {
         with_fft2l(c->d.Nx / 2, [&](auto n) {
             constexpr int M = decltype(n)::value;

@@ -117,17 +117,17 @@ __global__ void __launch_bounds__(256) kg_col(const __grid_constant__ GroupTable
 #undef DFDM_BLOCK_IDX
 }
 
-// ---- wall-bounded y solve ----
+// ---- wall-bounded y solve: YS_COLS columns of the flattened (kz, kx) index per block (k_ysolve3) ----
 struct YJob {
     dim3 grid;
     Dims d;
     float2 *spec;
     const double *rpiv, *lo, *up;
 };
-__global__ void __launch_bounds__(64) kg_ysolve(const __grid_constant__ GroupTable<YJob> g) {
+__global__ void __launch_bounds__(YS_COLS) kg_ysolve(const __grid_constant__ GroupTable<YJob> g) {
     const int j = group_job(g.start, g.njobs, blockIdx.x);
     const YJob &J = g.jobs[j];
-    k_ysolve2_body<float, 16>(at(g, j), J.d, J.spec, J.rpiv, J.lo, J.up);
+    k_ysolve3_body<float>(at(g, j), J.d, J.spec, J.rpiv, J.lo, J.up);
 }
 
 // ---- inverse x transform ----

@@ -239,6 +239,81 @@ __global__ void __launch_bounds__(64) k_ysolve2(Dims d, typename cplx_t<T>::type
     k_ysolve2_body<T, CH>(HwBlock(), d, spec, rpiv, lo, up);
 }
 
+// The same solve with whole columns staged in shared memory.  k_ysolve2's sweeps wait for one HBM latency per chunk
+// of CH rows (2 n / CH waits per column), with too few columns per SM to hide them, and write b' to global memory
+// and read it back.  Here a block owns YS_COLS
+// consecutive columns of the flattened (kz, kx) index, one thread each; it issues the cp.async copies of all n rows
+// of its columns' spectrum and pivots at once (one latency per block), runs both recurrences from shared memory
+// (b' rounded to the storage type in place, as k_ysolve2 stores it) and writes each row of x once.  The arithmetic
+// is k_ysolve2's, operation for operation.  Shared memory: n * YS_COLS * (sizeof(C) + 8) + 16 n bytes, so that only
+// as many columns sweep at once on an SM as their rows fit: the library uses it where at least three blocks fit
+// (in FP32 up to Ny ~ 140), k_ysolve2 above.  The grouped launch (kernels_group.cuh) always uses it.
+constexpr int YS_COLS = 32;
+template <typename T> __host__ __device__ constexpr size_t ysolve3_smem(int n) {
+    return (size_t)n * YS_COLS * (sizeof(typename cplx_t<T>::type) + sizeof(double)) + (size_t)2 * n * sizeof(double);
+}
+template <typename T, class BC>
+__device__ __forceinline__ void k_ysolve3_body(const BC &bc, const Dims &d, typename cplx_t<T>::type *__restrict__ spec,
+                                                const double *__restrict__ rpiv, const double *__restrict__ lo,
+                                                const double *__restrict__ up) {
+    typedef typename cplx_t<T>::type C;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int Nxc = d.Nxc, n = d.Ny;
+    double *piv = reinterpret_cast<double *>(smem_raw);         // [r * YS_COLS + lane]
+    double *sco = piv + (size_t)n * YS_COLS;                       // DL at [0, n), DU at [n, 2n)
+    C *v = reinterpret_cast<C *>(sco + 2 * n);                     // [r * YS_COLS + lane]
+    const int lane = threadIdx.x;
+    const int c = bc.idx().x * YS_COLS + lane;
+    const bool own = c < Nxc * d.Nz;
+    const int kz = own ? c / Nxc : 0, kx = own ? c - kz * Nxc : 0;
+    C *col = spec + (size_t)kz * n * Nxc + kx;
+    const double *rp = rpiv + (size_t)kz * n * Nxc + kx;
+    if (own) {
+        for (int r = 0; r < n; ++r) {
+            cp_async<sizeof(C)>(v + r * YS_COLS + lane, col + (size_t)r * Nxc);
+            cp_async<8>(piv + r * YS_COLS + lane, rp + (size_t)r * Nxc);
+        }
+    }
+    cp_async_commit();
+    for (int r = lane; r < n; r += YS_COLS) { sco[r] = lo[r]; sco[n + r] = up[r]; }
+    cp_async_wait_all();
+    __syncthreads();
+    if (!own) return;
+    const double *slo = sco, *sup = sco + n;
+    C v0 = v[lane];
+    double br = (double)v0.x, bi = (double)v0.y, rprev = piv[lane];
+#pragma unroll 4
+    for (int r = 1; r < n; ++r) {
+        const C x = v[r * YS_COLS + lane];
+        const double m = slo[r] * rprev;
+        br = (double)x.x - m * br;
+        bi = (double)x.y - m * bi;
+        C o; o.x = (T)br; o.y = (T)bi;
+        v[r * YS_COLS + lane] = o;
+        rprev = piv[r * YS_COLS + lane];
+    }
+    double xr = br * rprev, xi = bi * rprev;
+    {
+        C o; o.x = (T)xr; o.y = (T)xi;
+        col[(size_t)(n - 1) * Nxc] = o;
+    }
+#pragma unroll 4
+    for (int r = n - 2; r >= 0; --r) {
+        const C x = v[r * YS_COLS + lane];
+        const double rv = piv[r * YS_COLS + lane];
+        xr = ((double)x.x - sup[r] * xr) * rv;
+        xi = ((double)x.y - sup[r] * xi) * rv;
+        C o; o.x = (T)xr; o.y = (T)xi;
+        col[(size_t)r * Nxc] = o;
+    }
+}
+template <typename T>
+__global__ void __launch_bounds__(YS_COLS) k_ysolve3(Dims d, typename cplx_t<T>::type *__restrict__ spec,
+                                                     const double *__restrict__ rpiv, const double *__restrict__ lo,
+                                                     const double *__restrict__ up) {
+    k_ysolve3_body<T>(HwBlock(), d, spec, rpiv, lo, up);
+}
+
 // ---- 4. inverse complex-to-real x transform, writes the pseudo-pressure phi ----------------------------------
 //   Z_k = (X_k + conj X_{M-k}) + i (X_k - conj X_{M-k}) conj(W_Nx^k),  z = IFFT_M(Z),  x_2n = Re z_n, x_2n+1 = Im z_n
 // (unnormalised like cufftExecZ2D); the imaginary parts of X_0 and X_M are dropped, as the real part of the

@@ -62,3 +62,25 @@ def test_odd_shapes_fused_equals_separate(c):
             b = _run(c, prec, variant=v, fused=True)
             for key, x, y in zip("UVWP", a, b):
                 assert np.array_equal(x, y), (prec, v, key, float(np.abs(x - y).max()))
+
+
+def test_a_later_context_of_a_smaller_grid_leaves_earlier_launches_valid():
+    """Kernels whose shared memory depends on the grid (the staged y solve, the Stockham transforms) keep their
+    dynamic shared-memory cap at the device maximum: a context created later, on a smaller grid, must not lower it
+    under an earlier context's launches and captured graphs."""
+    import math
+    big = cases.channel(32, 128, 32, 2 * math.pi, math.pi, 2.0, 180.0, 15.6, 1e-3, 7, 0, "chan_ny128")
+    small = cases.channel(32, 24, 32, 2 * math.pi, math.pi, 2.0, 180.0, 15.6, 1e-3, 8, 0, "chan_ny24")
+    ref = _run(big, "fp32", steps=2)
+    for graphs in (False, True):
+        s1 = Solver(big, "fp32", graphs=graphs)
+        s1.set_state(*cases.initial_condition(big))
+        s1.compute_time_step_RK3(1)
+        s2 = Solver(small, "fp32")
+        s2.set_state(*cases.initial_condition(small))
+        s2.compute_time_step_RK3(1)
+        s1.compute_time_step_RK3(1)
+        for x, y in zip(s1.get_state(), ref):
+            assert np.array_equal(x, y)
+        s1.close()
+        s2.close()
