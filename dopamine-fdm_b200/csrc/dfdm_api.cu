@@ -1720,6 +1720,36 @@ int dfdm_set_landing_times(dfdm_ctx *c, int n, const double *t_land) {
 }
 
 // ---- the step ----
+// Programmatic dependent launch in the captured steps: every kernel-to-kernel edge of the graph becomes a
+// programmatic edge (the destination may be scheduled once every block of the source has started, and waits in
+// pdl_enter for the source's completion).  An edge the runtime does not accept as programmatic stays as it was.
+static int make_programmatic(cudaGraph_t g) {
+    size_t n = 0;
+    if (cudaGraphGetEdges_v2(g, nullptr, nullptr, nullptr, &n) != cudaSuccess) { cudaGetLastError(); return DFDM_OK; }
+    std::vector<cudaGraphNode_t> from(n), to(n);
+    std::vector<cudaGraphEdgeData> ed(n);
+    if (n == 0 || cudaGraphGetEdges_v2(g, from.data(), to.data(), ed.data(), &n) != cudaSuccess) {
+        cudaGetLastError();
+        return DFDM_OK;
+    }
+    for (size_t i = 0; i < n; ++i) {
+        cudaGraphNodeType a, b;
+        if (cudaGraphNodeGetType(from[i], &a) != cudaSuccess || cudaGraphNodeGetType(to[i], &b) != cudaSuccess) continue;
+        if (a != cudaGraphNodeTypeKernel || b != cudaGraphNodeTypeKernel || ed[i].type != cudaGraphDependencyTypeDefault)
+            continue;
+        cudaGraphEdgeData pe;
+        std::memset(&pe, 0, sizeof(pe));
+        pe.type = cudaGraphDependencyTypeProgrammatic;
+        pe.from_port = cudaGraphKernelNodePortProgrammatic;
+        CK(cudaGraphRemoveDependencies_v2(g, &from[i], &to[i], &ed[i], 1));
+        if (cudaGraphAddDependencies_v2(g, &from[i], &to[i], &pe, 1) != cudaSuccess) {
+            cudaGetLastError();
+            CK(cudaGraphAddDependencies_v2(g, &from[i], &to[i], &ed[i], 1));
+        }
+    }
+    return DFDM_OK;
+}
+
 static int step_n(dfdm_ctx *c, int nsteps) {
     for (int n = 0; n < nsteps; ++n) {
         double to = c->t;
@@ -1737,6 +1767,7 @@ static int step_n(dfdm_ctx *c, int nsteps) {
                 if (rc) { if (g) cudaGraphDestroy(g); return rc; }
                 if (e != cudaSuccess) return fail(DFDM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
                 c->graph = g;
+                if (int rp = make_programmatic(c->graph)) return rp;
                 CK(cudaGraphInstantiate(&c->gexec, c->graph, 0));
             }
             CK(cudaGraphLaunch(c->gexec, c->stream));
@@ -2877,6 +2908,7 @@ int dfdm_group_step_async(dfdm_group *g, int nsteps) {
             if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }
             if (e != cudaSuccess) return fail(DFDM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
             g->graph = gr;
+            if (int rp = make_programmatic(g->graph)) return rp;
             CK(cudaGraphInstantiate(&g->gexec, g->graph, 0));
         }
         CK(cudaGraphLaunch(g->gexec, g->stream));

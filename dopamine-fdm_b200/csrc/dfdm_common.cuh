@@ -17,6 +17,14 @@
 
 namespace dfdm {
 
+// Programmatic dependent launch.  Every kernel of the library starts with pdl_enter(), which waits until the kernel
+// before it has completed and its memory is visible, before this grid reads or writes anything.  The library turns
+// the kernel-to-kernel edges of its captured graphs into programmatic edges, so the next grid is launched as the
+// blocks of this one exit, without the launch gap of a full dependency; elsewhere (plain stream launches) the wait
+// returns at once.  No kernel triggers its dependents early: blocks of later grids would then wait on SM slots that
+// the running grid needs (measured: 23 % slower steps at 256 x 192 x 256).
+__device__ __forceinline__ void pdl_enter() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
 // Block coordinates of a kernel body.  A per-case kernel passes HwBlock, whose accessors read the hardware registers
 // at each use (the body then compiles as if it named blockIdx / gridDim itself); a grouped launch (kernels_group.cuh)
 // passes JobBlock, the block's coordinates in its own case's grid.

@@ -131,6 +131,7 @@ template <typename T, bool VEC>
 __global__ void __launch_bounds__(256) k_bulk_partial(Dims d, const T *__restrict__ U, const double *__restrict__ dyc,
                                                       const double *__restrict__ dzc, const double *__restrict__ ubd,
                                                       double *__restrict__ part) {
+    pdl_enter();
     k_bulk_partial_body<T, VEC>(HwBlock(), d, U, dyc, dzc, ubd, part);
 }
 
@@ -152,6 +153,7 @@ __device__ __forceinline__ void k_bulk_final_body(const BC &bc, int nparts, cons
 }
 __global__ void __launch_bounds__(256) k_bulk_final(int nparts, const double *__restrict__ part, double Ub_target,
                                                     double *__restrict__ out) {
+    pdl_enter();
     k_bulk_final_body(HwBlock(), nparts, part, Ub_target, out);
 }
 
@@ -177,6 +179,7 @@ __device__ __forceinline__ void k_shift_body(const BC &bc, const Dims &d, T *__r
 }
 template <typename T>
 __global__ void __launch_bounds__(256) k_shift(Dims d, T *__restrict__ U, const double *__restrict__ dU) {
+    pdl_enter();
     k_shift_body<T>(HwBlock(), d, U, dU);
 }
 
@@ -191,6 +194,7 @@ __global__ void __launch_bounds__(256) k_monitor_rows(Dims d, const T *__restric
                                                       const double *__restrict__ dxc, const double *__restrict__ dyc,
                                                       const double *__restrict__ dzc, unsigned long long *__restrict__ out,
                                                       int *__restrict__ flag) {
+    pdl_enter();
     double mdiv = 0.0, mu = 0.0;
     int bad = 0;
     const int rows = d.Ny * d.Nz, Nx = d.Nx, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
@@ -237,6 +241,7 @@ __global__ void __launch_bounds__(256) k_monitor_rows(Dims d, const T *__restric
 // Nx*(Nz+1).  One block, compensated per-thread sums then a fixed tree.
 __global__ void __launch_bounds__(256) k_wall_diag(int Nx, int Nz, const double *__restrict__ tx,
                                                    double *__restrict__ out) {
+    pdl_enter();
     Kahan s, w; s.init(); w.init();
     const int plane = Nx * Nz;
     for (int q = threadIdx.x; q < plane + Nx; q += blockDim.x) {
@@ -253,6 +258,7 @@ __global__ void __launch_bounds__(256) k_wall_diag(int Nx, int Nz, const double 
 __global__ void k_monitor_final(const unsigned long long *__restrict__ bits, const int *__restrict__ flag,
                                 const double *__restrict__ bulk, const double *__restrict__ wsum, int ncol,
                                 const double *__restrict__ dtt, double t_host, double dt_host, double *__restrict__ out) {
+    pdl_enter();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const double dt = dtt ? dtt[2] : dt_host, t = dtt ? dtt[1] : t_host;
     out[0] = t;
@@ -281,6 +287,7 @@ __global__ void __launch_bounds__(256) k_cfl(Dims d, const T *__restrict__ U, co
                                              const T *__restrict__ W, const T *__restrict__ NU,
                                              const double *__restrict__ ubd, double inv_dx, const double *__restrict__ dyc,
                                              const double *__restrict__ dzc, double nu, unsigned long long *__restrict__ out) {
+    pdl_enter();
     typedef Chunk<T> Ch;
     constexpr int NV = Ch::NV;
     double mv = 0.0;
@@ -351,6 +358,7 @@ __global__ void __launch_bounds__(256) k_cfl(Dims d, const T *__restrict__ U, co
 // The step's dt goes to dtt[0] and t advances.
 __global__ void k_select_dt(const unsigned long long *__restrict__ cfl, double *__restrict__ dtt, int adaptive,
                             double cfl_target, double cfl_safety, double dt_min, double dt_max) {
+    pdl_enter();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double dt = dtt[2];
     if (adaptive) {
@@ -374,6 +382,7 @@ __global__ void __launch_bounds__(256) k_ke_partial(Dims d, const T *__restrict_
                                                     const T *__restrict__ W, double dx, const double *__restrict__ dyc,
                                                     const double *__restrict__ dzc, const double *__restrict__ ubd,
                                                     double *__restrict__ part) {
+    pdl_enter();
     Kahan s, w; s.init(); w.init();
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x) {
         int i = (int)(p % d.Nx);
@@ -390,6 +399,7 @@ __global__ void __launch_bounds__(256) k_ke_partial(Dims d, const T *__restrict_
 }
 
 __global__ void k_ratio_final(int nparts, const double *__restrict__ part, double *__restrict__ out) {
+    pdl_enter();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     Kahan s, w; s.init(); w.init();
     for (int b = 0; b < nparts; ++b) { s.add(part[2 * b]); w.add(part[2 * b + 1]); }
@@ -434,6 +444,7 @@ __device__ __forceinline__ long long map_ghost(const Dims &d, int kind, int I, i
 template <typename T>
 __global__ void __launch_bounds__(256) k_pack(Dims d, int kind, int n1, int n2, int n3, const T *__restrict__ f,
                                               const double *__restrict__ ubd, double *__restrict__ out) {
+    pdl_enter();
     long long n = (long long)n1 * n2 * n3;
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
         int I = (int)(p % n1) + 1;
@@ -455,6 +466,7 @@ __global__ void __launch_bounds__(256) k_pack(Dims d, int kind, int n1, int n2, 
 template <typename T>
 __global__ void __launch_bounds__(256) k_unpack(Dims d, int kind, int n1, int n2, const double *__restrict__ in,
                                                 const double *__restrict__ ubd, T *__restrict__ f) {
+    pdl_enter();
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x) {
         int i = (int)(p % d.Nx);
         long long q = p / d.Nx;
@@ -475,6 +487,7 @@ __global__ void __launch_bounds__(256) k_unpack(Dims d, int kind, int n1, int n2
 template <typename T>
 __global__ void __launch_bounds__(256) k_pack_interior(Dims d, int n1, int n2, int n3, const T *__restrict__ f,
                                                        double *__restrict__ out) {
+    pdl_enter();
     long long n = (long long)n1 * n2 * n3;
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
         int i = (int)(p % n1);
@@ -489,6 +502,7 @@ __global__ void __launch_bounds__(256) k_pack_interior(Dims d, int n1, int n2, i
 // Interior rows map to the device planes; the duplicated periodic row repeats row 0 and the ghost rows copy the
 // nearest computed row, as compute_flat_wall_eqwm does (src/wallmodel.f90:515-522, :571-578).
 __global__ void k_pack_tau(Dims d, int is_z, int n1, int n3, const double *__restrict__ t, double *__restrict__ out) {
+    pdl_enter();
     long long n = (long long)n1 * 2 * n3;
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
         int i = (int)(p % n1) - 1;
@@ -508,6 +522,7 @@ __global__ void k_pack_tau(Dims d, int is_z, int n1, int n3, const double *__res
 // Real field in the rhs_p shape (2:nxg, 2:nyg-1, 2:nzg) -> independent centres.
 template <typename T>
 __global__ void __launch_bounds__(256) k_unpack_rhs_p(Dims d, int n1, int n2, const double *__restrict__ in, T *__restrict__ f) {
+    pdl_enter();
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x) {
         int i = (int)(p % d.Nx);
         long long q = p / d.Nx;
@@ -521,6 +536,7 @@ __global__ void __launch_bounds__(256) k_unpack_rhs_p(Dims d, int n1, int n2, co
 // that the reference leaves unset at one rank are written as copies of the next wrap.
 template <typename T>
 __global__ void __launch_bounds__(256) k_pack_rhs_p(Dims d, int n1, int n2, int n3, const T *__restrict__ f, double *__restrict__ out) {
+    pdl_enter();
     long long n = (long long)n1 * n2 * n3;
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
         int i = (int)(p % n1);

@@ -135,6 +135,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_fwd_x2(PoissonA
                                                 typename cplx_t<T>::type *__restrict__ spec,
                                                 const typename cplx_t<T>::type *__restrict__ tw,
                                                 const typename cplx_t<T>::type *__restrict__ twr) {
+    pdl_enter();
     k_fwd_x2_body<T, FROM_DIV, M>(HwBlock(), a, lx, U, V, W, src, spec, tw, twr);
 }
 
@@ -193,6 +194,7 @@ template <typename T, int M>
 __global__ void __launch_bounds__(256) k_inv_x2(PoissonArgs<T> a, int lx, const typename cplx_t<T>::type *__restrict__ spec,
                                                 T *__restrict__ phi, const typename cplx_t<T>::type *__restrict__ tw,
                                                 const typename cplx_t<T>::type *__restrict__ twr) {
+    pdl_enter();
     k_inv_x2_body<T, M>(HwBlock(), a, lx, spec, phi, tw, twr);
 }
 
@@ -204,6 +206,7 @@ __global__ void __launch_bounds__(256) k_col2(Dims d, typename cplx_t<T>::type *
                                               const typename cplx_t<T>::type *__restrict__ tw,
                                               const double *__restrict__ kxx, const double *__restrict__ kyy,
                                               const double *__restrict__ kzz) {
+    pdl_enter();
 #define DFDM_BLOCK_IDX blockIdx
 #include "k_col2_body.inc"
 #undef DFDM_BLOCK_IDX

@@ -62,6 +62,7 @@ struct StageJob {
 };
 template <bool CORR>
 __global__ void __launch_bounds__(256, 2) kg_stage2(const __grid_constant__ GroupTable<StageJob> g) {
+    pdl_enter();
     const int j = group_job(g.start, g.njobs, blockIdx.x);
     const StageJob &J = g.jobs[j];
     k_tiled2_body<false, false, 8, false, CORR>(at(g, j), J.a, J.U, J.V, J.W, J.nu, J.tau_x, J.tau_z, J.sc, J.kc,
@@ -69,6 +70,7 @@ __global__ void __launch_bounds__(256, 2) kg_stage2(const __grid_constant__ Grou
 }
 template <bool CORR>
 __global__ void __launch_bounds__(256, 3) kg_stage1(const __grid_constant__ GroupTable<StageJob> g) {
+    pdl_enter();
     const int j = group_job(g.start, g.njobs, blockIdx.x);
     const StageJob &J = g.jobs[j];
     k_tiled_body<float, false, false, 32, 8, 0, CORR>(at(g, j), J.a, J.U, J.V, J.W, J.nu, J.tau_x, J.tau_z, J.sc,
@@ -88,6 +90,7 @@ struct FwdXJob {
 };
 template <int M>
 __global__ void __launch_bounds__(256, 4) kg_fwd_x(const __grid_constant__ GroupTable<FwdXJob> g) {
+    pdl_enter();
     const int j = group_job(g.start, g.njobs, blockIdx.x);
     const FwdXJob &J = g.jobs[j];
     k_fwd_x2_body<float, true, M>(at(g, j), J.a, J.lx, J.U, J.V, J.W, J.src, J.spec, J.tw, J.twr);
@@ -103,6 +106,7 @@ struct ColJob {
 };
 template <int MODE, int L>
 __global__ void __launch_bounds__(256) kg_col(const __grid_constant__ GroupTable<ColJob> g) {
+    pdl_enter();
     typedef float T;
     constexpr int NL = 16;
     const int j = group_job(g.start, g.njobs, blockIdx.x);
@@ -125,6 +129,7 @@ struct YJob {
     const double *rpiv, *lo, *up;
 };
 __global__ void __launch_bounds__(YS_COLS) kg_ysolve(const __grid_constant__ GroupTable<YJob> g) {
+    pdl_enter();
     const int j = group_job(g.start, g.njobs, blockIdx.x);
     const YJob &J = g.jobs[j];
     k_ysolve3_body<float>(at(g, j), J.d, J.spec, J.rpiv, J.lo, J.up);
@@ -141,6 +146,7 @@ struct InvXJob {
 };
 template <int M>
 __global__ void __launch_bounds__(256) kg_inv_x(const __grid_constant__ GroupTable<InvXJob> g) {
+    pdl_enter();
     const int j = group_job(g.start, g.njobs, blockIdx.x);
     const InvXJob &J = g.jobs[j];
     k_inv_x2_body<float, M>(at(g, j), J.a, J.lx, J.spec, J.phi, J.tw, J.twr);
@@ -155,6 +161,7 @@ struct CorrJob {
     const float *uo, *vo, *wo;
 };
 __global__ void __launch_bounds__(256) kg_correct4(const __grid_constant__ GroupTable<CorrJob> g) {
+    pdl_enter();
     const int j = group_job(g.start, g.njobs, blockIdx.x);
     const CorrJob &J = g.jobs[j];
     k_correct4_body<float>(at(g, j), J.a, J.phi, J.us, J.vs, J.ws, J.U, J.V, J.W, J.P, J.uo, J.vo, J.wo);
@@ -169,6 +176,7 @@ struct BulkJob {
     double *part;
 };
 __global__ void __launch_bounds__(256) kg_bulk_partial(const __grid_constant__ GroupTable<BulkJob> g) {
+    pdl_enter();
     const int j = group_job(g.start, g.njobs, blockIdx.x);
     const BulkJob &J = g.jobs[j];
     k_bulk_partial_body<float, true>(at(g, j), J.d, J.U, J.dyc, J.dzc, J.ubd, J.part);
@@ -181,6 +189,7 @@ struct FinalJob {
     double *out;
 };
 __global__ void __launch_bounds__(256) kg_bulk_final(const __grid_constant__ GroupTable<FinalJob> g) {
+    pdl_enter();
     const int j = group_job(g.start, g.njobs, blockIdx.x);
     const FinalJob &J = g.jobs[j];
     k_bulk_final_body(at(g, j), J.nparts, J.part, J.Ub_target, J.out);
@@ -192,6 +201,7 @@ struct ShiftJob {
     const double *dU;
 };
 __global__ void __launch_bounds__(256) kg_shift(const __grid_constant__ GroupTable<ShiftJob> g) {
+    pdl_enter();
     const int j = group_job(g.start, g.njobs, blockIdx.x);
     const ShiftJob &J = g.jobs[j];
     k_shift_body<float>(at(g, j), J.d, J.U, J.dU);

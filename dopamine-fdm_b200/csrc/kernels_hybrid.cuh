@@ -81,6 +81,7 @@ template <typename T, int ORD, int VW>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (ORD == 5 ? 3 : 4) : (ORD == 5 ? 1 : 2))
     k_adv_hybrid_faces(HybArgs<T> h, int kc, const T *__restrict__ U, const T *__restrict__ V, const T *__restrict__ W,
                        T *__restrict__ out) {
+    pdl_enter();
     constexpr int TX = 32, TY = 8, H = ORD == 5 ? 3 : 2, HX = 4, PX = TX + 2 * HX, PY = TY + 2 * H, PS = PX * PY;
     constexpr int NT = TX * TY, NP = 8;
     // the loader copies VW consecutive x cells at a time (VW = 4 in FP32 when Nx % 4 == 0, else 2): every vector

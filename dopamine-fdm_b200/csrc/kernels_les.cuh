@@ -41,6 +41,7 @@ __global__ void __launch_bounds__(les::NT, 2) k_les(StepArgs<T> a, const T *__re
                                                     T *__restrict__ f1u, T *__restrict__ f1v, T *__restrict__ f1w,
                                                     T *__restrict__ us, T *__restrict__ vs, T *__restrict__ wsf,
                                                     T *__restrict__ nut_out) {
+    pdl_enter();
     using namespace les;
     constexpr int PER = (PS + NT - 1) / NT, PERP = (PSP + NT - 1) / NT;
     extern __shared__ __align__(16) unsigned char smem_raw[];

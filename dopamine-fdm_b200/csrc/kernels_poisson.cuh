@@ -32,6 +32,7 @@ __global__ void __launch_bounds__(256) k_fwd_x(PoissonArgs<T> a, int lx, const T
                                                typename cplx_t<T>::type *__restrict__ spec, FFTPlan p,
                                                const typename cplx_t<T>::type *__restrict__ tw,
                                                const typename cplx_t<T>::type *__restrict__ twr) {
+    pdl_enter();
     typedef typename cplx_t<T>::type C;
     typedef Arith<T> A;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -92,6 +93,7 @@ __global__ void __launch_bounds__(256) k_col_fft(Dims d, typename cplx_t<T>::typ
                                                  const typename cplx_t<T>::type *__restrict__ tw,
                                                  const double *__restrict__ kxx, const double *__restrict__ kyy,
                                                  const double *__restrict__ kzz) {
+    pdl_enter();
     typedef typename cplx_t<T>::type C;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int L = p.n;
@@ -236,6 +238,7 @@ template <typename T, int CH>
 __global__ void __launch_bounds__(64) k_ysolve2(Dims d, typename cplx_t<T>::type *__restrict__ spec,
                                                 const double *__restrict__ rpiv, const double *__restrict__ lo,
                                                 const double *__restrict__ up) {
+    pdl_enter();
     k_ysolve2_body<T, CH>(HwBlock(), d, spec, rpiv, lo, up);
 }
 
@@ -311,6 +314,7 @@ template <typename T>
 __global__ void __launch_bounds__(YS_COLS) k_ysolve3(Dims d, typename cplx_t<T>::type *__restrict__ spec,
                                                      const double *__restrict__ rpiv, const double *__restrict__ lo,
                                                      const double *__restrict__ up) {
+    pdl_enter();
     k_ysolve3_body<T>(HwBlock(), d, spec, rpiv, lo, up);
 }
 
@@ -323,6 +327,7 @@ __global__ void __launch_bounds__(256) k_inv_x(PoissonArgs<T> a, int lx, const t
                                                T *__restrict__ phi, FFTPlan p,
                                                const typename cplx_t<T>::type *__restrict__ tw,
                                                const typename cplx_t<T>::type *__restrict__ twr) {
+    pdl_enter();
     typedef typename cplx_t<T>::type C;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Dims &d = a.d;
@@ -364,6 +369,7 @@ __global__ void __launch_bounds__(256) k_correct(PoissonArgs<T> a, const T *__re
                                                  const T *__restrict__ vs, const T *__restrict__ ws, T *__restrict__ U,
                                                  T *__restrict__ V, T *__restrict__ W, T *__restrict__ P,
                                                  const T *__restrict__ uo, const T *__restrict__ vo, const T *__restrict__ wo) {
+    pdl_enter();
     typedef Arith<T> A;
     const Dims &d = a.d;
     const int Nx = d.Nx, Ny = d.Ny, Nz = d.Nz, plane = Nx * Ny;
@@ -456,6 +462,7 @@ __global__ void __launch_bounds__(256) k_correct4(PoissonArgs<T> a, const T *__r
                                                   const T *__restrict__ vs, const T *__restrict__ ws, T *__restrict__ U,
                                                   T *__restrict__ V, T *__restrict__ W, T *__restrict__ P,
                                                   const T *__restrict__ uo, const T *__restrict__ vo, const T *__restrict__ wo) {
+    pdl_enter();
     k_correct4_body<T>(HwBlock(), a, phi, us, vs, ws, U, V, W, P, uo, vo, wo);
 }
 

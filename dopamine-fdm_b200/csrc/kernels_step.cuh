@@ -144,6 +144,7 @@ struct WallState {
 template <typename T>
 __global__ void k_wm_filter(StepArgs<T> a, WallState ws, const T *__restrict__ U, const T *__restrict__ W, int seed,
                             double dt_fixed, const double *__restrict__ dtp, double Tf_fac) {
+    pdl_enter();
     const Dims &d = a.d;
     const double dt = dtp ? *dtp : dt_fixed;   // adaptive time step: from device memory
     int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
@@ -169,6 +170,7 @@ __global__ void k_wm_filter(StepArgs<T> a, WallState ws, const T *__restrict__ U
 // compute_flat_wall_eqwm (src/wallmodel.f90:442-583), smooth Reichardt law, matching height = first centre.
 template <typename T>
 __global__ void k_wall_model(StepArgs<T> a, WallState ws, const T *__restrict__ U, const T *__restrict__ W, int filter) {
+    pdl_enter();
     const Dims &d = a.d;
     int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
     if (i >= d.Nx) return;
@@ -282,6 +284,7 @@ template <> struct AxisLocal<double> {
 template <typename T, bool CORR>
 __global__ void k_wall_sgs(StepArgs<T> a, const T *__restrict__ U, const T *__restrict__ W, const T *__restrict__ phi,
                            double *__restrict__ wfac) {
+    pdl_enter();
     const Dims &d = a.d;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
     if (i >= d.Nx) return;
@@ -792,6 +795,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) k_tiled(StepAr
                                                   T *__restrict__ wo, T *__restrict__ f1u, T *__restrict__ f1v,
                                                   T *__restrict__ f1w, T *__restrict__ us, T *__restrict__ vs,
                                                   T *__restrict__ wsf, T *__restrict__ rhs_only, T *__restrict__ nut_out) {
+    pdl_enter();
     k_tiled_body<T, LES, WM, TX, TY, KIND, CORR>(HwBlock(), a, U, V, W, NU, tau_x, tau_z, sc, kc, uo, vo, wo, f1u, f1v, f1w, us, vs, wsf, rhs_only, nut_out);
 }
 
@@ -1046,6 +1050,7 @@ __global__ void __launch_bounds__(32 * TY, 512 / (32 * TY)) k_tiled2(StepArgs<fl
                                                    float *__restrict__ wo, float *__restrict__ f1u, float *__restrict__ f1v,
                                                    float *__restrict__ f1w, float *__restrict__ us, float *__restrict__ vs,
                                                    float *__restrict__ wsf, float *__restrict__ rhs_only) {
+    pdl_enter();
     k_tiled2_body<LES, WM, TY, HYB, CORR>(HwBlock(), a, U, V, W, NU, tau_x, tau_z, sc, kc, uo, vo, wo, f1u, f1v, f1w, us, vs, wsf, rhs_only);
 }
 

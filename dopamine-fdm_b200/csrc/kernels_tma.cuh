@@ -100,6 +100,7 @@ __global__ void __launch_bounds__(256, 2) k_tma2(StepArgs<float> a, const __grid
                                                  float *__restrict__ f1w, float *__restrict__ us, float *__restrict__ vs,
                                                  float *__restrict__ wsf, float *__restrict__ rhs_only,
                                                  int *__restrict__ err) {
+    pdl_enter();
     using namespace tma;
     constexpr int NF = LES ? 4 : 3, PX = BX;
     constexpr int NPAIR = 34;   // pairs at tile columns 2..69 (x = i0-2 .. i0+65): every column a stencil reads
