@@ -264,6 +264,67 @@ def cpu_baseline(c, seconds):
 
 
 # ---------------------------------------------------------------------------------------------------------------
+def group_bench(local):
+    """Serving groups against per-context graphs on one stream each: cell-steps/s of 20 steps of the same cases
+    (CUDA events, best of 3), for 16 cases of 32^3, 16 of 64^3, a 16-case mix of 32^3-128^3 and 64 cases of 32^3
+    (half Taylor-Green, half channel; a case's first steps taken before the timing)."""
+    import torch
+    from dfdm import cases, serve
+    from dfdm.native import Group, Solver
+
+    def ready(c):
+        s = Solver(c, "fp32", graphs=True)
+        s.set_state(*cases.initial_condition(c))
+        s.compute_time_step_RK3(2)
+        return s
+
+    def best(fn, st, reps=3):
+        """Device seconds of fn's work on the streams st: from an event on st[0] that every stream waits on, to an
+        event on st[0] after every stream's work (best of reps)."""
+        t = 1e9
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st[0])
+            for x in st[1:]:
+                x.wait_event(e0)
+            fn()
+            for x in st[1:]:
+                ev = torch.cuda.Event()
+                ev.record(x)
+                st[0].wait_event(ev)
+            e1.record(st[0])
+            e1.synchronize()
+            t = min(t, e0.elapsed_time(e1) * 1e-3)
+        return t
+
+    K = 20
+    out = {}
+    for label, grids, n in [("16x32^3", (32,), 16), ("16x64^3", (64,), 16), ("16-case mix 32^3-128^3", (32, 48, 64, 96, 128), 16),
+                            ("64x32^3", (32,), 64)]:
+        rng = np.random.default_rng(1)
+        cs = [serve.serve_case("tgv" if q % 2 else "chan", int(rng.choice(grids)), 1000.0, q) for q in range(n)]
+        cells = sum(c.n_cells for c in cs)
+        per = [ready(c) for c in cs]
+        pst = [torch.cuda.ExternalStream(s.stream_handle, device=local) for s in per]
+        t_per = best(lambda: [s.compute_time_step_RK3_async(K) for s in per], pst)
+        grp = [ready(c) for c in cs]
+        g = Group(grp)
+        g.step(1)
+        gst = [torch.cuda.ExternalStream(g.stream_handle, device=local)]
+        t_grp = best(lambda: g.step_async(K), gst)
+        launches = g.launch_count()
+        g.step(1)
+        per_step = g.launch_count() - launches
+        out[label] = {"cells": cells, "per_context_streams_cell_steps_per_s": cells * K / t_per,
+                      "group_cell_steps_per_s": cells * K / t_grp, "group_over_per_context": t_per / t_grp,
+                      "group_ms_per_step": t_grp / K * 1e3, "group_launches_per_step": per_step}
+        g.close()
+        for s in per + grp:
+            s.close()
+    return out
+
+
 def serve_bench(args, local, rank, ws, gather):
     """The serving stream (256 requests, Poisson arrivals at 4/s, FP32-mixed, 150 GB admission budget) through the
     grouped loop (serve.GroupScheduler: the admitted cases of each shape class step as one serving group, one grouped
@@ -284,6 +345,7 @@ def serve_bench(args, local, rank, ws, gather):
     serve.Scheduler(pex, 150e9).run(warm)
     runs = serve.saturated_throughput(pex, serve.Scheduler, reqs[rank::ws][:args.serve_saturated], 150e9)
     per = sum(gather(float(np.median(runs))))
+    out["group_steps"] = group_bench(local)
     out.update({"loop": "grouped per shape class (serve.GroupScheduler)", "arrival_rate_per_s": args.serve_rate,
                 "precision": "fp32-mixed",
                 "per_context_saturated_throughput_cell_steps_per_s": per,

@@ -2549,6 +2549,11 @@ struct dfdm_group {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     bool own_stream = false;               // created by dfdm_group_create (stream argument NULL)
+    // at most this many cells per graph branch (0: one branch per class).  Measured on one B200 (FP32, graphed
+    // steps, cell-steps/s against per-context graphs on one stream each): 16 x 32^3 1.27x, 64 x 32^3 1.79x,
+    // 16 x 48^3 1.02x, 16 x 64^3 0.96x, 8 x 96^3 0.98x, a 32^3-128^3 mix 0.98x; one branch per class gave 0.92x at
+    // 16 x 64^3 and 1.5x at 64 x 32^3.
+    long long branch_cells = 512 * 1024;
     cudaEvent_t ev = nullptr;              // orders the members' own streams with the group's launches
     // the branch streams and fork/join events of the step's capture, released once the capture has ended
     std::vector<cudaStream_t> cap_streams;
@@ -2774,7 +2779,24 @@ int group_step_enqueue(dfdm_group *g) {
         const int v = (c->stage_variant == 1 || (c->stage_variant == 2 && c->tma_ok)) ? 1 : 0;
         classes[{v, c->d.Nx, c->d.Nz, c->yper ? c->d.Ny : -1}].push_back(c);
     }
-    if (classes.size() == 1) return members_step_enqueue(g->cs, g->stream);
+    // classes larger than branch_cells split into several branches (consecutive members, in group order)
+    std::vector<std::vector<dfdm_ctx *>> branches;
+    for (auto &kv : classes) {
+        std::vector<dfdm_ctx *> cur;
+        long long cells = 0;
+        for (dfdm_ctx *c : kv.second) {
+            const long long n = (long long)c->d.Nx * c->d.Ny * c->d.Nz;
+            if (!cur.empty() && g->branch_cells > 0 && cells + n > g->branch_cells) {
+                branches.push_back(cur);
+                cur.clear();
+                cells = 0;
+            }
+            cur.push_back(c);
+            cells += n;
+        }
+        branches.push_back(cur);
+    }
+    if (branches.size() == 1) return members_step_enqueue(g->cs, g->stream);
     cudaEvent_t fork = nullptr;
     int rc = DFDM_OK;
     auto check = [&](cudaError_t e, const char *what) {
@@ -2783,7 +2805,7 @@ int group_step_enqueue(dfdm_group *g) {
     check(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "fork event creation");
     if (fork) g->cap_events.push_back(fork);
     check(cudaEventRecord(fork, g->stream), "fork event record");
-    for (auto &kv : classes) {
+    for (auto &members : branches) {
         if (rc) break;
         cudaStream_t b = nullptr;
         cudaEvent_t j = nullptr;
@@ -2793,11 +2815,11 @@ int group_step_enqueue(dfdm_group *g) {
         if (j) g->cap_events.push_back(j);
         if (rc) break;
         check(cudaStreamWaitEvent(b, fork, 0), "branch wait on the fork");
-        if (!rc) rc = members_step_enqueue(kv.second, b);
+        if (!rc) rc = members_step_enqueue(members, b);
         check(cudaEventRecord(j, b), "join event record");
         check(cudaStreamWaitEvent(g->stream, j, 0), "wait on the join");
     }
-    if (rc) g_err += " (" + std::to_string(classes.size()) + " shape classes)";
+    if (rc) g_err += " (" + std::to_string(branches.size()) + " branches)";
     return rc;
 }
 
@@ -2924,6 +2946,15 @@ int dfdm_group_step_async(dfdm_group *g, int nsteps) {
 int dfdm_group_synchronize(dfdm_group *g) {
     if (!g) return fail(DFDM_ERR_INVALID, "null group");
     CK(cudaStreamSynchronize(g->stream));
+    return DFDM_OK;
+}
+
+int dfdm_group_set_branch_cells(dfdm_group *g, long long cells) {
+    if (!g || cells < 0) return fail(DFDM_ERR_INVALID, "null group or negative cell count");
+    if (g->branch_cells != cells) {
+        g->branch_cells = cells;
+        group_destroy_graph(g);   // recaptured at the next step
+    }
     return DFDM_OK;
 }
 

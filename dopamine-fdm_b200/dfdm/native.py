@@ -37,7 +37,7 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_write_box_snapshot", "dfdm_set_landing_times", "dfdm_write_snapshot_ex", "dfdm_get_stage_timing",
            "dfdm_set_sgs_in_tile", "dfdm_get_sgs_in_tile", "dfdm_group_create", "dfdm_group_step_async",
            "dfdm_group_synchronize", "dfdm_group_launch_count", "dfdm_group_destroy", "dfdm_get_stream",
-           "dfdm_group_get_stream"]
+           "dfdm_group_get_stream", "dfdm_group_set_branch_cells"]
 
 
 class DfdmError(RuntimeError):
@@ -123,6 +123,7 @@ def load(build_if_missing: bool = True):
         "dfdm_group_destroy": (c_int, [c_void_p]),
         "dfdm_get_stream": (c_int, [c_void_p, POINTER(c_void_p)]),
         "dfdm_group_get_stream": (c_int, [c_void_p, POINTER(c_void_p)]),
+        "dfdm_group_set_branch_cells": (c_int, [c_void_p, ctypes.c_longlong]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -474,6 +475,10 @@ class Group:
         v = ctypes.c_longlong(0)
         _check(load().dfdm_group_launch_count(self.h, ctypes.byref(v)))
         return int(v.value)
+
+    def set_branch_cells(self, cells: int) -> None:
+        """At most `cells` cells per graph branch (0: one branch per shape class); results do not change."""
+        _check(load().dfdm_group_set_branch_cells(self.h, int(cells)))
 
     def close(self):
         if getattr(self, "h", None):

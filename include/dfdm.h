@@ -309,7 +309,8 @@ int dfdm_launch_count(dfdm_ctx *ctx, long long *count);
  * step (stage kernel, div + forward x transform, z transforms, y solve or periodic-y transform, inverse x transform,
  * stage-3 correction, constant-flux sum and shift) is ONE launch for all the class's members, whose blocks find
  * their case in a job table and run the per-case kernel's code on it.  One group step is captured once as a CUDA
- * graph, each class on a branch of its own, so that the classes' launches overlap.  A member's results do not depend on the other members: a case steps
+ * graph, each class (or each part of a class up to dfdm_group_set_branch_cells cells) on a branch of its own, so that
+ * the branches' launches overlap.  A member's results do not depend on the other members: a case steps
  * bit-identically in a group of one and in any mix, on any stream.  Against k dfdm_compute_time_step_rk3 steps of
  * the same context they agree to FP32 rounding: the grouped kernels are a separate compilation of the per-case
  * kernels' source, whose scalar multiply-add contractions may differ.
@@ -329,6 +330,10 @@ int dfdm_group_create(dfdm_ctx *const *ctxs, int n, void *stream, dfdm_group **o
 int dfdm_group_step_async(dfdm_group *group, int nsteps);
 int dfdm_group_synchronize(dfdm_group *group);
 int dfdm_group_get_stream(dfdm_group *group, void **cuda_stream);
+/* At most `cells` cells per graph branch (default 524288): a shape class with more splits into several branches of
+ * consecutive members, which overlap on the device as the classes do (0: one branch per class).  Results do not
+ * change.  The group's graph is recaptured at its next step. */
+int dfdm_group_set_branch_cells(dfdm_group *group, long long cells);
 /* Number of the library's kernels the group has enqueued (graph replays included). */
 int dfdm_group_launch_count(dfdm_group *group, long long *count);
 int dfdm_group_destroy(dfdm_group *group);

@@ -22,6 +22,7 @@ MIX = [("tgv", 32, 800.0, 3), ("chan", 48, 0.0, 5), ("tgv", 64, 1600.0, 7), ("ch
        ("tgv", 48, 2400.0, 13), ("chan", 64, 0.0, 17), ("tgv", 32, 1200.0, 19)]
 
 GROUP_MAX = 24   # jobs per grouped launch (kernels_group.cuh)
+BRANCH_CELLS = 512 * 1024   # default cells per graph branch (dfdm_group_set_branch_cells)
 
 
 def _first_step(case, stream=None):
@@ -32,18 +33,29 @@ def _first_step(case, stream=None):
 
 
 def _expected_launches(solvers):
-    """Kernels of one group step.  The members fall into shape classes (stage-kernel form, Nx, Nz, periodic Ny); per
-    class and RK stage: the stage kernel, the forward and the inverse x transform, the forward and the inverse z
-    transform, the y solve (walls) or the periodic-y transform; per class the stage-3 correction and, for its
-    constant-flux cases, the bulk sum, its reduction and the shift.  Each takes one launch per GROUP_MAX jobs."""
+    """Kernels of one group step.  The members fall into shape classes (stage-kernel form, Nx, Nz, periodic Ny), split
+    into branches of consecutive members of at most BRANCH_CELLS cells; per branch and RK stage: the stage kernel, the
+    forward and the inverse x transform, the forward and the inverse z transform, the y solve (walls) or the
+    periodic-y transform; per branch the stage-3 correction and, for its constant-flux cases, the bulk sum, its
+    reduction and the shift.  Each takes one launch per GROUP_MAX jobs."""
     from collections import defaultdict
     up = lambda n: -(-n // GROUP_MAX)
     classes = defaultdict(list)
     for s in solvers:
         per = s.case.ny if s.case.y_bc_type == 0 else -1
         classes[(1 if s.stage_variant()[0] else 0, s.case.nx, s.case.nz, per)].append(s)
-    total = 0
+    branches = []
     for members in classes.values():
+        cur, cells = [], 0
+        for s in members:
+            if cur and cells + s.case.n_cells > BRANCH_CELLS:
+                branches.append(cur)
+                cur, cells = [], 0
+            cur.append(s)
+            cells += s.case.n_cells
+        branches.append(cur)
+    total = 0
+    for members in branches:
         n = len(members)
         flux = sum(s.case.flow_forcing_mode == 1 for s in members)
         total += 3 * 6 * up(n) + up(n) + 3 * up(flux)
@@ -147,7 +159,7 @@ def test_more_members_than_one_job_table():
     """Thirty members, one job table each, in two shape classes of 15; each is bit-identical to its group of one."""
     cs = [serve.serve_case("tgv" if q % 2 else "chan", 32, 900.0 + 50 * q, 100 + q) for q in range(30)]
     big, launched, expected = _grouped(cs, 2)
-    assert launched == expected and launched <= 2 * 2 * (19 * 1 + 3)   # two classes of 15: 41 launches a step
+    assert launched == expected and launched <= 2 * 2 * (19 * 1 + 3)   # two branches of 15 (491,520 cells each)
     for c, b in zip(cs, big):
         one, _, _ = _grouped([c], 2)
         for x, y in zip(one[0], b):
@@ -194,3 +206,25 @@ def test_ineligible_members_are_refused():
         Group([fresh, fresh])
     for s in (s64, fresh, les):
         s.close()
+
+
+def test_branch_splitting_leaves_results_unchanged():
+    """A class of eight 64^3 cases stepped as one branch, as branches of at most 2^19 cells (two cases) and as one
+    branch per case: bit-identical states, and the launch counts of the branch model."""
+    cs = [serve.serve_case("tgv", 64, 1000.0 + 100 * q, 200 + q) for q in range(8)]
+    ref = None
+    for cells, nbranch in [(0, 1), (1 << 19, 4), (1, 8)]:
+        ss = [_first_step(c) for c in cs]
+        with Group(ss) as g:
+            g.set_branch_cells(cells)
+            before = g.launch_count()
+            g.step(2)
+            assert g.launch_count() - before == 2 * nbranch * (3 * 6 + 1)
+        st = [s.get_state() for s in ss]
+        for s in ss:
+            s.close()
+        if ref is None:
+            ref = st
+        for a, b in zip(st, ref):
+            for x, y in zip(a, b):
+                assert np.array_equal(x, y)
