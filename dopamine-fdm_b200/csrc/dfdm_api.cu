@@ -2554,6 +2554,8 @@ struct dfdm_group {
     // 16 x 48^3 1.02x, 16 x 64^3 0.96x, 8 x 96^3 0.98x, a 32^3-128^3 mix 0.98x; one branch per class gave 0.92x at
     // 16 x 64^3 and 1.5x at 64 x 32^3.
     long long branch_cells = 512 * 1024;
+    std::map<const dfdm_ctx *, int> kc;    // tuned z-planes per block of the members' grouped stage launches
+    bool tuned = false;
     cudaEvent_t ev = nullptr;              // orders the members' own streams with the group's launches
     // the branch streams and fork/join events of the step's capture, released once the capture has ended
     std::vector<cudaStream_t> cap_streams;
@@ -2598,7 +2600,44 @@ int group_eligible(const dfdm_ctx *c) {
 }
 
 // one step of the cases `cs` on stream st (the launch sequence of step_enqueue, family by family across the cases)
-int members_step_enqueue(const std::vector<dfdm_ctx *> &cs, cudaStream_t st) {
+// the stage form a member runs in a group: variant 2 is variant 1's arithmetic (the per-case launch falls back to
+// variant 0 without TMA)
+int group_stage_form(const dfdm_ctx *c) { return (c->stage_variant == 1 || (c->stage_variant == 2 && c->tma_ok)) ? 1 : 0; }
+
+// one member's stage-kernel job of RK stage s (the pointers as they stand; with s >= 2 after the u* swap), kc planes per
+// block
+StageJob group_stage_job(dfdm_ctx *c, int s, int kc) {
+    typedef Impl<float> I;
+    const bool corr = s >= 2;
+    StageJob J;
+    const int v = group_stage_form(c);
+    J.kc = kc;
+    J.grid = v ? tile_grid(c->d, J.kc, TILE_X2) : tile_grid(c->d, J.kc);
+    J.a = step_args<float>(c);
+    J.U = corr ? (const float *)c->us2 : (const float *)c->u;
+    J.V = corr ? (const float *)c->vs2 : (const float *)c->v;
+    J.W = corr ? (const float *)c->ws2 : (const float *)c->w;
+    J.tau_x = c->wsd.tau_x; J.tau_z = c->wsd.tau_z;
+    StageCoef sc;
+    sc.stage = s;
+    sc.dt_a11 = c->prm.dt * (8.0 / 15.0);
+    sc.dt = c->prm.dt;
+    sc.c1 = 1.0 / 4.0;
+    sc.c2 = (s == 2) ? 5.0 / 12.0 : 3.0 / 4.0;
+    sc.incr = I::incr_form(c, s);
+    sc.dtp = nullptr;
+    sc.no_uo = 1;
+    J.sc = sc;
+    J.uo = (float *)c->u; J.vo = (float *)c->v; J.wo = (float *)c->w;   // fused: U is the RK base state
+    J.f1u = (float *)c->f1u; J.f1v = (float *)c->f1v; J.f1w = (float *)c->f1w;
+    J.us = (float *)c->us; J.vs = (float *)c->vs; J.wsf = (float *)c->wsf;
+    J.nu = nullptr; J.rhs_only = nullptr; J.nut_out = nullptr;
+    return J;
+}
+
+// one step of the cases `cs` on stream st (the launch sequence of step_enqueue, family by family across the cases);
+// kc: the stage kernels' z-planes per block of each member (absent: the member's own choice)
+int members_step_enqueue(const std::vector<dfdm_ctx *> &cs, cudaStream_t st, const std::map<const dfdm_ctx *, int> &kc) {
     typedef Impl<float> I;
     typedef float2 C;
     constexpr int NL = I::NL;
@@ -2608,31 +2647,9 @@ int members_step_enqueue(const std::vector<dfdm_ctx *> &cs, cudaStream_t st) {
         const bool corr = s >= 2;
         for (dfdm_ctx *c : cs) {
             if (corr) { std::swap(c->us, c->us2); std::swap(c->vs, c->vs2); std::swap(c->wsf, c->ws2); }
-            StageJob J;
-            // variant 2 is variant 1's arithmetic (the per-case launch falls back to variant 0 without TMA)
-            const int v = (c->stage_variant == 1 || (c->stage_variant == 2 && c->tma_ok)) ? 1 : 0;
-            J.kc = v ? c->kc_stage2 : c->kc_stage;
-            J.grid = v ? tile_grid(c->d, J.kc, TILE_X2) : tile_grid(c->d, J.kc);
-            J.a = step_args<float>(c);
-            J.U = corr ? (const float *)c->us2 : (const float *)c->u;
-            J.V = corr ? (const float *)c->vs2 : (const float *)c->v;
-            J.W = corr ? (const float *)c->ws2 : (const float *)c->w;
-            J.tau_x = c->wsd.tau_x; J.tau_z = c->wsd.tau_z;
-            StageCoef sc;
-            sc.stage = s;
-            sc.dt_a11 = c->prm.dt * (8.0 / 15.0);
-            sc.dt = c->prm.dt;
-            sc.c1 = 1.0 / 4.0;
-            sc.c2 = (s == 2) ? 5.0 / 12.0 : 3.0 / 4.0;
-            sc.incr = I::incr_form(c, s);
-            sc.dtp = nullptr;
-            sc.no_uo = 1;
-            J.sc = sc;
-            J.uo = (float *)c->u; J.vo = (float *)c->v; J.wo = (float *)c->w;   // fused: U is the RK base state
-            J.f1u = (float *)c->f1u; J.f1v = (float *)c->f1v; J.f1w = (float *)c->f1w;
-            J.us = (float *)c->us; J.vs = (float *)c->vs; J.wsf = (float *)c->wsf;
-            J.nu = nullptr; J.rhs_only = nullptr; J.nut_out = nullptr;
-            stage[v].push_back(J);
+            const int v = group_stage_form(c);
+            auto it = kc.find(c);
+            stage[v].push_back(group_stage_job(c, s, it != kc.end() ? it->second : (v ? c->kc_stage2 : c->kc_stage)));
         }
         int rc;
         if (corr) {
@@ -2769,17 +2786,11 @@ int members_step_enqueue(const std::vector<dfdm_ctx *> &cs, cudaStream_t st) {
     return DFDM_OK;
 }
 
-// A group's cases fall into shape classes: the same stage-kernel form, Nx, Nz and periodic Ny, so that every kernel
-// family of a class is one instantiation, i.e. one launch.  Each class is captured on a branch of its own (forked
-// from the group's stream and joined back), so the classes' launches overlap on the device as independent streams'
-// would, while the cases of a class share their launches.
-int group_step_enqueue(dfdm_group *g) {
+// the members split into branches: shape classes (stage form, Nx, Nz, periodic Ny), each cut into runs of consecutive
+// members of at most branch_cells cells
+std::vector<std::vector<dfdm_ctx *>> group_branches(const dfdm_group *g) {
     std::map<std::array<int, 4>, std::vector<dfdm_ctx *>> classes;
-    for (dfdm_ctx *c : g->cs) {
-        const int v = (c->stage_variant == 1 || (c->stage_variant == 2 && c->tma_ok)) ? 1 : 0;
-        classes[{v, c->d.Nx, c->d.Nz, c->yper ? c->d.Ny : -1}].push_back(c);
-    }
-    // classes larger than branch_cells split into several branches (consecutive members, in group order)
+    for (dfdm_ctx *c : g->cs) classes[{group_stage_form(c), c->d.Nx, c->d.Nz, c->yper ? c->d.Ny : -1}].push_back(c);
     std::vector<std::vector<dfdm_ctx *>> branches;
     for (auto &kv : classes) {
         std::vector<dfdm_ctx *> cur;
@@ -2796,7 +2807,91 @@ int group_step_enqueue(dfdm_group *g) {
         }
         branches.push_back(cur);
     }
-    if (branches.size() == 1) return members_step_enqueue(g->cs, g->stream);
+    return branches;
+}
+
+// Tile shapes of the grouped stage launches.  A member's own z-chunk (kc) fills the GPU with that case alone; in a
+// group the tiles of all members of a branch share the device, and longer chunks re-read fewer halo planes.  For each
+// branch the candidates are the members' own kc, the chunking the same wave model (choose_kc) picks for the branch's
+// tiles together, and one chunk per column; each is timed with stage-1 launches of the branch (2 + 3 launches, CUDA
+// events on the group's stream) and the fastest kept.  The stage kernel's arithmetic does not depend on kc, so neither
+// do the results.  Stage-1 launches write only F1 and u*, which every step's stage 1 rewrites before reading, so the
+// timing leaves the members' state untouched.  The choice is cached per device, branch shape and member count.
+std::mutex g_group_kc_mu;
+std::map<std::array<long long, 7>, int> g_group_kc;
+
+int group_tune(dfdm_group *g) {
+    g->kc.clear();
+    int dev = 0, nsm = 148;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    int rc = DFDM_OK;
+    for (auto &members : group_branches(g)) {
+        dfdm_ctx *c0 = members[0];
+        const int v = group_stage_form(c0);
+        const Dims &d = c0->d;
+        const std::array<long long, 7> key = {dev, v, d.Nx, d.Ny, d.Nz, c0->yper, (long long)members.size()};
+        int choice = -1;
+        {
+            std::lock_guard<std::mutex> lk(g_group_kc_mu);
+            auto it = g_group_kc.find(key);
+            if (it != g_group_kc.end()) choice = it->second;
+        }
+        if (choice < 0) {
+            int occ = 1;
+            const void *fn = v ? (const void *)kg_stage2<false> : (const void *)kg_stage1<false>;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, 0) != cudaSuccess) occ = 1;
+            const int tx = v ? TILE_X2 : TILE_X;
+            // the wave model over the branch's tiles: as choose_kc with every member's columns side by side
+            Dims dd = d;
+            dd.Ny = d.Ny * (int)members.size();
+            const int own = v ? c0->kc_stage2 : c0->kc_stage;
+            const int cands[3] = {own, choose_kc(dd, occ, nsm, tx), d.Nz};
+            double best = 1e30;
+            for (int q = 0; q < 3 && !rc; ++q) {
+                const int kc = cands[q];
+                bool seen = false;
+                for (int r = 0; r < q; ++r) seen = seen || cands[r] == kc;
+                if (seen) continue;
+                std::vector<StageJob> jobs;
+                for (dfdm_ctx *c : members) jobs.push_back(group_stage_job(c, 1, kc));
+                auto go = [&]() {
+                    return launch_groups(jobs, [&](const GroupTable<StageJob> &t, int nb) {
+                        if (v) kg_stage2<false><<<nb, 256, 0, g->stream>>>(t);
+                        else kg_stage1<false><<<nb, 256, 0, g->stream>>>(t);
+                    });
+                };
+                for (int r = 0; r < 2 && !rc; ++r) rc = go();
+                if (rc) break;
+                cudaEventRecord(e0, g->stream);
+                for (int r = 0; r < 3 && !rc; ++r) rc = go();
+                cudaEventRecord(e1, g->stream);
+                if (cudaEventSynchronize(e1) != cudaSuccess) { rc = fail(DFDM_ERR_CUDA, "group tuning failed"); break; }
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms < best) { best = ms; choice = kc; }
+            }
+            if (rc) break;
+            std::lock_guard<std::mutex> lk(g_group_kc_mu);
+            g_group_kc[key] = choice;
+        }
+        for (dfdm_ctx *c : members) g->kc[c] = choice;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
+// A group's cases fall into shape classes: the same stage-kernel form, Nx, Nz and periodic Ny, so that every kernel
+// family of a class is one instantiation, i.e. one launch.  Each branch (a class, or a run of its members) is
+// captured on a graph branch of its own (forked from the group's stream and joined back), so the branches' launches
+// overlap on the device as independent streams' would, while the cases of a branch share their launches.
+int group_step_enqueue(dfdm_group *g) {
+    const std::vector<std::vector<dfdm_ctx *>> branches = group_branches(g);
+    if (branches.size() == 1) return members_step_enqueue(g->cs, g->stream, g->kc);
     cudaEvent_t fork = nullptr;
     int rc = DFDM_OK;
     auto check = [&](cudaError_t e, const char *what) {
@@ -2815,7 +2910,7 @@ int group_step_enqueue(dfdm_group *g) {
         if (j) g->cap_events.push_back(j);
         if (rc) break;
         check(cudaStreamWaitEvent(b, fork, 0), "branch wait on the fork");
-        if (!rc) rc = members_step_enqueue(members, b);
+        if (!rc) rc = members_step_enqueue(members, b, g->kc);
         check(cudaEventRecord(j, b), "join event record");
         check(cudaStreamWaitEvent(g->stream, j, 0), "wait on the join");
     }
@@ -2917,6 +3012,10 @@ int dfdm_group_step_async(dfdm_group *g, int nsteps) {
             CK(cudaEventRecord(g->ev, c->stream));
             CK(cudaStreamWaitEvent(g->stream, g->ev, 0));
         }
+    if (!g->tuned) {   // the grouped stage launches' tile shapes, before the first capture
+        if (int rc = group_tune(g)) return rc;
+        g->tuned = true;
+    }
     for (int n = 0; n < nsteps; ++n) {
         if (!g->gexec) {   // one step of the whole group, captured once per group
             CK(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
@@ -2953,7 +3052,8 @@ int dfdm_group_set_branch_cells(dfdm_group *g, long long cells) {
     if (!g || cells < 0) return fail(DFDM_ERR_INVALID, "null group or negative cell count");
     if (g->branch_cells != cells) {
         g->branch_cells = cells;
-        group_destroy_graph(g);   // recaptured at the next step
+        group_destroy_graph(g);   // recaptured (and its tile shapes re-chosen) at the next step
+        g->tuned = false;
     }
     return DFDM_OK;
 }

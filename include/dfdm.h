@@ -323,6 +323,10 @@ int dfdm_launch_count(dfdm_ctx *ctx, long long *count);
  *    returns it; destroyed with the group).  group_step_async orders itself after the members' earlier work on
  *    their own streams and their later work after it, with events (no host wait), and advances each member's time
  *    by nsteps * dt.  group_synchronize waits for the group's stream.
+ *  - Before its first step a group picks the z-chunk of its grouped stage launches per branch, timing the members' own
+ *    chunking, the wave model's choice for the branch's tiles together and one chunk per column with stage-1 launches
+ *    (which write only F1 and u*, both rewritten by every step); the choice is cached per branch shape and member
+ *    count.  Results do not depend on it.
  *  - The members must outlive the group's enqueued steps; destroying the group does not wait for them (its graph is
  *    released when they are done) and leaves the members as they are. */
 typedef struct dfdm_group dfdm_group;
