@@ -2543,6 +2543,12 @@ int dfdm_kernel_bytes(dfdm_ctx *c, int which, double *bytes) {
 // ================================================================================================================
 // Serving groups: the steady steps of several FP32-mixed contexts advanced together, one grouped launch per kernel
 // family (and transform length) for all of them.  See kernels_group.cuh.
+// tile shape of a member's grouped stage launches: z-planes per block, and whether resident blocks walk the tiles
+struct GroupTile {
+    int kc;
+    bool walk;
+};
+
 struct dfdm_group {
     std::vector<dfdm_ctx *> cs;
     cudaStream_t stream = nullptr;
@@ -2554,8 +2560,10 @@ struct dfdm_group {
     // 16 x 48^3 1.02x, 16 x 64^3 0.96x, 8 x 96^3 0.98x, a 32^3-128^3 mix 0.98x; one branch per class gave 0.92x at
     // 16 x 64^3 and 1.5x at 64 x 32^3.
     long long branch_cells = 512 * 1024;
-    std::map<const dfdm_ctx *, int> kc;    // tuned z-planes per block of the members' grouped stage launches
+    std::map<const dfdm_ctx *, GroupTile> tile;   // tuned tile shape of the members' grouped stage launches
+    int walk_cap[2] = {0, 0};              // resident blocks of the walking stage kernels (form 0, 1) on the device
     bool tuned = false;
+    GroupTile forced{-1, false};           // dfdm_group_set_stage_tiles (kc < 0: tuned)
     cudaEvent_t ev = nullptr;              // orders the members' own streams with the group's launches
     // the branch streams and fork/join events of the step's capture, released once the capture has ended
     std::vector<cudaStream_t> cap_streams;
@@ -2600,6 +2608,21 @@ int group_eligible(const dfdm_ctx *c) {
 }
 
 // one step of the cases `cs` on stream st (the launch sequence of step_enqueue, family by family across the cases)
+// the grouped stage launch of one form (0 one cell per thread, 1 packed pairs) and RK stage kind (corr: stages 2, 3):
+// one block per tile, or (walk) at most walk_cap[v] resident blocks walking the tiles
+int launch_stage_jobs(const std::vector<StageJob> &jobs, int v, bool corr, bool walk, const int *walk_cap, cudaStream_t st) {
+    return launch_groups(jobs, [&](const GroupTable<StageJob> &t, int nb) {
+        const int g = walk ? std::max(1, std::min(nb, walk_cap[v])) : nb;
+        if (v == 1) {
+            if (walk) { if (corr) kg_stage2_walk<true><<<g, 256, 0, st>>>(t); else kg_stage2_walk<false><<<g, 256, 0, st>>>(t); }
+            else { if (corr) kg_stage2<true><<<g, 256, 0, st>>>(t); else kg_stage2<false><<<g, 256, 0, st>>>(t); }
+        } else {
+            if (walk) { if (corr) kg_stage1_walk<true><<<g, 256, 0, st>>>(t); else kg_stage1_walk<false><<<g, 256, 0, st>>>(t); }
+            else { if (corr) kg_stage1<true><<<g, 256, 0, st>>>(t); else kg_stage1<false><<<g, 256, 0, st>>>(t); }
+        }
+    });
+}
+
 // the stage form a member runs in a group: variant 2 is variant 1's arithmetic (the per-case launch falls back to
 // variant 0 without TMA)
 int group_stage_form(const dfdm_ctx *c) { return (c->stage_variant == 1 || (c->stage_variant == 2 && c->tma_ok)) ? 1 : 0; }
@@ -2635,9 +2658,11 @@ StageJob group_stage_job(dfdm_ctx *c, int s, int kc) {
     return J;
 }
 
-// one step of the cases `cs` on stream st (the launch sequence of step_enqueue, family by family across the cases);
-// kc: the stage kernels' z-planes per block of each member (absent: the member's own choice)
-int members_step_enqueue(const std::vector<dfdm_ctx *> &cs, cudaStream_t st, const std::map<const dfdm_ctx *, int> &kc) {
+// one step of the cases `cs` (one branch) on stream st (the launch sequence of step_enqueue, family by family across
+// the cases); tile: the stage launches' z-planes per block of each member and whether they walk the tiles with
+// resident blocks (absent: the member's own kc, one block per tile); walk_cap: resident blocks of the walking kernels
+int members_step_enqueue(const std::vector<dfdm_ctx *> &cs, cudaStream_t st,
+                         const std::map<const dfdm_ctx *, GroupTile> &tile, const int *walk_cap) {
     typedef Impl<float> I;
     typedef float2 C;
     constexpr int NL = I::NL;
@@ -2648,17 +2673,14 @@ int members_step_enqueue(const std::vector<dfdm_ctx *> &cs, cudaStream_t st, con
         for (dfdm_ctx *c : cs) {
             if (corr) { std::swap(c->us, c->us2); std::swap(c->vs, c->vs2); std::swap(c->wsf, c->ws2); }
             const int v = group_stage_form(c);
-            auto it = kc.find(c);
-            stage[v].push_back(group_stage_job(c, s, it != kc.end() ? it->second : (v ? c->kc_stage2 : c->kc_stage)));
+            auto it = tile.find(c);
+            stage[v].push_back(group_stage_job(c, s, it != tile.end() ? it->second.kc : (v ? c->kc_stage2 : c->kc_stage)));
         }
+        auto it0 = tile.find(cs[0]);
+        const bool walk = it0 != tile.end() && it0->second.walk;
         int rc;
-        if (corr) {
-            if ((rc = launch_groups(stage[1], [&](const GroupTable<StageJob> &t, int nb) { kg_stage2<true><<<nb, 256, 0, st>>>(t); }))) return rc;
-            if ((rc = launch_groups(stage[0], [&](const GroupTable<StageJob> &t, int nb) { kg_stage1<true><<<nb, 256, 0, st>>>(t); }))) return rc;
-        } else {
-            if ((rc = launch_groups(stage[1], [&](const GroupTable<StageJob> &t, int nb) { kg_stage2<false><<<nb, 256, 0, st>>>(t); }))) return rc;
-            if ((rc = launch_groups(stage[0], [&](const GroupTable<StageJob> &t, int nb) { kg_stage1<false><<<nb, 256, 0, st>>>(t); }))) return rc;
-        }
+        for (int v = 1; v >= 0; --v)
+            if ((rc = launch_stage_jobs(stage[v], v, corr, walk, walk_cap, st))) return rc;
         // ---- div u* + forward x, per length ----
         std::map<int, std::vector<FwdXJob>> fx;
         std::map<int, size_t> fx_smem;
@@ -2813,34 +2835,48 @@ std::vector<std::vector<dfdm_ctx *>> group_branches(const dfdm_group *g) {
 // Tile shapes of the grouped stage launches.  A member's own z-chunk (kc) fills the GPU with that case alone; in a
 // group the tiles of all members of a branch share the device, and longer chunks re-read fewer halo planes.  For each
 // branch the candidates are the members' own kc, the chunking the same wave model (choose_kc) picks for the branch's
-// tiles together, and one chunk per column; each is timed with stage-1 launches of the branch (2 + 3 launches, CUDA
-// events on the group's stream) and the fastest kept.  The stage kernel's arithmetic does not depend on kc, so neither
+// tiles together, and one chunk per column, each with one block per tile or with resident blocks walking the tiles;
+// each is timed with stage-1 launches of the branch (2 + 3 launches, CUDA events on the group's stream) and the
+// fastest kept.  The stage kernel's arithmetic does not depend on kc, so neither
 // do the results.  Stage-1 launches write only F1 and u*, which every step's stage 1 rewrites before reading, so the
 // timing leaves the members' state untouched.  The choice is cached per device, branch shape and member count.
-std::mutex g_group_kc_mu;
-std::map<std::array<long long, 7>, int> g_group_kc;
+std::mutex g_group_tile_mu;
+std::map<std::array<long long, 7>, GroupTile> g_group_tile;
 
 int group_tune(dfdm_group *g) {
-    g->kc.clear();
+    g->tile.clear();
+    if (g->forced.kc >= 0) {   // set by the caller: 0 keeps each member's own kc
+        for (dfdm_ctx *c : g->cs) {
+            const int own = group_stage_form(c) ? c->kc_stage2 : c->kc_stage;
+            g->tile[c] = GroupTile{g->forced.kc > 0 ? std::min(g->forced.kc, c->d.Nz) : own, g->forced.walk};
+        }
+    }
     int dev = 0, nsm = 148;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    for (int v = 0; v < 2; ++v) {
+        int occ = 1;
+        const void *fn = v ? (const void *)kg_stage2_walk<true> : (const void *)kg_stage1_walk<true>;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, 0) != cudaSuccess) occ = 1;
+        g->walk_cap[v] = std::max(1, occ) * nsm;
+    }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     int rc = DFDM_OK;
     for (auto &members : group_branches(g)) {
+        if (g->forced.kc >= 0) break;
         dfdm_ctx *c0 = members[0];
         const int v = group_stage_form(c0);
         const Dims &d = c0->d;
         const std::array<long long, 7> key = {dev, v, d.Nx, d.Ny, d.Nz, c0->yper, (long long)members.size()};
-        int choice = -1;
+        GroupTile choice{-1, false};
         {
-            std::lock_guard<std::mutex> lk(g_group_kc_mu);
-            auto it = g_group_kc.find(key);
-            if (it != g_group_kc.end()) choice = it->second;
+            std::lock_guard<std::mutex> lk(g_group_tile_mu);
+            auto it = g_group_tile.find(key);
+            if (it != g_group_tile.end()) choice = it->second;
         }
-        if (choice < 0) {
+        if (choice.kc < 0) {
             int occ = 1;
             const void *fn = v ? (const void *)kg_stage2<false> : (const void *)kg_stage1<false>;
             if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, 0) != cudaSuccess) occ = 1;
@@ -2849,36 +2885,31 @@ int group_tune(dfdm_group *g) {
             Dims dd = d;
             dd.Ny = d.Ny * (int)members.size();
             const int own = v ? c0->kc_stage2 : c0->kc_stage;
-            const int cands[3] = {own, choose_kc(dd, occ, nsm, tx), d.Nz};
+            const int kcs[3] = {own, choose_kc(dd, occ, nsm, tx), d.Nz};
             double best = 1e30;
-            for (int q = 0; q < 3 && !rc; ++q) {
-                const int kc = cands[q];
+            for (int q = 0; q < 6 && !rc; ++q) {
+                const int kc = kcs[q % 3];
+                const bool walk = q >= 3;
                 bool seen = false;
-                for (int r = 0; r < q; ++r) seen = seen || cands[r] == kc;
+                for (int r = 0; r < q % 3; ++r) seen = seen || kcs[r] == kc;
                 if (seen) continue;
                 std::vector<StageJob> jobs;
                 for (dfdm_ctx *c : members) jobs.push_back(group_stage_job(c, 1, kc));
-                auto go = [&]() {
-                    return launch_groups(jobs, [&](const GroupTable<StageJob> &t, int nb) {
-                        if (v) kg_stage2<false><<<nb, 256, 0, g->stream>>>(t);
-                        else kg_stage1<false><<<nb, 256, 0, g->stream>>>(t);
-                    });
-                };
-                for (int r = 0; r < 2 && !rc; ++r) rc = go();
+                for (int r = 0; r < 2 && !rc; ++r) rc = launch_stage_jobs(jobs, v, false, walk, g->walk_cap, g->stream);
                 if (rc) break;
                 cudaEventRecord(e0, g->stream);
-                for (int r = 0; r < 3 && !rc; ++r) rc = go();
+                for (int r = 0; r < 3 && !rc; ++r) rc = launch_stage_jobs(jobs, v, false, walk, g->walk_cap, g->stream);
                 cudaEventRecord(e1, g->stream);
                 if (cudaEventSynchronize(e1) != cudaSuccess) { rc = fail(DFDM_ERR_CUDA, "group tuning failed"); break; }
                 float ms = 0.0f;
                 cudaEventElapsedTime(&ms, e0, e1);
-                if (ms < best) { best = ms; choice = kc; }
+                if (ms < best) { best = ms; choice = GroupTile{kc, walk}; }
             }
             if (rc) break;
-            std::lock_guard<std::mutex> lk(g_group_kc_mu);
-            g_group_kc[key] = choice;
+            std::lock_guard<std::mutex> lk(g_group_tile_mu);
+            g_group_tile[key] = choice;
         }
-        for (dfdm_ctx *c : members) g->kc[c] = choice;
+        for (dfdm_ctx *c : members) g->tile[c] = choice;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -2891,7 +2922,7 @@ int group_tune(dfdm_group *g) {
 // overlap on the device as independent streams' would, while the cases of a branch share their launches.
 int group_step_enqueue(dfdm_group *g) {
     const std::vector<std::vector<dfdm_ctx *>> branches = group_branches(g);
-    if (branches.size() == 1) return members_step_enqueue(g->cs, g->stream, g->kc);
+    if (branches.size() == 1) return members_step_enqueue(g->cs, g->stream, g->tile, g->walk_cap);
     cudaEvent_t fork = nullptr;
     int rc = DFDM_OK;
     auto check = [&](cudaError_t e, const char *what) {
@@ -2910,7 +2941,7 @@ int group_step_enqueue(dfdm_group *g) {
         if (j) g->cap_events.push_back(j);
         if (rc) break;
         check(cudaStreamWaitEvent(b, fork, 0), "branch wait on the fork");
-        if (!rc) rc = members_step_enqueue(members, b, g->kc);
+        if (!rc) rc = members_step_enqueue(members, b, g->tile, g->walk_cap);
         check(cudaEventRecord(j, b), "join event record");
         check(cudaStreamWaitEvent(g->stream, j, 0), "wait on the join");
     }
@@ -3055,6 +3086,14 @@ int dfdm_group_set_branch_cells(dfdm_group *g, long long cells) {
         group_destroy_graph(g);   // recaptured (and its tile shapes re-chosen) at the next step
         g->tuned = false;
     }
+    return DFDM_OK;
+}
+
+int dfdm_group_set_stage_tiles(dfdm_group *g, int kc, int walk) {
+    if (!g) return fail(DFDM_ERR_INVALID, "null group");
+    g->forced = GroupTile{kc < 0 ? -1 : kc, walk != 0};
+    g->tuned = false;
+    group_destroy_graph(g);   // recaptured at the next step
     return DFDM_OK;
 }
 

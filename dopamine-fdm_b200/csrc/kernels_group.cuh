@@ -34,10 +34,10 @@ __device__ __forceinline__ int group_job(const int *start, int njobs, int b) {
     }
     return lo;
 }
-// block coordinates of this block in job j's own grid
-template <class Job> __device__ __forceinline__ JobBlock at(const GroupTable<Job> &g, int j) {
+// block coordinates of linear tile b (of job j) in job j's own grid; at(g, j) is this block's
+template <class Job> __device__ __forceinline__ JobBlock at(const GroupTable<Job> &g, int j, int b) {
     const dim3 gd = g.jobs[j].grid;
-    const int local = (int)blockIdx.x - g.start[j];
+    const int local = b - g.start[j];
     JobBlock r;
     r.b.x = local % gd.x;
     const int t = local / gd.x;
@@ -46,6 +46,7 @@ template <class Job> __device__ __forceinline__ JobBlock at(const GroupTable<Job
     r.g = gd;
     return r;
 }
+template <class Job> __device__ __forceinline__ JobBlock at(const GroupTable<Job> &g, int j) { return at(g, j, (int)blockIdx.x); }
 
 // ---- the stage kernel (DNS, no wall model): packed pairs (variant 1) or one cell per thread (variant 0) ----
 struct StageJob {
@@ -76,6 +77,38 @@ __global__ void __launch_bounds__(256, 3) kg_stage1(const __grid_constant__ Grou
     k_tiled_body<float, false, false, 32, 8, 0, CORR>(at(g, j), J.a, J.U, J.V, J.W, J.nu, J.tau_x, J.tau_z, J.sc,
                                                       J.kc, J.uo, J.vo, J.wo, J.f1u, J.f1v, J.f1w, J.us, J.vs, J.wsf,
                                                       J.rhs_only, J.nut_out);
+}
+
+// The same stage kernels as persistent blocks: a grid of at most the resident capacity walks the table's tiles
+// (tile b, b + gridDim.x, ...).  Between tiles a block waits for its last cp.async copies and synchronises, so the next
+// tile's loads cannot overtake the previous tile's reads of shared memory.  The group's tuner times this form against
+// one block per tile and keeps the faster.
+template <bool CORR>
+__global__ void __launch_bounds__(256, 2) kg_stage2_walk(const __grid_constant__ GroupTable<StageJob> g) {
+    pdl_enter();
+    const int total = g.start[g.njobs];
+    for (int b = blockIdx.x; b < total; b += gridDim.x) {
+        const int j = group_job(g.start, g.njobs, b);
+        const StageJob &J = g.jobs[j];
+        k_tiled2_body<false, false, 8, false, CORR>(at(g, j, b), J.a, J.U, J.V, J.W, J.nu, J.tau_x, J.tau_z, J.sc, J.kc,
+                                                    J.uo, J.vo, J.wo, J.f1u, J.f1v, J.f1w, J.us, J.vs, J.wsf, J.rhs_only);
+        cp_async_wait_all();
+        __syncthreads();
+    }
+}
+template <bool CORR>
+__global__ void __launch_bounds__(256, 3) kg_stage1_walk(const __grid_constant__ GroupTable<StageJob> g) {
+    pdl_enter();
+    const int total = g.start[g.njobs];
+    for (int b = blockIdx.x; b < total; b += gridDim.x) {
+        const int j = group_job(g.start, g.njobs, b);
+        const StageJob &J = g.jobs[j];
+        k_tiled_body<float, false, false, 32, 8, 0, CORR>(at(g, j, b), J.a, J.U, J.V, J.W, J.nu, J.tau_x, J.tau_z, J.sc,
+                                                          J.kc, J.uo, J.vo, J.wo, J.f1u, J.f1v, J.f1w, J.us, J.vs, J.wsf,
+                                                          J.rhs_only, J.nut_out);
+        cp_async_wait_all();
+        __syncthreads();
+    }
 }
 
 // ---- div u* + forward x transform, length Nx = 2M ----

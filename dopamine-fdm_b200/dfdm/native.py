@@ -37,7 +37,7 @@ EXPORTS = ["dfdm_default_params", "dfdm_last_error", "dfdm_version", "dfdm_creat
            "dfdm_write_box_snapshot", "dfdm_set_landing_times", "dfdm_write_snapshot_ex", "dfdm_get_stage_timing",
            "dfdm_set_sgs_in_tile", "dfdm_get_sgs_in_tile", "dfdm_group_create", "dfdm_group_step_async",
            "dfdm_group_synchronize", "dfdm_group_launch_count", "dfdm_group_destroy", "dfdm_get_stream",
-           "dfdm_group_get_stream", "dfdm_group_set_branch_cells"]
+           "dfdm_group_get_stream", "dfdm_group_set_branch_cells", "dfdm_group_set_stage_tiles"]
 
 
 class DfdmError(RuntimeError):
@@ -124,6 +124,7 @@ def load(build_if_missing: bool = True):
         "dfdm_get_stream": (c_int, [c_void_p, POINTER(c_void_p)]),
         "dfdm_group_get_stream": (c_int, [c_void_p, POINTER(c_void_p)]),
         "dfdm_group_set_branch_cells": (c_int, [c_void_p, ctypes.c_longlong]),
+        "dfdm_group_set_stage_tiles": (c_int, [c_void_p, c_int, c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -479,6 +480,11 @@ class Group:
     def set_branch_cells(self, cells: int) -> None:
         """At most `cells` cells per graph branch (0: one branch per shape class); results do not change."""
         _check(load().dfdm_group_set_branch_cells(self.h, int(cells)))
+
+    def set_stage_tiles(self, kc: int = -1, walk: bool = False) -> None:
+        """Fix the grouped stage launches' tile shape: kc > 0 z-planes per block, 0 each member's own, with walking
+        resident blocks if walk; kc < 0 returns to the group's timed choice.  Results do not change."""
+        _check(load().dfdm_group_set_stage_tiles(self.h, int(kc), int(bool(walk))))
 
     def close(self):
         if getattr(self, "h", None):

@@ -323,10 +323,12 @@ int dfdm_launch_count(dfdm_ctx *ctx, long long *count);
  *    returns it; destroyed with the group).  group_step_async orders itself after the members' earlier work on
  *    their own streams and their later work after it, with events (no host wait), and advances each member's time
  *    by nsteps * dt.  group_synchronize waits for the group's stream.
- *  - Before its first step a group picks the z-chunk of its grouped stage launches per branch, timing the members' own
- *    chunking, the wave model's choice for the branch's tiles together and one chunk per column with stage-1 launches
- *    (which write only F1 and u*, both rewritten by every step); the choice is cached per branch shape and member
- *    count.  Results do not depend on it.
+ *  - Before its first step a group picks the tile shape of its grouped stage launches per branch: the z-chunk (the
+ *    members' own chunking, the wave model's choice for the branch's tiles together, or one chunk per column) and
+ *    whether one block runs per tile or resident blocks walk the tiles.  It times the candidates with stage-1
+ *    launches (which write only F1 and u*, both rewritten by every step) and caches the choice per branch shape and
+ *    member count.  Results do not depend on it.  dfdm_group_set_stage_tiles fixes it instead: kc > 0 planes per
+ *    block (clipped to Nz), 0 each member's own; walk 1 for walking blocks; kc < 0 returns to the timed choice.
  *  - The members must outlive the group's enqueued steps; destroying the group does not wait for them (its graph is
  *    released when they are done) and leaves the members as they are. */
 typedef struct dfdm_group dfdm_group;
@@ -338,6 +340,7 @@ int dfdm_group_get_stream(dfdm_group *group, void **cuda_stream);
  * consecutive members, which overlap on the device as the classes do (0: one branch per class).  Results do not
  * change.  The group's graph is recaptured at its next step. */
 int dfdm_group_set_branch_cells(dfdm_group *group, long long cells);
+int dfdm_group_set_stage_tiles(dfdm_group *group, int kc, int walk);
 /* Number of the library's kernels the group has enqueued (graph replays included). */
 int dfdm_group_launch_count(dfdm_group *group, long long *count);
 int dfdm_group_destroy(dfdm_group *group);

@@ -228,3 +228,24 @@ def test_branch_splitting_leaves_results_unchanged():
         for a, b in zip(st, ref):
             for x, y in zip(a, b):
                 assert np.array_equal(x, y)
+
+
+def test_stage_tile_shapes_leave_results_unchanged():
+    """The grouped stage launches with each member's own z-chunk, with 4 planes per block, with one chunk per column,
+    each with one block per tile and with resident blocks walking the tiles (more tiles than resident blocks at 4
+    planes), and with the group's timed choice: bit-identical states."""
+    cs = [serve.serve_case("tgv" if q % 2 else "chan", 48, 1000.0 + 10 * q, 300 + q) for q in range(6)]
+    ref = None
+    for kc, walk in [(-1, False), (0, False), (4, False), (4, True), (0, True), (1000, True)]:
+        ss = [_first_step(c) for c in cs]
+        with Group(ss) as g:
+            g.set_stage_tiles(kc, walk)
+            g.step(3)
+        st = [s.get_state() for s in ss]
+        for s in ss:
+            s.close()
+        if ref is None:
+            ref = st
+        for a, b in zip(st, ref):
+            for x, y in zip(a, b):
+                assert np.array_equal(x, y), (kc, walk)
