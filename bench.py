@@ -626,6 +626,34 @@ def main():
                        "oracle": "FP64 C++ restatement of the reference, same grid, initial condition and dt"}
         out["accuracy"] = acc
 
+        # the DCT-IV pressure solve of an inflow/outflow-x grid (257 x 128 x 128 independent cells)
+        cc = cases.inflow_outflow(258, 129, 130, grid_type=2)
+        rhs = np.asfortranarray(np.random.default_rng(258).standard_normal(cc.shapes()["rhs_p"]))
+        o = oracle.Oracle(cc)
+        t0 = time.perf_counter()
+        want = o.solve_poisson(rhs)
+        t_oracle = time.perf_counter() - t0
+        o.close()
+        N, nzp = cc.nx - 1, cc.nz - 2
+        cells = N * (cc.ny - 1) * nzp
+        io = {"grid": [N, cc.ny - 1, nzp], "oracle_s_per_solve": t_oracle,
+              "path": "dfdm_solve_poisson (FP64 host arrays in and out, synchronous), host wall clock, best of 3 "
+                      "batches of 10 after 3 warm-up calls"}
+        for prec in ("fp32", "fp64"):
+            with Solver(cc, prec) as sv:
+                for _ in range(3):
+                    got = sv.solve_poisson_equation(rhs)
+                best = 1e30
+                for _ in range(3):
+                    t0 = time.perf_counter()
+                    for _ in range(10):
+                        sv.solve_poisson_equation(rhs)
+                    best = min(best, (time.perf_counter() - t0) / 10)
+            err = float(np.linalg.norm((got[:N, :, :nzp] - want[:N, :, :nzp]).ravel()) /
+                        np.linalg.norm(want[:N, :, :nzp].ravel()))
+            io[prec] = {"ms_per_solve": best * 1e3, "cells_per_s": cells / best, "rel_l2_vs_oracle": err}
+        out["inflow_outflow_poisson"] = io
+
     # ---- serving stream ----
     if not args.no_serve:
         def gather(obj):

@@ -168,6 +168,10 @@ struct dfdm_ctx {
     // two-level register transforms (fft_reg.cuh) where the length has a split; Stockham otherwise
     bool x2 = false, z2 = false, y2 = false;
     bool ys3 = false;                           // walls in y: the staged-column y solve (k_ysolve3) fits
+    // inflow/outflow x (x_bc_type = 1): a context for the DCT-IV pressure solve only (dfdm_solve_poisson); Nx = nx - 1
+    // cells, every x mode kx = 0..Nx-1 in the spectrum, d_dct the Nx x Nx DCT-IV matrix
+    bool xdct = false;
+    void *d_dct = nullptr;   // the DCT-IV matrix, in the context's precision
     int lx2 = 1, lxi2 = 1, thr_z2 = 256, thr_y2 = 256;   // x lines per block: forward, inverse
     size_t smem_x2 = 0, smem_xi2 = 0, smem_z2 = 0, smem_y2 = 0;
     cudaStream_t own_stream = nullptr, stream = nullptr;
@@ -359,6 +363,8 @@ int choose_kc(const Dims &d, int blocks_per_sm, int nsm, int tx = TILE_X, int ty
     return std::max(1, best_kc);
 }
 
+int reduce_grid(const Dims &d);
+
 template <typename T> struct Impl {
     typedef typename cplx_t<T>::type C;
     static constexpr int CT = (sizeof(T) == 8) ? 4 : 8;    // kx columns per block of the column transforms (64 B rows)
@@ -431,6 +437,58 @@ template <typename T> struct Impl {
         return DFDM_OK;
     }
 
+
+    // the transforms of a DCT-IV Poisson context: z (two-level or Stockham) and the y solve
+    static int setup_poisson_only(dfdm_ctx *c) {
+        const Dims &d = c->d;
+        int optin = 0, dev = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        c->tzx = CT;
+        c->smem_z = 2 * (size_t)d.Nz * c->tzx * sizeof(C);
+        if (c->smem_z > (size_t)optin) return fail(DFDM_ERR_UNSUPPORTED, "grid too large for the shared-memory transforms");
+        for (const void *fn : {(const void *)k_col_fft<T, 0, CT>, (const void *)k_col_fft<T, 1, CT>})
+            CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        int rc = DFDM_OK;
+        c->z2 = with_fft2l(d.Nz, [&](auto n) {
+            constexpr int N = decltype(n)::value;
+            c->smem_z2 = (size_t)N * NL * sizeof(C);
+            c->thr_z2 = col_threads(Split<N>::N1, Split<N>::N2);
+            for (const void *fn : {(const void *)k_col2<T, 0, NL, N>, (const void *)k_col2<T, 1, NL, N>})
+                if (!rc && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_z2) != cudaSuccess)
+                    rc = fail(DFDM_ERR_CUDA, "cudaFuncSetAttribute failed");
+        });
+        if (rc) return rc;
+        c->ys3 = false;
+        if (ysolve3_smem<T>(d.Ny) <= (size_t)optin) {
+            CK(cudaFuncSetAttribute(k_ysolve3<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+            int ys_occ = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ys_occ, k_ysolve3<T>, YS_COLS, (int)ysolve3_smem<T>(d.Ny)));
+            c->ys3 = ys_occ >= 3;
+        }
+        return DFDM_OK;
+    }
+    // dfdm_solve_poisson on a DCT-IV context: staging (rhs_p) -> phi -> DCT-IV x -> z -> y solve -> z^-1 -> DCT-IV x
+    // -> phi / (2 nxp nzp) -> staging
+    static int solve_dct(dfdm_ctx *c, int n1, int n2, int n3) {
+        const Dims &d = c->d;
+        const size_t n = (size_t)n1 * n2 * n3;
+        k_unpack_rhs_p<T><<<reduce_grid(d), 256, 0, c->stream>>>(d, n1, n2, c->staging, f(c->phi));
+        CKL();
+        const int nb = (d.Ny * d.Nz + dct_lines<T>() - 1) / dct_lines<T>();
+        const int nt = ((d.Nx + DCT_RK - 1) / DCT_RK + 31) / 32 * 32;
+        k_dct_x<T><<<nb, nt, 0, c->stream>>>(d, f(c->phi), f(c->d_dct), (C *)c->spec);
+        CKL();
+        for (int which : {3, 4, 5})
+            if (int rc = launch(c, which, 1)) return rc;
+        const T inv_norm = (T)(1.0 / (2.0 * (double)d.Nx * (double)d.Nz));
+        k_idct_x<T><<<nb, nt, 0, c->stream>>>(d, (const C *)c->spec, f(c->d_dct), inv_norm, f(c->phi));
+        CKL();
+        k_pack_rhs_p_dct<T><<<(int)std::min<size_t>((n + 255) / 256, 148 * 8), 256, 0, c->stream>>>(d, n1, n2, n3, f(c->phi),
+                                                                                                    c->staging);
+        CKL();
+        return DFDM_OK;
+    }
 
     static int setup_kernels(dfdm_ctx *c) {
         const Dims &d = c->d;
@@ -996,8 +1054,15 @@ template <typename F> int dispatch(dfdm_ctx *c, F fn) {
     return fn(Impl<float>());
 }
 
+int check_any(dfdm_ctx *c) {
+    if (!c) return fail(DFDM_ERR_INVALID, "null context");
+    return DFDM_OK;
+}
 int check_ctx(dfdm_ctx *c) {
     if (!c) return fail(DFDM_ERR_INVALID, "null context");
+    if (c->xdct)
+        return fail(DFDM_ERR_UNSUPPORTED, "a context of an inflow/outflow-x grid (x_bc_type = 1) serves dfdm_solve_poisson "
+                                          "only: the step's stencils need periodic x");
     return DFDM_OK;
 }
 
@@ -1033,8 +1098,15 @@ int validate(const dfdm_grid *g, const dfdm_params *p) {
     if (!g->x || !g->y || !g->z) return fail(DFDM_ERR_INVALID, "grid face arrays must not be NULL");
     if (g->nx % 2 || g->nz % 2) return fail(DFDM_ERR_INVALID, "Error: nx and nz must be even");
     if (g->nx < 6 || g->nz < 6 || g->ny < 4) return fail(DFDM_ERR_INVALID, "grid too small (nx, nz >= 6, ny >= 4)");
-    if (g->x_bc_type != 0 || g->z_bc_type != 0)
-        return fail(DFDM_ERR_UNSUPPORTED, "only periodic x and z are on the single-phase path (x_bc_type = z_bc_type = 0)");
+    if ((g->x_bc_type != 0 && g->x_bc_type != 1) || g->z_bc_type != 0)
+        return fail(DFDM_ERR_UNSUPPORTED, "x_bc_type must be 0 (periodic) or 1 (inflow/outflow) and z_bc_type 0 (periodic)");
+    if (g->x_bc_type == 1) {   // the DCT-IV Poisson path (src/initialization.f90:95-99: walls in y, periodic z)
+        if (g->y_bc_type != 1)
+            return fail(DFDM_ERR_INVALID, "ERROR: GPU_POISSON with y_bc_type=0 (periodic y) requires x_bc_type=0 too");
+        if (g->nx - 1 > DCT_NMAX)
+            return fail(DFDM_ERR_UNSUPPORTED, "inflow/outflow x: at most " + std::to_string(DCT_NMAX) + " x cells (nx <= " +
+                                                  std::to_string(DCT_NMAX + 1) + ")");
+    }
     if (g->y_bc_type != 0 && g->y_bc_type != 1) return fail(DFDM_ERR_INVALID, "y_bc_type must be 0 or 1");
     if (g->y_bc_type == 1 && (g->bc_face_ylo != 1 || g->bc_face_yhi != 1))
         return fail(DFDM_ERR_UNSUPPORTED, "only no-slip y walls (bc_face_ylo = bc_face_yhi = 1) are supported");
@@ -1057,7 +1129,8 @@ int validate(const dfdm_grid *g, const dfdm_params *p) {
     FFTPlan tmp;
     int Nx = g->nx - 2, Nz = g->nz - 2;
     int Ny = g->y_bc_type == 0 ? g->ny - 2 : g->ny - 1;
-    if (!make_fft_plan(Nx / 2, tmp) || !make_fft_plan(Nz, tmp) || (g->y_bc_type == 0 && !make_fft_plan(Ny, tmp)))
+    if ((g->x_bc_type == 0 && !make_fft_plan(Nx / 2, tmp)) || !make_fft_plan(Nz, tmp) ||
+        (g->y_bc_type == 0 && !make_fft_plan(Ny, tmp)))
         return fail(DFDM_ERR_UNSUPPORTED, "transform lengths must factor into 2, 3 and 5");
     if (Ny > MAX_NY) return fail(DFDM_ERR_UNSUPPORTED, "ny too large for the y solve");
     if ((double)Nx * Ny * Nz * 3.0 >= 2147483647.0)
@@ -1080,6 +1153,10 @@ bool fuse_eligible(const dfdm_params *p) {
 // Bytes of the buffers dfdm_create carves from the context's arena (every sub-allocation 256-byte aligned).
 size_t arena_bytes(const dfdm_grid *g, const dfdm_params *p) {
     size_t ts = p->precision == DFDM_FP64 ? 8 : 4;
+    if (g->x_bc_type == 1) {   // the DCT-IV Poisson context: phi, the spectrum, the pivot table, the DCT matrix
+        size_t Nx = g->nx - 1, Nz = g->nz - 2, Ny = g->ny - 1;
+        return Nx * Ny * Nz * (ts + 2 * ts + 8) + Nx * (Nx + 3) * 8 + (1 << 20);
+    }
     size_t Nx = g->nx - 2, Nz = g->nz - 2, Ny = g->y_bc_type == 0 ? g->ny - 2 : g->ny - 1;
     size_t cells = Nx * Ny * Nz, spec = (Nx / 2 + 1) * Ny * Nz;
     size_t n = cells * ts * (3 /*u*/ + 3 /*uo*/ + 3 /*F1*/ + 3 /*u**/ + 1 /*P*/ + 1 /*phi*/ + (p->sgs_model ? 1 : 0) +
@@ -1132,6 +1209,135 @@ int dfdm_footprint_bytes(const dfdm_grid *grid, const dfdm_params *params, size_
     return DFDM_OK;
 }
 
+// A context for the DCT-IV pressure solve of an inflow/outflow-x grid (x_bc_type = 1, walls in y, periodic z): the
+// grid, the y operator, the modified wavenumbers (DCT-IV in x: kxx(i) = 2 (cos(pi (2i+1) / (2 nxp)) - 1) / dx^2,
+// src/initialization.f90:455-457; no null-mode fix, the DCT-IV modes have none, src/projection.f90:292), the pivot table,
+// the z transforms and the DCT-IV matrix.  Only dfdm_solve_poisson (and the stream and lifetime calls) accept it.
+static int create_dct(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
+    dfdm_ctx *c = new dfdm_ctx();
+    c->xdct = true;
+    c->prm = *prm;
+    c->prec = prm->precision;
+    c->ts = c->prec == DFDM_FP64 ? 8 : 4;
+    c->nx = g->nx; c->ny = g->ny; c->nz = g->nz;
+    c->nxg = g->nx + 1; c->nyg = g->ny + 1; c->nzg = g->nz + 1;
+    c->yper = 0;
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return fail(DFDM_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    c->stream = c->own_stream;
+    auto bail = [&](int code) { dfdm_destroy(c); return code; };
+    int rc;
+    c->x.assign(c->nx + 1, 0.0); c->y.assign(c->ny + 1, 0.0); c->z.assign(c->nz + 1, 0.0);
+    for (int i = 1; i <= c->nx; ++i) c->x[i] = g->x[i - 1];
+    for (int j = 1; j <= c->ny; ++j) c->y[j] = g->y[j - 1];
+    for (int k = 1; k <= c->nz; ++k) c->z[k] = g->z[k - 1];
+    centres_of(c->x, c->nx, c->xg); centres_of(c->y, c->ny, c->yg); centres_of(c->z, c->nz, c->zg);
+    double dxmin = 1e300, dzmin = 1e300;
+    for (int i = 1; i <= c->nxg - 1; ++i) dxmin = std::min(dxmin, c->xg[i + 1] - c->xg[i]);
+    for (int k = 1; k <= c->nzg - 1; ++k) dzmin = std::min(dzmin, c->zg[k + 1] - c->zg[k]);
+    c->dx = dxmin; c->dz = dzmin;
+    Dims &d = c->d;
+    d.Nx = c->nx - 1; d.Nz = c->nz - 2; d.Ny = c->ny - 1; d.NyV = d.Ny - 1;
+    d.Nxc = d.Nx;
+    d.yper = 0;
+    d.plane = (long long)d.Nx * d.Ny;
+    d.cells = d.plane * d.Nz;
+    c->arena_size = arena_bytes(g, prm);
+    {
+        cudaError_t e = cudaMalloc((void **)&c->arena, c->arena_size);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            c->arena = nullptr;
+            return bail(fail(DFDM_ERR_NOMEM, std::string("cudaMalloc of the context arena failed: ") + cudaGetErrorString(e)));
+        }
+        c->allocs.push_back(c->arena);
+    }
+    c->in_create = true;
+    if ((rc = dalloc(c, &c->phi, (size_t)d.cells * c->ts))) return bail(rc);
+    if ((rc = dalloc(c, &c->spec, (size_t)d.Nxc * d.Ny * d.Nz * 2 * c->ts))) return bail(rc);
+    const int nxp = d.Nx, nzp = d.Nz;
+    std::vector<double> kxx(d.Nxc), kzz(d.Nz), kyy(1, 0.0);
+    for (int i = 0; i < d.Nxc; ++i)
+        kxx[i] = 2.0 * (std::cos(PI * (double)(2 * i + 1) / (2.0 * (double)nxp)) - 1.0) / std::pow(c->dx, 2.0);
+    const int cz = (int)std::ceil((double)nzp / 2.0);
+    for (int k = 0; k < nzp; ++k) {
+        double kk = (k <= cz) ? (double)k : (double)(-nzp + k);
+        kzz[k] = 2.0 * (std::cos(2.0 * PI * kk / (double)nzp) - 1.0) / std::pow(c->dz, 2.0);
+    }
+    std::vector<double> lo(d.Ny, 0.0), di(d.Ny, 0.0), up(d.Ny, 0.0);
+    {   // Dyy (src/initialization.f90:507-535)
+        const std::vector<double> &y = c->y, &yg = c->yg;
+        const int nyg = c->nyg;
+        auto abc = [&](int j, double &a, double &b, double &cc) {
+            a = 1.0 / (y[j] - y[j - 1]) / (yg[j + 1] - yg[j]);
+            b = 1.0 / (y[j] - y[j - 1]) * (-1.0 / (yg[j + 1] - yg[j]) - 1.0 / (yg[j] - yg[j - 1]));
+            cc = 1.0 / (y[j] - y[j - 1]) / (yg[j] - yg[j - 1]);
+        };
+        for (int j = 3; j <= nyg - 2; ++j) {
+            double a, b, cc; abc(j, a, b, cc);
+            up[j - 2] = a; lo[j - 2] = cc; di[j - 2] = b;
+        }
+        double a, b, cc;
+        abc(2, a, b, cc); di[0] = b + cc; up[0] = a;
+        abc(nyg - 1, a, b, cc); di[nyg - 3] = a + b; lo[nyg - 3] = cc;
+    }
+    void *tmp = nullptr;
+    if ((rc = upload_as<double>(c, &tmp, kxx))) return bail(rc);
+    c->d_kxx = (double *)tmp;
+    if ((rc = upload_as<double>(c, &tmp, kzz))) return bail(rc);
+    c->d_kzz = (double *)tmp;
+    if ((rc = upload_as<double>(c, &tmp, kyy))) return bail(rc);
+    c->d_kyy = (double *)tmp;
+    if ((rc = upload_as<double>(c, &tmp, lo))) return bail(rc);
+    c->d_lo = (double *)tmp;
+    if ((rc = upload_as<double>(c, &tmp, di))) return bail(rc);
+    c->d_di = (double *)tmp;
+    if ((rc = upload_as<double>(c, &tmp, up))) return bail(rc);
+    c->d_up = (double *)tmp;
+    {
+        std::vector<double> rpiv((size_t)d.Nxc * d.Ny * d.Nz);
+        for (int kz = 0; kz < d.Nz; ++kz)
+            for (int kx = 0; kx < d.Nxc; ++kx) {
+                const double lam = kxx[kx] + kzz[kz];
+                double D = di[0] + lam;
+                const size_t b = (size_t)kz * d.Ny * d.Nxc + kx;
+                rpiv[b] = 1.0 / D;
+                for (int r = 1; r < d.Ny; ++r) {
+                    const double m = lo[r] / D;
+                    D = (di[r] + lam) - m * up[r - 1];
+                    if (D == 0.0) return bail(fail(DFDM_ERR_INVALID, "singular pressure operator"));
+                    rpiv[b + (size_t)r * d.Nxc] = 1.0 / D;
+                }
+            }
+        if ((rc = upload_as<double>(c, &tmp, rpiv))) return bail(rc);
+        c->d_rpiv = (double *)tmp;
+    }
+    {   // C[k][n] = 2 cos(pi (2n+1)(2k+1) / (4 nxp)), the angle reduced exactly modulo 2 pi (8 nxp quarter-steps);
+        // rows padded with zeros to the kernels' 16-byte pitch
+        const long P = 8L * nxp;
+        const long pitch = c->prec == DFDM_FP64 ? dct_pitch<double>(nxp) : dct_pitch<float>(nxp);
+        std::vector<double> cs((size_t)P), C((size_t)(nxp * pitch), 0.0);
+        for (long m = 0; m < P; ++m) cs[(size_t)m] = std::cos(PI * (double)m / (4.0 * (double)nxp));
+        for (long k = 0; k < nxp; ++k)
+            for (long n = 0; n < nxp; ++n) C[(size_t)(k * pitch + n)] = 2.0 * cs[(size_t)(((2 * n + 1) * (2 * k + 1)) % P)];
+        if ((rc = c->prec == DFDM_FP64 ? upload_as<double>(c, &tmp, C) : upload_as<float>(c, &tmp, C))) return bail(rc);
+        c->d_dct = tmp;
+    }
+    make_fft_plan(d.Nz, c->plan_z);
+    auto tws = [&](void **dst, int n, int count) {
+        return c->prec == DFDM_FP64 ? upload_twiddles<double>(c, dst, n, count) : upload_twiddles<float>(c, dst, n, count);
+    };
+    if ((rc = tws(&c->tw_z, d.Nz, d.Nz))) return bail(rc);
+    c->in_create = false;
+    rc = dispatch(c, [&](auto impl) { return decltype(impl)::setup_poisson_only(c); });
+    if (rc) return bail(rc);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(DFDM_ERR_CUDA, "set-up synchronisation failed"));
+    *out = c;
+    return DFDM_OK;
+}
+
 int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
     g_err.clear();
     if (!out) return fail(DFDM_ERR_INVALID, "null output pointer");
@@ -1143,6 +1349,7 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
         cudaGetLastError();
         return fail(DFDM_ERR_CUDA, "no CUDA device: the dfdm library has no CPU fallback");
     }
+    if (g->x_bc_type == 1) return create_dct(g, prm, out);
     dfdm_ctx *c = new dfdm_ctx();
     c->prm = *prm;
     c->prec = prm->precision;
@@ -1395,14 +1602,14 @@ int dfdm_destroy(dfdm_ctx *c) {
 }
 
 int dfdm_get_stream(dfdm_ctx *c, void **s) {
-    if (int rc = check_ctx(c)) return rc;
+    if (int rc = check_any(c)) return rc;
     if (!s) return fail(DFDM_ERR_INVALID, "null output");
     *s = (void *)c->stream;
     return DFDM_OK;
 }
 
 int dfdm_set_stream(dfdm_ctx *c, void *s) {
-    if (int rc = check_ctx(c)) return rc;
+    if (int rc = check_any(c)) return rc;
     CK(cudaStreamSynchronize(c->stream));
     c->stream = s ? (cudaStream_t)s : c->own_stream;
     destroy_graph(c);
@@ -1423,7 +1630,7 @@ static int check_err_flag(dfdm_ctx *c) {
 extern "C" {
 
 int dfdm_synchronize(dfdm_ctx *c) {
-    if (int rc = check_ctx(c)) return rc;
+    if (int rc = check_any(c)) return rc;
     CK(cudaStreamSynchronize(c->stream));
     if (c->cin) CK(cudaStreamSynchronize(c->cin));
     if (c->cout) CK(cudaStreamSynchronize(c->cout));
@@ -1902,7 +2109,7 @@ int dfdm_compute_projection_step(dfdm_ctx *c, int save_p) {
 
 int dfdm_solve_poisson(dfdm_ctx *c, const double *rhs_in, double *phi_out) {
     g_err.clear();
-    if (int rc = check_ctx(c)) return rc;
+    if (int rc = check_any(c)) return rc;
     if (!rhs_in || !phi_out) return fail(DFDM_ERR_INVALID, "null array");
     const Dims &d = c->d;
     int n1 = c->nxg - 1, n2 = c->nyg - 2, n3 = c->nzg - 1;
@@ -1910,6 +2117,15 @@ int dfdm_solve_poisson(dfdm_ctx *c, const double *rhs_in, double *phi_out) {
     int rc = ensure_staging(c, n);
     if (rc) return rc;
     CK(cudaMemcpyAsync(c->staging, rhs_in, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (c->xdct) {
+        long long before = g_launches;
+        rc = dispatch(c, [&](auto impl) { return decltype(impl)::solve_dct(c, n1, n2, n3); });
+        c->launches += g_launches - before;
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(phi_out, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return DFDM_OK;
+    }
     rc = dispatch(c, [&](auto impl) {
         typedef decltype(impl) I;
         typedef typename std::remove_pointer<decltype(I::f(nullptr))>::type T;
@@ -2508,7 +2724,7 @@ int dfdm_get_stage_timing(dfdm_ctx *c, int variant, double *ms) {
 }
 
 int dfdm_launch_count(dfdm_ctx *c, long long *count) {
-    if (int rc = check_ctx(c)) return rc;
+    if (int rc = check_any(c)) return rc;
     if (!count) return fail(DFDM_ERR_INVALID, "null output");
     *count = c->launches;
     return DFDM_OK;

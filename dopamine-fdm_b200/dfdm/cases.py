@@ -34,6 +34,7 @@ class Case:
     grid_type: int = 1           # 1 uniform y, 2 symmetric tanh
     alpha_grid: float = 0.0
     y_bc_type: int = 1           # 0 periodic, 1 walls
+    x_bc_type: int = 0           # 0 periodic, 1 inflow/outflow (the DCT-IV Poisson path only)
     nu: float = 1e-3
     dt: float = 1e-3
     dPdx: float = 0.0
@@ -326,6 +327,13 @@ def chan_les_vreman_small() -> Case:
     """The wall-modelled LES regression grid with the Vreman closure (sgs_model = 1, Cs_vreman = 0.17) in place of
     AMD: the other eddy-viscosity branch of compute_vreman (src/sgs_model.f90:212-216)."""
     return chan_les_amd_small().with_(name="chan_les_vreman_small", sgs_model=1)
+
+
+def inflow_outflow(nx: int = 18, ny: int = 17, nz: int = 18, grid_type: int = 2, name: Optional[str] = None) -> Case:
+    """An inflow/outflow-x grid (x_bc_type = 1) with y walls and periodic z, 3 x 2 x 1.5: the pressure solve of the
+    DCT-IV path (src/projection.f90:124-130,334-343) only; such a case does not step."""
+    return Case(name=name or f"inflow_outflow{nx}", nx=nx, ny=ny, nz=nz, Lx_i=3.0, Ly_i=2.0, Lz_i=1.5,
+                grid_type=grid_type, alpha_grid=2.0, y_bc_type=1, x_bc_type=1, nu=0.01, dt=0.002, ic="zero")
 
 
 CONFIGS = {"tgv64": tgv, "chan180": chan180, "les395": les395, "chan550": chan550,

@@ -52,7 +52,7 @@ typedef struct dfdm_grid {
     const double *x;           /* x(1:nx) face coordinates, uniform */
     const double *y;           /* y(1:ny) face coordinates, may be stretched */
     const double *z;           /* z(1:nz) face coordinates, uniform */
-    int x_bc_type;             /* 0 periodic (the only value on this path) */
+    int x_bc_type;             /* 0 periodic; 1 inflow/outflow (a context for dfdm_solve_poisson only, see below) */
     int y_bc_type;             /* 0 periodic, 1 walls */
     int z_bc_type;             /* 0 periodic (the only value on this path) */
     int bc_face_ylo, bc_face_yhi; /* 1 no-slip (the only value on this path) */
@@ -93,7 +93,11 @@ const char *dfdm_last_error(void);
 /* Library version string. */
 const char *dfdm_version(void);
 
-/* ---- lifetime: replaces initialize's device part (src/initialization.f90:37-862) ---- */
+/* ---- lifetime: replaces initialize's device part (src/initialization.f90:37-862) ----
+ * x_bc_type = 1 (inflow/outflow x; needs y walls, y_bc_type = 1, and nx - 1 <= 257) creates a context for the
+ * DCT-IV pressure solve alone (src/projection.f90:124-130,334-343): dfdm_solve_poisson, the stream calls,
+ * dfdm_synchronize, dfdm_launch_count and dfdm_destroy accept it, every other entry point returns
+ * DFDM_ERR_UNSUPPORTED (the inflow/outflow step, boundary conditions and convective outflow are not built). */
 int dfdm_create(const dfdm_grid *grid, const dfdm_params *params, dfdm_ctx **out);
 int dfdm_destroy(dfdm_ctx *ctx);
 /* Bytes of device memory a context of this grid and precision would hold (serving admission). */
@@ -146,7 +150,11 @@ int dfdm_apply_boundary_conditions(dfdm_ctx *ctx, int after_projection);
  * resident velocity. save_p = 1 also stores P = phi/(dt*3/4) as the third RK stage does. */
 int dfdm_compute_projection_step(dfdm_ctx *ctx, int save_p);
 /* solve_poisson_equation's solve alone (src/projection.f90:100-382): rhs_p in, pseudo-pressure out, both in
- * the reference shape (2:nxg,2:nyg-1,2:nzg); the output ghost planes follow apply_periodic_xz_pressure. */
+ * the reference shape (2:nxg,2:nyg-1,2:nzg); the output ghost planes follow apply_periodic_xz_pressure.
+ * On an inflow/outflow-x context (x_bc_type = 1) the x transform is the DCT-IV (FFTW REDFT11) of the nx - 1
+ * cells 2:nxg-1 with kxx(i) = 2 (cos(pi (2i+1) / (2 (nx-1))) - 1) / dx^2 and no null-mode fix; the output's
+ * plane i = nxg keeps the input, as the reference's array does, and the z plane nzg (unset by the reference's
+ * apply_periodic_xz_pressure at one rank) keeps the input too. */
 int dfdm_solve_poisson(dfdm_ctx *ctx, const double *rhs_p_in, double *phi_out);
 /* No counterpart in the reference: dfdm_solve_poisson with no device allocation in the call.
  * dfdm_solve_poisson grows a per-context staging buffer with cudaMalloc on first use (and frees and regrows it,

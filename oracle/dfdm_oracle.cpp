@@ -232,15 +232,24 @@ struct Oracle {
         for (int k = 1; k <= nzg - 1; ++k) dzmin = std::min(dzmin, zg[k + 1] - zg[k]);
         Lx = x[nx] - x[1]; Ly = y[ny] - y[1]; Lz = z[nz] - z[1];
         dx = dxmin; dz = dzmin;
-        nxp = nxm - 1;   // x periodic
+        // x periodic: the last interior cell duplicates the first (nxp = nxm - 1); inflow/outflow x (x_bc_type 1,
+        // the DCT-IV path): all nxm cells (src/initialization.f90:330-336)
+        nxp = x_bc_type == 0 ? nxm - 1 : nxm;
         nzp = nzm - 1;   // z periodic
         int mx = nxp - 1, mz = nzp - 1;
         kxx.assign(mx + 1, 0.0); kzz.assign(mz + 1, 0.0);
         int cx = (int)std::ceil((double)nxp / 2.0), cz = (int)std::ceil((double)nzp / 2.0);
-        for (int i = 0; i <= cx; ++i)
-            kxx[i] = 2.0 * (std::cos(2.0 * pi * (double)i / (double)nxp) - 1.0) / std::pow(dx, 2.0);
-        for (int i = cx + 1; i <= mx; ++i)
-            kxx[i] = 2.0 * (std::cos(2.0 * pi * (double)(-nxp + i) / (double)nxp) - 1.0) / std::pow(dx, 2.0);
+        if (x_bc_type == 0) {
+            for (int i = 0; i <= cx; ++i)
+                kxx[i] = 2.0 * (std::cos(2.0 * pi * (double)i / (double)nxp) - 1.0) / std::pow(dx, 2.0);
+            for (int i = cx + 1; i <= mx; ++i)
+                kxx[i] = 2.0 * (std::cos(2.0 * pi * (double)(-nxp + i) / (double)nxp) - 1.0) / std::pow(dx, 2.0);
+        } else {   // DCT-IV (quarter-wave) modified wavenumber (src/initialization.f90:455-457)
+            for (int i = 0; i <= mx; ++i)
+                kxx[i] = 2.0 * (std::cos(pi * (double)(2 * i + 1) / (2.0 * (double)nxp)) - 1.0) / std::pow(dx, 2.0);
+            dct_cos.assign((size_t)8 * nxp, 0.0);
+            for (int m = 0; m < 8 * nxp; ++m) dct_cos[m] = std::cos(pi * (double)m / (4.0 * (double)nxp));
+        }
         for (int k = 0; k <= cz; ++k)
             kzz[k] = 2.0 * (std::cos(2.0 * pi * (double)k / (double)nzp) - 1.0) / std::pow(dz, 2.0);
         for (int k = cz + 1; k <= mz; ++k)
@@ -308,8 +317,24 @@ struct Oracle {
         tau_x.init(1, nx, 1, 2, 1, nzg); tau_z.init(1, nxg, 1, 2, 1, nz);
         wmf_ux.init(1, nx, 1, 2, 1, nzg); wmf_wx.init(1, nx, 1, 2, 1, nzg); wmf_tx.init(1, nx, 1, 2, 1, nzg);
         wmf_uz.init(1, nxg, 1, 2, 1, nz); wmf_wz.init(1, nxg, 1, 2, 1, nz); wmf_tz.init(1, nxg, 1, 2, 1, nz);
-        fx.init(nxp); fz.init(nzp);
+        if (x_bc_type == 0) fx.init(nxp);
+        fz.init(nzp);
         return 0;
+    }
+
+    // DCT-IV of one x line, unnormalised (FFTW REDFT11, which the reference's CPU build plans; its GPU build forms the
+    // same coefficients through a zero-padded 4N-point FFT, src/poisson_gpu.f90:139-180):
+    //   Y_k = 2 sum_n x_n cos(pi (2n+1)(2k+1) / (4N)),  k = 0..N-1.
+    // Computed by the definition with the cosines tabulated at the exact multiples m = (2n+1)(2k+1) mod 8N of pi/(4N).
+    // It is its own inverse up to 2N.
+    std::vector<double> dct_cos;   // cos(pi m / (4 nxp)), m = 0..8 nxp - 1
+    void dct4(const double *in, double *out) const {
+        const long N = nxp, P = 8 * N;
+        for (long k = 0; k < N; ++k) {
+            double acc = 0.0;
+            for (long n = 0; n < N; ++n) acc += in[n] * dct_cos[(size_t)(((2 * n + 1) * (2 * k + 1)) % P)];
+            out[k] = 2.0 * acc;
+        }
     }
 
     // ---- boundary conditions (src/boundary_conditions.f90:186-260, one rank) ----
@@ -968,9 +993,20 @@ struct Oracle {
         for (long k = 0; k < n3; ++k)
             for (long j = 0; j < n2; ++j)
                 for (long i = 0; i < n1; ++i) c[id(i, j, k)] = cplx(rhs_p((int)i + 2, (int)j + 2, (int)k + 2), 0.0);
-        // forward x (batched over (j,k)), then z
+        // forward x (batched over (j,k)): FFT, or with inflow/outflow x the real DCT-IV (src/projection.f90:124-130)
+        if (x_bc_type == 0) {
 #pragma omp parallel for
-        for (long jk = 0; jk < n2 * n3; ++jk) fx.exec(&c[(size_t)(jk * n1)], 1, false);
+            for (long jk = 0; jk < n2 * n3; ++jk) fx.exec(&c[(size_t)(jk * n1)], 1, false);
+        } else {
+#pragma omp parallel for
+            for (long jk = 0; jk < n2 * n3; ++jk) {
+                std::vector<double> a((size_t)n1), b((size_t)n1);
+                for (long i = 0; i < n1; ++i) a[i] = c[(size_t)(jk * n1 + i)].real();
+                dct4(a.data(), b.data());
+                for (long i = 0; i < n1; ++i) c[(size_t)(jk * n1 + i)] = cplx(b[i], 0.0);
+            }
+        }
+        // then z
 #pragma omp parallel for
         for (long ij = 0; ij < n1 * n2; ++ij) fz.exec(&c[(size_t)ij], n1 * n2, false);
         if (y_bc_type == 0) {
@@ -1014,15 +1050,29 @@ struct Oracle {
         }
 #pragma omp parallel for
         for (long ij = 0; ij < n1 * n2; ++ij) fz.exec(&c[(size_t)ij], n1 * n2, true);
+        if (x_bc_type == 0) {
 #pragma omp parallel for
-        for (long jk = 0; jk < n2 * n3; ++jk) fx.exec(&c[(size_t)(jk * n1)], 1, true);
-        double norm = (double)((long)nxp * (long)nzp);
-        for (long k = 0; k < n3; ++k)
-            for (long j = 0; j < n2; ++j)
-                for (long i = 0; i < n1; ++i) rhs_p((int)i + 2, (int)j + 2, (int)k + 2) = c[id(i, j, k)].real() / norm;
-        // apply_periodic_xz_pressure (:441-500), one rank
-        for (int k = 2; k <= nzg; ++k)
-            for (int j = 2; j <= nyg - 1; ++j) rhs_p(nxg - 1, j, k) = rhs_p(2, j, k);
+            for (long jk = 0; jk < n2 * n3; ++jk) fx.exec(&c[(size_t)(jk * n1)], 1, true);
+            double norm = (double)((long)nxp * (long)nzp);
+            for (long k = 0; k < n3; ++k)
+                for (long j = 0; j < n2; ++j)
+                    for (long i = 0; i < n1; ++i) rhs_p((int)i + 2, (int)j + 2, (int)k + 2) = c[id(i, j, k)].real() / norm;
+        } else {   // real part, DCT-IV again, / (2 nxp nzp) (src/projection.f90:334-343)
+            const double norm = 2.0 * (double)nxp * (double)nzp;
+#pragma omp parallel for
+            for (long jk = 0; jk < n2 * n3; ++jk) {
+                std::vector<double> a((size_t)n1), b((size_t)n1);
+                for (long i = 0; i < n1; ++i) a[i] = c[(size_t)(jk * n1 + i)].real();
+                dct4(a.data(), b.data());
+                const long j = jk % n2, k = jk / n2;
+                for (long i = 0; i < n1; ++i) rhs_p((int)i + 2, (int)j + 2, (int)k + 2) = b[i] / norm;
+            }
+        }
+        // apply_periodic_xz_pressure (:441-500), one rank: the x copy only with periodic x (inflow/outflow x leaves
+        // the plane nxg as it was)
+        if (x_bc_type == 0)
+            for (int k = 2; k <= nzg; ++k)
+                for (int j = 2; j <= nyg - 1; ++j) rhs_p(nxg - 1, j, k) = rhs_p(2, j, k);
         for (int j = 2; j <= nyg - 1; ++j)
             for (int i = 2; i <= nxg - 1; ++i) rhs_p(i, j, nzp + 2) = rhs_p(i, j, 2);
         if (y_bc_type == 0)
@@ -1321,8 +1371,18 @@ int orc_grid_array(void *h, int which, double *out) {
     case 5: for (int j = 2; j <= o->nyg - 1; ++j) out[j - 2] = o->Dyy_d[j]; return o->nyg - 2;
     case 6: for (int j = 1; j <= o->ny; ++j) out[j - 1] = o->wy0[j]; return o->ny;
     case 7: out[0] = o->dx; out[1] = o->dz; return 2;
+    case 8: for (int j = 2; j <= o->nyg - 1; ++j) out[j - 2] = o->Dyy_l[j]; return o->nyg - 2;   // Dyy(j, j-1)
+    case 9: for (int j = 2; j <= o->nyg - 1; ++j) out[j - 2] = o->Dyy_u[j]; return o->nyg - 2;   // Dyy(j, j+1)
     }
     return 0;
+}
+
+// the DCT-IV of one x line of an inflow/outflow-x oracle (nxp values in, nxp out); -1 for a periodic-x oracle
+int orc_dct4(void *h, const double *in, double *out) {
+    Oracle *o = (Oracle *)h;
+    if (o->x_bc_type != 1) return -1;
+    o->dct4(in, out);
+    return o->nxp;
 }
 // raw FFT and zgtsv entry points for cross-checks against numpy / scipy
 void orc_fft(int n, double *re_im, int inverse) {

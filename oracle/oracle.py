@@ -64,6 +64,8 @@ def lib():
         L.orc_gtsv_swaps.argtypes = [c_void_p]
         L.orc_grid_array.restype = c_int
         L.orc_grid_array.argtypes = [c_void_p, c_int, POINTER(c_double)]
+        L.orc_dct4.restype = c_int
+        L.orc_dct4.argtypes = [c_void_p, POINTER(c_double), POINTER(c_double)]
         L.orc_fft.argtypes = [c_int, POINTER(c_double), c_int]
         L.orc_zgtsv.restype = c_int
         L.orc_zgtsv.argtypes = [c_int] + [POINTER(c_double)] * 4
@@ -214,6 +216,15 @@ class Oracle:
 
     def gtsv_swaps(self) -> int:
         return int(lib().orc_gtsv_swaps(self.h))
+
+    def dct4(self, line) -> np.ndarray:
+        """The DCT-IV of one x line (inflow/outflow x only): 2 sum_n x_n cos(pi (2n+1)(2k+1) / (4N))."""
+        a = np.ascontiguousarray(line, dtype=np.float64)
+        out = np.zeros_like(a)
+        n = lib().orc_dct4(self.h, dptr(a), dptr(out))
+        if n != a.size:
+            raise ValueError("the oracle's DCT-IV needs an inflow/outflow-x case of the line's length")
+        return out
 
     def grid_array(self, which: int) -> np.ndarray:
         out = np.zeros(max(self.case.nx, self.case.ny, self.case.nz) + 8)
