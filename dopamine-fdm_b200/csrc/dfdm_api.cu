@@ -475,8 +475,7 @@ template <typename T> struct Impl {
         const size_t n = (size_t)n1 * n2 * n3;
         k_unpack_rhs_p<T><<<reduce_grid(d), 256, 0, c->stream>>>(d, n1, n2, c->staging, f(c->phi));
         CKL();
-        const int nb = (d.Ny * d.Nz + dct_lines<T>() - 1) / dct_lines<T>();
-        const int nt = ((d.Nx + DCT_RK - 1) / DCT_RK + 31) / 32 * 32;
+        const int nb = (d.Ny * d.Nz + DCT_LINES - 1) / DCT_LINES, nt = (d.Nx + 31) / 32 * 32;
         k_dct_x<T><<<nb, nt, 0, c->stream>>>(d, f(c->phi), f(c->d_dct), (C *)c->spec);
         CKL();
         for (int which : {3, 4, 5})
@@ -1155,7 +1154,7 @@ size_t arena_bytes(const dfdm_grid *g, const dfdm_params *p) {
     size_t ts = p->precision == DFDM_FP64 ? 8 : 4;
     if (g->x_bc_type == 1) {   // the DCT-IV Poisson context: phi, the spectrum, the pivot table, the DCT matrix
         size_t Nx = g->nx - 1, Nz = g->nz - 2, Ny = g->ny - 1;
-        return Nx * Ny * Nz * (ts + 2 * ts + 8) + Nx * (Nx + 3) * 8 + (1 << 20);
+        return Nx * Ny * Nz * (ts + 2 * ts + 8) + Nx * Nx * 8 + (1 << 20);
     }
     size_t Nx = g->nx - 2, Nz = g->nz - 2, Ny = g->y_bc_type == 0 ? g->ny - 2 : g->ny - 1;
     size_t cells = Nx * Ny * Nz, spec = (Nx / 2 + 1) * Ny * Nz;
@@ -1314,14 +1313,12 @@ static int create_dct(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out
         if ((rc = upload_as<double>(c, &tmp, rpiv))) return bail(rc);
         c->d_rpiv = (double *)tmp;
     }
-    {   // C[k][n] = 2 cos(pi (2n+1)(2k+1) / (4 nxp)), the angle reduced exactly modulo 2 pi (8 nxp quarter-steps);
-        // rows padded with zeros to the kernels' 16-byte pitch
+    {   // C[k][n] = 2 cos(pi (2n+1)(2k+1) / (4 nxp)), the angle reduced exactly modulo 2 pi (8 nxp quarter-steps)
         const long P = 8L * nxp;
-        const long pitch = c->prec == DFDM_FP64 ? dct_pitch<double>(nxp) : dct_pitch<float>(nxp);
-        std::vector<double> cs((size_t)P), C((size_t)(nxp * pitch), 0.0);
+        std::vector<double> cs((size_t)P), C((size_t)(nxp * nxp));
         for (long m = 0; m < P; ++m) cs[(size_t)m] = std::cos(PI * (double)m / (4.0 * (double)nxp));
         for (long k = 0; k < nxp; ++k)
-            for (long n = 0; n < nxp; ++n) C[(size_t)(k * pitch + n)] = 2.0 * cs[(size_t)(((2 * n + 1) * (2 * k + 1)) % P)];
+            for (long n = 0; n < nxp; ++n) C[(size_t)(k * nxp + n)] = 2.0 * cs[(size_t)(((2 * n + 1) * (2 * k + 1)) % P)];
         if ((rc = c->prec == DFDM_FP64 ? upload_as<double>(c, &tmp, C) : upload_as<float>(c, &tmp, C))) return bail(rc);
         c->d_dct = tmp;
     }

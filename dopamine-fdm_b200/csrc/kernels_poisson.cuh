@@ -323,122 +323,98 @@ __global__ void __launch_bounds__(YS_COLS) k_ysolve3(Dims d, typename cplx_t<T>:
 // The real DCT-IV of every x line, Y_k = 2 sum_n x_n cos(pi (2n+1)(2k+1) / (4N)) (FFTW REDFT11, which the reference's
 // CPU build plans and its GPU build forms through a zero-padded 4N-point FFT), as a product with the N x N matrix
 // C[k][n] of those coefficients (symmetric; built on the host in FP64 with the angle reduced exactly, stored in the
-// context's precision T with rows padded to a 16-byte pitch).  N = nx - 1 is odd and can be prime (257), so the
-// matrix product replaces a fast transform.  A block stages L lines in shared memory as [n][line] (the lines' values
-// at one n contiguous, read as vectors at one address by every thread of a warp) and streams the rows of C through
-// two shared buffers of NB rows with 16-byte cp.async, the next chunk in flight while the current one is used;
-// thread t of kt threads produces outputs t, t + kt, t + 2 kt, t + 3 kt of all L lines and accumulates in T.
-// Measured at 257 x 128 x 128 FP32: one output per thread with C read through L1 ran at the shared-memory bound of
-// the broadcast loads (127 us); four outputs per thread with C through L1 waited on those loads (172 us).
-// Forward: x lines (the real field, x fastest) to the spectrum's kx columns (imaginary parts zero, kx = 0..N-1);
-// inverse: the real parts of the spectrum's lines to the real field, times 1 / (2 N nzp) (the DCT-IV is its own
-// inverse up to 2N).
-constexpr int DCT_RK = 4, DCT_NMAX = 257, DCT_THREADS = 96;   // outputs per thread; the longest line; threads
-constexpr int DCT_PMAX = (DCT_NMAX + 3) / 4 * 4;               // the longest padded row
-static_assert(DCT_THREADS >= ((DCT_NMAX + DCT_RK - 1) / DCT_RK + 31) / 32 * 32, "threads for the longest line");
+// context's precision T).  N = nx - 1 is odd and can be prime (257), so the matrix product replaces a fast transform.
+// A block stages DCT_LINES lines in shared memory as [n][line] (the lines' values at one n contiguous, read as
+// vectors at one address by every thread of a warp); thread t < N produces output t of all of them, reading row n of
+// C at consecutive t (coalesced, through L1) and accumulating in T.  Forward: x lines (the real field, x fastest) to
+// the spectrum's kx columns (imaginary parts zero, kx = 0..N-1); inverse: the real parts of the spectrum's lines to
+// the real field, times 1 / (2 N nzp) (the DCT-IV is its own inverse up to 2N).
+constexpr int DCT_LINES = 16, DCT_NMAX = 257, DCT_THREADS = 288;   // lines per block; the longest line; threads
+static_assert(DCT_THREADS >= (DCT_NMAX + 31) / 32 * 32, "one thread per output of the longest line");
 template <typename T> struct DctVec;
-template <> struct DctVec<float> { typedef float4 type; static constexpr int W = 4, L = 16, NB = 8; };
-template <> struct DctVec<double> { typedef double2 type; static constexpr int W = 2, L = 8, NB = 4; };
+template <> struct DctVec<float> { typedef float4 type; static constexpr int W = 4; };
+template <> struct DctVec<double> { typedef double2 type; static constexpr int W = 2; };
 template <typename T>
-__host__ __device__ constexpr int dct_lines() { return DctVec<T>::L; }
-// the row pitch of the stored matrix, in elements: rows start on 16-byte boundaries
-template <typename T>
-__host__ __device__ constexpr int dct_pitch(int N) { return (N + DctVec<T>::W - 1) / DctVec<T>::W * DctVec<T>::W; }
-// acc[j][l] = sum_n C[n][t + j kt] ln[n][l] over the block's L lines
-template <typename T>
-__device__ __forceinline__ void dct_tile(const T *__restrict__ C, int N, int t, int kt, const T *__restrict__ ln,
-                                         T *__restrict__ cs, T (&acc)[DCT_RK][DctVec<T>::L]) {
+__device__ __forceinline__ void dct_accumulate(T cv, const T *__restrict__ v, T (&acc)[DCT_LINES]) {
     typedef typename DctVec<T>::type V;
-    constexpr int W = DctVec<T>::W, L = DctVec<T>::L, NB = DctVec<T>::NB;
-    const int P = dct_pitch<T>(N), nv = P / W, nchunks = (N + NB - 1) / NB;
-    auto issue = [&](int ch, int buf) {
-        const int n0 = ch * NB, rows = min(NB, N - n0);
-        for (int e = threadIdx.x; e < rows * nv; e += blockDim.x) {
-            const int r = e / nv, v = e - r * nv;
-            cp_async<16>(cs + (buf * NB + r) * DCT_PMAX + v * W, C + (size_t)(n0 + r) * P + v * W);
-        }
-        cp_async_commit();
+    constexpr int W = DctVec<T>::W;
+#pragma unroll
+    for (int q = 0; q < DCT_LINES / W; ++q) {
+        const V x = reinterpret_cast<const V *>(v)[q];
+        const T *xs = reinterpret_cast<const T *>(&x);
+#pragma unroll
+        for (int w = 0; w < W; ++w) acc[q * W + w] = fma(cv, xs[w], acc[q * W + w]);
+    }
+}
+// acc[l] += sum_n col[n * N] * ln[n][l]: the column's coefficients are loaded DCT_AHEAD at a time, one group ahead of
+// the group being accumulated (the matrix is shared by every block and mostly served by L1).
+constexpr int DCT_AHEAD = 8;
+template <typename T>
+__device__ __forceinline__ void dct_column(const T *__restrict__ col, int N, const T *__restrict__ ln, T (&acc)[DCT_LINES]) {
+    T ca[DCT_AHEAD], cb[DCT_AHEAD];
+    auto load = [&](T (&c)[DCT_AHEAD], int n0) {
+#pragma unroll
+        for (int q = 0; q < DCT_AHEAD; ++q) c[q] = __ldg(col + (size_t)(n0 + q) * N);
     };
-    int kj[DCT_RK];
+    auto proc = [&](const T (&c)[DCT_AHEAD], int n0) {
 #pragma unroll
-    for (int j = 0; j < DCT_RK; ++j) {
-        kj[j] = t + j * kt;
-        if (kj[j] >= N) kj[j] = 0;   // a valid address; the output is not written
-#pragma unroll
-        for (int l = 0; l < L; ++l) acc[j][l] = T(0);
+        for (int q = 0; q < DCT_AHEAD; ++q) dct_accumulate<T>(c[q], ln + (n0 + q) * DCT_LINES, acc);
+    };
+    const int full = N / DCT_AHEAD * DCT_AHEAD;
+    int n0 = 0;
+    if (full > 0) load(ca, 0);
+    for (; n0 + 2 * DCT_AHEAD <= full; n0 += 2 * DCT_AHEAD) {
+        load(cb, n0 + DCT_AHEAD);
+        proc(ca, n0);
+        if (n0 + 2 * DCT_AHEAD < full) load(ca, n0 + 2 * DCT_AHEAD);
+        proc(cb, n0 + DCT_AHEAD);
     }
-    issue(0, 0);
-    for (int ch = 0; ch < nchunks; ++ch) {
-        cp_async_wait_all();
-        __syncthreads();   // chunk ch (and, at ch = 0, the lines) visible; the buffer of chunk ch - 1 free
-        if (ch + 1 < nchunks) issue(ch + 1, (ch + 1) & 1);
-        const T *cb = cs + (ch & 1) * NB * DCT_PMAX;
-        const int n0 = ch * NB, rows = min(NB, N - n0);
-#pragma unroll
-        for (int r = 0; r < NB; ++r) {
-            if (r >= rows) break;
-            T c[DCT_RK];
-#pragma unroll
-            for (int j = 0; j < DCT_RK; ++j) c[j] = cb[r * DCT_PMAX + kj[j]];
-#pragma unroll
-            for (int q = 0; q < L / W; ++q) {
-                const V x = reinterpret_cast<const V *>(ln + (n0 + r) * L)[q];
-                const T *xs = reinterpret_cast<const T *>(&x);
-#pragma unroll
-                for (int w = 0; w < W; ++w)
-#pragma unroll
-                    for (int j = 0; j < DCT_RK; ++j) acc[j][q * W + w] = fma(c[j], xs[w], acc[j][q * W + w]);
-            }
-        }
-    }
+    if (n0 < full) { proc(ca, n0); n0 += DCT_AHEAD; }
+    for (; n0 < N; ++n0) dct_accumulate<T>(__ldg(col + (size_t)n0 * N), ln + n0 * DCT_LINES, acc);
 }
 template <typename T>
 __global__ void __launch_bounds__(DCT_THREADS) k_dct_x(Dims d, const T *__restrict__ src, const T *__restrict__ C,
                                                        typename cplx_t<T>::type *__restrict__ spec) {
     pdl_enter();
-    constexpr int L = DctVec<T>::L;
-    __shared__ __align__(16) T ln[DCT_NMAX * L];
-    __shared__ __align__(16) T cs[2 * DctVec<T>::NB * DCT_PMAX];
-    const int N = d.Nx, nlines = d.Ny * d.Nz, kt = blockDim.x;
-    const int line0 = blockIdx.x * L, nl = min(L, nlines - line0);
-    for (int e = threadIdx.x; e < L * N; e += blockDim.x) {
+    __shared__ __align__(16) T ln[DCT_LINES * DCT_NMAX];
+    const int N = d.Nx, nlines = d.Ny * d.Nz;
+    const int line0 = blockIdx.x * DCT_LINES, nl = min(DCT_LINES, nlines - line0);
+    for (int e = threadIdx.x; e < DCT_LINES * N; e += blockDim.x) {
         const int l = e / N, n = e - l * N;
-        ln[n * L + l] = l < nl ? src[(size_t)(line0 + l) * N + n] : T(0);
+        ln[n * DCT_LINES + l] = l < nl ? src[(size_t)(line0 + l) * N + n] : T(0);
     }
-    T acc[DCT_RK][L];
-    dct_tile<T>(C, N, threadIdx.x, kt, ln, cs, acc);
+    __syncthreads();
+    const int k = threadIdx.x;
+    if (k >= N) return;
+    T acc[DCT_LINES];
 #pragma unroll
-    for (int j = 0; j < DCT_RK; ++j) {
-        const int k = threadIdx.x + j * kt;
-        if (k >= N) continue;
+    for (int l = 0; l < DCT_LINES; ++l) acc[l] = T(0);
+    dct_column<T>(C + k, N, ln, acc);
 #pragma unroll
-        for (int l = 0; l < L; ++l)
-            if (l < nl) spec[(size_t)(line0 + l) * N + k] = mkc<T>(acc[j][l], T(0));
-    }
+    for (int l = 0; l < DCT_LINES; ++l)
+        if (l < nl) spec[(size_t)(line0 + l) * N + k] = mkc<T>(acc[l], T(0));
 }
 template <typename T>
 __global__ void __launch_bounds__(DCT_THREADS) k_idct_x(Dims d, const typename cplx_t<T>::type *__restrict__ spec,
                                                         const T *__restrict__ C, T inv_norm, T *__restrict__ dst) {
     pdl_enter();
-    constexpr int L = DctVec<T>::L;
-    __shared__ __align__(16) T ln[DCT_NMAX * L];
-    __shared__ __align__(16) T cs[2 * DctVec<T>::NB * DCT_PMAX];
-    const int N = d.Nx, nlines = d.Ny * d.Nz, kt = blockDim.x;
-    const int line0 = blockIdx.x * L, nl = min(L, nlines - line0);
-    for (int e = threadIdx.x; e < L * N; e += blockDim.x) {
+    __shared__ __align__(16) T ln[DCT_LINES * DCT_NMAX];
+    const int N = d.Nx, nlines = d.Ny * d.Nz;
+    const int line0 = blockIdx.x * DCT_LINES, nl = min(DCT_LINES, nlines - line0);
+    for (int e = threadIdx.x; e < DCT_LINES * N; e += blockDim.x) {
         const int l = e / N, k = e - l * N;
-        ln[k * L + l] = l < nl ? spec[(size_t)(line0 + l) * N + k].x : T(0);
+        ln[k * DCT_LINES + l] = l < nl ? spec[(size_t)(line0 + l) * N + k].x : T(0);
     }
-    T acc[DCT_RK][L];
-    dct_tile<T>(C, N, threadIdx.x, kt, ln, cs, acc);
+    __syncthreads();
+    const int n = threadIdx.x;
+    if (n >= N) return;
+    T acc[DCT_LINES];
 #pragma unroll
-    for (int j = 0; j < DCT_RK; ++j) {
-        const int n = threadIdx.x + j * kt;
-        if (n >= N) continue;
+    for (int l = 0; l < DCT_LINES; ++l) acc[l] = T(0);
+    dct_column<T>(C + n, N, ln, acc);
 #pragma unroll
-        for (int l = 0; l < L; ++l)
-            if (l < nl) dst[(size_t)(line0 + l) * N + n] = acc[j][l] * inv_norm;
-    }
+    for (int l = 0; l < DCT_LINES; ++l)
+        if (l < nl) dst[(size_t)(line0 + l) * N + n] = acc[l] * inv_norm;
 }
 // The solved field back into rhs_p's shape for inflow/outflow x: x cells 0..Nx-1 and the periodic z copy
 // (rhs_p(:, :, nzp+2) = rhs_p(:, :, 2)); the planes the reference leaves alone (x plane nxg, z plane nzg) keep the
