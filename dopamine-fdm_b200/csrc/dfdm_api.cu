@@ -26,6 +26,7 @@
 #include "kernels_hybrid.cuh"
 #include "kernels_tma.cuh"
 #include "kernels_les.cuh"
+#include "tridiag_eigen.h"
 #include "kernels_group.cuh"
 
 using namespace dfdm;
@@ -172,6 +173,10 @@ struct dfdm_ctx {
     // cells, every x mode kx = 0..Nx-1 in the spectrum, d_dct the Nx x Nx DCT-IV matrix
     bool xdct = false;
     void *d_dct = nullptr;   // the DCT-IV matrix, in the context's precision
+    // the 4-wall duct (z_bc_type = 1 with walls in y): a context for its pressure solve only; Nz = nz - 1 cells, the
+    // z-eigenmode transforms (forward, inverse) in the context's precision, and a second spectrum for them
+    bool duct = false;
+    void *d_zf = nullptr, *d_zi = nullptr, *spec2 = nullptr;
     int lx2 = 1, lxi2 = 1, thr_z2 = 256, thr_y2 = 256;   // x lines per block: forward, inverse
     size_t smem_x2 = 0, smem_xi2 = 0, smem_z2 = 0, smem_y2 = 0;
     cudaStream_t own_stream = nullptr, stream = nullptr;
@@ -459,6 +464,11 @@ template <typename T> struct Impl {
                     rc = fail(DFDM_ERR_CUDA, "cudaFuncSetAttribute failed");
         });
         if (rc) return rc;
+        return setup_ys3(c, optin);
+    }
+    // the staged-column y solve where three of its blocks fit on an SM (as setup_kernels decides it)
+    static int setup_ys3(dfdm_ctx *c, int optin) {
+        const Dims &d = c->d;
         c->ys3 = false;
         if (ysolve3_smem<T>(d.Ny) <= (size_t)optin) {
             CK(cudaFuncSetAttribute(k_ysolve3<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
@@ -466,6 +476,51 @@ template <typename T> struct Impl {
             CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ys_occ, k_ysolve3<T>, YS_COLS, (int)ysolve3_smem<T>(d.Ny)));
             c->ys3 = ys_occ >= 3;
         }
+        return DFDM_OK;
+    }
+    // the transforms of a duct Poisson context: x (two-level or Stockham) and the y solve
+    static int setup_duct_only(dfdm_ctx *c) {
+        const Dims &d = c->d;
+        int optin = 0, dev = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        const int M = d.Nx / 2;
+        c->lx = std::max(1, std::min(64, 1024 / std::max(1, M)));
+        c->smem_x = 2 * (size_t)c->lx * M * sizeof(C);
+        if (c->smem_x > (size_t)optin) return fail(DFDM_ERR_UNSUPPORTED, "grid too large for the shared-memory transforms");
+        CK(cudaFuncSetAttribute(k_fwd_x<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        CK(cudaFuncSetAttribute(k_inv_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        if (int rc = setup_ys3(c, optin)) return rc;
+        return setup_fft2l(c);
+    }
+    // dfdm_solve_poisson on a duct context: staging (rhs_p) -> phi -> x FFT -> z eigenmodes -> y solve per (kx, mode)
+    // -> z^-1 -> x FFT^-1 -> staging.  The eigenmode transforms run out of place; the y solve works on whichever
+    // buffer is the context's spectrum, so the two are swapped around it.
+    static int solve_duct(dfdm_ctx *c, int n1, int n2, int n3) {
+        const Dims &d = c->d;
+        const size_t n = (size_t)n1 * n2 * n3;
+        cudaStream_t st = c->stream;
+        k_unpack_rhs_p<T><<<reduce_grid(d), 256, 0, st>>>(d, n1, n2, c->staging, f(c->phi));
+        CKL();
+        if (int rc = fwd_x(c, false, f(c->phi))) return rc;
+        const long long cols = (long long)d.Ny * d.Nxc;
+        const dim3 g((unsigned)((cols + ZEIG_COLS - 1) / ZEIG_COLS), (unsigned)((d.Nz + ZEIG_RM - 1) / ZEIG_RM));
+        k_zeig<T><<<g, ZEIG_COLS, 0, st>>>(d, (const C *)c->spec, (C *)c->spec2, f(c->d_zf));
+        CKL();
+        {
+            struct Swap {
+                dfdm_ctx *c;
+                explicit Swap(dfdm_ctx *cc) : c(cc) { std::swap(c->spec, c->spec2); }
+                ~Swap() { std::swap(c->spec, c->spec2); }
+            } swapped(c);
+            if (int rc = launch(c, 4, 1)) return rc;
+            k_zeig<T><<<g, ZEIG_COLS, 0, st>>>(d, (const C *)c->spec, (C *)c->spec2, f(c->d_zi));
+            CKL();
+        }
+        if (int rc = launch(c, 6, 1)) return rc;
+        k_pack_rhs_p_bc<T><<<(int)std::min<size_t>((n + 255) / 256, 148 * 8), 256, 0, st>>>(d, n1, n2, n3, 1, 0, f(c->phi),
+                                                                                           c->staging);
+        CKL();
         return DFDM_OK;
     }
     // dfdm_solve_poisson on a DCT-IV context: staging (rhs_p) -> phi -> DCT-IV x -> z -> y solve -> z^-1 -> DCT-IV x
@@ -483,8 +538,8 @@ template <typename T> struct Impl {
         const T inv_norm = (T)(1.0 / (2.0 * (double)d.Nx * (double)d.Nz));
         k_idct_x<T><<<nb, nt, 0, c->stream>>>(d, (const C *)c->spec, f(c->d_dct), inv_norm, f(c->phi));
         CKL();
-        k_pack_rhs_p_dct<T><<<(int)std::min<size_t>((n + 255) / 256, 148 * 8), 256, 0, c->stream>>>(d, n1, n2, n3, f(c->phi),
-                                                                                                    c->staging);
+        k_pack_rhs_p_bc<T><<<(int)std::min<size_t>((n + 255) / 256, 148 * 8), 256, 0, c->stream>>>(d, n1, n2, n3, 0, 1,
+                                                                                                   f(c->phi), c->staging);
         CKL();
         return DFDM_OK;
     }
@@ -1062,6 +1117,9 @@ int check_ctx(dfdm_ctx *c) {
     if (c->xdct)
         return fail(DFDM_ERR_UNSUPPORTED, "a context of an inflow/outflow-x grid (x_bc_type = 1) serves dfdm_solve_poisson "
                                           "only: the step's stencils need periodic x");
+    if (c->duct)
+        return fail(DFDM_ERR_UNSUPPORTED, "a context of a 4-wall duct (z_bc_type = 1) serves dfdm_solve_poisson only: the "
+                                          "step's stencils need periodic z");
     return DFDM_OK;
 }
 
@@ -1097,8 +1155,20 @@ int validate(const dfdm_grid *g, const dfdm_params *p) {
     if (!g->x || !g->y || !g->z) return fail(DFDM_ERR_INVALID, "grid face arrays must not be NULL");
     if (g->nx % 2 || g->nz % 2) return fail(DFDM_ERR_INVALID, "Error: nx and nz must be even");
     if (g->nx < 6 || g->nz < 6 || g->ny < 4) return fail(DFDM_ERR_INVALID, "grid too small (nx, nz >= 6, ny >= 4)");
-    if ((g->x_bc_type != 0 && g->x_bc_type != 1) || g->z_bc_type != 0)
-        return fail(DFDM_ERR_UNSUPPORTED, "x_bc_type must be 0 (periodic) or 1 (inflow/outflow) and z_bc_type 0 (periodic)");
+    if ((g->x_bc_type != 0 && g->x_bc_type != 1) || (g->z_bc_type != 0 && g->z_bc_type != 1))
+        return fail(DFDM_ERR_UNSUPPORTED, "x_bc_type must be 0 (periodic) or 1 (inflow/outflow) and z_bc_type 0 (periodic) "
+                                          "or 1 (walls)");
+    if (g->z_bc_type == 1) {   // the 4-wall duct's Poisson path (src/initialization.f90:98-100)
+        if (g->x_bc_type != 0)
+            return fail(DFDM_ERR_UNSUPPORTED, "ERROR: GPU_POISSON build only supports z_bc_type=1 (spanwise wall) with "
+                                              "x_bc_type=0 (periodic x)");
+        if (g->y_bc_type != 1)
+            return fail(DFDM_ERR_UNSUPPORTED, "z walls with periodic y (the spanwise wall alone) are not built: only the "
+                                              "4-wall duct (y_bc_type = 1)");
+        if (g->nz - 1 > ZEIG_NMAX)
+            return fail(DFDM_ERR_UNSUPPORTED, "4-wall duct: at most " + std::to_string(ZEIG_NMAX) + " z cells (nz <= " +
+                                                  std::to_string(ZEIG_NMAX + 1) + ")");
+    }
     if (g->x_bc_type == 1) {   // the DCT-IV Poisson path (src/initialization.f90:95-99: walls in y, periodic z)
         if (g->y_bc_type != 1)
             return fail(DFDM_ERR_INVALID, "ERROR: GPU_POISSON with y_bc_type=0 (periodic y) requires x_bc_type=0 too");
@@ -1128,7 +1198,7 @@ int validate(const dfdm_grid *g, const dfdm_params *p) {
     FFTPlan tmp;
     int Nx = g->nx - 2, Nz = g->nz - 2;
     int Ny = g->y_bc_type == 0 ? g->ny - 2 : g->ny - 1;
-    if ((g->x_bc_type == 0 && !make_fft_plan(Nx / 2, tmp)) || !make_fft_plan(Nz, tmp) ||
+    if ((g->x_bc_type == 0 && !make_fft_plan(Nx / 2, tmp)) || (g->z_bc_type == 0 && !make_fft_plan(Nz, tmp)) ||
         (g->y_bc_type == 0 && !make_fft_plan(Ny, tmp)))
         return fail(DFDM_ERR_UNSUPPORTED, "transform lengths must factor into 2, 3 and 5");
     if (Ny > MAX_NY) return fail(DFDM_ERR_UNSUPPORTED, "ny too large for the y solve");
@@ -1155,6 +1225,10 @@ size_t arena_bytes(const dfdm_grid *g, const dfdm_params *p) {
     if (g->x_bc_type == 1) {   // the DCT-IV Poisson context: phi, the spectrum, the pivot table, the DCT matrix
         size_t Nx = g->nx - 1, Nz = g->nz - 2, Ny = g->ny - 1;
         return Nx * Ny * Nz * (ts + 2 * ts + 8) + Nx * Nx * 8 + (1 << 20);
+    }
+    if (g->z_bc_type == 1) {   // the duct's Poisson context: phi, two spectra, the pivot table, two eigenmode matrices
+        size_t Nx = g->nx - 2, Nz = g->nz - 1, Ny = g->ny - 1, Nxc = Nx / 2 + 1;
+        return Nx * Ny * Nz * ts + Nxc * Ny * Nz * (4 * ts + 8) + 2 * Nz * Nz * ts + (1 << 20);
     }
     size_t Nx = g->nx - 2, Nz = g->nz - 2, Ny = g->y_bc_type == 0 ? g->ny - 2 : g->ny - 1;
     size_t cells = Nx * Ny * Nz, spec = (Nx / 2 + 1) * Ny * Nz;
@@ -1208,13 +1282,19 @@ int dfdm_footprint_bytes(const dfdm_grid *grid, const dfdm_params *params, size_
     return DFDM_OK;
 }
 
-// A context for the DCT-IV pressure solve of an inflow/outflow-x grid (x_bc_type = 1, walls in y, periodic z): the
-// grid, the y operator, the modified wavenumbers (DCT-IV in x: kxx(i) = 2 (cos(pi (2i+1) / (2 nxp)) - 1) / dx^2,
-// src/initialization.f90:455-457; no null-mode fix, the DCT-IV modes have none, src/projection.f90:292), the pivot table,
-// the z transforms and the DCT-IV matrix.  Only dfdm_solve_poisson (and the stream and lifetime calls) accept it.
-static int create_dct(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
+// A context for one of the pressure solves whose step is not built, served by dfdm_solve_poisson alone (and the
+// stream and lifetime calls):
+//  - inflow/outflow x (x_bc_type = 1, walls in y, periodic z): the DCT-IV wavenumbers in x, kxx(i) =
+//    2 (cos(pi (2i+1) / (2 nxp)) - 1) / dx^2 (src/initialization.f90:455-457), no null-mode fix (the DCT-IV modes have
+//    none, src/projection.f90:292), the z transforms and the N x N DCT-IV matrix;
+//  - the 4-wall duct (z_bc_type = 1 with walls in y, periodic x): the x transforms, Dzz (src/initialization.f90:
+//    543-572) and the eigenbasis of S = W^(1/2) Dzz W^(-1/2) (:579-608), whose eigenvalues lambda_z(m) stand in for kzz;
+//    the null mode pinned where kx = 0 meets the zero eigenvalue (src/projection.f90:200-207);
+// with, for both, the y operator Dyy and the pivot table of every (kx, z mode) system.
+static int create_poisson_only(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
     dfdm_ctx *c = new dfdm_ctx();
-    c->xdct = true;
+    c->xdct = g->x_bc_type == 1;
+    c->duct = g->z_bc_type == 1;
     c->prm = *prm;
     c->prec = prm->precision;
     c->ts = c->prec == DFDM_FP64 ? 8 : 4;
@@ -1238,8 +1318,10 @@ static int create_dct(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out
     for (int k = 1; k <= c->nzg - 1; ++k) dzmin = std::min(dzmin, c->zg[k + 1] - c->zg[k]);
     c->dx = dxmin; c->dz = dzmin;
     Dims &d = c->d;
-    d.Nx = c->nx - 1; d.Nz = c->nz - 2; d.Ny = c->ny - 1; d.NyV = d.Ny - 1;
-    d.Nxc = d.Nx;
+    d.Nx = c->xdct ? c->nx - 1 : c->nx - 2;
+    d.Nz = c->duct ? c->nz - 1 : c->nz - 2;
+    d.Ny = c->ny - 1; d.NyV = d.Ny - 1;
+    d.Nxc = c->xdct ? d.Nx : d.Nx / 2 + 1;
     d.yper = 0;
     d.plane = (long long)d.Nx * d.Ny;
     d.cells = d.plane * d.Nz;
@@ -1254,38 +1336,65 @@ static int create_dct(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out
         c->allocs.push_back(c->arena);
     }
     c->in_create = true;
+    const size_t spec_bytes = (size_t)d.Nxc * d.Ny * d.Nz * 2 * c->ts;
     if ((rc = dalloc(c, &c->phi, (size_t)d.cells * c->ts))) return bail(rc);
-    if ((rc = dalloc(c, &c->spec, (size_t)d.Nxc * d.Ny * d.Nz * 2 * c->ts))) return bail(rc);
+    if ((rc = dalloc(c, &c->spec, spec_bytes))) return bail(rc);
+    if (c->duct && (rc = dalloc(c, &c->spec2, spec_bytes))) return bail(rc);
     const int nxp = d.Nx, nzp = d.Nz;
-    std::vector<double> kxx(d.Nxc), kzz(d.Nz), kyy(1, 0.0);
-    for (int i = 0; i < d.Nxc; ++i)
-        kxx[i] = 2.0 * (std::cos(PI * (double)(2 * i + 1) / (2.0 * (double)nxp)) - 1.0) / std::pow(c->dx, 2.0);
-    const int cz = (int)std::ceil((double)nzp / 2.0);
-    for (int k = 0; k < nzp; ++k) {
-        double kk = (k <= cz) ? (double)k : (double)(-nzp + k);
-        kzz[k] = 2.0 * (std::cos(2.0 * PI * kk / (double)nzp) - 1.0) / std::pow(c->dz, 2.0);
+    std::vector<double> kxx(d.Nxc), kzz(d.Nz, 0.0), kyy(1, 0.0);
+    if (c->xdct) {
+        for (int i = 0; i < d.Nxc; ++i)
+            kxx[i] = 2.0 * (std::cos(PI * (double)(2 * i + 1) / (2.0 * (double)nxp)) - 1.0) / std::pow(c->dx, 2.0);
+    } else {
+        const int cx = (int)std::ceil((double)nxp / 2.0);
+        for (int i = 0; i < d.Nxc; ++i) {
+            const double ii = (i <= cx) ? (double)i : (double)(-nxp + i);
+            kxx[i] = 2.0 * (std::cos(2.0 * PI * ii / (double)nxp) - 1.0) / std::pow(c->dx, 2.0);
+        }
     }
-    std::vector<double> lo(d.Ny, 0.0), di(d.Ny, 0.0), up(d.Ny, 0.0);
-    {   // Dyy (src/initialization.f90:507-535)
-        const std::vector<double> &y = c->y, &yg = c->yg;
-        const int nyg = c->nyg;
+    // the second-difference operator of a wall-bounded direction (Dyy, src/initialization.f90:507-535; Dzz the same
+    // on the z grid, :543-572): rows 2..n+1 of faces f and centres fg as (lower, diagonal, upper), 0-based
+    auto wall_operator = [](const std::vector<double> &f, const std::vector<double> &fg, int ng, std::vector<double> &lo,
+                            std::vector<double> &di, std::vector<double> &up) {
+        const int n = ng - 2;
+        lo.assign(n, 0.0); di.assign(n, 0.0); up.assign(n, 0.0);
         auto abc = [&](int j, double &a, double &b, double &cc) {
-            a = 1.0 / (y[j] - y[j - 1]) / (yg[j + 1] - yg[j]);
-            b = 1.0 / (y[j] - y[j - 1]) * (-1.0 / (yg[j + 1] - yg[j]) - 1.0 / (yg[j] - yg[j - 1]));
-            cc = 1.0 / (y[j] - y[j - 1]) / (yg[j] - yg[j - 1]);
+            a = 1.0 / (f[j] - f[j - 1]) / (fg[j + 1] - fg[j]);
+            b = 1.0 / (f[j] - f[j - 1]) * (-1.0 / (fg[j + 1] - fg[j]) - 1.0 / (fg[j] - fg[j - 1]));
+            cc = 1.0 / (f[j] - f[j - 1]) / (fg[j] - fg[j - 1]);
         };
-        for (int j = 3; j <= nyg - 2; ++j) {
+        for (int j = 3; j <= ng - 2; ++j) {
             double a, b, cc; abc(j, a, b, cc);
             up[j - 2] = a; lo[j - 2] = cc; di[j - 2] = b;
         }
         double a, b, cc;
         abc(2, a, b, cc); di[0] = b + cc; up[0] = a;
-        abc(nyg - 1, a, b, cc); di[nyg - 3] = a + b; lo[nyg - 3] = cc;
+        abc(ng - 1, a, b, cc); di[ng - 3] = a + b; lo[ng - 3] = cc;
+    };
+    std::vector<double> lo, di, up;
+    wall_operator(c->y, c->yg, c->nyg, lo, di, up);
+    std::vector<double> lambda_z, Qz, sqrt_w;
+    if (c->duct) {
+        std::vector<double> zlo, zdi, zup;
+        wall_operator(c->z, c->zg, c->nzg, zlo, zdi, zup);
+        std::vector<double> w(nzp), off(std::max(0, nzp - 1));
+        sqrt_w.resize(nzp);
+        for (int k = 0; k < nzp; ++k) { w[k] = c->z[k + 2] - c->z[k + 1]; sqrt_w[k] = std::sqrt(w[k]); }
+        for (int k = 0; k + 1 < nzp; ++k) off[k] = 1.0 / ((c->zg[k + 3] - c->zg[k + 2]) * std::sqrt(w[k] * w[k + 1]));
+        lambda_z = zdi;   // S's diagonal is Dzz's
+        if (!tridiag_eigen(lambda_z, off, Qz))
+            return bail(fail(DFDM_ERR_INVALID, "ERROR: the spanwise (z) wall operator could not be diagonalised (4-wall duct)"));
+    } else {
+        const int cz = (int)std::ceil((double)nzp / 2.0);
+        for (int k = 0; k < nzp; ++k) {
+            const double kk = (k <= cz) ? (double)k : (double)(-nzp + k);
+            kzz[k] = 2.0 * (std::cos(2.0 * PI * kk / (double)nzp) - 1.0) / std::pow(c->dz, 2.0);
+        }
     }
     void *tmp = nullptr;
     if ((rc = upload_as<double>(c, &tmp, kxx))) return bail(rc);
     c->d_kxx = (double *)tmp;
-    if ((rc = upload_as<double>(c, &tmp, kzz))) return bail(rc);
+    if ((rc = upload_as<double>(c, &tmp, c->duct ? lambda_z : kzz))) return bail(rc);
     c->d_kzz = (double *)tmp;
     if ((rc = upload_as<double>(c, &tmp, kyy))) return bail(rc);
     c->d_kyy = (double *)tmp;
@@ -1296,11 +1405,16 @@ static int create_dct(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out
     if ((rc = upload_as<double>(c, &tmp, up))) return bail(rc);
     c->d_up = (double *)tmp;
     {
+        double lmax = 0.0;
+        for (double l : lambda_z) lmax = std::max(lmax, std::fabs(l));
         std::vector<double> rpiv((size_t)d.Nxc * d.Ny * d.Nz);
         for (int kz = 0; kz < d.Nz; ++kz)
             for (int kx = 0; kx < d.Nxc; ++kx) {
-                const double lam = kxx[kx] + kzz[kz];
+                const double lz = c->duct ? lambda_z[kz] : kzz[kz];
+                const double lam = kxx[kx] + lz;
                 double D = di[0] + lam;
+                // the duct's null mode: kx = 0 with the zero eigenvalue, found by magnitude (src/projection.f90:206)
+                if (c->duct && kx == 0 && std::fabs(lz) < 1e-8 * lmax) D = 3.0 / 2.0 * D;
                 const size_t b = (size_t)kz * d.Ny * d.Nxc + kx;
                 rpiv[b] = 1.0 / D;
                 for (int r = 1; r < d.Ny; ++r) {
@@ -1313,22 +1427,44 @@ static int create_dct(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out
         if ((rc = upload_as<double>(c, &tmp, rpiv))) return bail(rc);
         c->d_rpiv = (double *)tmp;
     }
-    {   // C[k][n] = 2 cos(pi (2n+1)(2k+1) / (4 nxp)), the angle reduced exactly modulo 2 pi (8 nxp quarter-steps)
+    auto upload_t = [&](void **dst, const std::vector<double> &v) {
+        return c->prec == DFDM_FP64 ? upload_as<double>(c, dst, v) : upload_as<float>(c, dst, v);
+    };
+    auto tws = [&](void **dst, int n, int count) {
+        return c->prec == DFDM_FP64 ? upload_twiddles<double>(c, dst, n, count) : upload_twiddles<float>(c, dst, n, count);
+    };
+    if (c->xdct) {   // C[k][n] = 2 cos(pi (2n+1)(2k+1) / (4 nxp)), the angle reduced exactly modulo 2 pi (8 nxp quarter-steps)
         const long P = 8L * nxp;
         std::vector<double> cs((size_t)P), C((size_t)(nxp * nxp));
         for (long m = 0; m < P; ++m) cs[(size_t)m] = std::cos(PI * (double)m / (4.0 * (double)nxp));
         for (long k = 0; k < nxp; ++k)
             for (long n = 0; n < nxp; ++n) C[(size_t)(k * nxp + n)] = 2.0 * cs[(size_t)(((2 * n + 1) * (2 * k + 1)) % P)];
-        if ((rc = c->prec == DFDM_FP64 ? upload_as<double>(c, &tmp, C) : upload_as<float>(c, &tmp, C))) return bail(rc);
-        c->d_dct = tmp;
+        if ((rc = upload_t(&c->d_dct, C))) return bail(rc);
+        make_fft_plan(d.Nz, c->plan_z);
+        if ((rc = tws(&c->tw_z, d.Nz, d.Nz))) return bail(rc);
+    } else {
+        // the eigenmode transforms, [source index][destination index]: forward Qz(k,m) sqrt(w_k); inverse
+        // Qz(k,m) / sqrt(w_k) times nzp, which the inverse x transform's division by nxp nzp takes back out
+        std::vector<double> zf((size_t)nzp * nzp), zi((size_t)nzp * nzp);
+        for (int k = 0; k < nzp; ++k)
+            for (int m = 0; m < nzp; ++m) {
+                zf[(size_t)k * nzp + m] = Qz[(size_t)k * nzp + m] * sqrt_w[k];
+                zi[(size_t)m * nzp + k] = Qz[(size_t)k * nzp + m] / sqrt_w[k] * (double)nzp;
+            }
+        if ((rc = upload_t(&c->d_zf, zf))) return bail(rc);
+        if ((rc = upload_t(&c->d_zi, zi))) return bail(rc);
+        make_fft_plan(d.Nx / 2, c->plan_x);
+        if ((rc = tws(&c->tw_x, d.Nx / 2, d.Nx / 2))) return bail(rc);
+        if ((rc = tws(&c->twr_x, d.Nx, d.Nx / 2 + 1))) return bail(rc);
+        // the x kernels take the metric views of the full step; zeroed, and never read by the transforms
+        std::vector<double> my((size_t)6 * (d.Ny + 3), 0.0), mz((size_t)6 * (d.Nz + 3), 0.0);
+        if ((rc = upload_t(&c->my_t, my))) return bail(rc);
+        if ((rc = upload_t(&c->mz_t, mz))) return bail(rc);
     }
-    make_fft_plan(d.Nz, c->plan_z);
-    auto tws = [&](void **dst, int n, int count) {
-        return c->prec == DFDM_FP64 ? upload_twiddles<double>(c, dst, n, count) : upload_twiddles<float>(c, dst, n, count);
-    };
-    if ((rc = tws(&c->tw_z, d.Nz, d.Nz))) return bail(rc);
     c->in_create = false;
-    rc = dispatch(c, [&](auto impl) { return decltype(impl)::setup_poisson_only(c); });
+    rc = dispatch(c, [&](auto impl) {
+        return c->duct ? decltype(impl)::setup_duct_only(c) : decltype(impl)::setup_poisson_only(c);
+    });
     if (rc) return bail(rc);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(DFDM_ERR_CUDA, "set-up synchronisation failed"));
     *out = c;
@@ -1346,7 +1482,7 @@ int dfdm_create(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
         cudaGetLastError();
         return fail(DFDM_ERR_CUDA, "no CUDA device: the dfdm library has no CPU fallback");
     }
-    if (g->x_bc_type == 1) return create_dct(g, prm, out);
+    if (g->x_bc_type == 1 || g->z_bc_type == 1) return create_poisson_only(g, prm, out);
     dfdm_ctx *c = new dfdm_ctx();
     c->prm = *prm;
     c->prec = prm->precision;
@@ -2114,9 +2250,11 @@ int dfdm_solve_poisson(dfdm_ctx *c, const double *rhs_in, double *phi_out) {
     int rc = ensure_staging(c, n);
     if (rc) return rc;
     CK(cudaMemcpyAsync(c->staging, rhs_in, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    if (c->xdct) {
+    if (c->xdct || c->duct) {
         long long before = g_launches;
-        rc = dispatch(c, [&](auto impl) { return decltype(impl)::solve_dct(c, n1, n2, n3); });
+        rc = dispatch(c, [&](auto impl) {
+            return c->duct ? decltype(impl)::solve_duct(c, n1, n2, n3) : decltype(impl)::solve_dct(c, n1, n2, n3);
+        });
         c->launches += g_launches - before;
         if (rc) return rc;
         CK(cudaMemcpyAsync(phi_out, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));

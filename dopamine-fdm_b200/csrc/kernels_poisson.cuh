@@ -416,21 +416,79 @@ __global__ void __launch_bounds__(DCT_THREADS) k_idct_x(Dims d, const typename c
     for (int l = 0; l < DCT_LINES; ++l)
         if (l < nl) dst[(size_t)(line0 + l) * N + n] = acc[l] * inv_norm;
 }
-// The solved field back into rhs_p's shape for inflow/outflow x: x cells 0..Nx-1 and the periodic z copy
-// (rhs_p(:, :, nzp+2) = rhs_p(:, :, 2)); the planes the reference leaves alone (x plane nxg, z plane nzg) keep the
-// input the caller passed, which the staging buffer still holds.
+// The solved field back into rhs_p's shape for the Poisson-only contexts.  x: with periodic x (xwrap) the copies of
+// apply_periodic_xz_pressure (rhs_p(nxg-1) = rhs_p(2)) and of the next wrap for the plane nxg, as k_pack_rhs_p
+// writes them; with inflow/outflow x the plane nxg is left alone.  z: with periodic z (zwrap) the copy
+// rhs_p(:, :, nzp+2) = rhs_p(:, :, 2); with z walls no copy.  Points left alone keep the input the caller passed,
+// which the staging buffer still holds.
 template <typename T>
-__global__ void __launch_bounds__(256) k_pack_rhs_p_dct(Dims d, int n1, int n2, int n3, const T *__restrict__ f,
-                                                        double *__restrict__ out) {
+__global__ void __launch_bounds__(256) k_pack_rhs_p_bc(Dims d, int n1, int n2, int n3, int xwrap, int zwrap,
+                                                       const T *__restrict__ f, double *__restrict__ out) {
     pdl_enter();
     long long n = (long long)n1 * n2 * n3;
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(p % n1);
+        int i = (int)(p % n1);
         const long long q = p / n1;
-        const int j = (int)(q % n2), k = (int)(q / n2);
-        if (i >= d.Nx || k > d.Nz) continue;
-        out[p] = (double)f[((long long)(k % d.Nz) * d.Ny + j) * d.Nx + i];
+        const int j = (int)(q % n2);
+        int k = (int)(q / n2);
+        if (k < d.Nz && i >= d.Nx) {
+            if (!xwrap) continue;
+            i %= d.Nx;
+        }
+        if (k >= d.Nz) {
+            if (!zwrap) {
+                // a z wall leaves the plane nzg alone, except for the x copy rhs_p(nxg-1) = rhs_p(2), which covers
+                // every z plane: the input at i = 0, which nothing writes at this k
+                if (xwrap && i == d.Nx) out[p] = out[p - d.Nx];
+                continue;
+            }
+            if (k > d.Nz) continue;
+            k = 0;
+            if (i >= d.Nx) {
+                if (!xwrap) continue;
+                i %= d.Nx;
+            }
+        }
+        out[p] = (double)f[((long long)k * d.Ny + j) * d.Nx + i];
     }
+}
+
+// ---- the 4-wall duct (z walls with y walls; src/projection.f90:172-217, GPU src/poisson_gpu.f90:498-589) ----------
+// The z-eigenmode transform: out[m][col] = sum_k M[k][m] in[k][col] over the spectrum's columns col = j Nxc + kx
+// (z is the slowest index, so each k is one contiguous row of Ny Nxc complex values).  Forward, M[k][m] =
+// Qz(k,m) sqrt(w_k) (projection onto the orthonormal eigenbasis of S = W^(1/2) Dzz W^(-1/2) after scaling by the
+// square root of the cell width); inverse, M[m][k] = Qz(k,m) / sqrt(w_k), times nzp so that the inverse x kernel's
+// division by nxp nzp leaves the 1/nxp of a solve in physical z.  A block takes ZEIG_COLS columns and ZEIG_RM
+// outputs m, with its slice of M in shared memory; each thread walks its column down k (coalesced rows).
+constexpr int ZEIG_NMAX = 512, ZEIG_RM = 8, ZEIG_COLS = 128;
+template <typename T>
+__global__ void __launch_bounds__(ZEIG_COLS) k_zeig(Dims d, const typename cplx_t<T>::type *__restrict__ in,
+                                                    typename cplx_t<T>::type *__restrict__ out, const T *__restrict__ M) {
+    pdl_enter();
+    __shared__ T ms[ZEIG_NMAX * ZEIG_RM];
+    const int n = d.Nz, m0 = blockIdx.y * ZEIG_RM;
+    const long long cols = (long long)d.Ny * d.Nxc;
+    for (int e = threadIdx.x; e < n * ZEIG_RM; e += blockDim.x) {
+        const int k = e / ZEIG_RM, q = e - k * ZEIG_RM;
+        ms[e] = m0 + q < n ? M[(size_t)k * n + m0 + q] : T(0);
+    }
+    __syncthreads();
+    const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= cols) return;
+    T ar[ZEIG_RM], ai[ZEIG_RM];
+#pragma unroll
+    for (int q = 0; q < ZEIG_RM; ++q) { ar[q] = T(0); ai[q] = T(0); }
+    for (int k = 0; k < n; ++k) {
+        const typename cplx_t<T>::type v = in[(size_t)k * cols + col];
+#pragma unroll
+        for (int q = 0; q < ZEIG_RM; ++q) {
+            ar[q] = fma(ms[k * ZEIG_RM + q], v.x, ar[q]);
+            ai[q] = fma(ms[k * ZEIG_RM + q], v.y, ai[q]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < ZEIG_RM; ++q)
+        if (m0 + q < n) out[(size_t)(m0 + q) * cols + col] = mkc<T>(ar[q], ai[q]);
 }
 
 // ---- 4. inverse complex-to-real x transform, writes the pseudo-pressure phi ----------------------------------

@@ -51,7 +51,7 @@ class GridHolder:
     def __init__(self, case: Case):
         self.x, self.y, self.z = (np.ascontiguousarray(a, dtype=np.float64) for a in faces(case))
         self.grid = DfdmGrid(case.nx, case.ny, case.nz, dptr(self.x), dptr(self.y), dptr(self.z),
-                             case.x_bc_type, case.y_bc_type, 0, 1, 1)
+                             case.x_bc_type, case.y_bc_type, case.z_bc_type, 1, 1)
 
 
 def make_params(case: Case, precision: int = DFDM_FP64) -> DfdmParams:

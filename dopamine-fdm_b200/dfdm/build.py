@@ -32,7 +32,8 @@ def sources():
 
 
 def deps():
-    return (sources() + sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + sorted(glob.glob(os.path.join(CSRC, "*.inc")))
+    return (sources() + sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + sorted(glob.glob(os.path.join(CSRC, "*.inc"))) +
+            sorted(glob.glob(os.path.join(CSRC, "*.h")))
             + [os.path.join(INCLUDE, "dfdm.h")])
 
 

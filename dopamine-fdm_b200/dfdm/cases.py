@@ -35,6 +35,7 @@ class Case:
     alpha_grid: float = 0.0
     y_bc_type: int = 1           # 0 periodic, 1 walls
     x_bc_type: int = 0           # 0 periodic, 1 inflow/outflow (the DCT-IV Poisson path only)
+    z_bc_type: int = 0           # 0 periodic, 1 walls (with y walls: the 4-wall duct's Poisson path only)
     nu: float = 1e-3
     dt: float = 1e-3
     dPdx: float = 0.0
@@ -334,6 +335,13 @@ def inflow_outflow(nx: int = 18, ny: int = 17, nz: int = 18, grid_type: int = 2,
     DCT-IV path (src/projection.f90:124-130,334-343) only; such a case does not step."""
     return Case(name=name or f"inflow_outflow{nx}", nx=nx, ny=ny, nz=nz, Lx_i=3.0, Ly_i=2.0, Lz_i=1.5,
                 grid_type=grid_type, alpha_grid=2.0, y_bc_type=1, x_bc_type=1, nu=0.01, dt=0.002, ic="zero")
+
+
+def duct(nx: int = 18, ny: int = 17, nz: int = 18, grid_type: int = 2, name: Optional[str] = None) -> Case:
+    """A 4-wall duct (z_bc_type = 1 with y walls, periodic x), 3 x 2 x 1.5: the pressure solve of the z-eigenmode
+    path (src/projection.f90:172-217) only; such a case does not step."""
+    return Case(name=name or f"duct{nx}", nx=nx, ny=ny, nz=nz, Lx_i=3.0, Ly_i=2.0, Lz_i=1.5, grid_type=grid_type,
+                alpha_grid=2.0, y_bc_type=1, z_bc_type=1, nu=0.01, dt=0.002, ic="zero")
 
 
 CONFIGS = {"tgv64": tgv, "chan180": chan180, "les395": les395, "chan550": chan550,

@@ -186,6 +186,9 @@ struct Oracle {
     int nxp, nzp;                              // Fourier lengths
     std::vector<double> kxx, kzz, kyy;         // 0-based mode index
     std::vector<double> Dyy_d, Dyy_l, Dyy_u;   // Dyy(j,j), Dyy(j,j-1), Dyy(j,j+1), index j (1-based)
+    // 4-wall duct (z_bc_type 1 with y walls): Dzz rows 2..nzg-1 (1-based index k), and the eigenbasis of
+    // S = W^(1/2) Dzz W^(-1/2): lambda_z ascending, Qz(k, m) = Qz[k * nzm + m] orthonormal, sqrt_w_z(k)
+    std::vector<double> Dzz_d, Dzz_l, Dzz_u, lambda_z, Qz, sqrt_w_z;
     std::vector<double> wy0, wy1, wz0, wz1;    // weight_y_0(1:ny), weight_z_0(1:nz), 1-based
     double rk_t[4], rk_coef[4][4];
     dfdm_params prm;
@@ -235,7 +238,7 @@ struct Oracle {
         // x periodic: the last interior cell duplicates the first (nxp = nxm - 1); inflow/outflow x (x_bc_type 1,
         // the DCT-IV path): all nxm cells (src/initialization.f90:330-336)
         nxp = x_bc_type == 0 ? nxm - 1 : nxm;
-        nzp = nzm - 1;   // z periodic
+        nzp = z_bc_type == 0 ? nzm - 1 : nzm;   // z periodic; a z wall keeps every point (:338-345)
         int mx = nxp - 1, mz = nzp - 1;
         kxx.assign(mx + 1, 0.0); kzz.assign(mz + 1, 0.0);
         int cx = (int)std::ceil((double)nxp / 2.0), cz = (int)std::ceil((double)nzp / 2.0);
@@ -250,10 +253,14 @@ struct Oracle {
             dct_cos.assign((size_t)8 * nxp, 0.0);
             for (int m = 0; m < 8 * nxp; ++m) dct_cos[m] = std::cos(pi * (double)m / (4.0 * (double)nxp));
         }
-        for (int k = 0; k <= cz; ++k)
-            kzz[k] = 2.0 * (std::cos(2.0 * pi * (double)k / (double)nzp) - 1.0) / std::pow(dz, 2.0);
-        for (int k = cz + 1; k <= mz; ++k)
-            kzz[k] = 2.0 * (std::cos(2.0 * pi * (double)(-nzp + k) / (double)nzp) - 1.0) / std::pow(dz, 2.0);
+        if (z_bc_type == 0) {
+            for (int k = 0; k <= cz; ++k)
+                kzz[k] = 2.0 * (std::cos(2.0 * pi * (double)k / (double)nzp) - 1.0) / std::pow(dz, 2.0);
+            for (int k = cz + 1; k <= mz; ++k)
+                kzz[k] = 2.0 * (std::cos(2.0 * pi * (double)(-nzp + k) / (double)nzp) - 1.0) / std::pow(dz, 2.0);
+        } else {
+            setup_duct();
+        }
         if (y_bc_type == 0) {
             int nyp = nym - 1;
             kyy.assign(nyp, 0.0);
@@ -318,8 +325,72 @@ struct Oracle {
         wmf_ux.init(1, nx, 1, 2, 1, nzg); wmf_wx.init(1, nx, 1, 2, 1, nzg); wmf_tx.init(1, nx, 1, 2, 1, nzg);
         wmf_uz.init(1, nxg, 1, 2, 1, nz); wmf_wz.init(1, nxg, 1, 2, 1, nz); wmf_tz.init(1, nxg, 1, 2, 1, nz);
         if (x_bc_type == 0) fx.init(nxp);
-        fz.init(nzp);
+        if (z_bc_type == 0) fz.init(nzp);
         return 0;
+    }
+
+    // Dzz with z walls (src/initialization.f90:543-572, the construction of Dyy on the z grid) and the duct's
+    // eigenbasis (:579-618): S = W^(1/2) Dzz W^(-1/2), W = diag of the interior cell widths, is symmetric
+    // tridiagonal with S's diagonal = Dzz's and S(k,k+1) = 1 / ((zg(k+2) - zg(k+1)) sqrt(w(k) w(k+1))).  The
+    // reference diagonalises it with LAPACK dstev; here the cyclic Jacobi method (Golub & Van Loan, Matrix
+    // Computations, 8.5) rotates the dense matrix to diagonal form, and the pairs are sorted ascending as dstev
+    // returns them.  Eigenvector signs may differ from dstev's; the solve does not depend on them.
+    void setup_duct() {
+        Dzz_d.assign(nzg + 1, 0.0); Dzz_l.assign(nzg + 1, 0.0); Dzz_u.assign(nzg + 1, 0.0);
+        auto abc = [&](int k, double &a, double &b, double &c) {
+            a = 1.0 / (z[k] - z[k - 1]) / (zg[k + 1] - zg[k]);
+            b = 1.0 / (z[k] - z[k - 1]) * (-1.0 / (zg[k + 1] - zg[k]) - 1.0 / (zg[k] - zg[k - 1]));
+            c = 1.0 / (z[k] - z[k - 1]) / (zg[k] - zg[k - 1]);
+        };
+        for (int k = 3; k <= nzg - 2; ++k) { double a, b, c; abc(k, a, b, c); Dzz_u[k] = a; Dzz_l[k] = c; Dzz_d[k] = b; }
+        { double a, b, c; abc(2, a, b, c); Dzz_d[2] = b + c; Dzz_u[2] = a; }
+        { double a, b, c; abc(nzg - 1, a, b, c); Dzz_d[nzg - 1] = a + b; Dzz_l[nzg - 1] = c; }
+        const int n = nzm;
+        std::vector<double> w(n);
+        sqrt_w_z.assign(n, 0.0);
+        for (int k = 0; k < n; ++k) { w[k] = z[k + 2] - z[k + 1]; sqrt_w_z[k] = std::sqrt(w[k]); }
+        std::vector<double> A((size_t)n * n, 0.0), V((size_t)n * n, 0.0);
+        for (int k = 0; k < n; ++k) { A[(size_t)k * n + k] = Dzz_d[k + 2]; V[(size_t)k * n + k] = 1.0; }
+        for (int k = 0; k + 1 < n; ++k) {
+            const double e = 1.0 / ((zg[k + 3] - zg[k + 2]) * std::sqrt(w[k] * w[k + 1]));
+            A[(size_t)k * n + k + 1] = e; A[(size_t)(k + 1) * n + k] = e;
+        }
+        auto a = [&](int i, int j) -> double & { return A[(size_t)i * n + j]; };
+        for (int sweep = 0; sweep < 100; ++sweep) {
+            double off = 0.0, tot = 0.0;
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j) { tot += a(i, j) * a(i, j); if (i != j) off += a(i, j) * a(i, j); }
+            if (off <= 1e-30 * tot) break;
+            for (int p0 = 0; p0 < n - 1; ++p0)
+                for (int q0 = p0 + 1; q0 < n; ++q0) {
+                    const double apq = a(p0, q0);
+                    if (apq == 0.0) continue;
+                    // the symmetric Schur rotation that zeroes (p, q)
+                    const double tau = (a(q0, q0) - a(p0, p0)) / (2.0 * apq);
+                    const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (std::fabs(tau) + std::sqrt(1.0 + tau * tau));
+                    const double cs = 1.0 / std::sqrt(1.0 + tt * tt), sn = tt * cs;
+                    for (int k = 0; k < n; ++k) {   // A <- A J (columns p, q)
+                        const double akp = a(k, p0), akq = a(k, q0);
+                        a(k, p0) = cs * akp - sn * akq; a(k, q0) = sn * akp + cs * akq;
+                    }
+                    for (int k = 0; k < n; ++k) {   // A <- J^T A (rows p, q)
+                        const double apk = a(p0, k), aqk = a(q0, k);
+                        a(p0, k) = cs * apk - sn * aqk; a(q0, k) = sn * apk + cs * aqk;
+                    }
+                    for (int k = 0; k < n; ++k) {   // V <- V J
+                        const double vkp = V[(size_t)k * n + p0], vkq = V[(size_t)k * n + q0];
+                        V[(size_t)k * n + p0] = cs * vkp - sn * vkq; V[(size_t)k * n + q0] = sn * vkp + cs * vkq;
+                    }
+                }
+        }
+        std::vector<int> order(n);
+        for (int m = 0; m < n; ++m) order[m] = m;
+        std::sort(order.begin(), order.end(), [&](int i, int j) { return a(i, i) < a(j, j); });
+        lambda_z.assign(n, 0.0); Qz.assign((size_t)n * n, 0.0);
+        for (int m = 0; m < n; ++m) {
+            lambda_z[m] = a(order[m], order[m]);
+            for (int k = 0; k < n; ++k) Qz[(size_t)k * n + m] = V[(size_t)k * n + order[m]];
+        }
     }
 
     // DCT-IV of one x line, unnormalised (FFTW REDFT11, which the reference's CPU build plans; its GPU build forms the
@@ -1007,9 +1078,47 @@ struct Oracle {
             }
         }
         // then z
+        if (z_bc_type == 0) {
 #pragma omp parallel for
-        for (long ij = 0; ij < n1 * n2; ++ij) fz.exec(&c[(size_t)ij], n1 * n2, false);
-        if (y_bc_type == 0) {
+            for (long ij = 0; ij < n1 * n2; ++ij) fz.exec(&c[(size_t)ij], n1 * n2, false);
+        }
+        if (z_bc_type == 1) {
+            // 4-wall duct (src/projection.f90:172-217): per x mode, project onto the eigenbasis after scaling by
+            // sqrt(cell width), one y-tridiagonal solve per eigenmode with lambda_z(m) in place of kzz, then
+            // unproject and unscale
+            const int nr = nym, nm = (int)n3;
+            double lmax = 0.0;
+            for (int m = 0; m < nm; ++m) lmax = std::max(lmax, std::fabs(lambda_z[m]));
+            long swaps = 0; int info_max = 0;
+#pragma omp parallel for reduction(+ : swaps) reduction(max : info_max)
+            for (long i = 0; i < n1; ++i) {
+                std::vector<cplx> zh((size_t)n2 * nm), DL(nr), D(nr), DU(nr), B(nr);
+                for (long j = 0; j < n2; ++j)
+                    for (int m = 0; m < nm; ++m) {
+                        cplx acc(0.0, 0.0);
+                        for (int k = 0; k < nm; ++k) acc += c[id(i, j, k)] * sqrt_w_z[k] * Qz[(size_t)k * nm + m];
+                        zh[(size_t)(j + n2 * m)] = acc;
+                    }
+                for (int m = 0; m < nm; ++m) {
+                    for (int j = 2; j <= nyg - 2; ++j) { DL[j - 2] = Dyy_l[j + 1]; DU[j - 2] = Dyy_u[j]; }
+                    const double wavenum_sum = kxx[i] + lambda_z[m];
+                    for (int j = 2; j <= nyg - 1; ++j) D[j - 2] = Dyy_d[j] + wavenum_sum;
+                    if (x_bc_type == 0 && i == 0 && std::fabs(lambda_z[m]) < 1e-8 * lmax) D[0] = 3.0 / 2.0 * D[0];
+                    for (int j = 0; j < nr; ++j) B[j] = zh[(size_t)(j + n2 * m)];
+                    long sw = 0;
+                    const int info = zgtsv(nr, DL.data(), D.data(), DU.data(), B.data(), &sw);
+                    swaps += sw; info_max = std::max(info_max, info);
+                    for (int j = 0; j < nr; ++j) zh[(size_t)(j + n2 * m)] = B[j];
+                }
+                for (long j = 0; j < n2; ++j)
+                    for (int k = 0; k < nm; ++k) {
+                        cplx acc(0.0, 0.0);
+                        for (int m = 0; m < nm; ++m) acc += zh[(size_t)(j + n2 * m)] * Qz[(size_t)k * nm + m];
+                        c[id(i, j, k)] = acc / sqrt_w_z[k];
+                    }
+            }
+            gtsv_swaps += swaps; last_info = info_max;
+        } else if (y_bc_type == 0) {
             int nyp = nym - 1;
 #pragma omp parallel for
             for (long k = 0; k < n3; ++k)
@@ -1048,12 +1157,15 @@ struct Oracle {
             }
             gtsv_swaps += swaps; last_info = info_max;
         }
+        if (z_bc_type == 0) {
 #pragma omp parallel for
-        for (long ij = 0; ij < n1 * n2; ++ij) fz.exec(&c[(size_t)ij], n1 * n2, true);
+            for (long ij = 0; ij < n1 * n2; ++ij) fz.exec(&c[(size_t)ij], n1 * n2, true);
+        }
         if (x_bc_type == 0) {
 #pragma omp parallel for
             for (long jk = 0; jk < n2 * n3; ++jk) fx.exec(&c[(size_t)(jk * n1)], 1, true);
-            double norm = (double)((long)nxp * (long)nzp);
+            // a z wall is solved in physical z: no z normalisation (:326-332)
+            double norm = z_bc_type == 0 ? (double)((long)nxp * (long)nzp) : (double)nxp;
             for (long k = 0; k < n3; ++k)
                 for (long j = 0; j < n2; ++j)
                     for (long i = 0; i < n1; ++i) rhs_p((int)i + 2, (int)j + 2, (int)k + 2) = c[id(i, j, k)].real() / norm;
@@ -1073,8 +1185,9 @@ struct Oracle {
         if (x_bc_type == 0)
             for (int k = 2; k <= nzg; ++k)
                 for (int j = 2; j <= nyg - 1; ++j) rhs_p(nxg - 1, j, k) = rhs_p(2, j, k);
-        for (int j = 2; j <= nyg - 1; ++j)
-            for (int i = 2; i <= nxg - 1; ++i) rhs_p(i, j, nzp + 2) = rhs_p(i, j, 2);
+        if (z_bc_type == 0)   // no z copy with a z wall (:473-476)
+            for (int j = 2; j <= nyg - 1; ++j)
+                for (int i = 2; i <= nxg - 1; ++i) rhs_p(i, j, nzp + 2) = rhs_p(i, j, 2);
         if (y_bc_type == 0)
             for (int k = 2; k <= nzg; ++k)
                 for (int i = 2; i <= nxg; ++i) rhs_p(i, nyg - 1, k) = rhs_p(i, 2, k);
@@ -1359,7 +1472,8 @@ double orc_max_divergence(void *h) { return ((Oracle *)h)->check_divergence(); }
 double orc_kinetic_energy(void *h) { return ((Oracle *)h)->kinetic_energy(); }
 long orc_gtsv_swaps(void *h) { return ((Oracle *)h)->gtsv_swaps; }
 // grid-derived quantities, for known-answer tests: which = 0 xg, 1 yg, 2 zg (1..n+1 entries), 3 kxx, 4 kzz,
-// 5 Dyy diag (index 2..nyg-1), 6 weight_y_0 (1..ny), 7 dx/dz pair
+// 5 Dyy diag (index 2..nyg-1), 6 weight_y_0 (1..ny), 7 dx/dz pair, 8/9 Dyy lower/upper; with z walls 10-12 Dzz
+// diag/lower/upper (index 2..nzg-1), 13 lambda_z (ascending), 14 sqrt(cell width)
 int orc_grid_array(void *h, int which, double *out) {
     Oracle *o = (Oracle *)h;
     switch (which) {
@@ -1373,6 +1487,14 @@ int orc_grid_array(void *h, int which, double *out) {
     case 7: out[0] = o->dx; out[1] = o->dz; return 2;
     case 8: for (int j = 2; j <= o->nyg - 1; ++j) out[j - 2] = o->Dyy_l[j]; return o->nyg - 2;   // Dyy(j, j-1)
     case 9: for (int j = 2; j <= o->nyg - 1; ++j) out[j - 2] = o->Dyy_u[j]; return o->nyg - 2;   // Dyy(j, j+1)
+    }
+    if (o->z_bc_type != 1) return 0;
+    switch (which) {   // the duct's z operator and eigenbasis
+    case 10: for (int k = 2; k <= o->nzg - 1; ++k) out[k - 2] = o->Dzz_d[k]; return o->nzg - 2;
+    case 11: for (int k = 2; k <= o->nzg - 1; ++k) out[k - 2] = o->Dzz_l[k]; return o->nzg - 2;   // Dzz(k, k-1)
+    case 12: for (int k = 2; k <= o->nzg - 1; ++k) out[k - 2] = o->Dzz_u[k]; return o->nzg - 2;   // Dzz(k, k+1)
+    case 13: for (int m = 0; m < o->nzm; ++m) out[m] = o->lambda_z[m]; return o->nzm;
+    case 14: for (int k = 0; k < o->nzm; ++k) out[k] = o->sqrt_w_z[k]; return o->nzm;
     }
     return 0;
 }
