@@ -654,6 +654,43 @@ def main():
             io[prec] = {"ms_per_solve": best * 1e3, "cells_per_s": cells / best, "rel_l2_vs_oracle": err}
         out["inflow_outflow_poisson"] = io
 
+        # the 4-wall duct's pressure solve (256 x 128 x 129 independent cells); its right-hand side is the discrete
+        # operator applied to a seeded random field, so that it lies in the operator's range
+        cc = cases.duct(258, 129, 130, grid_type=2)
+        o = oracle.Oracle(cc)
+        rng = np.random.default_rng(130)
+        rhs = np.asfortranarray(rng.standard_normal(cc.shapes()["rhs_p"]))
+        Nx, Ny, Nz = cc.nx - 2, cc.ny - 1, cc.nz - 1
+        q = rng.standard_normal((Nx, Ny, Nz))
+        dx = o.grid_array(7)[0]
+        dy, ly, uy = o.grid_array(5), o.grid_array(8), o.grid_array(9)
+        dzz, lz, uz = o.grid_array(10), o.grid_array(11), o.grid_array(12)
+        a = (np.roll(q, -1, axis=0) - 2.0 * q + np.roll(q, 1, axis=0)) / dx**2 + dy[None, :, None] * q + dzz[None, None, :] * q
+        a[:, 1:, :] += ly[None, 1:, None] * q[:, :-1, :]
+        a[:, :-1, :] += uy[None, :-1, None] * q[:, 1:, :]
+        a[:, :, 1:] += lz[None, None, 1:] * q[:, :, :-1]
+        a[:, :, :-1] += uz[None, None, :-1] * q[:, :, 1:]
+        rhs[:Nx, :Ny, :Nz] = a
+        t0 = time.perf_counter()
+        want = o.solve_poisson(rhs)
+        t_oracle = time.perf_counter() - t0
+        o.close()
+        dp = {"grid": [Nx, Ny, Nz], "oracle_s_per_solve": t_oracle, "path": io["path"]}
+        for prec in ("fp32", "fp64"):
+            with Solver(cc, prec) as sv:
+                for _ in range(3):
+                    got = sv.solve_poisson_equation(rhs)
+                best = 1e30
+                for _ in range(3):
+                    t0 = time.perf_counter()
+                    for _ in range(10):
+                        sv.solve_poisson_equation(rhs)
+                    best = min(best, (time.perf_counter() - t0) / 10)
+            err = float(np.linalg.norm((got[:Nx, :, :Nz] - want[:Nx, :, :Nz]).ravel()) /
+                        np.linalg.norm(want[:Nx, :, :Nz].ravel()))
+            dp[prec] = {"ms_per_solve": best * 1e3, "cells_per_s": Nx * Ny * Nz / best, "rel_l2_vs_oracle": err}
+        out["duct_poisson"] = dp
+
     # ---- serving stream ----
     if not args.no_serve:
         def gather(obj):

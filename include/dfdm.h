@@ -54,7 +54,7 @@ typedef struct dfdm_grid {
     const double *z;           /* z(1:nz) face coordinates, uniform */
     int x_bc_type;             /* 0 periodic; 1 inflow/outflow (a context for dfdm_solve_poisson only, see below) */
     int y_bc_type;             /* 0 periodic, 1 walls */
-    int z_bc_type;             /* 0 periodic (the only value on this path) */
+    int z_bc_type;             /* 0 periodic; 1 walls (with y walls: the 4-wall duct, a context for dfdm_solve_poisson only) */
     int bc_face_ylo, bc_face_yhi; /* 1 no-slip (the only value on this path) */
 } dfdm_grid;
 
@@ -97,7 +97,11 @@ const char *dfdm_version(void);
  * x_bc_type = 1 (inflow/outflow x; needs y walls, y_bc_type = 1, and nx - 1 <= 257) creates a context for the
  * DCT-IV pressure solve alone (src/projection.f90:124-130,334-343): dfdm_solve_poisson, the stream calls,
  * dfdm_synchronize, dfdm_launch_count and dfdm_destroy accept it, every other entry point returns
- * DFDM_ERR_UNSUPPORTED (the inflow/outflow step, boundary conditions and convective outflow are not built). */
+ * DFDM_ERR_UNSUPPORTED (the inflow/outflow step, boundary conditions and convective outflow are not built).
+ * z_bc_type = 1 with y walls and periodic x (the 4-wall duct; nz - 1 <= 512) likewise creates a context for the
+ * duct's pressure solve alone (src/projection.f90:172-217): the z-eigenmode transform of Dzz (diagonalised once here,
+ * as the reference's dstev call at src/initialization.f90:579-608 does), one y-tridiagonal solve per (kx, z mode).
+ * Other z-wall combinations return DFDM_ERR_UNSUPPORTED, as the reference's GPU build rejects them. */
 int dfdm_create(const dfdm_grid *grid, const dfdm_params *params, dfdm_ctx **out);
 int dfdm_destroy(dfdm_ctx *ctx);
 /* Bytes of device memory a context of this grid and precision would hold (serving admission). */
@@ -154,7 +158,9 @@ int dfdm_compute_projection_step(dfdm_ctx *ctx, int save_p);
  * On an inflow/outflow-x context (x_bc_type = 1) the x transform is the DCT-IV (FFTW REDFT11) of the nx - 1
  * cells 2:nxg-1 with kxx(i) = 2 (cos(pi (2i+1) / (2 (nx-1))) - 1) / dx^2 and no null-mode fix; the output's
  * plane i = nxg keeps the input, as the reference's array does, and the z plane nzg (unset by the reference's
- * apply_periodic_xz_pressure at one rank) keeps the input too. */
+ * apply_periodic_xz_pressure at one rank) keeps the input too.
+ * On a 4-wall duct context (z_bc_type = 1) the z direction is solved in physical space through Dzz's eigenbasis; the
+ * output's z plane nzg keeps the input (no z copy with a wall) apart from the x copy rhs_p(nxg-1) = rhs_p(2). */
 int dfdm_solve_poisson(dfdm_ctx *ctx, const double *rhs_p_in, double *phi_out);
 /* No counterpart in the reference: dfdm_solve_poisson with no device allocation in the call.
  * dfdm_solve_poisson grows a per-context staging buffer with cudaMalloc on first use (and frees and regrows it,
