@@ -504,7 +504,7 @@ template <typename T> struct Impl {
         CKL();
         if (int rc = fwd_x(c, false, f(c->phi))) return rc;
         const long long cols = (long long)d.Ny * d.Nxc;
-        const dim3 g((unsigned)((cols + ZEIG_COLS - 1) / ZEIG_COLS), (unsigned)((d.Nz + ZEIG_RM - 1) / ZEIG_RM));
+        const dim3 g((unsigned)((cols + ZEIG_COLS - 1) / ZEIG_COLS), (unsigned)((d.Nz + zeig_modes<T>() - 1) / zeig_modes<T>()));
         k_zeig<T><<<g, ZEIG_COLS, 0, st>>>(d, (const C *)c->spec, (C *)c->spec2, f(c->d_zf));
         CKL();
         {

@@ -458,36 +458,48 @@ __global__ void __launch_bounds__(256) k_pack_rhs_p_bc(Dims d, int n1, int n2, i
 // (z is the slowest index, so each k is one contiguous row of Ny Nxc complex values).  Forward, M[k][m] =
 // Qz(k,m) sqrt(w_k) (projection onto the orthonormal eigenbasis of S = W^(1/2) Dzz W^(-1/2) after scaling by the
 // square root of the cell width); inverse, M[m][k] = Qz(k,m) / sqrt(w_k), times nzp so that the inverse x kernel's
-// division by nxp nzp leaves the 1/nxp of a solve in physical z.  A block takes ZEIG_COLS columns and ZEIG_RM
-// outputs m, with its slice of M in shared memory; each thread walks its column down k (coalesced rows).
-constexpr int ZEIG_NMAX = 512, ZEIG_RM = 8, ZEIG_COLS = 128;
+// division by nxp nzp leaves the 1/nxp of a solve in physical z.  A block takes ZEIG_COLS columns and
+// zeig_modes<T>() outputs m, with its slice of M in shared memory; each thread walks its column down k (coalesced
+// rows), so the rows are read Nz / zeig_modes times, from L2.
+constexpr int ZEIG_NMAX = 512, ZEIG_COLS = 128;
+template <typename T> __host__ __device__ constexpr int zeig_modes() { return sizeof(T) == 4 ? 16 : 8; }   // outputs m per block
 template <typename T>
 __global__ void __launch_bounds__(ZEIG_COLS) k_zeig(Dims d, const typename cplx_t<T>::type *__restrict__ in,
                                                     typename cplx_t<T>::type *__restrict__ out, const T *__restrict__ M) {
     pdl_enter();
-    __shared__ T ms[ZEIG_NMAX * ZEIG_RM];
-    const int n = d.Nz, m0 = blockIdx.y * ZEIG_RM;
+    constexpr int RM = zeig_modes<T>();
+    __shared__ __align__(16) T ms[ZEIG_NMAX * RM];
+    const int n = d.Nz, m0 = blockIdx.y * RM;
     const long long cols = (long long)d.Ny * d.Nxc;
-    for (int e = threadIdx.x; e < n * ZEIG_RM; e += blockDim.x) {
-        const int k = e / ZEIG_RM, q = e - k * ZEIG_RM;
+    for (int e = threadIdx.x; e < n * RM; e += blockDim.x) {
+        const int k = e / RM, q = e - k * RM;
         ms[e] = m0 + q < n ? M[(size_t)k * n + m0 + q] : T(0);
     }
     __syncthreads();
     const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= cols) return;
-    T ar[ZEIG_RM], ai[ZEIG_RM];
+    T ar[RM], ai[RM];
 #pragma unroll
-    for (int q = 0; q < ZEIG_RM; ++q) { ar[q] = T(0); ai[q] = T(0); }
+    for (int q = 0; q < RM; ++q) { ar[q] = T(0); ai[q] = T(0); }
     for (int k = 0; k < n; ++k) {
         const typename cplx_t<T>::type v = in[(size_t)k * cols + col];
+        T mk[RM];
 #pragma unroll
-        for (int q = 0; q < ZEIG_RM; ++q) {
-            ar[q] = fma(ms[k * ZEIG_RM + q], v.x, ar[q]);
-            ai[q] = fma(ms[k * ZEIG_RM + q], v.y, ai[q]);
+        for (int q = 0; q < RM; q += 16 / sizeof(T)) {   // the row's coefficients as 16-byte broadcast loads
+            typedef typename std::conditional<sizeof(T) == 4, float4, double2>::type V;
+            const V w = *reinterpret_cast<const V *>(ms + k * RM + q);
+            const T *ws = reinterpret_cast<const T *>(&w);
+#pragma unroll
+            for (int u = 0; u < (int)(16 / sizeof(T)); ++u) mk[q + u] = ws[u];
+        }
+#pragma unroll
+        for (int q = 0; q < RM; ++q) {
+            ar[q] = fma(mk[q], v.x, ar[q]);
+            ai[q] = fma(mk[q], v.y, ai[q]);
         }
     }
 #pragma unroll
-    for (int q = 0; q < ZEIG_RM; ++q)
+    for (int q = 0; q < RM; ++q)
         if (m0 + q < n) out[(size_t)(m0 + q) * cols + col] = mkc<T>(ar[q], ai[q]);
 }
 
