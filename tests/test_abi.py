@@ -51,6 +51,28 @@ def test_invalid_inputs_are_rejected_with_the_reference_message(mutate, code, ms
     assert e.value.code == code and msg in str(e.value)
 
 
+@pytest.mark.parametrize("case,code,msg", [
+    (cases.inflow_outflow(260, 17, 18), 4, "at most 257 x cells"),
+    (cases.inflow_outflow(18, 17, 18).with_(y_bc_type=0), 1, "requires x_bc_type=0"),
+    (cases.duct(18, 17, 514), 4, "at most 512 z cells"),
+    (cases.duct(18, 17, 18).with_(x_bc_type=1), 4, "x_bc_type=0 (periodic x)"),
+    (cases.duct(18, 17, 18).with_(y_bc_type=0), 4, "spanwise wall alone"),
+    (cases.duct(18, 17, 17), 1, "even"),
+])
+def test_poisson_only_grids_outside_the_built_paths_are_rejected(case, code, msg):
+    """The inflow/outflow and duct pressure solves: their size limits and the boundary combinations the reference's
+    GPU build rejects (src/initialization.f90:95-100), refused before any device work."""
+    with pytest.raises(native.DfdmError) as e:
+        native.footprint_bytes(case)
+    assert e.value.code == code and msg in str(e.value)
+
+
+def test_poisson_only_footprints_at_their_largest_sizes():
+    for c in (cases.inflow_outflow(258, 129, 130), cases.duct(258, 129, 512), cases.duct(18, 17, 18)):
+        for prec in ("fp32", "fp64"):
+            assert native.footprint_bytes(c, prec) > 0
+
+
 def test_footprint_scales_with_precision():
     c = cases.chan550()
     b64 = native.footprint_bytes(c, "fp64")

@@ -6,7 +6,7 @@ import pytest
 
 from dfdm.native import DfdmError, Solver
 
-from test_oracle_duct import duct_rhs
+from test_oracle_duct import duct_rhs, operator
 from dfdm.cases import duct
 
 pytestmark = pytest.mark.gpu
@@ -41,6 +41,41 @@ def test_duct_poisson_matches_the_oracle(oracle_mod, prec, tol, nx, ny, nz, grid
     assert np.array_equal(got[Nx], got[0])                   # apply_periodic_xz_pressure's x copy
     assert np.array_equal(got[:Nx + 1, :, Nz], want[:Nx + 1, :, Nz])   # the plane nzg as the reference leaves it
     assert np.array_equal(got, again)
+
+
+def test_duct_at_the_largest_z_size(oracle_mod):
+    """511 z cells (nz = 512, the largest even nz within the 512-cell limit of the eigenmode kernel's shared matrix
+    slice).  The z spectrum then spans (2 Nz / pi)^2 ~ 1e5, which amplifies the rounding of any FP64 solve: the oracle
+    itself lands 1.4e-12 (relative L2) from the exact answer here, against 8.6e-14 at 129 cells, so the FP64 bar is
+    1e-11, checked against the exact solution (the right-hand side is the operator applied to a known field, which
+    the solve returns up to the constant null mode) and against the oracle.  That right-hand side is dominated by its
+    high modes (|q| / dz^2), so its low-mode coefficients are small differences of large terms: in FP32 they lose
+    about 1e-4 (relative L2) before the 1/lambda amplification.  The FP32-mixed check (1e-5 against the oracle) takes
+    a white-noise right-hand side, whose modes are of one size, as the other FP32 Poisson tests do."""
+    c = duct(18, 17, 512, 1)
+    o = oracle_mod.Oracle(c)
+    Nx, Ny, Nz = c.nx - 2, c.ny - 1, c.nz - 1
+    rng = np.random.default_rng(512)
+    rhs = np.asfortranarray(rng.standard_normal((c.nx, c.ny - 1, c.nz)))
+    q = rng.standard_normal((Nx, Ny, Nz))
+    rhs[:Nx, :Ny, :Nz] = operator(o, q, o.grid_array(7)[0])
+    want = o.solve_poisson(rhs)
+    o.close()
+
+    def centred(a):
+        return a - a.mean()
+
+    with Solver(c, "fp64") as s:
+        got = s.solve_poisson_equation(rhs)[:Nx, :, :Nz]
+    assert rel_l2(got, want[:Nx, :, :Nz]) <= 1e-11
+    assert rel_l2(centred(got), centred(q)) <= 1e-11
+    white = np.asfortranarray(rng.standard_normal((c.nx, c.ny - 1, c.nz)))
+    o = oracle_mod.Oracle(c)
+    want = o.solve_poisson(white)
+    o.close()
+    with Solver(c, "fp32") as s:
+        got = s.solve_poisson_equation(white)[:Nx, :, :Nz]
+    assert rel_l2(got, want[:Nx, :, :Nz]) <= 1e-5
 
 
 def test_duct_context_refuses_the_stepping_entry_points():
