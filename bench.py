@@ -368,6 +368,7 @@ def main():
     import torch
     import torch.distributed as dist
     from dfdm.native import KERNELS, Solver
+    from dfdm.native import load as native_lib
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -626,6 +627,31 @@ def main():
                        "oracle": "FP64 C++ restatement of the reference, same grid, initial condition and dt"}
         out["accuracy"] = acc
 
+        def poisson_call_time(fn):
+            """Best of 3 batches of 10 calls, after 3 warm-up calls (seconds per call, host wall clock)."""
+            for _ in range(3):
+                fn()
+            best = 1e30
+            for _ in range(3):
+                t0 = time.perf_counter()
+                for _ in range(10):
+                    fn()
+                best = min(best, (time.perf_counter() - t0) / 10)
+            return best
+
+        def pinned_solve(sv, rhs):
+            """dfdm_solve_poisson from and to page-locked copies of rhs (the C call a host with pinned arrays makes)."""
+            import ctypes
+            pin_in = torch.from_numpy(rhs.ravel(order="K")).pin_memory()
+            pin_out = torch.empty_like(pin_in).pin_memory()
+            P = ctypes.POINTER(ctypes.c_double)
+            lib = native_lib()
+            call = lambda: lib.dfdm_solve_poisson(sv.h, ctypes.cast(pin_in.data_ptr(), P),   # noqa: E731
+                                                  ctypes.cast(pin_out.data_ptr(), P))
+            if call() != 0:
+                raise RuntimeError("dfdm_solve_poisson from pinned arrays failed")
+            return call
+
         # the DCT-IV pressure solve of an inflow/outflow-x grid (257 x 128 x 128 independent cells)
         cc = cases.inflow_outflow(258, 129, 130, grid_type=2)
         rhs = np.asfortranarray(np.random.default_rng(258).standard_normal(cc.shapes()["rhs_p"]))
@@ -637,21 +663,18 @@ def main():
         N, nzp = cc.nx - 1, cc.nz - 2
         cells = N * (cc.ny - 1) * nzp
         io = {"grid": [N, cc.ny - 1, nzp], "oracle_s_per_solve": t_oracle,
-              "path": "dfdm_solve_poisson (FP64 host arrays in and out, synchronous), host wall clock, best of 3 "
-                      "batches of 10 after 3 warm-up calls"}
+              "path": "dfdm_solve_poisson (FP64 pageable host arrays in and out, the output array reused, synchronous), "
+                      "host wall clock, best of 3 batches of 10 after 3 warm-up calls; pinned: the same from page-locked "
+                      "arrays"}
         for prec in ("fp32", "fp64"):
             with Solver(cc, prec) as sv:
-                for _ in range(3):
-                    got = sv.solve_poisson_equation(rhs)
-                best = 1e30
-                for _ in range(3):
-                    t0 = time.perf_counter()
-                    for _ in range(10):
-                        sv.solve_poisson_equation(rhs)
-                    best = min(best, (time.perf_counter() - t0) / 10)
+                got = np.zeros_like(rhs, order="F")
+                best = poisson_call_time(lambda: sv.solve_poisson_equation(rhs, out=got))
+                best_pinned = poisson_call_time(pinned_solve(sv, rhs))
             err = float(np.linalg.norm((got[:N, :, :nzp] - want[:N, :, :nzp]).ravel()) /
                         np.linalg.norm(want[:N, :, :nzp].ravel()))
-            io[prec] = {"ms_per_solve": best * 1e3, "cells_per_s": cells / best, "rel_l2_vs_oracle": err}
+            io[prec] = {"ms_per_solve": best * 1e3, "cells_per_s": cells / best, "rel_l2_vs_oracle": err,
+                        "pinned_ms_per_solve": best_pinned * 1e3}
         out["inflow_outflow_poisson"] = io
 
         # the 4-wall duct's pressure solve (256 x 128 x 129 independent cells); its right-hand side is the discrete
@@ -678,17 +701,13 @@ def main():
         dp = {"grid": [Nx, Ny, Nz], "oracle_s_per_solve": t_oracle, "path": io["path"]}
         for prec in ("fp32", "fp64"):
             with Solver(cc, prec) as sv:
-                for _ in range(3):
-                    got = sv.solve_poisson_equation(rhs)
-                best = 1e30
-                for _ in range(3):
-                    t0 = time.perf_counter()
-                    for _ in range(10):
-                        sv.solve_poisson_equation(rhs)
-                    best = min(best, (time.perf_counter() - t0) / 10)
+                got = np.zeros_like(rhs, order="F")
+                best = poisson_call_time(lambda: sv.solve_poisson_equation(rhs, out=got))
+                best_pinned = poisson_call_time(pinned_solve(sv, rhs))
             err = float(np.linalg.norm((got[:Nx, :, :Nz] - want[:Nx, :, :Nz]).ravel()) /
                         np.linalg.norm(want[:Nx, :, :Nz].ravel()))
-            dp[prec] = {"ms_per_solve": best * 1e3, "cells_per_s": Nx * Ny * Nz / best, "rel_l2_vs_oracle": err}
+            dp[prec] = {"ms_per_solve": best * 1e3, "cells_per_s": Nx * Ny * Nz / best, "rel_l2_vs_oracle": err,
+                        "pinned_ms_per_solve": best_pinned * 1e3}
         out["duct_poisson"] = dp
 
     # ---- serving stream ----

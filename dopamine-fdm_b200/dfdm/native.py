@@ -292,9 +292,15 @@ class Solver:
     def compute_projection_step(self, save_p: bool = False):
         _check(load().dfdm_compute_projection_step(self.h, int(save_p)))
 
-    def solve_poisson_equation(self, rhs_p):
+    def solve_poisson_equation(self, rhs_p, out=None):
+        """phi for rhs_p, both in the reference's (2:nxg, 2:nyg-1, 2:nzg) shape.  out: an FP64 Fortran-order array of
+        that shape to write into (rhs_p itself solves in place, as the reference's subroutine does); a caller that
+        solves repeatedly should pass one, since a fresh array's first-touch page faults land inside the copy."""
         a = np.asfortranarray(rhs_p, dtype=np.float64)
-        out = np.zeros_like(a, order="F")
+        if out is None:
+            out = np.zeros_like(a, order="F")
+        elif out.shape != a.shape or out.dtype != np.float64 or not out.flags.f_contiguous:
+            raise ValueError("out must be an FP64 Fortran-order array of rhs_p's shape")
         _check(load().dfdm_solve_poisson(self.h, dptr(a), dptr(out)))
         return out
 
