@@ -177,6 +177,10 @@ struct dfdm_ctx {
     // z-eigenmode transforms (forward, inverse) in the context's precision, and a second spectrum for them
     bool duct = false;
     void *d_zf = nullptr, *d_zi = nullptr, *spec2 = nullptr;
+    // spanwise walls alone (z_bc_type = 1 with periodic y): a context for that pressure solve only, holding the field
+    // with y and z exchanged (Ny = nz - 1 wall-bounded cells, Nz = ny - 2 periodic rows) so that the channel's
+    // transforms and y solve serve it
+    bool zwall = false;
     int lx2 = 1, lxi2 = 1, thr_z2 = 256, thr_y2 = 256;   // x lines per block: forward, inverse
     size_t smem_x2 = 0, smem_xi2 = 0, smem_z2 = 0, smem_y2 = 0;
     cudaStream_t own_stream = nullptr, stream = nullptr;
@@ -490,8 +494,30 @@ template <typename T> struct Impl {
         if (c->smem_x > (size_t)optin) return fail(DFDM_ERR_UNSUPPORTED, "grid too large for the shared-memory transforms");
         CK(cudaFuncSetAttribute(k_fwd_x<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
         CK(cudaFuncSetAttribute(k_inv_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        if (c->zwall) {   // the periodic axis, transformed by the z kernels
+            c->tzx = CT;
+            c->smem_z = 2 * (size_t)d.Nz * c->tzx * sizeof(C);
+            if (c->smem_z > (size_t)optin) return fail(DFDM_ERR_UNSUPPORTED, "grid too large for the shared-memory transforms");
+            for (const void *fn : {(const void *)k_col_fft<T, 0, CT>, (const void *)k_col_fft<T, 1, CT>})
+                CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        }
         if (int rc = setup_ys3(c, optin)) return rc;
         return setup_fft2l(c);
+    }
+    // dfdm_solve_poisson on a spanwise-wall context: the channel's chain on the field with y and z exchanged
+    static int solve_zwall(dfdm_ctx *c, int n1, int n2, int n3) {
+        const Dims &d = c->d;
+        const size_t n = (size_t)n1 * n2 * n3;
+        cudaStream_t st = c->stream;
+        k_unpack_rhs_p_swap<T><<<reduce_grid(d), 256, 0, st>>>(d, n1, n2, c->staging, f(c->phi));
+        CKL();
+        if (int rc = fwd_x(c, false, f(c->phi))) return rc;
+        for (int which : {3, 4, 5, 6})
+            if (int rc = launch(c, which, 1)) return rc;
+        k_pack_rhs_p_swap<T><<<(int)std::min<size_t>((n + 255) / 256, 148 * 8), 256, 0, st>>>(d, n1, n2, n3, f(c->phi),
+                                                                                             c->staging);
+        CKL();
+        return DFDM_OK;
     }
     // dfdm_solve_poisson on a duct context: staging (rhs_p) -> phi -> x FFT -> z eigenmodes -> y solve per (kx, mode)
     // -> z^-1 -> x FFT^-1 -> staging.  The eigenmode transforms run out of place; the y solve works on whichever
@@ -1117,9 +1143,9 @@ int check_ctx(dfdm_ctx *c) {
     if (c->xdct)
         return fail(DFDM_ERR_UNSUPPORTED, "a context of an inflow/outflow-x grid (x_bc_type = 1) serves dfdm_solve_poisson "
                                           "only: the step's stencils need periodic x");
-    if (c->duct)
-        return fail(DFDM_ERR_UNSUPPORTED, "a context of a 4-wall duct (z_bc_type = 1) serves dfdm_solve_poisson only: the "
-                                          "step's stencils need periodic z");
+    if (c->duct || c->zwall)
+        return fail(DFDM_ERR_UNSUPPORTED, "a context of a grid with z walls (z_bc_type = 1) serves dfdm_solve_poisson only: "
+                                          "the step's stencils need periodic z");
     return DFDM_OK;
 }
 
@@ -1162,12 +1188,11 @@ int validate(const dfdm_grid *g, const dfdm_params *p) {
         if (g->x_bc_type != 0)
             return fail(DFDM_ERR_UNSUPPORTED, "ERROR: GPU_POISSON build only supports z_bc_type=1 (spanwise wall) with "
                                               "x_bc_type=0 (periodic x)");
-        if (g->y_bc_type != 1)
-            return fail(DFDM_ERR_UNSUPPORTED, "z walls with periodic y (the spanwise wall alone) are not built: only the "
-                                              "4-wall duct (y_bc_type = 1)");
-        if (g->nz - 1 > ZEIG_NMAX)
+        if (g->y_bc_type == 1 && g->nz - 1 > ZEIG_NMAX)
             return fail(DFDM_ERR_UNSUPPORTED, "4-wall duct: at most " + std::to_string(ZEIG_NMAX) + " z cells (nz <= " +
                                                   std::to_string(ZEIG_NMAX + 1) + ")");
+        if (g->y_bc_type == 0 && g->nz - 1 > MAX_NY)   // spanwise walls: z is solved by the y-solve kernels
+            return fail(DFDM_ERR_UNSUPPORTED, "spanwise walls: at most " + std::to_string(MAX_NY) + " z cells");
     }
     if (g->x_bc_type == 1) {   // the DCT-IV Poisson path (src/initialization.f90:95-99: walls in y, periodic z)
         if (g->y_bc_type != 1)
@@ -1225,6 +1250,10 @@ size_t arena_bytes(const dfdm_grid *g, const dfdm_params *p) {
     if (g->x_bc_type == 1) {   // the DCT-IV Poisson context: phi, the spectrum, the pivot table, the DCT matrix
         size_t Nx = g->nx - 1, Nz = g->nz - 2, Ny = g->ny - 1;
         return Nx * Ny * Nz * (ts + 2 * ts + 8) + Nx * Nx * 8 + (1 << 20);
+    }
+    if (g->z_bc_type == 1 && g->y_bc_type == 0) {   // spanwise walls: phi, the spectrum, the pivot table
+        size_t Nx = g->nx - 2, Nw = g->nz - 1, Np = g->ny - 2, Nxc = Nx / 2 + 1;
+        return Nx * Nw * Np * ts + Nxc * Nw * Np * (2 * ts + 8) + (1 << 20);
     }
     if (g->z_bc_type == 1) {   // the duct's Poisson context: phi, two spectra, the pivot table, two eigenmode matrices
         size_t Nx = g->nx - 2, Nz = g->nz - 1, Ny = g->ny - 1, Nxc = Nx / 2 + 1;
@@ -1294,7 +1323,8 @@ int dfdm_footprint_bytes(const dfdm_grid *grid, const dfdm_params *params, size_
 static int create_poisson_only(const dfdm_grid *g, const dfdm_params *prm, dfdm_ctx **out) {
     dfdm_ctx *c = new dfdm_ctx();
     c->xdct = g->x_bc_type == 1;
-    c->duct = g->z_bc_type == 1;
+    c->duct = g->z_bc_type == 1 && g->y_bc_type == 1;
+    c->zwall = g->z_bc_type == 1 && g->y_bc_type == 0;
     c->prm = *prm;
     c->prec = prm->precision;
     c->ts = c->prec == DFDM_FP64 ? 8 : 4;
@@ -1319,8 +1349,9 @@ static int create_poisson_only(const dfdm_grid *g, const dfdm_params *prm, dfdm_
     c->dx = dxmin; c->dz = dzmin;
     Dims &d = c->d;
     d.Nx = c->xdct ? c->nx - 1 : c->nx - 2;
-    d.Nz = c->duct ? c->nz - 1 : c->nz - 2;
-    d.Ny = c->ny - 1; d.NyV = d.Ny - 1;
+    d.Nz = c->duct ? c->nz - 1 : c->zwall ? c->ny - 2 : c->nz - 2;
+    d.Ny = c->zwall ? c->nz - 1 : c->ny - 1;
+    d.NyV = d.Ny - 1;
     d.Nxc = c->xdct ? d.Nx : d.Nx / 2 + 1;
     d.yper = 0;
     d.plane = (long long)d.Nx * d.Ny;
@@ -1372,7 +1403,8 @@ static int create_poisson_only(const dfdm_grid *g, const dfdm_params *prm, dfdm_
         abc(ng - 1, a, b, cc); di[ng - 3] = a + b; lo[ng - 3] = cc;
     };
     std::vector<double> lo, di, up;
-    wall_operator(c->y, c->yg, c->nyg, lo, di, up);
+    if (c->zwall) wall_operator(c->z, c->zg, c->nzg, lo, di, up);   // the wall axis is z
+    else wall_operator(c->y, c->yg, c->nyg, lo, di, up);
     std::vector<double> lambda_z, Qz, sqrt_w;
     if (c->duct) {
         std::vector<double> zlo, zdi, zup;
@@ -1385,10 +1417,12 @@ static int create_poisson_only(const dfdm_grid *g, const dfdm_params *prm, dfdm_
         if (!tridiag_eigen(lambda_z, off, Qz))
             return bail(fail(DFDM_ERR_INVALID, "ERROR: the spanwise (z) wall operator could not be diagonalised (4-wall duct)"));
     } else {
+        // the periodic axis: z, or with spanwise walls y (kyy, src/initialization.f90:436-447: uniform y, dy = y(2) - y(1))
+        const double h = c->zwall ? c->y[2] - c->y[1] : c->dz;
         const int cz = (int)std::ceil((double)nzp / 2.0);
         for (int k = 0; k < nzp; ++k) {
             const double kk = (k <= cz) ? (double)k : (double)(-nzp + k);
-            kzz[k] = 2.0 * (std::cos(2.0 * PI * kk / (double)nzp) - 1.0) / std::pow(c->dz, 2.0);
+            kzz[k] = 2.0 * (std::cos(2.0 * PI * kk / (double)nzp) - 1.0) / std::pow(h, 2.0);
         }
     }
     void *tmp = nullptr;
@@ -1415,6 +1449,8 @@ static int create_poisson_only(const dfdm_grid *g, const dfdm_params *prm, dfdm_
                 double D = di[0] + lam;
                 // the duct's null mode: kx = 0 with the zero eigenvalue, found by magnitude (src/projection.f90:206)
                 if (c->duct && kx == 0 && std::fabs(lz) < 1e-8 * lmax) D = 3.0 / 2.0 * D;
+                // spanwise walls: the (kx, ky) = (0, 0) system, as the y-wall branch pins its own (src/projection.f90:242)
+                if (c->zwall && kx == 0 && kz == 0) D = 3.0 / 2.0 * D;
                 const size_t b = (size_t)kz * d.Ny * d.Nxc + kx;
                 rpiv[b] = 1.0 / D;
                 for (int r = 1; r < d.Ny; ++r) {
@@ -1442,6 +1478,15 @@ static int create_poisson_only(const dfdm_grid *g, const dfdm_params *prm, dfdm_
         if ((rc = upload_t(&c->d_dct, C))) return bail(rc);
         make_fft_plan(d.Nz, c->plan_z);
         if ((rc = tws(&c->tw_z, d.Nz, d.Nz))) return bail(rc);
+    } else if (c->zwall) {
+        make_fft_plan(d.Nx / 2, c->plan_x);
+        if ((rc = tws(&c->tw_x, d.Nx / 2, d.Nx / 2))) return bail(rc);
+        if ((rc = tws(&c->twr_x, d.Nx, d.Nx / 2 + 1))) return bail(rc);
+        make_fft_plan(d.Nz, c->plan_z);
+        if ((rc = tws(&c->tw_z, d.Nz, d.Nz))) return bail(rc);
+        std::vector<double> my((size_t)6 * (d.Ny + 3), 0.0), mz((size_t)6 * (d.Nz + 3), 0.0);
+        if ((rc = upload_t(&c->my_t, my))) return bail(rc);
+        if ((rc = upload_t(&c->mz_t, mz))) return bail(rc);
     } else {
         // the eigenmode transforms, [source index][destination index]: forward Qz(k,m) sqrt(w_k); inverse
         // Qz(k,m) / sqrt(w_k) times nzp, which the inverse x transform's division by nxp nzp takes back out
@@ -1463,7 +1508,7 @@ static int create_poisson_only(const dfdm_grid *g, const dfdm_params *prm, dfdm_
     }
     c->in_create = false;
     rc = dispatch(c, [&](auto impl) {
-        return c->duct ? decltype(impl)::setup_duct_only(c) : decltype(impl)::setup_poisson_only(c);
+        return c->xdct ? decltype(impl)::setup_poisson_only(c) : decltype(impl)::setup_duct_only(c);
     });
     if (rc) return bail(rc);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(DFDM_ERR_CUDA, "set-up synchronisation failed"));
@@ -2250,10 +2295,11 @@ int dfdm_solve_poisson(dfdm_ctx *c, const double *rhs_in, double *phi_out) {
     int rc = ensure_staging(c, n);
     if (rc) return rc;
     CK(cudaMemcpyAsync(c->staging, rhs_in, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    if (c->xdct || c->duct) {
+    if (c->xdct || c->duct || c->zwall) {
         long long before = g_launches;
         rc = dispatch(c, [&](auto impl) {
-            return c->duct ? decltype(impl)::solve_duct(c, n1, n2, n3) : decltype(impl)::solve_dct(c, n1, n2, n3);
+            typedef decltype(impl) I;
+            return c->duct ? I::solve_duct(c, n1, n2, n3) : c->zwall ? I::solve_zwall(c, n1, n2, n3) : I::solve_dct(c, n1, n2, n3);
         });
         c->launches += g_launches - before;
         if (rc) return rc;

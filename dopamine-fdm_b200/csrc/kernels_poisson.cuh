@@ -453,6 +453,45 @@ __global__ void __launch_bounds__(256) k_pack_rhs_p_bc(Dims d, int n1, int n2, i
     }
 }
 
+// ---- spanwise walls alone (z walls, periodic x and y; src/projection.f90:136-143,219-250,310-316) -------------------
+// The operator is the channel's with y and z exchanged, so the context stores the field as [y][z][x] (Dims: Ny = the
+// nz - 1 wall-bounded z cells, Nz = the nyp periodic y rows) and runs the channel's chain unchanged: x FFT, FFT along
+// the periodic axis, one tridiagonal solve per (kx, ky) along the wall axis, and the inverses.  rhs_p (x, y, z) ->
+// the swapped field:
+template <typename T>
+__global__ void __launch_bounds__(256) k_unpack_rhs_p_swap(Dims d, int n1, int n2, const double *__restrict__ in,
+                                                           T *__restrict__ f) {
+    pdl_enter();
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < d.cells; p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p % d.Nx);
+        const long long q = p / d.Nx;
+        const int kz = (int)(q % d.Ny), jy = (int)(q / d.Ny);
+        f[p] = (T)in[((long long)kz * n2 + jy) * n1 + i];
+    }
+}
+// ... and back into rhs_p's shape with the reference's copies: x (rhs_p(nxg-1) = rhs_p(2); the plane nxg as the next
+// wrap, as k_pack_rhs_p writes it), then y (rhs_p(:, nyg-1, :) = rhs_p(:, 2, :)), both over every z plane; the wall
+// plane nzg is otherwise left as passed.  On that plane each copy reads a point that no thread writes.
+template <typename T>
+__global__ void __launch_bounds__(256) k_pack_rhs_p_swap(Dims d, int n1, int n2, int n3, const T *__restrict__ f,
+                                                         double *__restrict__ out) {
+    pdl_enter();
+    const long long n = (long long)n1 * n2 * n3;
+    const int nyp = d.Nz;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p % n1);
+        const long long q = p / n1;
+        const int j = (int)(q % n2), k = (int)(q / n2);
+        if (k < d.Ny) {
+            const int ii = i % d.Nx, jj = j % nyp;
+            out[p] = (double)f[((long long)jj * d.Ny + k) * d.Nx + ii];
+        } else {
+            const int si = i == d.Nx ? 0 : i, sj = j == nyp ? 0 : j;
+            if (si != i || sj != j) out[p] = out[((long long)k * n2 + sj) * n1 + si];
+        }
+    }
+}
+
 // ---- the 4-wall duct (z walls with y walls; src/projection.f90:172-217, GPU src/poisson_gpu.f90:498-589) ----------
 // The z-eigenmode transform: out[m][col] = sum_k M[k][m] in[k][col] over the spectrum's columns col = j Nxc + kx
 // (z is the slowest index, so each k is one contiguous row of Ny Nxc complex values).  Forward, M[k][m] =

@@ -344,6 +344,13 @@ def duct(nx: int = 18, ny: int = 17, nz: int = 18, grid_type: int = 2, name: Opt
                 alpha_grid=2.0, y_bc_type=1, z_bc_type=1, nu=0.01, dt=0.002, ic="zero")
 
 
+def spanwise_wall(nx: int = 18, ny: int = 18, nz: int = 18, name: Optional[str] = None) -> Case:
+    """Spanwise walls alone (z_bc_type = 1 with periodic x and y), 3 x 2 x 1.5: the pressure solve of the z-wall path
+    (src/projection.f90:136-143,219-250) only; such a case does not step."""
+    return Case(name=name or f"spanwise_wall{nx}", nx=nx, ny=ny, nz=nz, Lx_i=3.0, Ly_i=2.0, Lz_i=1.5, grid_type=1,
+                y_bc_type=0, z_bc_type=1, nu=0.01, dt=0.002, ic="zero")
+
+
 CONFIGS = {"tgv64": tgv, "chan180": chan180, "les395": les395, "chan550": chan550,
            "tgv_small": tgv_small, "chan_small": chan_small, "chan_les_amd_small": chan_les_amd_small,
            "chan_les_vreman_small": chan_les_vreman_small}

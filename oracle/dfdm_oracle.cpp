@@ -1089,7 +1089,39 @@ struct Oracle {
 #pragma omp parallel for
             for (long ij = 0; ij < n1 * n2; ++ij) fz.exec(&c[(size_t)ij], n1 * n2, false);
         }
-        if (z_bc_type == 1) {
+        if (z_bc_type == 1 && y_bc_type == 0) {
+            // spanwise walls alone (src/projection.f90:136-143, 219-250, 310-316): FFT in y over the nyp independent
+            // rows, one z-tridiagonal solve per (kx, ky) with Dzz and kxx + kyy, the (0,0) mode pinned as the y-wall
+            // branch pins its own, then the inverse y FFT and / nyp (the row nyp+1 rides through untransformed and
+            // is replaced by the periodic y copy below)
+            const int nyp = nym - 1, nr = (int)n3;
+#pragma omp parallel for
+            for (long k = 0; k < n3; ++k)
+                for (long i = 0; i < n1; ++i) fy.exec(&c[id(i, 0, k)], n1, false);
+            long swaps = 0; int info_max = 0;
+#pragma omp parallel for reduction(+ : swaps) reduction(max : info_max)
+            for (long j = 0; j < nyp; ++j) {
+                std::vector<cplx> DL(nr), D(nr), DU(nr), B(nr);
+                for (long i = 0; i < n1; ++i) {
+                    for (int k = 2; k <= nzg - 2; ++k) { DL[k - 2] = Dzz_l[k + 1]; DU[k - 2] = Dzz_u[k]; }
+                    const double wavenum_sum = kxx[i] + kyy[j];
+                    for (int k = 2; k <= nzg - 1; ++k) D[k - 2] = Dzz_d[k] + wavenum_sum;
+                    if (x_bc_type == 0 && i == 0 && j == 0) D[0] = 3.0 / 2.0 * D[0];
+                    for (int k = 0; k < nr; ++k) B[k] = c[id(i, j, k)];
+                    long sw = 0;
+                    const int info = zgtsv(nr, DL.data(), D.data(), DU.data(), B.data(), &sw);
+                    swaps += sw; info_max = std::max(info_max, info);
+                    for (int k = 0; k < nr; ++k) c[id(i, j, k)] = B[k];
+                }
+            }
+            gtsv_swaps += swaps; last_info = info_max;
+#pragma omp parallel for
+            for (long k = 0; k < n3; ++k)
+                for (long i = 0; i < n1; ++i) fy.exec(&c[id(i, 0, k)], n1, true);
+            for (long k = 0; k < n3; ++k)
+                for (long j = 0; j < nyp; ++j)
+                    for (long i = 0; i < n1; ++i) c[id(i, j, k)] = c[id(i, j, k)] / (double)nyp;
+        } else if (z_bc_type == 1) {
             // 4-wall duct (src/projection.f90:172-217): per x mode, project onto the eigenbasis after scaling by
             // sqrt(cell width), one y-tridiagonal solve per eigenmode with lambda_z(m) in place of kzz, then
             // unproject and unscale

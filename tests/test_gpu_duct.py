@@ -6,8 +6,8 @@ import pytest
 
 from dfdm.native import DfdmError, Solver
 
-from test_oracle_duct import duct_rhs, operator
-from dfdm.cases import duct
+from test_oracle_duct import duct_rhs, operator, spanwise_rhs
+from dfdm.cases import duct, spanwise_wall
 
 pytestmark = pytest.mark.gpu
 
@@ -96,10 +96,29 @@ def test_duct_context_refuses_the_stepping_entry_points():
         s.synchronize()
 
 
-def test_duct_needs_periodic_x_and_y_walls():
+def test_z_walls_need_periodic_x():
     with pytest.raises(DfdmError) as e:
         Solver(duct().with_(x_bc_type=1), "fp32")
     assert e.value.code == DFDM_ERR_UNSUPPORTED
     with pytest.raises(DfdmError) as e:
-        Solver(duct().with_(y_bc_type=0), "fp32")
+        Solver(spanwise_wall().with_(x_bc_type=1), "fp32")
     assert e.value.code == DFDM_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32", 1e-5)])
+@pytest.mark.parametrize("nx,ny,nz", [(18, 18, 18), (34, 26, 40), (66, 34, 130), (130, 98, 66)])
+def test_spanwise_wall_poisson_matches_the_oracle(oracle_mod, prec, tol, nx, ny, nz):
+    """Spanwise walls with periodic x and y (src/projection.f90:136-143,219-250): against the oracle, and the copies the
+    reference makes (x, then y, over every z plane) with the z-wall plane otherwise as passed."""
+    c = spanwise_wall(nx, ny, nz)
+    o = oracle_mod.Oracle(c)
+    rhs, _ = spanwise_rhs(o, c, nx + ny + nz)
+    want = o.solve_poisson(rhs)
+    o.close()
+    with Solver(c, prec) as s:
+        got = s.solve_poisson_equation(rhs)
+    Nx, nyp, Nz = nx - 2, ny - 2, nz - 1
+    assert rel_l2(got[:Nx, :nyp, :Nz], want[:Nx, :nyp, :Nz]) <= tol
+    assert np.array_equal(got[Nx], got[0])
+    assert np.array_equal(got[:, nyp, :], got[:, 0, :])
+    assert np.array_equal(got[:Nx + 1, :, Nz], want[:Nx + 1, :, Nz])

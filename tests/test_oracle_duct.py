@@ -10,7 +10,7 @@ import sys
 import numpy as np
 import pytest
 
-from dfdm.cases import duct
+from dfdm.cases import duct, spanwise_wall
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -74,4 +74,45 @@ def test_duct_solution_satisfies_the_discrete_problem(oracle_mod, nx, ny, nz, gr
     # no z copy with a z wall: the plane nzg keeps its input, except for the x copy, which covers every z plane
     assert np.array_equal(phi[:Nx, :, Nz], rhs[:Nx, :, Nz])
     assert np.array_equal(phi[Nx + 1, :, Nz], rhs[Nx + 1, :, Nz])
+    o.close()
+
+
+def spanwise_operator(o, p, dx, dy):
+    """The discrete Laplacian of the spanwise-wall solve (x: Nx periodic cells, y: nyp periodic rows, z: Nz planes)."""
+    dzz, lz, uz = o.grid_array(10), o.grid_array(11), o.grid_array(12)
+    out = (np.roll(p, -1, axis=0) - 2.0 * p + np.roll(p, 1, axis=0)) / dx**2
+    out += (np.roll(p, -1, axis=1) - 2.0 * p + np.roll(p, 1, axis=1)) / dy**2
+    out += dzz[None, None, :] * p
+    out[:, :, 1:] += lz[None, None, 1:] * p[:, :, :-1]
+    out[:, :, :-1] += uz[None, None, :-1] * p[:, :, 1:]
+    return out
+
+
+def spanwise_rhs(o, c, seed):
+    """rhs_p in the reference's shape whose solved part is the spanwise-wall operator applied to a random field."""
+    Nx, nyp, Nz = c.nx - 2, c.ny - 2, c.nz - 1
+    rng = np.random.default_rng(seed)
+    rhs = np.asfortranarray(rng.standard_normal((c.nx, c.ny - 1, c.nz)))
+    q = rng.standard_normal((Nx, nyp, Nz))
+    rhs[:Nx, :nyp, :Nz] = spanwise_operator(o, q, o.grid_array(7)[0], c.Ly_i / (c.ny - 1))
+    return rhs, q
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(18, 18, 18), (34, 26, 40)])
+def test_spanwise_wall_solution_satisfies_the_discrete_problem(oracle_mod, nx, ny, nz):
+    """Spanwise walls with periodic x and y (src/projection.f90:219-250): FFT in x and y, a z-tridiagonal solve per
+    (kx, ky); the solution satisfies the operator, and the periodic copies and the untouched z-wall plane are as the
+    reference leaves them (x copy, then y copy, both over every plane)."""
+    c = spanwise_wall(nx, ny, nz)
+    o = oracle_mod.Oracle(c)
+    Nx, nyp, Nz = nx - 2, ny - 2, nz - 1
+    rhs, q = spanwise_rhs(o, c, 11)
+    phi = o.solve_poisson(rhs)
+    res = spanwise_operator(o, phi[:Nx, :nyp, :Nz], o.grid_array(7)[0], c.Ly_i / (ny - 1)) - rhs[:Nx, :nyp, :Nz]
+    assert np.max(np.abs(res)) <= 1e-10 * np.max(np.abs(rhs[:Nx, :nyp, :Nz])), np.max(np.abs(res))
+    e = phi[:Nx, :nyp, :Nz] - q
+    assert np.max(np.abs(e - e.mean())) <= 1e-10 * np.max(np.abs(q))
+    assert np.array_equal(phi[Nx], phi[0])               # x copy
+    assert np.array_equal(phi[:, nyp, :], phi[:, 0, :])   # y copy
+    assert np.array_equal(phi[:Nx, :nyp, Nz], rhs[:Nx, :nyp, Nz])   # the z-wall plane keeps its input
     o.close()
