@@ -710,6 +710,28 @@ def main():
                         "pinned_ms_per_solve": best_pinned * 1e3}
         out["duct_poisson"] = dp
 
+        # spanwise walls alone (256 x 128 x 129 independent cells: periodic x and y, z walls)
+        cc = cases.spanwise_wall(258, 130, 130)
+        o = oracle.Oracle(cc)
+        rng = np.random.default_rng(131)
+        rhs = np.asfortranarray(rng.standard_normal(cc.shapes()["rhs_p"]))
+        t0 = time.perf_counter()
+        want = o.solve_poisson(rhs)
+        t_oracle = time.perf_counter() - t0
+        o.close()
+        Nx, nyp, Nz = cc.nx - 2, cc.ny - 2, cc.nz - 1
+        sw = {"grid": [Nx, nyp, Nz], "oracle_s_per_solve": t_oracle, "path": io["path"]}
+        for prec in ("fp32", "fp64"):
+            with Solver(cc, prec) as sv:
+                got = np.zeros_like(rhs, order="F")
+                best = poisson_call_time(lambda: sv.solve_poisson_equation(rhs, out=got))
+                best_pinned = poisson_call_time(pinned_solve(sv, rhs))
+            err = float(np.linalg.norm((got[:Nx, :nyp, :Nz] - want[:Nx, :nyp, :Nz]).ravel()) /
+                        np.linalg.norm(want[:Nx, :nyp, :Nz].ravel()))
+            sw[prec] = {"ms_per_solve": best * 1e3, "cells_per_s": Nx * nyp * Nz / best, "rel_l2_vs_oracle": err,
+                        "pinned_ms_per_solve": best_pinned * 1e3}
+        out["spanwise_wall_poisson"] = sw
+
     # ---- serving stream ----
     if not args.no_serve:
         def gather(obj):

@@ -54,7 +54,7 @@ typedef struct dfdm_grid {
     const double *z;           /* z(1:nz) face coordinates, uniform */
     int x_bc_type;             /* 0 periodic; 1 inflow/outflow (a context for dfdm_solve_poisson only, see below) */
     int y_bc_type;             /* 0 periodic, 1 walls */
-    int z_bc_type;             /* 0 periodic; 1 walls (with y walls: the 4-wall duct, a context for dfdm_solve_poisson only) */
+    int z_bc_type;             /* 0 periodic; 1 walls (a context for dfdm_solve_poisson only: the duct or spanwise walls) */
     int bc_face_ylo, bc_face_yhi; /* 1 no-slip (the only value on this path) */
 } dfdm_grid;
 
@@ -101,7 +101,9 @@ const char *dfdm_version(void);
  * z_bc_type = 1 with y walls and periodic x (the 4-wall duct; nz - 1 <= 512) likewise creates a context for the
  * duct's pressure solve alone (src/projection.f90:172-217): the z-eigenmode transform of Dzz (diagonalised once here,
  * as the reference's dstev call at src/initialization.f90:579-608 does), one y-tridiagonal solve per (kx, z mode).
- * Other z-wall combinations return DFDM_ERR_UNSUPPORTED, as the reference's GPU build rejects them. */
+ * z_bc_type = 1 with periodic x and y (spanwise walls alone; nz - 1 <= 1024) creates a context for that pressure
+ * solve (src/projection.f90:136-143,219-250): FFT in x and y, one z-tridiagonal solve per (kx, ky). The reference's
+ * CPU build solves it; its GPU build rejects it. z walls with inflow/outflow x return DFDM_ERR_UNSUPPORTED. */
 int dfdm_create(const dfdm_grid *grid, const dfdm_params *params, dfdm_ctx **out);
 int dfdm_destroy(dfdm_ctx *ctx);
 /* Bytes of device memory a context of this grid and precision would hold (serving admission). */
@@ -160,7 +162,8 @@ int dfdm_compute_projection_step(dfdm_ctx *ctx, int save_p);
  * plane i = nxg keeps the input, as the reference's array does, and the z plane nzg (unset by the reference's
  * apply_periodic_xz_pressure at one rank) keeps the input too.
  * On a 4-wall duct context (z_bc_type = 1) the z direction is solved in physical space through Dzz's eigenbasis; the
- * output's z plane nzg keeps the input (no z copy with a wall) apart from the x copy rhs_p(nxg-1) = rhs_p(2). */
+ * output's z plane nzg keeps the input (no z copy with a wall) apart from the x copy rhs_p(nxg-1) = rhs_p(2); with
+ * spanwise walls (periodic y) the y copy rhs_p(:, nyg-1, :) = rhs_p(:, 2, :) covers that plane too. */
 int dfdm_solve_poisson(dfdm_ctx *ctx, const double *rhs_p_in, double *phi_out);
 /* No counterpart in the reference: dfdm_solve_poisson with no device allocation in the call.
  * dfdm_solve_poisson grows a per-context staging buffer with cudaMalloc on first use (and frees and regrows it,
