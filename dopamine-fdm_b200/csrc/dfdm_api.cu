@@ -528,7 +528,14 @@ template <typename T> struct Impl {
         cudaStream_t st = c->stream;
         k_unpack_rhs_p<T><<<reduce_grid(d), 256, 0, st>>>(d, n1, n2, c->staging, f(c->phi));
         CKL();
-        if (int rc = fwd_x(c, false, f(c->phi))) return rc;
+        // x: the FFT, or with inflow/outflow x the DCT-IV (the duct of the reference's CPU build)
+        const int nbd = (d.Ny * d.Nz + DCT_LINES - 1) / DCT_LINES, ntd = (d.Nx + 31) / 32 * 32;
+        if (c->xdct) {
+            k_dct_x<T><<<nbd, ntd, 0, st>>>(d, f(c->phi), f(c->d_dct), (C *)c->spec);
+            CKL();
+        } else if (int rc = fwd_x(c, false, f(c->phi))) {
+            return rc;
+        }
         const long long cols = (long long)d.Ny * d.Nxc;
         const dim3 g((unsigned)((cols + ZEIG_COLS - 1) / ZEIG_COLS), (unsigned)((d.Nz + zeig_modes<T>() - 1) / zeig_modes<T>()));
         k_zeig<T><<<g, ZEIG_COLS, 0, st>>>(d, (const C *)c->spec, (C *)c->spec2, f(c->d_zf));
@@ -543,9 +550,15 @@ template <typename T> struct Impl {
             k_zeig<T><<<g, ZEIG_COLS, 0, st>>>(d, (const C *)c->spec, (C *)c->spec2, f(c->d_zi));
             CKL();
         }
-        if (int rc = launch(c, 6, 1)) return rc;
-        k_pack_rhs_p_bc<T><<<(int)std::min<size_t>((n + 255) / 256, 148 * 8), 256, 0, st>>>(d, n1, n2, n3, 1, 0, f(c->phi),
-                                                                                           c->staging);
+        if (c->xdct) {
+            const T inv_norm = (T)(1.0 / (2.0 * (double)d.Nx * (double)d.Nz));   // the nzp cancels the inverse matrix's
+            k_idct_x<T><<<nbd, ntd, 0, st>>>(d, (const C *)c->spec, f(c->d_dct), inv_norm, f(c->phi));
+            CKL();
+        } else if (int rc = launch(c, 6, 1)) {
+            return rc;
+        }
+        k_pack_rhs_p_bc<T><<<(int)std::min<size_t>((n + 255) / 256, 148 * 8), 256, 0, st>>>(d, n1, n2, n3, c->xdct ? 0 : 1,
+                                                                                           0, f(c->phi), c->staging);
         CKL();
         return DFDM_OK;
     }
@@ -1185,9 +1198,9 @@ int validate(const dfdm_grid *g, const dfdm_params *p) {
         return fail(DFDM_ERR_UNSUPPORTED, "x_bc_type must be 0 (periodic) or 1 (inflow/outflow) and z_bc_type 0 (periodic) "
                                           "or 1 (walls)");
     if (g->z_bc_type == 1) {   // the 4-wall duct's Poisson path (src/initialization.f90:98-100)
-        if (g->x_bc_type != 0)
-            return fail(DFDM_ERR_UNSUPPORTED, "ERROR: GPU_POISSON build only supports z_bc_type=1 (spanwise wall) with "
-                                              "x_bc_type=0 (periodic x)");
+        if (g->x_bc_type != 0 && g->y_bc_type != 1)   // inflow/outflow x with z walls: the duct only (CPU build)
+            return fail(DFDM_ERR_UNSUPPORTED, "spanwise walls with inflow/outflow x are not built: z_bc_type=1 with "
+                                              "x_bc_type=1 needs y walls (the 4-wall duct)");
         if (g->y_bc_type == 1 && g->nz - 1 > ZEIG_NMAX)
             return fail(DFDM_ERR_UNSUPPORTED, "4-wall duct: at most " + std::to_string(ZEIG_NMAX) + " z cells (nz <= " +
                                                   std::to_string(ZEIG_NMAX + 1) + ")");
@@ -1247,6 +1260,10 @@ bool fuse_eligible(const dfdm_params *p) {
 // Bytes of the buffers dfdm_create carves from the context's arena (every sub-allocation 256-byte aligned).
 size_t arena_bytes(const dfdm_grid *g, const dfdm_params *p) {
     size_t ts = p->precision == DFDM_FP64 ? 8 : 4;
+    if (g->x_bc_type == 1 && g->z_bc_type == 1) {   // the inflow/outflow duct: the DCT and the duct's buffers together
+        size_t Nx = g->nx - 1, Nz = g->nz - 1, Ny = g->ny - 1;
+        return Nx * Ny * Nz * ts + Nx * Ny * Nz * (4 * ts + 8) + Nx * Nx * 8 + 2 * Nz * Nz * ts + (1 << 20);
+    }
     if (g->x_bc_type == 1) {   // the DCT-IV Poisson context: phi, the spectrum, the pivot table, the DCT matrix
         size_t Nx = g->nx - 1, Nz = g->nz - 2, Ny = g->ny - 1;
         return Nx * Ny * Nz * (ts + 2 * ts + 8) + Nx * Nx * 8 + (1 << 20);
@@ -1448,7 +1465,7 @@ static int create_poisson_only(const dfdm_grid *g, const dfdm_params *prm, dfdm_
                 const double lam = kxx[kx] + lz;
                 double D = di[0] + lam;
                 // the duct's null mode: kx = 0 with the zero eigenvalue, found by magnitude (src/projection.f90:206)
-                if (c->duct && kx == 0 && std::fabs(lz) < 1e-8 * lmax) D = 3.0 / 2.0 * D;
+                if (c->duct && !c->xdct && kx == 0 && std::fabs(lz) < 1e-8 * lmax) D = 3.0 / 2.0 * D;
                 // spanwise walls: the (kx, ky) = (0, 0) system, as the y-wall branch pins its own (src/projection.f90:242)
                 if (c->zwall && kx == 0 && kz == 0) D = 3.0 / 2.0 * D;
                 const size_t b = (size_t)kz * d.Ny * d.Nxc + kx;
@@ -1469,27 +1486,28 @@ static int create_poisson_only(const dfdm_grid *g, const dfdm_params *prm, dfdm_
     auto tws = [&](void **dst, int n, int count) {
         return c->prec == DFDM_FP64 ? upload_twiddles<double>(c, dst, n, count) : upload_twiddles<float>(c, dst, n, count);
     };
-    if (c->xdct) {   // C[k][n] = 2 cos(pi (2n+1)(2k+1) / (4 nxp)), the angle reduced exactly modulo 2 pi (8 nxp quarter-steps)
+    // the x transform: the DCT-IV matrix, C[k][n] = 2 cos(pi (2n+1)(2k+1) / (4 nxp)) with the angle reduced exactly
+    // modulo 2 pi (8 nxp quarter-steps); or the real-to-complex FFT, whose kernels take the metric views of the full
+    // step (zeroed here, and never read by the transforms)
+    if (c->xdct) {
         const long P = 8L * nxp;
         std::vector<double> cs((size_t)P), C((size_t)(nxp * nxp));
         for (long m = 0; m < P; ++m) cs[(size_t)m] = std::cos(PI * (double)m / (4.0 * (double)nxp));
         for (long k = 0; k < nxp; ++k)
             for (long n = 0; n < nxp; ++n) C[(size_t)(k * nxp + n)] = 2.0 * cs[(size_t)(((2 * n + 1) * (2 * k + 1)) % P)];
         if ((rc = upload_t(&c->d_dct, C))) return bail(rc);
-        make_fft_plan(d.Nz, c->plan_z);
-        if ((rc = tws(&c->tw_z, d.Nz, d.Nz))) return bail(rc);
-    } else if (c->zwall) {
+    } else {
         make_fft_plan(d.Nx / 2, c->plan_x);
         if ((rc = tws(&c->tw_x, d.Nx / 2, d.Nx / 2))) return bail(rc);
         if ((rc = tws(&c->twr_x, d.Nx, d.Nx / 2 + 1))) return bail(rc);
-        make_fft_plan(d.Nz, c->plan_z);
-        if ((rc = tws(&c->tw_z, d.Nz, d.Nz))) return bail(rc);
         std::vector<double> my((size_t)6 * (d.Ny + 3), 0.0), mz((size_t)6 * (d.Nz + 3), 0.0);
         if ((rc = upload_t(&c->my_t, my))) return bail(rc);
         if ((rc = upload_t(&c->mz_t, mz))) return bail(rc);
-    } else {
-        // the eigenmode transforms, [source index][destination index]: forward Qz(k,m) sqrt(w_k); inverse
-        // Qz(k,m) / sqrt(w_k) times nzp, which the inverse x transform's division by nxp nzp takes back out
+    }
+    // the z transform: the duct's eigenmode matrices, [source index][destination index], forward Qz(k,m) sqrt(w_k),
+    // inverse Qz(k,m) / sqrt(w_k) times nzp, which the inverse x transform's division by nxp nzp (2 nxp nzp for the
+    // DCT-IV) takes back out; or the FFT of the periodic axis (z, or y with spanwise walls)
+    if (c->duct) {
         std::vector<double> zf((size_t)nzp * nzp), zi((size_t)nzp * nzp);
         for (int k = 0; k < nzp; ++k)
             for (int m = 0; m < nzp; ++m) {
@@ -1498,13 +1516,9 @@ static int create_poisson_only(const dfdm_grid *g, const dfdm_params *prm, dfdm_
             }
         if ((rc = upload_t(&c->d_zf, zf))) return bail(rc);
         if ((rc = upload_t(&c->d_zi, zi))) return bail(rc);
-        make_fft_plan(d.Nx / 2, c->plan_x);
-        if ((rc = tws(&c->tw_x, d.Nx / 2, d.Nx / 2))) return bail(rc);
-        if ((rc = tws(&c->twr_x, d.Nx, d.Nx / 2 + 1))) return bail(rc);
-        // the x kernels take the metric views of the full step; zeroed, and never read by the transforms
-        std::vector<double> my((size_t)6 * (d.Ny + 3), 0.0), mz((size_t)6 * (d.Nz + 3), 0.0);
-        if ((rc = upload_t(&c->my_t, my))) return bail(rc);
-        if ((rc = upload_t(&c->mz_t, mz))) return bail(rc);
+    } else {
+        make_fft_plan(d.Nz, c->plan_z);
+        if ((rc = tws(&c->tw_z, d.Nz, d.Nz))) return bail(rc);
     }
     c->in_create = false;
     rc = dispatch(c, [&](auto impl) {

@@ -344,6 +344,14 @@ def duct(nx: int = 18, ny: int = 17, nz: int = 18, grid_type: int = 2, name: Opt
                 alpha_grid=2.0, y_bc_type=1, z_bc_type=1, nu=0.01, dt=0.002, ic="zero")
 
 
+def inflow_duct(nx: int = 18, ny: int = 17, nz: int = 18, grid_type: int = 2, name: Optional[str] = None) -> Case:
+    """A 4-wall duct with inflow/outflow x (x_bc_type = 1, z_bc_type = 1, y walls), 3 x 2 x 1.5: the DCT-IV x transform
+    with the z-eigenmode transform (the reference's CPU build; src/projection.f90:124-130,172-217,334-343); the
+    pressure solve only."""
+    return Case(name=name or f"inflow_duct{nx}", nx=nx, ny=ny, nz=nz, Lx_i=3.0, Ly_i=2.0, Lz_i=1.5, grid_type=grid_type,
+                alpha_grid=2.0, y_bc_type=1, x_bc_type=1, z_bc_type=1, nu=0.01, dt=0.002, ic="zero")
+
+
 def spanwise_wall(nx: int = 18, ny: int = 18, nz: int = 18, name: Optional[str] = None) -> Case:
     """Spanwise walls alone (z_bc_type = 1 with periodic x and y), 3 x 2 x 1.5: the pressure solve of the z-wall path
     (src/projection.f90:136-143,219-250) only; such a case does not step."""

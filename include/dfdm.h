@@ -103,7 +103,9 @@ const char *dfdm_version(void);
  * as the reference's dstev call at src/initialization.f90:579-608 does), one y-tridiagonal solve per (kx, z mode).
  * z_bc_type = 1 with periodic x and y (spanwise walls alone; nz - 1 <= 1024) creates a context for that pressure
  * solve (src/projection.f90:136-143,219-250): FFT in x and y, one z-tridiagonal solve per (kx, ky). The reference's
- * CPU build solves it; its GPU build rejects it. z walls with inflow/outflow x return DFDM_ERR_UNSUPPORTED. */
+ * CPU build solves it; its GPU build rejects it. x_bc_type = 1 with z_bc_type = 1 and y walls (the duct with
+ * inflow/outflow x, also the CPU build's) combines the DCT-IV x transform with the z eigenmodes; spanwise walls with
+ * inflow/outflow x return DFDM_ERR_UNSUPPORTED. */
 int dfdm_create(const dfdm_grid *grid, const dfdm_params *params, dfdm_ctx **out);
 int dfdm_destroy(dfdm_ctx *ctx);
 /* Bytes of device memory a context of this grid and precision would hold (serving admission). */

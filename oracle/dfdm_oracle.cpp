@@ -1208,8 +1208,8 @@ struct Oracle {
             for (long k = 0; k < n3; ++k)
                 for (long j = 0; j < n2; ++j)
                     for (long i = 0; i < n1; ++i) rhs_p((int)i + 2, (int)j + 2, (int)k + 2) = c[id(i, j, k)].real() / norm;
-        } else {   // real part, DCT-IV again, / (2 nxp nzp) (src/projection.f90:334-343)
-            const double norm = 2.0 * (double)nxp * (double)nzp;
+        } else {   // real part, DCT-IV again, / (2 nxp nzp), or / (2 nxp) with z walls (src/projection.f90:334-343)
+            const double norm = z_bc_type == 0 ? 2.0 * (double)nxp * (double)nzp : 2.0 * (double)nxp;
 #pragma omp parallel for
             for (long jk = 0; jk < n2 * n3; ++jk) {
                 std::vector<double> a((size_t)n1), b((size_t)n1);

@@ -10,7 +10,7 @@ import sys
 import numpy as np
 import pytest
 
-from dfdm.cases import duct, spanwise_wall
+from dfdm.cases import duct, inflow_duct, spanwise_wall
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -115,4 +115,37 @@ def test_spanwise_wall_solution_satisfies_the_discrete_problem(oracle_mod, nx, n
     assert np.array_equal(phi[Nx], phi[0])               # x copy
     assert np.array_equal(phi[:, nyp, :], phi[:, 0, :])   # y copy
     assert np.array_equal(phi[:Nx, :nyp, Nz], rhs[:Nx, :nyp, Nz])   # the z-wall plane keeps its input
+    o.close()
+
+
+def inflow_duct_operator(o, p, dx):
+    """The discrete Laplacian of the inflow/outflow duct: x with the Neumann inflow (ghost p_-1 = p_0) and Dirichlet
+    outflow (ghost p_N = -p_(N-1)) of the DCT-IV basis, Dyy and Dzz with their wall rows."""
+    dy, ly, uy = o.grid_array(5), o.grid_array(8), o.grid_array(9)
+    dzz, lz, uz = o.grid_array(10), o.grid_array(11), o.grid_array(12)
+    px = np.concatenate([p[:1], p, -p[-1:]], axis=0)
+    out = (px[2:] - 2.0 * px[1:-1] + px[:-2]) / dx**2
+    out += dy[None, :, None] * p
+    out[:, 1:, :] += ly[None, 1:, None] * p[:, :-1, :]
+    out[:, :-1, :] += uy[None, :-1, None] * p[:, 1:, :]
+    out += dzz[None, None, :] * p
+    out[:, :, 1:] += lz[None, None, 1:] * p[:, :, :-1]
+    out[:, :, :-1] += uz[None, None, :-1] * p[:, :, 1:]
+    return out
+
+
+@pytest.mark.parametrize("nx,ny,nz,grid_type", [(18, 17, 18, 2), (34, 21, 26, 1)])
+def test_inflow_duct_solution_satisfies_the_discrete_problem(oracle_mod, nx, ny, nz, grid_type):
+    """The duct with inflow/outflow x (the reference's CPU build): DCT-IV in x, z eigenmodes, one y solve per
+    (kx, mode), no null mode (the outflow is Dirichlet), x normalised by 2 nxp; the planes i = nxg and k = nzg keep
+    their input."""
+    c = inflow_duct(nx, ny, nz, grid_type)
+    o = oracle_mod.Oracle(c)
+    N, Ny, Nz = nx - 1, ny - 1, nz - 1
+    rhs = np.asfortranarray(np.random.default_rng(3).standard_normal((nx, ny - 1, nz)))
+    phi = o.solve_poisson(rhs)
+    res = inflow_duct_operator(o, phi[:N, :Ny, :Nz], o.grid_array(7)[0]) - rhs[:N, :Ny, :Nz]
+    assert np.max(np.abs(res)) <= 1e-10 * np.max(np.abs(rhs)), np.max(np.abs(res))
+    assert np.array_equal(phi[N], rhs[N])
+    assert np.array_equal(phi[:, :, Nz], rhs[:, :, Nz])
     o.close()
