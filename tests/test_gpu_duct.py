@@ -148,3 +148,27 @@ def test_spanwise_wall_poisson_matches_the_oracle(oracle_mod, prec, tol, nx, ny,
     assert np.array_equal(got[Nx], got[0])
     assert np.array_equal(got[:, nyp, :], got[:, 0, :])
     assert np.array_equal(got[:Nx + 1, :, Nz], want[:Nx + 1, :, Nz])
+
+
+@pytest.mark.parametrize("kind", ["inflow_outflow", "duct", "spanwise_wall", "inflow_duct"])
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_footprint_bounds_the_device_memory_of_a_poisson_only_context(kind, prec):
+    """dfdm_footprint_bytes is an upper bound of what a Poisson-only context holds after a solve (arena and staging)."""
+    import torch
+    from dfdm import cases
+    from dfdm.native import footprint_bytes
+    c = {"inflow_outflow": cases.inflow_outflow(258, 129, 130), "duct": cases.duct(258, 129, 130),
+         "spanwise_wall": cases.spanwise_wall(258, 130, 130), "inflow_duct": cases.inflow_duct(258, 129, 130)}[kind]
+    warm = Solver(cases.duct(18, 17, 18), "fp32")   # module and runtime set-up outside the measurement
+    rhs = np.asfortranarray(np.random.default_rng(1).standard_normal(c.shapes()["rhs_p"]))
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    s = Solver(c, prec)
+    s.solve_poisson_equation(rhs)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    used = free0 - free1
+    fp = footprint_bytes(c, prec)
+    s.close()
+    warm.close()
+    assert 0 < used <= 1.02 * fp + (8 << 20), (kind, prec, used, fp)
